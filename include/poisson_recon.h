@@ -1,0 +1,179 @@
+/*
+ * poisson_recon.h — C ABI of the B200-native screened Poisson reconstructor.
+ *
+ * Drop-in for the reference crate's one public hot path,
+ *     pub fn reconstruct(points: &[OrientedPoint], params: &ReconstructParams)
+ *         -> (Mesh, ReconstructStats)                      (src/reconstructor.rs:25)
+ * with the crate's types mirrored field for field:
+ *     OrientedPoint     src/fem_tree.rs:10  (position Point3 + normal Vec3, 6 x f64)
+ *     ReconstructParams src/reconstructor.rs:8-15
+ *     ReconstructStats  src/reconstructor.rs:17-23
+ *     Mesh              src/marching_cubes.rs:8-11 (vertices [f64;3], triangles [usize;3])
+ *
+ * All entry points return a status (PR_OK = 0, negative on failure) and never abort;
+ * the message of the last failure on the calling thread is pr_last_error().
+ * Signatures carry plain pointers and sizes only.
+ */
+#ifndef POISSON_RECON_H
+#define POISSON_RECON_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define PR_OK 0
+#define PR_ERR_INVALID_ARGUMENT -1 /* bad pointer, depth outside [1,10], non-finite input, ... */
+#define PR_ERR_OUT_OF_MEMORY -2    /* device or host allocation failed */
+#define PR_ERR_CUDA -3             /* a CUDA call failed (message names it) */
+#define PR_ERR_NOT_CONVERGED -4    /* solver hit max_iters before target_rel_residual */
+#define PR_ERR_NO_DEVICE -5        /* no usable sm_100 device */
+#define PR_ERR_STATE -6            /* accessor called before a reconstruction */
+#define PR_ERR_INTERNAL -7
+
+/* solve_mode */
+#define PR_SOLVE_CONVERGED 0          /* solve the crate's fine system to target_rel_residual */
+#define PR_SOLVE_REFERENCE_SCHEDULE 1 /* the crate's cascade: D-2 system, GS(20)+CG(cg_iters),
+                                         one-level prolongation, GS(20)+CG(cg_iters/4); GS is
+                                         8-colour (parallel) instead of sequential Morton order */
+/* precision (converged mode) */
+#define PR_PRECISION_MIXED 0 /* FP32 multigrid-preconditioned CG + FP64 residual refinement */
+#define PR_PRECISION_FP64 1  /* FP64 multigrid-preconditioned CG throughout */
+
+/* OrientedPoint (src/fem_tree.rs:10): AoS, 48 bytes. */
+typedef struct pr_oriented_point {
+  double x, y, z;    /* position (model space) */
+  double nx, ny, nz; /* normal; need not be unit length (renormalised, src/reconstructor.rs:38) */
+} pr_oriented_point;
+
+/* ReconstructParams (src/reconstructor.rs:8-11): the crate's fields in order, then
+ * extensions.  pr_params_default() gives ReconstructParams::default() for the crate's
+ * fields (src/reconstructor.rs:14). */
+typedef struct pr_params {
+  uint32_t depth;          /* octree depth D; grid res = 2^D; 1 <= D <= 10 */
+  double samples_per_node; /* accepted and ignored, as in the crate */
+  double scale;            /* s = scale / max bbox extent (src/geometry.rs:384-388) */
+  double cg_accuracy;      /* reference schedule: CG stop ||r||^2 <= ||r0||^2 acc^2 */
+  uint64_t cg_iters;       /* reference schedule: coarse CG iterations (fine: /4) */
+  double point_weight;     /* screening weight; 0 disables screening */
+  int32_t verbose;         /* print stage timings to stderr */
+  /* --- extensions --- */
+  int32_t solve_mode;         /* PR_SOLVE_* (default PR_SOLVE_CONVERGED) */
+  int32_t precision;          /* PR_PRECISION_* (default PR_PRECISION_MIXED) */
+  double target_rel_residual; /* ||b - A x||_2 / ||b||_2 in FP64 (default 1e-6) */
+  uint32_t max_iters;         /* cap on preconditioned CG iterations, all passes (default 200) */
+  uint32_t smooth_sweeps;     /* multigrid pre/post Gauss-Seidel sweeps (default 1) */
+  double inner_rel_tol;       /* mixed: relative tolerance of each FP32 inner solve (default 1e-4) */
+  uint32_t reserved[8];
+} pr_params;
+
+/* Mesh (src/marching_cubes.rs:8-11).  Vertices are model-space [x,y,z] triples; triangles
+ * are vertex-index triples (the crate's usize -> uint64).  Library-owned: free with
+ * pr_mesh_free(). */
+typedef struct pr_mesh {
+  double* vertices;
+  uint64_t n_vertices;
+  uint64_t* triangles;
+  uint64_t n_triangles;
+} pr_mesh;
+
+/* ReconstructStats (src/reconstructor.rs:17-23), then extensions. */
+typedef struct pr_stats {
+  double time_transform, time_tree, time_system, time_solve, time_extract, time_total; /* seconds */
+  uint64_t fem_nodes;  /* res^3 */
+  uint64_t matrix_nnz; /* 0: the operator is matrix-free (the crate also leaves it 0) */
+  uint64_t mesh_vertices, mesh_triangles;
+  double iso_value;
+  /* --- extensions --- */
+  double rel_residual;          /* final ||b - A x|| / ||b|| (FP64) */
+  uint32_t pcg_iterations;      /* preconditioned CG iterations, summed over passes */
+  uint32_t refinement_steps;    /* FP64 outer residual steps (mixed precision) */
+  uint64_t points_in_cube;      /* points with at least one screening node */
+  double solve_bytes;           /* algorithmic HBM bytes moved by the solve */
+  double peak_device_bytes;     /* peak device memory held by the context */
+  int32_t converged;            /* converged mode: 1 if rel_residual <= target_rel_residual */
+  int32_t reserved_i;
+  double reserved[5];
+} pr_stats;
+
+/* ------------------------------------------------------------------ one-shot API */
+pr_params pr_params_default(void);
+
+/* reconstruct(points, params) -> (mesh, stats)  (src/reconstructor.rs:25-70).
+ * points: n AoS records of 6 doubles (host memory; pinned memory is copied faster).
+ * An empty input returns PR_OK with an empty mesh and zeroed stats, like the crate.
+ * out_stats may be NULL. */
+int pr_reconstruct(const double* points6, uint64_t n, const pr_params* params, pr_mesh* out_mesh,
+                   pr_stats* out_stats);
+void pr_mesh_free(pr_mesh* mesh);
+const char* pr_last_error(void);
+
+/* ------------------------------------------------------------------ context API
+ * A context owns one device, one CUDA stream (caller-provided or its own) and the
+ * device buffers of its last reconstruction (reused by the next call).  Calls on
+ * distinct contexts are thread-safe; one context must not be used concurrently. */
+typedef struct pr_context pr_context;
+
+/* stream: a cudaStream_t, or NULL for a context-owned stream. */
+int pr_context_create(int device, void* stream, pr_context** out_ctx);
+int pr_context_destroy(pr_context* ctx);
+
+int pr_ctx_reconstruct(pr_context* ctx, const double* points6, uint64_t n, const pr_params* params,
+                       pr_mesh* out_mesh, pr_stats* out_stats);
+/* Same, input already in device memory; the mesh stays on the device (read it with
+ * pr_ctx_mesh_device / pr_ctx_mesh_copy).  Nothing is copied between host and device
+ * except a few scalars. */
+int pr_ctx_reconstruct_device(pr_context* ctx, const double* d_points6, uint64_t n, const pr_params* params,
+                              pr_stats* out_stats);
+int pr_ctx_mesh_device(pr_context* ctx, const double** d_vertices, uint64_t* n_vertices,
+                       const uint64_t** d_triangles, uint64_t* n_triangles);
+int pr_ctx_mesh_copy(pr_context* ctx, pr_mesh* out_mesh);
+int pr_ctx_synchronize(pr_context* ctx);
+
+/* --- accessors of the last reconstruction's state (parity tests, diagnostics) --- */
+/* depth, res^3, the model->unit transform (column-major 4x4, src/geometry.rs:384-402) */
+int pr_ctx_info(pr_context* ctx, uint32_t* depth, uint64_t* fem_nodes, double* model_to_unit16);
+/* FP64 solved coefficients in the crate's FEM index order (Morton, x in bit 0). */
+int pr_ctx_get_coefficients(pr_context* ctx, double* out_n);
+/* FP64 right-hand side b (src/fem_tree.rs:251-299), FEM index order. */
+int pr_ctx_get_rhs(pr_context* ctx, double* out_n);
+/* Unit-cube points (AoS x y z nx ny nz) after the transform of src/reconstructor.rs:36-40. */
+int pr_ctx_get_unit_points(pr_context* ctx, double* out_6n);
+/* Normal field after splat + normalisation (src/fem_tree.rs:130-178), dense (n x 3) and
+ * node weights (n). */
+int pr_ctx_get_normal_field(pr_context* ctx, double* out_3n, double* out_weight_n);
+/* y = A x with the fine operator of src/fem_tree.rs:180-249 (stiffness + screening),
+ * matrix-free; precision PR_PRECISION_FP64 or PR_PRECISION_MIXED (FP32 operator, FP64 I/O). */
+int pr_ctx_apply_operator(pr_context* ctx, const double* x_n, double* y_n, int precision);
+/* Evaluate the implicit function (src/fem_tree.rs:490-513) of `coefficients` (NULL = the
+ * solved ones) at unit-cube points (3 doubles each). */
+int pr_ctx_evaluate(pr_context* ctx, const double* coefficients, const double* pts3, uint64_t n, double* out);
+/* Marching cubes (src/fem_tree.rs:576-636) of given FP64 coefficients at the context's depth
+ * and the given iso value; vertices in UNIT-CUBE space (no back-transform). */
+int pr_ctx_extract(pr_context* ctx, const double* coefficients, double iso, pr_mesh* out_mesh);
+/* Same, at an explicit depth, without a prior reconstruction. */
+int pr_ctx_extract_at_depth(pr_context* ctx, uint32_t depth, const double* coefficients, double iso,
+                            pr_mesh* out_mesh);
+
+/* y = A x on device-resident vectors (n = res^3 entries, float for PR_PRECISION_MIXED,
+ * double for PR_PRECISION_FP64), enqueued on the context's stream without synchronising.
+ * For benchmarks of the operator kernel. */
+int pr_ctx_apply_operator_device(pr_context* ctx, const void* d_x, void* d_y, int precision);
+
+/* Number of kernels launched by this library in this process (own kernels; library
+ * primitives such as radix sorts and scans are counted in *primitive_calls). */
+uint64_t pr_kernel_launches(uint64_t* primitive_calls);
+
+/* Library build information (static string). */
+const char* pr_version(void);
+/* sizeof(pr_params), sizeof(pr_mesh), sizeof(pr_stats), sizeof(pr_oriented_point): lets a
+ * binding check its struct layouts without a GPU. */
+void pr_abi_layout(uint64_t* out4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POISSON_RECON_H */

@@ -1,0 +1,880 @@
+// TEST INFRASTRUCTURE ONLY — the CPU oracle for parity checks and the CPU baseline.
+//
+// A C++ FP64 restatement of the reference crate's `reconstructor::reconstruct` path
+// (Avanatiker/PoissonReconstruction, crate `poisson-recon`).  It follows the Rust
+// sources operation by operation (no FMA contraction: build with -ffp-contract=off),
+// so that a quantity computed here equals the crate's bit for bit wherever the crate's
+// own order is deterministic.  Two places where the crate's order is NOT deterministic
+// are restated with a fixed order instead:
+//   * rayon `sum()` in dot/square_norm (src/solvers.rs:6-15) and in the iso average
+//     (src/reconstructor.rs:56) — here a fixed-chunk pairwise order;
+// Nothing here is part of the shipped library; only tests/, bench.py's CPU leg and
+// the smoke check load it.
+//
+// Parity status: the crate cannot be built in this environment (no Rust toolchain),
+// so this restatement is pinned by the crate's own unit tests (ported in
+// tests/test_oracle.py) and by hand-derived known answers; the fem_tree path has no
+// golden vectors in the reference.
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define PR_MC_TABLE_QUAL static const
+#include "../poissonreconstruction_b200/csrc/mc_tri_table.inc"
+
+namespace {
+
+typedef int64_t isize;
+
+// ---------------------------------------------------------------- casts (Rust `as`)
+// f64 -> isize / u64 are saturating in Rust (NaN -> 0).
+inline isize f64_to_isize(double v) {
+  if (std::isnan(v)) return 0;
+  if (v >= 9223372036854775807.0) return INT64_MAX;
+  if (v <= -9223372036854775808.0) return INT64_MIN;
+  return (isize)v;
+}
+inline uint64_t f64_to_u64(double v) {
+  if (std::isnan(v) || v <= 0.0) return 0;
+  if (v >= 18446744073709551615.0) return UINT64_MAX;
+  return (uint64_t)v;
+}
+
+// ---------------------------------------------------------------- Morton index
+// The crate's FEM index of a max-depth leaf is its position in the depth-first order
+// of `SortedTreeNodes::collect_nodes` (src/octree.rs:235-248) with child i at offset
+// (i&1, (i>>1)&1, (i>>2)&1) (src/octree.rs:145-153): the 3-D Morton code, x in bit 0.
+inline uint64_t spread3(uint64_t v) {
+  uint64_t r = 0;
+  for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
+  return r;
+}
+inline uint64_t compact3(uint64_t v) {
+  uint64_t r = 0;
+  for (int b = 0; b < 21; ++b) r |= ((v >> (3 * b)) & 1ull) << b;
+  return r;
+}
+inline uint64_t morton(uint64_t x, uint64_t y, uint64_t z) {
+  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+inline void unmorton(uint64_t m, uint64_t& x, uint64_t& y, uint64_t& z) {
+  x = compact3(m);
+  y = compact3(m >> 1);
+  z = compact3(m >> 2);
+}
+
+// ---------------------------------------------------------------- 1-D constants
+// src/fem_tree.rs:39-41
+inline double mass_1d(isize d) { d = d < 0 ? -d : d; return d == 0 ? 2. / 3. : (d == 1 ? 1. / 6. : 0.0); }
+inline double stiff_1d(isize d) { d = d < 0 ? -d : d; return d == 0 ? 2. : (d == 1 ? -1. : 0.0); }
+inline double deriv_mass_1d(isize d) { return d == 0 ? 0. : (d == 1 ? -0.5 : (d == -1 ? 0.5 : 0.0)); }
+// src/fem_tree.rs:44-48
+inline double stiffness_entry(double h, isize dx, isize dy, isize dz) {
+  return (stiff_1d(dx) * mass_1d(dy) * mass_1d(dz) + mass_1d(dx) * stiff_1d(dy) * mass_1d(dz) +
+          mass_1d(dx) * mass_1d(dy) * stiff_1d(dz)) * h;
+}
+// src/fem_tree.rs:640-642
+inline double bspline1(double t) {
+  if (t < 0.0 || t > 2.0) return 0.0;
+  if (t <= 1.0) return t;
+  return 2.0 - t;
+}
+// src/fem_tree.rs:645-649
+inline void contributing_offsets(double s, isize res, uint32_t& o0, uint32_t& o1) {
+  isize f = f64_to_isize(std::floor(s));
+  isize a = f - 1, b = f;
+  a = a < 0 ? 0 : (a > res - 1 ? res - 1 : a);
+  b = b < 0 ? 0 : (b > res - 1 ? res - 1 : b);
+  o0 = (uint32_t)a;
+  o1 = (uint32_t)b;
+}
+
+// deterministic sum (fixed chunking, independent of the thread count)
+double det_dot(const double* a, const double* b, uint64_t n) {
+  const uint64_t CH = 4096;
+  uint64_t nch = (n + CH - 1) / CH;
+  std::vector<double> part(nch, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < (int64_t)nch; ++c) {
+    uint64_t lo = (uint64_t)c * CH, hi = std::min(n, lo + CH);
+    double s = 0.0;
+    for (uint64_t i = lo; i < hi; ++i) s += a[i] * b[i];
+    part[c] = s;
+  }
+  // pairwise combine
+  while (part.size() > 1) {
+    std::vector<double> nx((part.size() + 1) / 2);
+    for (size_t i = 0; i < nx.size(); ++i)
+      nx[i] = part[2 * i] + (2 * i + 1 < part.size() ? part[2 * i + 1] : 0.0);
+    part.swap(nx);
+  }
+  return part.empty() ? 0.0 : part[0];
+}
+
+// ---------------------------------------------------------------- CSR (src/sparse.rs)
+struct Csr {
+  uint64_t rows = 0;
+  std::vector<uint64_t> ptr;   // rows+1
+  std::vector<uint32_t> col;
+  std::vector<double> val;
+  // src/sparse.rs:105-117 — row sum in entry order, starting at 0.0
+  void spmv(const double* x, double* y) const {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)rows; ++i) {
+      double s = 0.0;
+      for (uint64_t k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * x[col[k]];
+      y[i] = s;
+    }
+  }
+};
+
+// src/solvers.rs:164-175
+void gauss_seidel_sweep(const Csr& a, const double* b, double* x) {
+  for (uint64_t i = 0; i < a.rows; ++i) {
+    double diag = 0.0, sum = 0.0;
+    for (uint64_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+      if (a.col[k] == i) diag = a.val[k];
+      else sum += a.val[k] * x[a.col[k]];
+    }
+    if (diag != 0.0) x[i] = (b[i] - sum) / diag;
+  }
+}
+
+// src/solvers.rs:20-69
+uint64_t solve_cg(const Csr& a, const double* b, double* x, uint64_t max_iters, double accuracy) {
+  uint64_t n = a.rows;
+  std::vector<double> r(n), d(n), q(n);
+  a.spmv(x, q.data());
+  for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  d = r;
+  double delta_new = det_dot(r.data(), r.data(), n);
+  double delta_0 = delta_new;
+  if (delta_new == 0.0) return 0;
+  for (uint64_t iter = 0; iter < max_iters; ++iter) {
+    a.spmv(d.data(), q.data());
+    double dq = det_dot(d.data(), q.data(), n);
+    if (dq == 0.0) return iter + 1;
+    double alpha = delta_new / dq;
+    for (uint64_t i = 0; i < n; ++i) x[i] += alpha * d[i];
+    if ((iter + 1) % 10 == 0) {
+      a.spmv(x, q.data());
+      for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+    } else {
+      for (uint64_t i = 0; i < n; ++i) r[i] -= alpha * q[i];
+    }
+    double delta_old = delta_new;
+    delta_new = det_dot(r.data(), r.data(), n);
+    if (delta_new <= delta_0 * accuracy * accuracy) return iter + 1;
+    double beta = delta_new / delta_old;
+    if (std::isnan(beta) || std::isinf(beta)) break;
+    for (uint64_t i = 0; i < n; ++i) d[i] = r[i] + beta * d[i];
+  }
+  return max_iters;
+}
+
+struct P6 { double x, y, z, nx, ny, nz; };
+
+struct KeyHash {
+  size_t operator()(const std::array<uint64_t, 3>& k) const {
+    uint64_t h = k[0] * 0x9E3779B97F4A7C15ull;
+    h ^= k[1] + 0x7F4A7C159E3779B9ull + (h << 6) + (h >> 2);
+    h ^= k[2] + 0x94D049BB133111EBull + (h << 6) + (h >> 2);
+    return (size_t)h;
+  }
+};
+
+
+// Per-row accumulation in push order, then CSR sorted by column (src/fem_tree.rs:229-248).
+struct RowBuilder {
+  uint32_t D;
+  uint64_t res, n;
+  std::vector<double> slot;      // n * 27, slot index = (dz+1)*9+(dy+1)*3+(dx+1)
+  std::vector<uint32_t> present; // n bitmasks
+  RowBuilder(uint32_t depth, bool lexicographic) : D(depth) {
+    res = 1ull << D;
+    n = res * res * res;
+    slot.assign(n * 27, 0.0);
+    present.assign(n, 0u);
+    lex = lexicographic;
+  }
+  bool lex;
+  uint64_t index(uint64_t x, uint64_t y, uint64_t z) const {
+    return lex ? (z * res + y) * res + x : morton(x, y, z);
+  }
+  void coords(uint64_t i, uint64_t& x, uint64_t& y, uint64_t& z) const {
+    if (lex) { x = i % res; y = (i / res) % res; z = i / (res * res); }
+    else unmorton(i, x, y, z);
+  }
+  void push(uint64_t i, isize dx, isize dy, isize dz, double v) {
+    int s = (int)((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
+    slot[i * 27 + s] += v;
+    present[i] |= 1u << s;
+  }
+  Csr finish() {
+    Csr a;
+    a.rows = n;
+    a.ptr.assign(n + 1, 0);
+    for (uint64_t i = 0; i < n; ++i) a.ptr[i + 1] = a.ptr[i] + __builtin_popcount(present[i]);
+    a.col.resize(a.ptr[n]);
+    a.val.resize(a.ptr[n]);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+      uint64_t x, y, z;
+      coords(i, x, y, z);
+      std::pair<uint64_t, double> e[27];
+      int m = 0;
+      for (int s = 0; s < 27; ++s) {
+        if (!(present[i] >> s & 1u)) continue;
+        isize dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+        e[m++] = {index(x + dx, y + dy, z + dz), slot[(uint64_t)i * 27 + s]};
+      }
+      std::sort(e, e + m, [](const std::pair<uint64_t, double>& a1, const std::pair<uint64_t, double>& b1) {
+        return a1.first < b1.first;
+      });
+      uint64_t p = a.ptr[i];
+      for (int k = 0; k < m; ++k) { a.col[p + k] = (uint32_t)e[k].first; a.val[p + k] = e[k].second; }
+    }
+    std::vector<double>().swap(slot);
+    return a;
+  }
+};
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+struct orc_tree {
+  uint32_t D;
+  uint64_t res, n;
+  double h;
+  std::vector<P6> pts;          // unit-cube points
+  std::vector<double> nf;       // 3n normal field (after normalisation)
+  std::vector<double> nw;       // n node weights
+  Csr A;
+  bool have_A = false;
+  double pw_A = -1.0;
+};
+
+struct orc_mesh {
+  double* verts;   // 3*nv
+  uint64_t nv;
+  uint64_t* tris;  // 3*nt
+  uint64_t nt;
+};
+
+struct orc_params {
+  uint32_t depth;
+  double scale;
+  double cg_accuracy;
+  uint64_t cg_iters;
+  double point_weight;
+  int32_t solve_mode;        // 0 = reference schedule, 1 = converged
+  double target_rel_residual;
+  uint64_t max_iters;
+};
+
+struct orc_stats {
+  double iso_value;
+  uint64_t fem_nodes, mesh_vertices, mesh_triangles;
+  double rel_residual;
+  uint64_t iterations;
+  double time_tree, time_solve, time_extract, time_total;
+};
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+double orc_bspline1(double t) { return bspline1(t); }
+double orc_stiffness_entry(double h, int dx, int dy, int dz) { return stiffness_entry(h, dx, dy, dz); }
+uint64_t orc_morton(uint64_t x, uint64_t y, uint64_t z) { return morton(x, y, z); }
+
+// Mesh edge mask of a marching-cubes case: edge e (corners a,b of src/fem_tree.rs:585)
+// is cut iff the two corners classify differently.  Equals the crate's EDGE_TABLE.
+uint32_t orc_mc_edge_mask(uint32_t mc) {
+  static const int ev[12][2] = {{0,1},{1,2},{2,3},{3,0},{4,5},{5,6},{6,7},{7,4},{0,4},{1,5},{2,6},{3,7}};
+  uint32_t m = 0;
+  for (int e = 0; e < 12; ++e)
+    if (((mc >> ev[e][0]) & 1u) != ((mc >> ev[e][1]) & 1u)) m |= 1u << e;
+  return m;
+}
+// Triangle table row as edge indices (-1 terminated, 16 entries)
+void orc_mc_tri_row(uint32_t mc, int* out16) {
+  for (int i = 0; i < 16; ++i) out16[i] = -1;
+  for (int i = 0; i < 3 * PR_MC_NTRI[mc]; ++i) out16[i] = (int)((PR_MC_TRIS[mc] >> (4 * i)) & 15ull);
+}
+
+// ---------------------------------------------------------------- geometry
+// BBox::extend (src/geometry.rs:356-363): f64::min/max ignore NaN like fmin/fmax.
+void orc_bbox(const double* pts6, uint64_t n, double* bmin, double* bmax) {
+  for (int k = 0; k < 3; ++k) { bmin[k] = INFINITY; bmax[k] = -INFINITY; }
+  for (uint64_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      bmin[k] = std::fmin(bmin[k], pts6[6 * i + k]);
+      bmax[k] = std::fmax(bmax[k], pts6[6 * i + k]);
+    }
+}
+
+// unit_cube_transform (src/geometry.rs:384-402). m is column-major: m[col*4+row].
+void orc_unit_cube_transform(const double* bmin, const double* bmax, double scale, double* m) {
+  double c[3], s3[3];
+  for (int k = 0; k < 3; ++k) { c[k] = (bmin[k] + bmax[k]) * 0.5; s3[k] = bmax[k] - bmin[k]; }
+  double max_dim = std::fmax(std::fmax(s3[0], s3[1]), s3[2]);
+  double s = max_dim > 0.0 ? scale / max_dim : 1.0;
+  for (int i = 0; i < 16; ++i) m[i] = 0.0;
+  m[0] = s; m[5] = s; m[10] = s;
+  m[12] = -s * c[0] + 0.5; m[13] = -s * c[1] + 0.5; m[14] = -s * c[2] + 0.5; m[15] = 1.0;
+}
+
+// Mat4::inverse (src/geometry.rs:274-317)
+void orc_mat4_inverse(const double* M, double* out) {
+#define MM(col, row) M[(col) * 4 + (row)]
+  double a = MM(0,0), b = MM(1,0), c = MM(2,0);
+  double d = MM(0,1), e = MM(1,1), f = MM(2,1);
+  double g = MM(0,2), h = MM(1,2), i = MM(2,2);
+  double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+  for (int k = 0; k < 16; ++k) out[k] = 0.0;
+  if (std::fabs(det) < 1e-30) { out[0] = out[5] = out[10] = out[15] = 1.0; return; }
+  double inv_det = 1.0 / det;
+  double a_inv = (e * i - f * h) * inv_det, b_inv = (c * h - b * i) * inv_det, c_inv = (b * f - c * e) * inv_det;
+  double d_inv = (f * g - d * i) * inv_det, e_inv = (a * i - c * g) * inv_det, f_inv = (c * d - a * f) * inv_det;
+  double g_inv = (d * h - e * g) * inv_det, h_inv = (b * g - a * h) * inv_det, i_inv = (a * e - b * d) * inv_det;
+  double tx = MM(3,0), ty = MM(3,1), tz = MM(3,2);
+  double itx = -(a_inv * tx + b_inv * ty + c_inv * tz);
+  double ity = -(d_inv * tx + e_inv * ty + f_inv * tz);
+  double itz = -(g_inv * tx + h_inv * ty + i_inv * tz);
+  double cols[4][4] = {{a_inv, d_inv, g_inv, 0.0}, {b_inv, e_inv, h_inv, 0.0}, {c_inv, f_inv, i_inv, 0.0}, {itx, ity, itz, 1.0}};
+  for (int cc = 0; cc < 4; ++cc) for (int r = 0; r < 4; ++r) out[cc * 4 + r] = cols[cc][r];
+#undef MM
+}
+
+// Mat4::transform_point / transform_vector (src/geometry.rs:256-270), Vec3::normalize (:49-56)
+void orc_transform_point(const double* M, const double* p, double* out) {
+  for (int r = 0; r < 3; ++r) out[r] = M[0 * 4 + r] * p[0] + M[1 * 4 + r] * p[1] + M[2 * 4 + r] * p[2] + M[3 * 4 + r];
+}
+void orc_transform_points(const double* M, const double* pts6, uint64_t n, double* unit6) {
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < (int64_t)n; ++k) {
+    const double* p = pts6 + 6 * k;
+    double* o = unit6 + 6 * k;
+    for (int r = 0; r < 3; ++r) o[r] = M[0 * 4 + r] * p[0] + M[1 * 4 + r] * p[1] + M[2 * 4 + r] * p[2] + M[3 * 4 + r];
+    double v[3];
+    for (int r = 0; r < 3; ++r) v[r] = M[0 * 4 + r] * p[3] + M[1 * 4 + r] * p[4] + M[2 * 4 + r] * p[5];
+    double nn = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (nn > 0.0) { o[3] = v[0] / nn; o[4] = v[1] / nn; o[5] = v[2] / nn; }
+    else { o[3] = 0.0; o[4] = 0.0; o[5] = 0.0; }
+  }
+}
+
+// ---------------------------------------------------------------- tree
+// FEMTree::{initialize, finalize, splat_normal_field} (src/fem_tree.rs:83-178).
+orc_tree* orc_tree_new(uint32_t depth, const double* unit6, uint64_t npts) {
+  orc_tree* t = new orc_tree();
+  t->D = depth;
+  t->res = 1ull << depth;
+  t->n = t->res * t->res * t->res;
+  t->h = 1.0 / (double)t->res;
+  t->pts.resize(npts);
+  std::memcpy(t->pts.data(), unit6, npts * sizeof(P6));
+  t->nf.assign(3 * t->n, 0.0);
+  t->nw.assign(t->n, 0.0);
+  const double h = t->h;
+  const uint64_t res = t->res;
+  for (const P6& pt : t->pts) {
+    isize cx = f64_to_isize(std::floor(pt.x / h));
+    isize cy = f64_to_isize(std::floor(pt.y / h));
+    isize cz = f64_to_isize(std::floor(pt.z / h));
+    double tx = pt.x / h - (double)cx, ty = pt.y / h - (double)cy, tz = pt.z / h - (double)cz;
+    double bx0 = 1.0 - tx, bx1 = tx, by0 = 1.0 - ty, by1 = ty, bz0 = 1.0 - tz, bz1 = tz;
+    for (isize dz = 0; dz <= 1; ++dz)
+      for (isize dy = 0; dy <= 1; ++dy)
+        for (isize dx = 0; dx <= 1; ++dx) {
+          uint64_t ox = (uint64_t)(cx + dx), oy = (uint64_t)(cy + dy), oz = (uint64_t)(cz + dz);
+          if (ox >= res || oy >= res || oz >= res) continue;
+          uint64_t idx = morton(ox, oy, oz);
+          double bx = dx == 0 ? bx0 : bx1, by = dy == 0 ? by0 : by1, bz = dz == 0 ? bz0 : bz1;
+          double w = bx * by * bz;
+          t->nf[3 * idx + 0] += pt.nx * w;
+          t->nf[3 * idx + 1] += pt.ny * w;
+          t->nf[3 * idx + 2] += pt.nz * w;
+          t->nw[idx] += w;
+        }
+  }
+  for (uint64_t i = 0; i < t->n; ++i) {
+    if (t->nw[i] > 0.0) {
+      double inv = 1.0 / t->nw[i];
+      t->nf[3 * i + 0] = -t->nf[3 * i + 0] * inv;
+      t->nf[3 * i + 1] = -t->nf[3 * i + 1] * inv;
+      t->nf[3 * i + 2] = -t->nf[3 * i + 2] * inv;
+    }
+  }
+  return t;
+}
+
+void orc_tree_free(orc_tree* t) { delete t; }
+uint64_t orc_tree_nodes(const orc_tree* t) { return t->n; }
+
+void orc_tree_normal_field(const orc_tree* t, double* nf3, double* w) {
+  std::memcpy(nf3, t->nf.data(), 3 * t->n * sizeof(double));
+  std::memcpy(w, t->nw.data(), t->n * sizeof(double));
+}
+
+// trunc-cell basis of one point, as in assemble_system / assemble_rhs (src/fem_tree.rs:207-219, :283-295)
+static int screening_basis(const orc_tree* t, const P6& pt, uint64_t* idx, double* bx_, double* by_, double* bz_,
+                           int* cdx = nullptr, int* cdy = nullptr, int* cdz = nullptr) {
+  const double h = t->h;
+  isize cx = f64_to_isize(pt.x / h), cy = f64_to_isize(pt.y / h), cz = f64_to_isize(pt.z / h);
+  double tx = pt.x / h - (double)cx, ty = pt.y / h - (double)cy, tz = pt.z / h - (double)cz;
+  double bx0 = 1. - tx, bx1 = tx, by0 = 1. - ty, by1 = ty, bz0 = 1. - tz, bz1 = tz;
+  int m = 0;
+  for (isize dz = 0; dz <= 1; ++dz)
+    for (isize dy = 0; dy <= 1; ++dy)
+      for (isize dx = 0; dx <= 1; ++dx) {
+        uint32_t ox = (uint32_t)(uint64_t)(cx + dx), oy = (uint32_t)(uint64_t)(cy + dy), oz = (uint32_t)(uint64_t)(cz + dz);
+        if (ox >= (uint32_t)t->res || oy >= (uint32_t)t->res || oz >= (uint32_t)t->res) continue;
+        idx[m] = morton(ox, oy, oz);
+        bx_[m] = dx == 0 ? bx0 : bx1;
+        by_[m] = dy == 0 ? by0 : by1;
+        bz_[m] = dz == 0 ? bz0 : bz1;
+        if (cdx) { cdx[m] = (int)dx; cdy[m] = (int)dy; cdz[m] = (int)dz; }
+        ++m;
+      }
+  return m;
+}
+
+// FEMTree::assemble_rhs (src/fem_tree.rs:251-299)
+void orc_tree_rhs(const orc_tree* t, double pw, double* rhs) {
+  const uint64_t res = t->res;
+  const double h = t->h;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)t->n; ++i) {
+    uint64_t ix, iy, iz;
+    unmorton(i, ix, iy, iz);
+    double sum = 0.0;
+    for (isize dx = -1; dx <= 1; ++dx)
+      for (isize dy = -1; dy <= 1; ++dy)
+        for (isize dz = -1; dz <= 1; ++dz) {
+          isize jx = (isize)ix + dx, jy = (isize)iy + dy, jz = (isize)iz + dz;
+          if (jx < 0 || jx >= (isize)res || jy < 0 || jy >= (isize)res || jz < 0 || jz >= (isize)res) continue;
+          uint64_t j = morton(jx, jy, jz);
+          const double* v = &t->nf[3 * j];
+          sum += h * h * (v[0] * deriv_mass_1d(dx) * mass_1d(dy) * mass_1d(dz) +
+                          v[1] * mass_1d(dx) * deriv_mass_1d(dy) * mass_1d(dz) +
+                          v[2] * mass_1d(dx) * mass_1d(dy) * deriv_mass_1d(dz));
+        }
+    rhs[i] = sum;
+  }
+  if (pw > 0.0) {
+    double wh3 = pw * (h * h * h) / 1.5;
+    double target = 0.5;
+    for (const P6& pt : t->pts) {
+      uint64_t idx[8];
+      double bx[8], by[8], bz[8];
+      int m = screening_basis(t, pt, idx, bx, by, bz);
+      for (int k = 0; k < m; ++k) rhs[idx[k]] += wh3 * target * bx[k] * by[k] * bz[k];
+    }
+  }
+}
+
+// FEMTree::assemble_system (src/fem_tree.rs:180-249); returns nnz
+int64_t orc_tree_assemble(orc_tree* t, double pw) {
+  const uint64_t res = t->res;
+  const double h = t->h;
+  RowBuilder rb(t->D, false);
+  for (uint64_t i = 0; i < t->n; ++i) {
+    uint64_t ix, iy, iz;
+    unmorton(i, ix, iy, iz);
+    for (isize dx = -1; dx <= 1; ++dx)
+      for (isize dy = -1; dy <= 1; ++dy)
+        for (isize dz = -1; dz <= 1; ++dz) {
+          isize jx = (isize)ix + dx, jy = (isize)iy + dy, jz = (isize)iz + dz;
+          if (jx < 0 || jx >= (isize)res || jy < 0 || jy >= (isize)res || jz < 0 || jz >= (isize)res) continue;
+          double val = stiffness_entry(h, dx, dy, dz);
+          if (val != 0.0) rb.push(i, dx, dy, dz, val);
+        }
+  }
+  if (pw > 0.0) {
+    double wh3 = pw * (h * h * h) / 1.5;
+    double wg = wh3 * 0.005;
+    for (uint64_t i = 0; i < t->n; ++i) rb.push(i, 0, 0, 0, wg);
+    for (const P6& pt : t->pts) {
+      uint64_t idx[8];
+      double bx[8], by[8], bz[8];
+      int cdx[8], cdy[8], cdz[8];
+      int m = screening_basis(t, pt, idx, bx, by, bz, cdx, cdy, cdz);
+      double phi[8];
+      for (int k = 0; k < m; ++k) phi[k] = bx[k] * by[k] * bz[k];
+      for (int a = 0; a < m; ++a)
+        for (int b = 0; b < m; ++b)
+          rb.push(idx[a], (isize)cdx[b] - (isize)cdx[a], (isize)cdy[b] - (isize)cdy[a], (isize)cdz[b] - (isize)cdz[a],
+                  wh3 * phi[a] * phi[b]);
+    }
+  }
+  t->A = rb.finish();
+  t->have_A = true;
+  t->pw_A = pw;
+  return (int64_t)t->A.ptr[t->n];
+}
+
+void orc_tree_csr(const orc_tree* t, uint64_t* ptr, uint32_t* col, double* val) {
+  std::memcpy(ptr, t->A.ptr.data(), (t->n + 1) * sizeof(uint64_t));
+  std::memcpy(col, t->A.col.data(), t->A.col.size() * sizeof(uint32_t));
+  std::memcpy(val, t->A.val.data(), t->A.val.size() * sizeof(double));
+}
+
+int orc_tree_spmv(const orc_tree* t, const double* x, double* y) {
+  if (!t->have_A) return -1;
+  t->A.spmv(x, y);
+  return 0;
+}
+
+// FEMTree::build_system_at_depth (src/fem_tree.rs:346-404), lexicographic coarse index.
+static void build_system_at_depth(const orc_tree* t, uint32_t depth, double pw, Csr& A, std::vector<double>& rhs) {
+  const uint64_t res = 1ull << depth;
+  const double h = 1.0 / (double)res;
+  const uint64_t n = res * res * res;
+  double scale_factor = (double)(1ull << (2 * (t->D - depth)));
+  double effective_pw = pw * scale_factor;
+  RowBuilder rb(depth, true);
+  for (uint64_t z = 0; z < res; ++z)
+    for (uint64_t y = 0; y < res; ++y)
+      for (uint64_t x = 0; x < res; ++x) {
+        uint64_t i = (z * res + y) * res + x;
+        for (isize dz = -1; dz <= 1; ++dz)
+          for (isize dy = -1; dy <= 1; ++dy)
+            for (isize dx = -1; dx <= 1; ++dx) {
+              isize jx = (isize)x + dx, jy = (isize)y + dy, jz = (isize)z + dz;
+              if (jx < 0 || jx >= (isize)res || jy < 0 || jy >= (isize)res || jz < 0 || jz >= (isize)res) continue;
+              double v = stiffness_entry(h, dx, dy, dz);
+              if (v != 0.0) rb.push(i, dx, dy, dz, v);
+            }
+        if (effective_pw > 0.0) {
+          double wh3 = effective_pw * (h * h * h) / 1.5;
+          rb.push(i, 0, 0, 0, wh3 * 1.005);
+        }
+      }
+  A = rb.finish();
+  rhs.assign(n, 0.0);
+  for (uint64_t i = 0; i < t->n; ++i) {
+    uint64_t fx, fy, fz;
+    unmorton(i, fx, fy, fz);
+    uint64_t cx = fx >> (t->D - depth), cy = fy >> (t->D - depth), cz = fz >> (t->D - depth);
+    uint64_t ci = (cz * res + cy) * res + cx;
+    if (ci < n) rhs[ci] += t->nf[3 * i] + t->nf[3 * i + 1] + t->nf[3 * i + 2];
+  }
+  if (effective_pw > 0.0) {
+    double wh3 = effective_pw * (h * h * h) / 1.5;
+    for (uint64_t i = 0; i < n; ++i) rhs[i] += wh3 * 0.5;
+  }
+}
+
+// FEMTree::prolongate (src/fem_tree.rs:310-343): one-level stencil, whatever the gap.
+static void prolongate(const orc_tree* t, const std::vector<double>& coarse, uint32_t coarse_depth, std::vector<double>& fine) {
+  const isize fine_res = (isize)t->res;
+  const uint64_t cres = 1ull << coarse_depth;
+  fine.assign(t->n, 0.0);
+  const double bw[3] = {0.5, 1.0, 0.5};
+  for (uint64_t cz = 0; cz < cres; ++cz)
+    for (uint64_t cy = 0; cy < cres; ++cy)
+      for (uint64_t cx = 0; cx < cres; ++cx) {
+        uint64_t ci = (cz * cres + cy) * cres + cx;
+        if (ci >= coarse.size()) continue;
+        double v = coarse[ci];
+        if (v == 0.0) continue;
+        for (isize dz = 0; dz <= 2; ++dz) {
+          isize fz = (isize)cz * 2 + dz - 1;
+          if (fz < 0 || fz >= fine_res) continue;
+          for (isize dy = 0; dy <= 2; ++dy) {
+            isize fy = (isize)cy * 2 + dy - 1;
+            if (fy < 0 || fy >= fine_res) continue;
+            for (isize dx = 0; dx <= 2; ++dx) {
+              isize fx = (isize)cx * 2 + dx - 1;
+              if (fx < 0 || fx >= fine_res) continue;
+              double w = bw[dx] * bw[dy] * bw[dz];
+              fine[morton(fx, fy, fz)] += v * w;
+            }
+          }
+        }
+      }
+}
+
+// FEMTree::solve_cascadic (src/fem_tree.rs:458-487) with gs = 20 and base depth D-2
+// (src/reconstructor.rs:51-52).  x receives the fine solution.  info[0] = coarse CG
+// iterations, info[1] = fine CG iterations.
+int orc_tree_solve_reference(orc_tree* t, double pw, uint64_t cg_iters, double eps, double* x, uint64_t* info) {
+  const uint64_t gs = 20;
+  if (!t->have_A || t->pw_A != pw) orc_tree_assemble(t, pw);
+  std::vector<double> b(t->n);
+  orc_tree_rhs(t, pw, b.data());
+  uint32_t base_depth = t->D > 2 ? t->D - 2 : 0;
+  if (base_depth >= t->D) {
+    std::fill(x, x + t->n, 0.0);
+    for (uint64_t k = 0; k < gs; ++k) gauss_seidel_sweep(t->A, b.data(), x);
+    uint64_t it = solve_cg(t->A, b.data(), x, cg_iters, eps);
+    if (info) { info[0] = 0; info[1] = it; }
+    return 0;
+  }
+  Csr B;
+  std::vector<double> brhs;
+  build_system_at_depth(t, base_depth, pw, B, brhs);
+  std::vector<double> csol(brhs.size(), 0.0);
+  for (uint64_t k = 0; k < gs; ++k) gauss_seidel_sweep(B, brhs.data(), csol.data());
+  uint64_t itc = solve_cg(B, brhs.data(), csol.data(), cg_iters, eps);
+  std::vector<double> init;
+  prolongate(t, csol, base_depth, init);
+  std::memcpy(x, init.data(), t->n * sizeof(double));
+  for (uint64_t k = 0; k < gs; ++k) gauss_seidel_sweep(t->A, b.data(), x);
+  uint64_t itf = solve_cg(t->A, b.data(), x, cg_iters / 4, eps);
+  if (info) { info[0] = itc; info[1] = itf; }
+  return 0;
+}
+
+// Stage outputs of the reference schedule for diagnostics: coarse system RHS (lexicographic)
+// and the prolongated initial guess.
+int orc_tree_coarse_rhs(const orc_tree* t, double pw, double* brhs_out) {
+  uint32_t base_depth = t->D > 2 ? t->D - 2 : 0;
+  if (base_depth >= t->D) return -1;
+  Csr B;
+  std::vector<double> brhs;
+  build_system_at_depth(t, base_depth, pw, B, brhs);
+  std::memcpy(brhs_out, brhs.data(), brhs.size() * sizeof(double));
+  return 0;
+}
+int orc_tree_prolongate(const orc_tree* t, const double* coarse_lex, uint32_t coarse_depth, double* fine_out) {
+  std::vector<double> c(coarse_lex, coarse_lex + (1ull << (3 * coarse_depth)));
+  std::vector<double> f;
+  prolongate(t, c, coarse_depth, f);
+  std::memcpy(fine_out, f.data(), t->n * sizeof(double));
+  return 0;
+}
+
+// Converged solve of the same fine system: CG (the crate's loop, without its early exit)
+// until ||b - A x|| <= tol ||b||, x holds the initial guess on entry.
+uint64_t orc_tree_solve_converged(orc_tree* t, double pw, double tol, uint64_t maxit, double* x, double* relres) {
+  if (!t->have_A || t->pw_A != pw) orc_tree_assemble(t, pw);
+  const uint64_t n = t->n;
+  std::vector<double> b(n), r(n), d(n), q(n);
+  orc_tree_rhs(t, pw, b.data());
+  double bb = det_dot(b.data(), b.data(), n);
+  t->A.spmv(x, q.data());
+  for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  d = r;
+  double rr = det_dot(r.data(), r.data(), n);
+  uint64_t it = 0;
+  if (bb == 0.0) { if (relres) *relres = 0.0; return 0; }
+  while (it < maxit && rr > tol * tol * bb) {
+    t->A.spmv(d.data(), q.data());
+    double dq = det_dot(d.data(), q.data(), n);
+    if (dq == 0.0) break;
+    double alpha = rr / dq;
+    for (uint64_t i = 0; i < n; ++i) x[i] += alpha * d[i];
+    ++it;
+    if (it % 50 == 0) {
+      t->A.spmv(x, q.data());
+      for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+    } else {
+      for (uint64_t i = 0; i < n; ++i) r[i] -= alpha * q[i];
+    }
+    double rr_new = det_dot(r.data(), r.data(), n);
+    double beta = rr_new / rr;
+    rr = rr_new;
+    for (uint64_t i = 0; i < n; ++i) d[i] = r[i] + beta * d[i];
+  }
+  t->A.spmv(x, q.data());
+  for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  if (relres) *relres = std::sqrt(det_dot(r.data(), r.data(), n) / bb);
+  return it;
+}
+
+// ---------------------------------------------------------------- evaluate / iso / MC
+// FEMTree::evaluate (src/fem_tree.rs:490-513)
+double orc_evaluate(uint32_t D, const double* sol, double px, double py, double pz) {
+  const isize res = (isize)1 << D;
+  const double h = 1.0 / (double)res;
+  double sx = px / h, sy = py / h, sz = pz / h;
+  uint32_t ox[2], oy[2], oz[2];
+  contributing_offsets(sx, res, ox[0], ox[1]);
+  contributing_offsets(sy, res, oy[0], oy[1]);
+  contributing_offsets(sz, res, oz[0], oz[1]);
+  double bx[2] = {bspline1(sx - (double)ox[0]), bspline1(sx - (double)ox[1])};
+  double by[2] = {bspline1(sy - (double)oy[0]), bspline1(sy - (double)oy[1])};
+  double bz[2] = {bspline1(sz - (double)oz[0]), bspline1(sz - (double)oz[1])};
+  double v = 0.0;
+  for (int a = 0; a < 2; ++a) {
+    if (bx[a] == 0.0) continue;
+    for (int b = 0; b < 2; ++b) {
+      if (by[b] == 0.0) continue;
+      for (int c = 0; c < 2; ++c) {
+        if (bz[c] == 0.0) continue;
+        v += sol[morton(ox[a], oy[b], oz[c])] * bx[a] * by[b] * bz[c];
+      }
+    }
+  }
+  return v;
+}
+
+void orc_evaluate_many(uint32_t D, const double* sol, const double* pts, uint64_t stride, uint64_t n, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i)
+    out[i] = orc_evaluate(D, sol, pts[stride * i], pts[stride * i + 1], pts[stride * i + 2]);
+}
+
+// iso = mean of evaluate at the unit-cube points (src/reconstructor.rs:56)
+double orc_iso(uint32_t D, const double* sol, const double* unit6, uint64_t n) {
+  std::vector<double> v(n), one(n, 1.0);
+  orc_evaluate_many(D, sol, unit6, 6, n, v.data());
+  return det_dot(v.data(), one.data(), n) / (double)n;
+}
+
+
+
+// FEMTree::extract_surface (src/fem_tree.rs:576-636).  Vertices in unit-cube space.
+int orc_extract_surface(uint32_t D, const double* sol, double iso, orc_mesh* out) {
+  static const uint32_t co[8][3] = {{0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1}};
+  static const int ev[12][2] = {{0,1},{1,2},{2,3},{3,0},{4,5},{5,6},{6,7},{7,4},{0,4},{1,5},{2,6},{3,7}};
+  const uint64_t max_res = 1ull << D;
+  const uint64_t n = max_res * max_res * max_res;
+  const double w = 1.0 / (double)max_res;  // (max_res >> D) as f64 / max_res as f64
+  std::vector<double> verts;
+  std::vector<uint64_t> tris;
+  std::unordered_map<std::array<uint64_t, 3>, uint64_t, KeyHash> edge_hash;
+  for (uint64_t cell = 0; cell < n; ++cell) {
+    uint64_t off[3];
+    unmorton(cell, off[0], off[1], off[2]);
+    double cv[8];
+    uint32_t mc = 0;
+    for (int k = 0; k < 8; ++k) {
+      double p[3];
+      for (int a = 0; a < 3; ++a) p[a] = (double)(off[a] + co[k][a]) * w;
+      cv[k] = orc_evaluate(D, sol, p[0], p[1], p[2]);
+      if (cv[k] < iso) mc |= 1u << k;
+    }
+    uint32_t em = orc_mc_edge_mask(mc);
+    if (em == 0) continue;
+    uint64_t evi[12];
+    for (int e = 0; e < 12; ++e) {
+      evi[e] = UINT64_MAX;
+      if (!((em >> e) & 1u)) continue;
+      int a = ev[e][0], b = ev[e][1];
+      double dv = cv[b] - cv[a];
+      double t = std::fabs(dv) < 1e-15 ? 0.5 : (iso - cv[a]) / dv;
+      double pos[3];
+      for (int ax = 0; ax < 3; ++ax) {
+        double base = (double)(off[ax] + co[a][ax]) * w;
+        pos[ax] = base + t * (double)((int32_t)co[b][ax] - (int32_t)co[a][ax]) * w;
+      }
+      std::array<uint64_t, 3> key = {f64_to_u64(pos[0] * 1e9), f64_to_u64(pos[1] * 1e9), f64_to_u64(pos[2] * 1e9)};
+      auto it = edge_hash.find(key);
+      if (it != edge_hash.end()) evi[e] = it->second;
+      else {
+        uint64_t idx = verts.size() / 3;
+        edge_hash.emplace(key, idx);
+        verts.insert(verts.end(), pos, pos + 3);
+        evi[e] = idx;
+      }
+    }
+    for (int i = 0; i < 3 * PR_MC_NTRI[mc]; i += 3) {
+      for (int k = 0; k < 3; ++k) tris.push_back(evi[(PR_MC_TRIS[mc] >> (4 * (i + k))) & 15ull]);
+    }
+  }
+  out->nv = verts.size() / 3;
+  out->nt = tris.size() / 3;
+  out->verts = (double*)std::malloc(std::max<size_t>(1, verts.size()) * sizeof(double));
+  out->tris = (uint64_t*)std::malloc(std::max<size_t>(1, tris.size()) * sizeof(uint64_t));
+  if (!verts.empty()) std::memcpy(out->verts, verts.data(), verts.size() * sizeof(double));
+  if (!tris.empty()) std::memcpy(out->tris, tris.data(), tris.size() * sizeof(uint64_t));
+  return 0;
+}
+
+void orc_mesh_free(orc_mesh* m) {
+  std::free(m->verts);
+  std::free(m->tris);
+  m->verts = nullptr;
+  m->tris = nullptr;
+  m->nv = m->nt = 0;
+}
+
+// ---------------------------------------------------------------- generic CSR (ported unit tests)
+uint64_t orc_csr_cg(uint64_t n, const uint64_t* ptr, const uint32_t* col, const double* val, const double* b,
+                    double* x, uint64_t maxit, double acc) {
+  Csr a;
+  a.rows = n;
+  a.ptr.assign(ptr, ptr + n + 1);
+  a.col.assign(col, col + ptr[n]);
+  a.val.assign(val, val + ptr[n]);
+  return solve_cg(a, b, x, maxit, acc);
+}
+void orc_csr_spmv(uint64_t n, const uint64_t* ptr, const uint32_t* col, const double* val, const double* x, double* y) {
+  Csr a;
+  a.rows = n;
+  a.ptr.assign(ptr, ptr + n + 1);
+  a.col.assign(col, col + ptr[n]);
+  a.val.assign(val, val + ptr[n]);
+  a.spmv(x, y);
+}
+void orc_csr_gs_sweep(uint64_t n, const uint64_t* ptr, const uint32_t* col, const double* val, const double* b, double* x) {
+  Csr a;
+  a.rows = n;
+  a.ptr.assign(ptr, ptr + n + 1);
+  a.col.assign(col, col + ptr[n]);
+  a.val.assign(val, val + ptr[n]);
+  gauss_seidel_sweep(a, b, x);
+}
+
+// ---------------------------------------------------------------- full pipeline
+// reconstructor::reconstruct (src/reconstructor.rs:25-70).  solve_mode 0 runs the crate's
+// cascadic schedule; solve_mode 1 solves the same fine system to target_rel_residual.
+// coeffs (n doubles, Morton order) may be NULL.
+int orc_reconstruct(const double* pts6, uint64_t n, const orc_params* p, orc_mesh* mesh, orc_stats* st,
+                    double* coeffs) {
+  std::memset(st, 0, sizeof(*st));
+  mesh->verts = nullptr; mesh->tris = nullptr; mesh->nv = mesh->nt = 0;
+  if (n == 0) return 0;
+  double bmin[3], bmax[3], M[16], Minv[16];
+  orc_bbox(pts6, n, bmin, bmax);
+  orc_unit_cube_transform(bmin, bmax, p->scale, M);
+  orc_mat4_inverse(M, Minv);
+  std::vector<double> unit(6 * n);
+  orc_transform_points(M, pts6, n, unit.data());
+  orc_tree* t = orc_tree_new(p->depth, unit.data(), n);
+  st->fem_nodes = t->n;
+  std::vector<double> x(t->n, 0.0);
+  if (p->solve_mode == 0) {
+    uint64_t info[2];
+    orc_tree_solve_reference(t, p->point_weight, p->cg_iters, p->cg_accuracy, x.data(), info);
+    st->iterations = info[1];
+  } else {
+    double rr = 0.0;
+    st->iterations = orc_tree_solve_converged(t, p->point_weight, p->target_rel_residual, p->max_iters, x.data(), &rr);
+    st->rel_residual = rr;
+  }
+  double iso = orc_iso(t->D, x.data(), unit.data(), n);
+  st->iso_value = iso;
+  orc_extract_surface(t->D, x.data(), iso, mesh);
+  for (uint64_t v = 0; v < mesh->nv; ++v) {
+    double q[3];
+    orc_transform_point(Minv, mesh->verts + 3 * v, q);
+    std::memcpy(mesh->verts + 3 * v, q, sizeof(q));
+  }
+  st->mesh_vertices = mesh->nv;
+  st->mesh_triangles = mesh->nt;
+  if (coeffs) std::memcpy(coeffs, x.data(), t->n * sizeof(double));
+  orc_tree_free(t);
+  return 0;
+}
+
+}  // extern "C"

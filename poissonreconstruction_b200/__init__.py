@@ -1,0 +1,326 @@
+"""B200-native screened Poisson surface reconstruction.
+
+Python mirror of the reference crate's public path (``poisson_recon::reconstructor``):
+
+    reconstruct(points, params) -> (Mesh, ReconstructStats)       src/reconstructor.rs:25
+
+``points`` is an (N, 6) float64 array of ``x y z nx ny nz`` rows (the crate's
+``OrientedPoint``, src/fem_tree.rs:10).  Everything runs in ``libpoisson_recon_b200.so``
+through its C ABI (include/poisson_recon.h); there is no CPU fallback: importing works
+anywhere, but any computation raises if the library or a B200 is missing.
+"""
+import ctypes as C
+import dataclasses
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpoisson_recon_b200.so")
+
+PR_OK = 0
+PR_ERR_INVALID_ARGUMENT = -1
+PR_ERR_OUT_OF_MEMORY = -2
+PR_ERR_CUDA = -3
+PR_ERR_NOT_CONVERGED = -4
+PR_ERR_NO_DEVICE = -5
+PR_ERR_STATE = -6
+PR_ERR_INTERNAL = -7
+
+PR_SOLVE_CONVERGED = 0
+PR_SOLVE_REFERENCE_SCHEDULE = 1
+PR_PRECISION_MIXED = 0
+PR_PRECISION_FP64 = 1
+
+
+class PrParams(C.Structure):
+    _fields_ = [("depth", C.c_uint32), ("samples_per_node", C.c_double), ("scale", C.c_double),
+                ("cg_accuracy", C.c_double), ("cg_iters", C.c_uint64), ("point_weight", C.c_double),
+                ("verbose", C.c_int32), ("solve_mode", C.c_int32), ("precision", C.c_int32),
+                ("target_rel_residual", C.c_double), ("max_iters", C.c_uint32), ("smooth_sweeps", C.c_uint32),
+                ("inner_rel_tol", C.c_double), ("reserved", C.c_uint32 * 8)]
+
+
+class PrMesh(C.Structure):
+    _fields_ = [("vertices", C.POINTER(C.c_double)), ("n_vertices", C.c_uint64),
+                ("triangles", C.POINTER(C.c_uint64)), ("n_triangles", C.c_uint64)]
+
+
+class PrStats(C.Structure):
+    _fields_ = [("time_transform", C.c_double), ("time_tree", C.c_double), ("time_system", C.c_double),
+                ("time_solve", C.c_double), ("time_extract", C.c_double), ("time_total", C.c_double),
+                ("fem_nodes", C.c_uint64), ("matrix_nnz", C.c_uint64), ("mesh_vertices", C.c_uint64),
+                ("mesh_triangles", C.c_uint64), ("iso_value", C.c_double), ("rel_residual", C.c_double),
+                ("pcg_iterations", C.c_uint32), ("refinement_steps", C.c_uint32), ("points_in_cube", C.c_uint64),
+                ("solve_bytes", C.c_double), ("peak_device_bytes", C.c_double), ("converged", C.c_int32),
+                ("reserved_i", C.c_int32), ("reserved", C.c_double * 5)]
+
+
+# Every C-ABI entry point and its signature (checked against include/poisson_recon.h by the tests).
+_P = C.c_void_p
+SIGNATURES = {
+    "pr_version": (C.c_char_p, []),
+    "pr_abi_layout": (None, [_P]),
+    "pr_kernel_launches": (C.c_uint64, [C.POINTER(C.c_uint64)]),
+    "pr_ctx_apply_operator_device": (C.c_int, [_P, _P, _P, C.c_int]),
+    "pr_last_error": (C.c_char_p, []),
+    "pr_params_default": (PrParams, []),
+    "pr_reconstruct": (C.c_int, [_P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrMesh), C.POINTER(PrStats)]),
+    "pr_mesh_free": (None, [C.POINTER(PrMesh)]),
+    "pr_context_create": (C.c_int, [C.c_int, _P, C.POINTER(_P)]),
+    "pr_context_destroy": (C.c_int, [_P]),
+    "pr_ctx_reconstruct": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrMesh),
+                                     C.POINTER(PrStats)]),
+    "pr_ctx_reconstruct_device": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrStats)]),
+    "pr_ctx_mesh_device": (C.c_int, [_P, C.POINTER(_P), C.POINTER(C.c_uint64), C.POINTER(_P),
+                                     C.POINTER(C.c_uint64)]),
+    "pr_ctx_mesh_copy": (C.c_int, [_P, C.POINTER(PrMesh)]),
+    "pr_ctx_synchronize": (C.c_int, [_P]),
+    "pr_ctx_info": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), _P]),
+    "pr_ctx_get_coefficients": (C.c_int, [_P, _P]),
+    "pr_ctx_get_rhs": (C.c_int, [_P, _P]),
+    "pr_ctx_get_unit_points": (C.c_int, [_P, _P]),
+    "pr_ctx_get_normal_field": (C.c_int, [_P, _P, _P]),
+    "pr_ctx_apply_operator": (C.c_int, [_P, _P, _P, C.c_int]),
+    "pr_ctx_evaluate": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
+    "pr_ctx_extract": (C.c_int, [_P, _P, C.c_double, C.POINTER(PrMesh)]),
+    "pr_ctx_extract_at_depth": (C.c_int, [_P, C.c_uint32, _P, C.c_double, C.POINTER(PrMesh)]),
+}
+
+_LIB = None
+
+
+class ReconstructError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (status %d)" % (msg, code))
+        self.code = code
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("%s is missing: run `python -m poissonreconstruction_b200.build`" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _check(rc):
+    if rc != PR_OK:
+        raise ReconstructError(rc, lib().pr_last_error().decode())
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+@dataclasses.dataclass
+class ReconstructParams:
+    """src/reconstructor.rs:8-15 (defaults of ReconstructParams::default()) + extensions."""
+    depth: int = 8
+    samples_per_node: float = 1.5
+    scale: float = 1.1
+    cg_accuracy: float = 1e-3
+    cg_iters: int = 500
+    point_weight: float = 0.0
+    verbose: bool = False
+    solve_mode: int = PR_SOLVE_CONVERGED
+    precision: int = PR_PRECISION_MIXED
+    target_rel_residual: float = 1e-6
+    max_iters: int = 200
+    smooth_sweeps: int = 1
+    inner_rel_tol: float = 1e-4
+
+    def to_c(self):
+        p = PrParams()
+        for f in dataclasses.fields(self):
+            setattr(p, f.name, int(getattr(self, f.name)) if f.type in (int, bool, "int", "bool")
+                    else getattr(self, f.name))
+        return p
+
+
+@dataclasses.dataclass
+class Mesh:
+    """src/marching_cubes.rs:8-11: (V,3) float64 vertices, (T,3) uint64 vertex indices."""
+    vertices: np.ndarray
+    triangles: np.ndarray
+
+
+@dataclasses.dataclass
+class ReconstructStats:
+    time_transform: float = 0.0
+    time_tree: float = 0.0
+    time_system: float = 0.0
+    time_solve: float = 0.0
+    time_extract: float = 0.0
+    time_total: float = 0.0
+    fem_nodes: int = 0
+    matrix_nnz: int = 0
+    mesh_vertices: int = 0
+    mesh_triangles: int = 0
+    iso_value: float = 0.0
+    rel_residual: float = 0.0
+    pcg_iterations: int = 0
+    refinement_steps: int = 0
+    points_in_cube: int = 0
+    solve_bytes: float = 0.0
+    peak_device_bytes: float = 0.0
+    converged: int = 0
+
+    @classmethod
+    def from_c(cls, s):
+        return cls(**{f.name: getattr(s, f.name) for f in dataclasses.fields(cls)})
+
+
+def _take_mesh(m):
+    v = np.ctypeslib.as_array(m.vertices, shape=(m.n_vertices * 3,)).reshape(-1, 3).copy() \
+        if m.n_vertices else np.zeros((0, 3))
+    t = np.ctypeslib.as_array(m.triangles, shape=(m.n_triangles * 3,)).reshape(-1, 3).copy() \
+        if m.n_triangles else np.zeros((0, 3), np.uint64)
+    lib().pr_mesh_free(C.byref(m))
+    return Mesh(v, t)
+
+
+def _points(points):
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    if pts.ndim != 2 or pts.shape[1] != 6:
+        raise ValueError("points must be an (N, 6) array of x y z nx ny nz")
+    return pts
+
+
+def reconstruct(points, params=None):
+    """reconstructor::reconstruct (src/reconstructor.rs:25-70) on the GPU."""
+    params = params or ReconstructParams()
+    pts = _points(points)
+    p, m, s = params.to_c(), PrMesh(), PrStats()
+    _check(lib().pr_reconstruct(_ptr(pts), pts.shape[0], C.byref(p), C.byref(m), C.byref(s)))
+    return _take_mesh(m), ReconstructStats.from_c(s)
+
+
+class Context:
+    """A device context: owns a CUDA stream (or uses the one given) and the buffers of the
+    last reconstruction, whose intermediate state the accessors read."""
+
+    def __init__(self, device=0, stream=None):
+        h = C.c_void_p()
+        _check(lib().pr_context_create(int(device), C.c_void_p(stream) if stream else None, C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pr_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- reconstruction
+    def reconstruct(self, points, params=None):
+        params = params or ReconstructParams()
+        pts = _points(points)
+        p, m, s = params.to_c(), PrMesh(), PrStats()
+        _check(lib().pr_ctx_reconstruct(self._h, _ptr(pts), pts.shape[0], C.byref(p), C.byref(m), C.byref(s)))
+        return _take_mesh(m), ReconstructStats.from_c(s)
+
+    def reconstruct_device(self, d_points_ptr, n, params=None):
+        """Input already on the device (pointer to n x 6 float64); the mesh stays there."""
+        params = params or ReconstructParams()
+        p, s = params.to_c(), PrStats()
+        _check(lib().pr_ctx_reconstruct_device(self._h, C.c_void_p(d_points_ptr), int(n), C.byref(p), C.byref(s)))
+        return ReconstructStats.from_c(s)
+
+    def mesh_device(self):
+        dv, dt = C.c_void_p(), C.c_void_p()
+        nv, nt = C.c_uint64(), C.c_uint64()
+        _check(lib().pr_ctx_mesh_device(self._h, C.byref(dv), C.byref(nv), C.byref(dt), C.byref(nt)))
+        return dv.value, nv.value, dt.value, nt.value
+
+    def mesh(self):
+        m = PrMesh()
+        _check(lib().pr_ctx_mesh_copy(self._h, C.byref(m)))
+        return _take_mesh(m)
+
+    def synchronize(self):
+        _check(lib().pr_ctx_synchronize(self._h))
+
+    # -- accessors
+    def info(self):
+        d, n = C.c_uint32(), C.c_uint64()
+        m = np.zeros(16)
+        _check(lib().pr_ctx_info(self._h, C.byref(d), C.byref(n), _ptr(m)))
+        return d.value, n.value, m
+
+    def coefficients(self):
+        _, n, _ = self.info()
+        out = np.zeros(n)
+        _check(lib().pr_ctx_get_coefficients(self._h, _ptr(out)))
+        return out
+
+    def rhs(self):
+        _, n, _ = self.info()
+        out = np.zeros(n)
+        _check(lib().pr_ctx_get_rhs(self._h, _ptr(out)))
+        return out
+
+    def unit_points(self, n_points):
+        out = np.zeros((n_points, 6))
+        _check(lib().pr_ctx_get_unit_points(self._h, _ptr(out)))
+        return out
+
+    def normal_field(self):
+        _, n, _ = self.info()
+        nf, w = np.zeros((n, 3)), np.zeros(n)
+        _check(lib().pr_ctx_get_normal_field(self._h, _ptr(nf), _ptr(w)))
+        return nf, w
+
+    def apply_operator(self, x, precision=PR_PRECISION_FP64):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        _check(lib().pr_ctx_apply_operator(self._h, _ptr(x), _ptr(y), int(precision)))
+        return y
+
+    def apply_operator_device(self, d_x, d_y, precision=PR_PRECISION_MIXED):
+        """Enqueue y = A x on device pointers (no synchronisation)."""
+        _check(lib().pr_ctx_apply_operator_device(self._h, C.c_void_p(d_x), C.c_void_p(d_y), int(precision)))
+
+    def evaluate(self, pts3, coefficients=None):
+        pts3 = np.ascontiguousarray(pts3, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(pts3.shape[0])
+        co = None if coefficients is None else np.ascontiguousarray(coefficients, dtype=np.float64)
+        _check(lib().pr_ctx_evaluate(self._h, _ptr(co), _ptr(pts3), pts3.shape[0], _ptr(out)))
+        return out
+
+    def extract(self, coefficients, iso, depth=None):
+        """Marching cubes of given FP64 coefficients; vertices in unit-cube space."""
+        co = np.ascontiguousarray(coefficients, dtype=np.float64)
+        m = PrMesh()
+        if depth is None:
+            _check(lib().pr_ctx_extract(self._h, _ptr(co), float(iso), C.byref(m)))
+        else:
+            _check(lib().pr_ctx_extract_at_depth(self._h, int(depth), _ptr(co), float(iso), C.byref(m)))
+        return _take_mesh(m)
+
+
+def kernel_launches():
+    """(own kernel launches, library primitive calls) so far in this process."""
+    prim = C.c_uint64()
+    n = lib().pr_kernel_launches(C.byref(prim))
+    return n, prim.value
+
+
+__all__ = ["ReconstructParams", "ReconstructStats", "Mesh", "reconstruct", "Context", "ReconstructError", "lib"]

@@ -1,0 +1,488 @@
+// C ABI of libpoisson_recon_b200 (declared in include/poisson_recon.h).
+//
+// pr_reconstruct mirrors reconstructor::reconstruct (src/reconstructor.rs:25-70):
+//   bbox + unit-cube transform (stage_transform), tree + splat (stage_splat_rhs: the tree
+//   is implicit, the FEM index is the Morton index), solve (stage_solve), iso value and
+//   marching cubes (stage_iso / stage_extract), back-transform of the vertices.
+// Every entry point converts exceptions into a status code and a thread-local message.
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include <cmath>
+
+#include "pr_ops.cuh"
+
+namespace pr {
+void stage_solve_reference(pr_context* c, const pr_params& p, pr_stats& st);
+}
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return PR_OK;
+  } catch (const pr::Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return PR_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return PR_ERR_INTERNAL;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return PR_ERR_INTERNAL;
+  }
+}
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+void validate(const pr_params* p) {
+  PR_REQUIRE(p != nullptr, PR_ERR_INVALID_ARGUMENT, "params is NULL");
+  PR_REQUIRE(p->depth >= pr::kMinDepth && p->depth <= pr::kMaxDepth, PR_ERR_INVALID_ARGUMENT,
+             "depth must be in [1, 10] (dense grid of 2^(3 depth) nodes), got " + std::to_string(p->depth));
+  PR_REQUIRE(std::isfinite(p->scale) && p->scale > 0.0, PR_ERR_INVALID_ARGUMENT, "scale must be finite and > 0");
+  PR_REQUIRE(std::isfinite(p->point_weight) && p->point_weight >= 0.0, PR_ERR_INVALID_ARGUMENT,
+             "point_weight must be finite and >= 0");
+  PR_REQUIRE(p->solve_mode == PR_SOLVE_CONVERGED || p->solve_mode == PR_SOLVE_REFERENCE_SCHEDULE,
+             PR_ERR_INVALID_ARGUMENT, "unknown solve_mode");
+  PR_REQUIRE(p->precision == PR_PRECISION_MIXED || p->precision == PR_PRECISION_FP64, PR_ERR_INVALID_ARGUMENT,
+             "unknown precision");
+  PR_REQUIRE(!(p->target_rel_residual < 0.0) && std::isfinite(p->target_rel_residual), PR_ERR_INVALID_ARGUMENT,
+             "target_rel_residual must be finite and >= 0");
+}
+
+void set_device(pr_context* c) { PR_CUDA(cudaSetDevice(c->device)); }
+
+void copy_mesh_to_host(pr_context* c, pr_mesh* out) {
+  out->vertices = nullptr;
+  out->triangles = nullptr;
+  out->n_vertices = c->nv;
+  out->n_triangles = c->nt;
+  if (c->nv) {
+    out->vertices = (double*)std::malloc(3 * c->nv * sizeof(double));
+    if (!out->vertices) throw std::bad_alloc();
+    PR_CUDA(cudaMemcpyAsync(out->vertices, c->get<double>("mesh_v"), 3 * c->nv * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (c->nt) {
+    out->triangles = (uint64_t*)std::malloc(3 * c->nt * sizeof(uint64_t));
+    if (!out->triangles) {
+      std::free(out->vertices);
+      out->vertices = nullptr;
+      throw std::bad_alloc();
+    }
+    PR_CUDA(cudaMemcpyAsync(out->triangles, c->get<uint64_t>("mesh_t"), 3 * c->nt * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, c->stream));
+  }
+  c->sync();
+}
+
+// The pipeline on device-resident points (c->buf "pts6" or caller memory).
+void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_params& p, pr_stats& st, double t_start) {
+  double t0 = now_s();
+  pr::stage_transform(c, d_pts6, n, p.scale);
+  c->sync();
+  double t1 = now_s();
+  st.time_transform = t1 - t0 + (t0 - t_start);
+  pr::stage_splat_rhs(c, p.depth, p.point_weight);
+  c->sync();
+  double t2 = now_s();
+  st.time_tree = t2 - t1;  // tree (implicit) + splat + RHS + screening payload
+  st.time_system = 0.0;
+  st.fem_nodes = c->n;
+  st.points_in_cube = c->P_in;
+  if (p.solve_mode == PR_SOLVE_REFERENCE_SCHEDULE) pr::stage_solve_reference(c, p, st);
+  else pr::stage_solve(c, p, st);
+  c->sync();
+  double t3 = now_s();
+  st.time_solve = t3 - t2;
+  const double* x = c->get<double>("x64");
+  double iso = pr::stage_iso(c, x);
+  pr::stage_extract(c, c->D, x, iso, true);
+  c->sync();
+  double t4 = now_s();
+  st.time_extract = t4 - t3;
+  st.iso_value = iso;
+  st.mesh_vertices = c->nv;
+  st.mesh_triangles = c->nt;
+  st.peak_device_bytes = (double)c->peak_bytes;
+  if (p.verbose)
+    std::fprintf(stderr,
+                 "pr: depth=%u points=%llu xform=%.4f tree=%.4f solve=%.4f extract=%.4f s; pcg=%u refine=%u "
+                 "relres=%.3e iso=%.6f verts=%llu tris=%llu\n",
+                 p.depth, (unsigned long long)n, st.time_transform, st.time_tree, st.time_solve, st.time_extract,
+                 st.pcg_iterations, st.refinement_steps, st.rel_residual, iso, (unsigned long long)c->nv,
+                 (unsigned long long)c->nt);
+}
+
+void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr_params* params, bool device_input,
+                      pr_mesh* out_mesh, pr_stats* out_stats) {
+  double t_start = now_s();
+  validate(params);
+  PR_REQUIRE(n == 0 || points6 != nullptr, PR_ERR_INVALID_ARGUMENT, "points is NULL");
+  PR_REQUIRE(n <= pr::kMaxPoints, PR_ERR_INVALID_ARGUMENT, "at most 2^28 points per call");
+  set_device(c);
+  pr_stats st;
+  std::memset(&st, 0, sizeof(st));
+  c->have_state = false;
+  c->have_mesh = false;
+  c->have_coeffs = false;
+  c->nv = c->nt = 0;
+  if (out_mesh) std::memset(out_mesh, 0, sizeof(*out_mesh));
+  if (n == 0) {  // src/reconstructor.rs:28
+    c->have_mesh = true;
+    if (out_stats) *out_stats = st;
+    return;
+  }
+  const double* d_pts = points6;
+  if (!device_input) {
+    double* dp = c->buf<double>("pts6", 6 * n);
+    PR_CUDA(cudaMemcpyAsync(dp, points6, 6 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    d_pts = dp;
+  }
+  run_pipeline(c, d_pts, n, *params, st, t_start);
+  if (out_mesh) copy_mesh_to_host(c, out_mesh);
+  st.time_total = now_s() - t_start;
+  if (out_stats) *out_stats = st;
+}
+
+thread_local std::unique_ptr<pr_context, int (*)(pr_context*)> g_thread_ctx(nullptr, pr_context_destroy);
+
+}  // namespace
+
+static std::atomic<uint64_t> g_launches{0}, g_primitives{0};
+
+extern "C" {
+
+void pr_count_launch_(int primitive) {
+  if (primitive) g_primitives.fetch_add(1, std::memory_order_relaxed);
+  else g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+uint64_t pr_kernel_launches(uint64_t* primitive_calls) {
+  if (primitive_calls) *primitive_calls = g_primitives.load();
+  return g_launches.load();
+}
+
+int pr_ctx_apply_operator_device(pr_context* c, const void* d_x, void* d_y, int precision) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && d_x != nullptr && d_y != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    set_device(c);
+    if (precision == PR_PRECISION_FP64) pr::apply_operator64(c, (const double*)d_x, (double*)d_y);
+    else pr::apply_operator32(c, (const float*)d_x, (float*)d_y);
+  });
+}
+
+const char* pr_version(void) { return "poisson_recon_b200 0.1 (sm_100a)"; }
+
+void pr_abi_layout(uint64_t* out4) {
+  if (!out4) return;
+  out4[0] = sizeof(pr_params);
+  out4[1] = sizeof(pr_mesh);
+  out4[2] = sizeof(pr_stats);
+  out4[3] = sizeof(pr_oriented_point);
+}
+
+const char* pr_last_error(void) { return g_last_error.c_str(); }
+
+pr_params pr_params_default(void) {
+  pr_params p;
+  std::memset(&p, 0, sizeof(p));
+  // ReconstructParams::default() (src/reconstructor.rs:14)
+  p.depth = 8;
+  p.samples_per_node = 1.5;
+  p.scale = 1.1;
+  p.cg_accuracy = 1e-3;
+  p.cg_iters = 500;
+  p.point_weight = 0.0;
+  p.verbose = 0;
+  p.solve_mode = PR_SOLVE_CONVERGED;
+  p.precision = PR_PRECISION_MIXED;
+  p.target_rel_residual = 1e-6;
+  p.max_iters = 200;
+  p.smooth_sweeps = 1;
+  p.inner_rel_tol = 1e-4;
+  return p;
+}
+
+int pr_context_create(int device, void* stream, pr_context** out_ctx) {
+  return guard([&] {
+    PR_REQUIRE(out_ctx != nullptr, PR_ERR_INVALID_ARGUMENT, "out_ctx is NULL");
+    *out_ctx = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      throw pr::Error(PR_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    PR_REQUIRE(device >= 0 && device < count, PR_ERR_INVALID_ARGUMENT, "device index out of range");
+    cudaDeviceProp prop;
+    PR_CUDA(cudaGetDeviceProperties(&prop, device));
+    PR_REQUIRE(prop.major == 10, PR_ERR_NO_DEVICE,
+               std::string("library is built for sm_100a; device is ") + prop.name + " (sm_" +
+                   std::to_string(prop.major) + std::to_string(prop.minor) + ")");
+    PR_CUDA(cudaSetDevice(device));
+    std::unique_ptr<pr_context> c(new pr_context());
+    c->device = device;
+    if (stream) {
+      c->stream = (cudaStream_t)stream;
+      c->own_stream = false;
+    } else {
+      PR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      c->own_stream = true;
+    }
+    PR_CUDA(cudaMallocHost(&c->h_scalars, 64 * sizeof(double)));
+    *out_ctx = c.release();
+  });
+}
+
+int pr_context_destroy(pr_context* c) {
+  if (!c) return PR_OK;
+  return guard([&] {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->bufs)
+      if (kv.second.ptr) cudaFree(kv.second.ptr);
+    c->bufs.clear();
+    if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+  });
+}
+
+int pr_ctx_reconstruct(pr_context* c, const double* points6, uint64_t n, const pr_params* params, pr_mesh* out_mesh,
+                       pr_stats* out_stats) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(out_mesh != nullptr, PR_ERR_INVALID_ARGUMENT, "out_mesh is NULL");
+    reconstruct_impl(c, points6, n, params, false, out_mesh, out_stats);
+  });
+}
+
+int pr_ctx_reconstruct_device(pr_context* c, const double* d_points6, uint64_t n, const pr_params* params,
+                              pr_stats* out_stats) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    reconstruct_impl(c, d_points6, n, params, true, nullptr, out_stats);
+  });
+}
+
+int pr_reconstruct(const double* points6, uint64_t n, const pr_params* params, pr_mesh* out_mesh,
+                   pr_stats* out_stats) {
+  return guard([&] {
+    PR_REQUIRE(out_mesh != nullptr, PR_ERR_INVALID_ARGUMENT, "out_mesh is NULL");
+    validate(params);
+    PR_REQUIRE(n == 0 || points6 != nullptr, PR_ERR_INVALID_ARGUMENT, "points is NULL");
+    PR_REQUIRE(n <= pr::kMaxPoints, PR_ERR_INVALID_ARGUMENT, "at most 2^28 points per call");
+    if (n == 0) {  // src/reconstructor.rs:28: empty mesh, default stats; no device needed
+      std::memset(out_mesh, 0, sizeof(*out_mesh));
+      if (out_stats) std::memset(out_stats, 0, sizeof(*out_stats));
+      return;
+    }
+    if (!g_thread_ctx) {
+      pr_context* c = nullptr;
+      int rc = pr_context_create(0, nullptr, &c);
+      if (rc != PR_OK) throw pr::Error(rc, g_last_error);
+      g_thread_ctx.reset(c);
+    }
+    reconstruct_impl(g_thread_ctx.get(), points6, n, params, false, out_mesh, out_stats);
+  });
+}
+
+void pr_mesh_free(pr_mesh* m) {
+  if (!m) return;
+  std::free(m->vertices);
+  std::free(m->triangles);
+  m->vertices = nullptr;
+  m->triangles = nullptr;
+  m->n_vertices = m->n_triangles = 0;
+}
+
+int pr_ctx_mesh_device(pr_context* c, const double** dv, uint64_t* nv, const uint64_t** dt, uint64_t* nt) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(c->have_mesh, PR_ERR_STATE, "no mesh: run a reconstruction first");
+    if (dv) *dv = c->nv ? c->get<double>("mesh_v") : nullptr;
+    if (nv) *nv = c->nv;
+    if (dt) *dt = c->nt ? c->get<uint64_t>("mesh_t") : nullptr;
+    if (nt) *nt = c->nt;
+  });
+}
+
+int pr_ctx_mesh_copy(pr_context* c, pr_mesh* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && out != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_mesh, PR_ERR_STATE, "no mesh: run a reconstruction first");
+    set_device(c);
+    copy_mesh_to_host(c, out);
+  });
+}
+
+int pr_ctx_synchronize(pr_context* c) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    set_device(c);
+    c->sync();
+  });
+}
+
+int pr_ctx_info(pr_context* c, uint32_t* depth, uint64_t* fem_nodes, double* m16) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    if (depth) *depth = c->D;
+    if (fem_nodes) *fem_nodes = c->n;
+    if (m16) std::memcpy(m16, c->M, sizeof(c->M));
+  });
+}
+
+static void copy_dev_to_host(pr_context* c, const char* name, double* out, uint64_t count) {
+  PR_REQUIRE(out != nullptr, PR_ERR_INVALID_ARGUMENT, "output is NULL");
+  set_device(c);
+  PR_CUDA(cudaMemcpyAsync(out, c->get<double>(name), count * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  c->sync();
+}
+
+int pr_ctx_get_coefficients(pr_context* c, double* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(c->have_coeffs, PR_ERR_STATE, "no solved coefficients");
+    copy_dev_to_host(c, "x64", out, c->n);
+  });
+}
+
+int pr_ctx_get_rhs(pr_context* c, double* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    copy_dev_to_host(c, "b64", out, c->n);
+  });
+}
+
+int pr_ctx_get_unit_points(pr_context* c, double* out6) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && out6 != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_points, PR_ERR_STATE, "no points");
+    set_device(c);
+    std::unique_ptr<double[]> pos(new double[3 * c->P]), nrm(new double[3 * c->P]);
+    PR_CUDA(cudaMemcpyAsync(pos.get(), c->get<double>("upos"), 3 * c->P * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    PR_CUDA(cudaMemcpyAsync(nrm.get(), c->get<double>("unrm"), 3 * c->P * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    c->sync();
+    for (uint64_t i = 0; i < c->P; ++i)
+      for (int k = 0; k < 3; ++k) {
+        out6[6 * i + k] = pos[k * c->P + i];
+        out6[6 * i + 3 + k] = nrm[k * c->P + i];
+      }
+  });
+}
+
+int pr_ctx_get_normal_field(pr_context* c, double* out3, double* outw) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && out3 != nullptr && outw != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    set_device(c);
+    double* nf = c->buf<double>("acc_nf3", 3 * c->n);
+    double* w = c->buf<double>("acc_w", c->n);
+    pr::scatter_normal_field(c, nf, w);
+    PR_CUDA(cudaMemcpyAsync(out3, nf, 3 * c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PR_CUDA(cudaMemcpyAsync(outw, w, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    c->release("acc_nf3");
+    c->release("acc_w");
+  });
+}
+
+int pr_ctx_apply_operator(pr_context* c, const double* x, double* y, int precision) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && x != nullptr && y != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    set_device(c);
+    const uint64_t n = c->n;
+    double* dx = c->buf<double>("acc_x", n);
+    double* dy = c->buf<double>("acc_y", n);
+    PR_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (precision == PR_PRECISION_FP64) {
+      pr::apply_operator64(c, dx, dy);
+    } else {
+      float* fx = c->buf<float>("acc_fx", n);
+      float* fy = c->buf<float>("acc_fy", n);
+      pr::scale_convert<double, float>(c->stream, n, 1.0, dx, fx);
+      pr::apply_operator32(c, fx, fy);
+      pr::scale_convert<float, double>(c->stream, n, 1.0, fy, dy);
+    }
+    PR_CUDA(cudaMemcpyAsync(y, dy, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+  });
+}
+
+int pr_ctx_evaluate(pr_context* c, const double* coeffs, const double* pts3, uint64_t n, double* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && (pts3 != nullptr || n == 0) && (out != nullptr || n == 0), PR_ERR_INVALID_ARGUMENT,
+               "NULL argument");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    set_device(c);
+    if (n == 0) return;
+    const double* dx;
+    if (coeffs) {
+      double* t = c->buf<double>("acc_x", c->n);
+      PR_CUDA(cudaMemcpyAsync(t, coeffs, c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      dx = t;
+    } else {
+      PR_REQUIRE(c->have_coeffs, PR_ERR_STATE, "no solved coefficients");
+      dx = c->get<double>("x64");
+    }
+    double* dp = c->buf<double>("acc_pts", 3 * n);
+    double* dout = c->buf<double>("acc_out", n);
+    PR_CUDA(cudaMemcpyAsync(dp, pts3, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    pr::evaluate_points(c, c->D, dx, dp, 3, n, dout);
+    PR_CUDA(cudaMemcpyAsync(out, dout, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+  });
+}
+
+static void extract_common(pr_context* c, uint32_t depth, const double* coeffs, double iso, pr_mesh* out) {
+  PR_REQUIRE(coeffs != nullptr && out != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+  PR_REQUIRE(depth >= pr::kMinDepth && depth <= pr::kMaxDepth, PR_ERR_INVALID_ARGUMENT, "depth must be in [1, 10]");
+  PR_REQUIRE(std::isfinite(iso), PR_ERR_INVALID_ARGUMENT, "iso must be finite");
+  set_device(c);
+  std::memset(out, 0, sizeof(*out));
+  const uint64_t n = 1ull << (3 * depth);
+  double* dx = c->buf<double>("ext_x", n);
+  PR_CUDA(cudaMemcpyAsync(dx, coeffs, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  pr::stage_extract(c, depth, dx, iso, false);
+  copy_mesh_to_host(c, out);
+}
+
+int pr_ctx_extract(pr_context* c, const double* coeffs, double iso, pr_mesh* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    extract_common(c, c->D, coeffs, iso, out);
+  });
+}
+
+int pr_ctx_extract_at_depth(pr_context* c, uint32_t depth, const double* coeffs, double iso, pr_mesh* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    extract_common(c, depth, coeffs, iso, out);
+  });
+}
+
+}  // extern "C"

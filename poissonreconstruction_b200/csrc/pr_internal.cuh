@@ -1,0 +1,202 @@
+// Internal declarations shared by the CUDA translation units of libpoisson_recon_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/poisson_recon.h"
+
+namespace pr {
+
+// ------------------------------------------------------------------ errors
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define PR_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) {                                                                       \
+      int code_ = (e_ == cudaErrorMemoryAllocation) ? PR_ERR_OUT_OF_MEMORY : PR_ERR_CUDA;          \
+      throw ::pr::Error(code_, std::string(#call) + " failed: " + cudaGetErrorString(e_) + " at " + \
+                                   __FILE__ + ":" + std::to_string(__LINE__));                     \
+    }                                                                                              \
+  } while (0)
+
+// Every kernel launch of the library is followed by PR_CHECK_LAUNCH (error check + count);
+// every CUB primitive call by PR_COUNT_PRIMITIVE.
+extern "C" void pr_count_launch_(int primitive);
+#define PR_CHECK_LAUNCH()   \
+  do {                      \
+    pr_count_launch_(0);    \
+    PR_CUDA(cudaGetLastError()); \
+  } while (0)
+#define PR_COUNT_PRIMITIVE() pr_count_launch_(1)
+
+#define PR_REQUIRE(cond, code, msg)         \
+  do {                                      \
+    if (!(cond)) throw ::pr::Error(code, msg); \
+  } while (0)
+
+// ------------------------------------------------------------------ limits
+constexpr uint32_t kMinDepth = 1;
+constexpr uint32_t kMaxDepth = 10;              // dense grid: 2^30 nodes, 32-bit node index
+constexpr uint64_t kMaxPoints = 1ull << 28;     // 8 x points must fit a 31-bit pair index
+constexpr uint32_t kCoarsestDepth = 3;          // multigrid direct-solve level (512 nodes)
+constexpr int kDotBlocks = 1184;                // 8 x 148 SMs: fixed => deterministic dots
+
+// ------------------------------------------------------------------ Morton (x in bit 0)
+__host__ __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> 30 bits
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2)) & 0x030c30c3u;
+  v = (v | (v >> 4)) & 0x0300f00fu;
+  v = (v | (v >> 8)) & 0x030000ffu;
+  v = (v | (v >> 16)) & 0x000003ffu;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+__host__ __device__ __forceinline__ void unmorton3(uint32_t m, uint32_t& x, uint32_t& y, uint32_t& z) {
+  x = compact3(m);
+  y = compact3(m >> 1);
+  z = compact3(m >> 2);
+}
+
+// ------------------------------------------------------------------ exact FP64 (no contraction)
+// The crate (Rust) never fuses multiply-add; kernels that must match it bit for bit use
+// these round-to-nearest intrinsics, which the compiler never contracts.
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// Rust `f64 as i64` (saturating, NaN -> 0)
+__host__ __device__ __forceinline__ int64_t sat_i64(double v) {
+  if (v != v) return 0;
+  if (v >= 9223372036854775807.0) return INT64_MAX;
+  if (v <= -9223372036854775808.0) return INT64_MIN;
+  return (int64_t)v;
+}
+// Rust `f64 as u64` (saturating, NaN -> 0)
+__host__ __device__ __forceinline__ uint64_t sat_u64(double v) {
+  if (!(v > 0.0)) return 0;
+  if (v >= 18446744073709551615.0) return UINT64_MAX;
+  return (uint64_t)v;
+}
+
+// ------------------------------------------------------------------ device buffers
+struct DBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace pr
+
+// The context: one device, one stream, named device buffers reused across calls.
+struct pr_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::map<std::string, pr::DBuf> bufs;
+  size_t bytes_held = 0, peak_bytes = 0;
+  // pinned scalar staging (dot products, counters)
+  double* h_scalars = nullptr;  // 64 doubles
+  // --- state of the last reconstruction ---
+  bool have_state = false;
+  bool have_points = false;
+  uint32_t D = 0;
+  uint64_t n = 0;        // res^3
+  uint64_t P = 0;        // input points
+  uint64_t T = 0;        // splat-touched nodes
+  uint64_t S = 0;        // screened nodes
+  uint64_t S_pairs = 0;  // valid screening (node, point) pairs
+  uint64_t P_in = 0;     // points with >= 1 screening node
+  double pw = 0.0;
+  double M[16], Minv[16];
+  bool have_mesh = false;
+  uint64_t nv = 0, nt = 0;
+  bool have_coeffs = false;
+
+  template <typename T>
+  T* buf(const std::string& name, size_t count) {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    pr::DBuf& b = bufs[name];
+    if (b.cap < bytes) {
+      if (b.ptr) {
+        PR_CUDA(cudaStreamSynchronize(stream));
+        PR_CUDA(cudaFree(b.ptr));
+        bytes_held -= b.cap;
+        b.ptr = nullptr;
+        b.cap = 0;
+      }
+      size_t cap = (bytes + 255) & ~size_t(255);
+      cudaError_t e = cudaMalloc(&b.ptr, cap);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.ptr = nullptr;
+        throw pr::Error(PR_ERR_OUT_OF_MEMORY, "cudaMalloc(" + std::to_string(cap) + " bytes) for '" + name +
+                                                  "' failed: " + cudaGetErrorString(e));
+      }
+      b.cap = cap;
+      bytes_held += cap;
+      if (bytes_held > peak_bytes) peak_bytes = bytes_held;
+    }
+    return reinterpret_cast<T*>(b.ptr);
+  }
+  template <typename T>
+  T* get(const std::string& name) {
+    auto it = bufs.find(name);
+    if (it == bufs.end() || !it->second.ptr) throw pr::Error(PR_ERR_INTERNAL, "missing device buffer '" + name + "'");
+    return reinterpret_cast<T*>(it->second.ptr);
+  }
+  void release(const std::string& name) {
+    auto it = bufs.find(name);
+    if (it == bufs.end() || !it->second.ptr) return;
+    PR_CUDA(cudaStreamSynchronize(stream));
+    PR_CUDA(cudaFree(it->second.ptr));
+    bytes_held -= it->second.cap;
+    bufs.erase(it);
+  }
+  void sync() { PR_CUDA(cudaStreamSynchronize(stream)); }
+};
+
+namespace pr {
+
+// ------------------------------------------------------------------ stage entry points
+// setup (pr_setup.cu)
+void stage_transform(pr_context* c, const double* d_pts6, uint64_t n, double scale);
+void stage_splat_rhs(pr_context* c, uint32_t depth, double pw);
+// solve (pr_solve.cu): fills "x64"; returns rel residual etc. in stats
+void stage_solve(pr_context* c, const pr_params& p, pr_stats& st);
+// extract (pr_mc.cu)
+double stage_iso(pr_context* c, const double* d_x64);
+void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform);
+void evaluate_points(pr_context* c, uint32_t depth, const double* d_x64, const double* d_pts, uint64_t stride,
+                     uint64_t n, double* d_out);
+
+// operator helpers (pr_operator.cu), exposed for tests through the ABI
+void apply_operator64(pr_context* c, const double* d_x, double* d_y);
+void apply_operator32(pr_context* c, const float* d_x, float* d_y);
+
+// dense-scatter helpers for accessors
+void scatter_normal_field(pr_context* c, double* d_nf3, double* d_w);
+
+double dot64(pr_context* c, const double* a, const double* b, uint64_t n);
+
+}  // namespace pr

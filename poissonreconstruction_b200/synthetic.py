@@ -1,0 +1,89 @@
+"""Seeded synthetic oriented point clouds for tests and benchmarks.
+
+No public dataset is named for this workload, so every input is generated here from a
+fixed seed (numpy PCG64, seed = 20260000 + workload number).  Points are AoS rows
+``x y z nx ny nz`` in model space (float64 arrays; the "FP32 storage" workloads are
+rounded through float32 first).
+"""
+import numpy as np
+
+SEED_BASE = 20260000
+
+
+def _rng(seed):
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def sphere(n=100_000, seed=SEED_BASE + 1, radius=1.0):
+    """Uniform on a sphere centred at the origin, exact outward unit normals, FP64."""
+    rng = _rng(seed)
+    g = rng.standard_normal((n, 3))
+    u = g / np.linalg.norm(g, axis=1, keepdims=True)
+    return np.ascontiguousarray(np.hstack([radius * u, u]))
+
+
+def _tangent_rotate(rng, normals, angles):
+    """Rotate each unit normal by ``angles`` about a uniformly random tangent axis."""
+    a = rng.standard_normal(normals.shape)
+    a -= np.sum(a * normals, axis=1, keepdims=True) * normals
+    a /= np.linalg.norm(a, axis=1, keepdims=True)
+    b = np.cross(normals, a)  # tangent direction the normal tips towards
+    c, s = np.cos(angles)[:, None], np.sin(angles)[:, None]
+    out = c * normals + s * b
+    return out / np.linalg.norm(out, axis=1, keepdims=True)
+
+
+def torus(n=2_000_000, seed=SEED_BASE + 2, R=1.0, r=0.35, noise=0.002, normal_sigma=0.05, fp32=True):
+    """Area-uniform torus samples (rejection on (R + r cos v)/(R + r)), isotropic Gaussian
+    position noise, analytic normals tipped by a Gaussian angle about a random tangent axis."""
+    rng = _rng(seed)
+    us, vs = [], []
+    need = n
+    while need > 0:
+        m = int(need * 1.6) + 1024
+        u = rng.uniform(0, 2 * np.pi, m)
+        v = rng.uniform(0, 2 * np.pi, m)
+        keep = rng.uniform(0, 1, m) < (R + r * np.cos(v)) / (R + r)
+        us.append(u[keep])
+        vs.append(v[keep])
+        need -= int(keep.sum())
+    u = np.concatenate(us)[:n]
+    v = np.concatenate(vs)[:n]
+    cu, su, cv, sv = np.cos(u), np.sin(u), np.cos(v), np.sin(v)
+    pos = np.stack([(R + r * cv) * cu, (R + r * cv) * su, r * sv], axis=1)
+    nrm = np.stack([cv * cu, cv * su, sv], axis=1)
+    pos = pos + noise * rng.standard_normal(pos.shape)
+    nrm = _tangent_rotate(rng, nrm, normal_sigma * rng.standard_normal(n))
+    out = np.hstack([pos, nrm])
+    if fp32:
+        out = out.astype(np.float32).astype(np.float64)
+    return np.ascontiguousarray(out)
+
+
+def ellipsoid(n, seed, radii=(1.0, 0.7, 0.5), noise=0.0, fp32=False):
+    """Approximately area-uniform ellipsoid samples (rejection on the area element)."""
+    rng = _rng(seed)
+    a, b, c = radii
+    pts = []
+    need = n
+    while need > 0:
+        m = int(need * 2) + 1024
+        g = rng.standard_normal((m, 3))
+        u = g / np.linalg.norm(g, axis=1, keepdims=True)
+        p = u * np.array(radii)
+        nrm = p / np.array(radii) ** 2
+        dens = np.linalg.norm(nrm, axis=1) * a * b * c / np.array(radii).max()
+        keep = rng.uniform(0, 1, m) * dens.max() < dens
+        pts.append(np.hstack([p[keep], nrm[keep] / np.linalg.norm(nrm[keep], axis=1, keepdims=True)]))
+        need -= int(keep.sum())
+    out = np.concatenate(pts)[:n]
+    out[:, :3] += noise * rng.standard_normal((n, 3))
+    if fp32:
+        out = out.astype(np.float32).astype(np.float64)
+    return np.ascontiguousarray(out)
+
+
+WORKLOADS = {
+    "sphere_100k": dict(fn=sphere, depth=8, point_weight=4.0),
+    "torus_2m": dict(fn=torus, depth=10, point_weight=4.0),
+}
