@@ -207,7 +207,9 @@ def run_ours(a):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = dist_init(ws, "nccl")
-    stream = torch.cuda.current_stream(dev)
+    # the library runs on this (non-default) stream, so CUDA events recorded on it time its kernels
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx = prb.Context(local, stream=stream.cuda_stream)
 
     pts = synthetic.torus(a.points, seed=synthetic.SEED_BASE + 2 + 1000 * rank)
