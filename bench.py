@@ -53,6 +53,13 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=None, help="steps of the FP64 comparison (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-reps", type=int, default=20)
+    ap.add_argument("--kernel", default=None,
+                    help="micro-benchmark one solver kernel at --depth (spmv, spmv_xpby, smooth_first, smooth, "
+                         "smooth_prolong_dot, resid_restrict, stencil_per_node, or 'all')")
+    ap.add_argument("--fp64", action="store_true", help="--kernel in FP64")
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--only-device", action="store_true",
+                    help="warm-up + timed device-resident steps only (for profiler launch lists)")
     return ap.parse_args()
 
 
@@ -250,6 +257,14 @@ def run_ours(a):
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
+    if a.only_device:
+        if rank == 0:
+            st = stats[-1]
+            print(json.dumps({"ms_per_step": statistics.mean(ms_list), "solve_ms": 1000 * st.time_solve,
+                              "pcg_iterations": st.pcg_iterations, "refinement_steps": st.refinement_steps,
+                              "rel_residual": st.rel_residual, "launches_per_step": (l1 - l0) / max(1, a.steps)}))
+        ctx.close()
+        return 0
     ms_mean = statistics.mean(ms_list)
     ms_max = reduce_max(dist, ms_mean, dev)
     total_points = reduce_sum(dist, float(P), dev)
@@ -352,8 +367,29 @@ def run_ours(a):
     return 0
 
 
+def run_kernel_bench(a):
+    import poissonreconstruction_b200 as prb
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        pass
+    names = list(prb.Context.KERNELS) if a.kernel == "all" else [a.kernel]
+    prec = prb.PR_PRECISION_FP64 if a.fp64 else prb.PR_PRECISION_MIXED
+    with prb.Context(0) as ctx:
+        for nm in names:
+            ms, by = ctx.kernel_bench(nm, a.depth, prec, a.reps)
+            gbs = by / (ms / 1000.0) / 1e9
+            print(json.dumps({"kernel": nm, "depth": a.depth, "dtype": "f64" if a.fp64 else "f32",
+                              "ms_per_launch": ms, "algorithmic_bytes": by, "achieved_gbs": gbs,
+                              "frac_of_measured_peak": gbs / peak if peak else None}), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.kernel:
+        return run_kernel_bench(a)
     if a.impl == "reference":
         return run_reference(a)
     return run_ours(a)

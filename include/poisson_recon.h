@@ -163,6 +163,15 @@ int pr_ctx_extract_at_depth(pr_context* ctx, uint32_t depth, const double* coeff
  * For benchmarks of the operator kernel. */
 int pr_ctx_apply_operator_device(pr_context* ctx, const void* d_x, void* d_y, int precision);
 
+/* Micro-benchmark of one solver kernel on context-owned buffers at `depth` (4..10):
+ * kernel 0 = fine-level stencil SpMV, 1 = SpMV fused with d = z + beta d, 2 = multigrid
+ * smoothing sweep from zero, 3 = smoothing sweep, 4 = smoothing sweep fused with the
+ * prolongation and a dot product, 5 = residual fused with the restriction, 6 = per-node
+ * stencil.  Times `reps` launches with CUDA events on the context's stream; returns the
+ * mean ms per launch and the algorithmic HBM bytes per launch. */
+int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precision, int reps, double* ms_per_launch,
+                        double* bytes_per_launch);
+
 /* Number of kernels launched by this library in this process (own kernels; library
  * primitives such as radix sorts and scans are counted in *primitive_calls). */
 uint64_t pr_kernel_launches(uint64_t* primitive_calls);

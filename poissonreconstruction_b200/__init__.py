@@ -63,6 +63,8 @@ SIGNATURES = {
     "pr_abi_layout": (None, [_P]),
     "pr_kernel_launches": (C.c_uint64, [C.POINTER(C.c_uint64)]),
     "pr_ctx_apply_operator_device": (C.c_int, [_P, _P, _P, C.c_int]),
+    "pr_ctx_kernel_bench": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)]),
     "pr_last_error": (C.c_char_p, []),
     "pr_params_default": (PrParams, []),
     "pr_reconstruct": (C.c_int, [_P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrMesh), C.POINTER(PrStats)]),
@@ -297,6 +299,16 @@ class Context:
     def apply_operator_device(self, d_x, d_y, precision=PR_PRECISION_MIXED):
         """Enqueue y = A x on device pointers (no synchronisation)."""
         _check(lib().pr_ctx_apply_operator_device(self._h, C.c_void_p(d_x), C.c_void_p(d_y), int(precision)))
+
+    KERNELS = {"spmv": 0, "spmv_xpby": 1, "smooth_first": 2, "smooth": 3, "smooth_prolong_dot": 4,
+               "resid_restrict": 5, "stencil_per_node": 6}
+
+    def kernel_bench(self, kernel, depth, precision=PR_PRECISION_MIXED, reps=10):
+        """(ms per launch, algorithmic bytes per launch) of one solver kernel."""
+        ms, by = C.c_double(), C.c_double()
+        _check(lib().pr_ctx_kernel_bench(self._h, self.KERNELS[kernel], int(depth), int(precision), int(reps),
+                                         C.byref(ms), C.byref(by)))
+        return ms.value, by.value
 
     def evaluate(self, pts3, coefficients=None):
         pts3 = np.ascontiguousarray(pts3, dtype=np.float64).reshape(-1, 3)

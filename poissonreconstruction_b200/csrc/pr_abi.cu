@@ -15,7 +15,7 @@
 
 #include <cmath>
 
-#include "pr_ops.cuh"
+#include "pr_mg.cuh"
 
 namespace pr {
 void stage_solve_reference(pr_context* c, const pr_params& p, pr_stats& st);
@@ -185,6 +185,15 @@ int pr_ctx_apply_operator_device(pr_context* c, const void* d_x, void* d_y, int 
     set_device(c);
     if (precision == PR_PRECISION_FP64) pr::apply_operator64(c, (const double*)d_x, (double*)d_y);
     else pr::apply_operator32(c, (const float*)d_x, (float*)d_y);
+  });
+}
+
+int pr_ctx_kernel_bench(pr_context* c, int kernel, uint32_t depth, int precision, int reps, double* ms,
+                        double* bytes) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && ms != nullptr && bytes != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    set_device(c);
+    *ms = pr::kernel_bench(c, kernel, depth, precision, reps, bytes);
   });
 }
 

@@ -1,0 +1,1415 @@
+// Block-tiled multigrid and CG kernels.
+//
+// Vectors live in Morton order, so a TB^3 block (TB = 8 or 16) is TB^3 consecutive
+// entries: a CTA loads its block with coalesced loads, gathers the one-node halo of its
+// 26 neighbour blocks, and works in shared memory.  No kernel writes a vector that it
+// (or another CTA of the same launch) reads as halo: every halo-reading update writes a
+// second buffer, so each launch is deterministic.
+//
+// Operator of level l (Galerkin, exact for the 1-D linear prolongation):
+//   A_l = H (S_l (x) M_l (x) M_l + M_l (x) S_l (x) M_l + M_l (x) M_l (x) S_l) + shift I
+// with H the finest spacing and 1-D matrices M_l, S_l that are tridiagonal Toeplitz except
+// for the diagonal entry of node 0 (the coarse basis function at 0 is cut at the domain's
+// low face: the fine grid has no node -1).  Interior nodes see the crate's constant
+// stencil (src/fem_tree.rs:39-48) scaled to their level — centre, 12 edge and 8 corner
+// neighbours; nodes on a low face use per-face coefficients from an 8 x 27 table.
+//
+// Smoother: multicolour Gauss-Seidel inside each block (8 parity colours, exact), blocks
+// coupled through their halo values from before the sweep.  Forward sweeps relax colours
+// 0..7 and backward sweeps 7..0, each the adjoint of the other, so the V-cycle (forward
+// pre-, backward post-smoothing) is a symmetric preconditioner.  The smoother keeps its
+// tile in a parity-split layout (8 sub-tiles, one per parity class), in which the nodes
+// of one colour are contiguous and a warp's neighbour loads hit distinct banks.
+#include <cub/cub.cuh>
+
+#include <mutex>
+#include <set>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "pr_mg.cuh"
+
+namespace pr {
+
+namespace {
+
+template <int TB>
+struct Geo {
+  static constexpr int W = TB + 2;                  // tile width with a one-node halo
+  static constexpr int H = W / 2;                   // parity sub-tile width
+  static constexpr int H3 = H * H * H;
+  static constexpr int N = TB * TB * TB;            // nodes of a block
+  static constexpr int C = TB / 2;                  // colour lattice width
+  static constexpr int C3 = C * C * C;
+  static constexpr int LOGC = TB == 16 ? 3 : 2;
+  static constexpr int LT = TB == 16 ? 4 : 3;
+  static constexpr int THREADS = C3;                // one node per colour per thread
+  static constexpr int HALO = W * W * W - N;
+};
+
+template <typename T>
+struct DevCoef {
+  T c0, ce, cc;       // interior: centre (+shift), edge, corner (faces are 0 in the interior)
+  const T* table;     // [8 low-face masks][27 offsets], offset (dx+1) + 3(dy+1) + 9(dz+1)
+  int has_faces;      // level has low-face modifications
+};
+
+// parity-split index of tile coordinate u in [0, W)^3
+template <int TB>
+__device__ __forceinline__ int ps_index(int ux, int uy, int uz) {
+  constexpr int H = Geo<TB>::H, H3 = Geo<TB>::H3;
+  const int sub = (ux & 1) | ((uy & 1) << 1) | ((uz & 1) << 2);
+  return sub * H3 + ((uz >> 1) * H + (uy >> 1)) * H + (ux >> 1);
+}
+
+// h-th position of the one-node halo shell of a (TB+2)^3 tile: 6 faces, 12 edges, 8 corners
+template <int TB>
+__device__ __forceinline__ void halo_u(int h, int& ux, int& uy, int& uz) {
+  constexpr int W = TB + 2, F = TB * TB, LT = Geo<TB>::LT;
+  if (h < 6 * F) {
+    const int f = h >> (2 * LT), a = (h & (F - 1)) & (TB - 1), b = (h & (F - 1)) >> LT;
+    const int axis = f >> 1, side = (f & 1) ? W - 1 : 0;
+    if (axis == 0) { ux = side; uy = a + 1; uz = b + 1; }
+    else if (axis == 1) { ux = a + 1; uy = side; uz = b + 1; }
+    else { ux = a + 1; uy = b + 1; uz = side; }
+    return;
+  }
+  h -= 6 * F;
+  if (h < 12 * TB) {
+    const int e = h >> LT, a = (h & (TB - 1)) + 1, axis = e >> 2;
+    const int s0 = (e & 1) ? W - 1 : 0, s1 = (e & 2) ? W - 1 : 0;
+    if (axis == 0) { ux = a; uy = s0; uz = s1; }
+    else if (axis == 1) { ux = s0; uy = a; uz = s1; }
+    else { ux = s0; uy = s1; uz = a; }
+    return;
+  }
+  h -= 12 * TB;
+  ux = (h & 1) ? W - 1 : 0;
+  uy = (h & 2) ? W - 1 : 0;
+  uz = (h & 4) ? W - 1 : 0;
+}
+
+template <typename T>
+__device__ __forceinline__ T ldg_or0(const T* __restrict__ x, int gx, int gy, int gz, int res) {
+  if (gx < 0 || gy < 0 || gz < 0 || gx >= res || gy >= res || gz >= res) return (T)0;
+  return __ldg(x + morton3(gx, gy, gz));
+}
+
+// ------------------------------------------------------------------ smoother
+// MODE 0: xo = sweep(xi); MODE 1: xo = sweep(0) (xi unused); MODE 2: xo = sweep(xi + P ec).
+// DOT: part[block] = sum_i f_i xo_i over the block.
+template <typename T, int TB, int MODE, bool DOT, bool FWD>
+__global__ void __launch_bounds__(Geo<TB>::THREADS) k_smooth(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo,
+                                                           const T* __restrict__ f, const T* __restrict__ ec,
+                                                           DevCoef<T> k, double* __restrict__ part) {
+  using G = Geo<TB>;
+  constexpr int W = G::W, H = G::H, H3 = G::H3, N = G::N, C = G::C, C3 = G::C3, LOGC = G::LOGC;
+  constexpr int CW = TB / 2 + 2;  // coarse tile width (MODE 2): coarse [ox/2 - 1, ox/2 + TB/2]
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);  // W^3, parity-split
+  T* fs = tile + W * W * W;                  // N, colour-major: fs[col * C3 + lattice index]
+  T* ctile = fs + N;                         // CW^3 (MODE 2)
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * N;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int ox = (int)bx * TB, oy = (int)by * TB, oz = (int)bz * TB;
+  const int tid = threadIdx.x;
+  const int cox = ox / 2 - 1, coy = oy / 2 - 1, coz = oz / 2 - 1;
+
+  if (MODE == 2) {
+    const int resc = res >> 1;
+    for (int t = tid; t < CW * CW * CW; t += G::THREADS) {
+      const int cx = cox + t % CW, cy = coy + (t / CW) % CW, cz = coz + t / (CW * CW);
+      T v = 0;
+      if (cx >= 0 && cx < resc && cy >= 0 && cy < resc && cz >= 0 && cz < resc) v = __ldg(ec + morton3(cx, cy, cz));
+      ctile[t] = v;
+    }
+    __syncthreads();
+  }
+  // P ec at global (gx,gy,gz): even -> coarse g/2 (w 1), odd -> (g-1)/2, (g+1)/2 (w 1/2 each)
+  auto prolong = [&](int gx, int gy, int gz) -> T {
+    const int ax = (gx >> 1) - cox, ay = (gy >> 1) - coy, az = (gz >> 1) - coz;
+    const int nx = 1 + (gx & 1), ny = 1 + (gy & 1), nz = 1 + (gz & 1);
+    T s = 0;
+    for (int a = 0; a < nz; ++a)
+      for (int b = 0; b < ny; ++b)
+        for (int c = 0; c < nx; ++c) s += ctile[((az + a) * CW + (ay + b)) * CW + (ax + c)];
+    const T w = (T)(((gx & 1) ? 0.5 : 1.0) * ((gy & 1) ? 0.5 : 1.0) * ((gz & 1) ? 0.5 : 1.0));
+    return w * s;
+  };
+  // interior + f
+  for (int t = tid; t < N; t += G::THREADS) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)t, lx, ly, lz);
+    const int col = (lx & 1) | ((ly & 1) << 1) | ((lz & 1) << 2);
+    const int lat = (lx >> 1) | ((ly >> 1) << LOGC) | ((lz >> 1) << (2 * LOGC));
+    fs[col * C3 + lat] = __ldg(f + base + t);
+    T v = 0;
+    if (MODE != 1) v = __ldg(xi + base + t);
+    if (MODE == 2) v += prolong(ox + (int)lx, oy + (int)ly, oz + (int)lz);
+    tile[ps_index<TB>(lx + 1, ly + 1, lz + 1)] = v;
+  }
+  // halo
+  for (int h = tid; h < G::HALO; h += G::THREADS) {
+    int ux, uy, uz;
+    halo_u<TB>(h, ux, uy, uz);
+    T v = 0;
+    if (MODE != 1) {
+      const int gx = ox + ux - 1, gy = oy + uy - 1, gz = oz + uz - 1;
+      if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) {
+        v = __ldg(xi + morton3(gx, gy, gz));
+        if (MODE == 2) v += prolong(gx, gy, gz);
+      }
+    }
+    tile[ps_index<TB>(ux, uy, uz)] = v;
+  }
+  __syncthreads();
+
+  // Gauss-Seidel over the 8 colours
+  const int li = tid & (C - 1), lj = (tid >> LOGC) & (C - 1), lk = tid >> (2 * LOGC);
+#pragma unroll
+  for (int step = 0; step < 8; ++step) {
+    const int col = FWD ? step : 7 - step;
+    const int cx = col & 1, cy = (col >> 1) & 1, cz = col >> 2;
+    const int own = (1 - cx) | ((1 - cy) << 1) | ((1 - cz) << 2);  // sub-tile of tile coordinate l + 1
+    const int pos = ((lk + cz) * H + (lj + cy)) * H + (li + cx);
+    const int self = own * H3 + pos;
+    int mask = 0;
+    if (k.has_faces)
+      mask = ((ox == 0 && cx == 0 && li == 0) ? 1 : 0) | ((oy == 0 && cy == 0 && lj == 0) ? 2 : 0) |
+             ((oz == 0 && cz == 0 && lk == 0) ? 4 : 0);
+    T vals[27];
+#pragma unroll
+    for (int o = 0; o < 27; ++o) {
+      const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+      const int sub = own ^ ((dx != 0) | ((dy != 0) << 1) | ((dz != 0) << 2));
+      const int hx = dx == 0 ? 0 : (dx < 0 ? -cx : 1 - cx);
+      const int hy = dy == 0 ? 0 : (dy < 0 ? -cy : 1 - cy);
+      const int hz = dz == 0 ? 0 : (dz < 0 ? -cz : 1 - cz);
+      const int nzc = (dx != 0) + (dy != 0) + (dz != 0);
+      // faces are only read on the (rare) low-face path
+      vals[o] = (o == 13 || (nzc == 1 && mask == 0)) ? (T)0 : tile[sub * H3 + pos + (hz * H + hy) * H + hx];
+    }
+    const T fi = fs[col * C3 + tid];
+    T nv;
+    if (mask == 0) {
+      T se = 0, sc = 0;
+#pragma unroll
+      for (int o = 0; o < 27; ++o) {
+        const int nzc = (o % 3 != 1) + ((o / 3) % 3 != 1) + (o / 9 != 1);
+        if (nzc == 2) se += vals[o];
+        else if (nzc == 3) sc += vals[o];
+      }
+      nv = (fi - k.ce * se - k.cc * sc) / k.c0;
+    } else {
+      const T* cm = k.table + 27 * mask;
+      T off = 0;
+#pragma unroll
+      for (int o = 0; o < 27; ++o)
+        if (o != 13) off += cm[o] * vals[o];
+      nv = (fi - off) / cm[13];
+    }
+    tile[self] = nv;
+    __syncthreads();
+  }
+
+  double acc = 0.0;
+  for (int t = tid; t < N; t += G::THREADS) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)t, lx, ly, lz);
+    const T v = tile[ps_index<TB>(lx + 1, ly + 1, lz + 1)];
+    xo[base + t] = v;
+    if (DOT) {
+      const int col = (lx & 1) | ((ly & 1) << 1) | ((lz & 1) << 2);
+      const int lat = (lx >> 1) | ((ly >> 1) << LOGC) | ((lz >> 1) << (2 * LOGC));
+      acc += (double)v * (double)fs[col * C3 + lat];
+    }
+  }
+  if (DOT) {
+    typedef cub::BlockReduce<double, Geo<TB>::THREADS> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double s = BR(tmp).Sum(acc);
+    if (tid == 0) part[blk] = s;
+  }
+}
+
+// ------------------------------------------------------------------ stencil rows on a natural tile
+// tile index (ux,uy,uz) -> (uz*W + uy)*W + ux
+template <typename T, int W>
+__device__ __forceinline__ T row_general(const T* __restrict__ s, int idx, const T* __restrict__ cm) {
+  T r = 0;
+#pragma unroll
+  for (int o = 0; o < 27; ++o) {
+    const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+    r += cm[o] * s[idx + dx + W * dy + W * W * dz];
+  }
+  return r;
+}
+
+template <typename T, int W>
+__device__ __forceinline__ T row_interior(const T* __restrict__ s, int idx, T c0, T ce, T cc) {
+  T se = 0, sc = 0;
+#pragma unroll
+  for (int o = 0; o < 27; ++o) {
+    const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+    const int nzc = (dx != 0) + (dy != 0) + (dz != 0);
+    if (nzc == 2) se += s[idx + dx + W * dy + W * W * dz];
+    else if (nzc == 3) sc += s[idx + dx + W * dy + W * W * dz];
+  }
+  return c0 * s[idx] + ce * se + cc * sc;
+}
+
+// Column sweep along z: for the column (ux,uy) of a natural tile, output A x at tile
+// z coordinates uz0..uz0+ZL-1 through fn(k, centre value, row value).  Plane partial sums
+// are shared by the three outputs that use them.
+template <typename T, int W, int ZL, typename Fn>
+__device__ __forceinline__ void column_apply(const T* __restrict__ s, int ux, int uy, int uz0, T c0, T ce, T cc,
+                                             Fn fn) {
+  auto plane = [&](int uz, T& pc, T& pf, T& pe) {
+    const int b = (uz * W + uy) * W + ux;
+    pc = s[b];
+    pf = s[b - 1] + s[b + 1] + s[b - W] + s[b + W];
+    pe = s[b - 1 - W] + s[b + 1 - W] + s[b - 1 + W] + s[b + 1 + W];
+  };
+  T pcm, pfm, pem, pc0, pf0, pe0;
+  plane(uz0 - 1, pcm, pfm, pem);
+  plane(uz0, pc0, pf0, pe0);
+#pragma unroll
+  for (int k = 0; k < ZL; ++k) {
+    T pcp, pfp, pep;
+    plane(uz0 + k + 1, pcp, pfp, pep);
+    fn(k, pc0, c0 * pc0 + ce * (pe0 + pfm + pfp) + cc * (pem + pep));
+    pcm = pc0;
+    pfm = pf0;
+    pem = pe0;
+    pc0 = pcp;
+    pf0 = pfp;
+    pe0 = pep;
+  }
+  (void)pcm;
+}
+
+// ------------------------------------------------------------------ fine-level SpMV
+// XPBY: dn = z + beta d (tile and halo), dn written; q = A dn (stencil part); part = dn.q
+template <typename T, int TB, bool XPBY>
+__global__ void __launch_bounds__(Geo<TB>::THREADS) k_spmv(uint32_t D, const T* __restrict__ z,
+                                                         const T* __restrict__ d, T* __restrict__ dn, T beta,
+                                                         T* __restrict__ q, DevCoef<T> k, double* __restrict__ part) {
+  using G = Geo<TB>;
+  constexpr int W = G::W, N = G::N;
+  constexpr int SEG = G::THREADS / (TB * TB);  // z segments per column
+  constexpr int ZL = TB / SEG;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);  // W^3 natural
+  T* out = tile + W * W * W;                 // N, Morton-local
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * N;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int ox = (int)bx * TB, oy = (int)by * TB, oz = (int)bz * TB;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < N; t += G::THREADS) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)t, lx, ly, lz);
+    T v = __ldg(d + base + t);
+    if (XPBY) {
+      v = __ldg(z + base + t) + beta * v;
+      out[t] = v;  // staged dn for the coalesced store below
+    }
+    tile[((lz + 1) * W + (ly + 1)) * W + (lx + 1)] = v;
+  }
+  for (int h = tid; h < G::HALO; h += G::THREADS) {
+    int ux, uy, uz;
+    halo_u<TB>(h, ux, uy, uz);
+    const int gx = ox + ux - 1, gy = oy + uy - 1, gz = oz + uz - 1;
+    T v = 0;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) {
+      const uint32_t m = morton3(gx, gy, gz);
+      v = __ldg(d + m);
+      if (XPBY) v = __ldg(z + m) + beta * v;
+    }
+    tile[(uz * W + uy) * W + ux] = v;
+  }
+  __syncthreads();
+  if (XPBY) {
+    for (int t = tid; t < N; t += G::THREADS) dn[base + t] = out[t];
+    __syncthreads();
+  }
+  const int col = tid % (TB * TB), seg = tid / (TB * TB);
+  const int ux = col % TB + 1, uy = col / TB + 1;
+  double acc = 0.0;
+  column_apply<T, W, ZL>(tile, ux, uy, seg * ZL + 1, k.c0, k.ce, k.cc, [&](int kk, T dv, T y) {
+    const int lz = seg * ZL + kk;
+    out[morton3(ux - 1, uy - 1, lz)] = y;
+    acc += (double)dv * (double)y;
+  });
+  __syncthreads();
+  for (int t = tid; t < N; t += G::THREADS) q[base + t] = out[t];
+  typedef cub::BlockReduce<double, Geo<TB>::THREADS> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double s = BR(tmp).Sum(acc);
+  if (tid == 0) part[blk] = s;
+}
+
+// ------------------------------------------------------------------ residual + restriction
+// fc = P^T (f - A e) for the (TB/2)^3 coarse nodes whose fine centre lies in the block.
+// r is needed on local [-1, TB-1]^3: the block interior (z columns) plus its low shell.
+template <typename T, int TB>
+__global__ void __launch_bounds__(Geo<TB>::THREADS) k_resid_restrict(uint32_t D, const T* __restrict__ e,
+                                                                   const T* __restrict__ f, T* __restrict__ fc,
+                                                                   DevCoef<T> k) {
+  using G = Geo<TB>;
+  constexpr int N = G::N;
+  constexpr int WE = TB + 3;  // e over local [-2, TB]
+  constexpr int WR = TB + 1;  // r over local [-1, TB-1]
+  constexpr int TC = TB / 2;
+  constexpr int SEG = G::THREADS / (TB * TB);
+  constexpr int ZL = TB / SEG;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* et = reinterpret_cast<T*>(smem_raw);  // WE^3 natural, tile coordinate = local + 2
+  T* rt = et + WE * WE * WE;               // WR^3 natural, coordinate = local + 1
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * N;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int ox = (int)bx * TB, oy = (int)by * TB, oz = (int)bz * TB;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < N; t += G::THREADS) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)t, lx, ly, lz);
+    et[((lz + 2) * WE + (ly + 2)) * WE + (lx + 2)] = __ldg(e + base + t);
+    rt[((lz + 1) * WR + (ly + 1)) * WR + (lx + 1)] = __ldg(f + base + t);  // f first, r = f - A e below
+  }
+  for (int t = tid; t < WE * WE * WE; t += G::THREADS) {
+    const int tx = t % WE, ty = (t / WE) % WE, tz = t / (WE * WE);
+    if (tx >= 2 && tx < TB + 2 && ty >= 2 && ty < TB + 2 && tz >= 2 && tz < TB + 2) continue;
+    et[t] = ldg_or0(e, ox + tx - 2, oy + ty - 2, oz + tz - 2, res);
+  }
+  __syncthreads();
+  // interior: z columns with the interior rows
+  {
+    const int col = tid % (TB * TB), seg = tid / (TB * TB);
+    const int lx = col % TB, ly = col / TB;
+    column_apply<T, WE, ZL>(et, lx + 2, ly + 2, seg * ZL + 2, k.c0, k.ce, k.cc, [&](int kk, T, T y) {
+      const int lz = seg * ZL + kk;
+      rt[((lz + 1) * WR + (ly + 1)) * WR + (lx + 1)] -= y;
+    });
+  }
+  // low shell of r: local coordinate -1 on at least one axis
+  {
+    constexpr int S1 = WR * WR, S2 = TB * WR, S3 = TB * TB;
+    for (int t = tid; t < S1 + S2 + S3; t += G::THREADS) {
+      int lx, ly, lz;
+      if (t < S1) { lx = -1; ly = t % WR - 1; lz = t / WR - 1; }
+      else if (t < S1 + S2) { const int u = t - S1; lx = u % TB; ly = -1; lz = u / TB - 1; }
+      else { const int u = t - S1 - S2; lx = u % TB; ly = u / TB; lz = -1; }
+      const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+      T r = 0;
+      if (gx >= 0 && gy >= 0 && gz >= 0) {
+        const int ei = ((lz + 2) * WE + (ly + 2)) * WE + (lx + 2);
+        const int mask = k.has_faces ? ((gx == 0) | ((gy == 0) << 1) | ((gz == 0) << 2)) : 0;
+        const T y = mask ? row_general<T, WE>(et, ei, k.table + 27 * mask) : row_interior<T, WE>(et, ei, k.c0, k.ce, k.cc);
+        r = __ldg(f + morton3(gx, gy, gz)) - y;
+      }
+      rt[((lz + 1) * WR + (ly + 1)) * WR + (lx + 1)] = r;
+    }
+  }
+  __syncthreads();
+  if (k.has_faces && (ox == 0 || oy == 0 || oz == 0)) {
+    // interior nodes on a low domain face: replace the interior row by the face row
+    for (int t = tid; t < N; t += G::THREADS) {
+      uint32_t lx, ly, lz;
+      unmorton3((uint32_t)t, lx, ly, lz);
+      const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+      const int mask = (gx == 0) | ((gy == 0) << 1) | ((gz == 0) << 2);
+      if (!mask) continue;
+      const int ei = ((lz + 2) * WE + (ly + 2)) * WE + (lx + 2);
+      const T yi = row_interior<T, WE>(et, ei, k.c0, k.ce, k.cc);
+      const T yf = row_general<T, WE>(et, ei, k.table + 27 * mask);
+      rt[((lz + 1) * WR + (ly + 1)) * WR + (lx + 1)] += yi - yf;
+    }
+    __syncthreads();
+  }
+  const uint64_t cbase = (uint64_t)blk * (TC * TC * TC);
+  for (int t = tid; t < TC * TC * TC; t += G::THREADS) {
+    uint32_t cx, cy, cz;
+    unmorton3((uint32_t)t, cx, cy, cz);
+    const int fx = 2 * cx + 1, fy = 2 * cy + 1, fz = 2 * cz + 1;  // r tile coordinate of the fine centre
+    T s = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const T w = (T)((dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
+          s += w * rt[((fz + dz) * WR + (fy + dy)) * WR + (fx + dx)];
+        }
+    fc[cbase + t] = s;
+  }
+}
+
+// screening projection with the fused sum of squares: proj[p] = phi(p).x, part = sum proj^2
+template <typename T>
+__global__ void k_screen_project_sq(const uint32_t* __restrict__ key, const T* __restrict__ phi, uint64_t P,
+                                    uint32_t sentinel, const T* __restrict__ x, T* __restrict__ proj,
+                                    double* __restrict__ part) {
+  double acc = 0.0;
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
+    T s = 0;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const uint32_t key_ = key[8 * p + kk];
+      if (key_ != sentinel) s += phi[8 * p + kk] * x[key_];
+    }
+    proj[p] = s;
+    acc += (double)s * (double)s;
+  }
+  typedef cub::BlockReduce<double, 256> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// fixed-order sum of two partial arrays: out = sum(part) + scale2 * sum(part2)
+__global__ void __launch_bounds__(1024) k_sum_parts(const double* __restrict__ part, int np, double scale2,
+                                                    const double* __restrict__ part2, int np2,
+                                                    double* __restrict__ out) {
+  double s = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < np; i += 1024) s += part[i];
+  for (int i = threadIdx.x; i < np2; i += 1024) s2 += part2[i];
+  typedef cub::BlockReduce<double, 1024> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double a = BR(tmp).Sum(s);
+  __syncthreads();
+  const double b = BR(tmp).Sum(s2);
+  if (threadIdx.x == 0) out[0] = a + scale2 * b;
+}
+
+// ------------------------------------------------------------------ 16^3 smoother (levels >= 4)
+// 256 threads.  Tile: parity-split, sub-tile = 9 planes x 100 (9 rows of 9), so that the
+// 32 lanes of a warp (8 x-lattice positions x 4 z-pairs) hit 32 distinct banks.
+namespace s16 {
+constexpr int TB = 16, N = 4096, THREADS = 256;
+constexpr int RS = 9, PS = 100, SUB = 9 * PS;  // row / plane / sub-tile strides
+constexpr int TILE = 8 * SUB;
+constexpr int CW = 10;                         // coarse tile width
+
+__device__ __forceinline__ int ps(int ux, int uy, int uz) {
+  return ((ux & 1) | ((uy & 1) << 1) | ((uz & 1) << 2)) * SUB + (uz >> 1) * PS + (uy >> 1) * RS + (ux >> 1);
+}
+// spread the 4 low bits of v to bit positions 0,3,6,9
+__device__ __forceinline__ uint32_t sp4(uint32_t v) {
+  return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
+}
+// colour-major f layout: thread (li, kp, lj) of colour col reads lk = 2kp + s at
+// ((col*8 + lj)*2 + s)*32 + 8*kp + li  (conflict-free for the lane pattern)
+__device__ __forceinline__ int fidx(int lx, int ly, int lz) {
+  const int col = (lx & 1) | ((ly & 1) << 1) | ((lz & 1) << 2);
+  const int li = lx >> 1, lj = ly >> 1, lk = lz >> 1;
+  return ((col * 8 + lj) * 2 + (lk & 1)) * 32 + 8 * (lk >> 1) + li;
+}
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  typedef float4 type;
+};
+template <>
+struct Vec4<double> {
+  typedef double4 type;
+};
+
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ double4 ld4(const double* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st4(float* p, const float4& v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ void st4(double* p, const double4& v) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v.x, v.y);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v.z, v.w);
+}
+
+// local coordinates of element 4q of a 16^3 Morton block (q = quad index), x0 = y0 = 0
+__device__ __forceinline__ void quad_coords(int q, int& lx, int& ly, int& lz) {
+  lx = ((q >> 1) & 1) << 1 | ((q >> 4) & 1) << 2 | ((q >> 7) & 1) << 3;
+  ly = ((q >> 2) & 1) << 1 | ((q >> 5) & 1) << 2 | ((q >> 8) & 1) << 3;
+  lz = (q & 1) | ((q >> 3) & 1) << 1 | ((q >> 6) & 1) << 2 | ((q >> 9) & 1) << 3;
+}
+
+// Load the one-node halo of the block into a tile (idx: tile index of tile coordinates).
+// nb[27]: Morton base of the neighbour block (dx+1)+3(dy+1)+9(dz+1), or ~0u if outside.
+template <typename T, typename Idx, typename Xf>
+__device__ __forceinline__ void load_halo(T* tile, const T* __restrict__ x, const uint32_t* nb, Idx idx, Xf xf) {
+  const int t = threadIdx.x;
+  {  // faces: (a, b) = thread's in-face coordinates
+    const int a = t & 15, b = t >> 4;
+    const uint32_t sa = sp4(a), sb = sp4(b);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int axis = f >> 1, hi = f & 1;
+      const int nbi = axis == 0 ? (hi ? 14 : 12) : (axis == 1 ? (hi ? 16 : 10) : (hi ? 22 : 4));
+      const uint32_t side = hi ? 0u : 0x249u;  // neighbour-local coordinate 0 or 15, spread
+      uint32_t m;
+      int ux, uy, uz;
+      const int s = hi ? 17 : 0;
+      if (axis == 0) { m = side | (sa << 1) | (sb << 2); ux = s; uy = a + 1; uz = b + 1; }
+      else if (axis == 1) { m = sa | (side << 1) | (sb << 2); ux = a + 1; uy = s; uz = b + 1; }
+      else { m = sa | (sb << 1) | (side << 2); ux = a + 1; uy = b + 1; uz = s; }
+      const uint32_t base = nb[nbi];
+      tile[idx(ux, uy, uz)] = base != ~0u ? xf(base + m) : (T)0;
+    }
+  }
+  if (t < 192) {  // edges: 4 per axis, 16 nodes each
+    const int e = t >> 4, a = t & 15, axis = e >> 2, s1 = e & 1, s2 = (e >> 1) & 1;
+    const uint32_t sa = sp4(a);
+    const uint32_t c1 = s1 ? 0u : 0x249u, c2 = s2 ? 0u : 0x249u;
+    const int d1 = s1 ? 1 : -1, d2 = s2 ? 1 : -1;
+    const int u1 = s1 ? 17 : 0, u2 = s2 ? 17 : 0;
+    uint32_t m;
+    int ux, uy, uz, nbi;
+    if (axis == 0) { m = sa | (c1 << 1) | (c2 << 2); ux = a + 1; uy = u1; uz = u2; nbi = 1 + 3 * (d1 + 1) + 9 * (d2 + 1); }
+    else if (axis == 1) { m = c1 | (sa << 1) | (c2 << 2); ux = u1; uy = a + 1; uz = u2; nbi = (d1 + 1) + 3 + 9 * (d2 + 1); }
+    else { m = c1 | (c2 << 1) | (sa << 2); ux = u1; uy = u2; uz = a + 1; nbi = (d1 + 1) + 3 * (d2 + 1) + 9; }
+    const uint32_t base = nb[nbi];
+    tile[idx(ux, uy, uz)] = base != ~0u ? xf(base + m) : (T)0;
+  } else if (t < 200) {  // corners
+    const int c = t - 192;
+    const int sx = c & 1, sy = (c >> 1) & 1, sz = (c >> 2) & 1;
+    const uint32_t m = (sx ? 0u : 0x249u) | ((sy ? 0u : 0x249u) << 1) | ((sz ? 0u : 0x249u) << 2);
+    const int nbi = (sx ? 2 : 0) + 3 * (sy ? 2 : 0) + 9 * (sz ? 2 : 0);
+    const uint32_t base = nb[nbi];
+    tile[idx(sx ? 17 : 0, sy ? 17 : 0, sz ? 17 : 0)] = base != ~0u ? xf(base + m) : (T)0;
+  }
+}
+
+__device__ __forceinline__ void neighbour_bases(uint32_t* nb, uint32_t bx, uint32_t by, uint32_t bz, int nblk_axis) {
+  const int t = threadIdx.x;
+  if (t < 27) {
+    const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+    const int x = (int)bx + dx, y = (int)by + dy, z = (int)bz + dz;
+    nb[t] = (x < 0 || y < 0 || z < 0 || x >= nblk_axis || y >= nblk_axis || z >= nblk_axis)
+                ? ~0u
+                : (morton3((uint32_t)x, (uint32_t)y, (uint32_t)z) << 12);
+  }
+}
+
+// MODE 0: xo = sweep(xi); 1: xo = sweep(0); 2: xo = sweep(xi + P ec).  DOT: part = f.xo
+template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
+__global__ void __launch_bounds__(THREADS) k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo,
+                                                     const T* __restrict__ f, const T* __restrict__ ec, T c0inv,
+                                                     T ce, T cc, const T* __restrict__ table,
+                                                     double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
+  T* fs = tile + TILE;                       // N
+  T* ctile = fs + N;                         // CW^3 (MODE 2)
+  __shared__ uint32_t nb[27];
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * N;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int ox = (int)bx * TB, oy = (int)by * TB, oz = (int)bz * TB;
+  const int t = threadIdx.x;
+  if (MODE != 1) neighbour_bases(nb, bx, by, bz, res >> 4);
+  else if (t < 27) nb[t] = ~0u;  // zero halo
+  if (MODE == 2) {
+    const int cox = ox / 2 - 1, coy = oy / 2 - 1, coz = oz / 2 - 1, resc = res >> 1;
+    for (int i = t; i < CW * CW * CW; i += THREADS) {
+      const int cx = cox + i % CW, cy = coy + (i / CW) % CW, cz = coz + i / (CW * CW);
+      T v = 0;
+      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < resc && cy < resc && cz < resc) v = __ldg(ec + morton3(cx, cy, cz));
+      ctile[i] = v;
+    }
+  }
+  // interior: 4 quads per thread
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int q = t + 256 * r;
+    int lx, ly, lz;
+    quad_coords(q, lx, ly, lz);
+    const typename Vec4<T>::type fv = ld4(f + base + 4 * q);
+    fs[fidx(lx, ly, lz)] = fv.x;
+    fs[fidx(lx + 1, ly, lz)] = fv.y;
+    fs[fidx(lx, ly + 1, lz)] = fv.z;
+    fs[fidx(lx + 1, ly + 1, lz)] = fv.w;
+    typename Vec4<T>::type xv;
+    if (MODE == 1) xv.x = xv.y = xv.z = xv.w = (T)0;
+    else xv = ld4(xi + base + 4 * q);
+    tile[ps(lx + 1, ly + 1, lz + 1)] = xv.x;
+    tile[ps(lx + 2, ly + 1, lz + 1)] = xv.y;
+    tile[ps(lx + 1, ly + 2, lz + 1)] = xv.z;
+    tile[ps(lx + 2, ly + 2, lz + 1)] = xv.w;
+  }
+  __syncthreads();  // nb
+  load_halo<T>(tile, xi, nb, [](int ux, int uy, int uz) { return ps(ux, uy, uz); },
+               [&](uint32_t m) { return MODE == 1 ? (T)0 : __ldg(xi + m); });
+  __syncthreads();
+  if (MODE == 2) {
+    // tile += P ec: coarse cell m (per axis in [-1, 8]) covers fine tile coordinates 2m+1 (even
+    // global, coarse m+1) and 2m+2 (odd global, mean of coarse m+1 and m+2)
+    for (int i = t; i < 1000; i += THREADS) {
+      const int mx = i % 10 - 1, my = (i / 10) % 10 - 1, mz = i / 100 - 1;
+      T cv[2][2][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int ix = mx + 1 + c, iy = my + 1 + b, iz = mz + 1 + a;
+            cv[a][b][c] = (ix < CW && iy < CW && iz < CW) ? ctile[(iz * CW + iy) * CW + ix] : (T)0;
+          }
+      // along x: even (c0) and odd (0.5 (c0 + c1))
+      T vx[2][2][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          vx[a][b][0] = cv[a][b][0];
+          vx[a][b][1] = (T)0.5 * (cv[a][b][0] + cv[a][b][1]);
+        }
+      T vy[2][2][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          vy[a][0][c] = vx[a][0][c];
+          vy[a][1][c] = (T)0.5 * (vx[a][0][c] + vx[a][1][c]);
+        }
+#pragma unroll
+      for (int sz = 0; sz < 2; ++sz)
+#pragma unroll
+        for (int sy = 0; sy < 2; ++sy)
+#pragma unroll
+          for (int sx = 0; sx < 2; ++sx) {
+            const int ux = 2 * mx + 1 + sx, uy = 2 * my + 1 + sy, uz = 2 * mz + 1 + sz;
+            if (ux < 0 || uy < 0 || uz < 0 || ux > 17 || uy > 17 || uz > 17) continue;
+            const int gx = ox - 1 + ux, gy = oy - 1 + uy, gz = oz - 1 + uz;
+            if (gx < 0 || gy < 0 || gz < 0 || gx >= res || gy >= res || gz >= res) continue;
+            const T v = sz ? (T)0.5 * (vy[0][sy][sx] + vy[1][sy][sx]) : vy[0][sy][sx];
+            tile[ps(ux, uy, uz)] += v;
+          }
+    }
+    __syncthreads();
+  }
+
+  // Gauss-Seidel: lanes = 8 x-lattice positions x 4 z-pairs; warps = 8 y-lattice rows
+  const int li = t & 7, kp = (t >> 3) & 3, lj = t >> 5;
+  const bool faces = FACES && (ox == 0 || oy == 0 || oz == 0);
+#pragma unroll
+  for (int step = 0; step < 8; ++step) {
+    const int col = FWD ? step : 7 - step;
+    const int cx = col & 1, cy = (col >> 1) & 1, cz = col >> 2;
+    const int own = (1 - cx) | ((1 - cy) << 1) | ((1 - cz) << 2);
+    // sub-tile bases of the x/y/xy-flipped neighbours in the three z planes
+    const int hx = li + cx, hy = lj + cy;
+    // offsets inside a sub-tile for dx/dy = -1/+1 (depend on the colour bit)
+    const int xm = -cx, xp = 1 - cx, ym = -cy, yp = 1 - cy;
+    const int zm = -cz, zp = 1 - cz;
+    const int so = own * SUB, sx_ = (own ^ 1) * SUB, sy_ = (own ^ 2) * SUB, sxy = (own ^ 3) * SUB;
+    const int sz_ = (own ^ 4) * SUB, sxz = (own ^ 5) * SUB, syz = (own ^ 6) * SUB, sxyz = (own ^ 7) * SUB;
+    T nv[2];
+    T pfb, peb;  // plane below: cross sum (edges), diagonal sum (corners)
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int lk = 2 * kp + s;
+      const int hz = lk + cz;
+      const int pr = hy * RS + hx;  // row/column part
+      if (s == 0) {
+        const int pz = (hz + zm) * PS;
+        pfb = tile[sxz + pz + pr + xm] + tile[sxz + pz + pr + xp] + tile[syz + pz + pr + ym * RS] +
+              tile[syz + pz + pr + yp * RS];
+        peb = tile[sxyz + pz + pr + ym * RS + xm] + tile[sxyz + pz + pr + ym * RS + xp] +
+              tile[sxyz + pz + pr + yp * RS + xm] + tile[sxyz + pz + pr + yp * RS + xp];
+      }
+      const int p0 = hz * PS;
+      const T peo = tile[sxy + p0 + pr + ym * RS + xm] + tile[sxy + p0 + pr + ym * RS + xp] +
+                    tile[sxy + p0 + pr + yp * RS + xm] + tile[sxy + p0 + pr + yp * RS + xp];
+      const int pa = (hz + zp) * PS;
+      const T pfa = tile[sxz + pa + pr + xm] + tile[sxz + pa + pr + xp] + tile[syz + pa + pr + ym * RS] +
+                    tile[syz + pa + pr + yp * RS];
+      const T pea = tile[sxyz + pa + pr + ym * RS + xm] + tile[sxyz + pa + pr + ym * RS + xp] +
+                    tile[sxyz + pa + pr + yp * RS + xm] + tile[sxyz + pa + pr + yp * RS + xp];
+      const T fi = fs[((col * 8 + lj) * 2 + s) * 32 + 8 * kp + li];
+      T v = (fi - ce * (peo + pfb + pfa) - cc * (peb + pea)) * c0inv;
+      if (faces) {
+        const int mask = ((ox == 0 && cx == 0 && li == 0) ? 1 : 0) | ((oy == 0 && cy == 0 && lj == 0) ? 2 : 0) |
+                         ((oz == 0 && cz == 0 && lk == 0) ? 4 : 0);
+        if (mask) {
+          const T* cm = table + 27 * mask;
+          T off = 0;
+#pragma unroll
+          for (int o = 0; o < 27; ++o) {
+            if (o == 13) continue;
+            const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+            const int sub = own ^ ((dx != 0) | ((dy != 0) << 1) | ((dz != 0) << 2));
+            const int ddx = dx == 0 ? 0 : (dx < 0 ? xm : xp), ddy = dy == 0 ? 0 : (dy < 0 ? ym : yp);
+            const int ddz = dz == 0 ? 0 : (dz < 0 ? zm : zp);
+            off += cm[o] * tile[sub * SUB + (hz + ddz) * PS + (hy + ddy) * RS + hx + ddx];
+          }
+          v = (fi - off) / cm[13];
+        }
+      }
+      nv[s] = v;
+      pfb = pfa;
+      peb = pea;
+      (void)so;
+      (void)sx_;
+      (void)sy_;
+      (void)sz_;
+    }
+    const int pr = hy * RS + hx;
+    tile[so + (2 * kp + cz) * PS + pr] = nv[0];
+    tile[so + (2 * kp + 1 + cz) * PS + pr] = nv[1];
+    __syncthreads();
+  }
+
+  double acc = 0.0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int q = t + 256 * r;
+    int lx, ly, lz;
+    quad_coords(q, lx, ly, lz);
+    typename Vec4<T>::type v;
+    v.x = tile[ps(lx + 1, ly + 1, lz + 1)];
+    v.y = tile[ps(lx + 2, ly + 1, lz + 1)];
+    v.z = tile[ps(lx + 1, ly + 2, lz + 1)];
+    v.w = tile[ps(lx + 2, ly + 2, lz + 1)];
+    st4(xo + base + 4 * q, v);
+    if (DOT)
+      acc += (double)v.x * (double)fs[fidx(lx, ly, lz)] + (double)v.y * (double)fs[fidx(lx + 1, ly, lz)] +
+             (double)v.z * (double)fs[fidx(lx, ly + 1, lz)] + (double)v.w * (double)fs[fidx(lx + 1, ly + 1, lz)];
+  }
+  if (DOT) {
+    typedef cub::BlockReduce<double, THREADS> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double sum = BR(tmp).Sum(acc);
+    if (t == 0) part[blk] = sum;
+  }
+}
+
+template <typename T>
+constexpr size_t smem_bytes(int mode) {
+  return sizeof(T) * (TILE + N + (mode == 2 ? CW * CW * CW : 0));
+}
+}  // namespace s16
+
+// ------------------------------------------------------------------ 16^3 stencil SpMV (finest level)
+// Natural tile, row stride 18, plane stride 326 (8 planes = 16 banks apart): 512 threads =
+// 256 columns x 2 z-halves; lanes = 16 x-columns x 2 halves -> conflict-free plane loads.
+namespace n16 {
+constexpr int N = 4096, THREADS = 512;
+constexpr int RS = 18, PS = 326, TILE = 18 * PS;
+__device__ __forceinline__ int nat(int ux, int uy, int uz) { return uz * PS + uy * RS + ux; }
+
+// KIND 0: q = A d, part = d.q; 1: dn = z + beta d, q = A dn, part = dn.q;
+// 2: xn = x + beta e (x, xn: FP64 solution, e: correction of type E), r = b - A xn
+template <typename T, int KIND, typename E>
+__global__ void __launch_bounds__(THREADS) k_spmv16(uint32_t D, const T* __restrict__ a, const E* __restrict__ bvec,
+                                                   T* __restrict__ an, T beta, T* __restrict__ q, T c0, T ce, T cc,
+                                                   const T* __restrict__ rhs, double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
+  T* out = tile + TILE;                      // N (Morton-local)
+  __shared__ uint32_t nb[27];
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * N;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int t = threadIdx.x;
+  s16::neighbour_bases(nb, bx, by, bz, res >> 4);
+  // value of the (updated) vector at global Morton index m
+  auto val = [&](uint32_t m) -> T {
+    if (KIND == 0) return __ldg(a + m);
+    if (KIND == 1) return (T)__ldg(bvec + m) + beta * __ldg(a + m);
+    return __ldg(a + m) + beta * (T)__ldg(bvec + m);
+  };
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int qd = t + 512 * r;
+    int lx, ly, lz;
+    s16::quad_coords(qd, lx, ly, lz);
+    const uint64_t m = base + 4 * qd;
+    const typename s16::Vec4<T>::type av = s16::ld4(a + m);
+    T v0 = av.x, v1 = av.y, v2 = av.z, v3 = av.w;
+    if (KIND != 0) {
+      const typename s16::Vec4<E>::type bv = s16::ld4(bvec + m);
+      if (KIND == 1) {
+        v0 = (T)bv.x + beta * v0; v1 = (T)bv.y + beta * v1; v2 = (T)bv.z + beta * v2; v3 = (T)bv.w + beta * v3;
+      } else {
+        v0 += beta * (T)bv.x; v1 += beta * (T)bv.y; v2 += beta * (T)bv.z; v3 += beta * (T)bv.w;
+      }
+      out[4 * qd] = v0;
+      out[4 * qd + 1] = v1;
+      out[4 * qd + 2] = v2;
+      out[4 * qd + 3] = v3;
+    }
+    tile[nat(lx + 1, ly + 1, lz + 1)] = v0;
+    tile[nat(lx + 2, ly + 1, lz + 1)] = v1;
+    tile[nat(lx + 1, ly + 2, lz + 1)] = v2;
+    tile[nat(lx + 2, ly + 2, lz + 1)] = v3;
+  }
+  __syncthreads();
+  if (t < 256) s16::load_halo<T>(tile, a, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); }, val);
+  __syncthreads();
+  if (KIND != 0) {  // write the updated vector (coalesced from the staged copy)
+    for (int i = t; i < N; i += THREADS) an[base + i] = out[i];
+    __syncthreads();
+  }
+  // column sweep: lanes = 16 x-columns x 2 z-halves, warps = y rows
+  const int lx = t & 15, half = (t >> 4) & 1, ly = t >> 5;
+  const int ux = lx + 1, uy = ly + 1;
+  const uint32_t mxy = s16::sp4(lx) | (s16::sp4(ly) << 1);
+  auto plane = [&](int uz, T& pc, T& pf, T& pe) {
+    const int b0 = nat(ux, uy, uz);
+    pc = tile[b0];
+    pf = tile[b0 - 1] + tile[b0 + 1] + tile[b0 - RS] + tile[b0 + RS];
+    pe = tile[b0 - 1 - RS] + tile[b0 + 1 - RS] + tile[b0 - 1 + RS] + tile[b0 + 1 + RS];
+  };
+  T pcm, pfm, pem, pc0, pf0, pe0;
+  const int z0 = 8 * half;
+  plane(z0, pcm, pfm, pem);
+  plane(z0 + 1, pc0, pf0, pe0);
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    T pcp, pfp, pep;
+    plane(z0 + k + 2, pcp, pfp, pep);
+    const T y = c0 * pc0 + ce * (pe0 + pfm + pfp) + cc * (pem + pep);
+    const uint32_t li = mxy | (s16::sp4(z0 + k) << 2);
+    if (KIND == 2) {
+      out[li] = __ldg(rhs + base + li) - y;
+    } else {
+      out[li] = y;
+      acc += (double)pc0 * (double)y;
+    }
+    pcm = pc0; pfm = pf0; pem = pe0;
+    pc0 = pcp; pf0 = pfp; pe0 = pep;
+  }
+  (void)pcm;
+  __syncthreads();
+  for (int i = t; i < N; i += THREADS) q[base + i] = out[i];
+  if (KIND != 2) {
+    typedef cub::BlockReduce<double, THREADS> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double s = BR(tmp).Sum(acc);
+    if (t == 0) part[blk] = s;
+  }
+}
+template <typename T>
+constexpr size_t smem_bytes() {
+  return sizeof(T) * (TILE + N);
+}
+}  // namespace n16
+
+// ------------------------------------------------------------------ 16^3 residual + restriction
+// e on local [-2, 16] (tile coordinate = local + 2, width 19), r on local [-1, 15].
+namespace r16 {
+constexpr int N = 4096, THREADS = 512;
+constexpr int WE = 19, RSE = 19, PSE = 362;  // 8 planes = 2896 = 16 (mod 32): halves on disjoint banks
+constexpr int WR = 17;
+constexpr int ETILE = WE * PSE, RTILE = WR * WR * WR;
+__device__ __forceinline__ int eidx(int ux, int uy, int uz) { return uz * PSE + uy * RSE + ux; }
+__device__ __forceinline__ int ridx(int rx, int ry, int rz) { return (rz * WR + ry) * WR + rx; }
+
+template <typename T, bool FACES>
+__global__ void __launch_bounds__(THREADS) k_resid16(uint32_t D, const T* __restrict__ e, const T* __restrict__ f,
+                                                    T* __restrict__ fc, T c0, T ce, T cc,
+                                                    const T* __restrict__ table) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* et = reinterpret_cast<T*>(smem_raw);  // ETILE
+  T* rt = et + ETILE;                      // RTILE
+  __shared__ uint32_t nb[27];
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * N;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int ox = (int)bx * 16, oy = (int)by * 16, oz = (int)bz * 16;
+  const int t = threadIdx.x;
+  s16::neighbour_bases(nb, bx, by, bz, res >> 4);
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int qd = t + 512 * r;
+    int lx, ly, lz;
+    s16::quad_coords(qd, lx, ly, lz);
+    const typename s16::Vec4<T>::type ev = s16::ld4(e + base + 4 * qd);
+    const typename s16::Vec4<T>::type fv = s16::ld4(f + base + 4 * qd);
+    et[eidx(lx + 2, ly + 2, lz + 2)] = ev.x;
+    et[eidx(lx + 3, ly + 2, lz + 2)] = ev.y;
+    et[eidx(lx + 2, ly + 3, lz + 2)] = ev.z;
+    et[eidx(lx + 3, ly + 3, lz + 2)] = ev.w;
+    rt[ridx(lx + 1, ly + 1, lz + 1)] = fv.x;
+    rt[ridx(lx + 2, ly + 1, lz + 1)] = fv.y;
+    rt[ridx(lx + 1, ly + 2, lz + 1)] = fv.z;
+    rt[ridx(lx + 2, ly + 2, lz + 1)] = fv.w;
+  }
+  __syncthreads();
+  // one-node shell (local -1 and 16) through the structured loader; tile coordinate = u + 1
+  if (t < 256)
+    s16::load_halo<T>(et, e, nb, [](int ux, int uy, int uz) { return eidx(ux + 1, uy + 1, uz + 1); },
+                      [&](uint32_t m) { return __ldg(e + m); });
+  // second low layer (local -2 on some axis, all coordinates in [-2, 16])
+  for (int i = t; i < WE * WE * WE - 18 * 18 * 18; i += THREADS) {
+    int lx, ly, lz;
+    constexpr int S1 = WE * WE, S2 = 18 * WE;
+    if (i < S1) { lx = -2; ly = i % WE - 2; lz = i / WE - 2; }
+    else if (i < S1 + S2) { const int u = i - S1; lx = u % 18 - 1; ly = -2; lz = u / 18 - 2; }
+    else { const int u = i - S1 - S2; lx = u % 18 - 1; ly = u / 18 - 1; lz = -2; }
+    const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+    T v = 0;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) v = __ldg(e + morton3(gx, gy, gz));
+    et[eidx(lx + 2, ly + 2, lz + 2)] = v;
+  }
+  __syncthreads();
+  // interior r: columns (x, y), two z-halves of 8
+  {
+    const int lx = t & 15, half = (t >> 4) & 1, ly = t >> 5;  // lanes: 16 x-columns x 2 z-halves
+    auto plane = [&](int uz, T& pc, T& pf, T& pe) {
+      const int b0 = eidx(lx + 2, ly + 2, uz);
+      pc = et[b0];
+      pf = et[b0 - 1] + et[b0 + 1] + et[b0 - RSE] + et[b0 + RSE];
+      pe = et[b0 - 1 - RSE] + et[b0 + 1 - RSE] + et[b0 - 1 + RSE] + et[b0 + 1 + RSE];
+    };
+    T pcm, pfm, pem, pc0, pf0, pe0;
+    const int z0 = 8 * half;
+    plane(z0 + 1, pcm, pfm, pem);
+    plane(z0 + 2, pc0, pf0, pe0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      T pcp, pfp, pep;
+      plane(z0 + k + 3, pcp, pfp, pep);
+      const T y = c0 * pc0 + ce * (pe0 + pfm + pfp) + cc * (pem + pep);
+      rt[ridx(lx + 1, ly + 1, z0 + k + 1)] -= y;
+      pcm = pc0; pfm = pf0; pem = pe0;
+      pc0 = pcp; pf0 = pfp; pe0 = pep;
+    }
+    (void)pcm;
+  }
+  // low shell of r (local -1 on some axis)
+  {
+    constexpr int S1 = WR * WR, S2 = 16 * WR, S3 = 16 * 16;
+    for (int i = t; i < S1 + S2 + S3; i += THREADS) {
+      int lx, ly, lz;
+      if (i < S1) { lx = -1; ly = i % WR - 1; lz = i / WR - 1; }
+      else if (i < S1 + S2) { const int u = i - S1; lx = u % 16; ly = -1; lz = u / 16 - 1; }
+      else { const int u = i - S1 - S2; lx = u % 16; ly = u / 16; lz = -1; }
+      const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+      T r = 0;
+      if (gx >= 0 && gy >= 0 && gz >= 0) {
+        const int ei = eidx(lx + 2, ly + 2, lz + 2);
+        const int mask = FACES ? ((gx == 0) | ((gy == 0) << 1) | ((gz == 0) << 2)) : 0;
+        T y = 0;
+        if (mask) {
+          const T* cm = table + 27 * mask;
+#pragma unroll
+          for (int o = 0; o < 27; ++o)
+            y += cm[o] * et[ei + (o % 3 - 1) + RSE * ((o / 3) % 3 - 1) + PSE * (o / 9 - 1)];
+        } else {
+          T se = 0, sc = 0;
+#pragma unroll
+          for (int o = 0; o < 27; ++o) {
+            const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+            const int nzc = (dx != 0) + (dy != 0) + (dz != 0);
+            const T v = et[ei + dx + RSE * dy + PSE * dz];
+            if (nzc == 2) se += v;
+            else if (nzc == 3) sc += v;
+          }
+          y = c0 * et[ei] + ce * se + cc * sc;
+        }
+        r = __ldg(f + morton3(gx, gy, gz)) - y;
+      }
+      rt[ridx(lx + 1, ly + 1, lz + 1)] = r;
+    }
+  }
+  __syncthreads();
+  if (FACES && (ox == 0 || oy == 0 || oz == 0)) {
+    // interior nodes on a low domain face: replace the interior row by the face row
+    for (int i = t; i < N; i += THREADS) {
+      uint32_t lx, ly, lz;
+      unmorton3((uint32_t)i, lx, ly, lz);
+      const int mask = ((ox + (int)lx) == 0) | (((oy + (int)ly) == 0) << 1) | (((oz + (int)lz) == 0) << 2);
+      if (!mask) continue;
+      const int ei = eidx(lx + 2, ly + 2, lz + 2);
+      T yi = 0, yf = 0, se = 0, sc = 0;
+      const T* cm = table + 27 * mask;
+#pragma unroll
+      for (int o = 0; o < 27; ++o) {
+        const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+        const int nzc = (dx != 0) + (dy != 0) + (dz != 0);
+        const T v = et[ei + dx + RSE * dy + PSE * dz];
+        yf += cm[o] * v;
+        if (nzc == 2) se += v;
+        else if (nzc == 3) sc += v;
+      }
+      yi = c0 * et[ei] + ce * se + cc * sc;
+      rt[ridx(lx + 1, ly + 1, lz + 1)] += yi - yf;
+    }
+    __syncthreads();
+  }
+  // restriction to the 8^3 coarse nodes of the block (Morton-local order)
+  const uint64_t cbase = (uint64_t)blk * 512;
+  {
+    uint32_t cx, cy, cz;
+    unmorton3((uint32_t)t, cx, cy, cz);
+    const int fx = 2 * cx + 1, fy = 2 * cy + 1, fz = 2 * cz + 1;
+    T s = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy) {
+        const T wyz = (T)((dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
+        const int rb = ridx(fx, fy + dy, fz + dz);
+        s += wyz * ((T)0.5 * (rt[rb - 1] + rt[rb + 1]) + rt[rb]);
+      }
+    fc[cbase + t] = s;
+  }
+}
+template <typename T>
+constexpr size_t smem_bytes() {
+  return sizeof(T) * (ETILE + RTILE);
+}
+}  // namespace r16
+
+template <typename T>
+DevCoef<T> dev_coef(const LevelCoef& L, const T* table) {
+  DevCoef<T> k;
+  k.c0 = (T)L.c0;
+  k.ce = (T)L.ce;
+  k.cc = (T)L.cc;
+  k.table = table;
+  k.has_faces = L.has_faces ? 1 : 0;
+  return k;
+}
+
+inline int tile_for(uint32_t D) { return D >= 4 ? 16 : 8; }
+
+// dynamic shared memory beyond 48 KB needs a per-kernel opt-in (set once per kernel)
+template <typename K>
+void allow_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::set<const void*> done;
+  std::lock_guard<std::mutex> g(mu);
+  const void* key = reinterpret_cast<const void*>(kernel);
+  if (done.count(key)) return;
+  PR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done.insert(key);
+}
+
+template <typename T, int TB, int MODE, bool DOT, bool FWD>
+void launch_smooth(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const DevCoef<T>& k,
+                   double* part) {
+  using G = Geo<TB>;
+  constexpr int CW = TB / 2 + 2;
+  const size_t sm = sizeof(T) * (G::W * G::W * G::W + G::N + (MODE == 2 ? CW * CW * CW : 0));
+  const unsigned nb = 1u << (3 * (D - (TB == 16 ? 4 : 3)));
+  allow_smem(k_smooth<T, TB, MODE, DOT, FWD>, sm);
+  k_smooth<T, TB, MODE, DOT, FWD><<<nb, G::THREADS, sm, s>>>(D, xi, xo, f, ec, k, part);
+}
+
+template <typename T, int TB>
+void smooth_dispatch(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const DevCoef<T>& k,
+                     int mode, bool forward, double* part) {
+#define PR_SM(M, DT, FW) launch_smooth<T, TB, M, DT, FW>(s, D, xi, xo, f, ec, k, part)
+  if (mode == 1) {
+    if (forward) PR_SM(1, false, true);
+    else PR_SM(1, false, false);
+  } else if (mode == 2) {
+    if (part) {
+      if (forward) PR_SM(2, true, true);
+      else PR_SM(2, true, false);
+    } else {
+      if (forward) PR_SM(2, false, true);
+      else PR_SM(2, false, false);
+    }
+  } else {
+    if (part) {
+      if (forward) PR_SM(0, true, true);
+      else PR_SM(0, true, false);
+    } else {
+      if (forward) PR_SM(0, false, true);
+      else PR_SM(0, false, false);
+    }
+  }
+#undef PR_SM
+}
+
+template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
+void launch_s16(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const LevelCoef& L,
+                const T* table, double* part) {
+  const size_t sm = s16::smem_bytes<T>(MODE);
+  allow_smem(s16::k_smooth16<T, MODE, DOT, FWD, FACES>, sm);
+  s16::k_smooth16<T, MODE, DOT, FWD, FACES><<<1u << (3 * (D - 4)), s16::THREADS, sm, s>>>(
+      D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part);
+}
+
+template <typename T, int MODE, bool DOT, bool FWD>
+void launch_s16f(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const LevelCoef& L,
+                 const T* table, double* part) {
+  if (L.has_faces) launch_s16<T, MODE, DOT, FWD, true>(s, D, xi, xo, f, ec, L, table, part);
+  else launch_s16<T, MODE, DOT, FWD, false>(s, D, xi, xo, f, ec, L, table, part);
+}
+
+template <typename T>
+void smooth16_dispatch(cudaStream_t s, const LevelCoef& L, uint32_t D, const T* xi, T* xo, const T* f, const T* ec,
+                       const T* table, int mode, bool forward, double* part) {
+#define PR_S16(M, DT, FW) launch_s16f<T, M, DT, FW>(s, D, xi, xo, f, ec, L, table, part)
+  if (mode == 1) {
+    if (forward) PR_S16(1, false, true);
+    else PR_S16(1, false, false);
+  } else if (mode == 2) {
+    if (part) {
+      if (forward) PR_S16(2, true, true);
+      else PR_S16(2, true, false);
+    } else {
+      if (forward) PR_S16(2, false, true);
+      else PR_S16(2, false, false);
+    }
+  } else {
+    if (part) {
+      if (forward) PR_S16(0, true, true);
+      else PR_S16(0, true, false);
+    } else {
+      if (forward) PR_S16(0, false, true);
+      else PR_S16(0, false, false);
+    }
+  }
+#undef PR_S16
+}
+
+}  // namespace
+
+// ====================================================================== host side
+LevelCoef level_coef(uint32_t D, uint32_t l, double shift_l) {
+  // 1-D Galerkin recurrence (p^T m p for the linear prolongation p), from the fine level:
+  //   interior diagonal m0 -> 1.5 m0 + 2 m1, off-diagonal m1 -> m1 + m0/4,
+  //   node-0 diagonal  mb -> mb + m1 + m0/4  (the fine node -1 does not exist)
+  double m0 = 2.0 / 3.0, m1 = 1.0 / 6.0, mb = 2.0 / 3.0;
+  double s0 = 2.0, s1 = -1.0, sb = 2.0;
+  for (uint32_t k = D; k > l; --k) {
+    const double nm0 = 1.5 * m0 + 2.0 * m1, nm1 = m1 + 0.25 * m0, nmb = mb + m1 + 0.25 * m0;
+    const double ns0 = 1.5 * s0 + 2.0 * s1, ns1 = s1 + 0.25 * s0, nsb = sb + s1 + 0.25 * s0;
+    m0 = nm0;
+    m1 = nm1;
+    mb = nmb;
+    s0 = ns0;
+    s1 = ns1;
+    sb = nsb;
+  }
+  const double H = 1.0 / (double)(1u << D);
+  LevelCoef L;
+  L.depth = l;
+  L.shift = shift_l;
+  auto M = [&](int d, bool b) { return d == 0 ? (b ? mb : m0) : m1; };
+  auto S = [&](int d, bool b) { return d == 0 ? (b ? sb : s0) : s1; };
+  for (int mask = 0; mask < 8; ++mask)
+    for (int o = 0; o < 27; ++o) {
+      const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+      const bool bxm = mask & 1, bym = mask & 2, bzm = mask & 4;
+      double v = H * (S(dx, bxm) * M(dy, bym) * M(dz, bzm) + M(dx, bxm) * S(dy, bym) * M(dz, bzm) +
+                      M(dx, bxm) * M(dy, bym) * S(dz, bzm));
+      if (o == 13) v += shift_l;
+      L.table[mask][o] = v;
+    }
+  // interior values by offset class, o = (dx+1) + 3(dy+1) + 9(dz+1)
+  L.c0 = L.table[0][13];
+  L.ce = L.table[0][2 + 3 * 2 + 9 * 1];  // (1,1,0)
+  L.cc = L.table[0][2 + 3 * 2 + 9 * 2];  // (1,1,1)
+  L.cf = L.table[0][2 + 3 * 1 + 9 * 1];  // (1,0,0): 0 in exact arithmetic
+  if (std::fabs(L.cf) > 1e-12 * std::fabs(L.c0))
+    throw Error(PR_ERR_INTERNAL, "multigrid level has a non-zero interior face coupling");
+  L.cf = 0.0;
+  for (int mask = 0; mask < 8; ++mask)
+    for (int o = 0; o < 27; ++o)
+      if (std::fabs(L.table[mask][o]) <= 1e-12 * std::fabs(L.c0)) L.table[mask][o] = 0.0;
+  L.has_faces = (l < D);
+  return L;
+}
+
+template <typename T>
+void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, T* xo, const T* f, const T* ec,
+               int mode, bool forward, double* part) {
+  const uint32_t D = L.depth;
+  const DevCoef<T> k = dev_coef<T>(L, table);
+  if (tile_for(D) == 16) smooth16_dispatch<T>(s, L, D, xi, xo, f, ec, table, mode, forward, part);
+  else smooth_dispatch<T, 8>(s, D, xi, xo, f, ec, k, mode, forward, part);
+  PR_CHECK_LAUNCH();
+}
+
+template <typename T>
+void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc) {
+  const uint32_t D = L.depth;
+  const DevCoef<T> k = dev_coef<T>(L, table);
+  if (tile_for(D) == 16) {
+    const size_t sm = r16::smem_bytes<T>();
+    if (L.has_faces) {
+      allow_smem(r16::k_resid16<T, true>, sm);
+      r16::k_resid16<T, true><<<1u << (3 * (D - 4)), r16::THREADS, sm, s>>>(D, e, f, fc, (T)L.c0, (T)L.ce,
+                                                                            (T)L.cc, table);
+    } else {
+      allow_smem(r16::k_resid16<T, false>, sm);
+      r16::k_resid16<T, false><<<1u << (3 * (D - 4)), r16::THREADS, sm, s>>>(D, e, f, fc, (T)L.c0, (T)L.ce,
+                                                                             (T)L.cc, table);
+    }
+  } else {
+    const size_t sm = sizeof(T) * (11 * 11 * 11 + 9 * 9 * 9);
+    allow_smem(k_resid_restrict<T, 8>, sm);
+    k_resid_restrict<T, 8><<<1u << (3 * (D - 3)), Geo<8>::THREADS, sm, s>>>(D, e, f, fc, k);
+  }
+  PR_CHECK_LAUNCH();
+}
+
+template <typename T>
+void mg_spmv(cudaStream_t s, const LevelCoef& L, const T* table, const T* z, const T* d, T* dn, double beta,
+             bool xpby, T* q, double* part) {
+  const uint32_t D = L.depth;
+  const DevCoef<T> k = dev_coef<T>(L, table);
+  if (L.has_faces) throw Error(PR_ERR_INTERNAL, "mg_spmv is for the finest level");
+  if (tile_for(D) == 16) {
+    const unsigned nb = 1u << (3 * (D - 4));
+    const size_t sm = n16::smem_bytes<T>();
+    if (xpby) {
+      allow_smem(n16::k_spmv16<T, 1, T>, sm);
+      n16::k_spmv16<T, 1, T><<<nb, n16::THREADS, sm, s>>>(D, d, z, dn, (T)beta, q, (T)L.c0, (T)L.ce, (T)L.cc,
+                                                          nullptr, part);
+    } else {
+      allow_smem(n16::k_spmv16<T, 0, T>, sm);
+      n16::k_spmv16<T, 0, T><<<nb, n16::THREADS, sm, s>>>(D, d, nullptr, nullptr, (T)0, q, (T)L.c0, (T)L.ce,
+                                                          (T)L.cc, nullptr, part);
+    }
+  } else {
+    const unsigned nb = 1u << (3 * (D - 3));
+    const size_t sm = sizeof(T) * (10 * 10 * 10 + 512);
+    if (xpby) k_spmv<T, 8, true><<<nb, Geo<8>::THREADS, sm, s>>>(D, z, d, dn, (T)beta, q, k, part);
+    else k_spmv<T, 8, false><<<nb, Geo<8>::THREADS, sm, s>>>(D, z, d, dn, (T)beta, q, k, part);
+  }
+  PR_CHECK_LAUNCH();
+}
+
+template <typename E>
+void mg_resid_update(cudaStream_t s, const LevelCoef& L, const double* x, const E* e, double scale, double* xn,
+                     const double* b, double* r) {
+  const uint32_t D = L.depth;
+  if (D < 4 || L.has_faces) throw Error(PR_ERR_INTERNAL, "mg_resid_update needs the finest level, depth >= 4");
+  const size_t sm = n16::smem_bytes<double>();
+  allow_smem(n16::k_spmv16<double, 2, E>, sm);
+  n16::k_spmv16<double, 2, E><<<1u << (3 * (D - 4)), n16::THREADS, sm, s>>>(D, x, e, xn, scale, r, L.c0, L.ce, L.cc,
+                                                                            b, nullptr);
+  PR_CHECK_LAUNCH();
+}
+template void mg_resid_update<float>(cudaStream_t, const LevelCoef&, const double*, const float*, double, double*,
+                                     const double*, double*);
+template void mg_resid_update<double>(cudaStream_t, const LevelCoef&, const double*, const double*, double, double*,
+                                      const double*, double*);
+
+uint32_t mg_blocks(uint32_t D) { return tile_for(D) == 16 ? (1u << (3 * (D - 4))) : (1u << (3 * (D - 3))); }
+
+template <typename T>
+void screen_project_sq(cudaStream_t s, const Screen<T>& scr, const T* x, double* part, int nparts) {
+  k_screen_project_sq<T><<<nparts, 256, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, x, scr.proj, part);
+  PR_CHECK_LAUNCH();
+}
+
+void sum_parts(cudaStream_t s, const double* part, int np, double scale2, const double* part2, int np2, double* out) {
+  k_sum_parts<<<1, 1024, 0, s>>>(part, np, scale2, part2, np2, out);
+  PR_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------------ kernel micro-benchmark
+namespace {
+template <typename T>
+__global__ void k_fill(T* __restrict__ x, uint64_t n, uint32_t seed) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t h = (uint32_t)i * 2654435761u ^ seed;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    x[i] = (T)((double)(h & 0xffffff) / 16777216.0 - 0.5);
+  }
+}
+
+template <typename T>
+double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
+  cudaStream_t s = c->stream;
+  const uint64_t n = 1ull << (3 * D), nc = n / 8;
+  const std::string tn = std::is_same<T, double>::value ? "f64" : "f32";
+  T* x = c->buf<T>("kb_x_" + tn, n);
+  T* y = c->buf<T>("kb_y_" + tn, n);
+  T* f = c->buf<T>("kb_f_" + tn, n);
+  T* w = c->buf<T>("kb_w_" + tn, n);
+  T* ec = c->buf<T>("kb_c_" + tn, nc);
+  double* part = c->buf<double>("kb_part", std::max<uint32_t>(mg_blocks(D), kDotBlocks));
+  const unsigned g = 148 * 16;
+  k_fill<T><<<g, 256, 0, s>>>(x, n, 1u);
+  k_fill<T><<<g, 256, 0, s>>>(f, n, 2u);
+  k_fill<T><<<g, 256, 0, s>>>(w, n, 3u);
+  k_fill<T><<<g, 256, 0, s>>>(ec, nc, 4u);
+  PR_CHECK_LAUNCH();
+  const LevelCoef Lf = level_coef(D, D, 0.0), Lc = level_coef(D + 1, D, 0.0);  // fine level, a coarse level
+  std::vector<T> tab(216);
+  for (int m = 0; m < 8; ++m)
+    for (int o = 0; o < 27; ++o) tab[27 * m + o] = (T)Lc.table[m][o];
+  T* table = c->buf<T>("kb_tab_" + tn, 216);
+  PR_CUDA(cudaMemcpyAsync(table, tab.data(), 216 * sizeof(T), cudaMemcpyHostToDevice, s));
+  const double es = sizeof(T);
+  auto run = [&]() {
+    switch (kid) {
+      case 0: mg_spmv<T>(s, Lf, table, nullptr, x, nullptr, 0.0, false, y, part); break;
+      case 1: mg_spmv<T>(s, Lf, table, f, x, w, 0.5, true, y, part); break;
+      case 2: mg_smooth<T>(s, Lc, table, nullptr, y, f, nullptr, 1, true, nullptr); break;
+      case 3: mg_smooth<T>(s, Lc, table, x, y, f, nullptr, 0, true, nullptr); break;
+      case 4: mg_smooth<T>(s, Lc, table, x, y, f, ec, 2, false, part); break;
+      case 5: mg_resid_restrict<T>(s, Lc, table, x, f, ec); break;
+      case 6: stencil_apply<T>(s, D, x, nullptr, y, cast_coef<T>(stencil_coef(D, 0.0)), 0); break;
+      default: throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
+    }
+  };
+  const double nb = (double)n * es;
+  const double algo[] = {2 * nb, 4 * nb, 2 * nb, 3 * nb, 3 * nb + nb / 8, 2 * nb + nb / 8, 2 * nb};
+  *bytes = algo[kid];
+  run();
+  PR_CUDA(cudaStreamSynchronize(s));
+  cudaEvent_t e0, e1;
+  PR_CUDA(cudaEventCreate(&e0));
+  PR_CUDA(cudaEventCreate(&e1));
+  PR_CUDA(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) run();
+  PR_CUDA(cudaEventRecord(e1, s));
+  PR_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  PR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return (double)ms / reps;
+}
+}  // namespace
+
+double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps, double* bytes) {
+  if (D < 4 || D > kMaxDepth) throw Error(PR_ERR_INVALID_ARGUMENT, "kernel bench depth must be in [4, 10]");
+  if (reps < 1) reps = 1;
+  return precision == PR_PRECISION_FP64 ? bench_one<double>(c, kid, D, reps, bytes)
+                                        : bench_one<float>(c, kid, D, reps, bytes);
+}
+
+#define PR_INST(T)                                                                                                 \
+  template void mg_smooth<T>(cudaStream_t, const LevelCoef&, const T*, const T*, T*, const T*, const T*, int, bool, \
+                             double*);                                                                            \
+  template void mg_resid_restrict<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*);           \
+  template void mg_spmv<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, double, bool, T*,    \
+                           double*);                                                                              \
+  template void screen_project_sq<T>(cudaStream_t, const Screen<T>&, const T*, double*, int);
+PR_INST(float)
+PR_INST(double)
+#undef PR_INST
+
+}  // namespace pr

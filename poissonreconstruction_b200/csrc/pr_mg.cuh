@@ -1,0 +1,54 @@
+// Brick-tiled multigrid / CG kernels (pr_mg.cu).
+#pragma once
+
+#include <cmath>
+
+#include "pr_ops.cuh"
+
+namespace pr {
+
+// Galerkin operator of one multigrid level: interior constants and the 8 x 27 table of
+// low-face coefficients (mask bit a set = node index 0 on axis a), FP64 on the host.
+struct LevelCoef {
+  uint32_t depth = 0;
+  double shift = 0.0;
+  double c0 = 0, ce = 0, cc = 0, cf = 0;
+  double table[8][27];
+  bool has_faces = false;
+};
+
+// Level l of a hierarchy whose finest depth is D; shift_l is added to the diagonal.
+LevelCoef level_coef(uint32_t D, uint32_t l, double shift_l);
+
+// One smoothing sweep over all blocks of the level, out of place.  mode 0: xo = sweep(xi);
+// 1: xo = sweep(0) (xi unused); 2: xo = sweep(xi + P ec).  part (nullable): per-block f.xo
+// (mg_blocks entries).
+template <typename T>
+void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, T* xo, const T* f, const T* ec,
+               int mode, bool forward, double* part);
+// fc = P^T (f - A_l e)
+template <typename T>
+void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc);
+// finest level only.  xpby: dn = z + beta d, q = A dn; else q = A d.  Stencil part only;
+// per-block (dn or d).q into part.
+template <typename T>
+void mg_spmv(cudaStream_t s, const LevelCoef& L, const T* table, const T* z, const T* d, T* dn, double beta,
+             bool xpby, T* q, double* part);
+uint32_t mg_blocks(uint32_t depth);
+// finest level (depth >= 4), FP64: xn = x + scale * e (e: correction, float or double),
+// r = b - K xn (stencil part; the screening is applied separately).  x, xn: distinct buffers.
+template <typename E>
+void mg_resid_update(cudaStream_t s, const LevelCoef& L, const double* x, const E* e, double scale, double* xn,
+                     const double* b, double* r);
+// screening projection with per-block sums of squares (nparts blocks of 256 threads)
+template <typename T>
+void screen_project_sq(cudaStream_t s, const Screen<T>& scr, const T* x, double* part, int nparts);
+// out = sum(part[0:np]) + scale2 * sum(part2[0:np2]), fixed order
+void sum_parts(cudaStream_t s, const double* part, int np, double scale2, const double* part2, int np2, double* out);
+
+// Time `reps` launches of one kernel (ids: 0 spmv, 1 spmv+xpby, 2 smooth from zero,
+// 3 smooth, 4 smooth+prolongation+dot, 5 residual+restriction, 6 per-node stencil) at
+// depth D on context-owned buffers; returns ms per launch and the algorithmic bytes.
+double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps, double* bytes);
+
+}  // namespace pr

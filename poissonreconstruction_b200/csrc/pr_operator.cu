@@ -313,6 +313,14 @@ void screen_project(cudaStream_t s, const Screen<T>& scr, const T* x) {
 }
 
 template <typename T>
+void screen_gather(cudaStream_t s, const Screen<T>& scr, T* y, int sign) {
+  if (!scr.active()) return;
+  k_screen_gather<T><<<grid_for(scr.S), kThreads, 0, s>>>(scr.snode, scr.soff, scr.S, scr.sval, scr.phi, scr.proj,
+                                                          (T)sign * scr.wh3, y);
+  PR_CHECK_LAUNCH();
+}
+
+template <typename T>
 double dot(pr_context* c, const T* a, const T* b, uint64_t n) {
   double* part = c->buf<double>("dot_part", kDotBlocks);
   double* out = c->buf<double>("dot_out", 1);
@@ -397,6 +405,7 @@ void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e) {
   template void stencil_apply<T>(cudaStream_t, uint32_t, const T*, const T*, T*, Coef<T>, int);       \
   template void screen_apply<T>(cudaStream_t, const Screen<T>&, const T*, T*, int);                   \
   template void screen_project<T>(cudaStream_t, const Screen<T>&, const T*);                          \
+  template void screen_gather<T>(cudaStream_t, const Screen<T>&, T*, int);                            \
   template double dot<T>(pr_context*, const T*, const T*, uint64_t);                                  \
   template double cg_update<T>(pr_context*, uint64_t, double, const T*, const T*, T*, T*);            \
   template void xpby<T>(cudaStream_t, uint64_t, const T*, double, T*);                                \

@@ -46,6 +46,9 @@ void screen_apply(cudaStream_t s, const Screen<T>& scr, const T* x, T* y, int si
 // scr.proj[p] = phi(p) . x
 template <typename T>
 void screen_project(cudaStream_t s, const Screen<T>& scr, const T* x);
+// y += sign * wh3 * Phi proj  (proj from a previous projection)
+template <typename T>
+void screen_gather(cudaStream_t s, const Screen<T>& scr, T* y, int sign);
 
 // dot products (deterministic, accumulated in FP64); result returned on the host
 template <typename T>

@@ -9,17 +9,17 @@
 //   * mixed: preconditioned CG in FP32 (operator, vectors and V-cycle in FP32) inside an
 //     FP64 iterative-refinement loop: r = b - A x is formed in FP64, scaled to unit norm,
 //     solved approximately in FP32, and the correction is added to the FP64 x.
-// The V-cycle works on the constant-coefficient stencil A' = K + wg I of every depth
-// (rediscretised: the Galerkin coarse stiffness of nested trilinear spaces), relaxed with
-// multicolour block Gauss-Seidel (forward before, backward after the coarse correction, so
-// the preconditioner is symmetric), coarsest level 4^3 solved with a dense inverse.  The
-// per-point screening terms are in A but not in A' (they are below 1e-5 of the stiffness
-// diagonal at depth >= 8 and only slow convergence, never prevent it).
+// The V-cycle works on A' = K + wg I and its exact Galerkin coarse operators (P^T A' P for
+// the linear B-spline prolongation P), relaxed with multicolour Gauss-Seidel inside
+// 8^3 / 16^3 blocks (forward before, backward after the coarse correction, so the
+// preconditioner is symmetric); the coarsest level, 4^3, is solved with a dense inverse.
+// The per-point screening terms are in A but not in A' (below 1e-5 of the stiffness
+// diagonal at depth >= 8; they only slow convergence, never prevent it).
 #include <cmath>
 #include <cstdio>
 #include <vector>
 
-#include "pr_ops.cuh"
+#include "pr_mg.cuh"
 
 namespace pr {
 
@@ -27,25 +27,23 @@ namespace {
 
 constexpr uint32_t kCoarseDepth = 2;
 
-// Dense inverse of the constant stencil at depth Dc (Morton order), FP64 Cholesky.
-std::vector<double> dense_inverse(uint32_t Dc, const Coef<double>& c) {
+// Dense inverse of a level's Galerkin operator (depth Dc <= 2, Morton order), FP64 Cholesky.
+std::vector<double> dense_inverse(const LevelCoef& L) {
+  const uint32_t Dc = L.depth;
   const int res = 1 << Dc;
   const int n = res * res * res;
   std::vector<double> A((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i) {
     uint32_t ix, iy, iz;
     unmorton3((uint32_t)i, ix, iy, iz);
-    for (int dz = -1; dz <= 1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          int jx = (int)ix + dx, jy = (int)iy + dy, jz = (int)iz + dz;
-          if (jx < 0 || jx >= res || jy < 0 || jy >= res || jz < 0 || jz >= res) continue;
-          int nz = (dx != 0) + (dy != 0) + (dz != 0);
-          double v = nz == 0 ? c.c0 : (nz == 2 ? c.ce : (nz == 3 ? c.cc : 0.0));
-          A[(size_t)i * n + morton3(jx, jy, jz)] = v;
-        }
+    int mask = L.has_faces ? ((ix == 0) | ((iy == 0) << 1) | ((iz == 0) << 2)) : 0;
+    for (int o = 0; o < 27; ++o) {
+      int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
+      int jx = (int)ix + dx, jy = (int)iy + dy, jz = (int)iz + dz;
+      if (jx < 0 || jx >= res || jy < 0 || jy >= res || jz < 0 || jz >= res) continue;
+      A[(size_t)i * n + morton3(jx, jy, jz)] = L.table[mask][o];
+    }
   }
-  // Cholesky A = L L^T (lower, in place)
   for (int j = 0; j < n; ++j) {
     double d = A[(size_t)j * n + j];
     for (int k = 0; k < j; ++k) d -= A[(size_t)j * n + k] * A[(size_t)j * n + k];
@@ -58,7 +56,6 @@ std::vector<double> dense_inverse(uint32_t Dc, const Coef<double>& c) {
       A[(size_t)i * n + j] = s / d;
     }
   }
-  // inverse column by column: solve L L^T x = e_c
   std::vector<double> inv((size_t)n * n), y(n);
   for (int col = 0; col < n; ++col) {
     for (int i = 0; i < n; ++i) {
@@ -75,14 +72,17 @@ std::vector<double> dense_inverse(uint32_t Dc, const Coef<double>& c) {
   return inv;
 }
 
-// Multigrid V-cycle preconditioner on A' (constant stencil per depth)
+// Multigrid V-cycle preconditioner on A' = K + wg I with Galerkin coarse levels.
+// Level l holds f_l (right-hand side), a_l (after pre-smoothing) and e_l (result);
+// sweeps beyond the first ping-pong through t_l.
 template <typename T>
 struct Multigrid {
   pr_context* c = nullptr;
   uint32_t D = 0, Dc = 0;
   int sweeps = 1;
-  std::vector<Coef<T>> coef;
-  std::vector<T*> f, e, r;
+  std::vector<LevelCoef> L;
+  std::vector<T*> f, a, e, t;
+  T* tables = nullptr;  // [D+1][8*27]
   T* inv = nullptr;
   uint32_t nc = 0;
 
@@ -91,45 +91,130 @@ struct Multigrid {
     D = depth;
     Dc = std::min<uint32_t>(D, kCoarseDepth);
     sweeps = std::max(1, nsweeps);
-    coef.assign(D + 1, Coef<T>{});
+    L.assign(D + 1, LevelCoef());
     f.assign(D + 1, nullptr);
+    a.assign(D + 1, nullptr);
     e.assign(D + 1, nullptr);
-    r.assign(D + 1, nullptr);
+    t.assign(D + 1, nullptr);
+    std::vector<T> tab((size_t)(D + 1) * 216, (T)0);
     for (uint32_t l = Dc; l <= D; ++l) {
-      double shift = wg * std::pow(8.0, (double)(D - l));
-      coef[l] = cast_coef<T>(stencil_coef(l, shift));
-      uint64_t nl = 1ull << (3 * l);
-      std::string sfx = std::string("_") + tname<T>() + "_" + std::to_string(l);
+      L[l] = level_coef(D, l, wg * std::pow(8.0, (double)(D - l)));
+      for (int m = 0; m < 8; ++m)
+        for (int o = 0; o < 27; ++o) tab[(size_t)l * 216 + 27 * m + o] = (T)L[l].table[m][o];
+      const uint64_t nl = 1ull << (3 * l);
+      const std::string sfx = std::string("_") + tname<T>() + "_" + std::to_string(l);
       if (l < D) {
         f[l] = c->buf<T>("mg_f" + sfx, nl);
         e[l] = c->buf<T>("mg_e" + sfx, nl);
       }
-      if (l > Dc) r[l] = c->buf<T>("mg_r" + sfx, nl);
+      if (l > Dc) {
+        a[l] = c->buf<T>("mg_a" + sfx, nl);
+        if (sweeps > 1) t[l] = c->buf<T>("mg_t" + sfx, nl);
+      }
     }
+    tables = c->buf<T>(std::string("mg_tab_") + tname<T>(), tab.size());
     nc = 1u << (3 * Dc);
-    std::vector<double> invd = dense_inverse(Dc, stencil_coef(Dc, wg * std::pow(8.0, (double)(D - Dc))));
+    std::vector<double> invd = dense_inverse(L[Dc]);
     std::vector<T> invt(invd.begin(), invd.end());
     inv = c->buf<T>(std::string("mg_inv_") + tname<T>(), invt.size());
+    PR_CUDA(cudaMemcpyAsync(tables, tab.data(), tab.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
     PR_CUDA(cudaMemcpyAsync(inv, invt.data(), invt.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
-    c->sync();  // invt is a host temporary
+    c->sync();  // host temporaries
   }
+  const T* table(uint32_t l) const { return tables + (size_t)l * 216; }
 
-  void vcycle(uint32_t l, const T* fl, T* el) {
+  // el = V(fl); at the finest level `part` (nullable) receives per-block fl.el partials.
+  void vcycle(uint32_t l, const T* fl, T* el, double* part) {
     cudaStream_t s = c->stream;
     if (l == Dc) {
       dense_solve<T>(s, nc, inv, fl, el);
       return;
     }
-    const uint64_t nl = 1ull << (3 * l);
-    PR_CUDA(cudaMemsetAsync(el, 0, nl * sizeof(T), s));
-    for (int k = 0; k < sweeps; ++k) gs_sweep<T>(s, l, el, fl, coef[l], true);
-    stencil_apply<T>(s, l, el, fl, r[l], coef[l], 1);
-    restrict_to_coarse<T>(s, l, r[l], f[l - 1]);
-    vcycle(l - 1, f[l - 1], e[l - 1]);
-    prolong_add<T>(s, l, e[l - 1], el);
-    for (int k = 0; k < sweeps; ++k) gs_sweep<T>(s, l, el, fl, coef[l], false);
+    // pre-smoothing (forward) from zero; result in a_l
+    T* cur = a[l];
+    mg_smooth<T>(s, L[l], table(l), nullptr, cur, fl, nullptr, 1, true, nullptr);
+    for (int k = 1; k < sweeps; ++k) {
+      T* nxt = (cur == a[l]) ? t[l] : a[l];
+      mg_smooth<T>(s, L[l], table(l), cur, nxt, fl, nullptr, 0, true, nullptr);
+      cur = nxt;
+    }
+    mg_resid_restrict<T>(s, L[l], table(l), cur, fl, f[l - 1]);
+    vcycle(l - 1, f[l - 1], e[l - 1], nullptr);
+    // post-smoothing (backward): first sweep on cur + P e_{l-1}; the last sweep writes el
+    for (int k = 0; k < sweeps; ++k) {
+      const bool last = (k == sweeps - 1);
+      T* nxt = last ? el : ((cur == a[l]) ? t[l] : a[l]);
+      mg_smooth<T>(s, L[l], table(l), cur, nxt, fl, e[l - 1], k == 0 ? 2 : 0, false, last ? part : nullptr);
+      cur = nxt;
+    }
   }
-  void apply(const T* rhs, T* z) { vcycle(D, rhs, z); }
+  // z = M r; returns r.z
+  double apply(const T* r, T* z) {
+    const uint64_t n = 1ull << (3 * D);
+    if (D == Dc) {
+      dense_solve<T>(c->stream, nc, inv, r, z);
+      return dot<T>(c, r, z, n);
+    }
+    double* part = c->buf<double>("mg_part", mg_blocks(D));
+    double* out = c->buf<double>("mg_out", 1);
+    vcycle(D, r, z, part);
+    sum_parts(c->stream, part, (int)mg_blocks(D), 0.0, part, 0, out);
+    PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    return c->h_scalars[0];
+  }
+};
+
+// Fine operator for CG: tiled stencil SpMV (optionally fused with dn = z + beta d) plus
+// the per-point screening terms; returns dn.A dn from the fused partial sums.
+template <typename T>
+struct CgOperator {
+  pr_context* c = nullptr;
+  LevelCoef Lf;
+  T* table = nullptr;
+  Screen<T> scr;
+  uint32_t D = 0;
+  void init(pr_context* ctx, double wg) {
+    c = ctx;
+    D = c->D;
+    Lf = level_coef(D, D, wg);
+    std::vector<T> tab(216);
+    for (int m = 0; m < 8; ++m)
+      for (int o = 0; o < 27; ++o) tab[27 * m + o] = (T)Lf.table[m][o];
+    table = c->buf<T>(std::string("cg_tab_") + tname<T>(), 216);
+    PR_CUDA(cudaMemcpyAsync(table, tab.data(), 216 * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    c->sync();
+    scr = make_fine_op<T>(c, wg).scr;
+  }
+  // xpby: dn = z + beta d, q = A dn; else q = A d (dn unused).  Returns (dn or d).q
+  double apply_dot(const T* z, const T* d, T* dn, double beta, bool xpby, T* q) {
+    cudaStream_t s = c->stream;
+    const uint64_t n = c->n;
+    const T* dd = xpby ? dn : d;
+    if (D < 3) {  // grids below one 8^3 block: per-node kernels
+      if (xpby) {
+        PR_CUDA(cudaMemcpyAsync(dn, d, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        pr::xpby<T>(s, n, z, beta, dn);
+      }
+      stencil_apply<T>(s, D, dd, nullptr, q, cast_coef<T>(stencil_coef(D, Lf.shift)), 0);
+      screen_apply<T>(s, scr, dd, q, +1);
+      return dot<T>(c, dd, q, n);
+    }
+    double* part = c->buf<double>("cg_part", mg_blocks(D));
+    double* part2 = c->buf<double>("cg_part2", kDotBlocks);
+    double* out = c->buf<double>("cg_out", 1);
+    mg_spmv<T>(s, Lf, table, z, d, dn, beta, xpby, q, part);
+    int np2 = 0;
+    if (scr.active()) {
+      screen_project_sq<T>(s, scr, dd, part2, kDotBlocks);
+      screen_gather<T>(s, scr, q, +1);
+      np2 = kDotBlocks;
+    }
+    sum_parts(s, part, (int)mg_blocks(D), (double)scr.wh3, part2, np2, out);
+    PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    return c->h_scalars[0];
+  }
 };
 
 struct PcgResult {
@@ -139,32 +224,41 @@ struct PcgResult {
 };
 
 // Preconditioned CG from x = 0 on A x = b, until ||r|| <= tol_abs or maxit iterations.
+// The search direction ping-pongs between two buffers (the SpMV reads d with halos).
 template <typename T>
-PcgResult pcg(pr_context* c, const FineOp<T>& A, Multigrid<T>& M, const T* b, T* x, double tol_abs, int maxit) {
+PcgResult pcg(pr_context* c, CgOperator<T>& A, Multigrid<T>& M, const T* b, T* x, double tol_abs, int maxit) {
   const uint64_t n = c->n;
   cudaStream_t s = c->stream;
-  std::string t = tname<T>();
-  T* r = c->buf<T>("cg_r_" + t, n);
-  T* z = c->buf<T>("cg_z_" + t, n);
-  T* d = c->buf<T>("cg_d_" + t, n);
-  T* q = c->buf<T>("cg_q_" + t, n);
+  const std::string tn = tname<T>();
+  T* r = c->buf<T>("cg_r_" + tn, n);
+  T* z = c->buf<T>("cg_z_" + tn, n);
+  T* dA = c->buf<T>("cg_d_" + tn, n);
+  T* dB = c->buf<T>("cg_d2_" + tn, n);
+  T* q = c->buf<T>("cg_q_" + tn, n);
   PcgResult res;
   PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
   PR_CUDA(cudaMemcpyAsync(r, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
   double rr = dot<T>(c, r, r, n);
   res.rr = rr;
   if (!(std::sqrt(rr) > tol_abs) || maxit <= 0) return res;
-  M.apply(r, z);
-  PR_CUDA(cudaMemcpyAsync(d, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
-  double rz = dot<T>(c, r, z, n);
+  double rz = M.apply(r, z);
+  double beta = 0.0;
+  T* d = nullptr;  // current search direction
   for (int it = 0; it < maxit; ++it) {
-    A.apply(s, d, q);
-    double dq = dot<T>(c, d, q, n);
+    double dq;
+    if (it == 0) {
+      dq = A.apply_dot(z, z, nullptr, 0.0, false, q);  // d = z
+      d = z;
+    } else {
+      T* dn = (d == dA) ? dB : dA;
+      dq = A.apply_dot(z, d, dn, beta, true, q);
+      d = dn;
+    }
     if (!(dq > 0.0) || !std::isfinite(dq) || !(rz > 0.0)) {
       res.broke = true;
       break;
     }
-    double alpha = rz / dq;
+    const double alpha = rz / dq;
     rr = cg_update<T>(c, n, alpha, d, q, x, r);
     res.iters = it + 1;
     res.rr = rr;
@@ -173,11 +267,13 @@ PcgResult pcg(pr_context* c, const FineOp<T>& A, Multigrid<T>& M, const T* b, T*
       break;
     }
     if (std::sqrt(rr) <= tol_abs) break;
-    M.apply(r, z);
-    double rz_new = dot<T>(c, r, z, n);
-    double beta = rz_new / rz;
+    if (d == z) {  // the first direction aliases z: keep it before z is overwritten
+      PR_CUDA(cudaMemcpyAsync(dA, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      d = dA;
+    }
+    const double rz_new = M.apply(r, z);
+    beta = rz_new / rz;
     rz = rz_new;
-    xpby<T>(s, n, z, beta, d);
   }
   return res;
 }
@@ -205,21 +301,24 @@ double vcycle_bytes(uint32_t D, double es, int sweeps) {
 
 void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
   const uint64_t n = c->n;
+  const uint32_t D = c->D;
   cudaStream_t s = c->stream;
-  const double h = 1.0 / (double)(1u << c->D);
+  const double h = 1.0 / (double)(1u << D);
   const double wg = c->pw > 0.0 ? (c->pw * (h * h * h) / 1.5) * 0.005 : 0.0;
   const double* b = c->get<double>("b64");
-  double* x = c->buf<double>("x64", n);
+  double* xA = c->buf<double>("x64", n);
+  double* xB = c->buf<double>("x64b", n);
   double* r = c->buf<double>("r64", n);
   const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;
   const int max_iters = p.max_iters > 0 ? (int)p.max_iters : 200;
   const int sweeps = p.smooth_sweeps > 0 ? (int)p.smooth_sweeps : 1;
+  const bool mixed = p.precision != PR_PRECISION_FP64;
 
   st.pcg_iterations = 0;
   st.refinement_steps = 0;
   st.solve_bytes = 0.0;
-  PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
-  double bn = std::sqrt(dot<double>(c, b, b, n));
+  PR_CUDA(cudaMemsetAsync(xA, 0, n * sizeof(double), s));
+  const double bn = std::sqrt(dot<double>(c, b, b, n));
   if (bn == 0.0) {
     st.rel_residual = 0.0;
     st.converged = 1;
@@ -227,31 +326,52 @@ void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
     return;
   }
   FineOp<double> A64 = make_fine_op<double>(c, wg);
-  PR_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  double rn = bn;
-  int used = 0;
-  const bool mixed = p.precision != PR_PRECISION_FP64;
+  const LevelCoef L64 = level_coef(D, D, wg);
+  const bool fused = D >= 4;  // tiled residual-update kernel
   const double es = mixed ? 4.0 : 8.0;
-  const double per_iter = iter_bytes(n, es, c->P_in, es) + vcycle_bytes(c->D, es, sweeps);
+  const double per_iter = iter_bytes(n, es, c->P_in, es) + vcycle_bytes(D, es, sweeps);
+  const double resid_bytes = 36.0 * n + c->P_in * 2.0 * (8.0 * 8.0 + 32.0) + 8.0 * n;  // update+residual, norm
 
+  // x <- x + scale * e and r = b - A x (FP64); returns ||r||.  x ping-pongs between xA and xB.
+  double* x = xA;
+  auto update_residual = [&](const void* e, bool e_is_float, double scale) -> double {
+    if (fused) {
+      double* xn = (x == xA) ? xB : xA;
+      if (e_is_float) mg_resid_update<float>(s, L64, x, (const float*)e, scale, xn, b, r);
+      else mg_resid_update<double>(s, L64, x, (const double*)e, scale, xn, b, r);
+      x = xn;
+      if (A64.scr.active()) {
+        screen_project<double>(s, A64.scr, x);
+        screen_gather<double>(s, A64.scr, r, -1);
+      }
+    } else {
+      if (e_is_float) axpy<float, double>(s, n, scale, (const float*)e, x);
+      else axpy<double, double>(s, n, scale, (const double*)e, x);
+      A64.residual(s, x, b, r);
+    }
+    return std::sqrt(dot<double>(c, r, r, n));
+  };
+
+  double rn = bn;
+  const double* rsrc = b;  // current residual (b while x = 0)
+  int used = 0;
   if (mixed) {
-    FineOp<float> A32 = make_fine_op<float>(c, wg);
+    CgOperator<float> A32;
+    A32.init(c, wg);
     Multigrid<float> M32;
-    M32.init(c, c->D, wg, sweeps);
+    M32.init(c, D, wg, sweeps);
     float* r32 = c->buf<float>("r32", n);
     float* e32 = c->buf<float>("e32", n);
     const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
     while (rn > target * bn && used < max_iters) {
-      scale_convert<double, float>(s, n, 1.0 / rn, r, r32);
-      double tol = std::max(inner, 0.5 * target * bn / rn);
-      PcgResult pr_ = pcg<float>(c, A32, M32, r32, e32, tol, max_iters - used);
+      scale_convert<double, float>(s, n, 1.0 / rn, rsrc, r32);
+      const double tol = std::max(inner, 0.5 * target * bn / rn);
+      const PcgResult pr_ = pcg<float>(c, A32, M32, r32, e32, tol, max_iters - used);
       used += pr_.iters;
-      axpy<float, double>(s, n, rn, e32, x);
-      A64.residual(s, x, b, r);
-      double rn_new = std::sqrt(dot<double>(c, r, r, n));
+      const double rn_new = update_residual(e32, true, rn);
+      rsrc = r;
       st.refinement_steps++;
-      st.solve_bytes += pr_.iters * per_iter + 2.0 * n * 4.0 + 2.0 * n * 8.0 /*convert, axpy*/ +
-                        (3.0 * n * 8.0 + c->P_in * 2.0 * (8.0 * 8.0 + 32.0)) /*FP64 residual*/ + 2.0 * n * 8.0;
+      st.solve_bytes += pr_.iters * per_iter + 12.0 * n + resid_bytes;
       if (pr_.iters == 0 || !(rn_new < rn)) {  // no progress: stop
         rn = rn_new;
         break;
@@ -260,18 +380,18 @@ void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
     }
   } else {
     Multigrid<double> M64;
-    M64.init(c, c->D, wg, sweeps);
+    M64.init(c, D, wg, sweeps);
+    CgOperator<double> A64cg;
+    A64cg.init(c, wg);
     double* e64 = c->buf<double>("e64", n);
     while (rn > target * bn && used < max_iters) {
-      double tol = 0.5 * target * bn;  // absolute, on the current residual system
-      PcgResult pr_ = pcg<double>(c, A64, M64, r, e64, tol, max_iters - used);
+      const double tol = 0.5 * target * bn;  // absolute, on the current residual system
+      const PcgResult pr_ = pcg<double>(c, A64cg, M64, rsrc, e64, tol, max_iters - used);
       used += pr_.iters;
-      axpy<double, double>(s, n, 1.0, e64, x);
-      A64.residual(s, x, b, r);
-      double rn_new = std::sqrt(dot<double>(c, r, r, n));
+      const double rn_new = update_residual(e64, false, 1.0);
+      rsrc = r;
       st.refinement_steps++;
-      st.solve_bytes += pr_.iters * per_iter + 3.0 * n * 8.0 + (3.0 * n * 8.0 + c->P_in * 2.0 * (8.0 * 8.0 + 32.0)) +
-                        2.0 * n * 8.0;
+      st.solve_bytes += pr_.iters * per_iter + 8.0 * n + resid_bytes;
       if (pr_.iters == 0 || !(rn_new < rn)) {
         rn = rn_new;
         break;
@@ -279,6 +399,7 @@ void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
       rn = rn_new;
     }
   }
+  if (x != xA) PR_CUDA(cudaMemcpyAsync(xA, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   st.pcg_iterations = (uint32_t)used;
   st.rel_residual = rn / bn;
   st.converged = st.rel_residual <= target ? 1 : 0;
