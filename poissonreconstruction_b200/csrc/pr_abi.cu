@@ -12,6 +12,9 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
+#include <vector>
+#include <algorithm>
 
 #include <cmath>
 
@@ -67,28 +70,57 @@ void validate(const pr_params* p) {
 
 void set_device(pr_context* c) { PR_CUDA(cudaSetDevice(c->device)); }
 
+// host memcpy split over threads (first-touch page faults of fresh output buffers dominate)
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+  const size_t chunk = size_t(32) << 20;
+  unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  if (bytes < chunk || nt == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  nt = (unsigned)std::min<size_t>(nt, (bytes + chunk - 1) / chunk);
+  std::vector<std::thread> th;
+  const size_t per = (bytes + nt - 1) / nt;
+  for (unsigned i = 0; i < nt; ++i) {
+    const size_t lo = i * per, hi = std::min(bytes, lo + per);
+    if (lo >= hi) break;
+    th.emplace_back([=] { std::memcpy((char*)dst + lo, (const char*)src + lo, hi - lo); });
+  }
+  for (auto& t : th) t.join();
+}
+
 void copy_mesh_to_host(pr_context* c, pr_mesh* out) {
   out->vertices = nullptr;
   out->triangles = nullptr;
   out->n_vertices = c->nv;
   out->n_triangles = c->nt;
-  if (c->nv) {
-    out->vertices = (double*)std::malloc(3 * c->nv * sizeof(double));
-    if (!out->vertices) throw std::bad_alloc();
-    PR_CUDA(cudaMemcpyAsync(out->vertices, c->get<double>("mesh_v"), 3 * c->nv * sizeof(double),
-                            cudaMemcpyDeviceToHost, c->stream));
+  const size_t vb = 3 * c->nv * sizeof(double), tb = 3 * c->nt * sizeof(uint64_t);
+  if (vb + tb == 0) return;
+  if (c->h_stage_cap < vb + tb) {
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_cap = 0;
+    const size_t cap = (vb + tb) + ((vb + tb) >> 3);
+    PR_CUDA(cudaMallocHost(&c->h_stage, cap));
+    c->h_stage_cap = cap;
   }
-  if (c->nt) {
-    out->triangles = (uint64_t*)std::malloc(3 * c->nt * sizeof(uint64_t));
-    if (!out->triangles) {
-      std::free(out->vertices);
-      out->vertices = nullptr;
-      throw std::bad_alloc();
-    }
-    PR_CUDA(cudaMemcpyAsync(out->triangles, c->get<uint64_t>("mesh_t"), 3 * c->nt * sizeof(uint64_t),
-                            cudaMemcpyDeviceToHost, c->stream));
+  if (vb)
+    PR_CUDA(cudaMemcpyAsync(c->h_stage, c->get<double>("mesh_v"), vb, cudaMemcpyDeviceToHost, c->stream));
+  if (tb)
+    PR_CUDA(cudaMemcpyAsync(c->h_stage + vb, c->get<uint64_t>("mesh_t"), tb, cudaMemcpyDeviceToHost, c->stream));
+  out->vertices = vb ? (double*)std::malloc(vb) : nullptr;
+  out->triangles = tb ? (uint64_t*)std::malloc(tb) : nullptr;
+  if ((vb && !out->vertices) || (tb && !out->triangles)) {
+    std::free(out->vertices);
+    std::free(out->triangles);
+    out->vertices = nullptr;
+    out->triangles = nullptr;
+    c->sync();
+    throw std::bad_alloc();
   }
   c->sync();
+  if (vb) parallel_copy(out->vertices, c->h_stage, vb);
+  if (tb) parallel_copy(out->triangles, c->h_stage + vb, tb);
 }
 
 // The pipeline on device-resident points (c->buf "pts6" or caller memory).
@@ -269,6 +301,7 @@ int pr_context_destroy(pr_context* c) {
       if (kv.second.ptr) cudaFree(kv.second.ptr);
     c->bufs.clear();
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
   });

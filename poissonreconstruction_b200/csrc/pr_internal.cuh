@@ -116,6 +116,9 @@ struct pr_context {
   size_t bytes_held = 0, peak_bytes = 0;
   // pinned scalar staging (dot products, counters)
   double* h_scalars = nullptr;  // 64 doubles
+  // pinned staging for device->host mesh copies (grown on demand)
+  unsigned char* h_stage = nullptr;
+  size_t h_stage_cap = 0;
   // --- state of the last reconstruction ---
   bool have_state = false;
   bool have_points = false;

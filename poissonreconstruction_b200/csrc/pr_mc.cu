@@ -310,6 +310,128 @@ __global__ void k_mc_emit_tris(const uint8_t* __restrict__ acase, uint64_t A, co
 
 }  // namespace
 
+// ------------------------------------------------------------------ block-tiled classification (depth >= 4)
+// A CTA classifies the 16^3 cells of one Morton block.  Cell c has corners at grid
+// positions c + co[k]; the corner value is node (position - 1) per axis, so the CTA needs
+// nodes [-1, 15]^3 of its block: the block's own 16^3 nodes plus the low layer from the
+// neighbour blocks (zeros outside the domain, matching the crate's empty evaluation at 0).
+constexpr int MCW = 17;  // node tile width, tile coordinate = node local + 1
+
+__device__ __forceinline__ uint32_t sp4(uint32_t v) {
+  return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
+}
+
+__device__ void mc_load_tile(double* tile, const double* __restrict__ x, uint32_t blk, int res) {
+  const int t = threadIdx.x;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const uint64_t base = (uint64_t)blk << 12;
+  for (int i = t; i < 4096; i += blockDim.x) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)i, lx, ly, lz);
+    tile[((lz + 1) * MCW + (ly + 1)) * MCW + (lx + 1)] = __ldg(x + base + i);
+  }
+  // low layer: positions with a local coordinate -1 (817 of them)
+  const int nba = res >> 4;
+  for (int i = t; i < 817; i += blockDim.x) {
+    int lx, ly, lz;
+    if (i < 289) { lx = -1; ly = i % 17 - 1; lz = i / 17 - 1; }
+    else if (i < 561) { const int u = i - 289; lx = u % 16; ly = -1; lz = u / 16 - 1; }
+    else { const int u = i - 561; lx = u % 16; ly = u / 16; lz = -1; }
+    const int nx = (int)bx + (lx < 0 ? -1 : 0), ny = (int)by + (ly < 0 ? -1 : 0), nz = (int)bz + (lz < 0 ? -1 : 0);
+    double v = 0.0;
+    if (nx >= 0 && ny >= 0 && nz >= 0 && nx < nba && ny < nba && nz < nba) {
+      const uint32_t nb = morton3((uint32_t)nx, (uint32_t)ny, (uint32_t)nz) << 12;
+      v = __ldg(x + nb + (sp4((uint32_t)(lx & 15)) | (sp4((uint32_t)(ly & 15)) << 1) | (sp4((uint32_t)(lz & 15)) << 2)));
+    }
+    tile[((lz + 1) * MCW + (ly + 1)) * MCW + (lx + 1)] = v;
+  }
+}
+
+// case of local cell (lx,ly,lz) of block origin (ox,oy,oz); repeats of the corner node at
+// the top boundary (grid position res) are accumulated like the crate's evaluate()
+__device__ __forceinline__ uint32_t mc_tile_case(const double* tile, int lx, int ly, int lz, int ox, int oy, int oz,
+                                                 int res, double iso) {
+  uint32_t mc = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int cx = c_co[k][0], cy = c_co[k][1], cz = c_co[k][2];
+    const double s = tile[((lz + cz) * MCW + (ly + cy)) * MCW + (lx + cx)];
+    const int m = ((ox + lx + cx == res) ? 2 : 1) * ((oy + ly + cy == res) ? 2 : 1) * ((oz + lz + cz == res) ? 2 : 1);
+    double v = 0.0;
+    for (int i = 0; i < m; ++i) v = xadd(v, s);
+    if (v < iso) mc |= 1u << k;
+  }
+  return mc;
+}
+
+__global__ void __launch_bounds__(256) k_mc_block_count(const double* __restrict__ x, uint32_t D, double iso,
+                                                        uint32_t* __restrict__ blockcnt) {
+  __shared__ double tile[MCW * MCW * MCW];
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  mc_load_tile(tile, x, blk, res);
+  __syncthreads();
+  int cnt = 0;
+  for (int i = threadIdx.x; i < 4096; i += 256) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)i, lx, ly, lz);
+    const uint32_t mc = mc_tile_case(tile, lx, ly, lz, bx * 16, by * 16, bz * 16, res, iso);
+    cnt += (mc != 0u && mc != 255u);
+  }
+  typedef cub::BlockReduce<int, 256> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const int tot = BR(tmp).Sum(cnt);
+  if (threadIdx.x == 0) blockcnt[blk] = (uint32_t)tot;
+}
+
+// active blocks only (list from a compaction of blockcnt > 0); cells written in Morton order
+__global__ void __launch_bounds__(256) k_mc_block_emit(const double* __restrict__ x, uint32_t D, double iso,
+                                                       const uint32_t* __restrict__ ablk,
+                                                       const uint32_t* __restrict__ blockoff,
+                                                       uint32_t* __restrict__ acell, uint8_t* __restrict__ acase,
+                                                       uint32_t* __restrict__ nedge, uint32_t* __restrict__ ntri) {
+  __shared__ double tile[MCW * MCW * MCW];
+  const int res = 1 << D;
+  const uint32_t blk = ablk[blockIdx.x];
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  mc_load_tile(tile, x, blk, res);
+  __syncthreads();
+  typedef cub::BlockScan<int, 256> BS;
+  __shared__ typename BS::TempStorage tmp;
+  uint32_t running = blockoff[blk];
+  for (int chunk = 0; chunk < 16; ++chunk) {
+    const int i = chunk * 256 + threadIdx.x;  // Morton-local cell index
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)i, lx, ly, lz);
+    const uint32_t mc = mc_tile_case(tile, lx, ly, lz, bx * 16, by * 16, bz * 16, res, iso);
+    const int active = (mc != 0u && mc != 255u);
+    int off, tot;
+    BS(tmp).ExclusiveSum(active, off, tot);
+    if (active) {
+      const uint32_t a = running + (uint32_t)off;
+      acell[a] = (blk << 12) | (uint32_t)i;
+      acase[a] = (uint8_t)mc;
+      nedge[a] = __popc(edge_mask(mc));
+      ntri[a] = PR_MC_NTRI[mc];
+    }
+    running += (uint32_t)tot;
+    __syncthreads();  // temp storage reuse
+  }
+}
+
+__global__ void k_flags_nonzero(const uint32_t* __restrict__ cnt, uint32_t n, uint32_t* __restrict__ flag) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flag[i] = cnt[i] != 0;
+}
+__global__ void k_scatter_ids(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos, uint32_t n,
+                              uint32_t* __restrict__ ids) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (flag[i]) ids[pos[i]] = i;
+}
+
 // ====================================================================== host stages
 namespace {
 __global__ void k_gather_u64(const uint64_t* __restrict__ v, const uint32_t* __restrict__ perm, uint64_t E,
@@ -361,33 +483,72 @@ double stage_iso(pr_context* c, const double* d_x64) {
 
 void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool back_transform) {
   const uint64_t n = 1ull << (3 * D);
-  const unsigned nblk = (unsigned)((n + kThreads - 1) / kThreads);
   cudaStream_t s = c->stream;
-  uint32_t* blockcnt = c->buf<uint32_t>("mc_blockcnt", (size_t)nblk + 1);
-  uint32_t* blockoff = c->buf<uint32_t>("mc_blockoff", (size_t)nblk + 1);
-  k_mc_count<<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
-  PR_CHECK_LAUNCH();
-  PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
-  size_t tb = 0;
-  PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
-  void* tmp = c->buf<char>("cub_tmp", tb);
-  PR_COUNT_PRIMITIVE();
-  PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
-  uint32_t hA = 0;
-  PR_CUDA(cudaMemcpyAsync(&hA, blockoff + nblk, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  c->sync();
-  const uint64_t A = hA;
   c->nv = c->nt = 0;
   c->have_mesh = true;
-  if (A == 0) return;
-  uint32_t* acell = c->buf<uint32_t>("mc_acell", A);
-  uint8_t* acase = c->buf<uint8_t>("mc_acase", A);
-  uint32_t* nedge = c->buf<uint32_t>("mc_nedge", A + 1);
-  uint32_t* ntri = c->buf<uint32_t>("mc_ntri", A + 1);
-  uint32_t* eoff = c->buf<uint32_t>("mc_eoff", A + 1);
-  uint32_t* toff = c->buf<uint32_t>("mc_toff", A + 1);
-  k_mc_compact<<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
-  PR_CHECK_LAUNCH();
+  uint64_t A = 0;
+  uint32_t *acell, *nedge, *ntri, *eoff, *toff;
+  uint8_t* acase;
+  size_t tb = 0;
+  void* tmp = nullptr;
+  if (D >= 4) {
+    // 16^3 cell blocks: count per block, then emit the active blocks only
+    const uint32_t nblk = 1u << (3 * (D - 4));
+    uint32_t* blockcnt = c->buf<uint32_t>("mc_blockcnt", (size_t)nblk + 1);
+    uint32_t* blockoff = c->buf<uint32_t>("mc_blockoff", (size_t)nblk + 1);
+    uint32_t* flag = c->buf<uint32_t>("mc_flag", (size_t)nblk + 1);
+    uint32_t* fpos = c->buf<uint32_t>("mc_fpos", (size_t)nblk + 1);
+    uint32_t* ablk = c->buf<uint32_t>("mc_ablk", (size_t)nblk);
+    k_mc_block_count<<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
+    PR_CHECK_LAUNCH();
+    PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
+    k_flags_nonzero<<<grid_for(nblk + 1), kThreads, 0, s>>>(blockcnt, nblk + 1, flag);
+    PR_CHECK_LAUNCH();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
+    tmp = c->buf<char>("cub_tmp", tb);
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, fpos, (int64_t)nblk + 1, s));
+    k_scatter_ids<<<grid_for(nblk), kThreads, 0, s>>>(flag, fpos, nblk, ablk);
+    PR_CHECK_LAUNCH();
+    uint32_t hv[2] = {0, 0};
+    PR_CUDA(cudaMemcpyAsync(&hv[0], blockoff + nblk, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaMemcpyAsync(&hv[1], fpos + nblk, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    A = hv[0];
+    if (A == 0) return;
+    acell = c->buf<uint32_t>("mc_acell", A);
+    acase = c->buf<uint8_t>("mc_acase", A);
+    nedge = c->buf<uint32_t>("mc_nedge", A + 1);
+    ntri = c->buf<uint32_t>("mc_ntri", A + 1);
+    k_mc_block_emit<<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    PR_CHECK_LAUNCH();
+  } else {
+    const unsigned nblk = (unsigned)((n + kThreads - 1) / kThreads);
+    uint32_t* blockcnt = c->buf<uint32_t>("mc_blockcnt", (size_t)nblk + 1);
+    uint32_t* blockoff = c->buf<uint32_t>("mc_blockoff", (size_t)nblk + 1);
+    k_mc_count<<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
+    PR_CHECK_LAUNCH();
+    PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
+    tmp = c->buf<char>("cub_tmp", tb);
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
+    uint32_t hA = 0;
+    PR_CUDA(cudaMemcpyAsync(&hA, blockoff + nblk, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    A = hA;
+    if (A == 0) return;
+    acell = c->buf<uint32_t>("mc_acell", A);
+    acase = c->buf<uint8_t>("mc_acase", A);
+    nedge = c->buf<uint32_t>("mc_nedge", A + 1);
+    ntri = c->buf<uint32_t>("mc_ntri", A + 1);
+    k_mc_compact<<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
+    PR_CHECK_LAUNCH();
+  }
+  eoff = c->buf<uint32_t>("mc_eoff", A + 1);
+  toff = c->buf<uint32_t>("mc_toff", A + 1);
   PR_CUDA(cudaMemsetAsync(nedge + A, 0, sizeof(uint32_t), s));
   PR_CUDA(cudaMemsetAsync(ntri + A, 0, sizeof(uint32_t), s));
   tb = 0;

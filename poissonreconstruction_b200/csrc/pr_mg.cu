@@ -601,17 +601,92 @@ __device__ __forceinline__ void neighbour_bases(uint32_t* nb, uint32_t bx, uint3
   }
 }
 
+// Coarse tile for the prolongation: coarse block (8^3, Morton-contiguous) with a one-node
+// halo, natural layout 10^3, coordinate = coarse local + 1.
+template <typename T>
+__device__ __forceinline__ void load_coarse_tile(T* ctile, const T* __restrict__ ec, uint32_t blk, uint32_t bx,
+                                                 uint32_t by, uint32_t bz, int nblk_axis, uint32_t* cnb) {
+  const int t = threadIdx.x;
+  // interior: 512 contiguous coarse values
+  for (int i = t; i < 512; i += THREADS) {
+    uint32_t cx, cy, cz;
+    unmorton3((uint32_t)i, cx, cy, cz);
+    ctile[((cz + 1) * CW + (cy + 1)) * CW + (cx + 1)] = __ldg(ec + (uint64_t)blk * 512 + i);
+  }
+  // halo (488 positions): faces of 8x8 from the neighbour coarse blocks, then edges, corners
+  if (t < 27) {
+    const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+    const int x = (int)bx + dx, y = (int)by + dy, z = (int)bz + dz;
+    cnb[t] = (x < 0 || y < 0 || z < 0 || x >= nblk_axis || y >= nblk_axis || z >= nblk_axis)
+                 ? ~0u
+                 : (morton3((uint32_t)x, (uint32_t)y, (uint32_t)z) << 9);
+  }
+  __syncthreads();
+  auto sp3 = [](uint32_t v) { return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4); };
+  for (int i = t; i < 488; i += THREADS) {
+    int ux, uy, uz;
+    uint32_t mloc;
+    int nbi;
+    if (i < 384) {  // faces: 6 x 64
+      const int f = i >> 6, a = i & 7, b = (i >> 3) & 7, axis = f >> 1, hi = f & 1;
+      const uint32_t side = hi ? 0u : 0x49u;  // local 0 or 7, spread
+      const int s = hi ? 9 : 0;
+      if (axis == 0) { mloc = side | (sp3(a) << 1) | (sp3(b) << 2); ux = s; uy = a + 1; uz = b + 1; nbi = (hi ? 2 : 0) + 3 + 9; }
+      else if (axis == 1) { mloc = sp3(a) | (side << 1) | (sp3(b) << 2); ux = a + 1; uy = s; uz = b + 1; nbi = 1 + 3 * (hi ? 2 : 0) + 9; }
+      else { mloc = sp3(a) | (sp3(b) << 1) | (side << 2); ux = a + 1; uy = b + 1; uz = s; nbi = 1 + 3 + 9 * (hi ? 2 : 0); }
+    } else if (i < 480) {  // edges: 12 x 8
+      const int e = (i - 384) >> 3, a = (i - 384) & 7, axis = e >> 2, s1 = e & 1, s2 = (e >> 1) & 1;
+      const uint32_t c1 = s1 ? 0u : 0x49u, c2 = s2 ? 0u : 0x49u;
+      const int u1 = s1 ? 9 : 0, u2 = s2 ? 9 : 0, d1 = s1 ? 2 : 0, d2 = s2 ? 2 : 0;
+      if (axis == 0) { mloc = sp3(a) | (c1 << 1) | (c2 << 2); ux = a + 1; uy = u1; uz = u2; nbi = 1 + 3 * d1 + 9 * d2; }
+      else if (axis == 1) { mloc = c1 | (sp3(a) << 1) | (c2 << 2); ux = u1; uy = a + 1; uz = u2; nbi = d1 + 3 + 9 * d2; }
+      else { mloc = c1 | (c2 << 1) | (sp3(a) << 2); ux = u1; uy = u2; uz = a + 1; nbi = d1 + 3 * d2 + 9; }
+    } else {  // corners
+      const int c = i - 480, sx = c & 1, sy = (c >> 1) & 1, sz = (c >> 2) & 1;
+      mloc = (sx ? 0u : 0x49u) | ((sy ? 0u : 0x49u) << 1) | ((sz ? 0u : 0x49u) << 2);
+      ux = sx ? 9 : 0; uy = sy ? 9 : 0; uz = sz ? 9 : 0;
+      nbi = (sx ? 2 : 0) + 3 * (sy ? 2 : 0) + 9 * (sz ? 2 : 0);
+    }
+    const uint32_t b0 = cnb[nbi];
+    ctile[(uz * CW + uy) * CW + ux] = b0 != ~0u ? __ldg(ec + b0 + mloc) : (T)0;
+  }
+}
+
+// P ec at fine tile coordinate (ux,uy,uz) (fine local + 1); ctile coordinate = coarse local + 1.
+// Even fine local coordinate l -> coarse l/2 (w 1); odd -> (l-1)/2, (l+1)/2 (w 1/2 each).
+template <typename T>
+__device__ __forceinline__ T prolong_at(const T* ctile, int ux, int uy, int uz) {
+  const int lx = ux - 1, ly = uy - 1, lz = uz - 1;
+  const int ax = (lx >> 1) + 1, ay = (ly >> 1) + 1, az = (lz >> 1) + 1;  // floor(l/2) + 1
+  const int ox = lx & 1, oy = ly & 1, oz = lz & 1;
+  const T* c = ctile + (az * CW + ay) * CW + ax;
+  // the +1 neighbours exist (index <= CW-1) exactly when the coordinate is odd
+  T v00 = c[0];
+  T v01 = oy ? c[CW] : (T)0;
+  T v10 = oz ? c[CW * CW] : (T)0;
+  T v11 = (oy && oz) ? c[CW * CW + CW] : (T)0;
+  if (ox) {
+    v00 = (T)0.5 * (v00 + c[1]);
+    if (oy) v01 = (T)0.5 * (v01 + c[CW + 1]);
+    if (oz) v10 = (T)0.5 * (v10 + c[CW * CW + 1]);
+    if (oy && oz) v11 = (T)0.5 * (v11 + c[CW * CW + CW + 1]);
+  }
+  const T y0 = oy ? (T)0.5 * (v00 + v01) : v00;
+  const T y1 = oy ? (T)0.5 * (v10 + v11) : v10;
+  return oz ? (T)0.5 * (y0 + y1) : y0;
+}
+
 // MODE 0: xo = sweep(xi); 1: xo = sweep(0); 2: xo = sweep(xi + P ec).  DOT: part = f.xo
 template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
-__global__ void __launch_bounds__(THREADS) k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo,
-                                                     const T* __restrict__ f, const T* __restrict__ ec, T c0inv,
-                                                     T ce, T cc, const T* __restrict__ table,
-                                                     double* __restrict__ part) {
+__global__ void __launch_bounds__(THREADS, 4) k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo,
+                                                        const T* __restrict__ f, const T* __restrict__ ec, T c0inv,
+                                                        T ce, T cc, const T* __restrict__ table,
+                                                        double* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
   T* fs = tile + TILE;                       // N
   T* ctile = fs + N;                         // CW^3 (MODE 2)
-  __shared__ uint32_t nb[27];
+  __shared__ uint32_t nb[27], cnb[27];
   const int res = 1 << D;
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * N;
@@ -621,83 +696,52 @@ __global__ void __launch_bounds__(THREADS) k_smooth16(uint32_t D, const T* __res
   const int t = threadIdx.x;
   if (MODE != 1) neighbour_bases(nb, bx, by, bz, res >> 4);
   else if (t < 27) nb[t] = ~0u;  // zero halo
-  if (MODE == 2) {
-    const int cox = ox / 2 - 1, coy = oy / 2 - 1, coz = oz / 2 - 1, resc = res >> 1;
-    for (int i = t; i < CW * CW * CW; i += THREADS) {
-      const int cx = cox + i % CW, cy = coy + (i / CW) % CW, cz = coz + i / (CW * CW);
-      T v = 0;
-      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < resc && cy < resc && cz < resc) v = __ldg(ec + morton3(cx, cy, cz));
-      ctile[i] = v;
-    }
-  }
-  // interior: 4 quads per thread
+  if (MODE == 2) load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // contains a barrier
+  else __syncthreads();  // nb
+  // interior: 4 quads per thread; quad element e at tile offset qoff[e] from element 0
+  int tq[4];  // tile index of each quad's element 0
+  int fq[4];  // f index of each quad's element 0
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int q = t + 256 * r;
     int lx, ly, lz;
     quad_coords(q, lx, ly, lz);
+    tq[r] = ps(lx + 1, ly + 1, lz + 1);
+    fq[r] = fidx(lx, ly, lz);
     const typename Vec4<T>::type fv = ld4(f + base + 4 * q);
-    fs[fidx(lx, ly, lz)] = fv.x;
-    fs[fidx(lx + 1, ly, lz)] = fv.y;
-    fs[fidx(lx, ly + 1, lz)] = fv.z;
-    fs[fidx(lx + 1, ly + 1, lz)] = fv.w;
-    typename Vec4<T>::type xv;
-    if (MODE == 1) xv.x = xv.y = xv.z = xv.w = (T)0;
-    else xv = ld4(xi + base + 4 * q);
-    tile[ps(lx + 1, ly + 1, lz + 1)] = xv.x;
-    tile[ps(lx + 2, ly + 1, lz + 1)] = xv.y;
-    tile[ps(lx + 1, ly + 2, lz + 1)] = xv.z;
-    tile[ps(lx + 2, ly + 2, lz + 1)] = xv.w;
+    fs[fq[r]] = fv.x;
+    fs[fq[r] + 512] = fv.y;
+    fs[fq[r] + 1024] = fv.z;
+    fs[fq[r] + 1536] = fv.w;
+    T v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+    if (MODE != 1) {
+      const typename Vec4<T>::type xv = ld4(xi + base + 4 * q);
+      v0 = xv.x; v1 = xv.y; v2 = xv.z; v3 = xv.w;
+      if (MODE == 2) {
+        v0 += prolong_at<T>(ctile, lx + 1, ly + 1, lz + 1);
+        v1 += prolong_at<T>(ctile, lx + 2, ly + 1, lz + 1);
+        v2 += prolong_at<T>(ctile, lx + 1, ly + 2, lz + 1);
+        v3 += prolong_at<T>(ctile, lx + 2, ly + 2, lz + 1);
+      }
+    }
+    // ux = lx + 1 is odd: the x neighbour is in sub-tile (own ^ 1) = own - 1, one column on
+    tile[tq[r]] = v0;
+    tile[tq[r] - SUB + 1] = v1;
+    tile[tq[r] - 2 * SUB + RS] = v2;
+    tile[tq[r] - 3 * SUB + RS + 1] = v3;
   }
-  __syncthreads();  // nb
+  // halo (zeros outside the domain; in MODE 1 every neighbour base is ~0u)
   load_halo<T>(tile, xi, nb, [](int ux, int uy, int uz) { return ps(ux, uy, uz); },
-               [&](uint32_t m) { return MODE == 1 ? (T)0 : __ldg(xi + m); });
+               [&](uint32_t m) -> T { return MODE == 1 ? (T)0 : __ldg(xi + m); });
   __syncthreads();
   if (MODE == 2) {
-    // tile += P ec: coarse cell m (per axis in [-1, 8]) covers fine tile coordinates 2m+1 (even
-    // global, coarse m+1) and 2m+2 (odd global, mean of coarse m+1 and m+2)
-    for (int i = t; i < 1000; i += THREADS) {
-      const int mx = i % 10 - 1, my = (i / 10) % 10 - 1, mz = i / 100 - 1;
-      T cv[2][2][2];
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const int ix = mx + 1 + c, iy = my + 1 + b, iz = mz + 1 + a;
-            cv[a][b][c] = (ix < CW && iy < CW && iz < CW) ? ctile[(iz * CW + iy) * CW + ix] : (T)0;
-          }
-      // along x: even (c0) and odd (0.5 (c0 + c1))
-      T vx[2][2][2];
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          vx[a][b][0] = cv[a][b][0];
-          vx[a][b][1] = (T)0.5 * (cv[a][b][0] + cv[a][b][1]);
-        }
-      T vy[2][2][2];
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          vy[a][0][c] = vx[a][0][c];
-          vy[a][1][c] = (T)0.5 * (vx[a][0][c] + vx[a][1][c]);
-        }
-#pragma unroll
-      for (int sz = 0; sz < 2; ++sz)
-#pragma unroll
-        for (int sy = 0; sy < 2; ++sy)
-#pragma unroll
-          for (int sx = 0; sx < 2; ++sx) {
-            const int ux = 2 * mx + 1 + sx, uy = 2 * my + 1 + sy, uz = 2 * mz + 1 + sz;
-            if (ux < 0 || uy < 0 || uz < 0 || ux > 17 || uy > 17 || uz > 17) continue;
-            const int gx = ox - 1 + ux, gy = oy - 1 + uy, gz = oz - 1 + uz;
-            if (gx < 0 || gy < 0 || gz < 0 || gx >= res || gy >= res || gz >= res) continue;
-            const T v = sz ? (T)0.5 * (vy[0][sy][sx] + vy[1][sy][sx]) : vy[0][sy][sx];
-            tile[ps(ux, uy, uz)] += v;
-          }
+    // add P ec on the halo shell (in-domain positions only)
+    for (int i = t; i < 1736; i += THREADS) {
+      int ux, uy, uz;
+      halo_u<16>(i, ux, uy, uz);
+      const int gx = ox - 1 + ux, gy = oy - 1 + uy, gz = oz - 1 + uz;
+      if (gx < 0 || gy < 0 || gz < 0 || gx >= res || gy >= res || gz >= res) continue;
+      tile[ps(ux, uy, uz)] += prolong_at<T>(ctile, ux, uy, uz);
     }
     __syncthreads();
   }
@@ -705,40 +749,37 @@ __global__ void __launch_bounds__(THREADS) k_smooth16(uint32_t D, const T* __res
   // Gauss-Seidel: lanes = 8 x-lattice positions x 4 z-pairs; warps = 8 y-lattice rows
   const int li = t & 7, kp = (t >> 3) & 3, lj = t >> 5;
   const bool faces = FACES && (ox == 0 || oy == 0 || oz == 0);
+  double acc = 0.0;
 #pragma unroll
   for (int step = 0; step < 8; ++step) {
     const int col = FWD ? step : 7 - step;
     const int cx = col & 1, cy = (col >> 1) & 1, cz = col >> 2;
     const int own = (1 - cx) | ((1 - cy) << 1) | ((1 - cz) << 2);
-    // sub-tile bases of the x/y/xy-flipped neighbours in the three z planes
     const int hx = li + cx, hy = lj + cy;
-    // offsets inside a sub-tile for dx/dy = -1/+1 (depend on the colour bit)
     const int xm = -cx, xp = 1 - cx, ym = -cy, yp = 1 - cy;
     const int zm = -cz, zp = 1 - cz;
-    const int so = own * SUB, sx_ = (own ^ 1) * SUB, sy_ = (own ^ 2) * SUB, sxy = (own ^ 3) * SUB;
-    const int sz_ = (own ^ 4) * SUB, sxz = (own ^ 5) * SUB, syz = (own ^ 6) * SUB, sxyz = (own ^ 7) * SUB;
+    const int so = own * SUB, sxy = (own ^ 3) * SUB;
+    const int sxz = (own ^ 5) * SUB, syz = (own ^ 6) * SUB, sxyz = (own ^ 7) * SUB;
+    const int pr = hy * RS + hx;
     T nv[2];
-    T pfb, peb;  // plane below: cross sum (edges), diagonal sum (corners)
+    T pfb = 0, peb = 0;
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int lk = 2 * kp + s;
       const int hz = lk + cz;
-      const int pr = hy * RS + hx;  // row/column part
       if (s == 0) {
-        const int pz = (hz + zm) * PS;
-        pfb = tile[sxz + pz + pr + xm] + tile[sxz + pz + pr + xp] + tile[syz + pz + pr + ym * RS] +
-              tile[syz + pz + pr + yp * RS];
-        peb = tile[sxyz + pz + pr + ym * RS + xm] + tile[sxyz + pz + pr + ym * RS + xp] +
-              tile[sxyz + pz + pr + yp * RS + xm] + tile[sxyz + pz + pr + yp * RS + xp];
+        const int pz = (hz + zm) * PS + pr;
+        pfb = tile[sxz + pz + xm] + tile[sxz + pz + xp] + tile[syz + pz + ym * RS] + tile[syz + pz + yp * RS];
+        peb = tile[sxyz + pz + ym * RS + xm] + tile[sxyz + pz + ym * RS + xp] + tile[sxyz + pz + yp * RS + xm] +
+              tile[sxyz + pz + yp * RS + xp];
       }
-      const int p0 = hz * PS;
-      const T peo = tile[sxy + p0 + pr + ym * RS + xm] + tile[sxy + p0 + pr + ym * RS + xp] +
-                    tile[sxy + p0 + pr + yp * RS + xm] + tile[sxy + p0 + pr + yp * RS + xp];
-      const int pa = (hz + zp) * PS;
-      const T pfa = tile[sxz + pa + pr + xm] + tile[sxz + pa + pr + xp] + tile[syz + pa + pr + ym * RS] +
-                    tile[syz + pa + pr + yp * RS];
-      const T pea = tile[sxyz + pa + pr + ym * RS + xm] + tile[sxyz + pa + pr + ym * RS + xp] +
-                    tile[sxyz + pa + pr + yp * RS + xm] + tile[sxyz + pa + pr + yp * RS + xp];
+      const int p0 = hz * PS + pr;
+      const T peo = tile[sxy + p0 + ym * RS + xm] + tile[sxy + p0 + ym * RS + xp] + tile[sxy + p0 + yp * RS + xm] +
+                    tile[sxy + p0 + yp * RS + xp];
+      const int pa = (hz + zp) * PS + pr;
+      const T pfa = tile[sxz + pa + xm] + tile[sxz + pa + xp] + tile[syz + pa + ym * RS] + tile[syz + pa + yp * RS];
+      const T pea = tile[sxyz + pa + ym * RS + xm] + tile[sxyz + pa + ym * RS + xp] + tile[sxyz + pa + yp * RS + xm] +
+                    tile[sxyz + pa + yp * RS + xp];
       const T fi = fs[((col * 8 + lj) * 2 + s) * 32 + 8 * kp + li];
       T v = (fi - ce * (peo + pfb + pfa) - cc * (peb + pea)) * c0inv;
       if (faces) {
@@ -760,34 +801,23 @@ __global__ void __launch_bounds__(THREADS) k_smooth16(uint32_t D, const T* __res
         }
       }
       nv[s] = v;
+      if (DOT) acc += (double)fi * (double)v;  // the node's final value of this sweep
       pfb = pfa;
       peb = pea;
-      (void)so;
-      (void)sx_;
-      (void)sy_;
-      (void)sz_;
     }
-    const int pr = hy * RS + hx;
     tile[so + (2 * kp + cz) * PS + pr] = nv[0];
     tile[so + (2 * kp + 1 + cz) * PS + pr] = nv[1];
     __syncthreads();
   }
 
-  double acc = 0.0;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    const int q = t + 256 * r;
-    int lx, ly, lz;
-    quad_coords(q, lx, ly, lz);
     typename Vec4<T>::type v;
-    v.x = tile[ps(lx + 1, ly + 1, lz + 1)];
-    v.y = tile[ps(lx + 2, ly + 1, lz + 1)];
-    v.z = tile[ps(lx + 1, ly + 2, lz + 1)];
-    v.w = tile[ps(lx + 2, ly + 2, lz + 1)];
-    st4(xo + base + 4 * q, v);
-    if (DOT)
-      acc += (double)v.x * (double)fs[fidx(lx, ly, lz)] + (double)v.y * (double)fs[fidx(lx + 1, ly, lz)] +
-             (double)v.z * (double)fs[fidx(lx, ly + 1, lz)] + (double)v.w * (double)fs[fidx(lx + 1, ly + 1, lz)];
+    v.x = tile[tq[r]];
+    v.y = tile[tq[r] - SUB + 1];
+    v.z = tile[tq[r] - 2 * SUB + RS];
+    v.w = tile[tq[r] - 3 * SUB + RS + 1];
+    st4(xo + base + 4 * (t + 256 * r), v);
   }
   if (DOT) {
     typedef cub::BlockReduce<double, THREADS> BR;
@@ -795,6 +825,7 @@ __global__ void __launch_bounds__(THREADS) k_smooth16(uint32_t D, const T* __res
     const double sum = BR(tmp).Sum(acc);
     if (t == 0) part[blk] = sum;
   }
+  (void)fq;
 }
 
 template <typename T>

@@ -217,39 +217,81 @@ __device__ __forceinline__ double dmass1(int d) { return d == 0 ? 0.0 : (d == 1 
 
 constexpr uint32_t kEmpty = 0xffffffffu;
 
-// Laplacian part of assemble_rhs (src/fem_tree.rs:258-274), every node, exact order
-// dx (outer), dy, dz (inner).  Nodes without a touched neighbour get 0.
+// Laplacian part of assemble_rhs (src/fem_tree.rs:258-274) at node i, exact order dx
+// (outer), dy, dz (inner); neighbours without a touched node contribute exactly 0.
+__device__ __forceinline__ double rhs_node(uint32_t i, int res, double h2, const uint32_t* __restrict__ map,
+                                           const double* __restrict__ v, uint64_t T) {
+  uint32_t ix, iy, iz;
+  unmorton3(i, ix, iy, iz);
+  double sum = 0.0;
+  for (int dx = -1; dx <= 1; ++dx) {
+    const int jx = (int)ix + dx;
+    if (jx < 0 || jx >= res) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int jy = (int)iy + dy;
+      if (jy < 0 || jy >= res) continue;
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int jz = (int)iz + dz;
+        if (jz < 0 || jz >= res) continue;
+        const uint32_t slot = map[morton3(jx, jy, jz)];
+        if (slot == kEmpty) continue;
+        const double vx = v[slot], vy = v[T + slot], vz = v[2 * T + slot];
+        const double a = xmul(xmul(xmul(vx, dmass1(dx)), mass1(dy)), mass1(dz));
+        const double bb = xmul(xmul(xmul(vy, mass1(dx)), dmass1(dy)), mass1(dz));
+        const double cc = xmul(xmul(xmul(vz, mass1(dx)), mass1(dy)), dmass1(dz));
+        sum = xadd(sum, xmul(h2, xadd(xadd(a, bb), cc)));
+      }
+    }
+  }
+  return sum;
+}
+
+// every node (small grids)
 __global__ void k_rhs_dense(uint32_t D, const uint32_t* __restrict__ map, const double* __restrict__ v, uint64_t T,
                             double* __restrict__ b) {
   const int res = 1 << D;
   const double h = 1.0 / (double)res;
   const double h2 = xmul(h, h);
   const uint64_t n = 1ull << (3 * D);
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t ix, iy, iz;
-    unmorton3((uint32_t)i, ix, iy, iz);
-    double sum = 0.0;
-    for (int dx = -1; dx <= 1; ++dx) {
-      int jx = (int)ix + dx;
-      if (jx < 0 || jx >= res) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        int jy = (int)iy + dy;
-        if (jy < 0 || jy >= res) continue;
-        for (int dz = -1; dz <= 1; ++dz) {
-          int jz = (int)iz + dz;
-          if (jz < 0 || jz >= res) continue;
-          uint32_t slot = map[morton3(jx, jy, jz)];
-          if (slot == kEmpty) continue;
-          double vx = v[slot], vy = v[T + slot], vz = v[2 * T + slot];
-          double a = xmul(xmul(xmul(vx, dmass1(dx)), mass1(dy)), mass1(dz));
-          double bb = xmul(xmul(xmul(vy, mass1(dx)), dmass1(dy)), mass1(dz));
-          double cc = xmul(xmul(xmul(vz, mass1(dx)), mass1(dy)), dmass1(dz));
-          sum = xadd(sum, xmul(h2, xadd(xadd(a, bb), cc)));
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = rhs_node((uint32_t)i, res, h2, map, v, T);
+}
+
+// Only the 16^3 blocks that hold a touched node or border one; b is zero elsewhere.
+__global__ void k_mark_rhs_blocks(const uint32_t* __restrict__ tnode, uint64_t T, uint32_t nba,
+                                  uint32_t* __restrict__ flag) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t node = tnode[t];
+    uint32_t bx, by, bz, lx, ly, lz;
+    unmorton3(node >> 12, bx, by, bz);
+    unmorton3(node & 4095u, lx, ly, lz);
+    const int x0 = lx == 0 ? -1 : 0, x1 = lx == 15 ? 1 : 0;
+    const int y0 = ly == 0 ? -1 : 0, y1 = ly == 15 ? 1 : 0;
+    const int z0 = lz == 0 ? -1 : 0, z1 = lz == 15 ? 1 : 0;
+    for (int dz = z0; dz <= z1; ++dz)
+      for (int dy = y0; dy <= y1; ++dy)
+        for (int dx = x0; dx <= x1; ++dx) {
+          const int x = (int)bx + dx, y = (int)by + dy, z = (int)bz + dz;
+          if (x < 0 || y < 0 || z < 0 || x >= (int)nba || y >= (int)nba || z >= (int)nba) continue;
+          flag[morton3(x, y, z)] = 1u;
         }
-      }
-    }
-    b[i] = sum;
   }
+}
+
+__global__ void k_list_blocks(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos, uint32_t n,
+                              uint32_t* __restrict__ ids) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (flag[i]) ids[pos[i]] = i;
+}
+
+__global__ void __launch_bounds__(256) k_rhs_blocks(uint32_t D, const uint32_t* __restrict__ blocks,
+                                                    const uint32_t* __restrict__ map, const double* __restrict__ v,
+                                                    uint64_t T, double* __restrict__ b) {
+  const int res = 1 << D;
+  const double h = 1.0 / (double)res;
+  const double h2 = xmul(h, h);
+  const uint32_t base = blocks[blockIdx.x] << 12;
+  for (int k = threadIdx.x; k < 4096; k += 256) b[base + k] = rhs_node(base + (uint32_t)k, res, h2, map, v, T);
 }
 
 // Screening part of assemble_rhs (src/fem_tree.rs:276-297): b[node] += wh3*0.5*bx*by*bz per
@@ -430,8 +472,34 @@ void stage_splat_rhs(pr_context* c, uint32_t D, double pw) {
     PR_CHECK_LAUNCH();
   }
   double* b = c->buf<double>("b64", n);
-  k_rhs_dense<<<grid_for(n, kThreads, 1u << 22), kThreads, 0, c->stream>>>(D, map, v, T, b);
-  PR_CHECK_LAUNCH();
+  if (D >= 4 && T > 0) {
+    const uint32_t nblk = 1u << (3 * (D - 4));
+    uint32_t* flag = c->buf<uint32_t>("rhs_flag", (size_t)nblk + 1);
+    uint32_t* fpos = c->buf<uint32_t>("rhs_fpos", (size_t)nblk + 1);
+    uint32_t* ids = c->buf<uint32_t>("rhs_blocks", nblk);
+    PR_CUDA(cudaMemsetAsync(flag, 0, ((size_t)nblk + 1) * sizeof(uint32_t), c->stream));
+    PR_CUDA(cudaMemsetAsync(b, 0, n * sizeof(double), c->stream));
+    k_mark_rhs_blocks<<<grid_for(T), kThreads, 0, c->stream>>>(c->get<uint32_t>("splat_runkey"), T, 1u << (D - 4),
+                                                               flag);
+    PR_CHECK_LAUNCH();
+    size_t tb = 0;
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, fpos, (int64_t)nblk + 1, c->stream));
+    void* tmp = c->buf<char>("cub_tmp", tb);
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, flag, fpos, (int64_t)nblk + 1, c->stream));
+    k_list_blocks<<<grid_for(nblk), kThreads, 0, c->stream>>>(flag, fpos, nblk, ids);
+    PR_CHECK_LAUNCH();
+    uint32_t nact = 0;
+    PR_CUDA(cudaMemcpyAsync(&nact, fpos + nblk, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    if (nact > 0) {
+      k_rhs_blocks<<<nact, 256, 0, c->stream>>>(D, ids, map, v, T, b);
+      PR_CHECK_LAUNCH();
+    }
+  } else {
+    k_rhs_dense<<<grid_for(n, kThreads, 1u << 22), kThreads, 0, c->stream>>>(D, map, v, T, b);
+    PR_CHECK_LAUNCH();
+  }
 
   // --- screening: trunc cells; kept as per-point payload for the operator
   c->S = 0;
