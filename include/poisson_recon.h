@@ -176,6 +176,22 @@ int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precisi
  * primitives such as radix sorts and scans are counted in *primitive_calls). */
 uint64_t pr_kernel_launches(uint64_t* primitive_calls);
 
+/* Iso value without any device allocation.  No counterpart in the reference crate: it exists
+ * for callers that cannot allocate device memory — a host whose caching allocator already
+ * holds the free device memory (a raw cudaMalloc would fail or fragment it), or a
+ * latency-bound loop that must not pay for the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  Every input and the output are caller device pointers:
+ * d_coefficients (res^3 FP64 values in the FEM index order, res = 2^depth), d_points3 (n
+ * unit-cube points, x y z each), d_iso (1 double: the mean of the implicit function over the
+ * points, as in src/reconstructor.rs:56).  Enqueued on `stream` (NULL = default stream), no
+ * synchronisation.  Per-block partial sums live in a fixed 18,944-byte __device__ array that
+ * each GPU loading the library keeps until exit; the first call on a device (with that
+ * device current) resolves its address — make that first call before any stream capture.
+ * All calls share the array: calls whose kernels overlap on the GPU race.  Limits:
+ * 1 <= n <= 2^28 points, depth 1..10; anything else returns PR_ERR_INVALID_ARGUMENT. */
+int pr_iso_value_noalloc(uint32_t depth, const double* d_coefficients, const double* d_points3, uint64_t n,
+                         double* d_iso, void* stream);
+
 /* Library build information (static string). */
 const char* pr_version(void);
 /* sizeof(pr_params), sizeof(pr_mesh), sizeof(pr_stats), sizeof(pr_oriented_point): lets a

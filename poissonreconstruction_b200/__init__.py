@@ -63,6 +63,7 @@ SIGNATURES = {
     "pr_abi_layout": (None, [_P]),
     "pr_kernel_launches": (C.c_uint64, [C.POINTER(C.c_uint64)]),
     "pr_ctx_apply_operator_device": (C.c_int, [_P, _P, _P, C.c_int]),
+    "pr_iso_value_noalloc": (C.c_int, [C.c_uint32, _P, _P, C.c_uint64, _P, _P]),
     "pr_ctx_kernel_bench": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
                                       C.POINTER(C.c_double)]),
     "pr_last_error": (C.c_char_p, []),

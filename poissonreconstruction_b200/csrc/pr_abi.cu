@@ -196,6 +196,10 @@ thread_local std::unique_ptr<pr_context, int (*)(pr_context*)> g_thread_ctx(null
 
 }  // namespace
 
+namespace pr {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace pr
+
 static std::atomic<uint64_t> g_launches{0}, g_primitives{0};
 
 extern "C" {
