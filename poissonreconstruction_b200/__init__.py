@@ -12,6 +12,7 @@ anywhere, but any computation raises if the library or a B200 is missing.
 import ctypes as C
 import dataclasses
 import os
+import weakref
 
 import numpy as np
 
@@ -181,12 +182,34 @@ class ReconstructStats:
         return cls(**{f.name: getattr(s, f.name) for f in dataclasses.fields(cls)})
 
 
+_LIBC = None
+
+
+def _libc_free():
+    global _LIBC
+    if _LIBC is None:
+        _LIBC = C.CDLL(None).free
+        _LIBC.argtypes = [C.c_void_p]
+        _LIBC.restype = None
+    return _LIBC
+
+
+def _owned_array(ptr, count, ctype, dtype):
+    """numpy view of a malloc'd library buffer; the buffer is freed with the array."""
+    if not count:
+        return np.zeros((0, 3), dtype=dtype)
+    base = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count * 3,))
+    weakref.finalize(base, _libc_free(), C.cast(ptr, C.c_void_p).value)
+    return base.reshape(-1, 3)
+
+
 def _take_mesh(m):
-    v = np.ctypeslib.as_array(m.vertices, shape=(m.n_vertices * 3,)).reshape(-1, 3).copy() \
-        if m.n_vertices else np.zeros((0, 3))
-    t = np.ctypeslib.as_array(m.triangles, shape=(m.n_triangles * 3,)).reshape(-1, 3).copy() \
-        if m.n_triangles else np.zeros((0, 3), np.uint64)
-    lib().pr_mesh_free(C.byref(m))
+    """Take ownership of a pr_mesh without copying (the library allocates with malloc)."""
+    v = _owned_array(m.vertices, m.n_vertices, C.c_double, np.float64)
+    t = _owned_array(m.triangles, m.n_triangles, C.c_uint64, np.uint64)
+    m.vertices = None
+    m.triangles = None
+    m.n_vertices = m.n_triangles = 0
     return Mesh(v, t)
 
 
