@@ -172,6 +172,45 @@ int pr_ctx_apply_operator_device(pr_context* ctx, const void* d_x, void* d_y, in
 int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precision, int reps, double* ms_per_launch,
                         double* bytes_per_launch);
 
+/* ------------------------------------------------------------------ adjoint (gradients)
+ * No counterpart in the reference crate.  The implicit function chi(q) = evaluate(x, M q)
+ * (src/fem_tree.rs:490-513) of the solved coefficients x (A x = b, src/fem_tree.rs:180-299)
+ * at K query points q (MODEL space, mapped with the reconstruction's unit-cube transform M)
+ * is differentiated w.r.t. the input points' model-space positions and normals.  Given the
+ * upstream gradient g_k = dL/dchi_k, the adjoint solve A lambda = E^T g (A is symmetric; E =
+ * the evaluation matrix) gives dL/dtheta = lambda . db/dtheta - lambda . (dA/dtheta) x through
+ * the normalised splat (src/fem_tree.rs:130-178), the divergence RHS and the screening RHS and
+ * matrix.  M follows the bounding box of the input and is HELD FIXED (not differentiated).
+ * The basis is piecewise linear: at a point exactly on a cell face the one-sided derivative
+ * of the cell the point falls in is returned. */
+typedef struct pr_adjoint_stats {
+  double loss;          /* sum_k g_k chi_k, or mean chi_k^2 when dl_dchi was NULL */
+  double rel_residual;  /* adjoint solve ||E^T g - A lambda|| / ||E^T g|| */
+  uint32_t pcg_iterations;
+  uint32_t refinement_steps;
+  int32_t converged;
+  int32_t reserved_i;
+  double time_solve;  /* seconds in the adjoint solve */
+  double time_total;  /* seconds in the whole call */
+  double reserved[4];
+} pr_adjoint_stats;
+
+/* Forward without marching cubes: transform, splat, RHS and the solve of the crate's fine
+ * system (host points; stats as pr_ctx_reconstruct, mesh counts 0).  The state it leaves is
+ * what pr_ctx_loss_backward differentiates. */
+int pr_ctx_solve(pr_context* ctx, const double* points6, uint64_t n, const pr_params* params, pr_stats* out_stats);
+/* Backward of the last pr_ctx_solve / pr_ctx_reconstruct on this context (which must have
+ * used solve_mode PR_SOLVE_CONVERGED).  queries3: k model-space points (x y z); dl_dchi: k
+ * upstream gradients, or NULL for the loss L = mean_k chi_k^2.  Outputs (host, any may be
+ * NULL): chi (k), dl_dpositions and dl_dnormals (n x 3 each, the input's point order).  The
+ * adjoint solve uses the last call's precision and target_rel_residual. */
+int pr_ctx_loss_backward(pr_context* ctx, const double* queries3, uint64_t k, const double* dl_dchi, double* chi,
+                         double* dl_dpositions, double* dl_dnormals, pr_adjoint_stats* out_stats);
+/* One-shot: pr_ctx_solve + pr_ctx_loss_backward on the calling thread's default context. */
+int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params, const double* queries3, uint64_t k,
+                     const double* dl_dchi, double* chi, double* dl_dpositions, double* dl_dnormals,
+                     pr_adjoint_stats* out_stats);
+
 /* Number of kernels launched by this library in this process (own kernels; library
  * primitives such as radix sorts and scans are counted in *primitive_calls). */
 uint64_t pr_kernel_launches(uint64_t* primitive_calls);

@@ -84,6 +84,8 @@ def lib():
         "orc_csr_gs_sweep": (None, [_u64, _p, _p, _p, _p, _p]),
         "orc_reconstruct": (C.c_int, [_p, _u64, C.POINTER(OrcParams), C.POINTER(OrcMesh),
                                       C.POINTER(OrcStats), _p]),
+        "orc_loss": (_d, [_p, _u64, _u32, _d, _d, _p, _u64, _p, _d]),
+        "orc_loss_backward": (C.c_int, [_p, _u64, _u32, _d, _d, _p, _u64, _p, _d, _p, _p, _p, _p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -275,6 +277,31 @@ def reconstruct(pts6, depth=8, scale=1.1, cg_accuracy=1e-3, cg_iters=500, point_
     v, t = _take_mesh(m)
     stats = {f: getattr(st, f) for f, _ in OrcStats._fields_}
     return v, t, stats, coeffs
+
+
+# ------------------------------------------------------------------ adjoint
+def loss(pts6, queries3, depth, point_weight=4.0, scale=1.1, dl_dchi=None, tol=1e-13):
+    """L = mean chi(q)^2 (or sum g_k chi(q_k) with g = dl_dchi) after a converged FP64 solve;
+    the unit-cube transform follows the points' bbox (keep perturbations off its extremes)."""
+    pts6 = _f64(pts6, (-1, 6))
+    q = _f64(queries3, (-1, 3))
+    g = None if dl_dchi is None else _f64(dl_dchi)
+    return lib().orc_loss(_ptr(pts6), pts6.shape[0], int(depth), float(point_weight), float(scale), _ptr(q),
+                          q.shape[0], _ptr(g), float(tol))
+
+
+def loss_backward(pts6, queries3, depth, point_weight=4.0, scale=1.1, dl_dchi=None, tol=1e-13):
+    """(chi, dL/dpositions, dL/dnormals, L) in model space, the transform held fixed."""
+    pts6 = _f64(pts6, (-1, 6))
+    q = _f64(queries3, (-1, 3))
+    g = None if dl_dchi is None else _f64(dl_dchi)
+    n, k = pts6.shape[0], q.shape[0]
+    chi, dp, dn, L = np.zeros(k), np.zeros((n, 3)), np.zeros((n, 3)), C.c_double()
+    rc = lib().orc_loss_backward(_ptr(pts6), n, int(depth), float(point_weight), float(scale), _ptr(q), k, _ptr(g),
+                                 float(tol), _ptr(chi), _ptr(dp), _ptr(dn), C.byref(L))
+    if rc != 0:
+        raise ValueError("orc_loss_backward: empty input")
+    return chi, dp, dn, L.value
 
 
 # ------------------------------------------------------------------ generic CSR

@@ -877,4 +877,223 @@ int orc_reconstruct(const double* pts6, uint64_t n, const orc_params* p, orc_mes
   return 0;
 }
 
+// ---------------------------------------------------------------- adjoint (no reference counterpart)
+// Gradient of a loss on the implicit function at K query points.  chi_k = evaluate(x, M q_k)
+// (q_k in model space, M the unit-cube transform of the input, held fixed: the bbox is not
+// differentiated).  Upstream g_k = dL/dchi_k; with g = NULL the loss is L = mean_k chi_k^2
+// and g_k = 2 chi_k / K.  With A x = b (A symmetric) the adjoint is A lambda = E^T g, and
+//   dL/dtheta = lambda . (db/dtheta) - lambda . (dA/dtheta) x.
+// b = G nf + screening RHS, nf_j = -(sum_i phi_j(u_i) nu_i) / w_j, w_j = sum_i phi_j(u_i)
+// (splat, floor cells, src/fem_tree.rs:130-178; divergence stencil G, :251-274; screening
+// RHS and matrix on trunc cells, :276-297 and :220-228).
+
+// CG from x = 0 until ||b - A x|| <= tol ||b|| (explicit residual every 50 iterations).
+static uint64_t cg_to_tol(const Csr& A, const double* b, double* x, double tol, uint64_t maxit) {
+  const uint64_t n = A.rows;
+  std::vector<double> r(b, b + n), d(b, b + n), q(n);
+  std::fill(x, x + n, 0.0);
+  const double bb = det_dot(b, b, n);
+  if (bb == 0.0) return 0;
+  double rr = bb;
+  uint64_t it = 0;
+  while (it < maxit && rr > tol * tol * bb) {
+    A.spmv(d.data(), q.data());
+    const double dq = det_dot(d.data(), q.data(), n);
+    if (dq == 0.0) break;
+    const double alpha = rr / dq;
+    for (uint64_t i = 0; i < n; ++i) x[i] += alpha * d[i];
+    ++it;
+    if (it % 50 == 0) {
+      A.spmv(x, q.data());
+      for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+    } else {
+      for (uint64_t i = 0; i < n; ++i) r[i] -= alpha * q[i];
+    }
+    const double rr_new = det_dot(r.data(), r.data(), n);
+    const double beta = rr_new / rr;
+    rr = rr_new;
+    for (uint64_t i = 0; i < n; ++i) d[i] = r[i] + beta * d[i];
+  }
+  return it;
+}
+
+// Trilinear basis of one corner: value and gradient in unit-cube coordinates.  t: in-cell
+// coordinates; d: corner offsets; inv_h = 1/h.
+static inline void corner_basis(const double t[3], const int d[3], double inv_h, double& phi, double g[3]) {
+  double b[3], db[3];
+  for (int a = 0; a < 3; ++a) {
+    b[a] = d[a] ? t[a] : 1.0 - t[a];
+    db[a] = d[a] ? inv_h : -inv_h;
+  }
+  phi = b[0] * b[1] * b[2];
+  g[0] = db[0] * b[1] * b[2];
+  g[1] = b[0] * db[1] * b[2];
+  g[2] = b[0] * b[1] * db[2];
+}
+
+// Shared forward: transform, tree, converged solve of A x = b, chi at the queries.
+struct AdjFwd {
+  double M[16];
+  std::vector<double> unit;
+  orc_tree* t = nullptr;
+  std::vector<double> x, qu;
+  ~AdjFwd() { if (t) orc_tree_free(t); }
+};
+static void adj_forward(AdjFwd& f, const double* pts6, uint64_t n, uint32_t depth, double pw, double scale,
+                        const double* q3, uint64_t k, double tol, double* chi) {
+  double bmin[3], bmax[3];
+  orc_bbox(pts6, n, bmin, bmax);
+  orc_unit_cube_transform(bmin, bmax, scale, f.M);
+  f.unit.resize(6 * n);
+  orc_transform_points(f.M, pts6, n, f.unit.data());
+  f.t = orc_tree_new(depth, f.unit.data(), n);
+  orc_tree_assemble(f.t, pw);
+  std::vector<double> b(f.t->n);
+  orc_tree_rhs(f.t, pw, b.data());
+  f.x.assign(f.t->n, 0.0);
+  cg_to_tol(f.t->A, b.data(), f.x.data(), tol, 100000);
+  f.qu.resize(3 * k);
+  for (uint64_t i = 0; i < k; ++i) orc_transform_point(f.M, q3 + 3 * i, &f.qu[3 * i]);
+  orc_evaluate_many(depth, f.x.data(), f.qu.data(), 3, k, chi);
+}
+
+// Loss only (for finite differences): mean chi^2, or sum g_k chi_k when g is given.
+double orc_loss(const double* pts6, uint64_t n, uint32_t depth, double pw, double scale, const double* q3, uint64_t k,
+                const double* g, double tol) {
+  AdjFwd f;
+  std::vector<double> chi(k);
+  adj_forward(f, pts6, n, depth, pw, scale, q3, k, tol, chi.data());
+  double L = 0.0;
+  for (uint64_t i = 0; i < k; ++i) L += g ? g[i] * chi[i] : chi[i] * chi[i];
+  return g ? L : L / (double)k;
+}
+
+// Gradients w.r.t. the model-space positions and normals of the input (n x 3 each).
+int orc_loss_backward(const double* pts6, uint64_t n, uint32_t depth, double pw, double scale, const double* q3,
+                      uint64_t k, const double* dl_dchi, double tol, double* chi, double* dpos, double* dnrm,
+                      double* loss) {
+  if (n == 0 || k == 0) return -1;
+  AdjFwd f;
+  adj_forward(f, pts6, n, depth, pw, scale, q3, k, tol, chi);
+  orc_tree* t = f.t;
+  const isize res = (isize)t->res;
+  const double h = t->h, inv_h = 1.0 / h;
+  std::vector<double> g(k);
+  double L = 0.0;
+  for (uint64_t i = 0; i < k; ++i) {
+    g[i] = dl_dchi ? dl_dchi[i] : 2.0 * chi[i] / (double)k;
+    L += dl_dchi ? dl_dchi[i] * chi[i] : chi[i] * chi[i];
+  }
+  if (loss) *loss = dl_dchi ? L : L / (double)k;
+  // E^T g: the transpose of evaluate's shifted trilinear basis (src/fem_tree.rs:490-513)
+  std::vector<double> rhs(t->n, 0.0);
+  for (uint64_t i = 0; i < k; ++i) {
+    const double s[3] = {f.qu[3 * i] / h, f.qu[3 * i + 1] / h, f.qu[3 * i + 2] / h};
+    uint32_t o[3][2];
+    double bs[3][2];
+    for (int a = 0; a < 3; ++a) {
+      contributing_offsets(s[a], res, o[a][0], o[a][1]);
+      bs[a][0] = bspline1(s[a] - (double)o[a][0]);
+      bs[a][1] = bspline1(s[a] - (double)o[a][1]);
+    }
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 2; ++c)
+          rhs[morton(o[0][a], o[1][b], o[2][c])] += g[i] * bs[0][a] * bs[1][b] * bs[2][c];
+  }
+  std::vector<double> lam(t->n, 0.0);
+  cg_to_tol(t->A, rhs.data(), lam.data(), tol, 100000);
+  // mu_j = dL/dnf_j = G^T lambda at nodes with a splat weight
+  std::vector<double> mu(3 * t->n, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)t->n; ++j) {
+    if (!(t->nw[j] > 0.0)) continue;
+    uint64_t jx, jy, jz;
+    unmorton((uint64_t)j, jx, jy, jz);
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+    for (isize dx = -1; dx <= 1; ++dx)
+      for (isize dy = -1; dy <= 1; ++dy)
+        for (isize dz = -1; dz <= 1; ++dz) {
+          // row i = j - d sees node j at offset d
+          const isize ix = (isize)jx - dx, iy = (isize)jy - dy, iz = (isize)jz - dz;
+          if (ix < 0 || iy < 0 || iz < 0 || ix >= res || iy >= res || iz >= res) continue;
+          const double l = lam[morton(ix, iy, iz)] * h * h;
+          m0 += l * deriv_mass_1d(dx) * mass_1d(dy) * mass_1d(dz);
+          m1 += l * mass_1d(dx) * deriv_mass_1d(dy) * mass_1d(dz);
+          m2 += l * mass_1d(dx) * mass_1d(dy) * deriv_mass_1d(dz);
+        }
+    mu[3 * j] = m0;
+    mu[3 * j + 1] = m1;
+    mu[3 * j + 2] = m2;
+  }
+  const double wh3 = pw > 0.0 ? pw * (h * h * h) / 1.5 : 0.0;
+  const double s_m = f.M[0];
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < (int64_t)n; ++p) {
+    const double* u = &f.unit[6 * p];
+    const double nu[3] = {u[3], u[4], u[5]};
+    double gu[3] = {0, 0, 0}, gn[3] = {0, 0, 0};
+    {  // splat (floor cells)
+      isize c[3];
+      double tt[3];
+      for (int a = 0; a < 3; ++a) {
+        c[a] = f64_to_isize(std::floor(u[a] / h));
+        tt[a] = u[a] / h - (double)c[a];
+      }
+      for (int kk = 0; kk < 8; ++kk) {
+        const int d[3] = {kk & 1, (kk >> 1) & 1, kk >> 2};
+        const uint64_t ox = (uint64_t)(c[0] + d[0]), oy = (uint64_t)(c[1] + d[1]), oz = (uint64_t)(c[2] + d[2]);
+        if (ox >= t->res || oy >= t->res || oz >= t->res) continue;
+        const uint64_t j = morton(ox, oy, oz);
+        const double w = t->nw[j];
+        if (!(w > 0.0)) continue;
+        double phi, gp[3];
+        corner_basis(tt, d, inv_h, phi, gp);
+        const double* m = &mu[3 * j];
+        const double* nf = &t->nf[3 * j];
+        const double sdot = m[0] * (nu[0] + nf[0]) + m[1] * (nu[1] + nf[1]) + m[2] * (nu[2] + nf[2]);
+        for (int a = 0; a < 3; ++a) {
+          gn[a] -= phi / w * m[a];
+          gu[a] -= gp[a] / w * sdot;
+        }
+      }
+    }
+    if (pw > 0.0) {  // screening RHS and matrix (trunc cells)
+      isize c[3];
+      double tt[3];
+      for (int a = 0; a < 3; ++a) {
+        c[a] = f64_to_isize(u[a] / h);
+        tt[a] = u[a] / h - (double)c[a];
+      }
+      double Lv = 0.0, Xv = 0.0, gL[3] = {0, 0, 0}, gX[3] = {0, 0, 0};
+      for (int kk = 0; kk < 8; ++kk) {
+        const int d[3] = {kk & 1, (kk >> 1) & 1, kk >> 2};
+        const uint32_t ox = (uint32_t)(uint64_t)(c[0] + d[0]), oy = (uint32_t)(uint64_t)(c[1] + d[1]),
+                       oz = (uint32_t)(uint64_t)(c[2] + d[2]);
+        if (ox >= (uint32_t)t->res || oy >= (uint32_t)t->res || oz >= (uint32_t)t->res) continue;
+        const uint64_t j = morton(ox, oy, oz);
+        double phi, gp[3];
+        corner_basis(tt, d, inv_h, phi, gp);
+        Lv += phi * lam[j];
+        Xv += phi * f.x[j];
+        for (int a = 0; a < 3; ++a) {
+          gL[a] += gp[a] * lam[j];
+          gX[a] += gp[a] * f.x[j];
+        }
+      }
+      for (int a = 0; a < 3; ++a) gu[a] += wh3 * 0.5 * gL[a] - wh3 * (gL[a] * Xv + Lv * gX[a]);
+    }
+    // model space: u = s p + c (transform held fixed); nu = v/|v|, v = s n
+    const double* pm = pts6 + 6 * p;
+    const double v[3] = {s_m * pm[3], s_m * pm[4], s_m * pm[5]};
+    const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double ng = nu[0] * gn[0] + nu[1] * gn[1] + nu[2] * gn[2];
+    for (int a = 0; a < 3; ++a) {
+      dpos[3 * p + a] = s_m * gu[a];
+      dnrm[3 * p + a] = len > 0.0 ? s_m / len * (gn[a] - nu[a] * ng) : 0.0;
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"

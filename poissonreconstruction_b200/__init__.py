@@ -57,6 +57,12 @@ class PrStats(C.Structure):
                 ("reserved_i", C.c_int32), ("reserved", C.c_double * 5)]
 
 
+class PrAdjointStats(C.Structure):
+    _fields_ = [("loss", C.c_double), ("rel_residual", C.c_double), ("pcg_iterations", C.c_uint32),
+                ("refinement_steps", C.c_uint32), ("converged", C.c_int32), ("reserved_i", C.c_int32),
+                ("time_solve", C.c_double), ("time_total", C.c_double), ("reserved", C.c_double * 4)]
+
+
 # Every C-ABI entry point and its signature (checked against include/poisson_recon.h by the tests).
 _P = C.c_void_p
 SIGNATURES = {
@@ -89,6 +95,10 @@ SIGNATURES = {
     "pr_ctx_evaluate": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "pr_ctx_extract": (C.c_int, [_P, _P, C.c_double, C.POINTER(PrMesh)]),
     "pr_ctx_extract_at_depth": (C.c_int, [_P, C.c_uint32, _P, C.c_double, C.POINTER(PrMesh)]),
+    "pr_ctx_solve": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrStats)]),
+    "pr_ctx_loss_backward": (C.c_int, [_P, _P, C.c_uint64, _P, _P, _P, _P, C.POINTER(PrAdjointStats)]),
+    "pr_loss_backward": (C.c_int, [_P, C.c_uint64, C.POINTER(PrParams), _P, C.c_uint64, _P, _P, _P, _P,
+                                   C.POINTER(PrAdjointStats)]),
 }
 
 _LIB = None
@@ -229,6 +239,46 @@ def reconstruct(points, params=None):
     return _take_mesh(m), ReconstructStats.from_c(s)
 
 
+@dataclasses.dataclass
+class AdjointStats:
+    loss: float = 0.0
+    rel_residual: float = 0.0
+    pcg_iterations: int = 0
+    refinement_steps: int = 0
+    converged: int = 0
+    time_solve: float = 0.0
+    time_total: float = 0.0
+
+    @classmethod
+    def from_c(cls, s):
+        return cls(**{f.name: getattr(s, f.name) for f in dataclasses.fields(cls)})
+
+
+def _queries(queries, dl_dchi):
+    q = np.ascontiguousarray(queries, dtype=np.float64)
+    if q.ndim != 2 or q.shape[1] != 3:
+        raise ValueError("queries must be a (K, 3) array")
+    g = None
+    if dl_dchi is not None:
+        g = np.ascontiguousarray(dl_dchi, dtype=np.float64).reshape(-1)
+        if g.shape[0] != q.shape[0]:
+            raise ValueError("dl_dchi must have one entry per query")
+    return q, g
+
+
+def loss_backward(points, queries, params=None, dl_dchi=None):
+    """Solve, then differentiate chi at model-space `queries` (no counterpart in the reference).
+    Returns (chi, dL/dpositions, dL/dnormals, AdjointStats); with dl_dchi None, L = mean chi^2."""
+    params = params or ReconstructParams()
+    pts = _points(points)
+    q, g = _queries(queries, dl_dchi)
+    chi, dp, dn = np.zeros(q.shape[0]), np.zeros((pts.shape[0], 3)), np.zeros((pts.shape[0], 3))
+    p, s = params.to_c(), PrAdjointStats()
+    _check(lib().pr_loss_backward(_ptr(pts), pts.shape[0], C.byref(p), _ptr(q), q.shape[0], _ptr(g), _ptr(chi),
+                                  _ptr(dp), _ptr(dn), C.byref(s)))
+    return chi, dp, dn, AdjointStats.from_c(s)
+
+
 class Context:
     """A device context: owns a CUDA stream (or uses the one given) and the buffers of the
     last reconstruction, whose intermediate state the accessors read."""
@@ -261,7 +311,29 @@ class Context:
         pts = _points(points)
         p, m, s = params.to_c(), PrMesh(), PrStats()
         _check(lib().pr_ctx_reconstruct(self._h, _ptr(pts), pts.shape[0], C.byref(p), C.byref(m), C.byref(s)))
+        self._n_points = pts.shape[0]
         return _take_mesh(m), ReconstructStats.from_c(s)
+
+    def solve(self, points, params=None):
+        """Transform, splat, RHS and solve without marching cubes (state kept for the adjoint)."""
+        params = params or ReconstructParams()
+        pts = _points(points)
+        p, s = params.to_c(), PrStats()
+        _check(lib().pr_ctx_solve(self._h, _ptr(pts), pts.shape[0], C.byref(p), C.byref(s)))
+        self._n_points = pts.shape[0]
+        return ReconstructStats.from_c(s)
+
+    def loss_backward(self, queries, dl_dchi=None, n_points=None):
+        """Gradients of the last solve w.r.t. its points: (chi, dL/dpositions, dL/dnormals, stats)."""
+        q, g = _queries(queries, dl_dchi)
+        n = n_points if n_points is not None else getattr(self, "_n_points", None)
+        if n is None:
+            raise ValueError("n_points unknown: pass the point count of the last solve")
+        chi, dp, dn = np.zeros(q.shape[0]), np.zeros((n, 3)), np.zeros((n, 3))
+        s = PrAdjointStats()
+        _check(lib().pr_ctx_loss_backward(self._h, _ptr(q), q.shape[0], _ptr(g), _ptr(chi), _ptr(dp), _ptr(dn),
+                                          C.byref(s)))
+        return chi, dp, dn, AdjointStats.from_c(s)
 
     def reconstruct_device(self, d_points_ptr, n, params=None):
         """Input already on the device (pointer to n x 6 float64); the mesh stays there."""

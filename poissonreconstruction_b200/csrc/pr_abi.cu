@@ -124,7 +124,8 @@ void copy_mesh_to_host(pr_context* c, pr_mesh* out) {
 }
 
 // The pipeline on device-resident points (c->buf "pts6" or caller memory).
-void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_params& p, pr_stats& st, double t_start) {
+void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_params& p, pr_stats& st, double t_start,
+                  bool extract = true) {
   double t0 = now_s();
   pr::stage_transform(c, d_pts6, n, p.scale);
   c->sync();
@@ -137,11 +138,15 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   st.time_system = 0.0;
   st.fem_nodes = c->n;
   st.points_in_cube = c->P_in;
+  c->params = p;
   if (p.solve_mode == PR_SOLVE_REFERENCE_SCHEDULE) pr::stage_solve_reference(c, p, st);
   else pr::stage_solve(c, p, st);
+  c->coeffs_converged = p.solve_mode != PR_SOLVE_REFERENCE_SCHEDULE;
   c->sync();
   double t3 = now_s();
   st.time_solve = t3 - t2;
+  st.peak_device_bytes = (double)c->peak_bytes;
+  if (!extract) return;
   const double* x = c->get<double>("x64");
   double iso = pr::stage_iso(c, x);
   pr::stage_extract(c, c->D, x, iso, true);
@@ -162,7 +167,7 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
 }
 
 void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr_params* params, bool device_input,
-                      pr_mesh* out_mesh, pr_stats* out_stats) {
+                      pr_mesh* out_mesh, pr_stats* out_stats, bool extract = true) {
   double t_start = now_s();
   validate(params);
   PR_REQUIRE(n == 0 || points6 != nullptr, PR_ERR_INVALID_ARGUMENT, "points is NULL");
@@ -173,6 +178,7 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
   c->have_state = false;
   c->have_mesh = false;
   c->have_coeffs = false;
+  c->coeffs_converged = false;
   c->nv = c->nt = 0;
   if (out_mesh) std::memset(out_mesh, 0, sizeof(*out_mesh));
   if (n == 0) {  // src/reconstructor.rs:28
@@ -186,8 +192,8 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
     PR_CUDA(cudaMemcpyAsync(dp, points6, 6 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     d_pts = dp;
   }
-  run_pipeline(c, d_pts, n, *params, st, t_start);
-  if (out_mesh) copy_mesh_to_host(c, out_mesh);
+  run_pipeline(c, d_pts, n, *params, st, t_start, extract);
+  if (out_mesh && extract) copy_mesh_to_host(c, out_mesh);
   st.time_total = now_s() - t_start;
   if (out_stats) *out_stats = st;
 }
@@ -347,6 +353,78 @@ int pr_reconstruct(const double* points6, uint64_t n, const pr_params* params, p
       g_thread_ctx.reset(c);
     }
     reconstruct_impl(g_thread_ctx.get(), points6, n, params, false, out_mesh, out_stats);
+  });
+}
+
+int pr_ctx_solve(pr_context* c, const double* points6, uint64_t n, const pr_params* params, pr_stats* out_stats) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    reconstruct_impl(c, points6, n, params, false, nullptr, out_stats, false);
+  });
+}
+
+static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k, const double* dl_dchi, double* chi,
+                               double* dl_dpositions, double* dl_dnormals, pr_adjoint_stats* out_stats) {
+  const double t_start = now_s();
+  PR_REQUIRE(queries3 != nullptr, PR_ERR_INVALID_ARGUMENT, "queries is NULL");
+  PR_REQUIRE(k >= 1 && k <= pr::kMaxPoints, PR_ERR_INVALID_ARGUMENT, "k must be in [1, 2^28] query points");
+  PR_REQUIRE(c->have_state && c->have_coeffs, PR_ERR_STATE, "no solved reconstruction on this context");
+  PR_REQUIRE(c->coeffs_converged, PR_ERR_STATE,
+             "the last solve used the reference schedule; the adjoint needs solve_mode PR_SOLVE_CONVERGED");
+  for (uint64_t i = 0; i < 3 * k; ++i)
+    PR_REQUIRE(std::isfinite(queries3[i]), PR_ERR_INVALID_ARGUMENT, "non-finite query coordinate");
+  set_device(c);
+  pr_adjoint_stats st;
+  std::memset(&st, 0, sizeof(st));
+  double* dq = c->buf<double>("adj_q3", 3 * k);
+  PR_CUDA(cudaMemcpyAsync(dq, queries3, 3 * k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  double* ddl = nullptr;
+  if (dl_dchi) {
+    ddl = c->buf<double>("adj_dl", k);
+    PR_CUDA(cudaMemcpyAsync(ddl, dl_dchi, k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  double* dchi = c->buf<double>("adj_chi", k);
+  double* dpos = c->buf<double>("adj_dpos", 3 * c->P);
+  double* dnrm = c->buf<double>("adj_dnrm", 3 * c->P);
+  pr::adjoint_backward(c, dq, k, ddl, dchi, dpos, dnrm, st);
+  if (chi) PR_CUDA(cudaMemcpyAsync(chi, dchi, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (dl_dpositions)
+    PR_CUDA(cudaMemcpyAsync(dl_dpositions, dpos, 3 * c->P * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (dl_dnormals)
+    PR_CUDA(cudaMemcpyAsync(dl_dnormals, dnrm, 3 * c->P * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  c->sync();
+  st.time_total = now_s() - t_start;
+  if (out_stats) *out_stats = st;
+  if (!st.converged)
+    throw pr::Error(PR_ERR_NOT_CONVERGED, "adjoint solve stopped at relative residual " +
+                                              std::to_string(st.rel_residual) + " (outputs hold the last iterate)");
+}
+
+int pr_ctx_loss_backward(pr_context* c, const double* queries3, uint64_t k, const double* dl_dchi, double* chi,
+                         double* dl_dpositions, double* dl_dnormals, pr_adjoint_stats* out_stats) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    loss_backward_impl(c, queries3, k, dl_dchi, chi, dl_dpositions, dl_dnormals, out_stats);
+  });
+}
+
+int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params, const double* queries3, uint64_t k,
+                     const double* dl_dchi, double* chi, double* dl_dpositions, double* dl_dnormals,
+                     pr_adjoint_stats* out_stats) {
+  return guard([&] {
+    validate(params);
+    PR_REQUIRE(n >= 1 && points6 != nullptr, PR_ERR_INVALID_ARGUMENT, "the adjoint needs at least one point");
+    PR_REQUIRE(params->solve_mode == PR_SOLVE_CONVERGED, PR_ERR_INVALID_ARGUMENT,
+               "the adjoint needs solve_mode PR_SOLVE_CONVERGED");
+    if (!g_thread_ctx) {
+      pr_context* c = nullptr;
+      int rc = pr_context_create(0, nullptr, &c);
+      if (rc != PR_OK) throw pr::Error(rc, g_last_error);
+      g_thread_ctx.reset(c);
+    }
+    pr_context* c = g_thread_ctx.get();
+    reconstruct_impl(c, points6, n, params, false, nullptr, nullptr, false);
+    loss_backward_impl(c, queries3, k, dl_dchi, chi, dl_dpositions, dl_dnormals, out_stats);
   });
 }
 

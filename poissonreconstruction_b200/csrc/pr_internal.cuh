@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -134,6 +135,8 @@ struct pr_context {
   bool have_mesh = false;
   uint64_t nv = 0, nt = 0;
   bool have_coeffs = false;
+  bool coeffs_converged = false;  // x64 solves A x = b (converged mode), not the reference schedule
+  pr_params params{};             // parameters of the last reconstruction
 
   template <typename T>
   T* buf(const std::string& name, size_t count) {
@@ -185,8 +188,15 @@ namespace pr {
 // setup (pr_setup.cu)
 void stage_transform(pr_context* c, const double* d_pts6, uint64_t n, double scale);
 void stage_splat_rhs(pr_context* c, uint32_t depth, double pw);
+// Stable sort of m (key, value) pairs by key (keys < 2^(3D+1)) and run-length encoding into
+// the buffers tag_key/_val/_runkey/_runoff; the run of key 2^(3D) (sentinel) is dropped.
+// Returns the number of valid runs.
+uint64_t sort_and_segment(pr_context* c, const std::string& tag, uint32_t* keys_in, uint32_t* vals_in, uint64_t m,
+                          uint32_t D);
 // solve (pr_solve.cu): fills "x64"; returns rel residual etc. in stats
 void stage_solve(pr_context* c, const pr_params& p, pr_stats& st);
+// A x = b with the current system's operator (x = 0 initially; b, x: n doubles)
+void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double* b, double* x);
 // extract (pr_mc.cu)
 double stage_iso(pr_context* c, const double* d_x64);
 void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform);
@@ -201,5 +211,13 @@ void apply_operator32(pr_context* c, const float* d_x, float* d_y);
 void scatter_normal_field(pr_context* c, double* d_nf3, double* d_w);
 
 double dot64(pr_context* c, const double* a, const double* b, uint64_t n);
+
+// adjoint (pr_adjoint.cu): gradients of a loss on chi at model-space queries (device arrays)
+void adjoint_backward(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
+                      double* d_dpos, double* d_dnrm, pr_adjoint_stats& st);
+
+inline double now_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 }  // namespace pr

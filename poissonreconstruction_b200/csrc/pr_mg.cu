@@ -602,7 +602,7 @@ __device__ __forceinline__ void neighbour_bases(uint32_t* nb, uint32_t bx, uint3
 }
 
 // Coarse tile for the prolongation: coarse block (8^3, Morton-contiguous) with a one-node
-// halo, natural layout 10^3, coordinate = coarse local + 1.
+// halo, natural layout 10^3, coordinate = coarse local + 1.  Ends with a barrier.
 template <typename T>
 __device__ __forceinline__ void load_coarse_tile(T* ctile, const T* __restrict__ ec, uint32_t blk, uint32_t bx,
                                                  uint32_t by, uint32_t bz, int nblk_axis, uint32_t* cnb) {
@@ -650,6 +650,7 @@ __device__ __forceinline__ void load_coarse_tile(T* ctile, const T* __restrict__
     const uint32_t b0 = cnb[nbi];
     ctile[(uz * CW + uy) * CW + ux] = b0 != ~0u ? __ldg(ec + b0 + mloc) : (T)0;
   }
+  __syncthreads();  // the caller reads halo entries written by other threads
 }
 
 // P ec at fine tile coordinate (ux,uy,uz) (fine local + 1); ctile coordinate = coarse local + 1.
@@ -696,7 +697,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_smooth16(uint32_t D, const T* __
   const int t = threadIdx.x;
   if (MODE != 1) neighbour_bases(nb, bx, by, bz, res >> 4);
   else if (t < 27) nb[t] = ~0u;  // zero halo
-  if (MODE == 2) load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // contains a barrier
+  if (MODE == 2) load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // ends with a barrier
   else __syncthreads();  // nb
   // interior: 4 quads per thread; quad element e at tile offset qoff[e] from element 0
   int tq[4];  // tile index of each quad's element 0

@@ -86,7 +86,7 @@ struct Mat16 {
 
 // Mat4::transform_point + transform_vector + Vec3::normalize (src/reconstructor.rs:36-40)
 __global__ void k_transform(const double* __restrict__ pts6, uint64_t n, Mat16 M, double* __restrict__ upos,
-                            double* __restrict__ unrm) {
+                            double* __restrict__ unrm, double* __restrict__ ulen) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const double* p = pts6 + 6 * i;
     double v[3];
@@ -99,6 +99,7 @@ __global__ void k_transform(const double* __restrict__ pts6, uint64_t n, Mat16 M
     double nn = __dsqrt_rn(xadd(xadd(xmul(v[0], v[0]), xmul(v[1], v[1])), xmul(v[2], v[2])));
 #pragma unroll
     for (int r = 0; r < 3; ++r) unrm[r * n + i] = nn > 0.0 ? xdiv(v[r], nn) : 0.0;
+    ulen[i] = nn;  // |M n|, for the derivative of the normalisation
   }
 }
 
@@ -332,6 +333,8 @@ __global__ void k_scatter_nf(const uint32_t* __restrict__ run_key, uint64_t T, c
   }
 }
 
+}  // namespace
+
 // Sort 8P (key, pair) entries by key (stable) and run-length encode the keys.  Outputs:
 // sorted keys/vals, the distinct valid keys (`run_key`, length R) and their segment offsets
 // `run_off` (R+1).  Returns R.
@@ -369,8 +372,6 @@ uint64_t sort_and_segment(pr_context* c, const std::string& tag, uint32_t* keys_
   PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, run_cnt, run_off, (int64_t)(R + 1), c->stream));
   return R;
 }
-
-}  // namespace
 
 // ------------------------------------------------------------------ stage: transform
 void stage_transform(pr_context* c, const double* d_pts6, uint64_t P, double scale) {
@@ -438,7 +439,8 @@ void stage_transform(pr_context* c, const double* d_pts6, uint64_t P, double sca
   for (int k = 0; k < 16; ++k) m16.m[k] = M[k];
   double* upos = c->buf<double>("upos", 3 * P);
   double* unrm = c->buf<double>("unrm", 3 * P);
-  k_transform<<<grid_for(P), kThreads, 0, c->stream>>>(d_pts6, P, m16, upos, unrm);
+  double* ulen = c->buf<double>("ulen", P);
+  k_transform<<<grid_for(P), kThreads, 0, c->stream>>>(d_pts6, P, m16, upos, unrm, ulen);
   PR_CHECK_LAUNCH();
   c->P = P;
   c->have_points = true;

@@ -300,13 +300,18 @@ double vcycle_bytes(uint32_t D, double es, int sweeps) {
 }  // namespace
 
 void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
+  double* xA = c->buf<double>("x64", c->n);
+  solve_system(c, p, st, c->get<double>("b64"), xA);
+  c->have_coeffs = true;
+}
+
+// A x = b on the current system (the fine operator of the last setup), x = 0 initially.
+void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double* b, double* xA) {
   const uint64_t n = c->n;
   const uint32_t D = c->D;
   cudaStream_t s = c->stream;
   const double h = 1.0 / (double)(1u << D);
   const double wg = c->pw > 0.0 ? (c->pw * (h * h * h) / 1.5) * 0.005 : 0.0;
-  const double* b = c->get<double>("b64");
-  double* xA = c->buf<double>("x64", n);
   double* xB = c->buf<double>("x64b", n);
   double* r = c->buf<double>("r64", n);
   const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;
@@ -322,7 +327,6 @@ void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
   if (bn == 0.0) {
     st.rel_residual = 0.0;
     st.converged = 1;
-    c->have_coeffs = true;
     return;
   }
   FineOp<double> A64 = make_fine_op<double>(c, wg);
@@ -403,7 +407,6 @@ void stage_solve(pr_context* c, const pr_params& p, pr_stats& st) {
   st.pcg_iterations = (uint32_t)used;
   st.rel_residual = rn / bn;
   st.converged = st.rel_residual <= target ? 1 : 0;
-  c->have_coeffs = true;
 }
 
 // ------------------------------------------------------------------ operator access for tests

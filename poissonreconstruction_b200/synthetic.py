@@ -87,3 +87,59 @@ WORKLOADS = {
     "sphere_100k": dict(fn=sphere, depth=8, point_weight=4.0),
     "torus_2m": dict(fn=torus, depth=10, point_weight=4.0),
 }
+
+
+def _spow(x, e):
+    return np.sign(x) * np.abs(x) ** e
+
+
+def _superquadric_surface(u, v, e1, e2, axes):
+    a, b, c = axes
+    cv, sv, cu, su = np.cos(v), np.sin(v), np.cos(u), np.sin(u)
+    pos = np.stack([a * _spow(cv, e1) * _spow(cu, e2), b * _spow(cv, e1) * _spow(su, e2), c * _spow(sv, e1)], axis=1)
+    nrm = np.stack([_spow(cv, 2 - e1) * _spow(cu, 2 - e2) / a, _spow(cv, 2 - e1) * _spow(su, 2 - e2) / b,
+                    _spow(sv, 2 - e1) / c], axis=1)
+    ln = np.linalg.norm(nrm, axis=1, keepdims=True)
+    return pos, nrm / np.where(ln > 0, ln, 1.0)
+
+
+def _superquadric_params(rng, n, e1, e2, axes, nu=2048, nv=1024):
+    """(u, v) with density proportional to surface area: a parameter cell of an nu x nv grid
+    is drawn with probability equal to its share of the area (two triangles of the mapped
+    cell), then (u, v) uniform inside the cell.  The area element itself is unbounded on the
+    singular parameter lines of a superquadric with exponents below 1, so plain rejection
+    against its maximum does not work."""
+    ue = np.linspace(-np.pi, np.pi, nu + 1)
+    ve = np.linspace(-np.pi / 2, np.pi / 2, nv + 1)
+    gu, gv = np.meshgrid(ue, ve, indexing="ij")
+    pg = _superquadric_surface(gu.ravel(), gv.ravel(), e1, e2, axes)[0].reshape(nu + 1, nv + 1, 3)
+    p00, p10, p01, p11 = pg[:-1, :-1], pg[1:, :-1], pg[:-1, 1:], pg[1:, 1:]
+    area = 0.5 * (np.linalg.norm(np.cross(p10 - p00, p01 - p00), axis=2) +
+                  np.linalg.norm(np.cross(p10 - p11, p01 - p11), axis=2))
+    cdf = np.cumsum(area.ravel())
+    cell = np.minimum(np.searchsorted(cdf, rng.uniform(0, cdf[-1], n), side="right"), cdf.size - 1)
+    iu, iv = cell // nv, cell % nv
+    u = ue[iu] + (ue[1] - ue[0]) * rng.uniform(0, 1, n)
+    v = ve[iv] + (ve[1] - ve[0]) * rng.uniform(0, 1, n)
+    return u, v
+
+
+def superquadric(n=1_000_000, seed=SEED_BASE + 3, e1=0.5, e2=0.8, axes=(1.0, 0.7, 0.5), max_tilt_deg=20.0,
+                 fp32=True):
+    """Superquadric samples (area-weighted parameter cells), analytic normals tilted by an angle uniform in
+    [0, max_tilt_deg] about a random tangent axis; FP32-rounded."""
+    rng = _rng(seed)
+    u, v = _superquadric_params(rng, n, e1, e2, axes)
+    pos, nrm = _superquadric_surface(u, v, e1, e2, axes)
+    nrm = _tangent_rotate(rng, nrm, np.deg2rad(max_tilt_deg) * rng.uniform(0, 1, n))
+    out = np.hstack([pos, nrm])
+    if fp32:
+        out = out.astype(np.float32).astype(np.float64)
+    return np.ascontiguousarray(out)
+
+
+def superquadric_queries(k=200_000, seed=SEED_BASE + 103, e1=0.5, e2=0.8, axes=(1.0, 0.7, 0.5)):
+    """Query points on the true superquadric surface (a seed of their own)."""
+    rng = _rng(seed)
+    u, v = _superquadric_params(rng, k, e1, e2, axes)
+    return np.ascontiguousarray(_superquadric_surface(u, v, e1, e2, axes)[0])

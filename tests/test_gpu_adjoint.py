@@ -1,0 +1,160 @@
+"""Adjoint (gradients of a loss on the implicit function) on the GPU, through the C ABI:
+against the FP64 CPU oracle's adjoint, against finite differences of the GPU forward, and
+through the torch.autograd bridge.  No counterpart in the reference crate; the forward it
+differentiates is src/fem_tree.rs:130-299 and :490-513."""
+import numpy as np
+import pytest
+
+import oracle
+import poissonreconstruction_b200 as prb
+from poissonreconstruction_b200 import synthetic
+from tests.adjoint_cases import adjoint_case, fd_coordinates, fd_gradient
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(depth, fp64=True, target=1e-12):
+    return prb.ReconstructParams(depth=depth, point_weight=4.0,
+                                 precision=prb.PR_PRECISION_FP64 if fp64 else prb.PR_PRECISION_MIXED,
+                                 target_rel_residual=target, max_iters=400)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("depth", [4, 5, 6])
+@pytest.mark.parametrize("upstream", [False, True])
+def test_adjoint_matches_oracle_fp64(ctx, depth, upstream):
+    """FP64 GPU solve and adjoint vs the oracle's FP64 adjoint: relative L2 <= 1e-7."""
+    pts, q, rng = adjoint_case(P=2000, K=700, seed=11 + depth)
+    g = rng.normal(size=len(q)) if upstream else None
+    ctx.solve(pts, _params(depth))
+    chi, dp, dn, st = ctx.loss_backward(q, dl_dchi=g)
+    chi_o, dp_o, dn_o, L_o = oracle.loss_backward(pts, q, depth, dl_dchi=g)
+    assert st.converged == 1 and st.rel_residual <= 1e-12
+    assert _rel(chi, chi_o) <= 1e-9
+    assert st.loss == pytest.approx(L_o, rel=1e-9)
+    assert _rel(dp, dp_o) <= 1e-7
+    assert _rel(dn, dn_o) <= 1e-7
+
+
+def test_adjoint_mixed_precision(ctx):
+    """FP32 multigrid PCG + FP64 refinement at the default 1e-6 target: gradients within
+    relative L2 1e-5 of the oracle's."""
+    D = 6
+    pts, q, _ = adjoint_case(P=4000, K=1000, seed=3)
+    ctx.solve(pts, _params(D, fp64=False, target=1e-6))
+    _, dp, dn, st = ctx.loss_backward(q)
+    _, dp_o, dn_o, _ = oracle.loss_backward(pts, q, D)
+    assert st.converged == 1 and st.rel_residual <= 1e-6
+    assert _rel(dp, dp_o) <= 1e-5
+    assert _rel(dn, dn_o) <= 1e-5
+
+
+def test_adjoint_finite_differences_gpu(ctx):
+    """Central differences (fourth order, step 1e-4, model space) of the GPU forward (FP64
+    solve to 1e-13) vs the GPU adjoint, on 16 coordinates: <= 1e-4 relative."""
+    D = 6
+    pts, q, rng = adjoint_case(P=3000, K=800, seed=21)
+    p = _params(D, target=1e-13)
+
+    def loss(points):
+        ctx.solve(points, p)
+        _, _, m = ctx.info()
+        m = m.reshape(4, 4).T
+        chi = ctx.evaluate(q @ m[:3, :3].T + m[:3, 3])
+        return float(np.mean(chi ** 2))
+
+    ctx.solve(pts, p)
+    _, dp, dn, st = ctx.loss_backward(q)
+    grads = np.hstack([dp, dn])
+    gmax = np.abs(grads).max(axis=0)
+    for i, col in fd_coordinates(pts, D, rng, 16):
+        fd = fd_gradient(loss, pts, i, col)
+        an = grads[i, col]
+        assert abs(fd - an) <= 1e-4 * max(abs(an), 1e-2 * gmax[col]), (i, col, fd, an)
+
+
+def test_adjoint_is_deterministic_and_linear(ctx):
+    """Same call twice -> identical bits; gradients are linear in the upstream gradient."""
+    D = 6
+    pts, q, rng = adjoint_case(P=3000, K=900, seed=4)
+    ctx.solve(pts, _params(D, fp64=False, target=1e-6))
+    g1, g2 = rng.normal(size=len(q)), rng.normal(size=len(q))
+    _, a1, b1, _ = ctx.loss_backward(q, dl_dchi=g1)
+    _, a1b, b1b, _ = ctx.loss_backward(q, dl_dchi=g1)
+    assert np.array_equal(a1, a1b) and np.array_equal(b1, b1b)
+    _, a2, b2, _ = ctx.loss_backward(q, dl_dchi=g2)
+    _, a3, b3, _ = ctx.loss_backward(q, dl_dchi=g1 + g2)
+    assert _rel(a1 + a2, a3) <= 1e-5 and _rel(b1 + b2, b3) <= 1e-5
+
+
+def test_adjoint_one_shot_and_errors(ctx):
+    pts, q, _ = adjoint_case(P=1500, K=400, seed=8)
+    p = _params(5)
+    chi, dp, dn, st = prb.loss_backward(pts, q, p)
+    ctx.solve(pts, p)
+    chi2, dp2, dn2, _ = ctx.loss_backward(q)
+    assert np.array_equal(chi, chi2) and np.array_equal(dp, dp2) and np.array_equal(dn, dn2)
+    # the reference schedule does not solve A x = b: refused
+    ctx.solve(pts, prb.ReconstructParams(depth=5, point_weight=4.0, solve_mode=prb.PR_SOLVE_REFERENCE_SCHEDULE,
+                                         cg_iters=8))
+    with pytest.raises(prb.ReconstructError) as e:
+        ctx.loss_backward(q)
+    assert e.value.code == prb.PR_ERR_STATE
+    ctx.solve(pts, p)
+    with pytest.raises(prb.ReconstructError) as e:
+        ctx.loss_backward(np.zeros((0, 3)))
+    assert e.value.code == prb.PR_ERR_INVALID_ARGUMENT
+    with pytest.raises(prb.ReconstructError) as e:
+        ctx.loss_backward(np.array([[0.0, np.nan, 0.0]]))
+    assert e.value.code == prb.PR_ERR_INVALID_ARGUMENT
+
+
+def test_autograd_bridge():
+    torch = pytest.importorskip("torch")
+    from poissonreconstruction_b200.autograd import implicit_function
+    pts, q, _ = adjoint_case(P=2000, K=500, seed=9)
+    params = _params(5)
+    pos = torch.tensor(pts[:, :3], requires_grad=True)
+    nrm = torch.tensor(pts[:, 3:], requires_grad=True)
+    chi = implicit_function(pos, nrm, torch.tensor(q), params)
+    loss = (chi ** 2).mean()
+    loss.backward()
+    _, dp, dn, st = prb.loss_backward(pts, q, params)
+    assert float(loss) == pytest.approx(st.loss, rel=1e-12)
+    assert _rel(pos.grad.numpy(), dp) <= 1e-12
+    assert _rel(nrm.grad.numpy(), dn) <= 1e-12
+
+
+def test_adjoint_superquadric_depth8(ctx):
+    """Superquadric workload (eps1 0.5, eps2 0.8, axes 1/0.7/0.5, normals tilted up to 20 deg,
+    queries on the true surface) at depth 8 with 200k points: mixed-precision gradients vs the
+    FP64 GPU adjoint (1e-4 relative L2), and 8 finite differences of the FP64 GPU forward."""
+    D = 8
+    pts = synthetic.superquadric(200_000, seed=synthetic.SEED_BASE + 3)
+    q = synthetic.superquadric_queries(40_000)
+    ctx.solve(pts, _params(D, target=1e-12))
+    _, dp64, dn64, st64 = ctx.loss_backward(q)
+    assert st64.converged == 1
+    ctx.solve(pts, _params(D, fp64=False, target=1e-6))
+    _, dp, dn, st = ctx.loss_backward(q)
+    assert st.converged == 1
+    assert _rel(dp, dp64) <= 1e-4 and _rel(dn, dn64) <= 1e-4
+    p = _params(D, target=1e-12)
+
+    def loss(points):
+        ctx.solve(points, p)
+        _, _, m = ctx.info()
+        m = m.reshape(4, 4).T
+        chi = ctx.evaluate(q @ m[:3, :3].T + m[:3, 3])
+        return float(np.mean(chi ** 2))
+
+    rng = np.random.default_rng(1)
+    grads = np.hstack([dp64, dn64])
+    gmax = np.abs(grads).max(axis=0)
+    for i, col in fd_coordinates(pts, D, rng, 8):
+        fd = fd_gradient(loss, pts, i, col)
+        an = grads[i, col]
+        assert abs(fd - an) <= 1e-4 * max(abs(an), 1e-2 * gmax[col]), (i, col, fd, an)

@@ -218,3 +218,20 @@ def test_one_shot_api_matches_context():
         m2, s2 = c.reconstruct(pts, p)
     assert np.array_equal(m1.triangles, m2.triangles) and np.array_equal(m1.vertices, m2.vertices)
     assert s1.iso_value == s2.iso_value
+
+
+@pytest.mark.parametrize("precision", [prb.PR_PRECISION_MIXED, prb.PR_PRECISION_FP64])
+@pytest.mark.parametrize("depth", [5, 7])
+def test_solve_is_deterministic(precision, depth):
+    """Every reduction has a fixed order and no kernel reads what its own launch writes: the
+    same input gives the same coefficient bits, in one context and in a fresh one."""
+    pts = synthetic.torus(60_000, seed=17)
+    p = prb.ReconstructParams(depth=depth, point_weight=4.0, precision=precision)
+    with prb.Context(0) as c1, prb.Context(0) as c2:
+        c1.solve(pts, p)
+        x1 = c1.coefficients()
+        c1.solve(pts, p)
+        x2 = c1.coefficients()
+        c2.solve(pts, p)
+        x3 = c2.coefficients()
+    assert np.array_equal(x1, x2) and np.array_equal(x1, x3)

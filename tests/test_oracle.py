@@ -8,6 +8,7 @@ import pytest
 
 import oracle
 from poissonreconstruction_b200 import synthetic
+from tests.adjoint_cases import adjoint_case, fd_coordinates, fd_gradient
 
 REF = "/root/reference/src"
 
@@ -228,3 +229,24 @@ def test_empty_input():
     """src/reconstructor.rs:28: empty input -> empty mesh, default stats."""
     v, t, st, c = oracle.reconstruct(np.zeros((0, 6)), depth=4)
     assert len(v) == 0 and len(t) == 0 and st["iso_value"] == 0.0
+
+
+# ---------------------------------------------------------------- adjoint (no reference counterpart)
+@pytest.mark.parametrize("upstream", [False, True])
+def test_adjoint_matches_finite_differences(upstream):
+    """Oracle's analytic gradient (adjoint solve) vs central differences of the oracle's own
+    forward (fourth-order 5-point stencil, step 1e-4 in model space: the second-order stencil's
+    own error reaches 2e-4 where the splat normalisation 1/w is large): relative error <= 1e-4
+    against the coordinate's gradient, or against 1% of the largest entry of that column."""
+    D, eps = 5, 1e-4
+    pts, q, rng = adjoint_case()
+    g = rng.normal(size=len(q)) if upstream else None
+    chi, dp, dn, L = oracle.loss_backward(pts, q, D, dl_dchi=g)
+    assert L == pytest.approx(oracle.loss(pts, q, D, dl_dchi=g), rel=1e-12)
+    grads = np.hstack([dp, dn])
+    gmax = np.abs(grads).max(axis=0)
+    for i, col in fd_coordinates(pts, D, rng, 10):
+        fd = fd_gradient(lambda p: oracle.loss(p, q, D, dl_dchi=g), pts, i, col, eps)
+        an = grads[i, col]
+        ref = max(abs(an), 1e-2 * gmax[col])
+        assert abs(fd - an) <= 1e-4 * ref, (i, col, fd, an)
