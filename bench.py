@@ -12,8 +12,9 @@ residual refinement to a relative residual <= 1e-6.  One step = one full reconst
              back to host memory
   solve_gbs  algorithmic bytes of the solve / solve time; the FP64 solve of the same system
              is timed beside it (fp64_* keys)
-  roofline   the matrix-free operator (21-point stencil + screening) timed alone with CUDA
-             events on the library's stream
+  roofline   the solver kernel with the largest share of the step (the FP32 residual fused
+             with the restriction) timed alone with CUDA events on the library's stream; every
+             fine-level solver kernel is reported beside it under "kernels"
   cpu_baseline  the CPU oracle (the crate's schedule restated in C++) at depth 7 on the same
              cloud, extrapolated to depth 10 (x512 nodes): the crate itself needs ~1 TB of
              host RAM at depth 10
@@ -279,14 +280,21 @@ def run_ours(a):
     solve64_s = statistics.mean(s.time_solve for s in stats64)
 
     # e2e: host (pinned) input, mesh copied back, through the public call
-    e2e_ms = []
+    e2e_ms, e2e_lib, e2e_copy = [], [], []
     mesh = None
+    for _ in range(a.warmup):  # untimed: the first calls pin the host blocks the mesh lands in
+        mesh, _ = ctx.reconstruct(h_pts.numpy(), params)
     for _ in range(a.steps):
         flush.zero_()
         torch.cuda.synchronize(dev)
+        mesh = None  # free the previous mesh outside the timed region
         t0 = time.perf_counter()
         mesh, st_e = ctx.reconstruct(h_pts.numpy(), params)
         e2e_ms.append(1000.0 * (time.perf_counter() - t0))
+        e2e_lib.append(1000.0 * st_e.time_total)
+        e2e_stage = {"transform_incl_h2d": st_e.time_transform, "tree_splat_rhs": st_e.time_tree,
+                     "solve": st_e.time_solve, "extract": st_e.time_extract, "mesh_copy": st_e.time_mesh_copy}
+        e2e_copy.append(1000.0 * st_e.time_mesh_copy)
     e2e_ms_max = reduce_max(dist, statistics.mean(e2e_ms), dev)
     e2e_value = total_points / (e2e_ms_max / 1000.0)
     h2d = P * 48
@@ -347,7 +355,9 @@ def run_ours(a):
             "kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_ms_max},
+                    "ms_per_step": e2e_ms_max, "library_ms": statistics.mean(e2e_lib),
+                    "mesh_copy_ms": statistics.mean(e2e_copy),
+                    "last_step_stage_ms": {k: 1000.0 * v for k, v in e2e_stage.items()}},
             "clocks": clocks.summary(),
             "gpu_launches": int(l1 - l0),
             "gpu_launches_per_step": int((l1 - l0) / max(1, a.steps)),

@@ -72,7 +72,7 @@ typedef struct pr_params {
 
 /* Mesh (src/marching_cubes.rs:8-11).  Vertices are model-space [x,y,z] triples; triangles
  * are vertex-index triples (the crate's usize -> uint64).  Library-owned: free with
- * pr_mesh_free(). */
+ * pr_mesh_free() (or each array with pr_host_free()). */
 typedef struct pr_mesh {
   double* vertices;
   uint64_t n_vertices;
@@ -96,7 +96,8 @@ typedef struct pr_stats {
   double peak_device_bytes;     /* peak device memory held by the context */
   int32_t converged;            /* converged mode: 1 if rel_residual <= target_rel_residual */
   int32_t reserved_i;
-  double reserved[5];
+  double time_mesh_copy;        /* seconds copying the mesh to the caller's host memory */
+  double reserved[4];
 } pr_stats;
 
 /* ------------------------------------------------------------------ one-shot API */
@@ -108,7 +109,11 @@ pr_params pr_params_default(void);
  * out_stats may be NULL. */
 int pr_reconstruct(const double* points6, uint64_t n, const pr_params* params, pr_mesh* out_mesh,
                    pr_stats* out_stats);
+/* Frees a mesh returned by this library (both arrays).  Mesh arrays may live in pinned memory
+ * from a library pool: release them only through pr_mesh_free / pr_host_free, never free(). */
 void pr_mesh_free(pr_mesh* mesh);
+/* Frees ONE array of a returned mesh (for bindings that own the two arrays separately). */
+void pr_host_free(void* array);
 const char* pr_last_error(void);
 
 /* ------------------------------------------------------------------ context API

@@ -54,7 +54,7 @@ class PrStats(C.Structure):
                 ("mesh_triangles", C.c_uint64), ("iso_value", C.c_double), ("rel_residual", C.c_double),
                 ("pcg_iterations", C.c_uint32), ("refinement_steps", C.c_uint32), ("points_in_cube", C.c_uint64),
                 ("solve_bytes", C.c_double), ("peak_device_bytes", C.c_double), ("converged", C.c_int32),
-                ("reserved_i", C.c_int32), ("reserved", C.c_double * 5)]
+                ("reserved_i", C.c_int32), ("time_mesh_copy", C.c_double), ("reserved", C.c_double * 4)]
 
 
 class PrAdjointStats(C.Structure):
@@ -77,6 +77,7 @@ SIGNATURES = {
     "pr_params_default": (PrParams, []),
     "pr_reconstruct": (C.c_int, [_P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrMesh), C.POINTER(PrStats)]),
     "pr_mesh_free": (None, [C.POINTER(PrMesh)]),
+    "pr_host_free": (None, [_P]),
     "pr_context_create": (C.c_int, [C.c_int, _P, C.POINTER(_P)]),
     "pr_context_destroy": (C.c_int, [_P]),
     "pr_ctx_reconstruct": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrMesh),
@@ -186,35 +187,24 @@ class ReconstructStats:
     solve_bytes: float = 0.0
     peak_device_bytes: float = 0.0
     converged: int = 0
+    time_mesh_copy: float = 0.0
 
     @classmethod
     def from_c(cls, s):
         return cls(**{f.name: getattr(s, f.name) for f in dataclasses.fields(cls)})
 
 
-_LIBC = None
-
-
-def _libc_free():
-    global _LIBC
-    if _LIBC is None:
-        _LIBC = C.CDLL(None).free
-        _LIBC.argtypes = [C.c_void_p]
-        _LIBC.restype = None
-    return _LIBC
-
-
 def _owned_array(ptr, count, ctype, dtype):
-    """numpy view of a malloc'd library buffer; the buffer is freed with the array."""
+    """numpy view of a library-allocated mesh array; pr_host_free releases it with the array."""
     if not count:
         return np.zeros((0, 3), dtype=dtype)
     base = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count * 3,))
-    weakref.finalize(base, _libc_free(), C.cast(ptr, C.c_void_p).value)
+    weakref.finalize(base, lib().pr_host_free, C.cast(ptr, C.c_void_p).value)
     return base.reshape(-1, 3)
 
 
 def _take_mesh(m):
-    """Take ownership of a pr_mesh without copying (the library allocates with malloc)."""
+    """Take ownership of a pr_mesh's arrays without copying."""
     v = _owned_array(m.vertices, m.n_vertices, C.c_double, np.float64)
     t = _owned_array(m.triangles, m.n_triangles, C.c_uint64, np.uint64)
     m.vertices = None

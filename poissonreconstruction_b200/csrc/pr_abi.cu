@@ -5,7 +5,12 @@
 //   is implicit, the FEM index is the Morton index), solve (stage_solve), iso value and
 //   marching cubes (stage_iso / stage_extract), back-transform of the vertices.
 // Every entry point converts exceptions into a status code and a thread-local message.
+#include <sys/mman.h>
+
 #include <atomic>
+#include <unordered_map>
+#include <map>
+#include <mutex>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -70,57 +75,181 @@ void validate(const pr_params* p) {
 
 void set_device(pr_context* c) { PR_CUDA(cudaSetDevice(c->device)); }
 
-// host memcpy split over threads (first-touch page faults of fresh output buffers dominate)
-void parallel_copy(void* dst, const void* src, size_t bytes) {
-  const size_t chunk = size_t(32) << 20;
-  unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  if (bytes < chunk || nt == 1) {
-    std::memcpy(dst, src, bytes);
-    return;
+// Pool of pinned host blocks for returned meshes.  A mesh copied into pinned memory needs one
+// DMA and no host copy; pinning fresh memory is slow, so blocks released by pr_mesh_free /
+// pr_host_free are kept (up to PR_HOST_POOL_MB, default 4096; 0 disables the pool) and
+// handed out again to later meshes of a similar size.  Blocks stay pinned until exit.
+struct HostPool {
+  std::mutex mu;
+  std::multimap<size_t, void*> idle;        // capacity -> block
+  std::unordered_map<void*, size_t> owned;  // every pool block -> capacity
+  size_t idle_bytes = 0;
+  size_t limit = 0;
+  HostPool() {
+    const char* e = std::getenv("PR_HOST_POOL_MB");
+    limit = (size_t)(e ? std::strtoull(e, nullptr, 10) : 4096ull) << 20;
   }
-  nt = (unsigned)std::min<size_t>(nt, (bytes + chunk - 1) / chunk);
-  std::vector<std::thread> th;
-  const size_t per = (bytes + nt - 1) / nt;
-  for (unsigned i = 0; i < nt; ++i) {
-    const size_t lo = i * per, hi = std::min(bytes, lo + per);
-    if (lo >= hi) break;
-    th.emplace_back([=] { std::memcpy((char*)dst + lo, (const char*)src + lo, hi - lo); });
+};
+HostPool& host_pool() {
+  static HostPool* p = new HostPool();  // never destroyed: blocks may be freed during exit
+  return *p;
+}
+// A pinned block of >= bytes, or nullptr (pool disabled, or pinning failed).
+void* pool_alloc(size_t bytes) {
+  HostPool& hp = host_pool();
+  if (hp.limit == 0 || bytes == 0) return nullptr;
+  {
+    std::lock_guard<std::mutex> g(hp.mu);
+    auto it = hp.idle.lower_bound(bytes);
+    if (it != hp.idle.end() && it->first <= 2 * bytes + (size_t(64) << 20)) {
+      void* p = it->second;
+      hp.idle_bytes -= it->first;
+      hp.idle.erase(it);
+      return p;
+    }
   }
-  for (auto& t : th) t.join();
+  const size_t cap = (bytes + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, cap, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> g(hp.mu);
+  hp.owned[p] = cap;
+  return p;
+}
+// Returns false if p is not a pool block.
+bool pool_release(void* p) {
+  if (!p) return true;
+  HostPool& hp = host_pool();
+  std::vector<void*> evict;
+  {
+    std::lock_guard<std::mutex> g(hp.mu);
+    auto it = hp.owned.find(p);
+    if (it == hp.owned.end()) return false;
+    hp.idle.insert({it->second, p});
+    hp.idle_bytes += it->second;
+    while (hp.idle_bytes > hp.limit && !hp.idle.empty()) {  // drop the largest idle blocks
+      auto last = std::prev(hp.idle.end());
+      hp.idle_bytes -= last->first;
+      hp.owned.erase(last->second);
+      evict.push_back(last->second);
+      hp.idle.erase(last);
+    }
+  }
+  for (void* q : evict) cudaFreeHost(q);
+  return true;
 }
 
+// Host output buffer of the mesh: 2 MiB-aligned and advised for transparent huge pages when
+// large, so that first-touch page faults (which dominate a copy into fresh memory) are few.
+// Freed with free() like any malloc'd block.
+void* alloc_host_out(size_t bytes) {
+  if (bytes == 0) return nullptr;
+  if (bytes < (size_t(4) << 20)) return std::malloc(bytes);
+  void* p = nullptr;
+  if (posix_memalign(&p, size_t(2) << 20, bytes) != 0) return nullptr;
+  madvise(p, bytes & ~((size_t(2) << 20) - 1), MADV_HUGEPAGE);  // advisory; failure is harmless
+  return p;
+}
+
+// Device mesh -> caller memory: D2H copies of 8 MiB chunks into the context's pinned staging,
+// each followed by an event, while host threads copy finished chunks on to the output
+// buffers (the DMA of later chunks overlaps the host copies and page faults of earlier ones).
 void copy_mesh_to_host(pr_context* c, pr_mesh* out) {
   out->vertices = nullptr;
   out->triangles = nullptr;
   out->n_vertices = c->nv;
   out->n_triangles = c->nt;
   const size_t vb = 3 * c->nv * sizeof(double), tb = 3 * c->nt * sizeof(uint64_t);
-  if (vb + tb == 0) return;
-  if (c->h_stage_cap < vb + tb) {
+  const size_t total = vb + tb;
+  if (total == 0) return;
+  {  // pinned pool blocks: one DMA each, straight into the caller's arrays
+    void* pv = vb ? pool_alloc(vb) : nullptr;
+    void* pt = tb ? pool_alloc(tb) : nullptr;
+    if ((!vb || pv) && (!tb || pt)) {
+      if (vb) PR_CUDA(cudaMemcpyAsync(pv, c->get<double>("mesh_v"), vb, cudaMemcpyDeviceToHost, c->stream));
+      if (tb) PR_CUDA(cudaMemcpyAsync(pt, c->get<uint64_t>("mesh_t"), tb, cudaMemcpyDeviceToHost, c->stream));
+      const cudaError_t e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) {
+        pool_release(pv);
+        pool_release(pt);
+        throw pr::Error(PR_ERR_CUDA, std::string("mesh copy to host failed: ") + cudaGetErrorString(e));
+      }
+      out->vertices = static_cast<double*>(pv);
+      out->triangles = static_cast<uint64_t*>(pt);
+      return;
+    }
+    pool_release(pv);
+    pool_release(pt);
+  }
+  if (c->h_stage_cap < total) {
     if (c->h_stage) cudaFreeHost(c->h_stage);
     c->h_stage = nullptr;
     c->h_stage_cap = 0;
-    const size_t cap = (vb + tb) + ((vb + tb) >> 3);
+    const size_t cap = total + (total >> 3);
     PR_CUDA(cudaMallocHost(&c->h_stage, cap));
     c->h_stage_cap = cap;
   }
-  if (vb)
-    PR_CUDA(cudaMemcpyAsync(c->h_stage, c->get<double>("mesh_v"), vb, cudaMemcpyDeviceToHost, c->stream));
-  if (tb)
-    PR_CUDA(cudaMemcpyAsync(c->h_stage + vb, c->get<uint64_t>("mesh_t"), tb, cudaMemcpyDeviceToHost, c->stream));
-  out->vertices = vb ? (double*)std::malloc(vb) : nullptr;
-  out->triangles = tb ? (uint64_t*)std::malloc(tb) : nullptr;
-  if ((vb && !out->vertices) || (tb && !out->triangles)) {
-    std::free(out->vertices);
-    std::free(out->triangles);
-    out->vertices = nullptr;
-    out->triangles = nullptr;
+  const size_t CH = size_t(8) << 20;
+  const size_t nch = (total + CH - 1) / CH;
+  if (c->copy_events.size() < nch) {
+    const size_t have = c->copy_events.size();
+    c->copy_events.resize(nch, nullptr);
+    for (size_t k = have; k < nch; ++k) PR_CUDA(cudaEventCreateWithFlags(&c->copy_events[k], cudaEventDisableTiming));
+  }
+  const unsigned char* dv = reinterpret_cast<const unsigned char*>(vb ? c->get<double>("mesh_v") : nullptr);
+  const unsigned char* dt = reinterpret_cast<const unsigned char*>(tb ? c->get<uint64_t>("mesh_t") : nullptr);
+  for (size_t k = 0; k < nch; ++k) {  // chunk k covers bytes [k CH, min(total, (k+1) CH)) of [vertices | triangles]
+    size_t lo = k * CH;
+    const size_t hi = std::min(total, lo + CH);
+    while (lo < hi) {
+      const bool in_v = lo < vb;
+      const size_t end = in_v ? std::min(hi, vb) : hi;
+      const unsigned char* src = in_v ? dv + lo : dt + (lo - vb);
+      PR_CUDA(cudaMemcpyAsync(c->h_stage + lo, src, end - lo, cudaMemcpyDeviceToHost, c->stream));
+      lo = end;
+    }
+    PR_CUDA(cudaEventRecord(c->copy_events[k], c->stream));
+  }
+  unsigned char* ov = static_cast<unsigned char*>(alloc_host_out(vb));
+  unsigned char* ot = static_cast<unsigned char*>(alloc_host_out(tb));
+  if ((vb && !ov) || (tb && !ot)) {
+    std::free(ov);
+    std::free(ot);
     c->sync();
     throw std::bad_alloc();
   }
-  c->sync();
-  if (vb) parallel_copy(out->vertices, c->h_stage, vb);
-  if (tb) parallel_copy(out->triangles, c->h_stage + vb, tb);
+  const unsigned nt = (unsigned)std::max<size_t>(1, std::min<size_t>({8, nch, std::thread::hardware_concurrency()}));
+  std::atomic<int> failed{0};
+  auto worker = [&](unsigned id) {
+    for (size_t k = id; k < nch; k += nt) {
+      if (cudaEventSynchronize(c->copy_events[k]) != cudaSuccess) {
+        failed = 1;
+        return;
+      }
+      size_t lo = k * CH;
+      const size_t hi = std::min(total, lo + CH);
+      while (lo < hi) {
+        const bool in_v = lo < vb;
+        const size_t end = in_v ? std::min(hi, vb) : hi;
+        std::memcpy(in_v ? ov + lo : ot + (lo - vb), c->h_stage + lo, end - lo);
+        lo = end;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < nt; ++i) th.emplace_back(worker, i);
+  worker(0);
+  for (auto& t : th) t.join();
+  if (failed) {
+    std::free(ov);
+    std::free(ot);
+    PR_CUDA(cudaStreamSynchronize(c->stream));
+    throw pr::Error(PR_ERR_CUDA, "mesh copy to host failed");
+  }
+  out->vertices = reinterpret_cast<double*>(ov);
+  out->triangles = reinterpret_cast<uint64_t*>(ot);
 }
 
 // The pipeline on device-resident points (c->buf "pts6" or caller memory).
@@ -193,7 +322,11 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
     d_pts = dp;
   }
   run_pipeline(c, d_pts, n, *params, st, t_start, extract);
-  if (out_mesh && extract) copy_mesh_to_host(c, out_mesh);
+  if (out_mesh && extract) {
+    const double t_copy = now_s();
+    copy_mesh_to_host(c, out_mesh);
+    st.time_mesh_copy = now_s() - t_copy;
+  }
   st.time_total = now_s() - t_start;
   if (out_stats) *out_stats = st;
 }
@@ -310,6 +443,9 @@ int pr_context_destroy(pr_context* c) {
     for (auto& kv : c->bufs)
       if (kv.second.ptr) cudaFree(kv.second.ptr);
     c->bufs.clear();
+    for (cudaEvent_t e : c->copy_events)
+      if (e) cudaEventDestroy(e);
+    c->copy_events.clear();
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -428,10 +564,14 @@ int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params,
   });
 }
 
+void pr_host_free(void* p) {
+  if (!pool_release(p)) std::free(p);
+}
+
 void pr_mesh_free(pr_mesh* m) {
   if (!m) return;
-  std::free(m->vertices);
-  std::free(m->triangles);
+  pr_host_free(m->vertices);
+  pr_host_free(m->triangles);
   m->vertices = nullptr;
   m->triangles = nullptr;
   m->n_vertices = m->n_triangles = 0;

@@ -120,6 +120,7 @@ struct pr_context {
   // pinned staging for device->host mesh copies (grown on demand)
   unsigned char* h_stage = nullptr;
   size_t h_stage_cap = 0;
+  std::vector<cudaEvent_t> copy_events;  // one per staged chunk of a mesh copy
   // --- state of the last reconstruction ---
   bool have_state = false;
   bool have_points = false;
