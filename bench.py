@@ -59,6 +59,10 @@ def parse():
                          "smooth_prolong_dot, resid_restrict, stencil_per_node, or 'all')")
     ap.add_argument("--fp64", action="store_true", help="--kernel in FP64")
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead of the default workload: the batched workload with this many clouds "
+                         "(256 = the full batch), timed through pr_reconstruct_batch")
+    ap.add_argument("--concurrency", type=int, default=4, help="--batch: contexts (streams) used")
     ap.add_argument("--only-device", action="store_true",
                     help="warm-up + timed device-resident steps only (for profiler launch lists)")
     return ap.parse_args()
@@ -390,8 +394,41 @@ def run_kernel_bench(a):
     return 0
 
 
+def run_batch(a):
+    """Batched workload: clouds of 1e4..5e5 points (ellipsoids and tori, depth 7/8/9 by size),
+    end to end through pr_reconstruct_batch (host input, meshes back in host memory)."""
+    import poissonreconstruction_b200 as prb
+    from poissonreconstruction_b200 import synthetic
+    clouds = synthetic.batch_clouds(a.batch)
+    pts = [c for c, _ in clouds]
+    params = [prb.ReconstructParams(depth=d, point_weight=4.0) for _, d in clouds]
+    total = sum(len(c) for c in pts)
+    for _ in range(a.warmup):
+        out = prb.reconstruct_batch(pts, params, concurrency=a.concurrency)
+        del out
+    ms = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        out = prb.reconstruct_batch(pts, params, concurrency=a.concurrency)
+        ms.append(1000.0 * (time.perf_counter() - t0))
+        tris = sum(m.triangles.shape[0] for m, _ in out)
+        conv = all(st.converged for _, st in out)
+        del out
+    t = statistics.mean(ms)
+    print(json.dumps({"metric": "batched reconstruction throughput", "value": a.batch / (t / 1000.0),
+                      "unit": "clouds/s", "points_per_s": total / (t / 1000.0), "ms_per_batch": t,
+                      "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "data": "synthetic",
+                      "config": {"workload": "batch_%d" % a.batch, "clouds": a.batch, "points": total,
+                                 "depths": {str(d): sum(1 for _, dd in clouds if dd == d) for d in (7, 8, 9)},
+                                 "point_weight": 4.0, "concurrency": a.concurrency},
+                      "triangles": tris, "all_converged": conv}), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.batch:
+        return run_batch(a)
     if a.kernel:
         return run_kernel_bench(a)
     if a.impl == "reference":

@@ -177,6 +177,22 @@ int pr_ctx_apply_operator_device(pr_context* ctx, const void* d_x, void* d_y, in
 int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precision, int reps, double* ms_per_launch,
                         double* bytes_per_launch);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent clouds (each with its own params, e.g. its own depth).  One host thread per
+ * context drives that context's stream; clouds are taken largest first, so the kernels of
+ * several small reconstructions overlap on the GPU.  out_meshes[i] / out_stats[i] /
+ * out_status[i] belong to cloud i (out_stats and out_status may be NULL).  Returns PR_OK if
+ * every cloud succeeded, else the status of the lowest-numbered failed cloud (its message in
+ * pr_last_error); the other clouds' results are still written.  No counterpart in the
+ * reference crate, which reconstructs one cloud per call (src/reconstructor.rs:25). */
+int pr_ctx_reconstruct_batch(pr_context* const* ctxs, uint32_t n_ctx, const double* const* points6, const uint64_t* n,
+                             uint32_t count, const pr_params* params, pr_mesh* out_meshes, pr_stats* out_stats,
+                             int* out_status);
+/* Same on a library-owned set of `concurrency` contexts on device 0 (0 = 4), kept between calls
+ * (calls are serialised). */
+int pr_reconstruct_batch(const double* const* points6, const uint64_t* n, uint32_t count, const pr_params* params,
+                         uint32_t concurrency, pr_mesh* out_meshes, pr_stats* out_stats, int* out_status);
+
 /* ------------------------------------------------------------------ adjoint (gradients)
  * No counterpart in the reference crate.  The implicit function chi(q) = evaluate(x, M q)
  * (src/fem_tree.rs:490-513) of the solved coefficients x (A x = b, src/fem_tree.rs:180-299)

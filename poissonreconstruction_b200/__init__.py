@@ -96,6 +96,8 @@ SIGNATURES = {
     "pr_ctx_evaluate": (C.c_int, [_P, _P, _P, C.c_uint64, _P]),
     "pr_ctx_extract": (C.c_int, [_P, _P, C.c_double, C.POINTER(PrMesh)]),
     "pr_ctx_extract_at_depth": (C.c_int, [_P, C.c_uint32, _P, C.c_double, C.POINTER(PrMesh)]),
+    "pr_ctx_reconstruct_batch": (C.c_int, [_P, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P]),
+    "pr_reconstruct_batch": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P]),
     "pr_ctx_solve": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrStats)]),
     "pr_ctx_loss_backward": (C.c_int, [_P, _P, C.c_uint64, _P, _P, _P, _P, C.POINTER(PrAdjointStats)]),
     "pr_loss_backward": (C.c_int, [_P, C.c_uint64, C.POINTER(PrParams), _P, C.c_uint64, _P, _P, _P, _P,
@@ -227,6 +229,30 @@ def reconstruct(points, params=None):
     p, m, s = params.to_c(), PrMesh(), PrStats()
     _check(lib().pr_reconstruct(_ptr(pts), pts.shape[0], C.byref(p), C.byref(m), C.byref(s)))
     return _take_mesh(m), ReconstructStats.from_c(s)
+
+
+def reconstruct_batch(clouds, params=None, concurrency=4):
+    """Reconstruct independent clouds concurrently (no counterpart in the reference crate).
+
+    clouds: sequence of (N_i, 6) arrays; params: one ReconstructParams for all clouds or a
+    sequence with one per cloud.  Returns a list of (Mesh, ReconstructStats); raises on the
+    lowest-numbered failed cloud."""
+    pts = [_points(c) for c in clouds]
+    count = len(pts)
+    if params is None or isinstance(params, ReconstructParams):
+        params = [params or ReconstructParams()] * count
+    if len(params) != count:
+        raise ValueError("one params entry per cloud")
+    ptrs = (C.c_void_p * count)(*[p.ctypes.data for p in pts])
+    ns = (C.c_uint64 * count)(*[p.shape[0] for p in pts])
+    cps = (PrParams * count)(*[p.to_c() for p in params])
+    meshes = (PrMesh * count)()
+    stats = (PrStats * count)()
+    status = (C.c_int * count)()
+    rc = lib().pr_reconstruct_batch(ptrs, ns, count, cps, int(concurrency), meshes, stats, status)
+    out = [(_take_mesh(meshes[i]), ReconstructStats.from_c(stats[i])) for i in range(count)]
+    _check(rc)
+    return out
 
 
 @dataclasses.dataclass

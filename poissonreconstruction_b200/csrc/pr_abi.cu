@@ -564,6 +564,68 @@ int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params,
   });
 }
 
+int pr_ctx_reconstruct_batch(pr_context* const* ctxs, uint32_t n_ctx, const double* const* points6, const uint64_t* n,
+                             uint32_t count, const pr_params* params, pr_mesh* out_meshes, pr_stats* out_stats,
+                             int* out_status) {
+  std::vector<std::string> msgs;
+  std::vector<int> status;
+  const int rc = guard([&] {
+    PR_REQUIRE(count == 0 || (ctxs && n_ctx > 0 && points6 && n && params && out_meshes), PR_ERR_INVALID_ARGUMENT,
+               "NULL argument");
+    for (uint32_t i = 0; i < n_ctx && count > 0; ++i) PR_REQUIRE(ctxs[i] != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL context");
+    for (uint32_t i = 0; i < count; ++i) std::memset(&out_meshes[i], 0, sizeof(pr_mesh));
+    if (count == 0) return;
+    // largest clouds first, one host thread per context pulling the next cloud
+    std::vector<uint32_t> order(count);
+    for (uint32_t i = 0; i < count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return n[a] > n[b]; });
+    status.assign(count, PR_OK);
+    msgs.assign(count, std::string());
+    std::atomic<uint32_t> next{0};
+    auto worker = [&](uint32_t w) {
+      for (;;) {
+        const uint32_t k = next.fetch_add(1);
+        if (k >= count) return;
+        const uint32_t i = order[k];
+        pr_stats st;
+        const int r = pr_ctx_reconstruct(ctxs[w], points6[i], n[i], &params[i], &out_meshes[i], &st);
+        status[i] = r;
+        if (r != PR_OK) msgs[i] = g_last_error;
+        else if (out_stats) out_stats[i] = st;
+      }
+    };
+    const uint32_t nw = std::min(n_ctx, count);
+    std::vector<std::thread> th;
+    for (uint32_t w = 1; w < nw; ++w) th.emplace_back(worker, w);
+    worker(0);
+    for (auto& t : th) t.join();
+  });
+  if (out_status)
+    for (uint32_t i = 0; i < count; ++i) out_status[i] = i < status.size() ? status[i] : rc;
+  if (rc != PR_OK) return rc;
+  for (uint32_t i = 0; i < status.size(); ++i)
+    if (status[i] != PR_OK) {
+      g_last_error = "cloud " + std::to_string(i) + ": " + msgs[i];
+      return status[i];
+    }
+  return PR_OK;
+}
+
+int pr_reconstruct_batch(const double* const* points6, const uint64_t* n, uint32_t count, const pr_params* params,
+                         uint32_t concurrency, pr_mesh* out_meshes, pr_stats* out_stats, int* out_status) {
+  static std::mutex mu;
+  static std::vector<pr_context*> pool;  // device 0, kept for later calls
+  std::lock_guard<std::mutex> g(mu);
+  const uint32_t want = concurrency ? std::min<uint32_t>(concurrency, 64) : 4;
+  while (pool.size() < want) {
+    pr_context* c = nullptr;
+    const int rc = pr_context_create(0, nullptr, &c);
+    if (rc != PR_OK) return rc;
+    pool.push_back(c);
+  }
+  return pr_ctx_reconstruct_batch(pool.data(), want, points6, n, count, params, out_meshes, out_stats, out_status);
+}
+
 void pr_host_free(void* p) {
   if (!pool_release(p)) std::free(p);
 }

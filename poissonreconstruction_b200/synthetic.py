@@ -143,3 +143,26 @@ def superquadric_queries(k=200_000, seed=SEED_BASE + 103, e1=0.5, e2=0.8, axes=(
     rng = _rng(seed)
     u, v = _superquadric_params(rng, k, e1, e2, axes)
     return np.ascontiguousarray(_superquadric_surface(u, v, e1, e2, axes)[0])
+
+
+def batch_clouds(count=256, seed=SEED_BASE + 4, lo=10_000, hi=500_000):
+    """Batched workload: `count` clouds with sizes log-uniform in [lo, hi], each an ellipsoid
+    (radii U[0.3, 1.0]) or a torus (R, r from U[0.3, 1.0] with r < R), analytic normals,
+    position noise 0.001, FP32-rounded.  Returns [(points, depth)], depth 7 below 40k points,
+    8 below 160k, else 9."""
+    rng = _rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        sub = int(rng.integers(1 << 31))
+        if rng.uniform() < 0.5:
+            radii = tuple(rng.uniform(0.3, 1.0, 3))
+            pts = ellipsoid(n, sub, radii=radii, noise=0.001, fp32=True)
+        else:
+            a, b = sorted(rng.uniform(0.3, 1.0, 2))
+            while b - a < 1e-3:
+                a, b = sorted(rng.uniform(0.3, 1.0, 2))
+            pts = torus(n, sub, R=b, r=a, noise=0.001, normal_sigma=0.0, fp32=True)
+        depth = 7 if n < 40_000 else (8 if n < 160_000 else 9)
+        out.append((pts, depth))
+    return out
