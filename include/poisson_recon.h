@@ -232,6 +232,18 @@ int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params,
                      const double* dl_dchi, double* chi, double* dl_dpositions, double* dl_dnormals,
                      pr_adjoint_stats* out_stats);
 
+/* ------------------------------------------------------------------ PLY files (host)
+ * ply::read_oriented_points (src/ply.rs:13-70): ASCII as the crate reads it (header up to
+ * "end_header"; "element vertex N"; a header line containing "nx" or "normal_x" is required;
+ * every later line with >= 6 tokens gives x y z nx ny nz from its first six tokens, a token
+ * that does not parse as f64 reads as 0.0, shorter lines are skipped); extension: files in
+ * binary_little_endian, read by property name.  *out_points6 (n AoS records of 6 doubles) is
+ * library memory: free it with pr_host_free.  Errors carry the crate's messages. */
+int pr_ply_read_points(const char* path, double** out_points6, uint64_t* out_n);
+#define PR_PLY_ASCII 0  /* ply::write_mesh (src/ply.rs:73-107), byte for byte */
+#define PR_PLY_BINARY 1 /* binary_little_endian, double vertices, uint32 (or uint64) indices */
+int pr_ply_write_mesh(const char* path, const pr_mesh* mesh, int format);
+
 /* Number of kernels launched by this library in this process (own kernels; library
  * primitives such as radix sorts and scans are counted in *primitive_calls). */
 uint64_t pr_kernel_launches(uint64_t* primitive_calls);

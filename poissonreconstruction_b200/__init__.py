@@ -98,6 +98,8 @@ SIGNATURES = {
     "pr_ctx_extract_at_depth": (C.c_int, [_P, C.c_uint32, _P, C.c_double, C.POINTER(PrMesh)]),
     "pr_ctx_reconstruct_batch": (C.c_int, [_P, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P]),
     "pr_reconstruct_batch": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P]),
+    "pr_ply_read_points": (C.c_int, [C.c_char_p, C.POINTER(_P), C.POINTER(C.c_uint64)]),
+    "pr_ply_write_mesh": (C.c_int, [C.c_char_p, C.POINTER(PrMesh), C.c_int]),
     "pr_ctx_solve": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(PrParams), C.POINTER(PrStats)]),
     "pr_ctx_loss_backward": (C.c_int, [_P, _P, C.c_uint64, _P, _P, _P, _P, C.POINTER(PrAdjointStats)]),
     "pr_loss_backward": (C.c_int, [_P, C.c_uint64, C.POINTER(PrParams), _P, C.c_uint64, _P, _P, _P, _P,
@@ -229,6 +231,32 @@ def reconstruct(points, params=None):
     p, m, s = params.to_c(), PrMesh(), PrStats()
     _check(lib().pr_reconstruct(_ptr(pts), pts.shape[0], C.byref(p), C.byref(m), C.byref(s)))
     return _take_mesh(m), ReconstructStats.from_c(s)
+
+
+PR_PLY_ASCII = 0
+PR_PLY_BINARY = 1
+CLI_PATH = os.path.join(_HERE, "poisson-recon")
+
+
+def read_ply(path):
+    """ply::read_oriented_points (src/ply.rs:13-70): an (N, 6) float64 array x y z nx ny nz."""
+    p, n = C.c_void_p(), C.c_uint64()
+    _check(lib().pr_ply_read_points(os.fsencode(path), C.byref(p), C.byref(n)))
+    if n.value == 0:
+        return np.zeros((0, 6))
+    base = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(n.value * 6,))
+    out = base.reshape(-1, 6).copy()
+    lib().pr_host_free(p)
+    return out
+
+
+def write_ply(path, mesh, binary=False):
+    """ply::write_mesh (src/ply.rs:73-107); binary=True writes binary_little_endian."""
+    v = np.ascontiguousarray(mesh.vertices, dtype=np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(mesh.triangles, dtype=np.uint64).reshape(-1, 3)
+    m = PrMesh(v.ctypes.data_as(C.POINTER(C.c_double)), v.shape[0], t.ctypes.data_as(C.POINTER(C.c_uint64)),
+               t.shape[0])
+    _check(lib().pr_ply_write_mesh(os.fsencode(path), C.byref(m), PR_PLY_BINARY if binary else PR_PLY_ASCII))
 
 
 def reconstruct_batch(clouds, params=None, concurrency=4):

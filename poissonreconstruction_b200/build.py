@@ -29,8 +29,14 @@ def nvcc():
     raise RuntimeError("nvcc not found")
 
 
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I", os.path.join(ROOT, "include")]
+CLI_SRC = os.path.join(HERE, "cli", "poisson_recon_cli.cpp")
+CLI = os.path.join(HERE, "poisson-recon")
+
+
 def sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    """Library sources: CUDA (.cu, nvcc) and host-only C++ (.cpp, g++)."""
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def headers():
@@ -47,9 +53,12 @@ def _stale(target, deps):
 
 
 def compile_one(src, force, extra):
-    obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+    obj = os.path.join(BUILD, os.path.splitext(os.path.basename(src))[0] + ".o")
     if force or _stale(obj, [src] + headers()):
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [os.environ.get("CXX_HOST", "g++")] + CXX_FLAGS + ["-c", src, "-o", obj]
+        else:
+            cmd = [nvcc()] + ARCH + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, " ".join(cmd), r.stderr))
@@ -68,7 +77,19 @@ def build(force=False, jobs=None, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    build_cli(force)
     return LIB
+
+
+def build_cli(force=False):
+    """The `poisson-recon` command (the crate's CLI, src/main.rs), linked against the library."""
+    if force or _stale(CLI, [CLI_SRC, LIB, os.path.join(ROOT, "include", "poisson_recon.h")]):
+        cmd = [os.environ.get("CXX_HOST", "g++"), "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"),
+               CLI_SRC, "-o", CLI, "-L" + HERE, "-lpoisson_recon_b200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("CLI build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    return CLI
 
 
 def main():
