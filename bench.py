@@ -95,6 +95,12 @@ def reduce_max(dist, value, device):
     return float(t.item())
 
 
+def replica_seed(rank):
+    """Each rank reconstructs its own cloud of the same workload (replicas, weak scaling)."""
+    from poissonreconstruction_b200 import synthetic
+    return synthetic.SEED_BASE + 2 + 1000 * rank
+
+
 def reduce_sum(dist, value, device):
     if dist is None:
         return value
@@ -224,7 +230,7 @@ def run_ours(a):
     torch.cuda.set_stream(stream)
     ctx = prb.Context(local, stream=stream.cuda_stream)
 
-    pts = synthetic.torus(a.points, seed=synthetic.SEED_BASE + 2 + 1000 * rank)
+    pts = synthetic.torus(a.points, seed=replica_seed(rank))
     P = len(pts)
     d_pts = torch.from_numpy(pts).to(dev)
     h_pts = torch.from_numpy(pts).pin_memory()
