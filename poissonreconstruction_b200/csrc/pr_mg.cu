@@ -836,22 +836,68 @@ constexpr size_t smem_bytes(int mode) {
 }  // namespace s16
 
 // ------------------------------------------------------------------ 16^3 stencil SpMV (finest level)
-// Natural tile, row stride 18, plane stride 326 (8 planes = 16 banks apart): 512 threads =
-// 256 columns x 2 z-halves; lanes = 16 x-columns x 2 halves -> conflict-free plane loads.
+// 256 threads: thread = one 2x2 (x, y) quad column over 4 z planes (64 quads x 4 z segments).
+// Natural tile with a one-node halo; local x sits at offset x + 1 so that the pairs (x0-1, x0)
+// and (x0+1, x0+2) a quad's row needs are 8-byte (FP32) / 16-byte (FP64) aligned, and the row
+// stride of 24 puts the two quad rows of a half-warp on disjoint banks.  The planes are swept
+// in z once: each plane's in-plane sums go to the output row of the plane itself (centre,
+// in-plane edges) and to the rows above and below (edges and corners), so a thread keeps two
+// accumulators per node instead of three planes of sums.
 namespace n16 {
-constexpr int N = 4096, THREADS = 512;
-constexpr int RS = 18, PS = 326, TILE = 18 * PS;
-__device__ __forceinline__ int nat(int ux, int uy, int uz) { return uz * PS + uy * RS + ux; }
+constexpr int N = 4096, THREADS = 256, ZT = 4;
+constexpr int RS = 24, PS = 18 * RS + 4, TILE = 18 * PS;
+__device__ __forceinline__ int nat(int ux, int uy, int uz) { return uz * PS + uy * RS + ux; }  // u = local + 1
 
-// KIND 0: q = A d, part = d.q; 1: dn = z + beta d, q = A dn, part = dn.q;
-// 2: xn = x + beta e (x, xn: FP64 solution, e: correction of type E), r = b - A xn
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+  typedef float2 type;
+};
+template <>
+struct Pair<double> {
+  typedef double2 type;
+};
+
+// the 4 x 4 patch (rows y0-1..y0+2, columns x0-1..x0+2) of tile plane uz around quad (x0, y0)
+template <typename T, int RSX>
+__device__ __forceinline__ void patch(const T* tile, int off, T r[4][4]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const typename Pair<T>::type l = *reinterpret_cast<const typename Pair<T>::type*>(tile + off + j * RSX);
+    const typename Pair<T>::type h = *reinterpret_cast<const typename Pair<T>::type*>(tile + off + j * RSX + 2);
+    r[j][0] = l.x;
+    r[j][1] = l.y;
+    r[j][2] = h.x;
+    r[j][3] = h.y;
+  }
+}
+
+// in-plane sums of the quad's 4 nodes: tz = ce*faces + cc*diagonals (for the rows z-1, z+1),
+// own = c0*centre + ce*diagonals (for row z)
+template <typename T>
+__device__ __forceinline__ void plane_terms(const T r[4][4], T c0, T ce, T cc, T tz[4], T own[4], T ctr[4]) {
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int e = 2 * j + i, R = j + 1, Cc = i + 1;
+      const T pf = r[R][Cc - 1] + r[R][Cc + 1] + r[R - 1][Cc] + r[R + 1][Cc];
+      const T pe = r[R - 1][Cc - 1] + r[R - 1][Cc + 1] + r[R + 1][Cc - 1] + r[R + 1][Cc + 1];
+      tz[e] = ce * pf + cc * pe;
+      own[e] = c0 * r[R][Cc] + ce * pe;
+      ctr[e] = r[R][Cc];
+    }
+}
+
+// KIND 0: q = A a, part = a.q;  1: an = bvec + beta a, q = A an, part = an.q;
+// 2: an = a + beta bvec (FP64 solution + correction of type E), q = rhs - A an.
 template <typename T, int KIND, typename E>
-__global__ void __launch_bounds__(THREADS) k_spmv16(uint32_t D, const T* __restrict__ a, const E* __restrict__ bvec,
-                                                   T* __restrict__ an, T beta, T* __restrict__ q, T c0, T ce, T cc,
-                                                   const T* __restrict__ rhs, double* __restrict__ part) {
+__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
+    k_spmv16(uint32_t D, const T* __restrict__ a, const E* __restrict__ bvec, T* __restrict__ an, T beta,
+             T* __restrict__ q, T c0, T ce, T cc, const T* __restrict__ rhs, double* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
-  T* out = tile + TILE;                      // N (Morton-local)
+  T* tile = reinterpret_cast<T*>(smem_raw);
   __shared__ uint32_t nb[27];
   const int res = 1 << D;
   const uint32_t blk = blockIdx.x;
@@ -860,104 +906,101 @@ __global__ void __launch_bounds__(THREADS) k_spmv16(uint32_t D, const T* __restr
   unmorton3(blk, bx, by, bz);
   const int t = threadIdx.x;
   s16::neighbour_bases(nb, bx, by, bz, res >> 4);
-  // value of the (updated) vector at global Morton index m
   auto val = [&](uint32_t m) -> T {
     if (KIND == 0) return __ldg(a + m);
     if (KIND == 1) return (T)__ldg(bvec + m) + beta * __ldg(a + m);
     return __ldg(a + m) + beta * (T)__ldg(bvec + m);
   };
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int qd = t + 512 * r;
+  for (int r = 0; r < 4; ++r) {
+    const int qd = t + THREADS * r;
     int lx, ly, lz;
     s16::quad_coords(qd, lx, ly, lz);
     const uint64_t m = base + 4 * qd;
-    const typename s16::Vec4<T>::type av = s16::ld4(a + m);
-    T v0 = av.x, v1 = av.y, v2 = av.z, v3 = av.w;
+    typename s16::Vec4<T>::type v = s16::ld4(a + m);
     if (KIND != 0) {
       const typename s16::Vec4<E>::type bv = s16::ld4(bvec + m);
       if (KIND == 1) {
-        v0 = (T)bv.x + beta * v0; v1 = (T)bv.y + beta * v1; v2 = (T)bv.z + beta * v2; v3 = (T)bv.w + beta * v3;
+        v.x = (T)bv.x + beta * v.x; v.y = (T)bv.y + beta * v.y; v.z = (T)bv.z + beta * v.z; v.w = (T)bv.w + beta * v.w;
       } else {
-        v0 += beta * (T)bv.x; v1 += beta * (T)bv.y; v2 += beta * (T)bv.z; v3 += beta * (T)bv.w;
+        v.x += beta * (T)bv.x; v.y += beta * (T)bv.y; v.z += beta * (T)bv.z; v.w += beta * (T)bv.w;
       }
-      out[4 * qd] = v0;
-      out[4 * qd + 1] = v1;
-      out[4 * qd + 2] = v2;
-      out[4 * qd + 3] = v3;
+      s16::st4(an + m, v);
     }
-    tile[nat(lx + 1, ly + 1, lz + 1)] = v0;
-    tile[nat(lx + 2, ly + 1, lz + 1)] = v1;
-    tile[nat(lx + 1, ly + 2, lz + 1)] = v2;
-    tile[nat(lx + 2, ly + 2, lz + 1)] = v3;
+    T* p0 = tile + nat(lx + 1, ly + 1, lz + 1);
+    p0[0] = v.x;
+    p0[1] = v.y;
+    p0[RS] = v.z;
+    p0[RS + 1] = v.w;
   }
+  __syncthreads();  // nb
+  s16::load_halo<T>(tile, a, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); }, val);
   __syncthreads();
-  if (t < 256) s16::load_halo<T>(tile, a, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); }, val);
-  __syncthreads();
-  if (KIND != 0) {  // write the updated vector (coalesced from the staged copy)
-    for (int i = t; i < N; i += THREADS) an[base + i] = out[i];
-    __syncthreads();
-  }
-  // column sweep: lanes = 16 x-columns x 2 z-halves, warps = y rows
-  const int lx = t & 15, half = (t >> 4) & 1, ly = t >> 5;
-  const int ux = lx + 1, uy = ly + 1;
-  const uint32_t mxy = s16::sp4(lx) | (s16::sp4(ly) << 1);
-  auto plane = [&](int uz, T& pc, T& pf, T& pe) {
-    const int b0 = nat(ux, uy, uz);
-    pc = tile[b0];
-    pf = tile[b0 - 1] + tile[b0 + 1] + tile[b0 - RS] + tile[b0 + RS];
-    pe = tile[b0 - 1 - RS] + tile[b0 + 1 - RS] + tile[b0 - 1 + RS] + tile[b0 + 1 + RS];
-  };
-  T pcm, pfm, pem, pc0, pf0, pe0;
-  const int z0 = 8 * half;
-  plane(z0, pcm, pfm, pem);
-  plane(z0 + 1, pc0, pf0, pe0);
+  const int qi = t & 63, zs = t >> 6;
+  const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
+  const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
+  T cur[4] = {0, 0, 0, 0}, nxt[4] = {0, 0, 0, 0}, cprev[4] = {0, 0, 0, 0};
   double acc = 0.0;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    T pcp, pfp, pep;
-    plane(z0 + k + 2, pcp, pfp, pep);
-    const T y = c0 * pc0 + ce * (pe0 + pfm + pfp) + cc * (pem + pep);
-    const uint32_t li = mxy | (s16::sp4(z0 + k) << 2);
-    if (KIND == 2) {
-      out[li] = __ldg(rhs + base + li) - y;
-    } else {
-      out[li] = y;
-      acc += (double)pc0 * (double)y;
+  for (int p = 0; p < ZT + 2; ++p) {  // tile plane z0 + p = local z0 + p - 1
+    T r[4][4], tz[4], own[4], ctr[4];
+    patch<T, RS>(tile, nat(x0, y0, z0 + p), r);
+    plane_terms<T>(r, c0, ce, cc, tz, own, ctr);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      cur[e] += tz[e];
+      nxt[e] += own[e];
     }
-    pcm = pc0; pfm = pf0; pem = pe0;
-    pc0 = pcp; pf0 = pfp; pe0 = pep;
+    if (p >= 2) {  // row of local z0 + p - 2 is complete
+      const uint64_t m = base + (mq | (s16::sp4(z0 + p - 2) << 2));
+      typename s16::Vec4<T>::type o;
+      if (KIND == 2) {
+        const typename s16::Vec4<T>::type rv = s16::ld4(rhs + m);
+        o.x = rv.x - cur[0]; o.y = rv.y - cur[1]; o.z = rv.z - cur[2]; o.w = rv.w - cur[3];
+      } else {
+        o.x = cur[0]; o.y = cur[1]; o.z = cur[2]; o.w = cur[3];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc += (double)cprev[e] * (double)cur[e];
+      }
+      s16::st4(q + m, o);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      cur[e] = nxt[e];
+      nxt[e] = tz[e];
+      cprev[e] = ctr[e];
+    }
   }
-  (void)pcm;
-  __syncthreads();
-  for (int i = t; i < N; i += THREADS) q[base + i] = out[i];
   if (KIND != 2) {
     typedef cub::BlockReduce<double, THREADS> BR;
     __shared__ typename BR::TempStorage tmp;
-    const double s = BR(tmp).Sum(acc);
-    if (t == 0) part[blk] = s;
+    const double sdot = BR(tmp).Sum(acc);
+    if (t == 0) part[blk] = sdot;
   }
 }
 template <typename T>
 constexpr size_t smem_bytes() {
-  return sizeof(T) * (TILE + N);
+  return sizeof(T) * TILE;
 }
 }  // namespace n16
 
 // ------------------------------------------------------------------ 16^3 residual + restriction
-// e on local [-2, 16] (tile coordinate = local + 2, width 19), r on local [-1, 15].
+// e on local [-2, 16] (tile u = local + 2, row offset u + 1 so that a quad's row pairs are
+// aligned, row stride 24 as in the SpMV), r on local [-1, 15] (u = local + 1).  The 16^3
+// interior residual uses the SpMV's quad columns; the low shell (local -1 on some axis), which
+// the restriction of this block's coarse nodes also needs, is computed per node.
 namespace r16 {
-constexpr int N = 4096, THREADS = 512;
-constexpr int WE = 19, RSE = 19, PSE = 362;  // 8 planes = 2896 = 16 (mod 32): halves on disjoint banks
-constexpr int WR = 17;
-constexpr int ETILE = WE * PSE, RTILE = WR * WR * WR;
-__device__ __forceinline__ int eidx(int ux, int uy, int uz) { return uz * PSE + uy * RSE + ux; }
-__device__ __forceinline__ int ridx(int rx, int ry, int rz) { return (rz * WR + ry) * WR + rx; }
+constexpr int N = 4096, THREADS = 256, ZT = 4;
+constexpr int WE = 19, RSE = 24, PSE = WE * RSE + 4;
+constexpr int WR = 17, RSR = 18, PSR = WR * RSR;
+constexpr int ETILE = WE * PSE, RTILE = WR * PSR;
+__device__ __forceinline__ int eidx(int ux, int uy, int uz) { return uz * PSE + uy * RSE + ux + 1; }
+__device__ __forceinline__ int ridx(int rx, int ry, int rz) { return rz * PSR + ry * RSR + rx; }
 
 template <typename T, bool FACES>
-__global__ void __launch_bounds__(THREADS) k_resid16(uint32_t D, const T* __restrict__ e, const T* __restrict__ f,
-                                                    T* __restrict__ fc, T c0, T ce, T cc,
-                                                    const T* __restrict__ table) {
+__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
+    k_resid16(uint32_t D, const T* __restrict__ e, const T* __restrict__ f, T* __restrict__ fc, T c0, T ce, T cc,
+              const T* __restrict__ table) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* et = reinterpret_cast<T*>(smem_raw);  // ETILE
   T* rt = et + ETILE;                      // RTILE
@@ -971,26 +1014,21 @@ __global__ void __launch_bounds__(THREADS) k_resid16(uint32_t D, const T* __rest
   const int t = threadIdx.x;
   s16::neighbour_bases(nb, bx, by, bz, res >> 4);
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int qd = t + 512 * r;
+  for (int r = 0; r < 4; ++r) {
+    const int qd = t + THREADS * r;
     int lx, ly, lz;
     s16::quad_coords(qd, lx, ly, lz);
     const typename s16::Vec4<T>::type ev = s16::ld4(e + base + 4 * qd);
-    const typename s16::Vec4<T>::type fv = s16::ld4(f + base + 4 * qd);
-    et[eidx(lx + 2, ly + 2, lz + 2)] = ev.x;
-    et[eidx(lx + 3, ly + 2, lz + 2)] = ev.y;
-    et[eidx(lx + 2, ly + 3, lz + 2)] = ev.z;
-    et[eidx(lx + 3, ly + 3, lz + 2)] = ev.w;
-    rt[ridx(lx + 1, ly + 1, lz + 1)] = fv.x;
-    rt[ridx(lx + 2, ly + 1, lz + 1)] = fv.y;
-    rt[ridx(lx + 1, ly + 2, lz + 1)] = fv.z;
-    rt[ridx(lx + 2, ly + 2, lz + 1)] = fv.w;
+    T* p0 = et + eidx(lx + 2, ly + 2, lz + 2);
+    p0[0] = ev.x;
+    p0[1] = ev.y;
+    p0[RSE] = ev.z;
+    p0[RSE + 1] = ev.w;
   }
-  __syncthreads();
+  __syncthreads();  // nb
   // one-node shell (local -1 and 16) through the structured loader; tile coordinate = u + 1
-  if (t < 256)
-    s16::load_halo<T>(et, e, nb, [](int ux, int uy, int uz) { return eidx(ux + 1, uy + 1, uz + 1); },
-                      [&](uint32_t m) { return __ldg(e + m); });
+  s16::load_halo<T>(et, e, nb, [](int ux, int uy, int uz) { return eidx(ux + 1, uy + 1, uz + 1); },
+                    [&](uint32_t m) { return __ldg(e + m); });
   // second low layer (local -2 on some axis, all coordinates in [-2, 16])
   for (int i = t; i < WE * WE * WE - 18 * 18 * 18; i += THREADS) {
     int lx, ly, lz;
@@ -1004,29 +1042,36 @@ __global__ void __launch_bounds__(THREADS) k_resid16(uint32_t D, const T* __rest
     et[eidx(lx + 2, ly + 2, lz + 2)] = v;
   }
   __syncthreads();
-  // interior r: columns (x, y), two z-halves of 8
-  {
-    const int lx = t & 15, half = (t >> 4) & 1, ly = t >> 5;  // lanes: 16 x-columns x 2 z-halves
-    auto plane = [&](int uz, T& pc, T& pf, T& pe) {
-      const int b0 = eidx(lx + 2, ly + 2, uz);
-      pc = et[b0];
-      pf = et[b0 - 1] + et[b0 + 1] + et[b0 - RSE] + et[b0 + RSE];
-      pe = et[b0 - 1 - RSE] + et[b0 + 1 - RSE] + et[b0 - 1 + RSE] + et[b0 + 1 + RSE];
-    };
-    T pcm, pfm, pem, pc0, pf0, pe0;
-    const int z0 = 8 * half;
-    plane(z0 + 1, pcm, pfm, pem);
-    plane(z0 + 2, pc0, pf0, pe0);
+  {  // interior r = f - A e on quad columns, z swept once (see the SpMV)
+    const int qi = t & 63, zs = t >> 6;
+    const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
+    const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
+    T cur[4] = {0, 0, 0, 0}, nxt[4] = {0, 0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      T pcp, pfp, pep;
-      plane(z0 + k + 3, pcp, pfp, pep);
-      const T y = c0 * pc0 + ce * (pe0 + pfm + pfp) + cc * (pem + pep);
-      rt[ridx(lx + 1, ly + 1, z0 + k + 1)] -= y;
-      pcm = pc0; pfm = pf0; pem = pe0;
-      pc0 = pcp; pf0 = pfp; pe0 = pep;
+    for (int p = 0; p < ZT + 2; ++p) {  // local plane z0 + p - 1
+      T r[4][4], tz[4], own[4], ctr[4];
+      n16::patch<T, RSE>(et, eidx(x0 + 1, y0 + 1, z0 + p + 1), r);
+      n16::plane_terms<T>(r, c0, ce, cc, tz, own, ctr);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        cur[k] += tz[k];
+        nxt[k] += own[k];
+      }
+      if (p >= 2) {
+        const int lz = z0 + p - 2;
+        const typename s16::Vec4<T>::type fv = s16::ld4(f + base + (mq | (s16::sp4(lz) << 2)));
+        T* q0 = rt + ridx(x0 + 1, y0 + 1, lz + 1);
+        q0[0] = fv.x - cur[0];
+        q0[1] = fv.y - cur[1];
+        q0[RSR] = fv.z - cur[2];
+        q0[RSR + 1] = fv.w - cur[3];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        cur[k] = nxt[k];
+        nxt[k] = tz[k];
+      }
     }
-    (void)pcm;
   }
   // low shell of r (local -1 on some axis)
   {
@@ -1089,22 +1134,25 @@ __global__ void __launch_bounds__(THREADS) k_resid16(uint32_t D, const T* __rest
     }
     __syncthreads();
   }
-  // restriction to the 8^3 coarse nodes of the block (Morton-local order)
+  // restriction to the 8^3 coarse nodes of the block (Morton-local order): coarse c gathers
+  // fine 2c-1, 2c, 2c+1 per axis with weights 1/2, 1, 1/2 (r tile u = local + 1)
   const uint64_t cbase = (uint64_t)blk * 512;
-  {
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int ci = t + THREADS * k;
     uint32_t cx, cy, cz;
-    unmorton3((uint32_t)t, cx, cy, cz);
-    const int fx = 2 * cx + 1, fy = 2 * cy + 1, fz = 2 * cz + 1;
+    unmorton3((uint32_t)ci, cx, cy, cz);
     T s = 0;
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+    for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
-      for (int dy = -1; dy <= 1; ++dy) {
-        const T wyz = (T)((dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0));
-        const int rb = ridx(fx, fy + dy, fz + dz);
-        s += wyz * ((T)0.5 * (rt[rb - 1] + rt[rb + 1]) + rt[rb]);
+      for (int dy = 0; dy < 3; ++dy) {
+        const T wyz = (T)((dy == 1 ? 1.0 : 0.5) * (dz == 1 ? 1.0 : 0.5));
+        const T* row = rt + ridx(2 * cx, 2 * cy + dy, 2 * cz + dz);
+        const typename n16::Pair<T>::type lo = *reinterpret_cast<const typename n16::Pair<T>::type*>(row);
+        s += wyz * ((T)0.5 * (lo.x + row[2]) + lo.y);
       }
-    fc[cbase + t] = s;
+    fc[cbase + ci] = s;
   }
 }
 template <typename T>
