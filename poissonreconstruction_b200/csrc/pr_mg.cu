@@ -985,25 +985,25 @@ constexpr size_t smem_bytes() {
 }  // namespace n16
 
 // ------------------------------------------------------------------ 16^3 residual + restriction
-// e on local [-2, 16] (tile u = local + 2, row offset u + 1 so that a quad's row pairs are
-// aligned, row stride 24 as in the SpMV), r on local [-1, 15] (u = local + 1).  The 16^3
-// interior residual uses the SpMV's quad columns; the low shell (local -1 on some axis), which
-// the restriction of this block's coarse nodes also needs, is computed per node.
+// Two launches, no redundant work.  k_resid16: r = f - A e on the block's 16^3 nodes (the
+// SpMV's tile and quad columns), then (a) the part of the restriction to the block's 8^3 coarse
+// nodes that comes from its own fine nodes, and (b) the residual of its three high faces
+// (local 15 on an axis) into a face buffer of 3 x 256 values per block.  k_restrict_faces then
+// adds, to the coarse nodes on each block's low faces, the contributions of the fine nodes at
+// local -1, read from the low neighbours' face buffers.  Restriction: coarse c gathers fine
+// 2c-1, 2c, 2c+1 per axis with weights 1/2, 1, 1/2.
 namespace r16 {
-constexpr int N = 4096, THREADS = 256, ZT = 4;
-constexpr int WE = 19, RSE = 24, PSE = WE * RSE + 4;
-constexpr int WR = 17, RSR = 18, PSR = WR * RSR;
-constexpr int ETILE = WE * PSE, RTILE = WR * PSR;
-__device__ __forceinline__ int eidx(int ux, int uy, int uz) { return uz * PSE + uy * RSE + ux + 1; }
-__device__ __forceinline__ int ridx(int rx, int ry, int rz) { return rz * PSR + ry * RSR + rx; }
+constexpr int N = 4096, THREADS = 256, ZT = 4, FACE = 768;
+constexpr int RSR = 20, PSR = 16 * RSR + 8, RTILE = 16 * PSR;  // half-warps of the restriction on disjoint banks
+__device__ __forceinline__ int ridx(int x, int y, int z) { return z * PSR + y * RSR + x; }  // local coordinates
 
 template <typename T, bool FACES>
 __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
-    k_resid16(uint32_t D, const T* __restrict__ e, const T* __restrict__ f, T* __restrict__ fc, T c0, T ce, T cc,
-              const T* __restrict__ table) {
+    k_resid16(uint32_t D, const T* __restrict__ e, const T* __restrict__ f, T* __restrict__ fc,
+              T* __restrict__ face, T c0, T ce, T cc, const T* __restrict__ table) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* et = reinterpret_cast<T*>(smem_raw);  // ETILE
-  T* rt = et + ETILE;                      // RTILE
+  T* et = reinterpret_cast<T*>(smem_raw);  // n16::TILE
+  T* rt = et + n16::TILE;                  // RTILE
   __shared__ uint32_t nb[27];
   const int res = 1 << D;
   const uint32_t blk = blockIdx.x;
@@ -1019,30 +1019,17 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     int lx, ly, lz;
     s16::quad_coords(qd, lx, ly, lz);
     const typename s16::Vec4<T>::type ev = s16::ld4(e + base + 4 * qd);
-    T* p0 = et + eidx(lx + 2, ly + 2, lz + 2);
+    T* p0 = et + n16::nat(lx + 1, ly + 1, lz + 1);
     p0[0] = ev.x;
     p0[1] = ev.y;
-    p0[RSE] = ev.z;
-    p0[RSE + 1] = ev.w;
+    p0[n16::RS] = ev.z;
+    p0[n16::RS + 1] = ev.w;
   }
   __syncthreads();  // nb
-  // one-node shell (local -1 and 16) through the structured loader; tile coordinate = u + 1
-  s16::load_halo<T>(et, e, nb, [](int ux, int uy, int uz) { return eidx(ux + 1, uy + 1, uz + 1); },
+  s16::load_halo<T>(et, e, nb, [](int ux, int uy, int uz) { return n16::nat(ux, uy, uz); },
                     [&](uint32_t m) { return __ldg(e + m); });
-  // second low layer (local -2 on some axis, all coordinates in [-2, 16])
-  for (int i = t; i < WE * WE * WE - 18 * 18 * 18; i += THREADS) {
-    int lx, ly, lz;
-    constexpr int S1 = WE * WE, S2 = 18 * WE;
-    if (i < S1) { lx = -2; ly = i % WE - 2; lz = i / WE - 2; }
-    else if (i < S1 + S2) { const int u = i - S1; lx = u % 18 - 1; ly = -2; lz = u / 18 - 2; }
-    else { const int u = i - S1 - S2; lx = u % 18 - 1; ly = u / 18 - 1; lz = -2; }
-    const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
-    T v = 0;
-    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) v = __ldg(e + morton3(gx, gy, gz));
-    et[eidx(lx + 2, ly + 2, lz + 2)] = v;
-  }
   __syncthreads();
-  {  // interior r = f - A e on quad columns, z swept once (see the SpMV)
+  {  // r = f - A e on quad columns, z swept once
     const int qi = t & 63, zs = t >> 6;
     const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
     const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
@@ -1050,7 +1037,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
 #pragma unroll
     for (int p = 0; p < ZT + 2; ++p) {  // local plane z0 + p - 1
       T r[4][4], tz[4], own[4], ctr[4];
-      n16::patch<T, RSE>(et, eidx(x0 + 1, y0 + 1, z0 + p + 1), r);
+      n16::patch<T, n16::RS>(et, n16::nat(x0, y0, z0 + p), r);
       n16::plane_terms<T>(r, c0, ce, cc, tz, own, ctr);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -1060,7 +1047,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
       if (p >= 2) {
         const int lz = z0 + p - 2;
         const typename s16::Vec4<T>::type fv = s16::ld4(f + base + (mq | (s16::sp4(lz) << 2)));
-        T* q0 = rt + ridx(x0 + 1, y0 + 1, lz + 1);
+        T* q0 = rt + ridx(x0, y0, lz);
         q0[0] = fv.x - cur[0];
         q0[1] = fv.y - cur[1];
         q0[RSR] = fv.z - cur[2];
@@ -1073,69 +1060,32 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
       }
     }
   }
-  // low shell of r (local -1 on some axis)
-  {
-    constexpr int S1 = WR * WR, S2 = 16 * WR, S3 = 16 * 16;
-    for (int i = t; i < S1 + S2 + S3; i += THREADS) {
-      int lx, ly, lz;
-      if (i < S1) { lx = -1; ly = i % WR - 1; lz = i / WR - 1; }
-      else if (i < S1 + S2) { const int u = i - S1; lx = u % 16; ly = -1; lz = u / 16 - 1; }
-      else { const int u = i - S1 - S2; lx = u % 16; ly = u / 16; lz = -1; }
-      const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
-      T r = 0;
-      if (gx >= 0 && gy >= 0 && gz >= 0) {
-        const int ei = eidx(lx + 2, ly + 2, lz + 2);
-        const int mask = FACES ? ((gx == 0) | ((gy == 0) << 1) | ((gz == 0) << 2)) : 0;
-        T y = 0;
-        if (mask) {
-          const T* cm = table + 27 * mask;
-#pragma unroll
-          for (int o = 0; o < 27; ++o)
-            y += cm[o] * et[ei + (o % 3 - 1) + RSE * ((o / 3) % 3 - 1) + PSE * (o / 9 - 1)];
-        } else {
-          T se = 0, sc = 0;
-#pragma unroll
-          for (int o = 0; o < 27; ++o) {
-            const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
-            const int nzc = (dx != 0) + (dy != 0) + (dz != 0);
-            const T v = et[ei + dx + RSE * dy + PSE * dz];
-            if (nzc == 2) se += v;
-            else if (nzc == 3) sc += v;
-          }
-          y = c0 * et[ei] + ce * se + cc * sc;
-        }
-        r = __ldg(f + morton3(gx, gy, gz)) - y;
-      }
-      rt[ridx(lx + 1, ly + 1, lz + 1)] = r;
-    }
-  }
   __syncthreads();
   if (FACES && (ox == 0 || oy == 0 || oz == 0)) {
-    // interior nodes on a low domain face: replace the interior row by the face row
+    // nodes on a low domain face: replace the interior row by the face row
     for (int i = t; i < N; i += THREADS) {
       uint32_t lx, ly, lz;
       unmorton3((uint32_t)i, lx, ly, lz);
       const int mask = ((ox + (int)lx) == 0) | (((oy + (int)ly) == 0) << 1) | (((oz + (int)lz) == 0) << 2);
       if (!mask) continue;
-      const int ei = eidx(lx + 2, ly + 2, lz + 2);
-      T yi = 0, yf = 0, se = 0, sc = 0;
+      const int ei = n16::nat(lx + 1, ly + 1, lz + 1);
+      T yf = 0, se = 0, sc = 0;
       const T* cm = table + 27 * mask;
 #pragma unroll
       for (int o = 0; o < 27; ++o) {
         const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
         const int nzc = (dx != 0) + (dy != 0) + (dz != 0);
-        const T v = et[ei + dx + RSE * dy + PSE * dz];
+        const T v = et[ei + dx + n16::RS * dy + n16::PS * dz];
         yf += cm[o] * v;
         if (nzc == 2) se += v;
         else if (nzc == 3) sc += v;
       }
-      yi = c0 * et[ei] + ce * se + cc * sc;
-      rt[ridx(lx + 1, ly + 1, lz + 1)] += yi - yf;
+      const T yi = c0 * et[ei] + ce * se + cc * sc;
+      rt[ridx(lx, ly, lz)] += yi - yf;
     }
     __syncthreads();
   }
-  // restriction to the 8^3 coarse nodes of the block (Morton-local order): coarse c gathers
-  // fine 2c-1, 2c, 2c+1 per axis with weights 1/2, 1, 1/2 (r tile u = local + 1)
+  // own part of the restriction
   const uint64_t cbase = (uint64_t)blk * 512;
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
@@ -1144,20 +1094,73 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     unmorton3((uint32_t)ci, cx, cy, cz);
     T s = 0;
 #pragma unroll
-    for (int dz = 0; dz < 3; ++dz)
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int fz = 2 * (int)cz + dz;
+      if (fz < 0) continue;
 #pragma unroll
-      for (int dy = 0; dy < 3; ++dy) {
-        const T wyz = (T)((dy == 1 ? 1.0 : 0.5) * (dz == 1 ? 1.0 : 0.5));
-        const T* row = rt + ridx(2 * cx, 2 * cy + dy, 2 * cz + dz);
-        const typename n16::Pair<T>::type lo = *reinterpret_cast<const typename n16::Pair<T>::type*>(row);
-        s += wyz * ((T)0.5 * (lo.x + row[2]) + lo.y);
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int fy = 2 * (int)cy + dy;
+        if (fy < 0) continue;
+        const T wyz = (T)((dy == 0 ? 1.0 : 0.5) * (dz == 0 ? 1.0 : 0.5));
+        const T* row = rt + ridx(2 * cx, fy, fz);
+        const typename n16::Pair<T>::type pr = *reinterpret_cast<const typename n16::Pair<T>::type*>(row);
+        const T left = cx > 0 ? row[-1] : (T)0;
+        s += wyz * (pr.x + (T)0.5 * (pr.y + left));
       }
+    }
     fc[cbase + ci] = s;
+  }
+  // high faces of r: plane 0 x = 15 (a = y, b = z), 1 y = 15 (a = x, b = z), 2 z = 15 (a = x, b = y)
+  T* fb = face + (uint64_t)blk * FACE;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int a = t & 15, b = t >> 4;
+    const int x = k == 0 ? 15 : a, y = k == 1 ? 15 : (k == 0 ? a : b), z = k == 2 ? 15 : b;
+    fb[k * 256 + t] = rt[ridx(x, y, z)];
+  }
+}
+
+// Adds to the coarse nodes on each block's low faces the contributions of the fine nodes at
+// local -1 (high faces of the low neighbours), in a fixed order.
+template <typename T>
+__global__ void __launch_bounds__(192) k_restrict_faces(uint32_t D, const T* __restrict__ face, T* __restrict__ fc) {
+  const int nba = 1 << (D - 4);
+  const uint32_t blk = blockIdx.x;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  // boundary coarse node j of 169: the (cx, cy, cz) in [0,8)^3 with at least one zero
+  const int j = threadIdx.x;
+  if (j >= 169) return;
+  int cx, cy, cz;
+  if (j < 64) { cx = 0; cy = j & 7; cz = j >> 3; }
+  else if (j < 120) { cx = 1 + (j - 64) % 7; cy = 0; cz = (j - 64) / 7; }
+  else { cx = 1 + (j - 120) % 7; cy = 1 + (j - 120) / 7; cz = 0; }
+  T s = 0;
+  bool any = false;
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int fx = 2 * cx + dx, fy = 2 * cy + dy, fz = 2 * cz + dz;
+        if (fx >= 0 && fy >= 0 && fz >= 0) continue;  // inside this block: already counted
+        const int nx = (int)bx - (fx < 0), ny = (int)by - (fy < 0), nz = (int)bz - (fz < 0);
+        if (nx < 0 || ny < 0 || nz < 0 || nx >= nba || ny >= nba || nz >= nba) continue;  // outside the domain
+        const int lx = fx & 15, ly = fy & 15, lz = fz & 15;
+        const T* fb = face + (uint64_t)morton3((uint32_t)nx, (uint32_t)ny, (uint32_t)nz) * FACE;
+        const T v = lx == 15 ? fb[ly + 16 * lz] : (ly == 15 ? fb[256 + lx + 16 * lz] : fb[512 + lx + 16 * ly]);
+        s += (T)((dx == 0 ? 1.0 : 0.5) * (dy == 0 ? 1.0 : 0.5) * (dz == 0 ? 1.0 : 0.5)) * v;
+        any = true;
+      }
+  if (any) {
+    const uint64_t ci = (uint64_t)blk * 512 + morton3((uint32_t)cx, (uint32_t)cy, (uint32_t)cz);
+    fc[ci] += s;
   }
 }
 template <typename T>
 constexpr size_t smem_bytes() {
-  return sizeof(T) * (ETILE + RTILE);
+  return sizeof(T) * (n16::TILE + RTILE);
 }
 }  // namespace r16
 
@@ -1327,20 +1330,21 @@ void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, 
 }
 
 template <typename T>
-void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc) {
+void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc, T* face) {
   const uint32_t D = L.depth;
   const DevCoef<T> k = dev_coef<T>(L, table);
   if (tile_for(D) == 16) {
     const size_t sm = r16::smem_bytes<T>();
+    const unsigned nb = 1u << (3 * (D - 4));
     if (L.has_faces) {
       allow_smem(r16::k_resid16<T, true>, sm);
-      r16::k_resid16<T, true><<<1u << (3 * (D - 4)), r16::THREADS, sm, s>>>(D, e, f, fc, (T)L.c0, (T)L.ce,
-                                                                            (T)L.cc, table);
+      r16::k_resid16<T, true><<<nb, r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce, (T)L.cc, table);
     } else {
       allow_smem(r16::k_resid16<T, false>, sm);
-      r16::k_resid16<T, false><<<1u << (3 * (D - 4)), r16::THREADS, sm, s>>>(D, e, f, fc, (T)L.c0, (T)L.ce,
-                                                                             (T)L.cc, table);
+      r16::k_resid16<T, false><<<nb, r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce, (T)L.cc, table);
     }
+    PR_CHECK_LAUNCH();
+    r16::k_restrict_faces<T><<<nb, 192, 0, s>>>(D, face, fc);
   } else {
     const size_t sm = sizeof(T) * (11 * 11 * 11 + 9 * 9 * 9);
     allow_smem(k_resid_restrict<T, 8>, sm);
@@ -1348,6 +1352,8 @@ void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const
   }
   PR_CHECK_LAUNCH();
 }
+
+size_t mg_face_entries(uint32_t D) { return D >= 4 ? (size_t)r16::FACE << (3 * (D - 4)) : 0; }
 
 template <typename T>
 void mg_spmv(cudaStream_t s, const LevelCoef& L, const T* table, const T* z, const T* d, T* dn, double beta,
@@ -1428,6 +1434,7 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
   T* f = c->buf<T>("kb_f_" + tn, n);
   T* w = c->buf<T>("kb_w_" + tn, n);
   T* ec = c->buf<T>("kb_c_" + tn, nc);
+  T* face = c->buf<T>("kb_face_" + tn, std::max<size_t>(mg_face_entries(D), 1));
   double* part = c->buf<double>("kb_part", std::max<uint32_t>(mg_blocks(D), kDotBlocks));
   const unsigned g = 148 * 16;
   k_fill<T><<<g, 256, 0, s>>>(x, n, 1u);
@@ -1449,7 +1456,7 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
       case 2: mg_smooth<T>(s, Lc, table, nullptr, y, f, nullptr, 1, true, nullptr); break;
       case 3: mg_smooth<T>(s, Lc, table, x, y, f, nullptr, 0, true, nullptr); break;
       case 4: mg_smooth<T>(s, Lc, table, x, y, f, ec, 2, false, part); break;
-      case 5: mg_resid_restrict<T>(s, Lc, table, x, f, ec); break;
+      case 5: mg_resid_restrict<T>(s, Lc, table, x, f, ec, face); break;
       case 6: stencil_apply<T>(s, D, x, nullptr, y, cast_coef<T>(stencil_coef(D, 0.0)), 0); break;
       default: throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
     }
@@ -1484,7 +1491,7 @@ double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps,
 #define PR_INST(T)                                                                                                 \
   template void mg_smooth<T>(cudaStream_t, const LevelCoef&, const T*, const T*, T*, const T*, const T*, int, bool, \
                              double*);                                                                            \
-  template void mg_resid_restrict<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*);           \
+  template void mg_resid_restrict<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, T*);       \
   template void mg_spmv<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, double, bool, T*,    \
                            double*);                                                                              \
   template void screen_project_sq<T>(cudaStream_t, const Screen<T>&, const T*, double*, int);

@@ -26,9 +26,10 @@ LevelCoef level_coef(uint32_t D, uint32_t l, double shift_l);
 template <typename T>
 void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, T* xo, const T* f, const T* ec,
                int mode, bool forward, double* part);
-// fc = P^T (f - A_l e)
+// fc = P^T (f - A_l e); face: scratch of mg_face_entries(depth) values (levels >= 4)
 template <typename T>
-void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc);
+void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc, T* face);
+size_t mg_face_entries(uint32_t depth);
 // finest level only.  xpby: dn = z + beta d, q = A dn; else q = A d.  Stencil part only;
 // per-block (dn or d).q into part.
 template <typename T>

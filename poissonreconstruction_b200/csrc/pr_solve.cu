@@ -81,7 +81,7 @@ struct Multigrid {
   uint32_t D = 0, Dc = 0;
   int sweeps = 1;
   std::vector<LevelCoef> L;
-  std::vector<T*> f, a, e, t;
+  std::vector<T*> f, a, e, t, face;
   T* tables = nullptr;  // [D+1][8*27]
   T* inv = nullptr;
   uint32_t nc = 0;
@@ -96,6 +96,7 @@ struct Multigrid {
     a.assign(D + 1, nullptr);
     e.assign(D + 1, nullptr);
     t.assign(D + 1, nullptr);
+    face.assign(D + 1, nullptr);
     std::vector<T> tab((size_t)(D + 1) * 216, (T)0);
     for (uint32_t l = Dc; l <= D; ++l) {
       L[l] = level_coef(D, l, wg * std::pow(8.0, (double)(D - l)));
@@ -109,6 +110,7 @@ struct Multigrid {
       }
       if (l > Dc) {
         a[l] = c->buf<T>("mg_a" + sfx, nl);
+        if (mg_face_entries(l)) face[l] = c->buf<T>("mg_face" + sfx, mg_face_entries(l));
         if (sweeps > 1) t[l] = c->buf<T>("mg_t" + sfx, nl);
       }
     }
@@ -138,7 +140,7 @@ struct Multigrid {
       mg_smooth<T>(s, L[l], table(l), cur, nxt, fl, nullptr, 0, true, nullptr);
       cur = nxt;
     }
-    mg_resid_restrict<T>(s, L[l], table(l), cur, fl, f[l - 1]);
+    mg_resid_restrict<T>(s, L[l], table(l), cur, fl, f[l - 1], face[l]);
     vcycle(l - 1, f[l - 1], e[l - 1], nullptr);
     // post-smoothing (backward): first sweep on cur + P e_{l-1}; the last sweep writes el
     for (int k = 0; k < sweeps; ++k) {
