@@ -441,7 +441,8 @@ class Context:
         _check(lib().pr_ctx_apply_operator_device(self._h, C.c_void_p(d_x), C.c_void_p(d_y), int(precision)))
 
     KERNELS = {"spmv": 0, "spmv_xpby": 1, "smooth_first": 2, "smooth": 3, "smooth_prolong_dot": 4,
-               "resid_restrict": 5, "stencil_per_node": 6}
+               "resid_restrict": 5, "stencil_per_node": 6, "smooth_prolong_dot_coarse": 7,
+               "resid_restrict_coarse": 8}
 
     def kernel_bench(self, kernel, depth, precision=PR_PRECISION_MIXED, reps=10):
         """(ms per launch, algorithmic bytes per launch) of one solver kernel."""

@@ -677,162 +677,6 @@ __device__ __forceinline__ T prolong_at(const T* ctile, int ux, int uy, int uz) 
   return oz ? (T)0.5 * (y0 + y1) : y0;
 }
 
-// MODE 0: xo = sweep(xi); 1: xo = sweep(0); 2: xo = sweep(xi + P ec).  DOT: part = f.xo
-template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
-__global__ void __launch_bounds__(THREADS, 4) k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo,
-                                                        const T* __restrict__ f, const T* __restrict__ ec, T c0inv,
-                                                        T ce, T cc, const T* __restrict__ table,
-                                                        double* __restrict__ part) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
-  T* fs = tile + TILE;                       // N
-  T* ctile = fs + N;                         // CW^3 (MODE 2)
-  __shared__ uint32_t nb[27], cnb[27];
-  const int res = 1 << D;
-  const uint32_t blk = blockIdx.x;
-  const uint64_t base = (uint64_t)blk * N;
-  uint32_t bx, by, bz;
-  unmorton3(blk, bx, by, bz);
-  const int ox = (int)bx * TB, oy = (int)by * TB, oz = (int)bz * TB;
-  const int t = threadIdx.x;
-  if (MODE != 1) neighbour_bases(nb, bx, by, bz, res >> 4);
-  else if (t < 27) nb[t] = ~0u;  // zero halo
-  if (MODE == 2) load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // ends with a barrier
-  else __syncthreads();  // nb
-  // interior: 4 quads per thread; quad element e at tile offset qoff[e] from element 0
-  int tq[4];  // tile index of each quad's element 0
-  int fq[4];  // f index of each quad's element 0
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int q = t + 256 * r;
-    int lx, ly, lz;
-    quad_coords(q, lx, ly, lz);
-    tq[r] = ps(lx + 1, ly + 1, lz + 1);
-    fq[r] = fidx(lx, ly, lz);
-    const typename Vec4<T>::type fv = ld4(f + base + 4 * q);
-    fs[fq[r]] = fv.x;
-    fs[fq[r] + 512] = fv.y;
-    fs[fq[r] + 1024] = fv.z;
-    fs[fq[r] + 1536] = fv.w;
-    T v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-    if (MODE != 1) {
-      const typename Vec4<T>::type xv = ld4(xi + base + 4 * q);
-      v0 = xv.x; v1 = xv.y; v2 = xv.z; v3 = xv.w;
-      if (MODE == 2) {
-        v0 += prolong_at<T>(ctile, lx + 1, ly + 1, lz + 1);
-        v1 += prolong_at<T>(ctile, lx + 2, ly + 1, lz + 1);
-        v2 += prolong_at<T>(ctile, lx + 1, ly + 2, lz + 1);
-        v3 += prolong_at<T>(ctile, lx + 2, ly + 2, lz + 1);
-      }
-    }
-    // ux = lx + 1 is odd: the x neighbour is in sub-tile (own ^ 1) = own - 1, one column on
-    tile[tq[r]] = v0;
-    tile[tq[r] - SUB + 1] = v1;
-    tile[tq[r] - 2 * SUB + RS] = v2;
-    tile[tq[r] - 3 * SUB + RS + 1] = v3;
-  }
-  // halo (zeros outside the domain; in MODE 1 every neighbour base is ~0u)
-  load_halo<T>(tile, xi, nb, [](int ux, int uy, int uz) { return ps(ux, uy, uz); },
-               [&](uint32_t m) -> T { return MODE == 1 ? (T)0 : __ldg(xi + m); });
-  __syncthreads();
-  if (MODE == 2) {
-    // add P ec on the halo shell (in-domain positions only)
-    for (int i = t; i < 1736; i += THREADS) {
-      int ux, uy, uz;
-      halo_u<16>(i, ux, uy, uz);
-      const int gx = ox - 1 + ux, gy = oy - 1 + uy, gz = oz - 1 + uz;
-      if (gx < 0 || gy < 0 || gz < 0 || gx >= res || gy >= res || gz >= res) continue;
-      tile[ps(ux, uy, uz)] += prolong_at<T>(ctile, ux, uy, uz);
-    }
-    __syncthreads();
-  }
-
-  // Gauss-Seidel: lanes = 8 x-lattice positions x 4 z-pairs; warps = 8 y-lattice rows
-  const int li = t & 7, kp = (t >> 3) & 3, lj = t >> 5;
-  const bool faces = FACES && (ox == 0 || oy == 0 || oz == 0);
-  double acc = 0.0;
-#pragma unroll
-  for (int step = 0; step < 8; ++step) {
-    const int col = FWD ? step : 7 - step;
-    const int cx = col & 1, cy = (col >> 1) & 1, cz = col >> 2;
-    const int own = (1 - cx) | ((1 - cy) << 1) | ((1 - cz) << 2);
-    const int hx = li + cx, hy = lj + cy;
-    const int xm = -cx, xp = 1 - cx, ym = -cy, yp = 1 - cy;
-    const int zm = -cz, zp = 1 - cz;
-    const int so = own * SUB, sxy = (own ^ 3) * SUB;
-    const int sxz = (own ^ 5) * SUB, syz = (own ^ 6) * SUB, sxyz = (own ^ 7) * SUB;
-    const int pr = hy * RS + hx;
-    T nv[2];
-    T pfb = 0, peb = 0;
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const int lk = 2 * kp + s;
-      const int hz = lk + cz;
-      if (s == 0) {
-        const int pz = (hz + zm) * PS + pr;
-        pfb = tile[sxz + pz + xm] + tile[sxz + pz + xp] + tile[syz + pz + ym * RS] + tile[syz + pz + yp * RS];
-        peb = tile[sxyz + pz + ym * RS + xm] + tile[sxyz + pz + ym * RS + xp] + tile[sxyz + pz + yp * RS + xm] +
-              tile[sxyz + pz + yp * RS + xp];
-      }
-      const int p0 = hz * PS + pr;
-      const T peo = tile[sxy + p0 + ym * RS + xm] + tile[sxy + p0 + ym * RS + xp] + tile[sxy + p0 + yp * RS + xm] +
-                    tile[sxy + p0 + yp * RS + xp];
-      const int pa = (hz + zp) * PS + pr;
-      const T pfa = tile[sxz + pa + xm] + tile[sxz + pa + xp] + tile[syz + pa + ym * RS] + tile[syz + pa + yp * RS];
-      const T pea = tile[sxyz + pa + ym * RS + xm] + tile[sxyz + pa + ym * RS + xp] + tile[sxyz + pa + yp * RS + xm] +
-                    tile[sxyz + pa + yp * RS + xp];
-      const T fi = fs[((col * 8 + lj) * 2 + s) * 32 + 8 * kp + li];
-      T v = (fi - ce * (peo + pfb + pfa) - cc * (peb + pea)) * c0inv;
-      if (faces) {
-        const int mask = ((ox == 0 && cx == 0 && li == 0) ? 1 : 0) | ((oy == 0 && cy == 0 && lj == 0) ? 2 : 0) |
-                         ((oz == 0 && cz == 0 && lk == 0) ? 4 : 0);
-        if (mask) {
-          const T* cm = table + 27 * mask;
-          T off = 0;
-#pragma unroll
-          for (int o = 0; o < 27; ++o) {
-            if (o == 13) continue;
-            const int dx = o % 3 - 1, dy = (o / 3) % 3 - 1, dz = o / 9 - 1;
-            const int sub = own ^ ((dx != 0) | ((dy != 0) << 1) | ((dz != 0) << 2));
-            const int ddx = dx == 0 ? 0 : (dx < 0 ? xm : xp), ddy = dy == 0 ? 0 : (dy < 0 ? ym : yp);
-            const int ddz = dz == 0 ? 0 : (dz < 0 ? zm : zp);
-            off += cm[o] * tile[sub * SUB + (hz + ddz) * PS + (hy + ddy) * RS + hx + ddx];
-          }
-          v = (fi - off) / cm[13];
-        }
-      }
-      nv[s] = v;
-      if (DOT) acc += (double)fi * (double)v;  // the node's final value of this sweep
-      pfb = pfa;
-      peb = pea;
-    }
-    tile[so + (2 * kp + cz) * PS + pr] = nv[0];
-    tile[so + (2 * kp + 1 + cz) * PS + pr] = nv[1];
-    __syncthreads();
-  }
-
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    typename Vec4<T>::type v;
-    v.x = tile[tq[r]];
-    v.y = tile[tq[r] - SUB + 1];
-    v.z = tile[tq[r] - 2 * SUB + RS];
-    v.w = tile[tq[r] - 3 * SUB + RS + 1];
-    st4(xo + base + 4 * (t + 256 * r), v);
-  }
-  if (DOT) {
-    typedef cub::BlockReduce<double, THREADS> BR;
-    __shared__ typename BR::TempStorage tmp;
-    const double sum = BR(tmp).Sum(acc);
-    if (t == 0) part[blk] = sum;
-  }
-  (void)fq;
-}
-
-template <typename T>
-constexpr size_t smem_bytes(int mode) {
-  return sizeof(T) * (TILE + N + (mode == 2 ? CW * CW * CW : 0));
-}
 }  // namespace s16
 
 // ------------------------------------------------------------------ 16^3 stencil SpMV (finest level)
@@ -1164,6 +1008,246 @@ constexpr size_t smem_bytes() {
 }
 }  // namespace r16
 
+// ------------------------------------------------------------------ 16^3 smoother (levels >= 4)
+// Multicolour Gauss-Seidel in the block, blocks coupled through the halo values from before
+// the sweep.  Every level's interior stencil has no face couplings, so nodes that share the
+// parity of x and y are uncoupled along z: the sweep has 4 phases, one per (x, y) parity class,
+// each relaxing whole columns of that class at once (forward order (0,0) (1,0) (0,1) (1,1),
+// backward the reverse, each the adjoint of the other).  Thread = one 2x2 quad column over 4 z
+// planes of the SpMV's tile; in phase k it relaxes the class-k column of its quad, sweeping
+// the planes once: a plane's ring around the column gives its in-plane edge sum D (diagonals)
+// and face-adjacent sum F, and the node at z uses D(z), F(z-1), F(z+1), D(z-1), D(z+1).
+// FACES (coarse levels): nodes on the low domain faces use their 27-entry table row, which does
+// couple z-neighbours of the same class; those take the values from before the phase (new
+// values are written after a barrier), a Jacobi step along the column for those rows only.
+namespace g16 {
+constexpr int THREADS = 256, ZT = 4, CW = s16::CW;
+using n16::nat;
+using n16::PS;
+using n16::RS;
+using n16::TILE;
+
+// One phase: new values of the class-CLS column of the thread's quad (planes z0..z0+ZT-1).
+// On the thread's own planes the ring members inside its quad come from registers (v), the
+// other five from the tile (a pair and three scalars); the two halo planes read all eight.
+// ZERO: a forward sweep from zero, in which the classes after CLS are still zero everywhere
+// (their loads are skipped; phase 0 needs none).
+template <typename T, int CLS, bool ZERO>
+__device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int z0, const T (&fv)[ZT][4],
+                                             const T (&v)[ZT][4], T ce, T cc, T c0inv, T (&nv)[ZT]) {
+  typedef typename n16::Pair<T>::type P2;
+  constexpr int CX = CLS & 1, CY = CLS >> 1;
+  constexpr int EDX = CX == 0 ? -1 : 1, EDY = CY == 0 ? -1 : 1;  // direction of the external ring side
+  constexpr int EFX = (CX ^ 1) | (CY << 1), EFY = CX | ((CY ^ 1) << 1), ED = (CX ^ 1) | ((CY ^ 1) << 1);
+  // classes updated before CLS in a forward sweep are 0..CLS-1
+  constexpr bool NFX = !ZERO || EFX < CLS, NFY = !ZERO || EFY < CLS, ND = !ZERO || ED < CLS;
+  if (ZERO && CLS == 0) {
+#pragma unroll
+    for (int k = 0; k < ZT; ++k) nv[k] = fv[k][CLS] * c0inv;
+    return;
+  }
+  const int x = x0 + CX, y = y0 + CY;
+  const T* rbase = tile + nat(x, y, 0);  // ring row y-1, column x-1 of tile plane 0
+  T Dm = 0, Fm = 0, D0 = 0, F0 = 0;
+#pragma unroll
+  for (int p = 0; p < ZT + 2; ++p) {  // local plane z0 + p - 1
+    const T* r0 = rbase + (z0 + p) * PS;
+    T Dp = 0, Fp = 0;
+    if (p >= 1 && p <= ZT) {  // own plane: (x', y), (x, y'), (x', y') from registers
+      const int k = p - 1;
+      const T* rr = r0 + (EDY + 1) * RS;  // external row: columns x-1, x, x+1
+      T q0 = 0, q1 = 0, q2 = 0;
+      if (ND || NFY) {
+        if (CX == 0) {
+          const P2 pr = *reinterpret_cast<const P2*>(rr);
+          q0 = pr.x;
+          q1 = pr.y;
+          if (ND) q2 = rr[2];
+        } else {
+          const P2 pr = *reinterpret_cast<const P2*>(rr + 1);
+          if (ND) q0 = rr[0];
+          q1 = pr.x;
+          q2 = pr.y;
+        }
+      }
+      if (ND) Dp = (q0 + q2) + r0[(1 - EDY) * RS + EDX + 1] + v[k][ED];
+      if (NFY) Fp += q1 + v[k][EFY];
+      if (NFX) Fp += r0[RS + EDX + 1] + v[k][EFX];
+    } else {  // halo plane: the whole ring from the tile
+      T a0, a1, a2, c0v, c1, c2;
+      if (CX == 0) {
+        const P2 pa = *reinterpret_cast<const P2*>(r0);
+        const P2 pc = *reinterpret_cast<const P2*>(r0 + 2 * RS);
+        a0 = pa.x; a1 = pa.y; a2 = r0[2];
+        c0v = pc.x; c1 = pc.y; c2 = r0[2 * RS + 2];
+      } else {
+        const P2 pa = *reinterpret_cast<const P2*>(r0 + 1);
+        const P2 pc = *reinterpret_cast<const P2*>(r0 + 2 * RS + 1);
+        a0 = r0[0]; a1 = pa.x; a2 = pa.y;
+        c0v = r0[2 * RS]; c1 = pc.x; c2 = pc.y;
+      }
+      Dp = (a0 + a2) + (c0v + c2);
+      Fp = (a1 + c1) + (r0[RS] + r0[RS + 2]);
+    }
+    if (p >= 2) {  // node at local z0 + p - 2: edges D0 + Fm + Fp, corners Dm + Dp
+      const int k = p - 2;
+      nv[k] = (fv[k][CLS] - ce * (D0 + Fm + Fp) - cc * (Dm + Dp)) * c0inv;
+    }
+    Dm = D0;
+    Fm = F0;
+    D0 = Dp;
+    F0 = Fp;
+  }
+}
+
+// MODE 0: xo = sweep(xi); 1: xo = sweep(0); 2: xo = sweep(xi + P ec).  DOT: part = f.xo
+template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
+__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
+    k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo, const T* __restrict__ f,
+               const T* __restrict__ ec, T c0inv, T ce, T cc, const T* __restrict__ table,
+               double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
+  T* ctile = tile + TILE;                    // CW^3 (MODE 2)
+  __shared__ uint32_t nb[27], cnb[27];
+  const int res = 1 << D;
+  const uint32_t blk = blockIdx.x;
+  const uint64_t base = (uint64_t)blk * 4096;
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const int ox = (int)bx * 16, oy = (int)by * 16, oz = (int)bz * 16;
+  const int t = threadIdx.x;
+  if (MODE != 1) s16::neighbour_bases(nb, bx, by, bz, res >> 4);
+  else if (t < 27) nb[t] = ~0u;  // zero halo
+  if (MODE == 2) s16::load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // ends with a barrier
+  else __syncthreads();                                                                 // nb
+  const int qi = t & 63, zs = t >> 6;
+  const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
+  const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
+  T fv[ZT][4], v[ZT][4];
+#pragma unroll
+  for (int k = 0; k < ZT; ++k) {
+    const uint64_t m = base + (mq | (s16::sp4(z0 + k) << 2));
+    const typename s16::Vec4<T>::type fq = s16::ld4(f + m);
+    fv[k][0] = fq.x; fv[k][1] = fq.y; fv[k][2] = fq.z; fv[k][3] = fq.w;
+    if (MODE == 1) {
+      v[k][0] = v[k][1] = v[k][2] = v[k][3] = (T)0;
+    } else {
+      const typename s16::Vec4<T>::type xq = s16::ld4(xi + m);
+      v[k][0] = xq.x; v[k][1] = xq.y; v[k][2] = xq.z; v[k][3] = xq.w;
+    }
+  }
+  if (MODE == 2) {
+    // P ec on the quad column: coarse (cx, cx+1) x (cy, cy+1) at the coarse planes z0/2 .. z0/2+2
+    // (z0 even: planes z0, z0+2 lie on a coarse plane, z0+1, z0+3 halfway between two)
+    const int ax = x0 / 2 + 1, ay = y0 / 2 + 1, az = z0 / 2 + 1;
+    T pl[3][4];
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+      const T* c = ctile + ((az + w) * CW + ay) * CW + ax;
+      const T c00 = c[0], c10 = c[1], c01 = c[CW], c11 = c[CW + 1];
+      pl[w][0] = c00;
+      pl[w][1] = (T)0.5 * (c00 + c10);
+      pl[w][2] = (T)0.5 * (c00 + c01);
+      pl[w][3] = (T)0.25 * ((c00 + c10) + (c01 + c11));
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      v[0][e] += pl[0][e];
+      v[1][e] += (T)0.5 * (pl[0][e] + pl[1][e]);
+      v[2][e] += pl[1][e];
+      v[3][e] += (T)0.5 * (pl[1][e] + pl[2][e]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < ZT; ++k) {
+    T* p0 = tile + nat(x0 + 1, y0 + 1, z0 + k + 1);
+    p0[0] = v[k][0];
+    p0[1] = v[k][1];
+    p0[RS] = v[k][2];
+    p0[RS + 1] = v[k][3];
+  }
+  s16::load_halo<T>(tile, xi, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); },
+                    [&](uint32_t m) -> T { return MODE == 1 ? (T)0 : __ldg(xi + m); });
+  __syncthreads();
+  if (MODE == 2) {  // add P ec on the halo shell (in-domain positions only)
+    for (int i = t; i < 1736; i += THREADS) {
+      int ux, uy, uz;
+      halo_u<16>(i, ux, uy, uz);
+      const int gx = ox - 1 + ux, gy = oy - 1 + uy, gz = oz - 1 + uz;
+      if (gx < 0 || gy < 0 || gz < 0 || gx >= res || gy >= res || gz >= res) continue;
+      tile[nat(ux, uy, uz)] += s16::prolong_at<T>(ctile, ux, uy, uz);
+    }
+    __syncthreads();
+  }
+  const bool faces = FACES && (ox == 0 || oy == 0 || oz == 0);
+#pragma unroll
+  for (int ph = 0; ph < 4; ++ph) {
+    const int cls = FWD ? ph : 3 - ph;
+    const int cx = cls & 1, cy = cls >> 1;
+    const int x = x0 + cx, y = y0 + cy;
+    T nv[ZT];
+    constexpr bool ZERO = MODE == 1 && FWD;
+    switch (cls) {
+      case 0: relax_column<T, 0, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      case 1: relax_column<T, 1, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      case 2: relax_column<T, 2, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      default: relax_column<T, 3, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+    }
+    if (faces) {  // low-domain-face nodes of this column: their table rows, neighbours from the tile
+#pragma unroll 1
+      for (int k = 0; k < ZT; ++k) {
+        const int z = z0 + k;
+        const int mask = ((ox + x) == 0) | (((oy + y) == 0) << 1) | (((oz + z) == 0) << 2);
+        if (!mask) continue;
+        const T* cm = table + 27 * mask;
+        const int ei = nat(x + 1, y + 1, z + 1);
+        T off = 0;
+#pragma unroll 1
+        for (int o = 0; o < 27; ++o) {
+          if (o == 13) continue;
+          off += cm[o] * tile[ei + (o % 3 - 1) + RS * ((o / 3) % 3 - 1) + PS * (o / 9 - 1)];
+        }
+        const T fk = k == 0 ? fv[0][cls] : (k == 1 ? fv[1][cls] : (k == 2 ? fv[2][cls] : fv[3][cls]));
+        const T nvk = (fk - off) / cm[13];
+        if (k == 0) nv[0] = nvk;
+        else if (k == 1) nv[1] = nvk;
+        else if (k == 2) nv[2] = nvk;
+        else nv[3] = nvk;
+      }
+    }
+    if (FACES) __syncthreads();  // same-class column neighbours were read with their old values
+#pragma unroll
+    for (int k = 0; k < ZT; ++k) {
+      v[k][cls] = nv[k];
+      tile[nat(x + 1, y + 1, z0 + k + 1)] = nv[k];
+    }
+    __syncthreads();
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < ZT; ++k) {
+    const uint64_t m = base + (mq | (s16::sp4(z0 + k) << 2));
+    typename s16::Vec4<T>::type o;
+    o.x = v[k][0]; o.y = v[k][1]; o.z = v[k][2]; o.w = v[k][3];
+    s16::st4(xo + m, o);
+    if (DOT)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc += (double)fv[k][e] * (double)v[k][e];
+  }
+  if (DOT) {
+    typedef cub::BlockReduce<double, THREADS> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double sum = BR(tmp).Sum(acc);
+    if (t == 0) part[blk] = sum;
+  }
+}
+template <typename T>
+constexpr size_t smem_bytes(int mode) {
+  return sizeof(T) * (TILE + (mode == 2 ? CW * CW * CW : 0));
+}
+}  // namespace g16
+
 template <typename T>
 DevCoef<T> dev_coef(const LevelCoef& L, const T* table) {
   DevCoef<T> k;
@@ -1230,9 +1314,9 @@ void smooth_dispatch(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f,
 template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
 void launch_s16(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const LevelCoef& L,
                 const T* table, double* part) {
-  const size_t sm = s16::smem_bytes<T>(MODE);
-  allow_smem(s16::k_smooth16<T, MODE, DOT, FWD, FACES>, sm);
-  s16::k_smooth16<T, MODE, DOT, FWD, FACES><<<1u << (3 * (D - 4)), s16::THREADS, sm, s>>>(
+  const size_t sm = g16::smem_bytes<T>(MODE);
+  allow_smem(g16::k_smooth16<T, MODE, DOT, FWD, FACES>, sm);
+  g16::k_smooth16<T, MODE, DOT, FWD, FACES><<<1u << (3 * (D - 4)), g16::THREADS, sm, s>>>(
       D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part);
 }
 
@@ -1442,7 +1526,9 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
   k_fill<T><<<g, 256, 0, s>>>(w, n, 3u);
   k_fill<T><<<g, 256, 0, s>>>(ec, nc, 4u);
   PR_CHECK_LAUNCH();
-  const LevelCoef Lf = level_coef(D, D, 0.0), Lc = level_coef(D + 1, D, 0.0);  // fine level, a coarse level
+  // the finest level (no low-face rows: the variants that dominate a solve) and, for ids 7-8,
+  // a coarse level (low-face table rows)
+  const LevelCoef Lf = level_coef(D, D, 0.0), Lc = level_coef(D + 1, D, 0.0);
   std::vector<T> tab(216);
   for (int m = 0; m < 8; ++m)
     for (int o = 0; o < 27; ++o) tab[27 * m + o] = (T)Lc.table[m][o];
@@ -1453,16 +1539,20 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
     switch (kid) {
       case 0: mg_spmv<T>(s, Lf, table, nullptr, x, nullptr, 0.0, false, y, part); break;
       case 1: mg_spmv<T>(s, Lf, table, f, x, w, 0.5, true, y, part); break;
-      case 2: mg_smooth<T>(s, Lc, table, nullptr, y, f, nullptr, 1, true, nullptr); break;
-      case 3: mg_smooth<T>(s, Lc, table, x, y, f, nullptr, 0, true, nullptr); break;
-      case 4: mg_smooth<T>(s, Lc, table, x, y, f, ec, 2, false, part); break;
-      case 5: mg_resid_restrict<T>(s, Lc, table, x, f, ec, face); break;
+      case 2: mg_smooth<T>(s, Lf, table, nullptr, y, f, nullptr, 1, true, nullptr); break;
+      case 3: mg_smooth<T>(s, Lf, table, x, y, f, nullptr, 0, true, nullptr); break;
+      case 4: mg_smooth<T>(s, Lf, table, x, y, f, ec, 2, false, part); break;
+      case 5: mg_resid_restrict<T>(s, Lf, table, x, f, ec, face); break;
+      case 7: mg_smooth<T>(s, Lc, table, x, y, f, ec, 2, false, part); break;
+      case 8: mg_resid_restrict<T>(s, Lc, table, x, f, ec, face); break;
       case 6: stencil_apply<T>(s, D, x, nullptr, y, cast_coef<T>(stencil_coef(D, 0.0)), 0); break;
       default: throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
     }
   };
   const double nb = (double)n * es;
-  const double algo[] = {2 * nb, 4 * nb, 2 * nb, 3 * nb, 3 * nb + nb / 8, 2 * nb + nb / 8, 2 * nb};
+  const double algo[] = {2 * nb, 4 * nb, 2 * nb, 3 * nb, 3 * nb + nb / 8, 2 * nb + nb / 8, 2 * nb,
+                         3 * nb + nb / 8, 2 * nb + nb / 8};
+  if (kid < 0 || kid > 8) throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
   *bytes = algo[kid];
   run();
   PR_CUDA(cudaStreamSynchronize(s));
