@@ -1101,11 +1101,15 @@ __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int 
 }
 
 // MODE 0: xo = sweep(xi); 1: xo = sweep(0); 2: xo = sweep(xi + P ec).  DOT: part = f.xo
+// MODE 3 (finest level, forward): first the CG update x += alpha d, r -= alpha q in place
+// (pointwise), then xo = sweep(0) with f = the new r; part = per-block sums of r^2.  A sweep
+// from zero reads no halo, so updating r in place is race-free.
 template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
 __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo, const T* __restrict__ f,
                const T* __restrict__ ec, T c0inv, T ce, T cc, const T* __restrict__ table,
-               double* __restrict__ part) {
+               double* __restrict__ part, CgFuse<T> cg) {
+  static_assert(MODE != 3 || (FWD && !FACES), "the fused CG update is a forward sweep on the finest level");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
   T* ctile = tile + TILE;                    // CW^3 (MODE 2)
@@ -1117,7 +1121,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   unmorton3(blk, bx, by, bz);
   const int ox = (int)bx * 16, oy = (int)by * 16, oz = (int)bz * 16;
   const int t = threadIdx.x;
-  if (MODE != 1) s16::neighbour_bases(nb, bx, by, bz, res >> 4);
+  constexpr bool FROM_ZERO = MODE == 1 || MODE == 3;
+  if (!FROM_ZERO) s16::neighbour_bases(nb, bx, by, bz, res >> 4);
   else if (t < 27) nb[t] = ~0u;  // zero halo
   if (MODE == 2) s16::load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // ends with a barrier
   else __syncthreads();                                                                 // nb
@@ -1125,12 +1130,26 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
   const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
   T fv[ZT][4], v[ZT][4];
+  double rr = 0.0;
 #pragma unroll
   for (int k = 0; k < ZT; ++k) {
     const uint64_t m = base + (mq | (s16::sp4(z0 + k) << 2));
-    const typename s16::Vec4<T>::type fq = s16::ld4(f + m);
+    typename s16::Vec4<T>::type fq;
+    if (MODE == 3) {  // the CG update of this quad (plain loads: x and r are written here)
+      typedef typename s16::Vec4<T>::type V4;
+      V4 xq = *reinterpret_cast<const V4*>(cg.x + m);
+      const V4 dq = s16::ld4(cg.d + m), qq = s16::ld4(cg.q + m);
+      fq = *reinterpret_cast<const V4*>(cg.r + m);
+      xq.x += cg.alpha * dq.x; xq.y += cg.alpha * dq.y; xq.z += cg.alpha * dq.z; xq.w += cg.alpha * dq.w;
+      fq.x -= cg.alpha * qq.x; fq.y -= cg.alpha * qq.y; fq.z -= cg.alpha * qq.z; fq.w -= cg.alpha * qq.w;
+      s16::st4(cg.x + m, xq);
+      s16::st4(cg.r + m, fq);
+      rr += (double)fq.x * fq.x + (double)fq.y * fq.y + (double)fq.z * fq.z + (double)fq.w * fq.w;
+    } else {
+      fq = s16::ld4(f + m);
+    }
     fv[k][0] = fq.x; fv[k][1] = fq.y; fv[k][2] = fq.z; fv[k][3] = fq.w;
-    if (MODE == 1) {
+    if (FROM_ZERO) {
       v[k][0] = v[k][1] = v[k][2] = v[k][3] = (T)0;
     } else {
       const typename s16::Vec4<T>::type xq = s16::ld4(xi + m);
@@ -1168,7 +1187,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     p0[RS + 1] = v[k][3];
   }
   s16::load_halo<T>(tile, xi, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); },
-                    [&](uint32_t m) -> T { return MODE == 1 ? (T)0 : __ldg(xi + m); });
+                    [&](uint32_t m) -> T { return FROM_ZERO ? (T)0 : __ldg(xi + m); });
   __syncthreads();
   if (MODE == 2) {  // add P ec on the halo shell (in-domain positions only)
     for (int i = t; i < 1736; i += THREADS) {
@@ -1187,7 +1206,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     const int cx = cls & 1, cy = cls >> 1;
     const int x = x0 + cx, y = y0 + cy;
     T nv[ZT];
-    constexpr bool ZERO = MODE == 1 && FWD;
+    constexpr bool ZERO = FROM_ZERO && FWD;
     switch (cls) {
       case 0: relax_column<T, 0, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
       case 1: relax_column<T, 1, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
@@ -1235,10 +1254,10 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc += (double)fv[k][e] * (double)v[k][e];
   }
-  if (DOT) {
+  if (DOT || MODE == 3) {
     typedef cub::BlockReduce<double, THREADS> BR;
     __shared__ typename BR::TempStorage tmp;
-    const double sum = BR(tmp).Sum(acc);
+    const double sum = BR(tmp).Sum(MODE == 3 ? rr : acc);
     if (t == 0) part[blk] = sum;
   }
 }
@@ -1317,7 +1336,7 @@ void launch_s16(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, cons
   const size_t sm = g16::smem_bytes<T>(MODE);
   allow_smem(g16::k_smooth16<T, MODE, DOT, FWD, FACES>, sm);
   g16::k_smooth16<T, MODE, DOT, FWD, FACES><<<1u << (3 * (D - 4)), g16::THREADS, sm, s>>>(
-      D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part);
+      D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, CgFuse<T>());
 }
 
 template <typename T, int MODE, bool DOT, bool FWD>
@@ -1410,6 +1429,18 @@ void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, 
   const DevCoef<T> k = dev_coef<T>(L, table);
   if (tile_for(D) == 16) smooth16_dispatch<T>(s, L, D, xi, xo, f, ec, table, mode, forward, part);
   else smooth_dispatch<T, 8>(s, D, xi, xo, f, ec, k, mode, forward, part);
+  PR_CHECK_LAUNCH();
+}
+
+template <typename T>
+void mg_cg_update_presmooth(cudaStream_t s, const LevelCoef& L, const T* table, const CgFuse<T>& cg, T* xo,
+                            double* part) {
+  const uint32_t D = L.depth;
+  if (D < 4 || L.has_faces) throw Error(PR_ERR_INTERNAL, "the fused CG update needs the finest level, depth >= 4");
+  const size_t sm = g16::smem_bytes<T>(3);
+  allow_smem(g16::k_smooth16<T, 3, false, true, false>, sm);
+  g16::k_smooth16<T, 3, false, true, false><<<1u << (3 * (D - 4)), g16::THREADS, sm, s>>>(
+      D, nullptr, xo, nullptr, nullptr, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, cg);
   PR_CHECK_LAUNCH();
 }
 
@@ -1582,6 +1613,7 @@ double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps,
   template void mg_smooth<T>(cudaStream_t, const LevelCoef&, const T*, const T*, T*, const T*, const T*, int, bool, \
                              double*);                                                                            \
   template void mg_resid_restrict<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, T*);       \
+  template void mg_cg_update_presmooth<T>(cudaStream_t, const LevelCoef&, const T*, const CgFuse<T>&, T*, double*); \
   template void mg_spmv<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, double, bool, T*,    \
                            double*);                                                                              \
   template void screen_project_sq<T>(cudaStream_t, const Screen<T>&, const T*, double*, int);

@@ -26,6 +26,19 @@ LevelCoef level_coef(uint32_t D, uint32_t l, double shift_l);
 template <typename T>
 void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, T* xo, const T* f, const T* ec,
                int mode, bool forward, double* part);
+// CG update x += alpha d, r -= alpha q (in place) fused with the first pre-smoothing sweep from
+// zero of the finest level (depth >= 4): xo = sweep(0) on the new r; part = per-block r.r
+template <typename T>
+struct CgFuse {
+  T* x = nullptr;
+  const T* d = nullptr;
+  const T* q = nullptr;
+  T* r = nullptr;
+  T alpha = 0;
+};
+template <typename T>
+void mg_cg_update_presmooth(cudaStream_t s, const LevelCoef& L, const T* table, const CgFuse<T>& cg, T* xo,
+                            double* part);
 // fc = P^T (f - A_l e); face: scratch of mg_face_entries(depth) values (levels >= 4)
 template <typename T>
 void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc, T* face);

@@ -126,7 +126,8 @@ struct Multigrid {
   const T* table(uint32_t l) const { return tables + (size_t)l * 216; }
 
   // el = V(fl); at the finest level `part` (nullable) receives per-block fl.el partials.
-  void vcycle(uint32_t l, const T* fl, T* el, double* part) {
+  // presmoothed: the first pre-smoothing sweep of this level is already in a_l.
+  void vcycle(uint32_t l, const T* fl, T* el, double* part, bool presmoothed = false) {
     cudaStream_t s = c->stream;
     if (l == Dc) {
       dense_solve<T>(s, nc, inv, fl, el);
@@ -134,7 +135,7 @@ struct Multigrid {
     }
     // pre-smoothing (forward) from zero; result in a_l
     T* cur = a[l];
-    mg_smooth<T>(s, L[l], table(l), nullptr, cur, fl, nullptr, 1, true, nullptr);
+    if (!presmoothed) mg_smooth<T>(s, L[l], table(l), nullptr, cur, fl, nullptr, 1, true, nullptr);
     for (int k = 1; k < sweeps; ++k) {
       T* nxt = (cur == a[l]) ? t[l] : a[l];
       mg_smooth<T>(s, L[l], table(l), cur, nxt, fl, nullptr, 0, true, nullptr);
@@ -150,8 +151,26 @@ struct Multigrid {
       cur = nxt;
     }
   }
-  // z = M r; returns r.z
-  double apply(const T* r, T* z) {
+  // The CG update can be fused with the first pre-smoothing sweep of the finest level.
+  bool fuses_cg_update() const { return D >= 4 && D > Dc; }
+  // x += alpha d, r -= alpha q, first pre-smoothing sweep of r into a_D; returns r.r
+  double cg_update_presmooth(double alpha, const T* d, const T* q, T* x, T* r) {
+    double* part = c->buf<double>("mg_part", mg_blocks(D));
+    double* out = c->buf<double>("mg_out", 1);
+    CgFuse<T> cg;
+    cg.x = x;
+    cg.d = d;
+    cg.q = q;
+    cg.r = r;
+    cg.alpha = (T)alpha;
+    mg_cg_update_presmooth<T>(c->stream, L[D], table(D), cg, a[D], part);
+    sum_parts(c->stream, part, (int)mg_blocks(D), 0.0, part, 0, out);
+    PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    return c->h_scalars[0];
+  }
+  // z = M r; returns r.z.  presmoothed: a_D already holds the first sweep on r.
+  double apply(const T* r, T* z, bool presmoothed = false) {
     const uint64_t n = 1ull << (3 * D);
     if (D == Dc) {
       dense_solve<T>(c->stream, nc, inv, r, z);
@@ -159,7 +178,7 @@ struct Multigrid {
     }
     double* part = c->buf<double>("mg_part", mg_blocks(D));
     double* out = c->buf<double>("mg_out", 1);
-    vcycle(D, r, z, part);
+    vcycle(D, r, z, part, presmoothed);
     sum_parts(c->stream, part, (int)mg_blocks(D), 0.0, part, 0, out);
     PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     c->sync();
@@ -261,7 +280,8 @@ PcgResult pcg(pr_context* c, CgOperator<T>& A, Multigrid<T>& M, const T* b, T* x
       break;
     }
     const double alpha = rz / dq;
-    rr = cg_update<T>(c, n, alpha, d, q, x, r);
+    const bool fused = M.fuses_cg_update();
+    rr = fused ? M.cg_update_presmooth(alpha, d, q, x, r) : cg_update<T>(c, n, alpha, d, q, x, r);
     res.iters = it + 1;
     res.rr = rr;
     if (!std::isfinite(rr)) {
@@ -273,7 +293,7 @@ PcgResult pcg(pr_context* c, CgOperator<T>& A, Multigrid<T>& M, const T* b, T* x
       PR_CUDA(cudaMemcpyAsync(dA, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
       d = dA;
     }
-    const double rz_new = M.apply(r, z);
+    const double rz_new = M.apply(r, z, fused);
     beta = rz_new / rz;
     rz = rz_new;
   }
