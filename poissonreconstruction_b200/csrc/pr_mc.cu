@@ -348,37 +348,54 @@ __device__ void mc_load_tile(double* tile, const double* __restrict__ x, uint32_
   }
 }
 
-// case of local cell (lx,ly,lz) of block origin (ox,oy,oz); repeats of the corner node at
-// the top boundary (grid position res) are accumulated like the crate's evaluate()
-__device__ __forceinline__ uint32_t mc_tile_case(const double* tile, int lx, int ly, int lz, int ox, int oy, int oz,
-                                                 int res, double iso) {
-  uint32_t mc = 0;
+// Inside/outside bits of the tile's 17^3 corner positions, one 17-bit word per (y, z) row:
+// bit tx of row (ty, tz) is (corner value < iso) for grid position (o + t).  The value at a grid
+// position equal to res on k axes is the node value added 2^k times in sequence, like the crate's
+// evaluate() at the top boundary.  Every cell then reads 4 words instead of 8 doubles.
+__device__ __forceinline__ void mc_build_masks(const double* tile, uint32_t* mask, int ox, int oy, int oz, int res,
+                                               double iso) {
+  for (int r = threadIdx.x; r < MCW * MCW; r += blockDim.x) {
+    const int ty = r % MCW, tz = r / MCW;
+    const int myz = ((oy + ty == res) ? 2 : 1) * ((oz + tz == res) ? 2 : 1);
+    const double* row = tile + (tz * MCW + ty) * MCW;
+    uint32_t m = 0;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int cx = c_co[k][0], cy = c_co[k][1], cz = c_co[k][2];
-    const double s = tile[((lz + cz) * MCW + (ly + cy)) * MCW + (lx + cx)];
-    const int m = ((ox + lx + cx == res) ? 2 : 1) * ((oy + ly + cy == res) ? 2 : 1) * ((oz + lz + cz == res) ? 2 : 1);
-    double v = 0.0;
-    for (int i = 0; i < m; ++i) v = xadd(v, s);
-    if (v < iso) mc |= 1u << k;
+    for (int tx = 0; tx < MCW; ++tx) {
+      const double s = row[tx];
+      const int mult = myz * ((ox + tx == res) ? 2 : 1);
+      double v = s;
+      for (int i = 1; i < mult; ++i) v = xadd(v, s);
+      m |= (uint32_t)(v < iso) << tx;
+    }
+    mask[r] = m;
   }
-  return mc;
+}
+// case of local cell (lx, ly, lz) from the row masks (corner order of c_co)
+__device__ __forceinline__ uint32_t mc_mask_case(const uint32_t* mask, int lx, int ly, int lz) {
+  const uint32_t m00 = mask[lz * MCW + ly] >> lx, m10 = mask[lz * MCW + ly + 1] >> lx;
+  const uint32_t m01 = mask[(lz + 1) * MCW + ly] >> lx, m11 = mask[(lz + 1) * MCW + ly + 1] >> lx;
+  return (m00 & 1u) | ((m00 >> 1) & 1u) << 1 | ((m10 >> 1) & 1u) << 2 | (m10 & 1u) << 3 | (m01 & 1u) << 4 |
+         ((m01 >> 1) & 1u) << 5 | ((m11 >> 1) & 1u) << 6 | (m11 & 1u) << 7;
 }
 
 __global__ void __launch_bounds__(256) k_mc_block_count(const double* __restrict__ x, uint32_t D, double iso,
                                                         uint32_t* __restrict__ blockcnt) {
   __shared__ double tile[MCW * MCW * MCW];
+  __shared__ uint32_t mask[MCW * MCW];
   const int res = 1 << D;
   const uint32_t blk = blockIdx.x;
   uint32_t bx, by, bz;
   unmorton3(blk, bx, by, bz);
   mc_load_tile(tile, x, blk, res);
   __syncthreads();
+  mc_build_masks(tile, mask, bx * 16, by * 16, bz * 16, res, iso);
+  __syncthreads();
+  // thread = one x row of 16 cells
+  const int ly = threadIdx.x & 15, lz = threadIdx.x >> 4;
   int cnt = 0;
-  for (int i = threadIdx.x; i < 4096; i += 256) {
-    uint32_t lx, ly, lz;
-    unmorton3((uint32_t)i, lx, ly, lz);
-    const uint32_t mc = mc_tile_case(tile, lx, ly, lz, bx * 16, by * 16, bz * 16, res, iso);
+#pragma unroll 4
+  for (int lx = 0; lx < 16; ++lx) {
+    const uint32_t mc = mc_mask_case(mask, lx, ly, lz);
     cnt += (mc != 0u && mc != 255u);
   }
   typedef cub::BlockReduce<int, 256> BR;
@@ -394,11 +411,14 @@ __global__ void __launch_bounds__(256) k_mc_block_emit(const double* __restrict_
                                                        uint32_t* __restrict__ acell, uint8_t* __restrict__ acase,
                                                        uint32_t* __restrict__ nedge, uint32_t* __restrict__ ntri) {
   __shared__ double tile[MCW * MCW * MCW];
+  __shared__ uint32_t mask[MCW * MCW];
   const int res = 1 << D;
   const uint32_t blk = ablk[blockIdx.x];
   uint32_t bx, by, bz;
   unmorton3(blk, bx, by, bz);
   mc_load_tile(tile, x, blk, res);
+  __syncthreads();
+  mc_build_masks(tile, mask, bx * 16, by * 16, bz * 16, res, iso);
   __syncthreads();
   typedef cub::BlockScan<int, 256> BS;
   __shared__ typename BS::TempStorage tmp;
@@ -407,7 +427,7 @@ __global__ void __launch_bounds__(256) k_mc_block_emit(const double* __restrict_
     const int i = chunk * 256 + threadIdx.x;  // Morton-local cell index
     uint32_t lx, ly, lz;
     unmorton3((uint32_t)i, lx, ly, lz);
-    const uint32_t mc = mc_tile_case(tile, lx, ly, lz, bx * 16, by * 16, bz * 16, res, iso);
+    const uint32_t mc = mc_mask_case(mask, (int)lx, (int)ly, (int)lz);
     const int active = (mc != 0u && mc != 255u);
     int off, tot;
     BS(tmp).ExclusiveSum(active, off, tot);
