@@ -138,6 +138,21 @@ __global__ void k_xpby(uint64_t n, const T* __restrict__ z, T beta, T* __restric
     d[i] = z[i] + beta * d[i];
 }
 
+// y = (float)x with per-block sums of x^2 (FP64), one pass
+__global__ void k_convert_norm(uint64_t n, const double* __restrict__ x, float* __restrict__ y,
+                               double* __restrict__ part) {
+  double s = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    y[i] = (float)v;
+    s += v * v;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 template <typename Tin, typename Tout>
 __global__ void k_scale_convert(uint64_t n, double a, const Tin* __restrict__ x, Tout* __restrict__ y) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -344,6 +359,18 @@ double cg_update(pr_context* c, uint64_t n, double alpha, const T* d, const T* q
   PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   c->sync();
   return c->h_scalars[0];
+}
+
+double convert_norm(pr_context* c, const double* x, float* y, uint64_t n) {
+  double* part = c->buf<double>("dot_part", kDotBlocks);
+  double* out = c->buf<double>("dot_out", 1);
+  k_convert_norm<<<kDotBlocks, kThreads, 0, c->stream>>>(n, x, y, part);
+  PR_CHECK_LAUNCH();
+  k_sum_final<<<1, 32, 0, c->stream>>>(part, kDotBlocks, out);
+  PR_CHECK_LAUNCH();
+  PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  c->sync();
+  return std::sqrt(c->h_scalars[0]);
 }
 
 template <typename T>

@@ -61,6 +61,8 @@ double cg_update(pr_context* c, uint64_t n, double alpha, const T* d, const T* q
 template <typename T>
 void xpby(cudaStream_t s, uint64_t n, const T* z, double beta, T* d);
 // y = a * x  (conversion between types allowed)
+// y = (float)x; returns ||x|| (fixed-order FP64 sum)
+double convert_norm(pr_context* c, const double* x, float* y, uint64_t n);
 template <typename Tin, typename Tout>
 void scale_convert(cudaStream_t s, uint64_t n, double a, const Tin* x, Tout* y);
 // y += a * x  (conversion allowed)

@@ -345,7 +345,10 @@ void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double*
   st.refinement_steps = 0;
   st.solve_bytes = 0.0;
   PR_CUDA(cudaMemsetAsync(xA, 0, n * sizeof(double), s));
-  const double bn = std::sqrt(dot<double>(c, b, b, n));
+  // mixed: the FP32 system is the current FP64 residual rounded (unscaled: residuals stay far
+  // above the bottom of the FP32 range), its norm computed in the same pass
+  float* r32 = mixed ? c->buf<float>("r32", n) : nullptr;
+  const double bn = mixed ? convert_norm(c, b, r32, n) : std::sqrt(dot<double>(c, b, b, n));
   if (bn == 0.0) {
     st.rel_residual = 0.0;
     st.converged = 1;
@@ -358,9 +361,10 @@ void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double*
   const double per_iter = iter_bytes(n, es, c->P_in, es) + vcycle_bytes(D, es, sweeps);
   const double resid_bytes = 36.0 * n + c->P_in * 2.0 * (8.0 * 8.0 + 32.0) + 8.0 * n;  // update+residual, norm
 
-  // x <- x + scale * e and r = b - A x (FP64); returns ||r||.  x ping-pongs between xA and xB.
+  // x <- x + scale * e and r = b - A x (FP64); with_norm: returns ||r|| (else 0).  x ping-pongs
+  // between xA and xB.
   double* x = xA;
-  auto update_residual = [&](const void* e, bool e_is_float, double scale) -> double {
+  auto update_residual = [&](const void* e, bool e_is_float, double scale, bool with_norm = true) -> double {
     if (fused) {
       double* xn = (x == xA) ? xB : xA;
       if (e_is_float) mg_resid_update<float>(s, L64, x, (const float*)e, scale, xn, b, r);
@@ -375,7 +379,7 @@ void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double*
       else axpy<double, double>(s, n, scale, (const double*)e, x);
       A64.residual(s, x, b, r);
     }
-    return std::sqrt(dot<double>(c, r, r, n));
+    return with_norm ? std::sqrt(dot<double>(c, r, r, n)) : 0.0;
   };
 
   double rn = bn;
@@ -386,15 +390,14 @@ void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double*
     A32.init(c, wg);
     Multigrid<float> M32;
     M32.init(c, D, wg, sweeps);
-    float* r32 = c->buf<float>("r32", n);
     float* e32 = c->buf<float>("e32", n);
     const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
     while (rn > target * bn && used < max_iters) {
-      scale_convert<double, float>(s, n, 1.0 / rn, rsrc, r32);
       const double tol = std::max(inner, 0.5 * target * bn / rn);
-      const PcgResult pr_ = pcg<float>(c, A32, M32, r32, e32, tol, max_iters - used);
+      const PcgResult pr_ = pcg<float>(c, A32, M32, r32, e32, tol * rn, max_iters - used);
       used += pr_.iters;
-      const double rn_new = update_residual(e32, true, rn);
+      update_residual(e32, true, 1.0, false);
+      const double rn_new = convert_norm(c, r, r32, n);
       rsrc = r;
       st.refinement_steps++;
       st.solve_bytes += pr_.iters * per_iter + 12.0 * n + resid_bytes;
