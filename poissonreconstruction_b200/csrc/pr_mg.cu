@@ -831,13 +831,16 @@ constexpr size_t smem_bytes() {
 // ------------------------------------------------------------------ 16^3 residual + restriction
 // Two launches, no redundant work.  k_resid16: r = f - A e on the block's 16^3 nodes (the
 // SpMV's tile and quad columns), then (a) the part of the restriction to the block's 8^3 coarse
-// nodes that comes from its own fine nodes, and (b) the residual of its three high faces
-// (local 15 on an axis) into a face buffer of 3 x 256 values per block.  k_restrict_faces then
-// adds, to the coarse nodes on each block's low faces, the contributions of the fine nodes at
-// local -1, read from the low neighbours' face buffers.  Restriction: coarse c gathers fine
-// 2c-1, 2c, 2c+1 per axis with weights 1/2, 1, 1/2.
+// nodes that comes from its own fine nodes, and (b) the restriction partials its high faces
+// (local 15) owe the coarse nodes of its high neighbours: per face the sum over the face's other
+// two axes (8 x 8), per edge over the remaining axis (8), and the corner (1), into a face buffer
+// of 224 values per block.  k_restrict_faces adds to the coarse nodes on each block's low faces
+// these partials of its low neighbours, scaled by 1/2 per crossed axis.  Restriction: coarse c
+// gathers fine 2c-1, 2c, 2c+1 per axis with weights 1/2, 1, 1/2.
 namespace r16 {
-constexpr int N = 4096, THREADS = 256, ZT = 4, FACE = 768;
+constexpr int N = 4096, THREADS = 256, ZT = 4, FACE = 224;
+// face buffer layout: [0,64) x face (cy + 8 cz), [64,128) y face (cx + 8 cz), [128,192) z face
+// (cx + 8 cy), [192,200) xy edge (cz), [200,208) xz edge (cy), [208,216) yz edge (cx), 216 corner
 constexpr int RSR = 20, PSR = 16 * RSR + 8, RTILE = 16 * PSR;  // half-warps of the restriction on disjoint banks
 __device__ __forceinline__ int ridx(int x, int y, int z) { return z * PSR + y * RSR + x; }  // local coordinates
 
@@ -954,27 +957,55 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     }
     fc[cbase + ci] = s;
   }
-  // high faces of r: plane 0 x = 15 (a = y, b = z), 1 y = 15 (a = x, b = z), 2 z = 15 (a = x, b = y)
-  T* fb = face + (uint64_t)blk * FACE;
+  // restriction partials of the high faces, edges and corner
+  {
+    T* fb = face + (uint64_t)blk * FACE;
+    auto w = [](int d) { return (T)(d == 0 ? 1.0 : 0.5); };
+    if (t < 192) {  // faces: the two free axes restricted, the face axis at local 15
+      const int axis = t >> 6, i = t & 7, j = (t >> 3) & 7;
+      T acc = 0;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const int a = t & 15, b = t >> 4;
-    const int x = k == 0 ? 15 : a, y = k == 1 ? 15 : (k == 0 ? a : b), z = k == 2 ? 15 : b;
-    fb[k * 256 + t] = rt[ridx(x, y, z)];
+      for (int dj = -1; dj <= 1; ++dj) {
+        const int fj = 2 * j + dj;
+        if (fj < 0) continue;
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          const int fi = 2 * i + di;
+          if (fi < 0) continue;
+          const int x = axis == 0 ? 15 : fi, y = axis == 1 ? 15 : (axis == 0 ? fi : fj), z = axis == 2 ? 15 : fj;
+          acc += w(di) * w(dj) * rt[ridx(x, y, z)];
+        }
+      }
+      fb[t] = acc;
+    } else if (t < 216) {  // edges: the free axis restricted
+      const int e = (t - 192) >> 3, i = (t - 192) & 7;
+      T acc = 0;
+#pragma unroll
+      for (int di = -1; di <= 1; ++di) {
+        const int fi = 2 * i + di;
+        if (fi < 0) continue;
+        const int x = e == 2 ? fi : 15, y = e == 1 ? fi : 15, z = e == 0 ? fi : 15;
+        acc += w(di) * rt[ridx(x, y, z)];
+      }
+      fb[t] = acc;
+    } else if (t == 216) {
+      fb[216] = rt[ridx(15, 15, 15)];
+    }
   }
 }
 
-// Adds to the coarse nodes on each block's low faces the contributions of the fine nodes at
-// local -1 (high faces of the low neighbours), in a fixed order.
+// Adds to the coarse nodes on each block's low faces what the fine nodes at local -1 contribute:
+// the partials of the low neighbours (k_resid16), 1/2 per axis crossed, fixed order.  Four
+// blocks per CTA, 169 boundary coarse nodes per block.
 template <typename T>
-__global__ void __launch_bounds__(192) k_restrict_faces(uint32_t D, const T* __restrict__ face, T* __restrict__ fc) {
+__global__ void __launch_bounds__(768) k_restrict_faces(uint32_t D, const T* __restrict__ face, T* __restrict__ fc,
+                                                       uint32_t nblk) {
   const int nba = 1 << (D - 4);
-  const uint32_t blk = blockIdx.x;
+  const uint32_t blk = blockIdx.x * 4 + threadIdx.x / 192;
+  const int j = threadIdx.x % 192;
+  if (blk >= nblk || j >= 169) return;
   uint32_t bx, by, bz;
   unmorton3(blk, bx, by, bz);
-  // boundary coarse node j of 169: the (cx, cy, cz) in [0,8)^3 with at least one zero
-  const int j = threadIdx.x;
-  if (j >= 169) return;
   int cx, cy, cz;
   if (j < 64) { cx = 0; cy = j & 7; cz = j >> 3; }
   else if (j < 120) { cx = 1 + (j - 64) % 7; cy = 0; cz = (j - 64) / 7; }
@@ -982,25 +1013,27 @@ __global__ void __launch_bounds__(192) k_restrict_faces(uint32_t D, const T* __r
   T s = 0;
   bool any = false;
 #pragma unroll
-  for (int dz = -1; dz <= 1; ++dz)
-#pragma unroll
-    for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int fx = 2 * cx + dx, fy = 2 * cy + dy, fz = 2 * cz + dz;
-        if (fx >= 0 && fy >= 0 && fz >= 0) continue;  // inside this block: already counted
-        const int nx = (int)bx - (fx < 0), ny = (int)by - (fy < 0), nz = (int)bz - (fz < 0);
-        if (nx < 0 || ny < 0 || nz < 0 || nx >= nba || ny >= nba || nz >= nba) continue;  // outside the domain
-        const int lx = fx & 15, ly = fy & 15, lz = fz & 15;
-        const T* fb = face + (uint64_t)morton3((uint32_t)nx, (uint32_t)ny, (uint32_t)nz) * FACE;
-        const T v = lx == 15 ? fb[ly + 16 * lz] : (ly == 15 ? fb[256 + lx + 16 * lz] : fb[512 + lx + 16 * ly]);
-        s += (T)((dx == 0 ? 1.0 : 0.5) * (dy == 0 ? 1.0 : 0.5) * (dz == 0 ? 1.0 : 0.5)) * v;
-        any = true;
-      }
-  if (any) {
-    const uint64_t ci = (uint64_t)blk * 512 + morton3((uint32_t)cx, (uint32_t)cy, (uint32_t)cz);
-    fc[ci] += s;
+  for (int e = 1; e < 8; ++e) {
+    const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+    if ((ex && cx) || (ey && cy) || (ez && cz)) continue;  // only coarse index 0 reaches fine -1
+    const int nx = (int)bx - ex, ny = (int)by - ey, nz = (int)bz - ez;
+    if (nx < 0 || ny < 0 || nz < 0) continue;  // outside the domain
+    (void)nba;
+    const T* fb = face + (uint64_t)morton3((uint32_t)nx, (uint32_t)ny, (uint32_t)nz) * FACE;
+    T v;
+    switch (e) {
+      case 1: v = (T)0.5 * fb[cy + 8 * cz]; break;
+      case 2: v = (T)0.5 * fb[64 + cx + 8 * cz]; break;
+      case 4: v = (T)0.5 * fb[128 + cx + 8 * cy]; break;
+      case 3: v = (T)0.25 * fb[192 + cz]; break;
+      case 5: v = (T)0.25 * fb[200 + cy]; break;
+      case 6: v = (T)0.25 * fb[208 + cx]; break;
+      default: v = (T)0.125 * fb[216]; break;
+    }
+    s += v;
+    any = true;
   }
+  if (any) fc[(uint64_t)blk * 512 + morton3((uint32_t)cx, (uint32_t)cy, (uint32_t)cz)] += s;
 }
 template <typename T>
 constexpr size_t smem_bytes() {
@@ -1459,7 +1492,7 @@ void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const
       r16::k_resid16<T, false><<<nb, r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce, (T)L.cc, table);
     }
     PR_CHECK_LAUNCH();
-    r16::k_restrict_faces<T><<<nb, 192, 0, s>>>(D, face, fc);
+    r16::k_restrict_faces<T><<<(nb + 3) / 4, 768, 0, s>>>(D, face, fc, nb);
   } else {
     const size_t sm = sizeof(T) * (11 * 11 * 11 + 9 * 9 * 9);
     allow_smem(k_resid_restrict<T, 8>, sm);
