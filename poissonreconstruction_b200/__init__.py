@@ -442,7 +442,7 @@ class Context:
 
     KERNELS = {"spmv": 0, "spmv_xpby": 1, "smooth_first": 2, "smooth": 3, "smooth_prolong_dot": 4,
                "resid_restrict": 5, "stencil_per_node": 6, "smooth_prolong_dot_coarse": 7,
-               "resid_restrict_coarse": 8}
+               "resid_restrict_coarse": 8, "cg_update_presmooth": 9}
 
     def kernel_bench(self, kernel, depth, precision=PR_PRECISION_MIXED, reps=10):
         """(ms per launch, algorithmic bytes per launch) of one solver kernel."""

@@ -1583,12 +1583,14 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
   T* w = c->buf<T>("kb_w_" + tn, n);
   T* ec = c->buf<T>("kb_c_" + tn, nc);
   T* face = c->buf<T>("kb_face_" + tn, std::max<size_t>(mg_face_entries(D), 1));
+  T* r2 = c->buf<T>("kb_r_" + tn, n);
   double* part = c->buf<double>("kb_part", std::max<uint32_t>(mg_blocks(D), kDotBlocks));
   const unsigned g = 148 * 16;
   k_fill<T><<<g, 256, 0, s>>>(x, n, 1u);
   k_fill<T><<<g, 256, 0, s>>>(f, n, 2u);
   k_fill<T><<<g, 256, 0, s>>>(w, n, 3u);
   k_fill<T><<<g, 256, 0, s>>>(ec, nc, 4u);
+  k_fill<T><<<g, 256, 0, s>>>(r2, n, 5u);
   PR_CHECK_LAUNCH();
   // the finest level (no low-face rows: the variants that dominate a solve) and, for ids 7-8,
   // a coarse level (low-face table rows)
@@ -1609,14 +1611,24 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
       case 5: mg_resid_restrict<T>(s, Lf, table, x, f, ec, face); break;
       case 7: mg_smooth<T>(s, Lc, table, x, y, f, ec, 2, false, part); break;
       case 8: mg_resid_restrict<T>(s, Lc, table, x, f, ec, face); break;
+      case 9: {  // CG update fused with the first pre-smoothing sweep: x += a d, r -= a q, y = S(r)
+        CgFuse<T> cg;
+        cg.x = w;
+        cg.d = x;
+        cg.q = f;
+        cg.r = r2;
+        cg.alpha = (T)1e-3;  // small: the reps leave r and the update bounded
+        mg_cg_update_presmooth<T>(s, Lf, table, cg, y, part);
+        break;
+      }
       case 6: stencil_apply<T>(s, D, x, nullptr, y, cast_coef<T>(stencil_coef(D, 0.0)), 0); break;
       default: throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
     }
   };
   const double nb = (double)n * es;
   const double algo[] = {2 * nb, 4 * nb, 2 * nb, 3 * nb, 3 * nb + nb / 8, 2 * nb + nb / 8, 2 * nb,
-                         3 * nb + nb / 8, 2 * nb + nb / 8};
-  if (kid < 0 || kid > 8) throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
+                         3 * nb + nb / 8, 2 * nb + nb / 8, 7 * nb};
+  if (kid < 0 || kid > 9) throw Error(PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
   *bytes = algo[kid];
   run();
   PR_CUDA(cudaStreamSynchronize(s));
