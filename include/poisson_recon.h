@@ -67,7 +67,9 @@ typedef struct pr_params {
   uint32_t max_iters;         /* cap on preconditioned CG iterations, all passes (default 200) */
   uint32_t smooth_sweeps;     /* multigrid pre/post Gauss-Seidel sweeps (default 1) */
   double inner_rel_tol;       /* mixed: relative tolerance of each FP32 inner solve (default 1e-4) */
-  uint32_t reserved[8];
+  uint32_t degree;            /* B-spline degree of the node functions: 1 (the crate's; 0 means 1) or 2
+                                 (quadratic B-splines, converged mode only; default 1) */
+  uint32_t reserved[7];
 } pr_params;
 
 /* Mesh (src/marching_cubes.rs:8-11).  Vertices are model-space [x,y,z] triples; triangles

@@ -84,6 +84,16 @@ def lib():
         "orc_csr_gs_sweep": (None, [_u64, _p, _p, _p, _p, _p]),
         "orc_reconstruct": (C.c_int, [_p, _u64, C.POINTER(OrcParams), C.POINTER(OrcMesh),
                                       C.POINTER(OrcStats), _p]),
+        "orc_deg2_constants": (None, [_p, _p, _p]),
+        "orc_evaluate2": (_d, [_u32, _p, _d, _d, _d]),
+        "orc_tree2_new": (_p, [_u32, _p, _u64, _d]),
+        "orc_tree2_free": (None, [_p]),
+        "orc_tree2_normal_field": (None, [_p, _p, _p]),
+        "orc_tree2_rhs": (None, [_p, _p]),
+        "orc_tree2_apply": (None, [_p, _p, _p]),
+        "orc_tree2_solve": (_u64, [_p, _d, _u64, _p, _p]),
+        "orc_extract_surface2": (C.c_int, [_u32, _p, _d, C.POINTER(OrcMesh)]),
+        "orc_reconstruct2": (C.c_int, [_p, _u64, _u32, _d, _d, _d, _u64, C.POINTER(OrcMesh), _p, _p, _p]),
         "orc_loss": (_d, [_p, _u64, _u32, _d, _d, _p, _u64, _p, _d]),
         "orc_loss_backward": (C.c_int, [_p, _u64, _u32, _d, _d, _p, _u64, _p, _d, _p, _p, _p, _p]),
     }
@@ -277,6 +287,73 @@ def reconstruct(pts6, depth=8, scale=1.1, cg_accuracy=1e-3, cg_iters=500, point_
     v, t = _take_mesh(m)
     stats = {f: getattr(st, f) for f, _ in OrcStats._fields_}
     return v, t, stats, coeffs
+
+
+# ------------------------------------------------------------------ degree 2 (extension)
+def deg2_constants():
+    """1-D integrals of the quadratic B-spline at offsets -2..2: mass, stiffness, N2' N2."""
+    m, s, g = np.zeros(5), np.zeros(5), np.zeros(5)
+    lib().orc_deg2_constants(_ptr(m), _ptr(s), _ptr(g))
+    return m, s, g
+
+
+def evaluate2(depth, sol, pts3):
+    pts3 = _f64(pts3, (-1, 3))
+    sol = _f64(sol)
+    return np.array([lib().orc_evaluate2(int(depth), _ptr(sol), *p) for p in pts3])
+
+
+class Tree2:
+    """Degree-2 system on unit-cube points (pw: screening weight)."""
+
+    def __init__(self, depth, unit6, pw):
+        self.depth = int(depth)
+        self.unit = _f64(unit6, (-1, 6))
+        self._h = lib().orc_tree2_new(self.depth, _ptr(self.unit), self.unit.shape[0], float(pw))
+        self.n = 8 ** self.depth
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_tree2_free(self._h)
+            self._h = None
+
+    def normal_field(self):
+        nf, w = np.zeros((self.n, 3)), np.zeros(self.n)
+        lib().orc_tree2_normal_field(self._h, _ptr(nf), _ptr(w))
+        return nf, w
+
+    def rhs(self):
+        b = np.zeros(self.n)
+        lib().orc_tree2_rhs(self._h, _ptr(b))
+        return b
+
+    def apply(self, x):
+        x = _f64(x)
+        y = np.zeros(self.n)
+        lib().orc_tree2_apply(self._h, _ptr(x), _ptr(y))
+        return y
+
+    def solve(self, tol=1e-12, maxit=100000):
+        x, rr = np.zeros(self.n), C.c_double()
+        it = lib().orc_tree2_solve(self._h, float(tol), int(maxit), _ptr(x), C.byref(rr))
+        return x, it, rr.value
+
+
+def extract_surface2(depth, sol, iso_value):
+    m = OrcMesh()
+    lib().orc_extract_surface2(int(depth), _ptr(_f64(sol)), float(iso_value), C.byref(m))
+    return _take_mesh(m)
+
+
+def reconstruct2(pts6, depth, scale=1.1, point_weight=4.0, tol=1e-12, maxit=100000):
+    """(vertices, triangles, iso, relres, coefficients) of the degree-2 pipeline."""
+    pts6 = _f64(pts6, (-1, 6))
+    m, iso, rr = OrcMesh(), C.c_double(), C.c_double()
+    coeffs = np.zeros(8 ** depth)
+    lib().orc_reconstruct2(_ptr(pts6), pts6.shape[0], int(depth), float(scale), float(point_weight), float(tol),
+                           int(maxit), C.byref(m), C.byref(iso), C.byref(rr), _ptr(coeffs))
+    v, t = _take_mesh(m)
+    return v, t, iso.value, rr.value, coeffs
 
 
 # ------------------------------------------------------------------ adjoint

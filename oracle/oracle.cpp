@@ -742,8 +742,12 @@ double orc_iso(uint32_t D, const double* sol, const double* unit6, uint64_t n) {
 
 
 
-// FEMTree::extract_surface (src/fem_tree.rs:576-636).  Vertices in unit-cube space.
-int orc_extract_surface(uint32_t D, const double* sol, double iso, orc_mesh* out) {
+// FEMTree::extract_surface (src/fem_tree.rs:576-636).  Vertices in unit-cube space.  `eval` is the
+// implicit function (evaluate() at degree 1; the degree-2 evaluation for the extension).
+}  // extern "C"
+
+template <typename Eval>
+static int extract_surface_impl(uint32_t D, const double* sol, double iso, orc_mesh* out, Eval eval) {
   static const uint32_t co[8][3] = {{0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1}};
   static const int ev[12][2] = {{0,1},{1,2},{2,3},{3,0},{4,5},{5,6},{6,7},{7,4},{0,4},{1,5},{2,6},{3,7}};
   const uint64_t max_res = 1ull << D;
@@ -760,7 +764,7 @@ int orc_extract_surface(uint32_t D, const double* sol, double iso, orc_mesh* out
     for (int k = 0; k < 8; ++k) {
       double p[3];
       for (int a = 0; a < 3; ++a) p[a] = (double)(off[a] + co[k][a]) * w;
-      cv[k] = orc_evaluate(D, sol, p[0], p[1], p[2]);
+      cv[k] = eval(D, sol, p[0], p[1], p[2]);
       if (cv[k] < iso) mc |= 1u << k;
     }
     uint32_t em = orc_mc_edge_mask(mc);
@@ -798,6 +802,12 @@ int orc_extract_surface(uint32_t D, const double* sol, double iso, orc_mesh* out
   if (!verts.empty()) std::memcpy(out->verts, verts.data(), verts.size() * sizeof(double));
   if (!tris.empty()) std::memcpy(out->tris, tris.data(), tris.size() * sizeof(uint64_t));
   return 0;
+}
+
+extern "C" {
+
+int orc_extract_surface(uint32_t D, const double* sol, double iso, orc_mesh* out) {
+  return extract_surface_impl(D, sol, iso, out, orc_evaluate);
 }
 
 void orc_mesh_free(orc_mesh* m) {
@@ -1093,6 +1103,317 @@ int orc_loss_backward(const double* pts6, uint64_t n, uint32_t depth, double pw,
       dnrm[3 * p + a] = len > 0.0 ? s_m / len * (gn[a] - nu[a] * ng) : 0.0;
     }
   }
+  return 0;
+}
+
+// ================================================================ degree 2 (extension)
+// The crate's degree-2 code (src/bspline.rs:74-123, 322-417) is not on its reconstruction path.
+// This restatement defines the degree-2 system the library builds, on the crate's conventions:
+// node functions phi_i(x) = N2(x/h - i + 1), i in [0, res) (cell-centred quadratic B-splines,
+// src/bspline.rs:334-345), stencil values of the infinite grid on every row with neighbours
+// outside the grid omitted (as the crate's degree-1 stiffness, src/fem_tree.rs:180-249),
+//   A(d) = h (s m m + m s m + m m s)(d) + wg [d = 0] + wh3 sum_p phi(p) phi(p)^T,
+//   b_i  = h^2 sum_j sum_a nf_j^a (g m m)_a(j - i) + (wh3/2) sum_p phi_i(p),
+// with m, s, g the 1-D integrals of N2 N2, N2' N2', N2' N2 at offsets -2..2 (exact: 3-point
+// Gauss-Legendre per unit cell), nf the normalised splat of the normals with the same basis
+// (27 functions per point), wh3 = pw h^3 / 1.5 and wg = wh3 / 200 as at degree 1.  Grid vectors
+// are in Morton order like the degree-1 ones.
+}  // extern "C"
+namespace {
+double n2(double x) {
+  if (x <= 0.0 || x >= 3.0) return 0.0;
+  if (x <= 1.0) return 0.5 * x * x;
+  if (x <= 2.0) return 0.5 * (-2.0 * x * x + 6.0 * x - 3.0);
+  const double t = 3.0 - x;
+  return 0.5 * t * t;
+}
+double dn2(double x) {
+  if (x <= 0.0 || x >= 3.0) return 0.0;
+  if (x <= 1.0) return x;
+  if (x <= 2.0) return 3.0 - 2.0 * x;
+  return x - 3.0;
+}
+struct Deg2 {
+  double m[5], s[5], g[5];  // offset d = -2..2 at index d + 2
+  Deg2() {
+    const double gx[3] = {-0.7745966692414834, 0.0, 0.7745966692414834};
+    const double gw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    for (int d = -2; d <= 2; ++d) {
+      double am = 0.0, as = 0.0, ag = 0.0;
+      for (int c = -1; c < 5; ++c)
+        for (int q = 0; q < 3; ++q) {
+          const double t = c + 0.5 + 0.5 * gx[q], w = 0.5 * gw[q];
+          am += w * n2(t) * n2(t - d);
+          as += w * dn2(t) * dn2(t - d);
+          ag += w * dn2(t) * n2(t - d);
+        }
+      m[d + 2] = am;
+      s[d + 2] = as;
+      g[d + 2] = ag;
+    }
+  }
+};
+const Deg2& deg2() {
+  static const Deg2 k;
+  return k;
+}
+// basis of one axis at unit coordinate u: nodes o[3] (c-1, c, c+1) and weights b[3], grad db[3]
+// (d/du); valid[k] = node in [0, res)
+void axis2(double u, double h, isize res, isize* o, double* b, double* db) {
+  const double s = u / h;
+  const isize c = f64_to_isize(std::floor(s));
+  const double t = s - (double)c;
+  o[0] = c - 1; o[1] = c; o[2] = c + 1;
+  b[0] = 0.5 * (1.0 - t) * (1.0 - t);
+  b[1] = 0.5 * (-2.0 * t * t + 2.0 * t + 1.0);
+  b[2] = 0.5 * t * t;
+  db[0] = -(1.0 - t) / h;
+  db[1] = (1.0 - 2.0 * t) / h;
+  db[2] = t / h;
+  (void)res;
+}
+inline bool in_range(isize i, isize res) { return i >= 0 && i < res; }
+}  // namespace
+extern "C" {
+
+void orc_deg2_constants(double* m5, double* s5, double* g5) {
+  for (int k = 0; k < 5; ++k) {
+    m5[k] = deg2().m[k];
+    s5[k] = deg2().s[k];
+    g5[k] = deg2().g[k];
+  }
+}
+
+double orc_evaluate2(uint32_t D, const double* sol, double px, double py, double pz) {
+  const isize res = (isize)1 << D;
+  const double h = 1.0 / (double)res;
+  isize o[3][3];
+  double b[3][3], db[3][3];
+  axis2(px, h, res, o[0], b[0], db[0]);
+  axis2(py, h, res, o[1], b[1], db[1]);
+  axis2(pz, h, res, o[2], b[2], db[2]);
+  double v = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    if (!in_range(o[2][k], res)) continue;
+    for (int j = 0; j < 3; ++j) {
+      if (!in_range(o[1][j], res)) continue;
+      for (int i = 0; i < 3; ++i) {
+        if (!in_range(o[0][i], res)) continue;
+        v += sol[morton(o[0][i], o[1][j], o[2][k])] * b[0][i] * b[1][j] * b[2][k];
+      }
+    }
+  }
+  return v;
+}
+
+struct orc_tree2 {
+  uint32_t D;
+  isize res;
+  uint64_t n;
+  double h, pw;
+  std::vector<P6> pts;
+  std::vector<double> nf, nw;  // 3n normal field (normalised, negated), n weights
+};
+
+orc_tree2* orc_tree2_new(uint32_t depth, const double* unit6, uint64_t npts, double pw) {
+  orc_tree2* t = new orc_tree2();
+  t->D = depth;
+  t->res = (isize)1 << depth;
+  t->n = (uint64_t)t->res * t->res * t->res;
+  t->h = 1.0 / (double)t->res;
+  t->pw = pw;
+  t->pts.resize(npts);
+  std::memcpy(t->pts.data(), unit6, npts * sizeof(P6));
+  t->nf.assign(3 * t->n, 0.0);
+  t->nw.assign(t->n, 0.0);
+  for (const P6& p : t->pts) {
+    isize o[3][3];
+    double b[3][3], db[3][3];
+    axis2(p.x, t->h, t->res, o[0], b[0], db[0]);
+    axis2(p.y, t->h, t->res, o[1], b[1], db[1]);
+    axis2(p.z, t->h, t->res, o[2], b[2], db[2]);
+    for (int k = 0; k < 3; ++k)
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          if (!in_range(o[0][i], t->res) || !in_range(o[1][j], t->res) || !in_range(o[2][k], t->res)) continue;
+          const uint64_t idx = morton(o[0][i], o[1][j], o[2][k]);
+          const double w = b[0][i] * b[1][j] * b[2][k];
+          t->nf[3 * idx] += p.nx * w;
+          t->nf[3 * idx + 1] += p.ny * w;
+          t->nf[3 * idx + 2] += p.nz * w;
+          t->nw[idx] += w;
+        }
+  }
+  for (uint64_t i = 0; i < t->n; ++i)
+    if (t->nw[i] > 0.0)
+      for (int a = 0; a < 3; ++a) t->nf[3 * i + a] = -t->nf[3 * i + a] / t->nw[i];
+  return t;
+}
+void orc_tree2_free(orc_tree2* t) { delete t; }
+
+void orc_tree2_normal_field(const orc_tree2* t, double* nf3, double* w) {
+  std::memcpy(nf3, t->nf.data(), 3 * t->n * sizeof(double));
+  std::memcpy(w, t->nw.data(), t->n * sizeof(double));
+}
+
+void orc_tree2_rhs(const orc_tree2* t, double* b) {
+  const Deg2& K = deg2();
+  const isize res = t->res;
+  const double h2 = t->h * t->h;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)t->n; ++i) {
+    uint64_t ix, iy, iz;
+    unmorton((uint64_t)i, ix, iy, iz);
+    double sum = 0.0;
+    for (int dz = -2; dz <= 2; ++dz)
+      for (int dy = -2; dy <= 2; ++dy)
+        for (int dx = -2; dx <= 2; ++dx) {
+          const isize jx = (isize)ix + dx, jy = (isize)iy + dy, jz = (isize)iz + dz;
+          if (!in_range(jx, res) || !in_range(jy, res) || !in_range(jz, res)) continue;
+          const double* v = &t->nf[3 * morton(jx, jy, jz)];
+          sum += v[0] * K.g[dx + 2] * K.m[dy + 2] * K.m[dz + 2] + v[1] * K.m[dx + 2] * K.g[dy + 2] * K.m[dz + 2] +
+                 v[2] * K.m[dx + 2] * K.m[dy + 2] * K.g[dz + 2];
+        }
+    b[i] = h2 * sum;
+  }
+  if (t->pw > 0.0) {
+    const double wh3 = t->pw * t->h * t->h * t->h / 1.5;
+    for (const P6& p : t->pts) {
+      isize o[3][3];
+      double bb[3][3], db[3][3];
+      axis2(p.x, t->h, res, o[0], bb[0], db[0]);
+      axis2(p.y, t->h, res, o[1], bb[1], db[1]);
+      axis2(p.z, t->h, res, o[2], bb[2], db[2]);
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            if (!in_range(o[0][i], res) || !in_range(o[1][j], res) || !in_range(o[2][k], res)) continue;
+            b[morton(o[0][i], o[1][j], o[2][k])] += wh3 * 0.5 * bb[0][i] * bb[1][j] * bb[2][k];
+          }
+    }
+  }
+}
+
+// y = A x (125-point stencil + wg + screening), matrix-free
+void orc_tree2_apply(const orc_tree2* t, const double* x, double* y) {
+  const Deg2& K = deg2();
+  const isize res = t->res;
+  const double h = t->h;
+  const double wh3 = t->pw > 0.0 ? t->pw * h * h * h / 1.5 : 0.0;
+  const double wg = wh3 * 0.005;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)t->n; ++i) {
+    uint64_t ix, iy, iz;
+    unmorton((uint64_t)i, ix, iy, iz);
+    double sum = 0.0;
+    for (int dz = -2; dz <= 2; ++dz)
+      for (int dy = -2; dy <= 2; ++dy)
+        for (int dx = -2; dx <= 2; ++dx) {
+          const isize jx = (isize)ix + dx, jy = (isize)iy + dy, jz = (isize)iz + dz;
+          if (!in_range(jx, res) || !in_range(jy, res) || !in_range(jz, res)) continue;
+          const int a = dx + 2, bi = dy + 2, c = dz + 2;
+          const double st = K.s[a] * K.m[bi] * K.m[c] + K.m[a] * K.s[bi] * K.m[c] + K.m[a] * K.m[bi] * K.s[c];
+          sum += h * st * x[morton(jx, jy, jz)];
+        }
+    y[i] = sum + wg * x[i];
+  }
+  if (wh3 > 0.0) {
+    for (const P6& p : t->pts) {
+      isize o[3][3];
+      double bb[3][3], db[3][3];
+      axis2(p.x, h, res, o[0], bb[0], db[0]);
+      axis2(p.y, h, res, o[1], bb[1], db[1]);
+      axis2(p.z, h, res, o[2], bb[2], db[2]);
+      uint64_t idx[27];
+      double phi[27];
+      int m = 0;
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          for (int ii = 0; ii < 3; ++ii) {
+            if (!in_range(o[0][ii], res) || !in_range(o[1][j], res) || !in_range(o[2][k], res)) continue;
+            idx[m] = morton(o[0][ii], o[1][j], o[2][k]);
+            phi[m] = bb[0][ii] * bb[1][j] * bb[2][k];
+            ++m;
+          }
+      double proj = 0.0;
+      for (int q = 0; q < m; ++q) proj += phi[q] * x[idx[q]];
+      for (int q = 0; q < m; ++q) y[idx[q]] += wh3 * phi[q] * proj;
+    }
+  }
+}
+
+// CG (from x = 0) to ||b - A x|| <= tol ||b||; returns iterations, *relres the final relative residual
+uint64_t orc_tree2_solve(const orc_tree2* t, double tol, uint64_t maxit, double* x, double* relres) {
+  const uint64_t n = t->n;
+  std::vector<double> b(n), r(n), d(n), q(n);
+  orc_tree2_rhs(t, b.data());
+  std::fill(x, x + n, 0.0);
+  const double bb = det_dot(b.data(), b.data(), n);
+  if (bb == 0.0) {
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  r = b;
+  d = b;
+  double rr = bb;
+  uint64_t it = 0;
+  while (it < maxit && rr > tol * tol * bb) {
+    orc_tree2_apply(t, d.data(), q.data());
+    const double dq = det_dot(d.data(), q.data(), n);
+    if (dq == 0.0) break;
+    const double alpha = rr / dq;
+    for (uint64_t i = 0; i < n; ++i) x[i] += alpha * d[i];
+    ++it;
+    if (it % 50 == 0) {
+      orc_tree2_apply(t, x, q.data());
+      for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+    } else {
+      for (uint64_t i = 0; i < n; ++i) r[i] -= alpha * q[i];
+    }
+    const double rr_new = det_dot(r.data(), r.data(), n);
+    const double beta = rr_new / rr;
+    rr = rr_new;
+    for (uint64_t i = 0; i < n; ++i) d[i] = r[i] + beta * d[i];
+  }
+  orc_tree2_apply(t, x, q.data());
+  for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  if (relres) *relres = std::sqrt(det_dot(r.data(), r.data(), n) / bb);
+  return it;
+}
+
+double orc_evaluate2(uint32_t D, const double* sol, double px, double py, double pz);
+int orc_extract_surface2(uint32_t D, const double* sol, double iso, orc_mesh* out) {
+  return extract_surface_impl(D, sol, iso, out, orc_evaluate2);
+}
+
+// Degree-2 pipeline: transform (as reconstruct), tree2, converged CG, iso (mean of the degree-2
+// evaluation over the unit points), marching cubes on the degree-2 function, back-transform.
+int orc_reconstruct2(const double* pts6, uint64_t n, uint32_t depth, double scale, double pw, double tol,
+                     uint64_t maxit, orc_mesh* mesh, double* iso_out, double* relres, double* coeffs) {
+  mesh->verts = nullptr; mesh->tris = nullptr; mesh->nv = mesh->nt = 0;
+  if (n == 0) return 0;
+  double bmin[3], bmax[3], M[16], Minv[16];
+  orc_bbox(pts6, n, bmin, bmax);
+  orc_unit_cube_transform(bmin, bmax, scale, M);
+  orc_mat4_inverse(M, Minv);
+  std::vector<double> unit(6 * n);
+  orc_transform_points(M, pts6, n, unit.data());
+  orc_tree2* t = orc_tree2_new(depth, unit.data(), n, pw);
+  std::vector<double> x(t->n, 0.0);
+  orc_tree2_solve(t, tol, maxit, x.data(), relres);
+  std::vector<double> v(n), one(n, 1.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) v[i] = orc_evaluate2(depth, x.data(), unit[6 * i], unit[6 * i + 1], unit[6 * i + 2]);
+  const double iso = det_dot(v.data(), one.data(), n) / (double)n;
+  if (iso_out) *iso_out = iso;
+  orc_extract_surface2(depth, x.data(), iso, mesh);
+  for (uint64_t k = 0; k < mesh->nv; ++k) {
+    double q[3];
+    orc_transform_point(Minv, mesh->verts + 3 * k, q);
+    std::memcpy(mesh->verts + 3 * k, q, sizeof(q));
+  }
+  if (coeffs) std::memcpy(coeffs, x.data(), t->n * sizeof(double));
+  orc_tree2_free(t);
   return 0;
 }
 

@@ -39,7 +39,7 @@ class PrParams(C.Structure):
                 ("cg_accuracy", C.c_double), ("cg_iters", C.c_uint64), ("point_weight", C.c_double),
                 ("verbose", C.c_int32), ("solve_mode", C.c_int32), ("precision", C.c_int32),
                 ("target_rel_residual", C.c_double), ("max_iters", C.c_uint32), ("smooth_sweeps", C.c_uint32),
-                ("inner_rel_tol", C.c_double), ("reserved", C.c_uint32 * 8)]
+                ("inner_rel_tol", C.c_double), ("degree", C.c_uint32), ("reserved", C.c_uint32 * 7)]
 
 
 class PrMesh(C.Structure):
@@ -155,6 +155,7 @@ class ReconstructParams:
     max_iters: int = 200
     smooth_sweeps: int = 1
     inner_rel_tol: float = 1e-4
+    degree: int = 1
 
     def to_c(self):
         p = PrParams()

@@ -71,7 +71,12 @@ void validate(const pr_params* p) {
              "unknown precision");
   PR_REQUIRE(!(p->target_rel_residual < 0.0) && std::isfinite(p->target_rel_residual), PR_ERR_INVALID_ARGUMENT,
              "target_rel_residual must be finite and >= 0");
+  PR_REQUIRE(p->degree <= 2, PR_ERR_INVALID_ARGUMENT, "degree must be 1 or 2, got " + std::to_string(p->degree));
+  PR_REQUIRE(p->degree != 2 || p->solve_mode == PR_SOLVE_CONVERGED, PR_ERR_INVALID_ARGUMENT,
+             "degree 2 is solved in solve_mode PR_SOLVE_CONVERGED only");
 }
+
+int degree_of(const pr_params& p) { return p.degree == 2 ? 2 : 1; }
 
 void set_device(pr_context* c) { PR_CUDA(cudaSetDevice(c->device)); }
 
@@ -260,7 +265,9 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   c->sync();
   double t1 = now_s();
   st.time_transform = t1 - t0 + (t0 - t_start);
-  pr::stage_splat_rhs(c, p.depth, p.point_weight);
+  c->degree = degree_of(p);
+  if (c->degree == 2) pr::stage_setup_deg2(c, p.depth, p.point_weight);
+  else pr::stage_splat_rhs(c, p.depth, p.point_weight);
   c->sync();
   double t2 = now_s();
   st.time_tree = t2 - t1;  // tree (implicit) + splat + RHS + screening payload
@@ -268,7 +275,8 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   st.fem_nodes = c->n;
   st.points_in_cube = c->P_in;
   c->params = p;
-  if (p.solve_mode == PR_SOLVE_REFERENCE_SCHEDULE) pr::stage_solve_reference(c, p, st);
+  if (c->degree == 2) pr::stage_solve_deg2(c, p, st);
+  else if (p.solve_mode == PR_SOLVE_REFERENCE_SCHEDULE) pr::stage_solve_reference(c, p, st);
   else pr::stage_solve(c, p, st);
   c->coeffs_converged = p.solve_mode != PR_SOLVE_REFERENCE_SCHEDULE;
   c->sync();
@@ -278,7 +286,7 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   if (!extract) return;
   const double* x = c->get<double>("x64");
   double iso = pr::stage_iso(c, x);
-  pr::stage_extract(c, c->D, x, iso, true);
+  pr::stage_extract(c, c->D, x, iso, true, c->degree);
   c->sync();
   double t4 = now_s();
   st.time_extract = t4 - t3;
@@ -288,9 +296,9 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   st.peak_device_bytes = (double)c->peak_bytes;
   if (p.verbose)
     std::fprintf(stderr,
-                 "pr: depth=%u points=%llu xform=%.4f tree=%.4f solve=%.4f extract=%.4f s; pcg=%u refine=%u "
-                 "relres=%.3e iso=%.6f verts=%llu tris=%llu\n",
-                 p.depth, (unsigned long long)n, st.time_transform, st.time_tree, st.time_solve, st.time_extract,
+                 "pr: depth=%u degree=%d points=%llu xform=%.4f tree=%.4f solve=%.4f extract=%.4f s; pcg=%u "
+                 "refine=%u relres=%.3e iso=%.6f verts=%llu tris=%llu\n",
+                 p.depth, c->degree, (unsigned long long)n, st.time_transform, st.time_tree, st.time_solve, st.time_extract,
                  st.pcg_iterations, st.refinement_steps, st.rel_residual, iso, (unsigned long long)c->nv,
                  (unsigned long long)c->nt);
 }
@@ -358,8 +366,14 @@ int pr_ctx_apply_operator_device(pr_context* c, const void* d_x, void* d_y, int 
     PR_REQUIRE(c != nullptr && d_x != nullptr && d_y != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
     set_device(c);
-    if (precision == PR_PRECISION_FP64) pr::apply_operator64(c, (const double*)d_x, (double*)d_y);
-    else pr::apply_operator32(c, (const float*)d_x, (float*)d_y);
+    if (c->degree == 2) {
+      if (precision == PR_PRECISION_FP64) pr::deg2_apply_morton<double>(c, (const double*)d_x, (double*)d_y);
+      else pr::deg2_apply_morton<float>(c, (const float*)d_x, (float*)d_y);
+    } else if (precision == PR_PRECISION_FP64) {
+      pr::apply_operator64(c, (const double*)d_x, (double*)d_y);
+    } else {
+      pr::apply_operator32(c, (const float*)d_x, (float*)d_y);
+    }
   });
 }
 
@@ -398,6 +412,7 @@ pr_params pr_params_default(void) {
   p.solve_mode = PR_SOLVE_CONVERGED;
   p.precision = PR_PRECISION_MIXED;
   p.target_rel_residual = 1e-6;
+  p.degree = 1;
   p.max_iters = 200;
   p.smooth_sweeps = 1;
   p.inner_rel_tol = 1e-4;
@@ -507,6 +522,7 @@ static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k
   PR_REQUIRE(c->have_state && c->have_coeffs, PR_ERR_STATE, "no solved reconstruction on this context");
   PR_REQUIRE(c->coeffs_converged, PR_ERR_STATE,
              "the last solve used the reference schedule; the adjoint needs solve_mode PR_SOLVE_CONVERGED");
+  PR_REQUIRE(c->degree == 1, PR_ERR_STATE, "the adjoint is implemented for degree 1");
   for (uint64_t i = 0; i < 3 * k; ++i)
     PR_REQUIRE(std::isfinite(queries3[i]), PR_ERR_INVALID_ARGUMENT, "non-finite query coordinate");
   set_device(c);
@@ -552,6 +568,7 @@ int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params,
     PR_REQUIRE(n >= 1 && points6 != nullptr, PR_ERR_INVALID_ARGUMENT, "the adjoint needs at least one point");
     PR_REQUIRE(params->solve_mode == PR_SOLVE_CONVERGED, PR_ERR_INVALID_ARGUMENT,
                "the adjoint needs solve_mode PR_SOLVE_CONVERGED");
+    PR_REQUIRE(degree_of(*params) == 1, PR_ERR_INVALID_ARGUMENT, "the adjoint is implemented for degree 1");
     if (!g_thread_ctx) {
       pr_context* c = nullptr;
       int rc = pr_context_create(0, nullptr, &c);
@@ -696,6 +713,14 @@ int pr_ctx_get_rhs(pr_context* c, double* out) {
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    if (c->degree == 2) {
+      PR_REQUIRE(out != nullptr, PR_ERR_INVALID_ARGUMENT, "output is NULL");
+      set_device(c);
+      pr::deg2_rhs_morton(c, c->buf<double>("acc_b", c->n));
+      copy_dev_to_host(c, "acc_b", out, c->n);
+      c->release("acc_b");
+      return;
+    }
     copy_dev_to_host(c, "b64", out, c->n);
   });
 }
@@ -726,7 +751,8 @@ int pr_ctx_get_normal_field(pr_context* c, double* out3, double* outw) {
     set_device(c);
     double* nf = c->buf<double>("acc_nf3", 3 * c->n);
     double* w = c->buf<double>("acc_w", c->n);
-    pr::scatter_normal_field(c, nf, w);
+    if (c->degree == 2) pr::deg2_normal_field_morton(c, nf, w);
+    else pr::scatter_normal_field(c, nf, w);
     PR_CUDA(cudaMemcpyAsync(out3, nf, 3 * c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     PR_CUDA(cudaMemcpyAsync(outw, w, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     c->sync();
@@ -745,12 +771,14 @@ int pr_ctx_apply_operator(pr_context* c, const double* x, double* y, int precisi
     double* dy = c->buf<double>("acc_y", n);
     PR_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     if (precision == PR_PRECISION_FP64) {
-      pr::apply_operator64(c, dx, dy);
+      if (c->degree == 2) pr::deg2_apply_morton<double>(c, dx, dy);
+      else pr::apply_operator64(c, dx, dy);
     } else {
       float* fx = c->buf<float>("acc_fx", n);
       float* fy = c->buf<float>("acc_fy", n);
       pr::scale_convert<double, float>(c->stream, n, 1.0, dx, fx);
-      pr::apply_operator32(c, fx, fy);
+      if (c->degree == 2) pr::deg2_apply_morton<float>(c, fx, fy);
+      else pr::apply_operator32(c, fx, fy);
       pr::scale_convert<float, double>(c->stream, n, 1.0, fy, dy);
     }
     PR_CUDA(cudaMemcpyAsync(y, dy, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -777,13 +805,14 @@ int pr_ctx_evaluate(pr_context* c, const double* coeffs, const double* pts3, uin
     double* dp = c->buf<double>("acc_pts", 3 * n);
     double* dout = c->buf<double>("acc_out", n);
     PR_CUDA(cudaMemcpyAsync(dp, pts3, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    pr::evaluate_points(c, c->D, dx, dp, 3, n, dout);
+    pr::evaluate_points(c, c->D, dx, dp, 3, n, dout, c->degree);
     PR_CUDA(cudaMemcpyAsync(out, dout, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     c->sync();
   });
 }
 
-static void extract_common(pr_context* c, uint32_t depth, const double* coeffs, double iso, pr_mesh* out) {
+static void extract_common(pr_context* c, uint32_t depth, const double* coeffs, double iso, pr_mesh* out,
+                           int degree) {
   PR_REQUIRE(coeffs != nullptr && out != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
   PR_REQUIRE(depth >= pr::kMinDepth && depth <= pr::kMaxDepth, PR_ERR_INVALID_ARGUMENT, "depth must be in [1, 10]");
   PR_REQUIRE(std::isfinite(iso), PR_ERR_INVALID_ARGUMENT, "iso must be finite");
@@ -792,7 +821,7 @@ static void extract_common(pr_context* c, uint32_t depth, const double* coeffs, 
   const uint64_t n = 1ull << (3 * depth);
   double* dx = c->buf<double>("ext_x", n);
   PR_CUDA(cudaMemcpyAsync(dx, coeffs, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  pr::stage_extract(c, depth, dx, iso, false);
+  pr::stage_extract(c, depth, dx, iso, false, degree);
   copy_mesh_to_host(c, out);
 }
 
@@ -800,14 +829,14 @@ int pr_ctx_extract(pr_context* c, const double* coeffs, double iso, pr_mesh* out
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
-    extract_common(c, c->D, coeffs, iso, out);
+    extract_common(c, c->D, coeffs, iso, out, c->degree);
   });
 }
 
 int pr_ctx_extract_at_depth(pr_context* c, uint32_t depth, const double* coeffs, double iso, pr_mesh* out) {
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
-    extract_common(c, depth, coeffs, iso, out);
+    extract_common(c, depth, coeffs, iso, out, 1);
   });
 }
 

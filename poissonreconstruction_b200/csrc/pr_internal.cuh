@@ -137,6 +137,7 @@ struct pr_context {
   uint64_t nv = 0, nt = 0;
   bool have_coeffs = false;
   bool coeffs_converged = false;  // x64 solves A x = b (converged mode), not the reference schedule
+  int degree = 1;                 // node functions of the current state: 1 (the crate's) or 2
   pr_params params{};             // parameters of the last reconstruction
 
   template <typename T>
@@ -198,11 +199,19 @@ uint64_t sort_and_segment(pr_context* c, const std::string& tag, uint32_t* keys_
 void stage_solve(pr_context* c, const pr_params& p, pr_stats& st);
 // A x = b with the current system's operator (x = 0 initially; b, x: n doubles)
 void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double* b, double* x);
-// extract (pr_mc.cu)
+// degree 2 (pr_deg2.cu): natural-order system, solve, accessors in Morton order
+void stage_setup_deg2(pr_context* c, uint32_t depth, double pw);
+void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st);
+void deg2_rhs_morton(pr_context* c, double* d_out);
+void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w);
+template <typename T>
+void deg2_apply_morton(pr_context* c, const T* d_x, T* d_y);
+// extract (pr_mc.cu); `degree` selects the node functions (1: the crate's, 2: quadratic)
 double stage_iso(pr_context* c, const double* d_x64);
-void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform);
+void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform,
+                   int degree = 1);
 void evaluate_points(pr_context* c, uint32_t depth, const double* d_x64, const double* d_pts, uint64_t stride,
-                     uint64_t n, double* d_out);
+                     uint64_t n, double* d_out, int degree = 1);
 
 // operator helpers (pr_operator.cu), exposed for tests through the ABI
 void apply_operator64(pr_context* c, const double* d_x, double* d_y);

@@ -104,6 +104,72 @@ __device__ __forceinline__ double corner_value(const double* __restrict__ x, int
   return v;
 }
 
+// Degree-2 evaluation (the extension's quadratic node functions): per axis s = u / h, c = floor(s),
+// t = s - c, weights (1-t)^2/2, (-2t^2 + 2t + 1)/2, t^2/2 of nodes c-1, c, c+1; nodes outside the
+// grid are skipped; terms summed z-major, then y, then x, as ((x_j b_x) b_y) b_z.
+__device__ double eval_fem2(const double* __restrict__ x, uint32_t D, double px, double py, double pz) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  const double u[3] = {px, py, pz};
+  int64_t c[3];
+  double b[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double s = xdiv(u[a], h);
+    c[a] = sat_i64(floor(s));
+    const double t = xsub(s, (double)c[a]);
+    const double omt = xsub(1.0, t);
+    b[a][0] = xmul(xmul(0.5, omt), omt);
+    b[a][1] = xmul(0.5, xadd(xadd(xmul(xmul(-2.0, t), t), xmul(2.0, t)), 1.0));
+    b[a][2] = xmul(xmul(0.5, t), t);
+  }
+  double v = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    const int64_t z = c[2] + k - 1;
+    if (z < 0 || z >= res) continue;
+    for (int j = 0; j < 3; ++j) {
+      const int64_t y = c[1] + j - 1;
+      if (y < 0 || y >= res) continue;
+      for (int i = 0; i < 3; ++i) {
+        const int64_t xx = c[0] + i - 1;
+        if (xx < 0 || xx >= res) continue;
+        v = xadd(v, xmul(xmul(xmul(x[morton3((uint32_t)xx, (uint32_t)y, (uint32_t)z)], b[0][i]), b[1][j]), b[2][k]));
+      }
+    }
+  }
+  return v;
+}
+
+// eval_fem2 at the integer grid position (kx,ky,kz): t = 0 on every axis, so the weights are
+// 1/2, 1/2, 0 for nodes k-1, k, k+1; the zero-weight terms add +-0 and are left out (the sum
+// never holds -0), which keeps the result identical.
+__device__ __forceinline__ double corner_value2(const double* __restrict__ x, int res, int kx, int ky, int kz) {
+  double v = 0.0;
+#pragma unroll
+  for (int dz = -1; dz <= 0; ++dz) {
+    const int z = kz + dz;
+    if (z < 0 || z >= res) continue;
+#pragma unroll
+    for (int dy = -1; dy <= 0; ++dy) {
+      const int y = ky + dy;
+      if (y < 0 || y >= res) continue;
+#pragma unroll
+      for (int dx = -1; dx <= 0; ++dx) {
+        const int xx = kx + dx;
+        if (xx < 0 || xx >= res) continue;
+        v = xadd(v, xmul(xmul(xmul(x[morton3((uint32_t)xx, (uint32_t)y, (uint32_t)z)], 0.5), 0.5), 0.5));
+      }
+    }
+  }
+  return v;
+}
+
+template <int DEG>
+__device__ __forceinline__ double eval_deg(const double* __restrict__ x, uint32_t D, double px, double py, double pz) {
+  return DEG == 2 ? eval_fem2(x, D, px, py, pz) : eval_fem(x, D, px, py, pz);
+}
+
+template <int DEG>
 __device__ __forceinline__ uint32_t cell_case(const double* __restrict__ x, int res, uint32_t cell, double iso,
                                               double* cv) {
   uint32_t ox, oy, oz;
@@ -111,7 +177,8 @@ __device__ __forceinline__ uint32_t cell_case(const double* __restrict__ x, int 
   uint32_t mc = 0;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    cv[k] = corner_value(x, res, (int)ox + c_co[k][0], (int)oy + c_co[k][1], (int)oz + c_co[k][2]);
+    const int kx = (int)ox + c_co[k][0], ky = (int)oy + c_co[k][1], kz = (int)oz + c_co[k][2];
+    cv[k] = DEG == 2 ? corner_value2(x, res, kx, ky, kz) : corner_value(x, res, kx, ky, kz);
     if (cv[k] < iso) mc |= 1u << k;
   }
   return mc;
@@ -119,10 +186,12 @@ __device__ __forceinline__ uint32_t cell_case(const double* __restrict__ x, int 
 
 // ------------------------------------------------------------------ iso value
 // Per-point evaluate, then a deterministic compensated (Neumaier) sum.
+template <int DEG>
 __global__ void k_eval_points(const double* __restrict__ x, uint32_t D, const double* __restrict__ pts,
                               uint64_t stride_pt, uint64_t stride_axis, uint64_t n, double* __restrict__ out) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = eval_fem(x, D, pts[i * stride_pt], pts[i * stride_pt + stride_axis], pts[i * stride_pt + 2 * stride_axis]);
+    out[i] = eval_deg<DEG>(x, D, pts[i * stride_pt], pts[i * stride_pt + stride_axis],
+                           pts[i * stride_pt + 2 * stride_axis]);
 }
 
 struct Neu {
@@ -136,11 +205,12 @@ __device__ __forceinline__ Neu neu_add(Neu a, double v) {
   return a;
 }
 
+template <int DEG>
 __global__ void k_iso_partial(const double* __restrict__ x, uint32_t D, const double* __restrict__ upos, uint64_t P,
                               double* __restrict__ part) {
   Neu acc{0.0, 0.0};
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < P; i += (uint64_t)gridDim.x * blockDim.x)
-    acc = neu_add(acc, eval_fem(x, D, upos[i], upos[P + i], upos[2 * P + i]));
+    acc = neu_add(acc, eval_deg<DEG>(x, D, upos[i], upos[P + i], upos[2 * P + i]));
   __shared__ double ss[kThreads], sc[kThreads];
   ss[threadIdx.x] = acc.s;
   sc[threadIdx.x] = acc.c;
@@ -167,6 +237,7 @@ __global__ void k_iso_final(const double* __restrict__ part, int nb, double* __r
 }
 
 // ------------------------------------------------------------------ marching cubes
+template <int DEG>
 __global__ void k_mc_count(const double* __restrict__ x, uint32_t D, double iso, uint32_t* __restrict__ blockcnt) {
   const int res = 1 << D;
   const uint64_t n = 1ull << (3 * D);
@@ -174,7 +245,7 @@ __global__ void k_mc_count(const double* __restrict__ x, uint32_t D, double iso,
   int active = 0;
   if (cell < n) {
     double cv[8];
-    uint32_t mc = cell_case(x, res, (uint32_t)cell, iso, cv);
+    uint32_t mc = cell_case<DEG>(x, res, (uint32_t)cell, iso, cv);
     active = (mc != 0u && mc != 255u);
   }
   typedef cub::BlockReduce<int, kThreads> BR;
@@ -183,6 +254,7 @@ __global__ void k_mc_count(const double* __restrict__ x, uint32_t D, double iso,
   if (threadIdx.x == 0) blockcnt[blockIdx.x] = (uint32_t)tot;
 }
 
+template <int DEG>
 __global__ void k_mc_compact(const double* __restrict__ x, uint32_t D, double iso, const uint32_t* __restrict__ blockoff,
                              uint32_t* __restrict__ acell, uint8_t* __restrict__ acase, uint32_t* __restrict__ nedge,
                              uint32_t* __restrict__ ntri) {
@@ -193,7 +265,7 @@ __global__ void k_mc_compact(const double* __restrict__ x, uint32_t D, double is
   int active = 0;
   if (cell < n) {
     double cv[8];
-    mc = cell_case(x, res, (uint32_t)cell, iso, cv);
+    mc = cell_case<DEG>(x, res, (uint32_t)cell, iso, cv);
     active = (mc != 0u && mc != 255u);
   }
   typedef cub::BlockScan<int, kThreads> BS;
@@ -210,6 +282,7 @@ __global__ void k_mc_compact(const double* __restrict__ x, uint32_t D, double is
 }
 
 // Vertex slots: position exactly as src/fem_tree.rs:613-624, key as :625
+template <int DEG>
 __global__ void k_mc_vertices(const double* __restrict__ x, uint32_t D, double iso, const uint32_t* __restrict__ acell,
                               uint64_t A, const uint32_t* __restrict__ eoff, double* __restrict__ pos,
                               uint64_t* __restrict__ k1, uint32_t* __restrict__ k2, uint32_t* __restrict__ slot_id,
@@ -219,7 +292,7 @@ __global__ void k_mc_vertices(const double* __restrict__ x, uint32_t D, double i
   for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < A; a += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t cell = acell[a];
     double cv[8];
-    uint32_t mc = cell_case(x, res, cell, iso, cv);
+    uint32_t mc = cell_case<DEG>(x, res, cell, iso, cv);
     uint32_t em = edge_mask(mc);
     uint32_t ox, oy, oz;
     unmorton3(cell, ox, oy, oz);
@@ -370,6 +443,67 @@ __device__ __forceinline__ void mc_build_masks(const double* tile, uint32_t* mas
     mask[r] = m;
   }
 }
+// Degree 2: the corner value at grid position p is the sum over the nodes p-1, p per axis of
+// ((x 1/2) 1/2) 1/2, z-major, then y, then x (corner_value2).  The CTA stages nodes
+// [-1, 16]^3 of its block (zeros outside the domain, which add +0 like the skipped terms).
+constexpr int MCW2 = 18;  // node tile width, tile coordinate = node local + 1
+
+__device__ void mc_load_tile2(double* tile, const double* __restrict__ x, uint32_t blk, int res) {
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  const uint64_t base = (uint64_t)blk << 12;
+  for (int i = threadIdx.x; i < 4096; i += blockDim.x) {
+    uint32_t lx, ly, lz;
+    unmorton3((uint32_t)i, lx, ly, lz);
+    tile[((lz + 1) * MCW2 + (ly + 1)) * MCW2 + (lx + 1)] = __ldg(x + base + i);
+  }
+  // the shell: tile coordinates 0 or 17 on some axis
+  for (int i = threadIdx.x; i < MCW2 * MCW2 * MCW2; i += blockDim.x) {
+    const int tx = i % MCW2, ty = (i / MCW2) % MCW2, tz = i / (MCW2 * MCW2);
+    if (tx >= 1 && tx <= 16 && ty >= 1 && ty <= 16 && tz >= 1 && tz <= 16) continue;
+    const int gx = (int)bx * 16 + tx - 1, gy = (int)by * 16 + ty - 1, gz = (int)bz * 16 + tz - 1;
+    double v = 0.0;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res)
+      v = __ldg(x + morton3((uint32_t)gx, (uint32_t)gy, (uint32_t)gz));
+    tile[i] = v;
+  }
+}
+
+__device__ __forceinline__ void mc_build_masks2(const double* tile, uint32_t* mask, double iso) {
+  for (int r = threadIdx.x; r < MCW * MCW; r += blockDim.x) {
+    const int ty = r % MCW, tz = r / MCW;
+    uint32_t m = 0;
+    for (int tx = 0; tx < MCW; ++tx) {
+      double v = 0.0;
+#pragma unroll
+      for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+          for (int dx = 0; dx < 2; ++dx)
+            v = xadd(v, xmul(xmul(xmul(tile[((tz + dz) * MCW2 + ty + dy) * MCW2 + tx + dx], 0.5), 0.5), 0.5));
+      m |= (uint32_t)(v < iso) << tx;
+    }
+    mask[r] = m;
+  }
+}
+
+template <int DEG>
+__device__ __forceinline__ void mc_block_masks(double* tile, uint32_t* mask, const double* __restrict__ x,
+                                               uint32_t blk, int res, double iso) {
+  uint32_t bx, by, bz;
+  unmorton3(blk, bx, by, bz);
+  if (DEG == 2) {
+    mc_load_tile2(tile, x, blk, res);
+    __syncthreads();
+    mc_build_masks2(tile, mask, iso);
+  } else {
+    mc_load_tile(tile, x, blk, res);
+    __syncthreads();
+    mc_build_masks(tile, mask, bx * 16, by * 16, bz * 16, res, iso);
+  }
+}
+
 // case of local cell (lx, ly, lz) from the row masks (corner order of c_co)
 __device__ __forceinline__ uint32_t mc_mask_case(const uint32_t* mask, int lx, int ly, int lz) {
   const uint32_t m00 = mask[lz * MCW + ly] >> lx, m10 = mask[lz * MCW + ly + 1] >> lx;
@@ -378,17 +512,14 @@ __device__ __forceinline__ uint32_t mc_mask_case(const uint32_t* mask, int lx, i
          ((m01 >> 1) & 1u) << 5 | ((m11 >> 1) & 1u) << 6 | (m11 & 1u) << 7;
 }
 
+template <int DEG>
 __global__ void __launch_bounds__(256) k_mc_block_count(const double* __restrict__ x, uint32_t D, double iso,
                                                         uint32_t* __restrict__ blockcnt) {
-  __shared__ double tile[MCW * MCW * MCW];
+  __shared__ double tile[DEG == 2 ? MCW2 * MCW2 * MCW2 : MCW * MCW * MCW];
   __shared__ uint32_t mask[MCW * MCW];
   const int res = 1 << D;
   const uint32_t blk = blockIdx.x;
-  uint32_t bx, by, bz;
-  unmorton3(blk, bx, by, bz);
-  mc_load_tile(tile, x, blk, res);
-  __syncthreads();
-  mc_build_masks(tile, mask, bx * 16, by * 16, bz * 16, res, iso);
+  mc_block_masks<DEG>(tile, mask, x, blk, res, iso);
   __syncthreads();
   // thread = one x row of 16 cells
   const int ly = threadIdx.x & 15, lz = threadIdx.x >> 4;
@@ -405,20 +536,17 @@ __global__ void __launch_bounds__(256) k_mc_block_count(const double* __restrict
 }
 
 // active blocks only (list from a compaction of blockcnt > 0); cells written in Morton order
+template <int DEG>
 __global__ void __launch_bounds__(256) k_mc_block_emit(const double* __restrict__ x, uint32_t D, double iso,
                                                        const uint32_t* __restrict__ ablk,
                                                        const uint32_t* __restrict__ blockoff,
                                                        uint32_t* __restrict__ acell, uint8_t* __restrict__ acase,
                                                        uint32_t* __restrict__ nedge, uint32_t* __restrict__ ntri) {
-  __shared__ double tile[MCW * MCW * MCW];
+  __shared__ double tile[DEG == 2 ? MCW2 * MCW2 * MCW2 : MCW * MCW * MCW];
   __shared__ uint32_t mask[MCW * MCW];
   const int res = 1 << D;
   const uint32_t blk = ablk[blockIdx.x];
-  uint32_t bx, by, bz;
-  unmorton3(blk, bx, by, bz);
-  mc_load_tile(tile, x, blk, res);
-  __syncthreads();
-  mc_build_masks(tile, mask, bx * 16, by * 16, bz * 16, res, iso);
+  mc_block_masks<DEG>(tile, mask, x, blk, res, iso);
   __syncthreads();
   typedef cub::BlockScan<int, 256> BS;
   __shared__ typename BS::TempStorage tmp;
@@ -479,9 +607,10 @@ struct MaxOp {
   __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
 };
 void evaluate_points(pr_context* c, uint32_t D, const double* d_x64, const double* d_pts, uint64_t stride,
-                     uint64_t n, double* d_out) {
+                     uint64_t n, double* d_out, int degree) {
   if (n == 0) return;
-  k_eval_points<<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
+  if (degree == 2) k_eval_points<2><<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
+  else k_eval_points<1><<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
   PR_CHECK_LAUNCH();
 }
 
@@ -491,7 +620,8 @@ double stage_iso(pr_context* c, const double* d_x64) {
   if (nb < 1) nb = 1;
   double* part = c->buf<double>("iso_part", 2 * (size_t)nb);
   double* out = c->buf<double>("iso_out", 1);
-  k_iso_partial<<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, c->get<double>("upos"), P, part);
+  if (c->degree == 2) k_iso_partial<2><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, c->get<double>("upos"), P, part);
+  else k_iso_partial<1><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, c->get<double>("upos"), P, part);
   PR_CHECK_LAUNCH();
   k_iso_final<<<1, 32, 0, c->stream>>>(part, nb, out);
   PR_CHECK_LAUNCH();
@@ -501,7 +631,7 @@ double stage_iso(pr_context* c, const double* d_x64) {
   return sum / (double)P;
 }
 
-void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool back_transform) {
+void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool back_transform, int degree) {
   const uint64_t n = 1ull << (3 * D);
   cudaStream_t s = c->stream;
   c->nv = c->nt = 0;
@@ -519,7 +649,8 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     uint32_t* flag = c->buf<uint32_t>("mc_flag", (size_t)nblk + 1);
     uint32_t* fpos = c->buf<uint32_t>("mc_fpos", (size_t)nblk + 1);
     uint32_t* ablk = c->buf<uint32_t>("mc_ablk", (size_t)nblk);
-    k_mc_block_count<<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
+    if (degree == 2) k_mc_block_count<2><<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
+    else k_mc_block_count<1><<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
     PR_CHECK_LAUNCH();
     PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
     k_flags_nonzero<<<grid_for(nblk + 1), kThreads, 0, s>>>(blockcnt, nblk + 1, flag);
@@ -542,13 +673,15 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     acase = c->buf<uint8_t>("mc_acase", A);
     nedge = c->buf<uint32_t>("mc_nedge", A + 1);
     ntri = c->buf<uint32_t>("mc_ntri", A + 1);
-    k_mc_block_emit<<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    if (degree == 2) k_mc_block_emit<2><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    else k_mc_block_emit<1><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
     PR_CHECK_LAUNCH();
   } else {
     const unsigned nblk = (unsigned)((n + kThreads - 1) / kThreads);
     uint32_t* blockcnt = c->buf<uint32_t>("mc_blockcnt", (size_t)nblk + 1);
     uint32_t* blockoff = c->buf<uint32_t>("mc_blockoff", (size_t)nblk + 1);
-    k_mc_count<<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
+    if (degree == 2) k_mc_count<2><<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
+    else k_mc_count<1><<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
     PR_CHECK_LAUNCH();
     PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
     PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, blockcnt, blockoff, (int64_t)nblk + 1, s));
@@ -564,7 +697,8 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     acase = c->buf<uint8_t>("mc_acase", A);
     nedge = c->buf<uint32_t>("mc_nedge", A + 1);
     ntri = c->buf<uint32_t>("mc_ntri", A + 1);
-    k_mc_compact<<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
+    if (degree == 2) k_mc_compact<2><<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
+    else k_mc_compact<1><<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
     PR_CHECK_LAUNCH();
   }
   eoff = c->buf<uint32_t>("mc_eoff", A + 1);
@@ -593,7 +727,8 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
   uint32_t* sidb = c->buf<uint32_t>("mc_sidb", E);
   int* err = c->buf<int>("mc_err", 1);
   PR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  k_mc_vertices<<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
+  if (degree == 2) k_mc_vertices<2><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
+  else k_mc_vertices<1><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
   PR_CHECK_LAUNCH();
 
   // stable LSD sort: by k2 (z key), then by k1 (x,y key); ties keep slot order

@@ -1,0 +1,237 @@
+"""Degree-2 (quadratic B-spline) GPU path against the oracle's degree-2 restatement, through the
+C ABI (pr_params.degree = 2).
+
+Bit-exact: normal splat (values and weights), evaluation of the implicit function, marching-cubes
+vertices and triangles given identical coefficients and iso.  Tolerance: right-hand side and
+FP64 operator relative 1e-12 (the GPU sums the separable factors in another order), FP32 operator
+relative L2 1e-6; solved coefficients relative L2 <= 1e-6 against the oracle's FP64 CG solve of
+the same system; iso relative 1e-9; pipeline vertices <= 1e-5 x bbox diagonal.
+"""
+import functools
+
+import numpy as np
+import pytest
+
+import oracle
+import poissonreconstruction_b200 as prb
+from poissonreconstruction_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+COEF_TOL = 1e-6
+ISO_TOL = 1e-9
+VERT_TOL = 1e-5
+FP64_TOL = 1e-12
+
+
+@functools.lru_cache(maxsize=None)
+def cloud(name):
+    return {
+        "sphere": lambda: synthetic.sphere(4000, seed=21),
+        "torus": lambda: synthetic.torus(6000, seed=22),
+        "ellipsoid": lambda: synthetic.ellipsoid(5000, seed=23, radii=(1.0, 0.6, 0.3), noise=0.01),
+    }[name]()
+
+
+CASES = [("sphere", 4, 4.0), ("torus", 5, 4.0), ("ellipsoid", 5, 0.0), ("torus", 6, 4.0)]
+
+
+def params(depth, pw, **kw):
+    return prb.ReconstructParams(depth=depth, point_weight=pw, degree=2, **kw)
+
+
+@functools.lru_cache(maxsize=None)
+def oracle_tree(name, depth, pw):
+    unit, m = oracle.to_unit(cloud(name))
+    return oracle.Tree2(depth, unit, pw), unit, m
+
+
+@functools.lru_cache(maxsize=None)
+def oracle_solution(name, depth, pw):
+    t, _, _ = oracle_tree(name, depth, pw)
+    x, it, rr = t.solve(tol=1e-13, maxit=200000)
+    assert rr <= 1e-12, rr
+    return x
+
+
+@pytest.mark.parametrize("name,depth,pw", CASES)
+def test_setup(ctx, name, depth, pw):
+    ctx.solve(cloud(name), params(depth, pw))
+    t, unit, m = oracle_tree(name, depth, pw)
+    d, n, m_gpu = ctx.info()
+    assert d == depth and n == 8 ** depth and np.array_equal(m_gpu, m)
+    nf, w = t.normal_field()
+    nf_g, w_g = ctx.normal_field()
+    assert np.array_equal(w_g, w)
+    assert np.array_equal(nf_g, nf)
+    b, b_g = t.rhs(), ctx.rhs()
+    assert np.max(np.abs(b_g - b)) <= FP64_TOL * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("name,depth,pw", CASES)
+def test_operator(ctx, name, depth, pw):
+    ctx.solve(cloud(name), params(depth, pw))
+    t, _, _ = oracle_tree(name, depth, pw)
+    rng = np.random.default_rng(depth)
+    for x in (rng.standard_normal(t.n), np.ones(t.n)):
+        y_ref = t.apply(x)
+        y64 = ctx.apply_operator(x, prb.PR_PRECISION_FP64)
+        y32 = ctx.apply_operator(x, prb.PR_PRECISION_MIXED)
+        assert np.max(np.abs(y64 - y_ref)) <= FP64_TOL * np.max(np.abs(y_ref))
+        assert np.linalg.norm(y32 - y_ref) <= 1e-6 * np.linalg.norm(y_ref)
+
+
+@pytest.mark.parametrize("precision", [prb.PR_PRECISION_FP64, prb.PR_PRECISION_MIXED])
+@pytest.mark.parametrize("name,depth,pw", CASES)
+def test_converged_solve(ctx, name, depth, pw, precision):
+    pts = cloud(name)
+    mesh, st = ctx.reconstruct(pts, params(depth, pw, precision=precision, target_rel_residual=1e-10,
+                                           max_iters=400))
+    assert st.converged == 1 and st.rel_residual <= 1e-10, st
+    # a multigrid preconditioner: iterations do not grow with the depth
+    assert st.pcg_iterations <= 40, st.pcg_iterations
+    x_gpu = ctx.coefficients()
+    x_ref = oracle_solution(name, depth, pw)
+    err = np.linalg.norm(x_gpu - x_ref) / np.linalg.norm(x_ref)
+    assert err <= COEF_TOL, err
+    _, unit, m = oracle_tree(name, depth, pw)
+    iso_ref = np.mean(oracle.evaluate2(depth, x_gpu, unit[:, :3]))
+    assert abs(st.iso_value - iso_ref) <= ISO_TOL * abs(iso_ref)
+    # marching cubes of the GPU coefficients: bit-exact against the oracle
+    v_ref, t_ref = oracle.extract_surface2(depth, x_gpu, st.iso_value)
+    assert mesh.triangles.shape == t_ref.shape and np.array_equal(mesh.triangles, t_ref)
+    minv = oracle.mat4_inverse(m)
+    v_model = np.array([oracle.transform_point(minv, v) for v in v_ref]) if len(v_ref) else v_ref
+    assert np.array_equal(mesh.vertices, v_model)
+
+
+@pytest.mark.parametrize("depth", [2, 3, 4, 5])
+@pytest.mark.parametrize("iso", [-0.3, 0.0, 0.25])
+def test_marching_cubes_bit_exact_random_field(ctx, depth, iso):
+    ctx.solve(cloud("sphere"), params(depth, 4.0))
+    rng = np.random.default_rng(200 + depth)
+    x = rng.standard_normal(8 ** depth)
+    mesh = ctx.extract(x, iso)
+    v_ref, t_ref = oracle.extract_surface2(depth, x, iso)
+    assert np.array_equal(mesh.vertices, v_ref)
+    assert np.array_equal(mesh.triangles, t_ref)
+
+
+def test_marching_cubes_degenerate_values(ctx):
+    depth = 4
+    ctx.solve(cloud("sphere"), params(depth, 4.0))
+    rng = np.random.default_rng(9)
+    x = rng.integers(-2, 3, size=8 ** depth).astype(np.float64)
+    for iso in (0.0, 1.0, 0.5, -1.0, 0.125):
+        mesh = ctx.extract(x, iso)
+        v_ref, t_ref = oracle.extract_surface2(depth, x, iso)
+        assert np.array_equal(mesh.vertices, v_ref)
+        assert np.array_equal(mesh.triangles, t_ref)
+
+
+@pytest.mark.parametrize("depth", [3, 5])
+def test_evaluate_bit_exact(ctx, depth):
+    ctx.solve(cloud("torus"), params(depth, 4.0))
+    rng = np.random.default_rng(5)
+    q = rng.uniform(-0.1, 1.1, size=(5000, 3))
+    h = 1.0 / (1 << depth)
+    q[:100] = np.round(q[:100] / h) * h
+    x = rng.standard_normal(8 ** depth)
+    assert np.array_equal(ctx.evaluate(q, coefficients=x), oracle.evaluate2(depth, x, q))
+
+
+@pytest.mark.parametrize("name", ["sphere", "torus"])
+def test_pipeline_mesh_vs_oracle(ctx, name):
+    depth, pw = 5, 4.0
+    pts = cloud(name)
+    mesh, st = ctx.reconstruct(pts, params(depth, pw, target_rel_residual=1e-10))
+    v_ref, t_ref, iso_ref, rr, _ = oracle.reconstruct2(pts, depth, point_weight=pw, tol=1e-13)
+    assert rr <= 1e-12
+    assert abs(st.iso_value - iso_ref) <= ISO_TOL * abs(iso_ref)
+    lo, hi = pts[:, :3].min(0), pts[:, :3].max(0)
+    diag = np.linalg.norm(hi - lo)
+    if mesh.triangles.shape == t_ref.shape and np.array_equal(mesh.triangles, t_ref):
+        assert np.max(np.abs(mesh.vertices - v_ref)) <= VERT_TOL * diag
+    else:  # a corner value within rounding of iso flipped: compare nearest vertices
+        from scipy.spatial import cKDTree
+        d, _ = cKDTree(v_ref).query(mesh.vertices)
+        assert np.quantile(d, 0.99) <= VERT_TOL * diag
+
+
+@pytest.mark.parametrize("depth", [1, 2, 3])
+def test_small_depths(ctx, depth):
+    pts = cloud("sphere")
+    for precision in (prb.PR_PRECISION_FP64, prb.PR_PRECISION_MIXED):
+        mesh, st = ctx.reconstruct(pts, params(depth, 4.0, precision=precision, target_rel_residual=1e-12))
+        assert st.rel_residual <= 1e-12, st
+        x_ref = oracle_solution("sphere", depth, 4.0)
+        assert np.linalg.norm(ctx.coefficients() - x_ref) <= COEF_TOL * np.linalg.norm(x_ref)
+
+
+def test_default_tolerance_error_vs_fp64(ctx):
+    """At the default target (1e-6 relative residual) the mixed and the FP64 solves agree with
+    each other and with the converged oracle solution to the error that residual allows."""
+    name, depth, pw = "torus", 6, 4.0
+    pts = cloud(name)
+    x_ref = oracle_solution(name, depth, pw)
+    errs = {}
+    for precision in (prb.PR_PRECISION_MIXED, prb.PR_PRECISION_FP64):
+        _, st = ctx.reconstruct(pts, params(depth, pw, precision=precision))
+        assert st.converged == 1 and st.rel_residual <= 1e-6
+        errs[precision] = np.linalg.norm(ctx.coefficients() - x_ref) / np.linalg.norm(x_ref)
+    print("degree-2 coefficient error at 1e-6 residual: mixed %.2e, fp64 %.2e" %
+          (errs[prb.PR_PRECISION_MIXED], errs[prb.PR_PRECISION_FP64]))
+    assert max(errs.values()) <= 1e-4
+
+
+def test_edge_inputs(ctx):
+    one = np.array([[0.3, -0.2, 0.1, 0.0, 0.0, 2.0]])
+    mesh, st = ctx.reconstruct(one, params(4, 4.0))
+    assert st.fem_nodes == 8 ** 4
+    same = np.repeat(one, 50, axis=0)
+    ctx.solve(same, params(4, 4.0))
+    t = oracle.Tree2(4, oracle.to_unit(same)[0], 4.0)
+    nf, w = t.normal_field()
+    nf_g, w_g = ctx.normal_field()
+    assert np.array_equal(w_g, w) and np.array_equal(nf_g, nf)
+    # points exactly on cell boundaries (t = 0 on every axis)
+    g = np.stack(np.meshgrid(np.arange(5), np.arange(5), np.arange(5)), -1).reshape(-1, 3) / 4.0
+    grid_pts = np.hstack([g, np.tile([0.0, 1.0, 0.0], (len(g), 1))])
+    ctx.solve(grid_pts, params(3, 4.0, scale=1.0))
+    t = oracle.Tree2(3, oracle.to_unit(grid_pts, 1.0)[0], 4.0)
+    nf, w = t.normal_field()
+    nf_g, w_g = ctx.normal_field()
+    assert np.array_equal(w_g, w) and np.array_equal(nf_g, nf)
+    b = t.rhs()
+    assert np.max(np.abs(ctx.rhs() - b)) <= FP64_TOL * np.max(np.abs(b))
+
+
+def test_rejected_combinations(ctx):
+    pts = cloud("sphere")
+    with pytest.raises(prb.ReconstructError) as e:
+        ctx.reconstruct(pts, prb.ReconstructParams(depth=4, degree=3))
+    assert e.value.code == prb.PR_ERR_INVALID_ARGUMENT
+    with pytest.raises(prb.ReconstructError) as e:
+        ctx.reconstruct(pts, params(4, 4.0, solve_mode=prb.PR_SOLVE_REFERENCE_SCHEDULE))
+    assert e.value.code == prb.PR_ERR_INVALID_ARGUMENT
+    ctx.solve(pts, params(4, 4.0))
+    with pytest.raises(prb.ReconstructError) as e:
+        ctx.loss_backward(pts[:10, :3], n_points=len(pts))
+    assert e.value.code == prb.PR_ERR_STATE
+    # the context still serves degree 1 afterwards
+    mesh, st = ctx.reconstruct(pts, prb.ReconstructParams(depth=4, point_weight=4.0))
+    assert len(mesh.triangles) > 0
+
+
+@pytest.mark.parametrize("precision", [prb.PR_PRECISION_MIXED, prb.PR_PRECISION_FP64])
+def test_solve_is_deterministic(precision):
+    pts = synthetic.torus(60_000, seed=19)
+    p = params(7, 4.0, precision=precision)
+    with prb.Context(0) as c1, prb.Context(0) as c2:
+        c1.solve(pts, p)
+        x1 = c1.coefficients()
+        c1.solve(pts, p)
+        x2 = c1.coefficients()
+        c2.solve(pts, p)
+        x3 = c2.coefficients()
+    assert np.array_equal(x1, x2) and np.array_equal(x1, x3)

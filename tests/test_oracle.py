@@ -250,3 +250,112 @@ def test_adjoint_matches_finite_differences(upstream):
         an = grads[i, col]
         ref = max(abs(an), 1e-2 * gmax[col])
         assert abs(fd - an) <= 1e-4 * ref, (i, col, fd, an)
+
+
+# ---------------------------------------------------------------- degree 2 (extension)
+def test_deg2_constants_exact():
+    """1-D integrals of the quadratic B-spline (src/bspline.rs:334-345) at offsets -2..2."""
+    m, s, g = oracle.deg2_constants()
+    assert np.allclose(m, [1 / 120, 13 / 60, 11 / 20, 13 / 60, 1 / 120], rtol=0, atol=1e-15)
+    assert np.allclose(s, [-1 / 6, -1 / 3, 1.0, -1 / 3, -1 / 6], rtol=0, atol=1e-15)
+    assert np.allclose(g, [1 / 24, 5 / 12, 0.0, -5 / 12, -1 / 24], rtol=0, atol=1e-15)
+
+
+def test_deg2_basis_matches_crate_values():
+    """src/bspline.rs:412-417: N_2(0.5) = 0.125, N_2(1.5) = 0.75.  Node i carries
+    N_2(x/h - i + 1), so at s = x/h = 1.5 nodes 0, 1, 2 weigh N_2(2.5), N_2(1.5), N_2(0.5)."""
+    D = 2
+    h = 1.0 / (1 << D)
+    p = np.array([[1.5 * h, 1.5 * h, 1.5 * h]])
+    for node, weight in (((1, 1, 1), 0.75 ** 3), ((2, 1, 1), 0.125 * 0.75 ** 2), ((0, 2, 1), 0.125 ** 2 * 0.75),
+                         ((3, 1, 1), 0.0)):
+        x = np.zeros(8 ** D)
+        x[oracle.morton(*node)] = 1.0
+        assert oracle.evaluate2(D, x, p)[0] == weight
+
+
+def _kron_operator(D, pw_unit=None):
+    """Dense h (S M M + M S M + M M S) with truncated rows, in Morton order (x fastest axis)."""
+    m, s, _ = oracle.deg2_constants()
+    res = 1 << D
+
+    def band(c):
+        a = np.zeros((res, res))
+        for i in range(res):
+            for d in range(-2, 3):
+                if 0 <= i + d < res:
+                    a[i, i + d] = c[d + 2]
+        return a
+
+    M, S = band(m), band(s)
+    K = (np.kron(np.kron(M, M), S) + np.kron(np.kron(M, S), M) + np.kron(np.kron(S, M), M)) / res
+    perm = np.array([oracle.morton(i % res, (i // res) % res, i // (res * res)) for i in range(res ** 3)])
+    P = np.zeros_like(K)
+    P[perm[:, None], perm[None, :]] = K
+    return P
+
+
+def test_deg2_operator_matches_kronecker_definition():
+    pts = synthetic.sphere(500, seed=31)
+    unit, _ = oracle.to_unit(pts)
+    D = 3
+    t = oracle.Tree2(D, unit, 0.0)  # no screening: A = K exactly (wg = 0)
+    K = _kron_operator(D)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(t.n)
+    assert np.allclose(t.apply(x), K @ x, rtol=0, atol=1e-13 * np.abs(K @ x).max())
+    assert np.allclose(K, K.T)
+    assert np.linalg.eigvalsh(K).min() > 0
+
+
+def test_deg2_rhs_matches_kronecker_definition():
+    m, s, g = oracle.deg2_constants()
+    pts = synthetic.sphere(800, seed=32)
+    unit, _ = oracle.to_unit(pts)
+    D = 3
+    res = 1 << D
+    t = oracle.Tree2(D, unit, 0.0)
+    nf, w = t.normal_field()
+
+    def band(c):
+        a = np.zeros((res, res))
+        for i in range(res):
+            for d in range(-2, 3):
+                if 0 <= i + d < res:
+                    a[i, i + d] = c[d + 2]
+        return a
+
+    M, G = band(m), band(g)
+    perm = np.array([oracle.morton(i % res, (i // res) % res, i // (res * res)) for i in range(res ** 3)])
+    nat = nf[perm]  # natural order (x fastest)
+    b = (np.kron(np.kron(M, M), G) @ nat[:, 0] + np.kron(np.kron(M, G), M) @ nat[:, 1] +
+         np.kron(np.kron(G, M), M) @ nat[:, 2]) / res ** 2
+    b_ref = t.rhs()[perm]
+    assert np.allclose(b_ref, b, rtol=0, atol=1e-14 * np.abs(b).max())
+
+
+def test_deg2_normal_field_is_normalised_splat():
+    pts = synthetic.sphere(300, seed=33)
+    unit, _ = oracle.to_unit(pts, 0.5)  # unit coordinates in [0.25, 0.75]: all 27 nodes inside
+    t = oracle.Tree2(3, unit, 0.0)
+    nf, w = t.normal_field()
+    assert np.isclose(w.sum(), len(pts))  # partition of unity: 27 weights of a point sum to 1
+    hit = w > 0
+    assert np.all(np.linalg.norm(nf[hit], axis=1) <= 1.0 + 1e-12)
+
+
+def test_deg2_solve_and_pipeline():
+    pts = synthetic.sphere(3000, seed=34)
+    unit, _ = oracle.to_unit(pts)
+    t = oracle.Tree2(4, unit, 4.0)
+    rng = np.random.default_rng(2)
+    x, y = rng.standard_normal(t.n), rng.standard_normal(t.n)
+    assert abs(y @ t.apply(x) - x @ t.apply(y)) <= 1e-12 * abs(y @ t.apply(x))
+    sol, it, rr = t.solve(tol=1e-12)
+    assert rr <= 1e-12
+    v, tri, iso, rr2, c = oracle.reconstruct2(pts, 4)
+    assert rr2 <= 1e-12 and len(tri) > 100 and tri.max() < len(v)
+    # closed surface: every edge is shared by exactly two triangles
+    e = np.sort(np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]]), axis=1)
+    _, counts = np.unique(e, axis=0, return_counts=True)
+    assert np.all(counts == 2)
