@@ -176,7 +176,11 @@ int pr_ctx_apply_operator_device(pr_context* ctx, const void* d_x, void* d_y, in
  * prolongation and a dot product, 5 = residual fused with the restriction, 6 = per-node
  * stencil (ids 0-6 on the finest level's coefficients), 7 and 8 = ids 4 and 5 on a coarse
  * level's (rows on the low domain faces use their own table rows), 9 = the CG update fused
- * with the first pre-smoothing sweep.  Times `reps` launches
+ * with the first pre-smoothing sweep.  Degree 2 (finest level of `depth`): 20 = Chebyshev
+ * smoothing step (TMA-fed), 21 = the same with register staging, 22 / 23 = A x (TMA / register
+ * staging), 24 = f - A x (TMA), 25 = restriction, 26 = prolongation + add, 27 = first
+ * Chebyshev step, 28 = the first two steps fused (from f), 29 = the third step recomputing the
+ * first from f (TMA variants need depth >= 6).  Times `reps` launches
  * with CUDA events on the context's stream; returns the mean ms per launch and the
  * algorithmic HBM bytes per launch. */
 int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precision, int reps, double* ms_per_launch,

@@ -443,7 +443,10 @@ class Context:
 
     KERNELS = {"spmv": 0, "spmv_xpby": 1, "smooth_first": 2, "smooth": 3, "smooth_prolong_dot": 4,
                "resid_restrict": 5, "stencil_per_node": 6, "smooth_prolong_dot_coarse": 7,
-               "resid_restrict_coarse": 8, "cg_update_presmooth": 9}
+               "resid_restrict_coarse": 8, "cg_update_presmooth": 9,
+               # degree 2 (finest level of the given depth)
+               "d2_cheb": 20, "d2_cheb_regs": 21, "d2_apply": 22, "d2_apply_regs": 23, "d2_resid": 24,
+               "d2_restrict": 25, "d2_prolong": 26, "d2_cheb_first": 27, "d2_cheb_f": 28, "d2_cheb_pf": 29}
 
     def kernel_bench(self, kernel, depth, precision=PR_PRECISION_MIXED, reps=10):
         """(ms per launch, algorithmic bytes per launch) of one solver kernel."""

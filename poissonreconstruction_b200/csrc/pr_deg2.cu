@@ -24,6 +24,8 @@
 // 4^3 level is solved with a dense inverse.  FP32 inner solves with FP64 residual refinement,
 // or FP64 throughout.  The solved coefficients are permuted to the Morton order of the
 // degree-1 path for evaluation and marching cubes.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -39,7 +41,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int TX = 32, TY = 8;           // output columns of a CTA
 constexpr int SW = TX + 4, SH = TY + 4;  // staged input plane (halo 2)
-constexpr int kZChunk = 64;              // output planes per CTA
+constexpr int kZChunk = 64;              // output planes per CTA (k_op2)
+constexpr int kZChunk3 = 76;             // output planes per CTA (k_op3): 80 staged planes = 16 x 5
 constexpr int kChebSteps = 3;            // Chebyshev degree of one smoothing
 constexpr double kLamMax = 2.1;          // bound of the spectrum of D^-1 (K + wg I) on every level
 constexpr double kLamRatio = 15.0;       // smoothed interval [kLamMax / kLamRatio, kLamMax]
@@ -257,6 +260,412 @@ __global__ void __launch_bounds__(kThreads) k_op2(const T* __restrict__ x, const
   }
 }
 
+// ------------------------------------------------------------------ the TMA-fed operator
+// For levels with res >= 64 (k_op2 serves the smaller ones).  A CTA owns 64 x 8 columns, each
+// thread an x-adjacent pair of them, and streams up to 64 z planes.  One elected thread keeps five
+// planes in flight: per plane a tiled TMA load of the haloed input (box BW x 12 x 1 from a 16-byte
+// aligned x; the tensor map's zero fill supplies the halo outside the grid) and, for the epilogue,
+// the f / xp planes of the output two planes behind (box 64 x 8 x 1), completing on the stage's
+// mbarrier.  The five stages are also the five-plane z window, so the plane loop is unrolled by
+// five and every window index is static.
+//
+// Interior CTAs (all outputs at least `edge` rows from the x and y faces, where the level's 1-D
+// matrices equal their interior row) take the coefficients from the kernel parameters; the CTAs
+// along the x and y faces run the EDGE instantiation with per-thread rows.  Planes within `edge`
+// of the z faces read their z row from the tables in both.
+//
+// Waits are bounded: a wait that runs out sets *err, the CTA stops after the next barrier and
+// thread 0 waits (bounded again) for the loads it still has in flight.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// false once 2^22 polls have failed (each poll may itself suspend the thread for a while)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t k = 0; k < (1u << 22); ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
+template <typename T>
+struct Geo3 {
+  static constexpr int NS = 5;                          // stages = z window
+  static constexpr int TXP = 64;                        // output columns in x (32 pairs)
+  static constexpr int BW = sizeof(T) == 4 ? 72 : 68;   // staged width from a 16-byte aligned start
+  static constexpr int XOFF = sizeof(T) == 4 ? 2 : 0;   // stage column of global x0 - 2
+  static constexpr uint32_t XBYTES = BW * SH * sizeof(T);
+  static constexpr uint32_t OBYTES = TXP * TY * sizeof(T);
+  static constexpr size_t OFF_X = 0;
+  static constexpr size_t OFF_F = OFF_X + (size_t)NS * XBYTES;
+  static constexpr size_t OFF_P = OFF_F + (size_t)NS * OBYTES;
+  static constexpr size_t OFF_UM = OFF_P + (size_t)NS * OBYTES;
+  static constexpr size_t OFF_US = OFF_UM + 2 * (size_t)SH * TXP * sizeof(T);
+  static constexpr size_t OFF_K = OFF_US + 2 * (size_t)SH * TXP * sizeof(T);  // EDGE, kOpChebF: D^-1 scale
+  static constexpr size_t OFF_DX = OFF_K + (size_t)SH * BW * sizeof(T);      // EDGE: diagonal entries
+  static constexpr size_t OFF_BAR = OFF_DX + (size_t)(BW + SH) * 2 * sizeof(T);
+  static constexpr size_t BYTES = OFF_BAR + NS * 8 + 16;
+};
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  typedef float2 type;
+};
+template <>
+struct Vec2<double> {
+  typedef double2 type;
+};
+
+// kOpChebF:  out = (1 + ca) x1 + cb D^-1 (f - A x1), x1 = c0 D^-1 f (the first step from zero,
+//            then the second); the staged input is f.
+// kOpChebPF: out = x + ca (x - xp) + cb D^-1 (f - A x) with xp = c0 D^-1 f (the third step after
+//            kOpChebF: its previous iterate is recomputed from f).
+enum { kOpChebF = 3, kOpChebPF = 4 };
+
+template <typename T>
+struct Op3Args {
+  LevelView<T> lv;
+  T im[5], is[5];  // interior rows of the 1-D matrices
+  T invd;          // 1 / interior diagonal
+  int edge;        // rows [edge, res - edge) equal the interior row
+  T ca, cb, c0;
+  int use_p;       // kOpCheb: xp given
+  int nbx, nby;    // tiles per axis (x: 64 columns, y: 8 rows)
+  int all;         // EDGE: the grid enumerates every tile, not only the face tiles
+  int* err;
+};
+
+// the (x, y) tile of an EDGE CTA: the first and the last tile row, then the first and the last
+// tile of every row in between
+__device__ __forceinline__ void edge_tile(int j, int nbx, int nby, int all, int& bx, int& by) {
+  if (all || nbx <= 2 || nby <= 2) {
+    bx = j % nbx;
+    by = j / nbx;
+  } else if (j < 2 * nbx) {
+    bx = j % nbx;
+    by = j < nbx ? 0 : nby - 1;
+  } else {
+    const int k = j - 2 * nbx;
+    bx = (k & 1) ? nbx - 1 : 0;
+    by = 1 + (k >> 1);
+  }
+}
+
+// 5-tap filters.  Interior rows are symmetric (c[0] = c[4], c[1] = c[3]): two filters of the
+// same input share the pair sums.
+template <typename T>
+__device__ __forceinline__ void filt2_sym(const T* v, const T* m, const T* s, T& om, T& os) {
+  const T p0 = v[0] + v[4], p1 = v[1] + v[3];
+  om = m[0] * p0 + m[1] * p1 + m[2] * v[2];
+  os = s[0] * p0 + s[1] * p1 + s[2] * v[2];
+}
+template <typename T>
+__device__ __forceinline__ T filt(const T* v, const T* c) {
+  return c[0] * v[0] + c[1] * v[1] + c[2] * v[2] + c[3] * v[3] + c[4] * v[4];
+}
+
+template <typename T, int MODE, bool EDGE>
+__global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtensorMap mx,
+                                                  const __grid_constant__ CUtensorMap mf,
+                                                  const __grid_constant__ CUtensorMap mp, T* out,
+                                                  const __grid_constant__ Op3Args<T> A) {
+  typedef Geo3<T> G;
+  typedef typename Vec2<T>::type V2;
+  constexpr int NS = G::NS, BW = G::BW, XOFF = G::XOFF, TXP = G::TXP;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T(*s_x)[SH][BW] = reinterpret_cast<T(*)[SH][BW]>(smem + G::OFF_X);
+  T(*s_f)[TY][TXP] = reinterpret_cast<T(*)[TY][TXP]>(smem + G::OFF_F);
+  T(*s_p)[TY][TXP] = reinterpret_cast<T(*)[TY][TXP]>(smem + G::OFF_P);
+  T(*s_um)[SH][TXP] = reinterpret_cast<T(*)[SH][TXP]>(smem + G::OFF_UM);
+  T(*s_us)[SH][TXP] = reinterpret_cast<T(*)[SH][TXP]>(smem + G::OFF_US);
+  T(*s_k)[BW] = reinterpret_cast<T(*)[BW]>(smem + G::OFF_K);
+  T* s_dx = reinterpret_cast<T*>(smem + G::OFF_DX);  // [BW][2] then [SH][2]: (m, s) diagonal entries
+  T* s_dy = s_dx + 2 * BW;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NS * 8);
+  const LevelView<T>& lv = A.lv;
+  const int res = 1 << lv.L;
+  const int64_t plane = (int64_t)res * res;
+  const int t = threadIdx.x, p = t & 31, ty = t >> 5;
+  int bx, by;
+  if (EDGE) edge_tile(blockIdx.x, A.nbx, A.nby, A.all, bx, by);
+  else {
+    bx = blockIdx.x + 1;
+    by = blockIdx.y + 1;
+  }
+  const int x0 = bx * TXP, y0 = by * TY;
+  const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
+  const int gx = x0 + 2 * p, gy = y0 + ty;  // res >= 64: every column is inside the grid
+  const int nplanes = z1 - z0 + 4;
+  const int ngroups = (nplanes + NS - 1) / NS;  // planes past z1 + 1 read zeros and emit nothing
+  constexpr bool use_f = MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF;
+  const bool use_p = MODE == kOpCheb && A.use_p;
+  const uint32_t bytes = G::XBYTES + (use_f ? G::OBYTES : 0u) + (use_p ? G::OBYTES : 0u);
+  if (t == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (EDGE && MODE == kOpChebF) {
+    for (int i = t; i < BW; i += kThreads) {
+      const int X = x0 - 2 - XOFF + i;
+      const bool in = X >= 0 && X < res;
+      s_dx[2 * i] = in ? lv.tM[5 * X + 2] : T(0);
+      s_dx[2 * i + 1] = in ? lv.tS[5 * X + 2] : T(0);
+    }
+    for (int i = t; i < SH; i += kThreads) {
+      const int Y = y0 - 2 + i;
+      const bool in = Y >= 0 && Y < res;
+      s_dy[2 * i] = in ? lv.tM[5 * Y + 2] : T(0);
+      s_dy[2 * i + 1] = in ? lv.tS[5 * Y + 2] : T(0);
+    }
+  }
+  __syncthreads();
+  auto issue = [&](int it) {
+    const int s = it % NS, zin = z0 - 2 + it;
+    mbar_expect_tx(&bar[s], bytes);
+    tma_load_3d(&s_x[s][0][0], &mx, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
+    if (use_f) tma_load_3d(&s_f[s][0][0], &mf, x0, y0, zin - 2, &bar[s]);
+    if (use_p) tma_load_3d(&s_p[s][0][0], &mp, x0, y0, zin - 2, &bar[s]);
+  };
+  const int nissue = ngroups * NS;
+  if (t == 0)
+    for (int it = 0; it < NS; ++it) issue(it);
+  // EDGE: x rows of the pair and the y row of this thread
+  T cmx[2][5], csx[2][5], cmy[5], csy[5];
+  if (EDGE) {
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+      cmx[0][d] = lv.tM[5 * gx + d];
+      csx[0][d] = lv.tS[5 * gx + d];
+      cmx[1][d] = lv.tM[5 * gx + 5 + d];
+      csx[1][d] = lv.tS[5 * gx + 5 + d];
+      cmy[d] = lv.tM[5 * gy + d];
+      csy[d] = lv.tS[5 * gy + d];
+    }
+  }
+  // diagonal dg(z) = H (dA mz + dC sz) + wg of the two outputs, and its inverse on interior planes
+  T dA[2], dC[2], invI[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (EDGE) {
+      dA[j] = csx[j][2] * cmy[2] + cmx[j][2] * csy[2];
+      dC[j] = cmx[j][2] * cmy[2];
+      invI[j] = T(1) / (lv.H * (dA[j] * A.im[2] + dC[j] * A.is[2]) + lv.wg);
+    } else {
+      dA[j] = A.is[2] * A.im[2] + A.im[2] * A.is[2];
+      dC[j] = A.im[2] * A.im[2];
+      invI[j] = A.invd;
+    }
+  }
+  T wa[2][NS], wb[2][NS], wc[2][NS];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int k = 0; k < NS; ++k) wa[j][k] = wb[j][k] = wc[j][k] = T(0);
+  T* op = out + (int64_t)gx + (int64_t)res * gy + plane * (z0 - 4);  // output row of plane zo = z0 - 4 + it
+  int kstate = -1;  // EDGE kOpChebF: s_k holds the scales of: -1 nothing, 0 interior planes, 1 plane kzin
+  int kzin = 0;
+  int it = 0;
+  bool stop = false;
+  for (int g = 0; g < ngroups; ++g) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      it = g * NS + k;
+      if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
+        atomicExch(A.err, 1);
+        *s_abort = 1;
+      }
+      const int b = (g + k) & 1;  // = it & 1 (NS is odd)
+      const int zin = z0 - 2 + it;
+      const bool zin_int = zin >= A.edge && zin < res - A.edge;
+      // kOpChebF: the staged f becomes x1 = c0 D^-1 f
+      T kz = T(0);
+      if (MODE == kOpChebF) {
+        if (EDGE) {
+          if (zin_int ? kstate != 0 : (kstate != 1 || kzin != zin)) {
+            const bool zok = zin >= 0 && zin < res;
+            const int zr = zok ? zin : 0;
+            const T mz = zok ? lv.tM[5 * zr + 2] : T(0), sz = zok ? lv.tS[5 * zr + 2] : T(0);
+            for (int i = t; i < SH * BW; i += kThreads) {
+              const int r = i / BW, c = i % BW;
+              const T dxm = s_dx[2 * c], dxs = s_dx[2 * c + 1], dym = s_dy[2 * r], dys = s_dy[2 * r + 1];
+              const T dg = lv.H * (dxs * dym * mz + dxm * dys * mz + dxm * dym * sz) + lv.wg;
+              s_k[r][c] = (zok && dxm != T(0) && dym != T(0)) ? A.c0 / dg : T(0);
+            }
+            kstate = zin_int ? 0 : 1;
+            kzin = zin;
+            __syncthreads();
+          }
+        } else if (zin_int) {
+          kz = A.c0 * A.invd;
+        } else if (zin < 0 || zin >= res) {
+          kz = T(0);  // a zero-filled plane
+        } else {
+          const T mz = lv.tM[5 * zin + 2], sz = lv.tS[5 * zin + 2];
+          kz = A.c0 / (lv.H * (dA[0] * mz + dC[0] * sz) + lv.wg);
+        }
+      }
+      // x filter: rows ty and ty + 8 of the 12 staged rows, two outputs per thread
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int r = ty + 8 * q;
+        if (r < SH) {
+          const T* row = &s_x[k][r][2 * p + XOFF];
+          const V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
+                   v2 = *reinterpret_cast<const V2*>(row + 4);
+          T v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
+          T um0, um1, us0, us1;
+          if (EDGE) {
+            if (MODE == kOpChebF) {
+              const T* kr = &s_k[r][2 * p + XOFF];
+#pragma unroll
+              for (int e = 0; e < 6; ++e) v[e] *= kr[e];
+            }
+            um0 = filt(v, cmx[0]);
+            us0 = filt(v, csx[0]);
+            um1 = filt(v + 1, cmx[1]);
+            us1 = filt(v + 1, csx[1]);
+          } else {
+            filt2_sym(v, A.im, A.is, um0, us0);
+            filt2_sym(v + 1, A.im, A.is, um1, us1);
+            if (MODE == kOpChebF) {
+              um0 *= kz;
+              us0 *= kz;
+              um1 *= kz;
+              us1 *= kz;
+            }
+          }
+          *reinterpret_cast<V2*>(&s_um[b][r][2 * p]) = V2{um0, um1};
+          *reinterpret_cast<V2*>(&s_us[b][r][2 * p]) = V2{us0, us1};
+        }
+      }
+      // centre values: x (f for kOpChebF)
+      const V2 xc = *reinterpret_cast<const V2*>(&s_x[k][ty + 2][2 * p + 2 + XOFF]);
+      V2 fo = V2{T(0), T(0)}, po = V2{T(0), T(0)};
+      if (use_f) fo = *reinterpret_cast<const V2*>(&s_f[k][ty][2 * p]);
+      if (use_p) po = *reinterpret_cast<const V2*>(&s_p[k][ty][2 * p]);
+      __syncthreads();  // stage k is read; s_um/s_us[b] are written
+      if (*s_abort) {
+        stop = true;
+        break;
+      }
+      if (t == 0 && it + NS < nissue) issue(it + NS);
+      // y filter into the window slot k
+      {
+        T a0[5], a1[5], c0[5], c1[5];
+#pragma unroll
+        for (int d = 0; d < 5; ++d) {
+          const V2 a = *reinterpret_cast<const V2*>(&s_um[b][ty + d][2 * p]);
+          const V2 c = *reinterpret_cast<const V2*>(&s_us[b][ty + d][2 * p]);
+          a0[d] = a.x;
+          a1[d] = a.y;
+          c0[d] = c.x;
+          c1[d] = c.y;
+        }
+        T vmm0, vmm1, vms0, vms1, vsm0, vsm1;
+        if (EDGE) {
+          vmm0 = filt(a0, cmy);
+          vms0 = filt(a0, csy);
+          vmm1 = filt(a1, cmy);
+          vms1 = filt(a1, csy);
+          vsm0 = filt(c0, cmy);
+          vsm1 = filt(c1, cmy);
+        } else {
+          filt2_sym(a0, A.im, A.is, vmm0, vms0);
+          filt2_sym(a1, A.im, A.is, vmm1, vms1);
+          vsm0 = A.im[0] * (c0[0] + c0[4]) + A.im[1] * (c0[1] + c0[3]) + A.im[2] * c0[2];
+          vsm1 = A.im[0] * (c1[0] + c1[4]) + A.im[1] * (c1[1] + c1[3]) + A.im[2] * c1[2];
+        }
+        wa[0][k] = vsm0 + vms0;
+        wa[1][k] = vsm1 + vms1;
+        wb[0][k] = vmm0;
+        wb[1][k] = vmm1;
+      }
+      wc[0][k] = xc.x;
+      wc[1][k] = xc.y;
+      const int zo = zin - 2;
+      if ((unsigned)(zo - z0) < (unsigned)(z1 - z0)) {
+        const bool zint = zo >= A.edge && zo < res - A.edge;
+        T acc[2], inv[2];
+        if (zint) {
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const T* wA = wa[j];
+            const T* wB = wb[j];
+            acc[j] = A.im[0] * (wA[(k + 1) % NS] + wA[(k + 5) % NS]) + A.im[1] * (wA[(k + 2) % NS] + wA[(k + 4) % NS]) +
+                     A.im[2] * wA[(k + 3) % NS] + A.is[0] * (wB[(k + 1) % NS] + wB[(k + 5) % NS]) +
+                     A.is[1] * (wB[(k + 2) % NS] + wB[(k + 4) % NS]) + A.is[2] * wB[(k + 3) % NS];
+            inv[j] = invI[j];
+          }
+        } else {
+          T cz_m[5], cz_s[5];
+#pragma unroll
+          for (int d = 0; d < 5; ++d) {
+            cz_m[d] = lv.tM[5 * zo + d];
+            cz_s[d] = lv.tS[5 * zo + d];
+          }
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            T sacc = 0;
+#pragma unroll
+            for (int d = 0; d < 5; ++d) sacc += cz_m[d] * wa[j][(k + 1 + d) % NS] + cz_s[d] * wb[j][(k + 1 + d) % NS];
+            acc[j] = sacc;
+            inv[j] = T(1) / (lv.H * (dA[j] * cz_m[2] + dC[j] * cz_s[2]) + lv.wg);
+          }
+        }
+        T res2[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const T fj = j == 0 ? fo.x : fo.y;
+          const T pj = j == 0 ? po.x : po.y;
+          const T cj = wc[j][(k + 3) % NS];  // the output plane's centre (f for kOpChebF)
+          if (MODE == kOpChebF) {
+            const T x1 = A.c0 * inv[j] * cj;
+            const T ax = lv.H * acc[j] + lv.wg * x1;
+            res2[j] = (T(1) + A.ca) * x1 + A.cb * (cj - ax) * inv[j];
+          } else {
+            const T ax = lv.H * acc[j] + lv.wg * cj;
+            if (MODE == kOpApply) res2[j] = ax;
+            else if (MODE == kOpResid) res2[j] = fj - ax;
+            else if (MODE == kOpCheb) res2[j] = cj + A.ca * (cj - pj) + A.cb * (fj - ax) * inv[j];
+            else res2[j] = cj + A.ca * (cj - A.c0 * inv[j] * fj) + A.cb * (fj - ax) * inv[j];  // kOpChebPF
+          }
+        }
+        *reinterpret_cast<V2*>(op) = V2{res2[0], res2[1]};
+      }
+      op += plane;
+    }
+    if (stop) break;
+  }
+  if (stop && t == 0) {
+    // stopped early: let the loads still in flight land before the CTA's shared memory goes
+    for (int q = it; q < min(it + NS, nissue); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
+  }
+}
+
 // first Chebyshev step from x = 0: out = cb D^-1 f
 template <typename T>
 __global__ void k_cheb_first2(const T* __restrict__ f, T* __restrict__ out, LevelView<T> lv, T cb) {
@@ -271,12 +680,60 @@ __global__ void k_cheb_first2(const T* __restrict__ f, T* __restrict__ out, Leve
   }
 }
 
-// fc = P^T rf (fine level Lf -> coarse Lf - 1): coarse c <- fine 2c + k, k = -1..2 per axis
+// Grid transfers with the B2 subdivision P (fine 2c + k <- coarse c, weights 1/4, 3/4, 3/4, 1/4 for
+// k = -1..2), one thread per coarse node and separable: the prolongation (out = xf + P ec) writes the 2 x 2 x 2
+// fine block of coarse node c (fine 2c, 2c + 1 per axis) from the coarse 3 x 3 x 3 neighbourhood;
+// the restriction reads the fine 4 x 4 x 4 block 2c - 1 .. 2c + 2 as rows of a scalar, a pair and a
+// scalar.
 template <typename T>
-__global__ void k_restrict2(const T* __restrict__ rf, int Lf, T* __restrict__ fc) {
-  const int Lc = Lf - 1, rf_res = 1 << Lf;
+__global__ void k_prolong3(const T* __restrict__ xf, const T* __restrict__ ec, int Lf, T* __restrict__ out) {
+  typedef typename Vec2<T>::type V2;
+  const int Lc = Lf - 1, rc = 1 << Lc, rf = 1 << Lf;
+  const uint64_t nc = 1ull << (3 * Lc), m = (uint64_t)rc - 1;
+  const int64_t pc = (int64_t)rc * rc, pf = (int64_t)rf * rf;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int cx = (int)(i & m), cy = (int)((i >> Lc) & m), cz = (int)(i >> (2 * Lc));
+    T a[3][3][2];  // x pass: [dz][dy][fine x 2cx, 2cx + 1]
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        const int Z = cz + dz - 1, Y = cy + dy - 1;
+        T e0 = 0, e1 = 0, e2 = 0;
+        if (Z >= 0 && Z < rc && Y >= 0 && Y < rc) {
+          const T* row = ec + Z * pc + (int64_t)Y * rc;
+          e1 = row[cx];
+          if (cx > 0) e0 = row[cx - 1];
+          if (cx + 1 < rc) e2 = row[cx + 1];
+        }
+        a[dz][dy][0] = T(0.75) * e1 + T(0.25) * e0;
+        a[dz][dy][1] = T(0.75) * e1 + T(0.25) * e2;
+      }
+#pragma unroll
+    for (int zo = 0; zo < 2; ++zo)
+#pragma unroll
+      for (int yo = 0; yo < 2; ++yo) {
+        T v[2];
+#pragma unroll
+        for (int xo = 0; xo < 2; ++xo) {
+          T b[3];
+#pragma unroll
+          for (int dz = 0; dz < 3; ++dz) b[dz] = T(0.75) * a[dz][1][xo] + T(0.25) * a[dz][yo == 0 ? 0 : 2][xo];
+          v[xo] = T(0.75) * b[1] + T(0.25) * b[zo == 0 ? 0 : 2];
+        }
+        const int64_t f = (int64_t)(2 * cx) + (int64_t)rf * (2 * cy + yo) + pf * (2 * cz + zo);
+        const V2 x = *reinterpret_cast<const V2*>(xf + f);
+        *reinterpret_cast<V2*>(out + f) = V2{x.x + v[0], x.y + v[1]};
+      }
+  }
+}
+
+template <typename T>
+__global__ void k_restrict3(const T* __restrict__ rf, int Lf, T* __restrict__ fc) {
+  typedef typename Vec2<T>::type V2;
+  const int Lc = Lf - 1, res = 1 << Lf;
   const uint64_t nc = 1ull << (3 * Lc), m = (1ull << Lc) - 1;
-  const int64_t pf = (int64_t)rf_res * rf_res;
+  const int64_t pf = (int64_t)res * res;
   const T w[4] = {T(0.25), T(0.75), T(0.75), T(0.25)};
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x) {
     const int cx = (int)(i & m), cy = (int)((i >> Lc) & m), cz = (int)(i >> (2 * Lc));
@@ -284,55 +741,22 @@ __global__ void k_restrict2(const T* __restrict__ rf, int Lf, T* __restrict__ fc
 #pragma unroll
     for (int kz = 0; kz < 4; ++kz) {
       const int fz = 2 * cz - 1 + kz;
-      if (fz < 0 || fz >= rf_res) continue;
+      if (fz < 0 || fz >= res) continue;
       T az = 0;
 #pragma unroll
       for (int ky = 0; ky < 4; ++ky) {
         const int fy = 2 * cy - 1 + ky;
-        if (fy < 0 || fy >= rf_res) continue;
-        const T* row = rf + fz * pf + (int64_t)fy * rf_res;
-        T ay = 0;
-#pragma unroll
-        for (int kx = 0; kx < 4; ++kx) {
-          const int fx = 2 * cx - 1 + kx;
-          if (fx >= 0 && fx < rf_res) ay += w[kx] * row[fx];
-        }
-        az += w[ky] * ay;
+        if (fy < 0 || fy >= res) continue;
+        const T* row = rf + fz * pf + (int64_t)fy * res + 2 * cx;
+        const V2 c = *reinterpret_cast<const V2*>(row);
+        T ax = T(0.75) * (c.x + c.y);
+        if (cx > 0) ax += T(0.25) * row[-1];
+        if (2 * cx + 2 < res) ax += T(0.25) * row[2];
+        az += w[ky] * ax;
       }
       acc += w[kz] * az;
     }
     fc[i] = acc;
-  }
-}
-
-// out = xf + P ec (coarse Lf - 1 -> fine Lf); fine f <- coarse f/2 (3/4) and f/2 - 1 (1/4) for f
-// even, (f-1)/2 (3/4) and (f+1)/2 (1/4) for f odd
-template <typename T>
-__global__ void k_prolong2(const T* __restrict__ xf, const T* __restrict__ ec, int Lf, T* __restrict__ out) {
-  const int Lc = Lf - 1, rc = 1 << Lc;
-  const uint64_t n = 1ull << (3 * Lf), m = (1ull << Lf) - 1;
-  const int64_t pc = (int64_t)rc * rc;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const int f[3] = {(int)(i & m), (int)((i >> Lf) & m), (int)(i >> (2 * Lf))};
-    int c[3][2];
-    T w[3][2];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      c[a][0] = f[a] >> 1;
-      w[a][0] = T(0.75);
-      c[a][1] = (f[a] & 1) ? (f[a] >> 1) + 1 : (f[a] >> 1) - 1;
-      w[a][1] = (c[a][1] >= 0 && c[a][1] < rc) ? T(0.25) : T(0);
-      if (w[a][1] == T(0)) c[a][1] = c[a][0];
-    }
-    T acc = 0;
-#pragma unroll
-    for (int kz = 0; kz < 2; ++kz)
-#pragma unroll
-      for (int ky = 0; ky < 2; ++ky) {
-        const T* row = ec + c[2][kz] * pc + (int64_t)c[1][ky] * rc;
-        acc += w[2][kz] * w[1][ky] * (w[0][0] * row[c[0][0]] + w[0][1] * row[c[0][1]]);
-      }
-    out[i] = xf[i] + acc;
   }
 }
 
@@ -543,6 +967,67 @@ __global__ void k_nat3_to_morton_aos(const double* __restrict__ nf, uint32_t D, 
   }
 }
 
+// ------------------------------------------------------------------ host: tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    PR_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    PR_REQUIRE(p != nullptr && q == cudaDriverEntryPointSuccess, PR_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+// 3-D map of a res^3 natural-order grid with a (bx, by, 1) box; outside the grid reads 0
+template <typename T>
+CUtensorMap plane_map(const T* base, int L, uint32_t bx, uint32_t by) {
+  CUtensorMap m;
+  const cuuint64_t res = 1ull << L;
+  const cuuint64_t dims[3] = {res, res, res};
+  const cuuint64_t strides[2] = {res * sizeof(T), res * res * sizeof(T)};
+  const cuuint32_t box[3] = {bx, by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  PR_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15u) == 0 && (bx * sizeof(T)) % 16 == 0, PR_ERR_INTERNAL,
+             "tensor map: base or box not 16-byte aligned");
+  const CUresult r = encode_tiled()(&m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                                    3, const_cast<T*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PR_REQUIRE(r == CUDA_SUCCESS, PR_ERR_CUDA, "cuTensorMapEncodeTiled failed with " + std::to_string((int)r));
+  return m;
+}
+constexpr int kTmaMinLevel = 6;  // res >= 64: full 64-wide x tiles (k_op3)
+
+// launches k_op3 over the interior tiles and the face tiles of a level
+template <typename T, int MODE>
+void launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, const CUtensorMap& mp, T* out,
+                const Op3Args<T>& a, int nz) {
+  typedef Geo3<T> G;
+  static bool attr = false;  // once per instantiation pair
+  if (!attr) {
+    PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
+    PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
+    attr = true;
+  }
+  const int nbx = a.nbx, nby = a.nby;
+  // interior tiles need every output row at least `edge` from the faces: edge <= 8 (one tile row)
+  const bool split = nbx > 2 && nby > 2 && a.edge <= TY;
+  Op3Args<T> e = a;
+  e.all = split ? 0 : 1;
+  if (split) {
+    k_op3<T, MODE, false><<<dim3(nbx - 2, nby - 2, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+    PR_CHECK_LAUNCH();
+    k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+    PR_CHECK_LAUNCH();
+  } else {
+    k_op3<T, MODE, true><<<dim3(nbx * nby, 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+    PR_CHECK_LAUNCH();
+  }
+}
+
 // ------------------------------------------------------------------ host: the system
 template <typename T>
 struct Level2 {
@@ -551,6 +1036,8 @@ struct Level2 {
   T* tM = nullptr;
   T* tS = nullptr;
   double H = 0, wg = 0;
+  int edge = 0;           // rows [edge, res - edge) of tM, tS equal the interior row
+  double im[5], is[5];    // the interior rows
   T* f = nullptr;  // right-hand side (coarse levels)
   T* x = nullptr;  // iterate (coarse levels)
   T* y = nullptr;  // scratch
@@ -584,6 +1071,7 @@ struct System2 {
   int nc = 0;
   Screen2<T> scr;
   double bytes = 0.0;         // algorithmic HBM bytes of the launched kernels
+  int* err = nullptr;         // set by a TMA wait that ran out
 
   // levels D (finest) down to the dense 4^3 level; `multigrid` false: the finest level only
   void init(pr_context* ctx, uint32_t depth, double pw, bool multigrid) {
@@ -593,6 +1081,8 @@ struct System2 {
     const double wh3 = pw > 0.0 ? pw * h * h * h / 1.5 : 0.0;
     const double wg = wh3 * 0.005;
     const std::string tn = tn2<T>();
+    err = c->buf<int>("d2_err", 1);
+    PR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), c->stream));
     Band M = toeplitz(1 << D, consts().m), S = toeplitz(1 << D, consts().s);
     const int lmin = multigrid ? std::min<int>((int)D, 2) : (int)D;
     lv.clear();
@@ -612,6 +1102,21 @@ struct System2 {
       };
       q.tM = upload(M, "tM");
       q.tS = upload(S, "tS");
+      {
+        const int res = 1 << l, mid = res / 2;
+        auto same = [&](int i) {
+          for (int d = 0; d < 5; ++d)
+            if ((T)M[5 * i + d] != (T)M[5 * mid + d] || (T)S[5 * i + d] != (T)S[5 * mid + d]) return false;
+          return true;
+        };
+        int e = 0;
+        while (e < mid && !(same(e) && same(res - 1 - e))) ++e;
+        q.edge = e;
+        for (int d = 0; d < 5; ++d) {
+          q.im[d] = M[5 * mid + d];
+          q.is[d] = S[5 * mid + d];
+        }
+      }
       if (multigrid) {
         q.y = c->buf<T>("d2_y" + sfx, q.n);
         if (l != (int)D) {
@@ -704,42 +1209,101 @@ struct System2 {
              (double)scr.pairs * (4 + 2 * sizeof(T)) + (double)scr.S * (8 + 2 * sizeof(T));
   }
 
-  void op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0) {
+  // One operator pass on level li (modes k_op2 / k_op3); c0 is the first Chebyshev coefficient of
+  // the fused modes.  tma < 0: k_op3 on levels with res >= 64, k_op2 below.
+  void op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0,
+          int tma = -1, double c0 = 0.0) {
     const Level2<T>& q = lv[li];
     const int res = 1 << q.L;
-    dim3 grid((res + TX - 1) / TX, (res + TY - 1) / TY, (res + kZChunk - 1) / kZChunk);
     cudaStream_t s = c->stream;
     const LevelView<T> v = q.view();
-    if (mode == kOpApply) k_op2<T, kOpApply><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
-    else if (mode == kOpResid) k_op2<T, kOpResid><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
-    else k_op2<T, kOpCheb><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
-    PR_CHECK_LAUNCH();
-    bytes += (double)q.n * sizeof(T) * (2 + (mode != kOpApply ? 1 : 0) + (xp ? 1 : 0));
+    if (tma < 0) tma = q.L >= kTmaMinLevel;
+    if (tma) {
+      PR_REQUIRE(q.L >= kTmaMinLevel, PR_ERR_INTERNAL, "TMA operator below its minimum level");
+      typedef Geo3<T> G;
+      Op3Args<T> A;
+      A.lv = v;
+      for (int d = 0; d < 5; ++d) {
+        A.im[d] = (T)q.im[d];
+        A.is[d] = (T)q.is[d];
+      }
+      A.invd = (T)(1.0 / (q.H * ((q.is[2] * q.im[2] + q.im[2] * q.is[2]) * q.im[2] + q.im[2] * q.im[2] * q.is[2]) + q.wg));
+      A.edge = q.edge;
+      A.ca = (T)a;
+      A.cb = (T)b;
+      A.c0 = (T)c0;
+      A.use_p = (mode == kOpCheb && xp) ? 1 : 0;
+      A.nbx = res / G::TXP;
+      A.nby = res / TY;
+      A.err = err;
+      const int nz = (res + kZChunk3 - 1) / kZChunk3;
+      const CUtensorMap mx = plane_map<T>(x, q.L, G::BW, SH);
+      const CUtensorMap mf = f ? plane_map<T>(f, q.L, G::TXP, TY) : mx;
+      const CUtensorMap mp = xp ? plane_map<T>(xp, q.L, G::TXP, TY) : mx;
+      switch (mode) {
+        case kOpApply: launch_op3<T, kOpApply>(s, mx, mf, mp, out, A, nz); break;
+        case kOpResid: launch_op3<T, kOpResid>(s, mx, mf, mp, out, A, nz); break;
+        case kOpCheb: launch_op3<T, kOpCheb>(s, mx, mf, mp, out, A, nz); break;
+        case kOpChebF: launch_op3<T, kOpChebF>(s, mx, mf, mp, out, A, nz); break;
+        default: launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
+      }
+    } else {
+      PR_REQUIRE(mode <= kOpCheb, PR_ERR_INTERNAL, "fused Chebyshev modes need the TMA operator");
+      dim3 grid((res + TX - 1) / TX, (res + TY - 1) / TY, (res + kZChunk - 1) / kZChunk);
+      if (mode == kOpApply) k_op2<T, kOpApply><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
+      else if (mode == kOpResid) k_op2<T, kOpResid><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
+      else k_op2<T, kOpCheb><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
+      PR_CHECK_LAUNCH();
+    }
+    const int reads = mode == kOpApply || mode == kOpChebF ? 1 : (mode == kOpCheb && xp ? 3 : 2);
+    bytes += (double)q.n * sizeof(T) * (reads + 1);
   }
 
-  // Chebyshev smoothing on level li.  From zero (pre-smoothing): x1 in x, x2 in y, x3 in x.
-  // From y0 held in y (post-smoothing): y1 in x, y2 in y, y3 in x.
+  // throws if a TMA wait ran out since init()
+  void check() {
+    int h = 0;
+    PR_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    PR_REQUIRE(h == 0, PR_ERR_CUDA, "degree-2 operator: a TMA pipeline wait timed out");
+  }
+
+  // Chebyshev smoothing on level li.  From zero (pre-smoothing): x1 in x, x2 in y, x3 in x (on
+  // levels with res >= 64 the first two steps are one fused pass from f, and the third recomputes
+  // x1 from f).  From y0 held in y (post-smoothing): y1 in x, y2 in y, y3 in x.
   void chebyshev(int li, const T* f, T* x, T* y, bool from_zero) {
     const Level2<T>& q = lv[li];
     const double hi = kLamMax, lo = kLamMax / kLamRatio;
     const double th = 0.5 * (hi + lo), de = 0.5 * (hi - lo), sig = th / de;
+    double ca[kChebSteps], cb[kChebSteps];
     double rho = 1.0 / sig;
+    ca[0] = 0.0;
+    cb[0] = 1.0 / th;
+    for (int k = 1; k < kChebSteps; ++k) {
+      const double rn = 1.0 / (2.0 * sig - rho);
+      ca[k] = rn * rho;
+      cb[k] = 2.0 * rn / de;
+      rho = rn;
+    }
+    static_assert(kChebSteps == 3, "the fused pre-smoothing is written for three steps");
+    if (from_zero && q.L >= kTmaMinLevel) {
+      op(li, kOpChebF, f, nullptr, nullptr, y, ca[1], cb[1], 1, cb[0]);
+      op(li, kOpChebPF, y, f, nullptr, x, ca[2], cb[2], 1, cb[0]);
+      return;
+    }
     if (from_zero) {
-      k_cheb_first2<T><<<grid_for(q.n), kThreads, 0, c->stream>>>(f, x, q.view(), (T)(1.0 / th));
+      k_cheb_first2<T><<<grid_for(q.n), kThreads, 0, c->stream>>>(f, x, q.view(), (T)cb[0]);
       PR_CHECK_LAUNCH();
       bytes += 2.0 * q.n * sizeof(T);
     } else {
-      op(li, kOpCheb, y, f, nullptr, x, 0.0, 1.0 / th);
+      op(li, kOpCheb, y, f, nullptr, x, 0.0, cb[0]);
     }
     T* cur = x;
     T* prev = from_zero ? nullptr : y;
     for (int k = 1; k < kChebSteps; ++k) {
-      const double rn = 1.0 / (2.0 * sig - rho);
       T* dst = (cur == x) ? y : x;
-      op(li, kOpCheb, cur, f, prev, dst, rn * rho, 2.0 * rn / de);
+      op(li, kOpCheb, cur, f, prev, dst, ca[k], cb[k]);
       prev = cur;
       cur = dst;
-      rho = rn;
     }
     PR_REQUIRE(cur == x, PR_ERR_INTERNAL, "Chebyshev smoothing must end in its output buffer");
   }
@@ -756,11 +1320,11 @@ struct System2 {
     Level2<T>& qc = lv[li + 1];
     chebyshev(li, f, X, q.y, true);
     op(li, kOpResid, X, f, nullptr, q.y);
-    k_restrict2<T><<<grid_for(qc.n), kThreads, 0, s>>>(q.y, q.L, qc.f);
+    k_restrict3<T><<<grid_for(qc.n), kThreads, 0, s>>>(q.y, q.L, qc.f);
     PR_CHECK_LAUNCH();
     bytes += (double)(q.n + qc.n) * sizeof(T);
     vcycle(li + 1, qc.f, qc.x);
-    k_prolong2<T><<<grid_for(q.n), kThreads, 0, s>>>(X, qc.x, q.L, q.y);
+    k_prolong3<T><<<grid_for(qc.n), kThreads, 0, s>>>(X, qc.x, q.L, q.y);
     PR_CHECK_LAUNCH();
     bytes += (double)(2 * q.n + qc.n) * sizeof(T);
     chebyshev(li, f, X, q.y, false);
@@ -920,6 +1484,7 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
         if (stalled) break;
       }
       bytes += sys32.bytes;
+      sys32.check();
     } else {
       double* e64 = c->buf<double>("d2_e64", n);
       PR_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -940,6 +1505,7 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
     }
   }
   bytes += sys64.bytes;
+  sys64.check();
   st.pcg_iterations = (uint32_t)used;
   st.rel_residual = bn > 0.0 ? rn / bn : 0.0;
   st.converged = st.rel_residual <= target ? 1 : 0;
@@ -948,6 +1514,92 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
   k_nat_to_morton<double><<<grid_for(n), kThreads, 0, s>>>(x, D, xm);
   PR_CHECK_LAUNCH();
   c->have_coeffs = true;
+}
+
+namespace {
+template <typename T>
+__global__ void k_fill2(T* __restrict__ v, uint64_t n, uint32_t seed) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t h = (uint32_t)i * 2654435761u ^ seed * 40503u;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    v[i] = (T)((double)(h & 0xffffff) / 8388608.0 - 1.0);
+  }
+}
+
+template <typename T>
+double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
+  cudaStream_t s = c->stream;
+  const uint64_t n = 1ull << (3 * D), nc = n / 8;
+  const std::string tn = tn2<T>();
+  T* x = c->buf<T>("kb2_x_" + tn, n);
+  T* f = c->buf<T>("kb2_f_" + tn, n);
+  T* p = c->buf<T>("kb2_p_" + tn, n);
+  T* y = c->buf<T>("kb2_y_" + tn, n);
+  T* ec = c->buf<T>("kb2_c_" + tn, nc);
+  k_fill2<T><<<148 * 16, 256, 0, s>>>(x, n, 1u);
+  k_fill2<T><<<148 * 16, 256, 0, s>>>(f, n, 2u);
+  k_fill2<T><<<148 * 16, 256, 0, s>>>(p, n, 3u);
+  k_fill2<T><<<148 * 16, 256, 0, s>>>(ec, nc, 4u);
+  PR_CHECK_LAUNCH();
+  System2<T> sys;
+  sys.init(c, D, 4.0, false);
+  const double nb = (double)n * sizeof(T);
+  const double algo[] = {4 * nb, 4 * nb, 2 * nb, 2 * nb, 3 * nb, nb + nb / 8, 2 * nb + nb / 8, 2 * nb, 2 * nb, 3 * nb};
+  PR_REQUIRE(kid >= 0 && kid < 10, PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
+  PR_REQUIRE(D >= (uint32_t)kTmaMinLevel || (kid != 0 && kid != 2 && kid != 4 && kid < 8), PR_ERR_INVALID_ARGUMENT,
+             "the TMA operator needs depth >= 6");
+  *bytes = algo[kid];
+  const LevelView<T> v = sys.lv[0].view();
+  auto run = [&]() {
+    switch (kid) {
+      case 0: sys.op(0, kOpCheb, x, f, p, y, 0.3, 0.5, 1); break;
+      case 1: sys.op(0, kOpCheb, x, f, p, y, 0.3, 0.5, 0); break;
+      case 2: sys.op(0, kOpApply, x, nullptr, nullptr, y, 0.0, 0.0, 1); break;
+      case 3: sys.op(0, kOpApply, x, nullptr, nullptr, y, 0.0, 0.0, 0); break;
+      case 4: sys.op(0, kOpResid, x, f, nullptr, y, 0.0, 0.0, 1); break;
+      case 5:
+        k_restrict3<T><<<grid_for(nc), kThreads, 0, s>>>(x, (int)D, ec);
+        PR_CHECK_LAUNCH();
+        break;
+      case 6:
+        k_prolong3<T><<<grid_for(nc), kThreads, 0, s>>>(x, ec, (int)D, y);
+        PR_CHECK_LAUNCH();
+        break;
+      case 7:
+        k_cheb_first2<T><<<grid_for(n), kThreads, 0, s>>>(f, y, v, (T)0.5);
+        PR_CHECK_LAUNCH();
+        break;
+      case 8: sys.op(0, kOpChebF, f, nullptr, nullptr, y, 0.3, 0.5, 1, 0.6); break;
+      default: sys.op(0, kOpChebPF, x, f, nullptr, y, 0.3, 0.5, 1, 0.6); break;
+    }
+  };
+  run();
+  PR_CUDA(cudaStreamSynchronize(s));
+  cudaEvent_t e0, e1;
+  PR_CUDA(cudaEventCreate(&e0));
+  PR_CUDA(cudaEventCreate(&e1));
+  PR_CUDA(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) run();
+  PR_CUDA(cudaEventRecord(e1, s));
+  PR_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  PR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  sys.check();
+  return (double)ms / reps;
+}
+}  // namespace
+
+// Kernel bench of the degree-2 kernels on the finest level of depth D (synthetic vectors):
+// 0 Chebyshev step (TMA), 1 Chebyshev step (register staging), 2 A x (TMA), 3 A x (register
+// staging), 4 f - A x (TMA), 5 restriction, 6 prolongation + add, 7 first Chebyshev step,
+// 8 the first two steps fused (from f), 9 the third step with x1 recomputed from f.
+double deg2_kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps, double* bytes) {
+  if (reps < 1) reps = 1;
+  return precision == PR_PRECISION_FP64 ? bench2<double>(c, kid, D, reps, bytes) : bench2<float>(c, kid, D, reps, bytes);
 }
 
 // accessors in Morton order (the order of the degree-1 vectors and of the oracle)
@@ -975,6 +1627,7 @@ void deg2_apply_morton(pr_context* c, const T* d_x, T* d_y) {
   sys.set_screen(sizeof(T) == 8 ? (const T*)c->get<double>("d2_phi64") : (const T*)c->get<float>("d2_phi32"));
   sys.op(0, kOpApply, xn, nullptr, nullptr, yn);
   sys.screen(xn, yn, +1);
+  sys.check();
   k_nat_to_morton<T><<<grid_for(n), kThreads, 0, c->stream>>>(yn, c->D, d_y);
   PR_CHECK_LAUNCH();
 }

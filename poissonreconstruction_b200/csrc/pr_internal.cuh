@@ -206,6 +206,7 @@ void deg2_rhs_morton(pr_context* c, double* d_out);
 void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w);
 template <typename T>
 void deg2_apply_morton(pr_context* c, const T* d_x, T* d_y);
+double deg2_kernel_bench(pr_context* c, int kid, uint32_t depth, int precision, int reps, double* bytes);
 // extract (pr_mc.cu); `degree` selects the node functions (1: the crate's, 2: quadratic)
 double stage_iso(pr_context* c, const double* d_x64);
 void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform,

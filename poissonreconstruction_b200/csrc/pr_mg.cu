@@ -1649,6 +1649,7 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
 
 double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps, double* bytes) {
   if (D < 4 || D > kMaxDepth) throw Error(PR_ERR_INVALID_ARGUMENT, "kernel bench depth must be in [4, 10]");
+  if (kid >= 20) return deg2_kernel_bench(c, kid - 20, D, precision, reps, bytes);
   if (reps < 1) reps = 1;
   return precision == PR_PRECISION_FP64 ? bench_one<double>(c, kid, D, reps, bytes)
                                         : bench_one<float>(c, kid, D, reps, bytes);
