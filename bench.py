@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--points", type=int, default=2_000_000)
     ap.add_argument("--depth", type=int, default=10)
+    ap.add_argument("--degree", type=int, default=2, choices=[1, 2],
+                    help="B-spline degree of the headline workload (2: the quadratic basis of the depth-10 "
+                         "mixed-precision config; 1: the crate's own basis)")
+    ap.add_argument("--no-degree1", action="store_true", help="skip the secondary degree-1 measurement")
     ap.add_argument("--fp64-steps", type=int, default=None, help="steps of the FP64 comparison (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-reps", type=int, default=20)
@@ -206,8 +210,9 @@ def run_reference(a):
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": a.gpus,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "torus_2m_depth10", "points": len(pts), "depth": a.depth, "point_weight": 4.0,
-                      "cpu_sample_depth": CPU_DEPTH},
+           "config": {"workload": "torus_2m_depth%d_degree%d" % (a.depth, a.degree), "points": len(pts),
+                      "depth": a.depth, "point_weight": 4.0, "cpu_sample_depth": CPU_DEPTH,
+                      "reference_basis": "degree 1: the crate's reconstruct has no degree-2 path"},
            "cpu_baseline": {k: last[k] for k in ("value", "unit", "cores", "kind", "sample")},
            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -235,9 +240,9 @@ def run_ours(a):
     d_pts = torch.from_numpy(pts).to(dev)
     h_pts = torch.from_numpy(pts).pin_memory()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    params = prb.ReconstructParams(depth=a.depth, point_weight=4.0, scale=1.1,
+    params = prb.ReconstructParams(depth=a.depth, point_weight=4.0, scale=1.1, degree=a.degree,
                                    precision=prb.PR_PRECISION_MIXED, target_rel_residual=1e-6)
-    params64 = prb.ReconstructParams(depth=a.depth, point_weight=4.0, scale=1.1,
+    params64 = prb.ReconstructParams(depth=a.depth, point_weight=4.0, scale=1.1, degree=a.degree,
                                      precision=prb.PR_PRECISION_FP64, target_rel_residual=1e-6)
 
     def device_steps(par, k, record):
@@ -311,9 +316,10 @@ def run_ours(a):
     d2h = int(mesh.vertices.nbytes + mesh.triangles.nbytes)
 
     # roofline: every fine-level solver kernel timed alone with CUDA events on the library's
-    # stream; the roofline entry is the kernel with the largest share of the step's kernel time
-    # (ncu launch list of this workload: the post-smoothing sweep fused with the prolongation and
-    # the r.z product, 6 launches per step)
+    # stream; the roofline entry is the kernel with the largest share of the step's kernel time in
+    # the ncu launch list of this workload (degree 2: the Chebyshev smoothing step, three launches
+    # per V-cycle; degree 1: the post-smoothing sweep fused with the prolongation and the r.z
+    # product)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -323,11 +329,16 @@ def run_ours(a):
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     kernels = {}
-    for nm in ("smooth_prolong_dot", "cg_update_presmooth", "resid_restrict", "spmv_xpby", "spmv"):
+    if a.degree == 2:
+        names = ("d2_cheb", "d2_cheb_f", "d2_cheb_pf", "d2_resid", "d2_apply", "d2_restrict", "d2_prolong")
+        dom = "d2_cheb"
+    else:
+        names = ("smooth_prolong_dot", "cg_update_presmooth", "resid_restrict", "spmv_xpby", "spmv")
+        dom = "smooth_prolong_dot"
+    for nm in names:
         ms, by = ctx.kernel_bench(nm, a.depth, prb.PR_PRECISION_MIXED, a.roofline_reps)
         kernels[nm] = {"ms_per_launch": ms, "algorithmic_bytes": by, "achieved_gbs": by / (ms / 1000.0) / 1e9,
                        "frac": by / (ms / 1000.0) / 1e9 / peak}
-    dom = "smooth_prolong_dot"
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
@@ -341,12 +352,34 @@ def run_ours(a):
         cpu = cpu_sample(pts, a.depth)
         cpu.pop("seconds_measured", None)
 
+    # the other basis on the same cloud (device-resident steps, mixed and FP64), in a fresh context
+    # once the headline context has released its buffers
+    other = None
+    if not a.no_degree1 and a.degree == 2:
+        ctx.close()
+        ctx = prb.Context(local, stream=stream.cuda_stream)
+        q1 = prb.ReconstructParams(depth=a.depth, point_weight=4.0, scale=1.1, degree=1,
+                                   precision=prb.PR_PRECISION_MIXED, target_rel_residual=1e-6)
+        q1_64 = prb.ReconstructParams(depth=a.depth, point_weight=4.0, scale=1.1, degree=1,
+                                      precision=prb.PR_PRECISION_FP64, target_rel_residual=1e-6)
+        device_steps(q1, 1, False)
+        m1, s1 = device_steps(q1, a.steps, True)
+        m1_64, s1_64 = device_steps(q1_64, max(1, k64), True)
+        t1 = statistics.mean(x.time_solve for x in s1)
+        t1_64 = statistics.mean(x.time_solve for x in s1_64)
+        other = {"degree": 1, "value": total_points / (reduce_max(dist, statistics.mean(m1), dev) / 1000.0),
+                 "unit": "points/s", "ms_per_step": statistics.mean(m1), "solve_ms": 1000.0 * t1,
+                 "solve_gbs": s1[-1].solve_bytes / t1 / 1e9 if t1 > 0 else None,
+                 "pcg_iterations": s1[-1].pcg_iterations, "rel_residual": s1[-1].rel_residual,
+                 "fp64_solve_ms": 1000.0 * t1_64, "mixed_vs_fp64_solve_speedup": t1_64 / t1 if t1 > 0 else None}
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64 refinement", "data": "synthetic",
-            "config": {"workload": "torus_2m_depth10", "points": P, "depth": a.depth, "point_weight": 4.0,
+            "config": {"workload": "torus_2m_depth%d_degree%d" % (a.depth, a.degree), "points": P,
+                       "depth": a.depth, "degree": a.degree, "point_weight": 4.0,
                        "scale": 1.1, "precision": "fp32 pcg + fp64 refinement", "target_rel_residual": 1e-6,
                        "parallelism": "replicas" if ws > 1 else "single", "l2": "flushed between steps (256 MiB)"},
             "solve_gbs": solve_gbs, "solve_ms": 1000.0 * solve_s, "rel_residual": st.rel_residual,
@@ -364,6 +397,7 @@ def run_ours(a):
                          "traffic": traffic, "algorithmic_bytes": kernels[dom]["algorithmic_bytes"],
                          "ms_per_launch": kernels[dom]["ms_per_launch"]},
             "kernels": kernels,
+            "degree1": other,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms_max, "library_ms": statistics.mean(e2e_lib),

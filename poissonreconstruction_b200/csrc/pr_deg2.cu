@@ -24,6 +24,7 @@
 // 4^3 level is solved with a dense inverse.  FP32 inner solves with FP64 residual refinement,
 // or FP64 throughout.  The solved coefficients are permuted to the Morton order of the
 // degree-1 path for evaluation and marching cubes.
+#include <cub/cub.cuh>
 #include <cuda.h>
 
 #include <algorithm>
@@ -354,7 +355,10 @@ struct Op3Args {
   int use_p;       // kOpCheb: xp given
   int nbx, nby;    // tiles per axis (x: 64 columns, y: 8 rows)
   int all;         // EDGE: the grid enumerates every tile, not only the face tiles
+  int ox, oy;      // interior: tile of block (i, j) is (i + ox, j + oy)
   int* err;
+  double* dot;     // optional per-CTA partials: kOpApply x . out, kOpCheb f . out
+  int dot_base;    // index of this launch's first partial
 };
 
 // the (x, y) tile of an EDGE CTA: the first and the last tile row, then the first and the last
@@ -412,8 +416,8 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
   int bx, by;
   if (EDGE) edge_tile(blockIdx.x, A.nbx, A.nby, A.all, bx, by);
   else {
-    bx = blockIdx.x + 1;
-    by = blockIdx.y + 1;
+    bx = blockIdx.x + A.ox;
+    by = blockIdx.y + A.oy;
   }
   const int x0 = bx * TXP, y0 = by * TY;
   const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
@@ -486,6 +490,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
 #pragma unroll
     for (int k = 0; k < NS; ++k) wa[j][k] = wb[j][k] = wc[j][k] = T(0);
   T* op = out + (int64_t)gx + (int64_t)res * gy + plane * (z0 - 4);  // output row of plane zo = z0 - 4 + it
+  double dacc = 0.0;  // A.dot: this thread's share of the product
   int kstate = -1;  // EDGE kOpChebF: s_k holds the scales of: -1 nothing, 0 interior planes, 1 plane kzin
   int kzin = 0;
   int it = 0;
@@ -655,6 +660,8 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
           }
         }
         *reinterpret_cast<V2*>(op) = V2{res2[0], res2[1]};
+        if (MODE == kOpApply) dacc += (double)wc[0][(k + 3) % NS] * (double)res2[0] + (double)wc[1][(k + 3) % NS] * (double)res2[1];
+        if (MODE == kOpCheb) dacc += (double)fo.x * (double)res2[0] + (double)fo.y * (double)res2[1];
       }
       op += plane;
     }
@@ -664,6 +671,22 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
     // stopped early: let the loads still in flight land before the CTA's shared memory goes
     for (int q = it; q < min(it + NS, nissue); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
   }
+  if ((MODE == kOpApply || MODE == kOpCheb) && A.dot != nullptr) {
+    typedef cub::BlockReduce<double, kThreads> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double tot = BR(tmp).Sum(dacc);
+    if (t == 0)
+      A.dot[A.dot_base + (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = tot;
+  }
+}
+
+// one warp sums np partials in a fixed order
+__global__ void k_sum_parts(const double* __restrict__ part, int np, double* __restrict__ out) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += 32) s += part[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) out[0] = s;
 }
 
 // first Chebyshev step from x = 0: out = cb D^-1 f
@@ -917,9 +940,12 @@ __global__ void k_screen_rhs2(const uint32_t* __restrict__ snode, const uint32_t
 }
 
 // screening operator wh3 Phi (Phi^T x): per point projection, then a per node gather
+// (sq: optional per-block sums of proj^2, so that x . (wh3 Phi Phi^T x) = wh3 sum proj^2)
 template <typename T>
 __global__ void k_screen_proj2(const uint32_t* __restrict__ key, const T* __restrict__ phi, uint64_t P,
-                               uint32_t sentinel, const T* __restrict__ x, T* __restrict__ proj) {
+                               uint32_t sentinel, const T* __restrict__ x, T* __restrict__ proj,
+                               double* __restrict__ sq) {
+  double acc = 0.0;
   for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
     T s = 0;
     for (int k = 0; k < 27; ++k) {
@@ -927,6 +953,13 @@ __global__ void k_screen_proj2(const uint32_t* __restrict__ key, const T* __rest
       if (kk != sentinel) s += phi[27 * p + k] * x[kk];
     }
     proj[p] = s;
+    acc += (double)s * (double)s;
+  }
+  if (sq) {
+    typedef cub::BlockReduce<double, kThreads> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double tot = BR(tmp).Sum(acc);
+    if (threadIdx.x == 0) sq[blockIdx.x] = tot;
   }
 }
 template <typename T>
@@ -1002,9 +1035,10 @@ CUtensorMap plane_map(const T* base, int L, uint32_t bx, uint32_t by) {
 constexpr int kTmaMinLevel = 6;  // res >= 64: full 64-wide x tiles (k_op3)
 
 // launches k_op3 over the interior tiles and the face tiles of a level
+// returns the number of CTAs (= dot partials written when a.dot is set)
 template <typename T, int MODE>
-void launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, const CUtensorMap& mp, T* out,
-                const Op3Args<T>& a, int nz) {
+int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, const CUtensorMap& mp, T* out,
+               const Op3Args<T>& a, int nz) {
   typedef Geo3<T> G;
   static bool attr = false;  // once per instantiation pair
   if (!attr) {
@@ -1013,19 +1047,29 @@ void launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, co
     attr = true;
   }
   const int nbx = a.nbx, nby = a.nby;
+  Op3Args<T> e = a;
+  e.ox = e.oy = 0;
+  e.dot_base = 0;
+  if (a.edge == 0) {  // every row acts as the interior row: one launch of the interior variant
+    k_op3<T, MODE, false><<<dim3(nbx, nby, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+    PR_CHECK_LAUNCH();
+    return nbx * nby * nz;
+  }
   // interior tiles need every output row at least `edge` from the faces: edge <= 8 (one tile row)
   const bool split = nbx > 2 && nby > 2 && a.edge <= TY;
-  Op3Args<T> e = a;
   e.all = split ? 0 : 1;
   if (split) {
+    e.ox = e.oy = 1;
     k_op3<T, MODE, false><<<dim3(nbx - 2, nby - 2, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
     PR_CHECK_LAUNCH();
+    e.dot_base = (nbx - 2) * (nby - 2) * nz;
     k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
     PR_CHECK_LAUNCH();
   } else {
     k_op3<T, MODE, true><<<dim3(nbx * nby, 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
     PR_CHECK_LAUNCH();
   }
+  return nbx * nby * nz;
 }
 
 // ------------------------------------------------------------------ host: the system
@@ -1103,10 +1147,15 @@ struct System2 {
       q.tM = upload(M, "tM");
       q.tS = upload(S, "tS");
       {
+        // a row acts as the interior row when they agree on every column inside the grid: the
+        // kernels read zeros outside it (the truncated rows of the finest level are such rows)
         const int res = 1 << l, mid = res / 2;
         auto same = [&](int i) {
-          for (int d = 0; d < 5; ++d)
+          for (int d = 0; d < 5; ++d) {
+            const int col = i + d - 2;
+            if (col < 0 || col >= res) continue;
             if ((T)M[5 * i + d] != (T)M[5 * mid + d] || (T)S[5 * i + d] != (T)S[5 * mid + d]) return false;
+          }
           return true;
         };
         int e = 0;
@@ -1195,24 +1244,54 @@ struct System2 {
     scr.proj = c->buf<T>(std::string("d2_proj_") + tn2<T>(), c->P);
   }
 
-  // y += sign wh3 Phi Phi^T x
-  void screen(const T* x, T* y, int sign) {
-    if (scr.S == 0) return;
+  // y += sign wh3 Phi Phi^T x; with sq, per-block sums of (Phi^T x)^2; returns the block count
+  int screen(const T* x, T* y, int sign, double* sq = nullptr) {
+    if (scr.S == 0) return 0;
     cudaStream_t s = c->stream;
-    k_screen_proj2<T><<<grid_for(scr.P, 1u << 20), kThreads, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, x,
-                                                                      scr.proj);
+    const unsigned nb = grid_for(scr.P, 1u << 20);
+    k_screen_proj2<T><<<nb, kThreads, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, x, scr.proj, sq);
     PR_CHECK_LAUNCH();
     k_screen_gather2<T><<<grid_for(scr.S, 1u << 20), kThreads, 0, s>>>(scr.snode, scr.soff, scr.S, scr.sval, scr.phi,
                                                                         scr.proj, (T)(sign * scr.wh3), y);
     PR_CHECK_LAUNCH();
     bytes += (double)scr.P * 27 * (4 + 2 * sizeof(T)) + (double)scr.P * sizeof(T) +
              (double)scr.pairs * (4 + 2 * sizeof(T)) + (double)scr.S * (8 + 2 * sizeof(T));
+    return (int)nb;
+  }
+
+  // fused dot products (finest level on the TMA operator): per-CTA partials and their sums
+  double* parts_a = nullptr;  // operator partials
+  double* parts_b = nullptr;  // screening partials
+  double* sums = nullptr;     // 2 doubles
+  double* rz_parts = nullptr; // set by pcg2: the last post-smoothing step at level 0 writes f . out
+  int rz_np = 0;
+  bool fused_dots() const { return !lv.empty() && lv[0].L >= kTmaMinLevel; }
+  void alloc_parts() {
+    const int res = 1 << lv[0].L;
+    const size_t tiles = (size_t)(res / Geo3<T>::TXP) * (res / TY) * ((res + kZChunk3 - 1) / kZChunk3);
+    parts_a = c->buf<double>(std::string("d2_parts_a_") + tn2<T>(), tiles);
+    parts_b = c->buf<double>(std::string("d2_parts_b_") + tn2<T>(), 1u << 20);
+    sums = c->buf<double>(std::string("d2_sums_") + tn2<T>(), 2);
+  }
+  // na partials of parts_a + w * (nb partials of parts_b), summed in a fixed order
+  double sum_parts(int na, int nb, double w) {
+    cudaStream_t s = c->stream;
+    k_sum_parts<<<1, 32, 0, s>>>(parts_a, na, sums);
+    PR_CHECK_LAUNCH();
+    if (nb > 0) {
+      k_sum_parts<<<1, 32, 0, s>>>(parts_b, nb, sums + 1);
+      PR_CHECK_LAUNCH();
+    }
+    PR_CUDA(cudaMemcpyAsync(c->h_scalars, sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    return c->h_scalars[0] + (nb > 0 ? w * c->h_scalars[1] : 0.0);
   }
 
   // One operator pass on level li (modes k_op2 / k_op3); c0 is the first Chebyshev coefficient of
   // the fused modes.  tma < 0: k_op3 on levels with res >= 64, k_op2 below.
-  void op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0,
-          int tma = -1, double c0 = 0.0) {
+  int op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0,
+         int tma = -1, double c0 = 0.0, double* dot = nullptr) {
+    int nparts = 0;
     const Level2<T>& q = lv[li];
     const int res = 1 << q.L;
     cudaStream_t s = c->stream;
@@ -1236,19 +1315,22 @@ struct System2 {
       A.nbx = res / G::TXP;
       A.nby = res / TY;
       A.err = err;
+      A.dot = dot;
+      A.dot_base = 0;
       const int nz = (res + kZChunk3 - 1) / kZChunk3;
       const CUtensorMap mx = plane_map<T>(x, q.L, G::BW, SH);
       const CUtensorMap mf = f ? plane_map<T>(f, q.L, G::TXP, TY) : mx;
       const CUtensorMap mp = xp ? plane_map<T>(xp, q.L, G::TXP, TY) : mx;
       switch (mode) {
-        case kOpApply: launch_op3<T, kOpApply>(s, mx, mf, mp, out, A, nz); break;
-        case kOpResid: launch_op3<T, kOpResid>(s, mx, mf, mp, out, A, nz); break;
-        case kOpCheb: launch_op3<T, kOpCheb>(s, mx, mf, mp, out, A, nz); break;
-        case kOpChebF: launch_op3<T, kOpChebF>(s, mx, mf, mp, out, A, nz); break;
-        default: launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
+        case kOpApply: nparts = launch_op3<T, kOpApply>(s, mx, mf, mp, out, A, nz); break;
+        case kOpResid: nparts = launch_op3<T, kOpResid>(s, mx, mf, mp, out, A, nz); break;
+        case kOpCheb: nparts = launch_op3<T, kOpCheb>(s, mx, mf, mp, out, A, nz); break;
+        case kOpChebF: nparts = launch_op3<T, kOpChebF>(s, mx, mf, mp, out, A, nz); break;
+        default: nparts = launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
       }
     } else {
       PR_REQUIRE(mode <= kOpCheb, PR_ERR_INTERNAL, "fused Chebyshev modes need the TMA operator");
+      PR_REQUIRE(dot == nullptr, PR_ERR_INTERNAL, "fused dot products need the TMA operator");
       dim3 grid((res + TX - 1) / TX, (res + TY - 1) / TY, (res + kZChunk - 1) / kZChunk);
       if (mode == kOpApply) k_op2<T, kOpApply><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
       else if (mode == kOpResid) k_op2<T, kOpResid><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
@@ -1257,6 +1339,7 @@ struct System2 {
     }
     const int reads = mode == kOpApply || mode == kOpChebF ? 1 : (mode == kOpCheb && xp ? 3 : 2);
     bytes += (double)q.n * sizeof(T) * (reads + 1);
+    return nparts;
   }
 
   // throws if a TMA wait ran out since init()
@@ -1301,7 +1384,9 @@ struct System2 {
     T* prev = from_zero ? nullptr : y;
     for (int k = 1; k < kChebSteps; ++k) {
       T* dst = (cur == x) ? y : x;
-      op(li, kOpCheb, cur, f, prev, dst, ca[k], cb[k]);
+      const bool last_fine = li == 0 && !from_zero && k == kChebSteps - 1 && rz_parts != nullptr;
+      const int np = op(li, kOpCheb, cur, f, prev, dst, ca[k], cb[k], -1, 0.0, last_fine ? rz_parts : nullptr);
+      if (last_fine) rz_np = np;
       prev = cur;
       cur = dst;
     }
@@ -1341,31 +1426,53 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
   T* z = c->buf<T>("d2cg_z_" + tn, n);
   T* d = c->buf<T>("d2cg_d_" + tn, n);
   T* q = c->buf<T>("d2cg_q_" + tn, n);
+  const bool fused = sys.fused_dots();
+  if (fused) sys.alloc_parts();
   PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
   double rr = dot<T>(c, r, r, n);
   sys.bytes += 2.0 * n * sizeof(T);
   if (!(std::sqrt(rr) > tol_abs)) return 0;
-  sys.vcycle(0, r, z);
-  double rz = dot<T>(c, r, z, n);
+  // z = M r and r . z (fused: the last post-smoothing step of the finest level)
+  auto precondition = [&]() {
+    if (fused) {
+      sys.rz_parts = sys.parts_a;
+      sys.rz_np = 0;
+      sys.vcycle(0, r, z);
+      sys.rz_parts = nullptr;
+      PR_REQUIRE(sys.rz_np > 0, PR_ERR_INTERNAL, "fused r.z was not produced");
+      return sys.sum_parts(sys.rz_np, 0, 0.0);
+    }
+    sys.vcycle(0, r, z);
+    sys.bytes += 2.0 * n * sizeof(T);
+    return dot<T>(c, r, z, n);
+  };
+  double rz = precondition();
   PR_CUDA(cudaMemcpyAsync(d, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
-  sys.bytes += 4.0 * n * sizeof(T);
+  sys.bytes += 2.0 * n * sizeof(T);
   int it = 0;
   while (it < maxit) {
-    sys.op(0, kOpApply, d, nullptr, nullptr, q);
-    sys.screen(d, q, +1);
-    const double dq = dot<T>(c, d, q, n);
+    double dq;
+    if (fused) {
+      const int na = sys.op(0, kOpApply, d, nullptr, nullptr, q, 0.0, 0.0, -1, 0.0, sys.parts_a);
+      const int nb = sys.screen(d, q, +1, sys.parts_b);
+      dq = sys.sum_parts(na, nb, sys.scr.wh3);
+    } else {
+      sys.op(0, kOpApply, d, nullptr, nullptr, q);
+      sys.screen(d, q, +1);
+      dq = dot<T>(c, d, q, n);
+      sys.bytes += 2.0 * n * sizeof(T);
+    }
     if (!(dq > 0.0) || !(rz > 0.0)) break;
     const double alpha = rz / dq;
     rr = cg_update<T>(c, n, alpha, d, q, x, r);
-    sys.bytes += 8.0 * n * sizeof(T);
+    sys.bytes += 6.0 * n * sizeof(T);
     ++it;
     if (!std::isfinite(rr) || std::sqrt(rr) <= tol_abs) break;
-    sys.vcycle(0, r, z);
-    const double rz_new = dot<T>(c, r, z, n);
+    const double rz_new = precondition();
     const double beta = rz_new / rz;
     rz = rz_new;
     xpby<T>(s, n, z, beta, d);
-    sys.bytes += 5.0 * n * sizeof(T);
+    sys.bytes += 3.0 * n * sizeof(T);
   }
   return it;
 }

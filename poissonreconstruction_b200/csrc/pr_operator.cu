@@ -107,6 +107,130 @@ __global__ void k_dot_partial(const TA* __restrict__ a, const TB* __restrict__ b
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
+// 16-byte vector access in chunks of four elements (one float4, or two double2); used when every
+// pointer of a call is 16-byte aligned, the scalar kernels otherwise
+template <typename T>
+struct Q4 {
+  T v[4];
+};
+__device__ __forceinline__ Q4<float> ld4(const float* p, uint64_t i) {
+  const float4 a = reinterpret_cast<const float4*>(p)[i];
+  return Q4<float>{{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ Q4<double> ld4(const double* p, uint64_t i) {
+  const double2* q = reinterpret_cast<const double2*>(p) + 2 * i;
+  const double2 a = q[0], b = q[1];
+  return Q4<double>{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float* p, uint64_t i, const Q4<float>& v) {
+  reinterpret_cast<float4*>(p)[i] = make_float4(v.v[0], v.v[1], v.v[2], v.v[3]);
+}
+__device__ __forceinline__ void st4(double* p, uint64_t i, const Q4<double>& v) {
+  double2* q = reinterpret_cast<double2*>(p) + 2 * i;
+  q[0] = make_double2(v.v[0], v.v[1]);
+  q[1] = make_double2(v.v[2], v.v[3]);
+}
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <typename T>
+__global__ void k_dot_partial4(const T* __restrict__ a, const T* __restrict__ b, uint64_t n, double* __restrict__ part) {
+  double s = 0.0;
+  const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const Q4<T> x = ld4(a, i), y = ld4(b, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s += (double)x.v[k] * (double)y.v[k];
+  }
+  for (uint64_t i = 4 * n4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    s += (double)a[i] * (double)b[i];
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+template <typename T>
+__global__ void k_cg_update4(uint64_t n, T alpha, const T* __restrict__ d, const T* __restrict__ q, T* __restrict__ x,
+                             T* __restrict__ r, double* __restrict__ part) {
+  double s = 0.0;
+  const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const Q4<T> dv = ld4(d, i), qv = ld4(q, i);
+    Q4<T> xv = ld4(x, i), rv = ld4(r, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      xv.v[k] += alpha * dv.v[k];
+      rv.v[k] = rv.v[k] - alpha * qv.v[k];
+      s += (double)rv.v[k] * (double)rv.v[k];
+    }
+    st4(x, i, xv);
+    st4(r, i, rv);
+  }
+  for (uint64_t i = 4 * n4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    x[i] += alpha * d[i];
+    const T ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    s += (double)ri * (double)ri;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+template <typename T>
+__global__ void k_xpby4(uint64_t n, const T* __restrict__ z, T beta, T* __restrict__ d) {
+  const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const Q4<T> zv = ld4(z, i);
+    Q4<T> dv = ld4(d, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dv.v[k] = zv.v[k] + beta * dv.v[k];
+    st4(d, i, dv);
+  }
+  for (uint64_t i = 4 * n4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    d[i] = z[i] + beta * d[i];
+}
+
+template <typename Tin, typename Tout>
+__global__ void k_axpy4(uint64_t n, double a, const Tin* __restrict__ x, Tout* __restrict__ y) {
+  const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const Q4<Tin> xv = ld4(x, i);
+    Q4<Tout> yv = ld4(y, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) yv.v[k] = (Tout)((double)yv.v[k] + a * (double)xv.v[k]);
+    st4(y, i, yv);
+  }
+  for (uint64_t i = 4 * n4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    y[i] = (Tout)((double)y[i] + a * (double)x[i]);
+}
+
+__global__ void k_convert_norm4(uint64_t n, const double* __restrict__ x, float* __restrict__ y,
+                                double* __restrict__ part) {
+  double s = 0.0;
+  const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const Q4<double> v = ld4(x, i);
+    Q4<float> o;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      o.v[k] = (float)v.v[k];
+      s += v.v[k] * v.v[k];
+    }
+    st4(y, i, o);
+  }
+  for (uint64_t i = 4 * n4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double v = x[i];
+    y[i] = (float)v;
+    s += v * v;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 __global__ void k_sum_final(const double* __restrict__ part, int np, double* __restrict__ out) {
   // one warp, fixed order: lane-strided partial sums then a fixed shuffle tree
   double s = 0.0;
@@ -339,7 +463,8 @@ template <typename T>
 double dot(pr_context* c, const T* a, const T* b, uint64_t n) {
   double* part = c->buf<double>("dot_part", kDotBlocks);
   double* out = c->buf<double>("dot_out", 1);
-  k_dot_partial<T, T><<<kDotBlocks, kThreads, 0, c->stream>>>(a, b, n, part);
+  if (aligned16(a) && aligned16(b)) k_dot_partial4<T><<<kDotBlocks, kThreads, 0, c->stream>>>(a, b, n, part);
+  else k_dot_partial<T, T><<<kDotBlocks, kThreads, 0, c->stream>>>(a, b, n, part);
   PR_CHECK_LAUNCH();
   k_sum_final<<<1, 32, 0, c->stream>>>(part, kDotBlocks, out);
   PR_CHECK_LAUNCH();
@@ -352,7 +477,10 @@ template <typename T>
 double cg_update(pr_context* c, uint64_t n, double alpha, const T* d, const T* q, T* x, T* r) {
   double* part = c->buf<double>("dot_part", kDotBlocks);
   double* out = c->buf<double>("dot_out", 1);
-  k_cg_update<T><<<kDotBlocks, kThreads, 0, c->stream>>>(n, (T)alpha, d, q, x, r, part);
+  if (aligned16(d) && aligned16(q) && aligned16(x) && aligned16(r))
+    k_cg_update4<T><<<kDotBlocks, kThreads, 0, c->stream>>>(n, (T)alpha, d, q, x, r, part);
+  else
+    k_cg_update<T><<<kDotBlocks, kThreads, 0, c->stream>>>(n, (T)alpha, d, q, x, r, part);
   PR_CHECK_LAUNCH();
   k_sum_final<<<1, 32, 0, c->stream>>>(part, kDotBlocks, out);
   PR_CHECK_LAUNCH();
@@ -364,7 +492,8 @@ double cg_update(pr_context* c, uint64_t n, double alpha, const T* d, const T* q
 double convert_norm(pr_context* c, const double* x, float* y, uint64_t n) {
   double* part = c->buf<double>("dot_part", kDotBlocks);
   double* out = c->buf<double>("dot_out", 1);
-  k_convert_norm<<<kDotBlocks, kThreads, 0, c->stream>>>(n, x, y, part);
+  if (aligned16(x) && aligned16(y)) k_convert_norm4<<<kDotBlocks, kThreads, 0, c->stream>>>(n, x, y, part);
+  else k_convert_norm<<<kDotBlocks, kThreads, 0, c->stream>>>(n, x, y, part);
   PR_CHECK_LAUNCH();
   k_sum_final<<<1, 32, 0, c->stream>>>(part, kDotBlocks, out);
   PR_CHECK_LAUNCH();
@@ -375,7 +504,8 @@ double convert_norm(pr_context* c, const double* x, float* y, uint64_t n) {
 
 template <typename T>
 void xpby(cudaStream_t s, uint64_t n, const T* z, double beta, T* d) {
-  k_xpby<T><<<grid_for(n), kThreads, 0, s>>>(n, z, (T)beta, d);
+  if (aligned16(z) && aligned16(d)) k_xpby4<T><<<grid_for((n + 3) / 4), kThreads, 0, s>>>(n, z, (T)beta, d);
+  else k_xpby<T><<<grid_for(n), kThreads, 0, s>>>(n, z, (T)beta, d);
   PR_CHECK_LAUNCH();
 }
 
@@ -387,7 +517,8 @@ void scale_convert(cudaStream_t s, uint64_t n, double a, const Tin* x, Tout* y) 
 
 template <typename Tin, typename Tout>
 void axpy(cudaStream_t s, uint64_t n, double a, const Tin* x, Tout* y) {
-  k_axpy<Tin, Tout><<<grid_for(n), kThreads, 0, s>>>(n, a, x, y);
+  if (aligned16(x) && aligned16(y)) k_axpy4<Tin, Tout><<<grid_for((n + 3) / 4), kThreads, 0, s>>>(n, a, x, y);
+  else k_axpy<Tin, Tout><<<grid_for(n), kThreads, 0, s>>>(n, a, x, y);
   PR_CHECK_LAUNCH();
 }
 
