@@ -490,6 +490,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
 #pragma unroll
     for (int k = 0; k < NS; ++k) wa[j][k] = wb[j][k] = wc[j][k] = T(0);
   T* op = out + (int64_t)gx + (int64_t)res * gy + plane * (z0 - 4);  // output row of plane zo = z0 - 4 + it
+  const bool want_dot = A.dot != nullptr;
   double dacc = 0.0;  // A.dot: this thread's share of the product
   int kstate = -1;  // EDGE kOpChebF: s_k holds the scales of: -1 nothing, 0 interior planes, 1 plane kzin
   int kzin = 0;
@@ -660,8 +661,9 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
           }
         }
         *reinterpret_cast<V2*>(op) = V2{res2[0], res2[1]};
-        if (MODE == kOpApply) dacc += (double)wc[0][(k + 3) % NS] * (double)res2[0] + (double)wc[1][(k + 3) % NS] * (double)res2[1];
-        if (MODE == kOpCheb) dacc += (double)fo.x * (double)res2[0] + (double)fo.y * (double)res2[1];
+        if (MODE == kOpApply && want_dot)
+          dacc += (double)wc[0][(k + 3) % NS] * (double)res2[0] + (double)wc[1][(k + 3) % NS] * (double)res2[1];
+        if (MODE == kOpCheb && want_dot) dacc += (double)fo.x * (double)res2[0] + (double)fo.y * (double)res2[1];
       }
       op += plane;
     }
@@ -854,78 +856,131 @@ __global__ void k_splat2(const uint32_t* __restrict__ run_key, const uint32_t* _
   }
 }
 
-// b = h^2 sum_a (G_a M M) nf_a on the finest level, streamed like k_op2 (three inputs)
+// b = h^2 sum_a (G_a M M) nf_a on the finest level (res >= 64), TMA-fed like k_op3: a CTA owns
+// 64 x 8 columns (x pairs per thread) and streams up to kZChunk3 planes; four stages, each the three
+// haloed component planes (zero fill outside the grid = the truncated rows).  m is symmetric and
+// g antisymmetric (g[2] = 0), so each 5-tap filter is two pair sums or differences.
 struct RhsCoef {
   double g[5], m[5], h2;
+  int* err;
 };
-__global__ void __launch_bounds__(kThreads) k_rhs2(const double* __restrict__ nf, int L, RhsCoef k,
-                                                   double* __restrict__ b) {
-  __shared__ double s_in[3][SH][SW];
-  __shared__ double s_u[3][SH][TX];
+struct GeoR {
+  static constexpr int NS = 4;
+  static constexpr int TXP = 64;
+  static constexpr int BW = 68;                                      // from x0 - 2 (16-byte aligned)
+  static constexpr uint32_t PBYTES = BW * SH * sizeof(double);       // one component plane
+  static constexpr size_t OFF_U = (size_t)NS * 3 * PBYTES;
+  static constexpr size_t OFF_BAR = OFF_U + 3 * (size_t)SH * TXP * sizeof(double);
+  static constexpr size_t BYTES = OFF_BAR + NS * 8 + 16;
+};
+
+__device__ __forceinline__ double fsym(const double* v, const double* c) {
+  return c[0] * (v[0] + v[4]) + c[1] * (v[1] + v[3]) + c[2] * v[2];
+}
+__device__ __forceinline__ double fanti(const double* v, const double* c) {
+  return c[0] * (v[0] - v[4]) + c[1] * (v[1] - v[3]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_rhs3(const __grid_constant__ CUtensorMap m0,
+                                                   const __grid_constant__ CUtensorMap m1,
+                                                   const __grid_constant__ CUtensorMap m2, int L,
+                                                   const __grid_constant__ RhsCoef k, double* __restrict__ b) {
+  typedef GeoR G;
+  constexpr int NS = G::NS, BW = G::BW, TXP = G::TXP;
+  extern __shared__ __align__(128) unsigned char smem[];
+  double(*s_in)[3][SH][BW] = reinterpret_cast<double(*)[3][SH][BW]>(smem);
+  double(*s_u)[SH][TXP] = reinterpret_cast<double(*)[SH][TXP]>(smem + G::OFF_U);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NS * 8);
   const int res = 1 << L;
-  const int64_t plane = (int64_t)res * res, n = plane * res;
-  const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int z0 = blockIdx.z * kZChunk, z1 = min(z0 + kZChunk, res);
-  const int gx = x0 + tx, gy = y0 + ty;
-  const bool own = gx < res && gy < res;
-  const int e0 = t, e1 = t + kThreads;
-  const bool has1 = e1 < SH * SW;
-  const int r0 = e0 / SW, c0 = e0 % SW, r1 = has1 ? e1 / SW : 0, c1 = has1 ? e1 % SW : 0;
-  const int X0 = x0 - 2 + c0, Y0 = y0 - 2 + r0, X1 = x0 - 2 + c1, Y1 = y0 - 2 + r1;
-  const bool ok0 = X0 >= 0 && X0 < res && Y0 >= 0 && Y0 < res;
-  const bool ok1 = has1 && X1 >= 0 && X1 < res && Y1 >= 0 && Y1 < res;
-  const int64_t o0 = ok0 ? (int64_t)X0 + (int64_t)res * Y0 : 0, o1 = ok1 ? (int64_t)X1 + (int64_t)res * Y1 : 0;
-  double wa[5], wb[5];
+  const int64_t plane = (int64_t)res * res;
+  const int t = threadIdx.x, p = t & 31, ty = t >> 5;
+  const int x0 = blockIdx.x * TXP, y0 = blockIdx.y * TY;
+  const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
+  const int nplanes = z1 - z0 + 4;
+  if (t == 0) {
+    for (int q = 0; q < NS; ++q) mbar_init(&bar[q], 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int it) {
+    const int q = it % NS, zin = z0 - 2 + it;
+    mbar_expect_tx(&bar[q], 3 * G::PBYTES);
+    tma_load_3d(&s_in[q][0][0][0], &m0, x0 - 2, y0 - 2, zin, &bar[q]);
+    tma_load_3d(&s_in[q][1][0][0], &m1, x0 - 2, y0 - 2, zin, &bar[q]);
+    tma_load_3d(&s_in[q][2][0][0], &m2, x0 - 2, y0 - 2, zin, &bar[q]);
+  };
+  if (t == 0)
+    for (int it = 0; it < min(NS, nplanes); ++it) issue(it);
+  double wa[2][5], wb[2][5];
 #pragma unroll
-  for (int q = 0; q < 5; ++q) wa[q] = wb[q] = 0.0;
-  for (int zin = z0 - 2; zin <= z1 + 1; ++zin) {
-    const bool zok = zin >= 0 && zin < res;
+  for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      s_in[a][r0][c0] = (ok0 && zok) ? nf[a * n + o0 + zin * plane] : 0.0;
-      if (has1) s_in[a][r1][c1] = (ok1 && zok) ? nf[a * n + o1 + zin * plane] : 0.0;
+    for (int q = 0; q < 5; ++q) wa[j][q] = wb[j][q] = 0.0;
+  double* op = b + (int64_t)(x0 + 2 * p) + (int64_t)res * (y0 + ty) + plane * (z0 - 4);
+  int it = 0;
+  bool stop = false;
+  for (; it < nplanes; ++it) {
+    const int q = it % NS;
+    if (!mbar_wait(&bar[q], (uint32_t)(it / NS) & 1u)) {
+      atomicExch(k.err, 1);
+      *s_abort = 1;
     }
-    __syncthreads();
+    // x filters (G on component 0, M on 1 and 2) of rows ty and ty + 8
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int r = ty + 8 * q;
+    for (int rr = 0; rr < 2; ++rr) {
+      const int r = ty + 8 * rr;
       if (r < SH) {
-        double u0 = 0.0, u1 = 0.0, u2 = 0.0;
 #pragma unroll
-        for (int d = 0; d < 5; ++d) {
-          u0 += k.g[d] * s_in[0][r][tx + d];
-          u1 += k.m[d] * s_in[1][r][tx + d];
-          u2 += k.m[d] * s_in[2][r][tx + d];
+        for (int a = 0; a < 3; ++a) {
+          const double* row = &s_in[q][a][r][2 * p];
+          const double2 v0 = *reinterpret_cast<const double2*>(row), v1 = *reinterpret_cast<const double2*>(row + 2),
+                        v2 = *reinterpret_cast<const double2*>(row + 4);
+          const double v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
+          const double o0 = a == 0 ? fanti(v, k.g) : fsym(v, k.m);
+          const double o1 = a == 0 ? fanti(v + 1, k.g) : fsym(v + 1, k.m);
+          *reinterpret_cast<double2*>(&s_u[a][r][2 * p]) = make_double2(o0, o1);
         }
-        s_u[0][r][tx] = u0;
-        s_u[1][r][tx] = u1;
-        s_u[2][r][tx] = u2;
       }
     }
-    __syncthreads();
-    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-#pragma unroll
-    for (int d = 0; d < 5; ++d) {
-      v0 += k.m[d] * s_u[0][ty + d][tx];
-      v1 += k.g[d] * s_u[1][ty + d][tx];
-      v2 += k.m[d] * s_u[2][ty + d][tx];
+    __syncthreads();  // stage q is read, s_u written
+    if (*s_abort) {
+      stop = true;
+      break;
     }
+    if (t == 0 && it + NS < nplanes) issue(it + NS);
+    double col[3][2][5];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      wa[q] = wa[q + 1];
-      wb[q] = wb[q + 1];
-    }
-    wa[4] = v0 + v1;
-    wb[4] = v2;
-    const int zo = zin - 2;
-    if (own && zo >= z0 && zo < z1) {
-      double acc = 0.0;
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int d = 0; d < 5; ++d) acc += k.m[d] * wa[d] + k.g[d] * wb[d];
-      b[(int64_t)gx + (int64_t)res * gy + plane * zo] = k.h2 * acc;
+      for (int d = 0; d < 5; ++d) {
+        const double2 u = *reinterpret_cast<const double2*>(&s_u[a][ty + d][2 * p]);
+        col[a][0][d] = u.x;
+        col[a][1][d] = u.y;
+      }
+    __syncthreads();  // s_u is read before the next plane writes it
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+      for (int q2 = 0; q2 < 4; ++q2) {
+        wa[j][q2] = wa[j][q2 + 1];
+        wb[j][q2] = wb[j][q2 + 1];
+      }
+      wa[j][4] = fsym(col[0][j], k.m) + fanti(col[1][j], k.g);  // (G M) x + (M G) y, then M along z
+      wb[j][4] = fsym(col[2][j], k.m);                          // (M M) z, then G along z
     }
+    const int zo = z0 - 4 + it;
+    if (zo >= z0) {
+      double o[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) o[j] = k.h2 * (fsym(wa[j], k.m) + fanti(wb[j], k.g));
+      *reinterpret_cast<double2*>(op) = make_double2(o[0], o[1]);
+    }
+    op += plane;
   }
+  if (stop && t == 0)
+    for (int q = it; q < min(it + NS, nplanes); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
 }
 
 // screening right-hand side: b[node] += (wh3 / 2) sum of phi over the node's pairs
@@ -1479,6 +1534,66 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
 
 }  // namespace
 
+namespace {
+// b = h^2 sum_a (G_a M M) nf_a from the dense natural-order normal field (3 n)
+__global__ void k_rhs_small(const double* __restrict__ nf, int L, RhsCoef k, double* __restrict__ b) {
+  const int res = 1 << L;
+  const uint64_t n = 1ull << (3 * L);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i & (res - 1)), y = (int)((i >> L) & (res - 1)), z = (int)(i >> (2 * L));
+    double acc = 0.0;
+    for (int dz = -2; dz <= 2; ++dz) {
+      if (z + dz < 0 || z + dz >= res) continue;
+      for (int dy = -2; dy <= 2; ++dy) {
+        if (y + dy < 0 || y + dy >= res) continue;
+        for (int dx = -2; dx <= 2; ++dx) {
+          if (x + dx < 0 || x + dx >= res) continue;
+          const uint64_t j = (uint64_t)(x + dx) + (uint64_t)res * ((uint64_t)(y + dy) + (uint64_t)res * (z + dz));
+          acc += nf[j] * k.g[dx + 2] * k.m[dy + 2] * k.m[dz + 2] + nf[n + j] * k.m[dx + 2] * k.g[dy + 2] * k.m[dz + 2] +
+                 nf[2 * n + j] * k.m[dx + 2] * k.m[dy + 2] * k.g[dz + 2];
+        }
+      }
+    }
+    b[i] = k.h2 * acc;
+  }
+}
+
+void deg2_rhs(pr_context* c, const double* nf, double* b, uint32_t D, double h) {
+  cudaStream_t s = c->stream;
+  RhsCoef k;
+  for (int d = 0; d < 5; ++d) {
+    k.g[d] = consts().g[d];
+    k.m[d] = consts().m[d];
+  }
+  k.h2 = h * h;
+  int* err = c->buf<int>("d2_err", 1);
+  PR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  k.err = err;
+  const uint64_t n = 1ull << (3 * D);
+  const int res = 1 << D;
+  if ((int)D < kTmaMinLevel) {
+    k_rhs_small<<<grid_for(n), kThreads, 0, s>>>(nf, (int)D, k, b);
+    PR_CHECK_LAUNCH();
+    return;
+  }
+  static bool attr = false;
+  if (!attr) {
+    PR_CUDA(cudaFuncSetAttribute(k_rhs3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GeoR::BYTES));
+    attr = true;
+  }
+  const CUtensorMap m0 = plane_map<double>(nf, (int)D, GeoR::BW, SH);
+  const CUtensorMap m1 = plane_map<double>(nf + n, (int)D, GeoR::BW, SH);
+  const CUtensorMap m2 = plane_map<double>(nf + 2 * n, (int)D, GeoR::BW, SH);
+  const dim3 grid(res / GeoR::TXP, res / TY, (res + kZChunk3 - 1) / kZChunk3);
+  k_rhs3<<<grid, kThreads, GeoR::BYTES, s>>>(m0, m1, m2, (int)D, k, b);
+  PR_CHECK_LAUNCH();
+  int h_err = 0;
+  PR_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  c->sync();
+  PR_REQUIRE(h_err == 0, PR_ERR_CUDA, "degree-2 right-hand side: a TMA pipeline wait timed out");
+}
+}  // namespace
+
 // ------------------------------------------------------------------ stages
 // Splat, right-hand side and screening payload of the degree-2 system (natural order).
 void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
@@ -1519,17 +1634,8 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
     PR_CHECK_LAUNCH();
   }
   const double h = 1.0 / (double)(1u << D);
-  RhsCoef k;
-  for (int d = 0; d < 5; ++d) {
-    k.g[d] = consts().g[d];
-    k.m[d] = consts().m[d];
-  }
-  k.h2 = h * h;
   double* b = c->buf<double>("d2_b", n);
-  const int res = 1 << D;
-  dim3 grid((res + TX - 1) / TX, (res + TY - 1) / TY, (res + kZChunk - 1) / kZChunk);
-  k_rhs2<<<grid, kThreads, 0, s>>>(nf, (int)D, k, b);
-  PR_CHECK_LAUNCH();
+  deg2_rhs(c, nf, b, D, h);
   c->S = 0;
   c->S_pairs = 0;
   if (pw > 0.0 && T > 0) {
