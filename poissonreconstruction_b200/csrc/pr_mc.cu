@@ -469,17 +469,11 @@ __device__ void mc_load_tile2(double* tile, const double* __restrict__ x, uint32
   }
 }
 
-// every warp classifies 32 consecutive corners of the 17^3 (row-major, 17 per row); a ballot
-// collects their bits and one lane per touched row or-s them into its mask (zeroed by the caller
-// before the tile load)
 __device__ __forceinline__ void mc_build_masks2(const double* tile, uint32_t* mask, double iso) {
-  constexpr int NC = MCW * MCW * MCW;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int base = 32 * warp; base < NC; base += 32 * nwarps) {
-    const int c = base + lane;
-    bool in = false;
-    if (c < NC) {
-      const int tx = c % MCW, r = c / MCW, ty = r % MCW, tz = r / MCW;
+  for (int r = threadIdx.x; r < MCW * MCW; r += blockDim.x) {
+    const int ty = r % MCW, tz = r / MCW;
+    uint32_t m = 0;
+    for (int tx = 0; tx < MCW; ++tx) {
       double v = 0.0;
 #pragma unroll
       for (int dz = 0; dz < 2; ++dz)
@@ -488,15 +482,9 @@ __device__ __forceinline__ void mc_build_masks2(const double* tile, uint32_t* ma
 #pragma unroll
           for (int dx = 0; dx < 2; ++dx)
             v = xadd(v, xmul(xmul(xmul(tile[((tz + dz) * MCW2 + ty + dy) * MCW2 + tx + dx], 0.5), 0.5), 0.5));
-      in = v < iso;
+      m |= (uint32_t)(v < iso) << tx;
     }
-    const uint32_t bal = __ballot_sync(0xffffffffu, in);
-    const int r0 = base / MCW, r1 = min(base + 31, NC - 1) / MCW;
-    if (lane <= r1 - r0) {
-      const int r = r0 + lane, lo = MCW * r - base;  // warp lane of the row's corner 0 (may be < 0)
-      const uint32_t m = (lo >= 0 ? bal >> lo : bal << -lo) & ((1u << MCW) - 1u);
-      if (m) atomicOr(&mask[r], m);
-    }
+    mask[r] = m;
   }
 }
 
@@ -506,7 +494,6 @@ __device__ __forceinline__ void mc_block_masks(double* tile, uint32_t* mask, con
   uint32_t bx, by, bz;
   unmorton3(blk, bx, by, bz);
   if (DEG == 2) {
-    for (int r = threadIdx.x; r < MCW * MCW; r += blockDim.x) mask[r] = 0u;
     mc_load_tile2(tile, x, blk, res);
     __syncthreads();
     mc_build_masks2(tile, mask, iso);
