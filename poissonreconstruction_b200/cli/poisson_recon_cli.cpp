@@ -7,8 +7,8 @@
 //
 // Extensions (not in the crate): --solve-mode converged|reference (default converged: the
 // crate's fine system solved to --target-rel-residual; "reference" runs the crate's cascade
-// schedule), --precision mixed|fp64, --target-rel-residual R, --binary (binary PLY output),
-// --device N.
+// schedule), --precision mixed|fp64, --target-rel-residual R, --degree 1|2 (quadratic B-spline
+// node functions), --binary (binary PLY output), --device N.
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -43,6 +43,7 @@ void print_help() {
       "      --solve-mode <converged|reference>   solver (default converged)\n"
       "      --precision <mixed|fp64>             converged mode arithmetic [default: mixed]\n"
       "      --target-rel-residual <R>            converged mode target [default: 1e-6]\n"
+      "      --degree <1|2>                       B-spline degree of the node functions [default: 1]\n"
       "      --binary                             write binary_little_endian PLY\n"
       "      --device <N>                         CUDA device [default: 0]\n"
       "  -h, --help                               Print help\n"
@@ -77,6 +78,7 @@ struct Args {
   bool verbose = false, binary = false, have_input = false;
   int solve_mode = PR_SOLVE_CONVERGED, precision = PR_PRECISION_MIXED;
   double target = 1e-6;
+  unsigned degree = 1;
 };
 
 Args parse(int argc, char** argv) {
@@ -149,6 +151,11 @@ Args parse(int argc, char** argv) {
       if (v == "converged") a.solve_mode = PR_SOLVE_CONVERGED;
       else if (v == "reference") a.solve_mode = PR_SOLVE_REFERENCE_SCHEDULE;
       else usage_error("invalid value '" + v + "' for '--solve-mode'");
+    } else if (name == "degree") {
+      const std::string v = need();
+      if (v == "1") a.degree = 1;
+      else if (v == "2") a.degree = 2;
+      else usage_error("invalid value '" + v + "' for '--degree'");
     } else if (name == "precision") {
       const std::string v = need();
       if (v == "mixed") a.precision = PR_PRECISION_MIXED;
@@ -189,6 +196,7 @@ int main(int argc, char** argv) {
   p.solve_mode = a.solve_mode;
   p.precision = a.precision;
   p.target_rel_residual = a.target;
+  p.degree = a.degree;
 
   pr_context* ctx = nullptr;
   pr_mesh mesh;

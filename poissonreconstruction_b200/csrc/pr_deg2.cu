@@ -706,82 +706,113 @@ __global__ void k_cheb_first2(const T* __restrict__ f, T* __restrict__ out, Leve
 }
 
 // Grid transfers with the B2 subdivision P (fine 2c + k <- coarse c, weights 1/4, 3/4, 3/4, 1/4 for
-// k = -1..2), one thread per coarse node and separable: the prolongation (out = xf + P ec) writes the 2 x 2 x 2
-// fine block of coarse node c (fine 2c, 2c + 1 per axis) from the coarse 3 x 3 x 3 neighbourhood;
-// the restriction reads the fine 4 x 4 x 4 block 2c - 1 .. 2c + 2 as rows of a scalar, a pair and a
-// scalar.
+// k = -1..2), separable, two coarse nodes (2c', 2c' + 1) per thread: the prolongation
+// (out = xf + P ec) writes the fine 4 x 2 x 2 block 4c' .. 4c' + 3 from the coarse 4 x 3 x 3
+// neighbourhood; the restriction reads fine rows 4c' - 1 .. 4c' + 4 (a scalar, four 16-byte
+// aligned values, a scalar).
 template <typename T>
-__global__ void k_prolong3(const T* __restrict__ xf, const T* __restrict__ ec, int Lf, T* __restrict__ out) {
+struct F4 {
+  T v[4];
+};
+template <typename T>
+__device__ __forceinline__ F4<T> ld4x(const T* p) {
   typedef typename Vec2<T>::type V2;
-  const int Lc = Lf - 1, rc = 1 << Lc, rf = 1 << Lf;
-  const uint64_t nc = 1ull << (3 * Lc), m = (uint64_t)rc - 1;
+  if (sizeof(T) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    return F4<T>{{(T)a.x, (T)a.y, (T)a.z, (T)a.w}};
+  }
+  const V2 a = reinterpret_cast<const V2*>(p)[0], b = reinterpret_cast<const V2*>(p)[1];
+  return F4<T>{{a.x, a.y, b.x, b.y}};
+}
+template <typename T>
+__device__ __forceinline__ void st4x(T* p, const F4<T>& v) {
+  typedef typename Vec2<T>::type V2;
+  if (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)v.v[0], (float)v.v[1], (float)v.v[2], (float)v.v[3]);
+    return;
+  }
+  reinterpret_cast<V2*>(p)[0] = V2{v.v[0], v.v[1]};
+  reinterpret_cast<V2*>(p)[1] = V2{v.v[2], v.v[3]};
+}
+
+template <typename T>
+__global__ void k_prolong4(const T* __restrict__ xf, const T* __restrict__ ec, int Lf, T* __restrict__ out) {
+  typedef typename Vec2<T>::type V2;
+  const int Lc = Lf - 1, rc = 1 << Lc, rf = 1 << Lf, hc = rc >> 1;
+  const uint64_t np = 1ull << (3 * Lc - 1);
   const int64_t pc = (int64_t)rc * rc, pf = (int64_t)rf * rf;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x) {
-    const int cx = (int)(i & m), cy = (int)((i >> Lc) & m), cz = (int)(i >> (2 * Lc));
-    T a[3][3][2];  // x pass: [dz][dy][fine x 2cx, 2cx + 1]
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < np; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int cp = (int)(i % hc), cy = (int)((i / hc) % rc), cz = (int)(i / ((uint64_t)hc * rc));
+    const int c0 = 2 * cp;
+    T a[3][3][4];  // x pass: [dz][dy][fine x 4cp .. 4cp + 3]
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
       for (int dy = 0; dy < 3; ++dy) {
         const int Z = cz + dz - 1, Y = cy + dy - 1;
-        T e0 = 0, e1 = 0, e2 = 0;
+        T em = 0, e0 = 0, e1 = 0, ep = 0;  // coarse c0 - 1, c0, c0 + 1, c0 + 2
         if (Z >= 0 && Z < rc && Y >= 0 && Y < rc) {
           const T* row = ec + Z * pc + (int64_t)Y * rc;
-          e1 = row[cx];
-          if (cx > 0) e0 = row[cx - 1];
-          if (cx + 1 < rc) e2 = row[cx + 1];
+          const V2 e = *reinterpret_cast<const V2*>(row + c0);
+          e0 = e.x;
+          e1 = e.y;
+          if (c0 > 0) em = row[c0 - 1];
+          if (c0 + 2 < rc) ep = row[c0 + 2];
         }
-        a[dz][dy][0] = T(0.75) * e1 + T(0.25) * e0;
-        a[dz][dy][1] = T(0.75) * e1 + T(0.25) * e2;
+        a[dz][dy][0] = T(0.75) * e0 + T(0.25) * em;
+        a[dz][dy][1] = T(0.75) * e0 + T(0.25) * e1;
+        a[dz][dy][2] = T(0.75) * e1 + T(0.25) * e0;
+        a[dz][dy][3] = T(0.75) * e1 + T(0.25) * ep;
       }
 #pragma unroll
     for (int zo = 0; zo < 2; ++zo)
 #pragma unroll
       for (int yo = 0; yo < 2; ++yo) {
-        T v[2];
+        const int64_t f = (int64_t)(4 * cp) + (int64_t)rf * (2 * cy + yo) + pf * (2 * cz + zo);
+        F4<T> v = ld4x(xf + f);
 #pragma unroll
-        for (int xo = 0; xo < 2; ++xo) {
+        for (int xo = 0; xo < 4; ++xo) {
           T b[3];
 #pragma unroll
           for (int dz = 0; dz < 3; ++dz) b[dz] = T(0.75) * a[dz][1][xo] + T(0.25) * a[dz][yo == 0 ? 0 : 2][xo];
-          v[xo] = T(0.75) * b[1] + T(0.25) * b[zo == 0 ? 0 : 2];
+          v.v[xo] += T(0.75) * b[1] + T(0.25) * b[zo == 0 ? 0 : 2];
         }
-        const int64_t f = (int64_t)(2 * cx) + (int64_t)rf * (2 * cy + yo) + pf * (2 * cz + zo);
-        const V2 x = *reinterpret_cast<const V2*>(xf + f);
-        *reinterpret_cast<V2*>(out + f) = V2{x.x + v[0], x.y + v[1]};
+        st4x(out + f, v);
       }
   }
 }
 
 template <typename T>
-__global__ void k_restrict3(const T* __restrict__ rf, int Lf, T* __restrict__ fc) {
+__global__ void k_restrict4(const T* __restrict__ rf, int Lf, T* __restrict__ fc) {
   typedef typename Vec2<T>::type V2;
-  const int Lc = Lf - 1, res = 1 << Lf;
-  const uint64_t nc = 1ull << (3 * Lc), m = (1ull << Lc) - 1;
-  const int64_t pf = (int64_t)res * res;
+  const int Lc = Lf - 1, res = 1 << Lf, rc = 1 << Lc, hc = rc >> 1;
+  const uint64_t np = 1ull << (3 * Lc - 1);
+  const int64_t pf = (int64_t)res * res, pc = (int64_t)rc * rc;
   const T w[4] = {T(0.25), T(0.75), T(0.75), T(0.25)};
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x) {
-    const int cx = (int)(i & m), cy = (int)((i >> Lc) & m), cz = (int)(i >> (2 * Lc));
-    T acc = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < np; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int cp = (int)(i % hc), cy = (int)((i / hc) % rc), cz = (int)(i / ((uint64_t)hc * rc));
+    T acc0 = 0, acc1 = 0;
 #pragma unroll
     for (int kz = 0; kz < 4; ++kz) {
       const int fz = 2 * cz - 1 + kz;
       if (fz < 0 || fz >= res) continue;
-      T az = 0;
+      T az0 = 0, az1 = 0;
 #pragma unroll
       for (int ky = 0; ky < 4; ++ky) {
         const int fy = 2 * cy - 1 + ky;
         if (fy < 0 || fy >= res) continue;
-        const T* row = rf + fz * pf + (int64_t)fy * res + 2 * cx;
-        const V2 c = *reinterpret_cast<const V2*>(row);
-        T ax = T(0.75) * (c.x + c.y);
-        if (cx > 0) ax += T(0.25) * row[-1];
-        if (2 * cx + 2 < res) ax += T(0.25) * row[2];
-        az += w[ky] * ax;
+        const T* row = rf + fz * pf + (int64_t)fy * res + 4 * cp;
+        const F4<T> c = ld4x(row);
+        const T lo = cp > 0 ? row[-1] : T(0), hi = 4 * cp + 4 < res ? row[4] : T(0);
+        const T ax0 = T(0.25) * (lo + c.v[2]) + T(0.75) * (c.v[0] + c.v[1]);
+        const T ax1 = T(0.25) * (c.v[1] + hi) + T(0.75) * (c.v[2] + c.v[3]);
+        az0 += w[ky] * ax0;
+        az1 += w[ky] * ax1;
       }
-      acc += w[kz] * az;
+      acc0 += w[kz] * az0;
+      acc1 += w[kz] * az1;
     }
-    fc[i] = acc;
+    *reinterpret_cast<V2*>(fc + cz * pc + (int64_t)cy * rc + 2 * cp) = V2{acc0, acc1};
   }
 }
 
@@ -1460,11 +1491,11 @@ struct System2 {
     Level2<T>& qc = lv[li + 1];
     chebyshev(li, f, X, q.y, true);
     op(li, kOpResid, X, f, nullptr, q.y);
-    k_restrict3<T><<<grid_for(qc.n), kThreads, 0, s>>>(q.y, q.L, qc.f);
+    k_restrict4<T><<<grid_for(qc.n / 2), kThreads, 0, s>>>(q.y, q.L, qc.f);
     PR_CHECK_LAUNCH();
     bytes += (double)(q.n + qc.n) * sizeof(T);
     vcycle(li + 1, qc.f, qc.x);
-    k_prolong3<T><<<grid_for(qc.n), kThreads, 0, s>>>(X, qc.x, q.L, q.y);
+    k_prolong4<T><<<grid_for(qc.n / 2), kThreads, 0, s>>>(X, qc.x, q.L, q.y);
     PR_CHECK_LAUNCH();
     bytes += (double)(2 * q.n + qc.n) * sizeof(T);
     chebyshev(li, f, X, q.y, false);
@@ -1773,11 +1804,11 @@ double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
       case 3: sys.op(0, kOpApply, x, nullptr, nullptr, y, 0.0, 0.0, 0); break;
       case 4: sys.op(0, kOpResid, x, f, nullptr, y, 0.0, 0.0, 1); break;
       case 5:
-        k_restrict3<T><<<grid_for(nc), kThreads, 0, s>>>(x, (int)D, ec);
+        k_restrict4<T><<<grid_for(nc / 2), kThreads, 0, s>>>(x, (int)D, ec);
         PR_CHECK_LAUNCH();
         break;
       case 6:
-        k_prolong3<T><<<grid_for(nc), kThreads, 0, s>>>(x, ec, (int)D, y);
+        k_prolong4<T><<<grid_for(nc / 2), kThreads, 0, s>>>(x, ec, (int)D, y);
         PR_CHECK_LAUNCH();
         break;
       case 7:
