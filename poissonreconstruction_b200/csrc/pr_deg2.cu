@@ -377,17 +377,33 @@ __device__ __forceinline__ void edge_tile(int j, int nbx, int nby, int all, int&
   }
 }
 
-// 5-tap filters.  Interior rows are symmetric (c[0] = c[4], c[1] = c[3]): two filters of the
-// same input share the pair sums.
-template <typename T>
-__device__ __forceinline__ void filt2_sym(const T* v, const T* m, const T* s, T& om, T& os) {
-  const T p0 = v[0] + v[4], p1 = v[1] + v[3];
-  om = m[0] * p0 + m[1] * p1 + m[2] * v[2];
-  os = s[0] * p0 + s[1] * p1 + s[2] * v[2];
-}
+// 5-tap filters of the face tiles (general rows).
 template <typename T>
 __device__ __forceinline__ T filt(const T* v, const T* c) {
   return c[0] * v[0] + c[1] * v[1] + c[2] * v[2] + c[3] * v[3] + c[4] * v[4];
+}
+
+// Pair arithmetic for the two x-adjacent outputs of a thread: FP32 pairs use the packed two-wide
+// instructions (one instruction for both lanes), FP64 pairs two scalar operations.
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ double2 p_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 p_mul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 p_fma(double2 a, double2 b, double2 c) {
+  return make_double2(__fma_rn(a.x, b.x, c.x), __fma_rn(a.y, b.y, c.y));
+}
+template <typename V2, typename T>
+__device__ __forceinline__ V2 p_bc(T x) {
+  return V2{x, x};
+}
+// interior rows are symmetric (c[0] = c[4], c[1] = c[3]): om, os = the M and S filters of the taps
+// t0..t4 (pairs), sharing the pair sums
+template <typename V2>
+__device__ __forceinline__ void sym2(V2 t0, V2 t1, V2 t2, V2 t3, V2 t4, const V2* m, const V2* s, V2& om, V2& os) {
+  const V2 q0 = p_add(t0, t4), q1 = p_add(t1, t3);
+  om = p_fma(m[2], t2, p_fma(m[1], q1, p_mul(m[0], q0)));
+  os = p_fma(s[2], t2, p_fma(s[1], q1, p_mul(s[0], q0)));
 }
 
 template <typename T, int MODE, bool EDGE>
@@ -484,11 +500,32 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
       invI[j] = A.invd;
     }
   }
-  T wa[2][NS], wb[2][NS], wc[2][NS];
+  // interior: the symmetric rows as pairs and the epilogue of the interior planes as at most two
+  // pair operations on (acc, centre, f, xp), its coefficients folded here:
+  //   kOpApply   H acc + wg c                           kOpResid  f - H acc - wg c
+  //   kOpCheb    (1 + ca) c - ca xp + cb D^-1 r,  r = f - H acc - wg c
+  //   kOpChebPF  (1 + ca) c - ca c0 D^-1 f + cb D^-1 r
+  //   kOpChebF   x1 = c0 D^-1 c (c = f): (1 + ca) x1 + cb D^-1 (c - H acc - wg x1)
+  V2 pm[3], ps[3];
 #pragma unroll
-  for (int j = 0; j < 2; ++j)
+  for (int d = 0; d < 3; ++d) {
+    pm[d] = p_bc<V2>(A.im[d]);
+    ps[d] = p_bc<V2>(A.is[d]);
+  }
+  const T cbinv = A.cb * A.invd, c0inv = A.c0 * A.invd;
+  T e_acc, e_c, e_f, e_p;  // interior epilogue: res = e_acc acc + e_c c + e_f f + e_p xp (+ cb D^-1 f below)
+  if (MODE == kOpApply) { e_acc = lv.H; e_c = lv.wg; e_f = 0; e_p = 0; }
+  else if (MODE == kOpResid) { e_acc = -lv.H; e_c = -lv.wg; e_f = 1; e_p = 0; }
+  else if (MODE == kOpCheb) { e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv; e_p = -A.ca; }
+  else if (MODE == kOpChebPF) {
+    e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv - A.ca * c0inv; e_p = 0;
+  } else {  // kOpChebF
+    e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) * c0inv + cbinv * (T(1) - lv.wg * c0inv); e_f = 0; e_p = 0;
+  }
+  const V2 pe_acc = p_bc<V2>(e_acc), pe_c = p_bc<V2>(e_c), pe_f = p_bc<V2>(e_f), pe_p = p_bc<V2>(e_p);
+  V2 wa[NS], wb[NS], wc[NS];
 #pragma unroll
-    for (int k = 0; k < NS; ++k) wa[j][k] = wb[j][k] = wc[j][k] = T(0);
+  for (int k = 0; k < NS; ++k) wa[k] = wb[k] = wc[k] = V2{T(0), T(0)};
   T* op = out + (int64_t)gx + (int64_t)res * gy + plane * (z0 - 4);  // output row of plane zo = z0 - 4 + it
   const bool want_dot = A.dot != nullptr;
   double dacc = 0.0;  // A.dot: this thread's share of the product
@@ -526,7 +563,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
             __syncthreads();
           }
         } else if (zin_int) {
-          kz = A.c0 * A.invd;
+          kz = c0inv;
         } else if (zin < 0 || zin >= res) {
           kz = T(0);  // a zero-filled plane
         } else {
@@ -542,30 +579,28 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
           const T* row = &s_x[k][r][2 * p + XOFF];
           const V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
                    v2 = *reinterpret_cast<const V2*>(row + 4);
-          T v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
-          T um0, um1, us0, us1;
+          V2 um, us;
           if (EDGE) {
+            T v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
             if (MODE == kOpChebF) {
               const T* kr = &s_k[r][2 * p + XOFF];
 #pragma unroll
               for (int e = 0; e < 6; ++e) v[e] *= kr[e];
             }
-            um0 = filt(v, cmx[0]);
-            us0 = filt(v, csx[0]);
-            um1 = filt(v + 1, cmx[1]);
-            us1 = filt(v + 1, csx[1]);
+            um = V2{filt(v, cmx[0]), filt(v + 1, cmx[1])};
+            us = V2{filt(v, csx[0]), filt(v + 1, csx[1])};
           } else {
-            filt2_sym(v, A.im, A.is, um0, us0);
-            filt2_sym(v + 1, A.im, A.is, um1, us1);
+            // output 0 taps v0..v4, output 1 taps v1..v5: pairs (v0,v1) (v1,v2) (v2,v3) (v3,v4) (v4,v5)
+            const V2 v12 = V2{v0.y, v1.x}, v34 = V2{v1.y, v2.x};
+            sym2(v0, v12, v1, v34, v2, pm, ps, um, us);
             if (MODE == kOpChebF) {
-              um0 *= kz;
-              us0 *= kz;
-              um1 *= kz;
-              us1 *= kz;
+              const V2 kp = p_bc<V2>(kz);
+              um = p_mul(kp, um);
+              us = p_mul(kp, us);
             }
           }
-          *reinterpret_cast<V2*>(&s_um[b][r][2 * p]) = V2{um0, um1};
-          *reinterpret_cast<V2*>(&s_us[b][r][2 * p]) = V2{us0, us1};
+          *reinterpret_cast<V2*>(&s_um[b][r][2 * p]) = um;
+          *reinterpret_cast<V2*>(&s_us[b][r][2 * p]) = us;
         }
       }
       // centre values: x (f for kOpChebF)
@@ -581,89 +616,109 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
       if (t == 0 && it + NS < nissue) issue(it + NS);
       // y filter into the window slot k
       {
-        T a0[5], a1[5], c0[5], c1[5];
+        V2 a[5], c[5];
 #pragma unroll
         for (int d = 0; d < 5; ++d) {
-          const V2 a = *reinterpret_cast<const V2*>(&s_um[b][ty + d][2 * p]);
-          const V2 c = *reinterpret_cast<const V2*>(&s_us[b][ty + d][2 * p]);
-          a0[d] = a.x;
-          a1[d] = a.y;
-          c0[d] = c.x;
-          c1[d] = c.y;
+          a[d] = *reinterpret_cast<const V2*>(&s_um[b][ty + d][2 * p]);
+          c[d] = *reinterpret_cast<const V2*>(&s_us[b][ty + d][2 * p]);
         }
-        T vmm0, vmm1, vms0, vms1, vsm0, vsm1;
         if (EDGE) {
-          vmm0 = filt(a0, cmy);
-          vms0 = filt(a0, csy);
-          vmm1 = filt(a1, cmy);
-          vms1 = filt(a1, csy);
-          vsm0 = filt(c0, cmy);
-          vsm1 = filt(c1, cmy);
+          T a0[5], a1[5], c0[5], c1[5];
+#pragma unroll
+          for (int d = 0; d < 5; ++d) {
+            a0[d] = a[d].x;
+            a1[d] = a[d].y;
+            c0[d] = c[d].x;
+            c1[d] = c[d].y;
+          }
+          wa[k] = V2{filt(c0, cmy) + filt(a0, csy), filt(c1, cmy) + filt(a1, csy)};
+          wb[k] = V2{filt(a0, cmy), filt(a1, cmy)};
         } else {
-          filt2_sym(a0, A.im, A.is, vmm0, vms0);
-          filt2_sym(a1, A.im, A.is, vmm1, vms1);
-          vsm0 = A.im[0] * (c0[0] + c0[4]) + A.im[1] * (c0[1] + c0[3]) + A.im[2] * c0[2];
-          vsm1 = A.im[0] * (c1[0] + c1[4]) + A.im[1] * (c1[1] + c1[3]) + A.im[2] * c1[2];
+          V2 vmm, vms, vsm, unused;
+          sym2(a[0], a[1], a[2], a[3], a[4], pm, ps, vmm, vms);
+          sym2(c[0], c[1], c[2], c[3], c[4], pm, ps, vsm, unused);
+          wa[k] = p_add(vsm, vms);
+          wb[k] = vmm;
         }
-        wa[0][k] = vsm0 + vms0;
-        wa[1][k] = vsm1 + vms1;
-        wb[0][k] = vmm0;
-        wb[1][k] = vmm1;
       }
-      wc[0][k] = xc.x;
-      wc[1][k] = xc.y;
+      wc[k] = xc;
       const int zo = zin - 2;
       if ((unsigned)(zo - z0) < (unsigned)(z1 - z0)) {
         const bool zint = zo >= A.edge && zo < res - A.edge;
-        T acc[2], inv[2];
-        if (zint) {
-#pragma unroll
-          for (int j = 0; j < 2; ++j) {
-            const T* wA = wa[j];
-            const T* wB = wb[j];
-            acc[j] = A.im[0] * (wA[(k + 1) % NS] + wA[(k + 5) % NS]) + A.im[1] * (wA[(k + 2) % NS] + wA[(k + 4) % NS]) +
-                     A.im[2] * wA[(k + 3) % NS] + A.is[0] * (wB[(k + 1) % NS] + wB[(k + 5) % NS]) +
-                     A.is[1] * (wB[(k + 2) % NS] + wB[(k + 4) % NS]) + A.is[2] * wB[(k + 3) % NS];
-            inv[j] = invI[j];
-          }
+        V2 res2;
+        if (!EDGE && zint) {
+          // the symmetric z filter and the folded epilogue, both lanes at once
+          V2 acc, u;
+          sym2(wa[(k + 1) % NS], wa[(k + 2) % NS], wa[(k + 3) % NS], wa[(k + 4) % NS], wa[(k + 5) % NS], pm, ps, acc, u);
+          V2 um2, us2;
+          sym2(wb[(k + 1) % NS], wb[(k + 2) % NS], wb[(k + 3) % NS], wb[(k + 4) % NS], wb[(k + 5) % NS], pm, ps, um2, us2);
+          acc = p_add(acc, us2);
+          const V2 cc = wc[(k + 3) % NS];
+          res2 = p_fma(pe_c, cc, p_mul(pe_acc, acc));
+          if (MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF) res2 = p_fma(pe_f, fo, res2);
+          if (MODE == kOpCheb) res2 = p_fma(pe_p, po, res2);
         } else {
-          T cz_m[5], cz_s[5];
+          T acc[2], inv[2];
+          if (zint) {
 #pragma unroll
-          for (int d = 0; d < 5; ++d) {
-            cz_m[d] = lv.tM[5 * zo + d];
-            cz_s[d] = lv.tS[5 * zo + d];
+            for (int j = 0; j < 2; ++j) {
+              T wA[NS], wB[NS];
+#pragma unroll
+              for (int q = 0; q < NS; ++q) {
+                wA[q] = j == 0 ? wa[q].x : wa[q].y;
+                wB[q] = j == 0 ? wb[q].x : wb[q].y;
+              }
+              acc[j] = A.im[0] * (wA[(k + 1) % NS] + wA[(k + 5) % NS]) + A.im[1] * (wA[(k + 2) % NS] + wA[(k + 4) % NS]) +
+                       A.im[2] * wA[(k + 3) % NS] + A.is[0] * (wB[(k + 1) % NS] + wB[(k + 5) % NS]) +
+                       A.is[1] * (wB[(k + 2) % NS] + wB[(k + 4) % NS]) + A.is[2] * wB[(k + 3) % NS];
+              inv[j] = invI[j];
+            }
+          } else {
+            T cz_m[5], cz_s[5];
+#pragma unroll
+            for (int d = 0; d < 5; ++d) {
+              cz_m[d] = lv.tM[5 * zo + d];
+              cz_s[d] = lv.tS[5 * zo + d];
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              T sacc = 0;
+#pragma unroll
+              for (int d = 0; d < 5; ++d) {
+                const T wA = j == 0 ? wa[(k + 1 + d) % NS].x : wa[(k + 1 + d) % NS].y;
+                const T wB = j == 0 ? wb[(k + 1 + d) % NS].x : wb[(k + 1 + d) % NS].y;
+                sacc += cz_m[d] * wA + cz_s[d] * wB;
+              }
+              acc[j] = sacc;
+              inv[j] = T(1) / (lv.H * (dA[j] * cz_m[2] + dC[j] * cz_s[2]) + lv.wg);
+            }
           }
+          T rr2[2];
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
-            T sacc = 0;
-#pragma unroll
-            for (int d = 0; d < 5; ++d) sacc += cz_m[d] * wa[j][(k + 1 + d) % NS] + cz_s[d] * wb[j][(k + 1 + d) % NS];
-            acc[j] = sacc;
-            inv[j] = T(1) / (lv.H * (dA[j] * cz_m[2] + dC[j] * cz_s[2]) + lv.wg);
+            const T fj = j == 0 ? fo.x : fo.y;
+            const T pj = j == 0 ? po.x : po.y;
+            const T cj = j == 0 ? wc[(k + 3) % NS].x : wc[(k + 3) % NS].y;  // the centre (f for kOpChebF)
+            if (MODE == kOpChebF) {
+              const T x1 = A.c0 * inv[j] * cj;
+              const T ax = lv.H * acc[j] + lv.wg * x1;
+              rr2[j] = (T(1) + A.ca) * x1 + A.cb * (cj - ax) * inv[j];
+            } else {
+              const T ax = lv.H * acc[j] + lv.wg * cj;
+              if (MODE == kOpApply) rr2[j] = ax;
+              else if (MODE == kOpResid) rr2[j] = fj - ax;
+              else if (MODE == kOpCheb) rr2[j] = cj + A.ca * (cj - pj) + A.cb * (fj - ax) * inv[j];
+              else rr2[j] = cj + A.ca * (cj - A.c0 * inv[j] * fj) + A.cb * (fj - ax) * inv[j];  // kOpChebPF
+            }
           }
+          res2 = V2{rr2[0], rr2[1]};
         }
-        T res2[2];
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const T fj = j == 0 ? fo.x : fo.y;
-          const T pj = j == 0 ? po.x : po.y;
-          const T cj = wc[j][(k + 3) % NS];  // the output plane's centre (f for kOpChebF)
-          if (MODE == kOpChebF) {
-            const T x1 = A.c0 * inv[j] * cj;
-            const T ax = lv.H * acc[j] + lv.wg * x1;
-            res2[j] = (T(1) + A.ca) * x1 + A.cb * (cj - ax) * inv[j];
-          } else {
-            const T ax = lv.H * acc[j] + lv.wg * cj;
-            if (MODE == kOpApply) res2[j] = ax;
-            else if (MODE == kOpResid) res2[j] = fj - ax;
-            else if (MODE == kOpCheb) res2[j] = cj + A.ca * (cj - pj) + A.cb * (fj - ax) * inv[j];
-            else res2[j] = cj + A.ca * (cj - A.c0 * inv[j] * fj) + A.cb * (fj - ax) * inv[j];  // kOpChebPF
-          }
+        *reinterpret_cast<V2*>(op) = res2;
+        if (MODE == kOpApply && want_dot) {
+          const V2 cc = wc[(k + 3) % NS];
+          dacc += (double)cc.x * (double)res2.x + (double)cc.y * (double)res2.y;
         }
-        *reinterpret_cast<V2*>(op) = V2{res2[0], res2[1]};
-        if (MODE == kOpApply && want_dot)
-          dacc += (double)wc[0][(k + 3) % NS] * (double)res2[0] + (double)wc[1][(k + 3) % NS] * (double)res2[1];
-        if (MODE == kOpCheb && want_dot) dacc += (double)fo.x * (double)res2[0] + (double)fo.y * (double)res2[1];
+        if (MODE == kOpCheb && want_dot) dacc += (double)fo.x * (double)res2.x + (double)fo.y * (double)res2.y;
       }
       op += plane;
     }
