@@ -343,7 +343,10 @@ struct Vec2<double> {
 //            then the second); the staged input is f.
 // kOpChebPF: out = x + ca (x - xp) + cb D^-1 (f - A x) with xp = c0 D^-1 f (the third step after
 //            kOpChebF: its previous iterate is recomputed from f).
-enum { kOpChebF = 3, kOpChebPF = 4 };
+// kOpApplyD: the preconditioned CG direction update fused into the operator pass (second staged
+//            plane z): d = z + s1 dold (staged: dold, z), out = A d, out2 = d, xacc += s2 dold,
+//            dot d . out
+enum { kOpChebF = 3, kOpChebPF = 4, kOpApplyD = 5 };
 
 template <typename T>
 struct Op3Args {
@@ -357,8 +360,11 @@ struct Op3Args {
   int all;         // EDGE: the grid enumerates every tile, not only the face tiles
   int ox, oy;      // interior: tile of block (i, j) is (i + ox, j + oy)
   int* err;
-  double* dot;     // optional per-CTA partials: kOpApply x . out, kOpCheb f . out
+  double* dot;     // optional per-CTA partials: kOpApply x . out, kOpCheb f . out, kOpApplyD d . out
   int dot_base;    // index of this launch's first partial
+  T s1, s2;        // kOpApplyD: beta, alpha of the previous step
+  T* out2;         // kOpApplyD: d
+  T* xacc;         // kOpApplyD: the CG iterate
 };
 
 // the (x, y) tile of an EDGE CTA: the first and the last tile row, then the first and the last
@@ -441,8 +447,10 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
   const int nplanes = z1 - z0 + 4;
   const int ngroups = (nplanes + NS - 1) / NS;  // planes past z1 + 1 read zeros and emit nothing
   constexpr bool use_f = MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF;
+  constexpr bool two = MODE == kOpApplyD;  // second haloed plane, staged in the f/p space
   const bool use_p = MODE == kOpCheb && A.use_p;
-  const uint32_t bytes = G::XBYTES + (use_f ? G::OBYTES : 0u) + (use_p ? G::OBYTES : 0u);
+  const uint32_t bytes = G::XBYTES + (use_f ? G::OBYTES : 0u) + (use_p ? G::OBYTES : 0u) + (two ? G::XBYTES : 0u);
+  T(*s_z)[SH][BW] = reinterpret_cast<T(*)[SH][BW]>(smem + G::OFF_F);
   if (t == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
     *s_abort = 0;
@@ -469,6 +477,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
     tma_load_3d(&s_x[s][0][0], &mx, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
     if (use_f) tma_load_3d(&s_f[s][0][0], &mf, x0, y0, zin - 2, &bar[s]);
     if (use_p) tma_load_3d(&s_p[s][0][0], &mp, x0, y0, zin - 2, &bar[s]);
+    if (two) tma_load_3d(&s_z[s][0][0], &mf, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
   };
   const int nissue = ngroups * NS;
   if (t == 0)
@@ -514,7 +523,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
   }
   const T cbinv = A.cb * A.invd, c0inv = A.c0 * A.invd;
   T e_acc, e_c, e_f, e_p;  // interior epilogue: res = e_acc acc + e_c c + e_f f + e_p xp (+ cb D^-1 f below)
-  if (MODE == kOpApply) { e_acc = lv.H; e_c = lv.wg; e_f = 0; e_p = 0; }
+  if (MODE == kOpApply || MODE == kOpApplyD) { e_acc = lv.H; e_c = lv.wg; e_f = 0; e_p = 0; }
   else if (MODE == kOpResid) { e_acc = -lv.H; e_c = -lv.wg; e_f = 1; e_p = 0; }
   else if (MODE == kOpCheb) { e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv; e_p = -A.ca; }
   else if (MODE == kOpChebPF) {
@@ -523,9 +532,10 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
     e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) * c0inv + cbinv * (T(1) - lv.wg * c0inv); e_f = 0; e_p = 0;
   }
   const V2 pe_acc = p_bc<V2>(e_acc), pe_c = p_bc<V2>(e_c), pe_f = p_bc<V2>(e_f), pe_p = p_bc<V2>(e_p);
-  V2 wa[NS], wb[NS], wc[NS];
+  V2 wa[NS], wb[NS], wc[NS], wo[NS];  // wo: kOpApplyD, the centres of dold
 #pragma unroll
-  for (int k = 0; k < NS; ++k) wa[k] = wb[k] = wc[k] = V2{T(0), T(0)};
+  for (int k = 0; k < NS; ++k) wa[k] = wb[k] = wc[k] = wo[k] = V2{T(0), T(0)};
+  const V2 pbeta = p_bc<V2>(A.s1);
   T* op = out + (int64_t)gx + (int64_t)res * gy + plane * (z0 - 4);  // output row of plane zo = z0 - 4 + it
   const bool want_dot = A.dot != nullptr;
   double dacc = 0.0;  // A.dot: this thread's share of the product
@@ -537,6 +547,9 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
       it = g * NS + k;
+      // kOpApplyD: the iterate of this step's output plane, loaded before the wait
+      V2 xold = V2{T(0), T(0)};
+      if (two && (unsigned)(it - 4) < (unsigned)(z1 - z0)) xold = *reinterpret_cast<const V2*>(A.xacc + (op - out));
       if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
         atomicExch(A.err, 1);
         *s_abort = 1;
@@ -577,8 +590,14 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
         const int r = ty + 8 * q;
         if (r < SH) {
           const T* row = &s_x[k][r][2 * p + XOFF];
-          const V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
-                   v2 = *reinterpret_cast<const V2*>(row + 4);
+          V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
+             v2 = *reinterpret_cast<const V2*>(row + 4);
+          if (two) {  // d = z + beta dold
+            const T* zr = &s_z[k][r][2 * p + XOFF];
+            v0 = p_fma(pbeta, v0, *reinterpret_cast<const V2*>(zr));
+            v1 = p_fma(pbeta, v1, *reinterpret_cast<const V2*>(zr + 2));
+            v2 = p_fma(pbeta, v2, *reinterpret_cast<const V2*>(zr + 4));
+          }
           V2 um, us;
           if (EDGE) {
             T v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
@@ -603,8 +622,12 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
           *reinterpret_cast<V2*>(&s_us[b][r][2 * p]) = us;
         }
       }
-      // centre values: x (f for kOpChebF)
-      const V2 xc = *reinterpret_cast<const V2*>(&s_x[k][ty + 2][2 * p + 2 + XOFF]);
+      // centre values: x (f for kOpChebF; d = z + beta dold for kOpApplyD)
+      V2 xc = *reinterpret_cast<const V2*>(&s_x[k][ty + 2][2 * p + 2 + XOFF]);
+      if (two) {
+        wo[k] = xc;
+        xc = p_fma(pbeta, xc, *reinterpret_cast<const V2*>(&s_z[k][ty + 2][2 * p + 2 + XOFF]));
+      }
       V2 fo = V2{T(0), T(0)}, po = V2{T(0), T(0)};
       if (use_f) fo = *reinterpret_cast<const V2*>(&s_f[k][ty][2 * p]);
       if (use_p) po = *reinterpret_cast<const V2*>(&s_p[k][ty][2 * p]);
@@ -705,7 +728,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
               rr2[j] = (T(1) + A.ca) * x1 + A.cb * (cj - ax) * inv[j];
             } else {
               const T ax = lv.H * acc[j] + lv.wg * cj;
-              if (MODE == kOpApply) rr2[j] = ax;
+              if (MODE == kOpApply || MODE == kOpApplyD) rr2[j] = ax;
               else if (MODE == kOpResid) rr2[j] = fj - ax;
               else if (MODE == kOpCheb) rr2[j] = cj + A.ca * (cj - pj) + A.cb * (fj - ax) * inv[j];
               else rr2[j] = cj + A.ca * (cj - A.c0 * inv[j] * fj) + A.cb * (fj - ax) * inv[j];  // kOpChebPF
@@ -714,7 +737,11 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
           res2 = V2{rr2[0], rr2[1]};
         }
         *reinterpret_cast<V2*>(op) = res2;
-        if (MODE == kOpApply && want_dot) {
+        if (two) {
+          *reinterpret_cast<V2*>(A.out2 + (op - out)) = wc[(k + 3) % NS];
+          *reinterpret_cast<V2*>(A.xacc + (op - out)) = p_fma(p_bc<V2>(A.s2), wo[(k + 3) % NS], xold);
+        }
+        if ((MODE == kOpApply || MODE == kOpApplyD) && want_dot) {
           const V2 cc = wc[(k + 3) % NS];
           dacc += (double)cc.x * (double)res2.x + (double)cc.y * (double)res2.y;
         }
@@ -728,7 +755,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
     // stopped early: let the loads still in flight land before the CTA's shared memory goes
     for (int q = it; q < min(it + NS, nissue); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
   }
-  if ((MODE == kOpApply || MODE == kOpCheb) && A.dot != nullptr) {
+  if ((MODE == kOpApply || MODE == kOpCheb || MODE == kOpApplyD) && A.dot != nullptr) {
     typedef cub::BlockReduce<double, kThreads> BR;
     __shared__ typename BR::TempStorage tmp;
     const double tot = BR(tmp).Sum(dacc);
@@ -1430,8 +1457,14 @@ struct System2 {
 
   // One operator pass on level li (modes k_op2 / k_op3); c0 is the first Chebyshev coefficient of
   // the fused modes.  tma < 0: k_op3 on levels with res >= 64, k_op2 below.
+  // the fused CG direction update (kOpApplyD): f is the second staged plane (z)
+  struct Fuse {
+    T* out2 = nullptr;
+    T* xacc = nullptr;
+    double s1 = 0.0, s2 = 0.0;
+  };
   int op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0,
-         int tma = -1, double c0 = 0.0, double* dot = nullptr) {
+         int tma = -1, double c0 = 0.0, double* dot = nullptr, const Fuse* fu = nullptr) {
     int nparts = 0;
     const Level2<T>& q = lv[li];
     const int res = 1 << q.L;
@@ -1458,16 +1491,23 @@ struct System2 {
       A.err = err;
       A.dot = dot;
       A.dot_base = 0;
+      const bool two = mode == kOpApplyD;
+      PR_REQUIRE(!two || (fu && fu->out2 && fu->xacc && f), PR_ERR_INTERNAL, "fused CG pass without its operands");
+      A.s1 = two ? (T)fu->s1 : T(0);
+      A.s2 = two ? (T)fu->s2 : T(0);
+      A.out2 = two ? fu->out2 : nullptr;
+      A.xacc = two ? fu->xacc : nullptr;
       const int nz = (res + kZChunk3 - 1) / kZChunk3;
       const CUtensorMap mx = plane_map<T>(x, q.L, G::BW, SH);
-      const CUtensorMap mf = f ? plane_map<T>(f, q.L, G::TXP, TY) : mx;
+      const CUtensorMap mf = f ? (two ? plane_map<T>(f, q.L, G::BW, SH) : plane_map<T>(f, q.L, G::TXP, TY)) : mx;
       const CUtensorMap mp = xp ? plane_map<T>(xp, q.L, G::TXP, TY) : mx;
       switch (mode) {
         case kOpApply: nparts = launch_op3<T, kOpApply>(s, mx, mf, mp, out, A, nz); break;
         case kOpResid: nparts = launch_op3<T, kOpResid>(s, mx, mf, mp, out, A, nz); break;
         case kOpCheb: nparts = launch_op3<T, kOpCheb>(s, mx, mf, mp, out, A, nz); break;
         case kOpChebF: nparts = launch_op3<T, kOpChebF>(s, mx, mf, mp, out, A, nz); break;
-        default: nparts = launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
+        case kOpChebPF: nparts = launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
+        default: nparts = launch_op3<T, kOpApplyD>(s, mx, mf, mp, out, A, nz); break;
       }
     } else {
       PR_REQUIRE(mode <= kOpCheb, PR_ERR_INTERNAL, "fused Chebyshev modes need the TMA operator");
@@ -1478,8 +1518,9 @@ struct System2 {
       else k_op2<T, kOpCheb><<<grid, kThreads, 0, s>>>(x, f, xp, out, v, (T)a, (T)b);
       PR_CHECK_LAUNCH();
     }
-    const int reads = mode == kOpApply || mode == kOpChebF ? 1 : (mode == kOpCheb && xp ? 3 : 2);
-    bytes += (double)q.n * sizeof(T) * (reads + 1);
+    // vectors moved (reads + writes)
+    const int vecs = mode == kOpApplyD ? 6 : (mode == kOpApply || mode == kOpChebF ? 2 : (mode == kOpCheb && xp ? 4 : 3));
+    bytes += (double)q.n * sizeof(T) * vecs;
     return nparts;
   }
 
@@ -1557,8 +1598,12 @@ struct System2 {
   }
 };
 
-// preconditioned CG on the finest level from x = 0 to ||r|| <= tol_abs; r holds b on entry and
-// is overwritten with the recursively updated residual
+// preconditioned CG on the finest level from x = 0 to ||r|| <= tol_abs; r holds b on entry and is
+// overwritten with the recursively updated residual.  On the TMA operator (res >= 64) the vector
+// updates ride on passes that read the vectors anyway: d = z + beta d, q = A d, d . q and
+// x += alpha d (of the previous step) in the operator pass, r . z in the V-cycle's last smoothing
+// step; r -= alpha q with r . r is its own pass, so that convergence is known before the next
+// V-cycle.
 template <typename T>
 int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) {
   const uint64_t n = sys.lv[0].n;
@@ -1568,51 +1613,80 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
   T* d = c->buf<T>("d2cg_d_" + tn, n);
   T* q = c->buf<T>("d2cg_q_" + tn, n);
   const bool fused = sys.fused_dots();
-  if (fused) sys.alloc_parts();
   PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
   double rr = dot<T>(c, r, r, n);
   sys.bytes += 2.0 * n * sizeof(T);
   if (!(std::sqrt(rr) > tol_abs)) return 0;
-  // z = M r and r . z (fused: the last post-smoothing step of the finest level)
-  auto precondition = [&]() {
-    if (fused) {
-      sys.rz_parts = sys.parts_a;
-      sys.rz_np = 0;
-      sys.vcycle(0, r, z);
-      sys.rz_parts = nullptr;
-      PR_REQUIRE(sys.rz_np > 0, PR_ERR_INTERNAL, "fused r.z was not produced");
-      return sys.sum_parts(sys.rz_np, 0, 0.0);
-    }
-    sys.vcycle(0, r, z);
-    sys.bytes += 2.0 * n * sizeof(T);
-    return dot<T>(c, r, z, n);
-  };
-  double rz = precondition();
-  PR_CUDA(cudaMemcpyAsync(d, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
-  sys.bytes += 2.0 * n * sizeof(T);
   int it = 0;
-  while (it < maxit) {
-    double dq;
-    if (fused) {
-      const int na = sys.op(0, kOpApply, d, nullptr, nullptr, q, 0.0, 0.0, -1, 0.0, sys.parts_a);
-      const int nb = sys.screen(d, q, +1, sys.parts_b);
-      dq = sys.sum_parts(na, nb, sys.scr.wh3);
-    } else {
+  if (!fused) {
+    sys.vcycle(0, r, z);
+    double rz = dot<T>(c, r, z, n);
+    PR_CUDA(cudaMemcpyAsync(d, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    sys.bytes += 4.0 * n * sizeof(T);
+    while (it < maxit) {
       sys.op(0, kOpApply, d, nullptr, nullptr, q);
       sys.screen(d, q, +1);
-      dq = dot<T>(c, d, q, n);
+      const double dq = dot<T>(c, d, q, n);
       sys.bytes += 2.0 * n * sizeof(T);
+      if (!(dq > 0.0) || !(rz > 0.0)) break;
+      const double alpha = rz / dq;
+      rr = cg_update<T>(c, n, alpha, d, q, x, r);
+      sys.bytes += 6.0 * n * sizeof(T);
+      ++it;
+      if (!std::isfinite(rr) || std::sqrt(rr) <= tol_abs) break;
+      sys.vcycle(0, r, z);
+      const double rz_new = dot<T>(c, r, z, n);
+      const double beta = rz_new / rz;
+      rz = rz_new;
+      xpby<T>(s, n, z, beta, d);
+      sys.bytes += 5.0 * n * sizeof(T);
     }
+    return it;
+  }
+  sys.alloc_parts();
+  T* d2 = c->buf<T>("d2cg_d2_" + tn, n);
+  T* dcur = d;
+  T* dalt = d2;
+  const T* dprev = nullptr;
+  // z = M r, r . z
+  auto precondition = [&]() {
+    sys.rz_parts = sys.parts_a;
+    sys.rz_np = 0;
+    sys.vcycle(0, r, z);
+    sys.rz_parts = nullptr;
+    PR_REQUIRE(sys.rz_np > 0, PR_ERR_INTERNAL, "fused r.z was not produced");
+    return sys.sum_parts(sys.rz_np, 0, 0.0);
+  };
+  double rz = precondition();
+  double alpha = 0.0, alpha_prev = 0.0, beta = 0.0;
+  bool pending = false;  // x += alpha dcur not applied yet
+  while (it < maxit) {
+    // d = z + beta dprev (d = z at first), q = A d (+ screening), d . q, x += alpha_prev dprev
+    typename System2<T>::Fuse fu;
+    fu.out2 = dcur;
+    fu.xacc = x;
+    fu.s1 = dprev ? beta : 0.0;
+    fu.s2 = dprev ? alpha_prev : 0.0;
+    const int na = sys.op(0, kOpApplyD, dprev ? dprev : z, z, nullptr, q, 0.0, 0.0, -1, 0.0, sys.parts_a, &fu);
+    pending = false;
+    const int nb = sys.screen(dcur, q, +1, sys.parts_b);
+    const double dq = sys.sum_parts(na, nb, sys.scr.wh3);
     if (!(dq > 0.0) || !(rz > 0.0)) break;
-    const double alpha = rz / dq;
-    rr = cg_update<T>(c, n, alpha, d, q, x, r);
-    sys.bytes += 6.0 * n * sizeof(T);
+    alpha = rz / dq;
+    pending = true;
     ++it;
+    rr = r_update<T>(c, n, alpha, q, r);
+    sys.bytes += 3.0 * n * sizeof(T);
     if (!std::isfinite(rr) || std::sqrt(rr) <= tol_abs) break;
     const double rz_new = precondition();
-    const double beta = rz_new / rz;
+    beta = rz_new / rz;
     rz = rz_new;
-    xpby<T>(s, n, z, beta, d);
+    alpha_prev = alpha;
+    dprev = dcur;
+    std::swap(dcur, dalt);
+  }
+  if (pending) {
+    axpy<T, T>(s, n, alpha, dcur, x);
     sys.bytes += 3.0 * n * sizeof(T);
   }
   return it;

@@ -178,6 +178,33 @@ __global__ void k_cg_update4(uint64_t n, T alpha, const T* __restrict__ d, const
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
+// r -= alpha q with per-block sums of r^2 (the CG residual update when x is updated elsewhere)
+template <typename T>
+__global__ void k_r_update4(uint64_t n, T alpha, const T* __restrict__ q, T* __restrict__ r,
+                            double* __restrict__ part) {
+  double s = 0.0;
+  const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const Q4<T> qv = ld4(q, i);
+    Q4<T> rv = ld4(r, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      rv.v[k] = rv.v[k] - alpha * qv.v[k];
+      s += (double)rv.v[k] * (double)rv.v[k];
+    }
+    st4(r, i, rv);
+  }
+  for (uint64_t i = 4 * n4 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const T ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    s += (double)ri * (double)ri;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double t = BR(tmp).Sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 template <typename T>
 __global__ void k_xpby4(uint64_t n, const T* __restrict__ z, T beta, T* __restrict__ d) {
   const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
@@ -489,6 +516,20 @@ double cg_update(pr_context* c, uint64_t n, double alpha, const T* d, const T* q
   return c->h_scalars[0];
 }
 
+template <typename T>
+double r_update(pr_context* c, uint64_t n, double alpha, const T* q, T* r) {
+  PR_REQUIRE(aligned16(q) && aligned16(r), PR_ERR_INTERNAL, "r_update needs 16-byte aligned vectors");
+  double* part = c->buf<double>("dot_part", kDotBlocks);
+  double* out = c->buf<double>("dot_out", 1);
+  k_r_update4<T><<<kDotBlocks, kThreads, 0, c->stream>>>(n, (T)alpha, q, r, part);
+  PR_CHECK_LAUNCH();
+  k_sum_final<<<1, 32, 0, c->stream>>>(part, kDotBlocks, out);
+  PR_CHECK_LAUNCH();
+  PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  c->sync();
+  return c->h_scalars[0];
+}
+
 double convert_norm(pr_context* c, const double* x, float* y, uint64_t n) {
   double* part = c->buf<double>("dot_part", kDotBlocks);
   double* out = c->buf<double>("dot_out", 1);
@@ -566,6 +607,7 @@ void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e) {
   template void screen_gather<T>(cudaStream_t, const Screen<T>&, T*, int);                            \
   template double dot<T>(pr_context*, const T*, const T*, uint64_t);                                  \
   template double cg_update<T>(pr_context*, uint64_t, double, const T*, const T*, T*, T*);            \
+  template double r_update<T>(pr_context*, uint64_t, double, const T*, T*);                           \
   template void xpby<T>(cudaStream_t, uint64_t, const T*, double, T*);                                \
   template void gs_sweep<T>(cudaStream_t, uint32_t, T*, const T*, Coef<T>, bool);                     \
   template void restrict_to_coarse<T>(cudaStream_t, uint32_t, const T*, T*);                          \
@@ -578,6 +620,7 @@ template void scale_convert<double, float>(cudaStream_t, uint64_t, double, const
 template void scale_convert<float, double>(cudaStream_t, uint64_t, double, const float*, double*);
 template void scale_convert<double, double>(cudaStream_t, uint64_t, double, const double*, double*);
 template void axpy<float, double>(cudaStream_t, uint64_t, double, const float*, double*);
+template void axpy<float, float>(cudaStream_t, uint64_t, double, const float*, float*);
 template void axpy<double, double>(cudaStream_t, uint64_t, double, const double*, double*);
 
 double dot64(pr_context* c, const double* a, const double* b, uint64_t n) { return dot<double>(c, a, b, n); }

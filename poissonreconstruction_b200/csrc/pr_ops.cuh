@@ -57,6 +57,9 @@ double dot(pr_context* c, const T* a, const T* b, uint64_t n);
 // x += alpha d ; r -= alpha q ; returns r.r (host)
 template <typename T>
 double cg_update(pr_context* c, uint64_t n, double alpha, const T* d, const T* q, T* x, T* r);
+// r -= alpha q ; returns r.r (host)
+template <typename T>
+double r_update(pr_context* c, uint64_t n, double alpha, const T* q, T* r);
 // d = z + beta d
 template <typename T>
 void xpby(cudaStream_t s, uint64_t n, const T* z, double beta, T* d);
