@@ -43,7 +43,6 @@ struct Geo {
   static constexpr int C = TB / 2;                  // colour lattice width
   static constexpr int C3 = C * C * C;
   static constexpr int LOGC = TB == 16 ? 3 : 2;
-  static constexpr int LT = TB == 16 ? 4 : 3;
   static constexpr int THREADS = C3;                // one node per colour per thread
   static constexpr int HALO = W * W * W - N;
 };
@@ -66,7 +65,7 @@ __device__ __forceinline__ int ps_index(int ux, int uy, int uz) {
 // h-th position of the one-node halo shell of a (TB+2)^3 tile: 6 faces, 12 edges, 8 corners
 template <int TB>
 __device__ __forceinline__ void halo_u(int h, int& ux, int& uy, int& uz) {
-  constexpr int W = TB + 2, F = TB * TB, LT = Geo<TB>::LT;
+  constexpr int W = TB + 2, F = TB * TB, LT = TB == 16 ? 4 : 3;  // log2 TB
   if (h < 6 * F) {
     const int f = h >> (2 * LT), a = (h & (F - 1)) & (TB - 1), b = (h & (F - 1)) >> LT;
     const int axis = f >> 1, side = (f & 1) ? W - 1 : 0;
@@ -491,30 +490,15 @@ __global__ void __launch_bounds__(1024) k_sum_parts(const double* __restrict__ p
   if (threadIdx.x == 0) out[0] = a + scale2 * b;
 }
 
-// ------------------------------------------------------------------ 16^3 smoother (levels >= 4)
-// 256 threads.  Tile: parity-split, sub-tile = 9 planes x 100 (9 rows of 9), so that the
-// 32 lanes of a warp (8 x-lattice positions x 4 z-pairs) hit 32 distinct banks.
+// ------------------------------------------------------------------ helpers of the 16^3 block kernels
 namespace s16 {
-constexpr int TB = 16, N = 4096, THREADS = 256;
-constexpr int RS = 9, PS = 100, SUB = 9 * PS;  // row / plane / sub-tile strides
-constexpr int TILE = 8 * SUB;
-constexpr int CW = 10;                         // coarse tile width
+constexpr int THREADS = 256;
+constexpr int CW = 10;  // coarse tile width
 
-__device__ __forceinline__ int ps(int ux, int uy, int uz) {
-  return ((ux & 1) | ((uy & 1) << 1) | ((uz & 1) << 2)) * SUB + (uz >> 1) * PS + (uy >> 1) * RS + (ux >> 1);
-}
 // spread the 4 low bits of v to bit positions 0,3,6,9
 __device__ __forceinline__ uint32_t sp4(uint32_t v) {
   return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
 }
-// colour-major f layout: thread (li, kp, lj) of colour col reads lk = 2kp + s at
-// ((col*8 + lj)*2 + s)*32 + 8*kp + li  (conflict-free for the lane pattern)
-__device__ __forceinline__ int fidx(int lx, int ly, int lz) {
-  const int col = (lx & 1) | ((ly & 1) << 1) | ((lz & 1) << 2);
-  const int li = lx >> 1, lj = ly >> 1, lk = lz >> 1;
-  return ((col * 8 + lj) * 2 + (lk & 1)) * 32 + 8 * (lk >> 1) + li;
-}
-
 template <typename T>
 struct Vec4;
 template <>
