@@ -764,6 +764,194 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
   }
 }
 
+// A level whose every row is the interior row (edge 0: the finest level) with the y and z filters
+// in registers: 4 warps on the same 64 x 8 tile and stages as k_op3, each thread two output rows.
+// A thread runs the x filter of its six staged rows straight from the TMA stage (no shared
+// intermediate, one barrier per plane), the y filter on registers, and scatters each input plane
+// into the five output planes it touches (zin - 2 .. zin + 2, register accumulators rotating with
+// the stage index). Planes outside the grid are zero-filled and never emitted, so every tap uses
+// the interior coefficients and the body has no boundary path (its size bounds the instruction
+// cache). Same modes, epilogues and per-CTA dot partials as k_op3<T, MODE, false> at edge 0; for
+// kOpChebF the scale x1 = c0 D^-1 f is one constant there and folds into the epilogue.
+constexpr int kThreadsR = 128;
+template <typename T>
+struct Geo3R {
+  typedef Geo3<T> G;
+  static constexpr size_t OFF_BAR = G::OFF_P + (size_t)G::NS * G::OBYTES;
+  static constexpr size_t BYTES = OFF_BAR + G::NS * 8 + 16;
+};
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUtensorMap mx,
+                                                    const __grid_constant__ CUtensorMap mf,
+                                                    const __grid_constant__ CUtensorMap mp, T* out,
+                                                    const __grid_constant__ Op3Args<T> A) {
+  typedef Geo3<T> G;
+  typedef typename Vec2<T>::type V2;
+  constexpr int NS = G::NS, BW = G::BW, XOFF = G::XOFF, TXP = G::TXP, RY = 2;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T(*s_x)[SH][BW] = reinterpret_cast<T(*)[SH][BW]>(smem + G::OFF_X);
+  T(*s_f)[TY][TXP] = reinterpret_cast<T(*)[TY][TXP]>(smem + G::OFF_F);
+  T(*s_p)[TY][TXP] = reinterpret_cast<T(*)[TY][TXP]>(smem + G::OFF_P);
+  T(*s_z)[SH][BW] = reinterpret_cast<T(*)[SH][BW]>(smem + G::OFF_F);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + Geo3R<T>::OFF_BAR);
+  int* s_abort = reinterpret_cast<int*>(smem + Geo3R<T>::OFF_BAR + NS * 8);
+  const LevelView<T>& lv = A.lv;
+  const int res = 1 << lv.L;
+  const int64_t plane = (int64_t)res * res;
+  const int t = threadIdx.x, p = t & 31, ry = RY * (t >> 5);  // tile rows ry, ry + 1; staged ry .. ry + 5
+  const int x0 = blockIdx.x * TXP, y0 = blockIdx.y * TY;
+  const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
+  const int gx = x0 + 2 * p;
+  const int nplanes = z1 - z0 + 4;
+  const int ngroups = (nplanes + NS - 1) / NS;
+  constexpr bool use_f = MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF;
+  constexpr bool two = MODE == kOpApplyD;
+  const bool use_p = MODE == kOpCheb && A.use_p;
+  const uint32_t bytes = G::XBYTES + (use_f ? G::OBYTES : 0u) + (use_p ? G::OBYTES : 0u) + (two ? G::XBYTES : 0u);
+  if (t == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int it) {
+    const int s = it % NS, zin = z0 - 2 + it;
+    mbar_expect_tx(&bar[s], bytes);
+    tma_load_3d(&s_x[s][0][0], &mx, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
+    if (use_f) tma_load_3d(&s_f[s][0][0], &mf, x0, y0, zin - 2, &bar[s]);
+    if (use_p) tma_load_3d(&s_p[s][0][0], &mp, x0, y0, zin - 2, &bar[s]);
+    if (two) tma_load_3d(&s_z[s][0][0], &mf, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
+  };
+  const int nissue = ngroups * NS;
+  if (t == 0)
+    for (int it = 0; it < NS; ++it) issue(it);
+  V2 pm[3], ps[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    pm[d] = p_bc<V2>(A.im[d]);
+    ps[d] = p_bc<V2>(A.is[d]);
+  }
+  const T cbinv = A.cb * A.invd, c0inv = A.c0 * A.invd;
+  T e_acc, e_c, e_f, e_p;  // interior epilogue, as in k_op3
+  if (MODE == kOpApply || MODE == kOpApplyD) { e_acc = lv.H; e_c = lv.wg; e_f = 0; e_p = 0; }
+  else if (MODE == kOpResid) { e_acc = -lv.H; e_c = -lv.wg; e_f = 1; e_p = 0; }
+  else if (MODE == kOpCheb) { e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv; e_p = -A.ca; }
+  else if (MODE == kOpChebPF) {
+    e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv - A.ca * c0inv; e_p = 0;
+  } else {  // kOpChebF: acc filters f, x1 = c0inv f
+    e_acc = -cbinv * lv.H * c0inv; e_c = (T(1) + A.ca) * c0inv + cbinv * (T(1) - lv.wg * c0inv); e_f = 0; e_p = 0;
+  }
+  const V2 pe_acc = p_bc<V2>(e_acc), pe_c = p_bc<V2>(e_c), pe_f = p_bc<V2>(e_f), pe_p = p_bc<V2>(e_p);
+  // acc[j][s]: the output plane of slot s (zo = z0 - 4 + it for it = s mod NS) of row j, partial;
+  // wc, wo: centres of the staged planes (d, and dold for kOpApplyD) by stage
+  V2 acc[RY][NS], wc[RY][NS], wo[RY][NS];
+#pragma unroll
+  for (int j = 0; j < RY; ++j)
+#pragma unroll
+    for (int k = 0; k < NS; ++k) acc[j][k] = wc[j][k] = wo[j][k] = V2{T(0), T(0)};
+  const V2 pbeta = p_bc<V2>(A.s1);
+  T* op = out + (int64_t)gx + (int64_t)res * (y0 + ry) + plane * (z0 - 4);  // row ry of plane z0 - 4 + it
+  const bool want_dot = A.dot != nullptr;
+  double dacc = 0.0;
+  int it = 0;
+  bool stop = false;
+  for (int g = 0; g < ngroups; ++g) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      it = g * NS + k;
+      const bool emit = (unsigned)(it - 4) < (unsigned)(z1 - z0);
+      V2 xold[RY];
+#pragma unroll
+      for (int j = 0; j < RY; ++j) {
+        xold[j] = V2{T(0), T(0)};
+        if (two && emit) xold[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + (int64_t)j * res);
+      }
+      if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
+        atomicExch(A.err, 1);
+        *s_abort = 1;
+      }
+      // x filter of the staged rows ry .. ry + 5
+      V2 um[RY + 4], us[RY + 4];
+#pragma unroll
+      for (int r = 0; r < RY + 4; ++r) {
+        const T* row = &s_x[k][ry + r][2 * p + XOFF];
+        V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
+           v2 = *reinterpret_cast<const V2*>(row + 4);
+        if (two && (r == 2 || r == 3)) wo[r - 2][k] = v1;  // centre columns 2p, 2p + 1 of dold
+        if (two) {
+          const T* zr = &s_z[k][ry + r][2 * p + XOFF];
+          v0 = p_fma(pbeta, v0, *reinterpret_cast<const V2*>(zr));
+          v1 = p_fma(pbeta, v1, *reinterpret_cast<const V2*>(zr + 2));
+          v2 = p_fma(pbeta, v2, *reinterpret_cast<const V2*>(zr + 4));
+        }
+        if (r == 2 || r == 3) wc[r - 2][k] = v1;  // centre: x (f for kOpChebF; d for kOpApplyD)
+        const V2 v12 = V2{v0.y, v1.x}, v34 = V2{v1.y, v2.x};
+        sym2(v0, v12, v1, v34, v2, pm, ps, um[r], us[r]);
+      }
+      V2 fo[RY], po[RY];
+#pragma unroll
+      for (int j = 0; j < RY; ++j) {
+        fo[j] = po[j] = V2{T(0), T(0)};
+        if (use_f) fo[j] = *reinterpret_cast<const V2*>(&s_f[k][ry + j][2 * p]);
+        if (use_p) po[j] = *reinterpret_cast<const V2*>(&s_p[k][ry + j][2 * p]);
+      }
+      __syncthreads();  // stage k is read
+      if (*s_abort) {
+        stop = true;
+        break;
+      }
+      if (t == 0 && it + NS < nissue) issue(it + NS);
+#pragma unroll
+      for (int j = 0; j < RY; ++j) {
+        // y filter: wa = M_y us + S_y um, wb = M_y um
+        V2 vmm, vms, vsm, unused;
+        sym2(um[j], um[j + 1], um[j + 2], um[j + 3], um[j + 4], pm, ps, vmm, vms);
+        sym2(us[j], us[j + 1], us[j + 2], us[j + 3], us[j + 4], pm, ps, vsm, unused);
+        const V2 wa = p_add(vsm, vms), wb = vmm;
+        // z scatter: plane zin is tap 4 - e (= tap e, symmetric rows) of output plane zin - 2 + e,
+        // slot (k + e) mod NS
+#pragma unroll
+        for (int e = 0; e < 5; ++e) {
+          const V2 cm = pm[e < 3 ? e : 4 - e], cs = ps[e < 3 ? e : 4 - e];
+          V2& a = acc[j][(k + e) % NS];
+          a = e == 4 ? p_fma(cs, wb, p_mul(cm, wa)) : p_fma(cs, wb, p_fma(cm, wa, a));
+        }
+      }
+      if (emit) {
+#pragma unroll
+        for (int j = 0; j < RY; ++j) {
+          const V2 a = acc[j][k], cc = wc[j][(k + 3) % NS];
+          V2 res2 = p_fma(pe_c, cc, p_mul(pe_acc, a));
+          if (MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF) res2 = p_fma(pe_f, fo[j], res2);
+          if (MODE == kOpCheb) res2 = p_fma(pe_p, po[j], res2);
+          T* oj = op + (int64_t)j * res;
+          *reinterpret_cast<V2*>(oj) = res2;
+          if (two) {
+            *reinterpret_cast<V2*>(A.out2 + (oj - out)) = cc;
+            *reinterpret_cast<V2*>(A.xacc + (oj - out)) = p_fma(p_bc<V2>(A.s2), wo[j][(k + 3) % NS], xold[j]);
+          }
+          if ((MODE == kOpApply || MODE == kOpApplyD) && want_dot)
+            dacc += (double)cc.x * (double)res2.x + (double)cc.y * (double)res2.y;
+          if (MODE == kOpCheb && want_dot) dacc += (double)fo[j].x * (double)res2.x + (double)fo[j].y * (double)res2.y;
+        }
+      }
+      op += plane;
+    }
+    if (stop) break;
+  }
+  if (stop && t == 0) {
+    for (int q = it; q < min(it + NS, nissue); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
+  }
+  if ((MODE == kOpApply || MODE == kOpCheb || MODE == kOpApplyD) && A.dot != nullptr) {
+    typedef cub::BlockReduce<double, kThreadsR> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double tot = BR(tmp).Sum(dacc);
+    if (t == 0)
+      A.dot[A.dot_base + (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = tot;
+  }
+}
+
 // one warp sums np partials in a fixed order
 __global__ void k_sum_parts(const double* __restrict__ part, int np, double* __restrict__ out) {
   double s = 0.0;
@@ -1202,24 +1390,27 @@ CUtensorMap plane_map(const T* base, int L, uint32_t bx, uint32_t by) {
 }
 constexpr int kTmaMinLevel = 6;  // res >= 64: full 64-wide x tiles (k_op3)
 
-// launches k_op3 over the interior tiles and the face tiles of a level
+// launches the operator pass of a level: k_op3r when every row is the interior row, else k_op3
+// over the interior tiles and the face tiles
 // returns the number of CTAs (= dot partials written when a.dot is set)
 template <typename T, int MODE>
 int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, const CUtensorMap& mp, T* out,
                const Op3Args<T>& a, int nz) {
   typedef Geo3<T> G;
-  static bool attr = false;  // once per instantiation pair
+  typedef Geo3R<T> GR;
+  static bool attr = false;  // once per instantiation
   if (!attr) {
     PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
     PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
+    PR_CUDA(cudaFuncSetAttribute(k_op3r<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR::BYTES));
     attr = true;
   }
   const int nbx = a.nbx, nby = a.nby;
   Op3Args<T> e = a;
   e.ox = e.oy = 0;
   e.dot_base = 0;
-  if (a.edge == 0) {  // every row acts as the interior row: one launch of the interior variant
-    k_op3<T, MODE, false><<<dim3(nbx, nby, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+  if (a.edge == 0) {  // every row acts as the interior row: one launch of the register-window variant
+    k_op3r<T, MODE><<<dim3(nbx, nby, nz), kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
     PR_CHECK_LAUNCH();
     return nbx * nby * nz;
   }
