@@ -844,12 +844,12 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   }
   const V2 pe_acc = p_bc<V2>(e_acc), pe_c = p_bc<V2>(e_c), pe_f = p_bc<V2>(e_f), pe_p = p_bc<V2>(e_p);
   // acc[j][s]: the output plane of slot s (zo = z0 - 4 + it for it = s mod NS) of row j, partial;
-  // wc, wo: centres of the staged planes (d, and dold for kOpApplyD) by stage
-  V2 acc[RY][NS], wc[RY][NS], wo[RY][NS];
+  // wc: centres of the staged planes (x; f for kOpChebF, d for kOpApplyD) by stage
+  V2 acc[RY][NS], wc[RY][NS];
 #pragma unroll
   for (int j = 0; j < RY; ++j)
 #pragma unroll
-    for (int k = 0; k < NS; ++k) acc[j][k] = wc[j][k] = wo[j][k] = V2{T(0), T(0)};
+    for (int k = 0; k < NS; ++k) acc[j][k] = wc[j][k] = V2{T(0), T(0)};
   const V2 pbeta = p_bc<V2>(A.s1);
   T* op = out + (int64_t)gx + (int64_t)res * (y0 + ry) + plane * (z0 - 4);  // row ry of plane z0 - 4 + it
   const bool want_dot = A.dot != nullptr;
@@ -861,11 +861,14 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
     for (int k = 0; k < NS; ++k) {
       it = g * NS + k;
       const bool emit = (unsigned)(it - 4) < (unsigned)(z1 - z0);
+      // kOpApplyD: xacc += s2 dold on the staged plane zin = zo + 2 when it is one of this CTA's
+      // planes (the iterate of those rows, loaded before the wait)
+      const bool upd = two && (unsigned)(it - 2) < (unsigned)(z1 - z0);
       V2 xold[RY];
 #pragma unroll
       for (int j = 0; j < RY; ++j) {
         xold[j] = V2{T(0), T(0)};
-        if (two && emit) xold[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + (int64_t)j * res);
+        if (upd) xold[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + 2 * plane + (int64_t)j * res);
       }
       if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
         atomicExch(A.err, 1);
@@ -878,7 +881,9 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
         const T* row = &s_x[k][ry + r][2 * p + XOFF];
         V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
            v2 = *reinterpret_cast<const V2*>(row + 4);
-        if (two && (r == 2 || r == 3)) wo[r - 2][k] = v1;  // centre columns 2p, 2p + 1 of dold
+        if (upd && (r == 2 || r == 3))  // centre columns 2p, 2p + 1 of dold
+          *reinterpret_cast<V2*>(A.xacc + (op - out) + 2 * plane + (int64_t)(r - 2) * res) =
+              p_fma(p_bc<V2>(A.s2), v1, xold[r - 2]);
         if (two) {
           const T* zr = &s_z[k][ry + r][2 * p + XOFF];
           v0 = p_fma(pbeta, v0, *reinterpret_cast<const V2*>(zr));
@@ -927,10 +932,7 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
           if (MODE == kOpCheb) res2 = p_fma(pe_p, po[j], res2);
           T* oj = op + (int64_t)j * res;
           *reinterpret_cast<V2*>(oj) = res2;
-          if (two) {
-            *reinterpret_cast<V2*>(A.out2 + (oj - out)) = cc;
-            *reinterpret_cast<V2*>(A.xacc + (oj - out)) = p_fma(p_bc<V2>(A.s2), wo[j][(k + 3) % NS], xold[j]);
-          }
+          if (two) *reinterpret_cast<V2*>(A.out2 + (oj - out)) = cc;
           if ((MODE == kOpApply || MODE == kOpApplyD) && want_dot)
             dacc += (double)cc.x * (double)res2.x + (double)cc.y * (double)res2.y;
           if (MODE == kOpCheb && want_dot) dacc += (double)fo[j].x * (double)res2.x + (double)fo[j].y * (double)res2.y;
