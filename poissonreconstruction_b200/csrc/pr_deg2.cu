@@ -365,6 +365,7 @@ struct Op3Args {
   T s1, s2;        // kOpApplyD: beta, alpha of the previous step
   T* out2;         // kOpApplyD: d
   T* xacc;         // kOpApplyD: the CG iterate
+  int xmode;       // kOpApplyD: 0 leave xacc alone, 1 xacc = s2 dold (not read), 2 xacc += s2 dold
 };
 
 // the (x, y) tile of an EDGE CTA: the first and the last tile row, then the first and the last
@@ -549,7 +550,8 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
       it = g * NS + k;
       // kOpApplyD: the iterate of this step's output plane, loaded before the wait
       V2 xold = V2{T(0), T(0)};
-      if (two && (unsigned)(it - 4) < (unsigned)(z1 - z0)) xold = *reinterpret_cast<const V2*>(A.xacc + (op - out));
+      if (two && A.xmode == 2 && (unsigned)(it - 4) < (unsigned)(z1 - z0))
+        xold = *reinterpret_cast<const V2*>(A.xacc + (op - out));
       if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
         atomicExch(A.err, 1);
         *s_abort = 1;
@@ -739,7 +741,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
         *reinterpret_cast<V2*>(op) = res2;
         if (two) {
           *reinterpret_cast<V2*>(A.out2 + (op - out)) = wc[(k + 3) % NS];
-          *reinterpret_cast<V2*>(A.xacc + (op - out)) = p_fma(p_bc<V2>(A.s2), wo[(k + 3) % NS], xold);
+          if (A.xmode) *reinterpret_cast<V2*>(A.xacc + (op - out)) = p_fma(p_bc<V2>(A.s2), wo[(k + 3) % NS], xold);
         }
         if ((MODE == kOpApply || MODE == kOpApplyD) && want_dot) {
           const V2 cc = wc[(k + 3) % NS];
@@ -863,12 +865,12 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
       const bool emit = (unsigned)(it - 4) < (unsigned)(z1 - z0);
       // kOpApplyD: xacc += s2 dold on the staged plane zin = zo + 2 when it is one of this CTA's
       // planes (the iterate of those rows, loaded before the wait)
-      const bool upd = two && (unsigned)(it - 2) < (unsigned)(z1 - z0);
+      const bool upd = two && A.xmode && (unsigned)(it - 2) < (unsigned)(z1 - z0);
       V2 xold[RY];
 #pragma unroll
       for (int j = 0; j < RY; ++j) {
         xold[j] = V2{T(0), T(0)};
-        if (upd) xold[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + 2 * plane + (int64_t)j * res);
+        if (upd && A.xmode == 2) xold[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + 2 * plane + (int64_t)j * res);
       }
       if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
         atomicExch(A.err, 1);
@@ -1655,6 +1657,7 @@ struct System2 {
     T* out2 = nullptr;
     T* xacc = nullptr;
     double s1 = 0.0, s2 = 0.0;
+    int xmode = 2;  // see Op3Args::xmode
   };
   int op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0,
          int tma = -1, double c0 = 0.0, double* dot = nullptr, const Fuse* fu = nullptr) {
@@ -1690,6 +1693,7 @@ struct System2 {
       A.s2 = two ? (T)fu->s2 : T(0);
       A.out2 = two ? fu->out2 : nullptr;
       A.xacc = two ? fu->xacc : nullptr;
+      A.xmode = two ? fu->xmode : 0;
       const int nz = (res + kZChunk3 - 1) / kZChunk3;
       const CUtensorMap mx = plane_map<T>(x, q.L, G::BW, SH);
       const CUtensorMap mf = f ? (two ? plane_map<T>(f, q.L, G::BW, SH) : plane_map<T>(f, q.L, G::TXP, TY)) : mx;
@@ -1712,7 +1716,7 @@ struct System2 {
       PR_CHECK_LAUNCH();
     }
     // vectors moved (reads + writes)
-    const int vecs = mode == kOpApplyD ? 6 : (mode == kOpApply || mode == kOpChebF ? 2 : (mode == kOpCheb && xp ? 4 : 3));
+    const int vecs = mode == kOpApplyD ? 4 + (fu->xmode == 2 ? 2 : fu->xmode) : (mode == kOpApply || mode == kOpChebF ? 2 : (mode == kOpCheb && xp ? 4 : 3));
     bytes += (double)q.n * sizeof(T) * vecs;
     return nparts;
   }
@@ -1792,13 +1796,14 @@ struct System2 {
 };
 
 // preconditioned CG on the finest level from x = 0 to ||r|| <= tol_abs; r holds b on entry and is
-// overwritten with the recursively updated residual.  On the TMA operator (res >= 64) the vector
+// overwritten with the recursively updated residual; rr0 = r . r on entry when the caller knows it
+// (else negative).  On the TMA operator (res >= 64) the vector
 // updates ride on passes that read the vectors anyway: d = z + beta d, q = A d, d . q and
 // x += alpha d (of the previous step) in the operator pass, r . z in the V-cycle's last smoothing
 // step; r -= alpha q with r . r is its own pass, so that convergence is known before the next
 // V-cycle.
 template <typename T>
-int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) {
+int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit, double rr0 = -1.0) {
   const uint64_t n = sys.lv[0].n;
   cudaStream_t s = c->stream;
   const std::string tn = tn2<T>();
@@ -1806,10 +1811,17 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
   T* d = c->buf<T>("d2cg_d_" + tn, n);
   T* q = c->buf<T>("d2cg_q_" + tn, n);
   const bool fused = sys.fused_dots();
-  PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
-  double rr = dot<T>(c, r, r, n);
-  sys.bytes += 2.0 * n * sizeof(T);
-  if (!(std::sqrt(rr) > tol_abs)) return 0;
+  // the fused path defines x in its second direction pass (x = alpha d); the other one adds to it
+  if (!fused) PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
+  double rr = rr0;
+  if (rr < 0.0) {
+    rr = dot<T>(c, r, r, n);
+    sys.bytes += 2.0 * n * sizeof(T);
+  }
+  if (!(std::sqrt(rr) > tol_abs)) {
+    if (fused) PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
+    return 0;
+  }
   int it = 0;
   if (!fused) {
     sys.vcycle(0, r, z);
@@ -1853,6 +1865,7 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
   double rz = precondition();
   double alpha = 0.0, alpha_prev = 0.0, beta = 0.0;
   bool pending = false;  // x += alpha dcur not applied yet
+  bool x_def = false;    // x written (until then it is zero and never read)
   while (it < maxit) {
     // d = z + beta dprev (d = z at first), q = A d (+ screening), d . q, x += alpha_prev dprev
     typename System2<T>::Fuse fu;
@@ -1860,7 +1873,9 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
     fu.xacc = x;
     fu.s1 = dprev ? beta : 0.0;
     fu.s2 = dprev ? alpha_prev : 0.0;
+    fu.xmode = dprev ? (x_def ? 2 : 1) : 0;
     const int na = sys.op(0, kOpApplyD, dprev ? dprev : z, z, nullptr, q, 0.0, 0.0, -1, 0.0, sys.parts_a, &fu);
+    if (dprev) x_def = true;
     pending = false;
     const int nb = sys.screen(dcur, q, +1, sys.parts_b);
     const double dq = sys.sum_parts(na, nb, sys.scr.wh3);
@@ -1878,9 +1893,14 @@ int pcg2(pr_context* c, System2<T>& sys, T* r, T* x, double tol_abs, int maxit) 
     dprev = dcur;
     std::swap(dcur, dalt);
   }
-  if (pending) {
+  if (pending && x_def) {
     axpy<T, T>(s, n, alpha, dcur, x);
     sys.bytes += 3.0 * n * sizeof(T);
+  } else if (pending) {
+    scale_convert<T, T>(s, n, alpha, dcur, x);
+    sys.bytes += 2.0 * n * sizeof(T);
+  } else if (!x_def) {
+    PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
   }
   return it;
 }
@@ -2012,38 +2032,45 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
   const double* b = c->get<double>("d2_b");
   double* x = c->buf<double>("d2_x", n);
   double* r = c->buf<double>("d2_r", n);
-  PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
   const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;
   const int max_iters = p.max_iters > 0 ? (int)p.max_iters : 200;
   const bool mixed = p.precision != PR_PRECISION_FP64;
   st.pcg_iterations = 0;
   st.refinement_steps = 0;
-  const double bn = std::sqrt(dot<double>(c, b, b, n));
-  double bytes = 2.0 * n * 8;
   System2<double> sys64;
   sys64.init(c, D, c->pw, !mixed);
   sys64.set_screen(c->get<double>("d2_phi64"));
+  // ||b||: mixed, from the conversion of b that starts the FP32 solve; FP64, a dot product
+  float* r32 = mixed ? c->buf<float>("d2_r32", n) : nullptr;
+  const double bn = mixed ? convert_norm(c, b, r32, n) : std::sqrt(dot<double>(c, b, b, n));
+  double bytes = mixed ? 12.0 * n : 8.0 * n;
   double rn = bn;
   int used = 0;
+  bool x_zero = true;  // x = 0: the first correction is x itself (no zero fill, no x += e)
   if (bn > 0.0) {
     if (mixed) {
       System2<float> sys32;
       sys32.init(c, D, c->pw, true);
       sys32.set_screen(c->get<float>("d2_phi32"));
-      float* r32 = c->buf<float>("d2_r32", n);
       float* e32 = c->buf<float>("d2_e32", n);
       const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
-      rn = convert_norm(c, b, r32, n);
-      bytes += 12.0 * n;
       while (rn > target * bn && used < max_iters) {
         const double tol = std::max(inner, 0.5 * target * bn / rn);
-        const int it = pcg2<float>(c, sys32, r32, e32, tol * rn, max_iters - used);
+        // r32 . r32 differs from rn^2 only by the FP32 rounding of r32: good enough for the entry test
+        const int it = pcg2<float>(c, sys32, r32, e32, tol * rn, max_iters - used, rn * rn);
         used += it;
-        axpy<float, double>(s, n, 1.0, e32, x);
+        if (x_zero) {
+          scale_convert<float, double>(s, n, 1.0, e32, x);
+          bytes += 12.0 * n;
+        } else {
+          axpy<float, double>(s, n, 1.0, e32, x);
+          bytes += 20.0 * n;
+        }
+        x_zero = false;
         sys64.op(0, kOpResid, x, b, nullptr, r);  // r = b - A x
         sys64.screen(x, r, -1);
         const double rn_new = convert_norm(c, r, r32, n);
-        bytes += 20.0 * n + 12.0 * n;
+        bytes += 12.0 * n;
         st.refinement_steps++;
         const bool stalled = it == 0 || !(rn_new < rn);
         rn = rn_new;
@@ -2056,13 +2083,19 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
       PR_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
       bytes += 16.0 * n;
       while (rn > target * bn && used < max_iters) {
-        const int it = pcg2<double>(c, sys64, r, e64, 0.5 * target * bn, max_iters - used);
+        const int it = pcg2<double>(c, sys64, r, e64, 0.5 * target * bn, max_iters - used, rn * rn);
         used += it;
-        axpy<double, double>(s, n, 1.0, e64, x);
+        if (x_zero) {
+          std::swap(x, e64);  // x = 0 + e
+        } else {
+          axpy<double, double>(s, n, 1.0, e64, x);
+          bytes += 24.0 * n;
+        }
+        x_zero = false;
         sys64.op(0, kOpResid, x, b, nullptr, r);
         sys64.screen(x, r, -1);
         const double rn_new = std::sqrt(dot<double>(c, r, r, n));
-        bytes += 24.0 * n + 16.0 * n;
+        bytes += 16.0 * n;
         st.refinement_steps++;
         const bool stalled = it == 0 || !(rn_new < rn);
         rn = rn_new;
@@ -2070,6 +2103,7 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
       }
     }
   }
+  if (x_zero) PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
   bytes += sys64.bytes;
   sys64.check();
   st.pcg_iterations = (uint32_t)used;

@@ -618,6 +618,7 @@ PR_INST(double)
 #undef PR_INST
 template void scale_convert<double, float>(cudaStream_t, uint64_t, double, const double*, float*);
 template void scale_convert<float, double>(cudaStream_t, uint64_t, double, const float*, double*);
+template void scale_convert<float, float>(cudaStream_t, uint64_t, double, const float*, float*);
 template void scale_convert<double, double>(cudaStream_t, uint64_t, double, const double*, double*);
 template void axpy<float, double>(cudaStream_t, uint64_t, double, const float*, double*);
 template void axpy<float, float>(cudaStream_t, uint64_t, double, const float*, float*);

@@ -66,18 +66,26 @@ __global__ void k_bbox_partial(const double* __restrict__ pts6, uint64_t n, doub
     for (int k = 0; k < 6; ++k) part[6 * blockIdx.x + k] = s[k][0];
 }
 
+// one warp: lane l folds the partials l, l + 32, ..., then the lanes fold by shuffle (min and max
+// are exact, so the order does not change the result)
 __global__ void k_bbox_final(const double* __restrict__ part, int nparts, double* __restrict__ out) {
-  if (threadIdx.x != 0) return;
+  const int l = threadIdx.x;
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int b = 0; b < nparts; ++b)
+  for (int b = l; b < nparts; b += 32)
     for (int k = 0; k < 3; ++k) {
       lo[k] = fmin(lo[k], part[6 * b + k]);
       hi[k] = fmax(hi[k], part[6 * b + 3 + k]);
     }
-  for (int k = 0; k < 3; ++k) {
-    out[k] = lo[k];
-    out[3 + k] = hi[k];
-  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  if (l == 0)
+    for (int k = 0; k < 3; ++k) {
+      out[k] = lo[k];
+      out[3 + k] = hi[k];
+    }
 }
 
 struct Mat16 {
