@@ -346,7 +346,10 @@ struct Vec2<double> {
 // kOpApplyD: the preconditioned CG direction update fused into the operator pass (second staged
 //            plane z): d = z + s1 dold (staged: dold, z), out = A d, out2 = d, xacc += s2 dold,
 //            dot d . out
-enum { kOpChebF = 3, kOpChebPF = 4, kOpApplyD = 5 };
+// kOpRefine: the FP64 refinement step on a level without boundary rows (k_op3r only): staged x
+//            (skipped when xzero), the FP32 correction e and b; xn = x + e (written to out2),
+//            out = b - A xn, r32 = (float) out, dot out . out
+enum { kOpChebF = 3, kOpChebPF = 4, kOpApplyD = 5, kOpRefine = 6 };
 
 template <typename T>
 struct Op3Args {
@@ -366,6 +369,8 @@ struct Op3Args {
   T* out2;         // kOpApplyD: d
   T* xacc;         // kOpApplyD: the CG iterate
   int xmode;       // kOpApplyD: 0 leave xacc alone, 1 xacc = s2 dold (not read), 2 xacc += s2 dold
+  float* r32;      // kOpRefine: the residual rounded to FP32
+  int xzero;       // kOpRefine: x = 0 (not staged)
 };
 
 // the (x, y) tile of an EDGE CTA: the first and the last tile row, then the first and the last
@@ -807,10 +812,18 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   const int gx = x0 + 2 * p;
   const int nplanes = z1 - z0 + 4;
   const int ngroups = (nplanes + NS - 1) / NS;
-  constexpr bool use_f = MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF;
+  constexpr bool refine = MODE == kOpRefine;
+  constexpr bool use_f = MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF || refine;
   constexpr bool two = MODE == kOpApplyD;
   const bool use_p = MODE == kOpCheb && A.use_p;
-  const uint32_t bytes = G::XBYTES + (use_f ? G::OBYTES : 0u) + (use_p ? G::OBYTES : 0u) + (two ? G::XBYTES : 0u);
+  const bool use_x = !(refine && A.xzero);
+  // kOpRefine: e (FP32) staged 72 wide from x0 - 4 (16-byte aligned) in the xp space
+  constexpr int EW = 72;
+  constexpr uint32_t EBYTES = EW * SH * 4;
+  static_assert(!refine || (size_t)NS * EBYTES <= (size_t)NS * G::OBYTES, "e stages fit the xp space");
+  float(*s_e)[SH][EW] = reinterpret_cast<float(*)[SH][EW]>(smem + G::OFF_P);
+  const uint32_t bytes = (use_x ? G::XBYTES : 0u) + (use_f ? G::OBYTES : 0u) + (use_p ? G::OBYTES : 0u) +
+                         (two ? G::XBYTES : 0u) + (refine ? EBYTES : 0u);
   if (t == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
     *s_abort = 0;
@@ -820,10 +833,11 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   auto issue = [&](int it) {
     const int s = it % NS, zin = z0 - 2 + it;
     mbar_expect_tx(&bar[s], bytes);
-    tma_load_3d(&s_x[s][0][0], &mx, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
+    if (use_x) tma_load_3d(&s_x[s][0][0], &mx, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
     if (use_f) tma_load_3d(&s_f[s][0][0], &mf, x0, y0, zin - 2, &bar[s]);
     if (use_p) tma_load_3d(&s_p[s][0][0], &mp, x0, y0, zin - 2, &bar[s]);
     if (two) tma_load_3d(&s_z[s][0][0], &mf, x0 - 2 - XOFF, y0 - 2, zin, &bar[s]);
+    if (refine) tma_load_3d(&s_e[s][0][0], &mp, x0 - 4, y0 - 2, zin, &bar[s]);
   };
   const int nissue = ngroups * NS;
   if (t == 0)
@@ -837,7 +851,7 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   const T cbinv = A.cb * A.invd, c0inv = A.c0 * A.invd;
   T e_acc, e_c, e_f, e_p;  // interior epilogue, as in k_op3
   if (MODE == kOpApply || MODE == kOpApplyD) { e_acc = lv.H; e_c = lv.wg; e_f = 0; e_p = 0; }
-  else if (MODE == kOpResid) { e_acc = -lv.H; e_c = -lv.wg; e_f = 1; e_p = 0; }
+  else if (MODE == kOpResid || refine) { e_acc = -lv.H; e_c = -lv.wg; e_f = 1; e_p = 0; }
   else if (MODE == kOpCheb) { e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv; e_p = -A.ca; }
   else if (MODE == kOpChebPF) {
     e_acc = -cbinv * lv.H; e_c = (T(1) + A.ca) - cbinv * lv.wg; e_f = cbinv - A.ca * c0inv; e_p = 0;
@@ -865,7 +879,8 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
       const bool emit = (unsigned)(it - 4) < (unsigned)(z1 - z0);
       // kOpApplyD: xacc += s2 dold on the staged plane zin = zo + 2 when it is one of this CTA's
       // planes (the iterate of those rows, loaded before the wait)
-      const bool upd = two && A.xmode && (unsigned)(it - 2) < (unsigned)(z1 - z0);
+      const bool own = (unsigned)(it - 2) < (unsigned)(z1 - z0);  // staged plane zin is one of this CTA's
+      const bool upd = two && A.xmode && own;
       V2 xold[RY];
 #pragma unroll
       for (int j = 0; j < RY; ++j) {
@@ -881,8 +896,22 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
 #pragma unroll
       for (int r = 0; r < RY + 4; ++r) {
         const T* row = &s_x[k][ry + r][2 * p + XOFF];
-        V2 v0 = *reinterpret_cast<const V2*>(row), v1 = *reinterpret_cast<const V2*>(row + 2),
-           v2 = *reinterpret_cast<const V2*>(row + 4);
+        V2 v0 = V2{T(0), T(0)}, v1 = v0, v2 = v0;
+        if (use_x) {
+          v0 = *reinterpret_cast<const V2*>(row);
+          v1 = *reinterpret_cast<const V2*>(row + 2);
+          v2 = *reinterpret_cast<const V2*>(row + 4);
+        }
+        if (refine) {  // xn = x + e (e column c + 2 is x column c)
+          const float* er = &s_e[k][ry + r][2 * p + XOFF + 2];
+          const float2 e0 = *reinterpret_cast<const float2*>(er), e1 = *reinterpret_cast<const float2*>(er + 2),
+                       e2 = *reinterpret_cast<const float2*>(er + 4);
+          v0 = p_add(v0, V2{(T)e0.x, (T)e0.y});
+          v1 = p_add(v1, V2{(T)e1.x, (T)e1.y});
+          v2 = p_add(v2, V2{(T)e2.x, (T)e2.y});
+          if (own && (r == 2 || r == 3))
+            *reinterpret_cast<V2*>(A.out2 + (op - out) + 2 * plane + (int64_t)(r - 2) * res) = v1;
+        }
         if (upd && (r == 2 || r == 3))  // centre columns 2p, 2p + 1 of dold
           *reinterpret_cast<V2*>(A.xacc + (op - out) + 2 * plane + (int64_t)(r - 2) * res) =
               p_fma(p_bc<V2>(A.s2), v1, xold[r - 2]);
@@ -930,11 +959,15 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
         for (int j = 0; j < RY; ++j) {
           const V2 a = acc[j][k], cc = wc[j][(k + 3) % NS];
           V2 res2 = p_fma(pe_c, cc, p_mul(pe_acc, a));
-          if (MODE == kOpResid || MODE == kOpCheb || MODE == kOpChebPF) res2 = p_fma(pe_f, fo[j], res2);
+          if (use_f) res2 = p_fma(pe_f, fo[j], res2);
           if (MODE == kOpCheb) res2 = p_fma(pe_p, po[j], res2);
           T* oj = op + (int64_t)j * res;
           *reinterpret_cast<V2*>(oj) = res2;
           if (two) *reinterpret_cast<V2*>(A.out2 + (oj - out)) = cc;
+          if (refine) {
+            *reinterpret_cast<float2*>(A.r32 + (oj - out)) = make_float2((float)res2.x, (float)res2.y);
+            if (want_dot) dacc += (double)res2.x * (double)res2.x + (double)res2.y * (double)res2.y;
+          }
           if ((MODE == kOpApply || MODE == kOpApplyD) && want_dot)
             dacc += (double)cc.x * (double)res2.x + (double)cc.y * (double)res2.y;
           if (MODE == kOpCheb && want_dot) dacc += (double)fo[j].x * (double)res2.x + (double)fo[j].y * (double)res2.y;
@@ -947,7 +980,7 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   if (stop && t == 0) {
     for (int q = it; q < min(it + NS, nissue); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
   }
-  if ((MODE == kOpApply || MODE == kOpCheb || MODE == kOpApplyD) && A.dot != nullptr) {
+  if ((MODE == kOpApply || MODE == kOpCheb || MODE == kOpApplyD || refine) && A.dot != nullptr) {
     typedef cub::BlockReduce<double, kThreadsR> BR;
     __shared__ typename BR::TempStorage tmp;
     const double tot = BR(tmp).Sum(dacc);
@@ -1335,6 +1368,32 @@ __global__ void k_screen_gather2(const uint32_t* __restrict__ snode, const uint3
     y[snode[u]] += wh3s * acc;
   }
 }
+// k_screen_gather2 for the fused refinement: also rounds the updated residual to y32 and leaves
+// per-block sums of (y_new^2 - y_old^2), so that ||y||^2 = (the operator pass's sum of y_old^2)
+// + (these), every term in FP64
+template <typename T>
+__global__ void k_screen_gather2_fix(const uint32_t* __restrict__ snode, const uint32_t* __restrict__ soff, uint64_t S,
+                                     const uint32_t* __restrict__ sval, const T* __restrict__ phi,
+                                     const T* __restrict__ proj, T wh3s, T* __restrict__ y, float* __restrict__ y32,
+                                     double* __restrict__ part) {
+  double dsq = 0.0;
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < S; u += (uint64_t)gridDim.x * blockDim.x) {
+    T acc = 0;
+    for (uint32_t e = soff[u]; e < soff[u + 1]; ++e) {
+      const uint32_t pk = sval[e];
+      acc += phi[pk] * proj[pk / 27];
+    }
+    const uint32_t i = snode[u];
+    const T old = y[i], nw = old + wh3s * acc;
+    y[i] = nw;
+    y32[i] = (float)nw;
+    dsq += (double)nw * (double)nw - (double)old * (double)old;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double tot = BR(tmp).Sum(dsq);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
 
 // natural <-> Morton
 template <typename T>
@@ -1402,37 +1461,52 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
                const Op3Args<T>& a, int nz) {
   typedef Geo3<T> G;
   typedef Geo3R<T> GR;
-  static bool attr = false;  // once per instantiation
-  if (!attr) {
-    PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
-    PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
-    PR_CUDA(cudaFuncSetAttribute(k_op3r<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR::BYTES));
-    attr = true;
-  }
-  const int nbx = a.nbx, nby = a.nby;
-  Op3Args<T> e = a;
-  e.ox = e.oy = 0;
-  e.dot_base = 0;
-  if (a.edge == 0) {  // every row acts as the interior row: one launch of the register-window variant
-    k_op3r<T, MODE><<<dim3(nbx, nby, nz), kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
+  if constexpr (MODE == kOpRefine) {  // a level without boundary rows only
+    PR_REQUIRE(a.edge == 0, PR_ERR_INTERNAL, "the fused refinement needs a level without boundary rows");
+    static bool attr_r = false;
+    if (!attr_r) {
+      PR_CUDA(cudaFuncSetAttribute(k_op3r<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR::BYTES));
+      attr_r = true;
+    }
+    Op3Args<T> e = a;
+    e.ox = e.oy = 0;
+    e.dot_base = 0;
+    k_op3r<T, MODE><<<dim3(a.nbx, a.nby, nz), kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
     PR_CHECK_LAUNCH();
+    return a.nbx * a.nby * nz;
+  } else {
+    static bool attr = false;  // once per instantiation
+    if (!attr) {
+      PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
+      PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
+      PR_CUDA(cudaFuncSetAttribute(k_op3r<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR::BYTES));
+      attr = true;
+    }
+    const int nbx = a.nbx, nby = a.nby;
+    Op3Args<T> e = a;
+    e.ox = e.oy = 0;
+    e.dot_base = 0;
+    if (a.edge == 0) {  // every row acts as the interior row: one launch of the register-window variant
+      k_op3r<T, MODE><<<dim3(nbx, nby, nz), kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
+      PR_CHECK_LAUNCH();
+      return nbx * nby * nz;
+    }
+    // interior tiles need every output row at least `edge` from the faces: edge <= 8 (one tile row)
+    const bool split = nbx > 2 && nby > 2 && a.edge <= TY;
+    e.all = split ? 0 : 1;
+    if (split) {
+      e.ox = e.oy = 1;
+      k_op3<T, MODE, false><<<dim3(nbx - 2, nby - 2, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+      PR_CHECK_LAUNCH();
+      e.dot_base = (nbx - 2) * (nby - 2) * nz;
+      k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+      PR_CHECK_LAUNCH();
+    } else {
+      k_op3<T, MODE, true><<<dim3(nbx * nby, 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+      PR_CHECK_LAUNCH();
+    }
     return nbx * nby * nz;
   }
-  // interior tiles need every output row at least `edge` from the faces: edge <= 8 (one tile row)
-  const bool split = nbx > 2 && nby > 2 && a.edge <= TY;
-  e.all = split ? 0 : 1;
-  if (split) {
-    e.ox = e.oy = 1;
-    k_op3<T, MODE, false><<<dim3(nbx - 2, nby - 2, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
-    PR_CHECK_LAUNCH();
-    e.dot_base = (nbx - 2) * (nby - 2) * nz;
-    k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
-    PR_CHECK_LAUNCH();
-  } else {
-    k_op3<T, MODE, true><<<dim3(nbx * nby, 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
-    PR_CHECK_LAUNCH();
-  }
-  return nbx * nby * nz;
 }
 
 // ------------------------------------------------------------------ host: the system
@@ -1622,6 +1696,32 @@ struct System2 {
     return (int)nb;
   }
 
+  // The FP64 refinement step on the finest level in one operator pass: xn = x + e (x = 0 when
+  // xzero), r = b - A xn with the screening term, r32 = (float) r; returns ||r||
+  double refine(const T* x, const float* e32, const T* b, T* xn, T* r, float* r32, bool xzero) {
+    alloc_parts();
+    Fuse fu;
+    fu.out2 = xn;
+    fu.e32 = e32;
+    fu.r32 = r32;
+    fu.xzero = xzero;
+    const int na = op(0, kOpRefine, x, b, nullptr, r, 0.0, 0.0, 1, 0.0, parts_a, &fu);
+    int nb = 0;
+    if (scr.S > 0) {
+      cudaStream_t s = c->stream;
+      const unsigned np = grid_for(scr.P, 1u << 20);
+      k_screen_proj2<T><<<np, kThreads, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, xn, scr.proj, nullptr);
+      PR_CHECK_LAUNCH();
+      nb = (int)grid_for(scr.S, 1u << 20);
+      k_screen_gather2_fix<T><<<nb, kThreads, 0, s>>>(scr.snode, scr.soff, scr.S, scr.sval, scr.phi, scr.proj,
+                                                       (T)(-scr.wh3), r, r32, parts_b);
+      PR_CHECK_LAUNCH();
+      bytes += (double)scr.P * 27 * (4 + 2 * sizeof(T)) + (double)scr.P * sizeof(T) +
+               (double)scr.pairs * (4 + 2 * sizeof(T)) + (double)scr.S * (8 + 2 * sizeof(T) + 4);
+    }
+    return std::sqrt(std::max(0.0, sum_parts(na, nb, 1.0)));
+  }
+
   // fused dot products (finest level on the TMA operator): per-CTA partials and their sums
   double* parts_a = nullptr;  // operator partials
   double* parts_b = nullptr;  // screening partials
@@ -1657,7 +1757,10 @@ struct System2 {
     T* out2 = nullptr;
     T* xacc = nullptr;
     double s1 = 0.0, s2 = 0.0;
-    int xmode = 2;  // see Op3Args::xmode
+    int xmode = 2;               // see Op3Args::xmode
+    const float* e32 = nullptr;  // kOpRefine: the correction
+    float* r32 = nullptr;        // kOpRefine: the residual in FP32
+    bool xzero = false;          // kOpRefine: x = 0
   };
   int op(int li, int mode, const T* x, const T* f, const T* xp, T* out, double a = 0.0, double b = 0.0,
          int tma = -1, double c0 = 0.0, double* dot = nullptr, const Fuse* fu = nullptr) {
@@ -1687,23 +1790,31 @@ struct System2 {
       A.err = err;
       A.dot = dot;
       A.dot_base = 0;
-      const bool two = mode == kOpApplyD;
+      const bool two = mode == kOpApplyD, refine = mode == kOpRefine;
       PR_REQUIRE(!two || (fu && fu->out2 && fu->xacc && f), PR_ERR_INTERNAL, "fused CG pass without its operands");
+      PR_REQUIRE(!refine || (fu && fu->out2 && fu->e32 && fu->r32 && f && sizeof(T) == 8), PR_ERR_INTERNAL,
+                 "fused refinement without its operands");
+      A.r32 = refine ? fu->r32 : nullptr;
+      A.xzero = refine && fu->xzero ? 1 : 0;
       A.s1 = two ? (T)fu->s1 : T(0);
       A.s2 = two ? (T)fu->s2 : T(0);
-      A.out2 = two ? fu->out2 : nullptr;
+      A.out2 = (two || refine) ? fu->out2 : nullptr;
       A.xacc = two ? fu->xacc : nullptr;
       A.xmode = two ? fu->xmode : 0;
       const int nz = (res + kZChunk3 - 1) / kZChunk3;
       const CUtensorMap mx = plane_map<T>(x, q.L, G::BW, SH);
       const CUtensorMap mf = f ? (two ? plane_map<T>(f, q.L, G::BW, SH) : plane_map<T>(f, q.L, G::TXP, TY)) : mx;
-      const CUtensorMap mp = xp ? plane_map<T>(xp, q.L, G::TXP, TY) : mx;
+      const CUtensorMap mp = refine ? plane_map<float>(fu->e32, q.L, 72, SH)
+                                    : (xp ? plane_map<T>(xp, q.L, G::TXP, TY) : mx);
       switch (mode) {
         case kOpApply: nparts = launch_op3<T, kOpApply>(s, mx, mf, mp, out, A, nz); break;
         case kOpResid: nparts = launch_op3<T, kOpResid>(s, mx, mf, mp, out, A, nz); break;
         case kOpCheb: nparts = launch_op3<T, kOpCheb>(s, mx, mf, mp, out, A, nz); break;
         case kOpChebF: nparts = launch_op3<T, kOpChebF>(s, mx, mf, mp, out, A, nz); break;
         case kOpChebPF: nparts = launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
+        case kOpRefine:
+          if constexpr (sizeof(T) == 8) nparts = launch_op3<T, kOpRefine>(s, mx, mf, mp, out, A, nz);
+          break;
         default: nparts = launch_op3<T, kOpApplyD>(s, mx, mf, mp, out, A, nz); break;
       }
     } else {
@@ -1716,6 +1827,10 @@ struct System2 {
       PR_CHECK_LAUNCH();
     }
     // vectors moved (reads + writes)
+    if (mode == kOpRefine) {  // x (unless zero), b, xn, r in T; e, r32 in FP32
+      bytes += (double)q.n * (sizeof(T) * (fu->xzero ? 3 : 4) + 8);
+      return nparts;
+    }
     const int vecs = mode == kOpApplyD ? 4 + (fu->xmode == 2 ? 2 : fu->xmode) : (mode == kOpApply || mode == kOpChebF ? 2 : (mode == kOpCheb && xp ? 4 : 3));
     bytes += (double)q.n * sizeof(T) * vecs;
     return nparts;
@@ -2054,23 +2169,33 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
       sys32.set_screen(c->get<float>("d2_phi32"));
       float* e32 = c->buf<float>("d2_e32", n);
       const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
+      // on the TMA operator the refinement step (x += e, r = b - A x, r32, ||r||) is one pass
+      // into a second iterate buffer (the pass reads x with halos, so it cannot write x)
+      const bool fused_refine = D >= (uint32_t)kTmaMinLevel;
+      double* xn = fused_refine ? c->buf<double>("d2_x2", n) : nullptr;
       while (rn > target * bn && used < max_iters) {
         const double tol = std::max(inner, 0.5 * target * bn / rn);
         // r32 . r32 differs from rn^2 only by the FP32 rounding of r32: good enough for the entry test
         const int it = pcg2<float>(c, sys32, r32, e32, tol * rn, max_iters - used, rn * rn);
         used += it;
-        if (x_zero) {
-          scale_convert<float, double>(s, n, 1.0, e32, x);
-          bytes += 12.0 * n;
+        double rn_new;
+        if (fused_refine) {
+          rn_new = sys64.refine(x, e32, b, xn, r, r32, x_zero);
+          std::swap(x, xn);
         } else {
-          axpy<float, double>(s, n, 1.0, e32, x);
-          bytes += 20.0 * n;
+          if (x_zero) {
+            scale_convert<float, double>(s, n, 1.0, e32, x);
+            bytes += 12.0 * n;
+          } else {
+            axpy<float, double>(s, n, 1.0, e32, x);
+            bytes += 20.0 * n;
+          }
+          sys64.op(0, kOpResid, x, b, nullptr, r);  // r = b - A x
+          sys64.screen(x, r, -1);
+          rn_new = convert_norm(c, r, r32, n);
+          bytes += 12.0 * n;
         }
         x_zero = false;
-        sys64.op(0, kOpResid, x, b, nullptr, r);  // r = b - A x
-        sys64.screen(x, r, -1);
-        const double rn_new = convert_norm(c, r, r32, n);
-        bytes += 12.0 * n;
         st.refinement_steps++;
         const bool stalled = it == 0 || !(rn_new < rn);
         rn = rn_new;
