@@ -964,10 +964,9 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
           T* oj = op + (int64_t)j * res;
           *reinterpret_cast<V2*>(oj) = res2;
           if (two) *reinterpret_cast<V2*>(A.out2 + (oj - out)) = cc;
-          if (refine) {
-            *reinterpret_cast<float2*>(A.r32 + (oj - out)) = make_float2((float)res2.x, (float)res2.y);
-            if (want_dot) dacc += (double)res2.x * (double)res2.x + (double)res2.y * (double)res2.y;
-          }
+          if (refine) *reinterpret_cast<float2*>(A.r32 + (oj - out)) = make_float2((float)res2.x, (float)res2.y);
+          if ((MODE == kOpResid || refine) && want_dot)
+            dacc += (double)res2.x * (double)res2.x + (double)res2.y * (double)res2.y;
           if ((MODE == kOpApply || MODE == kOpApplyD) && want_dot)
             dacc += (double)cc.x * (double)res2.x + (double)cc.y * (double)res2.y;
           if (MODE == kOpCheb && want_dot) dacc += (double)fo[j].x * (double)res2.x + (double)fo[j].y * (double)res2.y;
@@ -980,7 +979,7 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   if (stop && t == 0) {
     for (int q = it; q < min(it + NS, nissue); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
   }
-  if ((MODE == kOpApply || MODE == kOpCheb || MODE == kOpApplyD || refine) && A.dot != nullptr) {
+  if ((MODE == kOpApply || MODE == kOpCheb || MODE == kOpApplyD || MODE == kOpResid || refine) && A.dot != nullptr) {
     typedef cub::BlockReduce<double, kThreadsR> BR;
     __shared__ typename BR::TempStorage tmp;
     const double tot = BR(tmp).Sum(dacc);
@@ -1368,7 +1367,7 @@ __global__ void k_screen_gather2(const uint32_t* __restrict__ snode, const uint3
     y[snode[u]] += wh3s * acc;
   }
 }
-// k_screen_gather2 for the fused refinement: also rounds the updated residual to y32 and leaves
+// k_screen_gather2 for the fused refinement: also rounds the updated residual to y32 (if given) and leaves
 // per-block sums of (y_new^2 - y_old^2), so that ||y||^2 = (the operator pass's sum of y_old^2)
 // + (these), every term in FP64
 template <typename T>
@@ -1386,7 +1385,7 @@ __global__ void k_screen_gather2_fix(const uint32_t* __restrict__ snode, const u
     const uint32_t i = snode[u];
     const T old = y[i], nw = old + wh3s * acc;
     y[i] = nw;
-    y32[i] = (float)nw;
+    if (y32) y32[i] = (float)nw;
     dsq += (double)nw * (double)nw - (double)old * (double)old;
   }
   typedef cub::BlockReduce<double, kThreads> BR;
@@ -1706,20 +1705,32 @@ struct System2 {
     fu.r32 = r32;
     fu.xzero = xzero;
     const int na = op(0, kOpRefine, x, b, nullptr, r, 0.0, 0.0, 1, 0.0, parts_a, &fu);
-    int nb = 0;
-    if (scr.S > 0) {
-      cudaStream_t s = c->stream;
-      const unsigned np = grid_for(scr.P, 1u << 20);
-      k_screen_proj2<T><<<np, kThreads, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, xn, scr.proj, nullptr);
-      PR_CHECK_LAUNCH();
-      nb = (int)grid_for(scr.S, 1u << 20);
-      k_screen_gather2_fix<T><<<nb, kThreads, 0, s>>>(scr.snode, scr.soff, scr.S, scr.sval, scr.phi, scr.proj,
-                                                       (T)(-scr.wh3), r, r32, parts_b);
-      PR_CHECK_LAUNCH();
-      bytes += (double)scr.P * 27 * (4 + 2 * sizeof(T)) + (double)scr.P * sizeof(T) +
-               (double)scr.pairs * (4 + 2 * sizeof(T)) + (double)scr.S * (8 + 2 * sizeof(T) + 4);
-    }
+    const int nb = screen_fix(xn, r, r32);
     return std::sqrt(std::max(0.0, sum_parts(na, nb, 1.0)));
+  }
+  // r = b - A x with the screening term on the finest level (TMA operator) and ||r|| from the
+  // pass's partials
+  double resid_norm(const T* x, const T* b, T* r) {
+    alloc_parts();
+    const int na = op(0, kOpResid, x, b, nullptr, r, 0.0, 0.0, 1, 0.0, parts_a);
+    const int nb = screen_fix(x, r, nullptr);
+    return std::sqrt(std::max(0.0, sum_parts(na, nb, 1.0)));
+  }
+  // r -= wh3 Phi Phi^T x with r32 (if given) updated at the screened nodes and per-block partials
+  // of the change of r . r in parts_b; returns the partial count
+  int screen_fix(const T* x, T* r, float* r32) {
+    if (scr.S == 0) return 0;
+    cudaStream_t s = c->stream;
+    const unsigned np = grid_for(scr.P, 1u << 20);
+    k_screen_proj2<T><<<np, kThreads, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, x, scr.proj, nullptr);
+    PR_CHECK_LAUNCH();
+    const int nb = (int)grid_for(scr.S, 1u << 20);
+    k_screen_gather2_fix<T><<<nb, kThreads, 0, s>>>(scr.snode, scr.soff, scr.S, scr.sval, scr.phi, scr.proj,
+                                                     (T)(-scr.wh3), r, r32, parts_b);
+    PR_CHECK_LAUNCH();
+    bytes += (double)scr.P * 27 * (4 + 2 * sizeof(T)) + (double)scr.P * sizeof(T) +
+             (double)scr.pairs * (4 + 2 * sizeof(T)) + (double)scr.S * (8 + 2 * sizeof(T) + (r32 ? 4 : 0));
+    return nb;
   }
 
   // fused dot products (finest level on the TMA operator): per-CTA partials and their sums
@@ -2217,10 +2228,15 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
           bytes += 24.0 * n;
         }
         x_zero = false;
-        sys64.op(0, kOpResid, x, b, nullptr, r);
-        sys64.screen(x, r, -1);
-        const double rn_new = std::sqrt(dot<double>(c, r, r, n));
-        bytes += 16.0 * n;
+        double rn_new;
+        if (D >= (uint32_t)kTmaMinLevel) {  // the norm from the residual pass's partials
+          rn_new = sys64.resid_norm(x, b, r);
+        } else {
+          sys64.op(0, kOpResid, x, b, nullptr, r);
+          sys64.screen(x, r, -1);
+          rn_new = std::sqrt(dot<double>(c, r, r, n));
+          bytes += 8.0 * n;
+        }
         st.refinement_steps++;
         const bool stalled = it == 0 || !(rn_new < rn);
         rn = rn_new;
