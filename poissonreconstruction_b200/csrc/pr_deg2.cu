@@ -1122,6 +1122,111 @@ __global__ void k_restrict4(const T* __restrict__ rf, int Lf, T* __restrict__ fc
   }
 }
 
+// The restriction on the TMA levels (fine res >= 64), streaming in z: a CTA owns a 64 x 16 fine
+// tile (32 x 8 coarse nodes) and kRestrictCZ coarse planes, with the fine planes 2 cz0 - 1 ..
+// 2 cz1 staged through a four-deep ring (72 x 18 FP32 / 68 x 18 FP64 boxes: fine rows y0 - 1 ..
+// y0 + 16 and the columns 4c' - 1 .. 4c' + 4 of every coarse pair). A thread owns one coarse
+// pair in one coarse row: x and y restriction from shared memory as in k_restrict4, z in
+// registers with the terms of every coarse plane added in the order kz = 0..3. Planes, rows and
+// columns outside the grid read as zeros.
+constexpr int kRestrictCZ = 38;  // coarse planes per CTA: 78 staged fine planes
+template <typename T>
+struct GeoRs {
+  static constexpr int NS = 4;
+  static constexpr int BW = Geo3<T>::BW, XOFF = Geo3<T>::XOFF;  // stage column of global x0 - 2 is XOFF
+  static constexpr int SR = 18;                                   // fine rows y0 - 1 .. y0 + 16
+  static constexpr uint32_t SBYTES = BW * SR * sizeof(T);    // one box
+  static constexpr uint32_t SSTRIDE = (SBYTES + 127) & ~127u;  // stages 128-byte aligned
+  static constexpr size_t OFF_BAR = (size_t)NS * SSTRIDE;
+  static constexpr size_t BYTES = OFF_BAR + NS * 8 + 16;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreadsR) k_restrict3(const __grid_constant__ CUtensorMap mr, int Lf,
+                                                         T* __restrict__ fc, int* __restrict__ err) {
+  typedef GeoRs<T> G;
+  typedef typename Vec2<T>::type V2;
+  constexpr int NS = G::NS, BW = G::BW, XOFF = G::XOFF;
+  extern __shared__ __align__(128) unsigned char smem[];
+  auto stage = [&](int st) { return reinterpret_cast<T*>(smem + (size_t)st * G::SSTRIDE); };  // [SR][BW]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NS * 8);
+  const int res = 1 << Lf, rc = res >> 1;
+  const int64_t pc = (int64_t)rc * rc;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;  // coarse pair tx, coarse row ty of the tile
+  const int x0 = blockIdx.x * 64, y0 = blockIdx.y * 16;
+  const int cz0 = blockIdx.z * kRestrictCZ, cz1 = min(cz0 + kRestrictCZ, rc);
+  const int nplanes = 2 * (cz1 - cz0) + 2;  // fine 2 cz0 - 1 .. 2 cz1
+  if (t == 0) {
+    for (int q = 0; q < NS; ++q) mbar_init(&bar[q], 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int q) {
+    mbar_expect_tx(&bar[q % NS], G::SBYTES);
+    tma_load_3d(stage(q % NS), &mr, x0 - 2 - XOFF, y0 - 1, 2 * cz0 - 1 + q, &bar[q % NS]);
+  };
+  if (t == 0)
+    for (int q = 0; q < NS && q < nplanes; ++q) issue(q);
+  const T w[4] = {T(0.25), T(0.75), T(0.75), T(0.25)};
+  const int c0 = 4 * tx + 2 + XOFF;  // stage column of fine 4c' (c' = x0 / 4 + tx)
+  T* out = fc + (int64_t)(x0 / 2 + 2 * tx) + (int64_t)rc * (y0 / 2 + ty);
+  T acc[2][2] = {{T(0), T(0)}, {T(0), T(0)}};  // [coarse plane cz, cz + 1][pair]
+  int q = 0;
+  bool stop = false;
+  for (; q < nplanes; ++q) {
+    const int st = q % NS;
+    if (!mbar_wait(&bar[st], (uint32_t)(q / NS) & 1u)) {
+      atomicExch(err, 1);
+      *s_abort = 1;
+    }
+    T az0 = 0, az1 = 0;  // x and y restriction of fine plane 2 cz0 - 1 + q
+#pragma unroll
+    for (int ky = 0; ky < 4; ++ky) {
+      const T* row = stage(st) + (2 * ty + ky) * BW + c0;
+      const F4<T> c = ld4x(row);
+      const T lo = row[-1], hi = row[4];
+      const T ax0 = T(0.25) * (lo + c.v[2]) + T(0.75) * (c.v[0] + c.v[1]);
+      const T ax1 = T(0.25) * (c.v[1] + hi) + T(0.75) * (c.v[2] + c.v[3]);
+      az0 += w[ky] * ax0;
+      az1 += w[ky] * ax1;
+    }
+    __syncthreads();  // stage st is read
+    if (*s_abort) {
+      stop = true;
+      break;
+    }
+    if (t == 0 && q + NS < nplanes) issue(q + NS);
+    // fine plane 2 cz0 - 1 + q is kz = (q & 1) of coarse cz0 + q / 2 (acc[1], or acc[0] while
+    // q < 2) and kz = 2 + (q & 1) of coarse cz0 + q / 2 - 1 (acc[0]), emitted after its kz = 3
+    const int kz = q & 1;
+    const T wn = kz ? T(0.75) : T(0.25), wc = kz ? T(0.25) : T(0.75);  // w[kz], w[2 + kz]
+    if (q < nplanes - 2) {
+      if (q >= 2) {
+        acc[1][0] += wn * az0;
+        acc[1][1] += wn * az1;
+      } else {
+        acc[0][0] += wn * az0;
+        acc[0][1] += wn * az1;
+      }
+    }
+    if (q >= 2) {
+      acc[0][0] += wc * az0;
+      acc[0][1] += wc * az1;
+      if (kz == 1) {
+        *reinterpret_cast<V2*>(out + (cz0 + q / 2 - 1) * pc) = V2{acc[0][0], acc[0][1]};
+        acc[0][0] = acc[1][0];
+        acc[0][1] = acc[1][1];
+        acc[1][0] = acc[1][1] = T(0);
+      }
+    }
+  }
+  if (stop && t == 0) {
+    for (int r = q; r < min(q + NS, nplanes); ++r) mbar_wait(&bar[r % NS], (uint32_t)(r / NS) & 1u);
+  }
+}
+
 // ------------------------------------------------------------------ setup kernels
 // degree-2 basis of one axis at unit coordinate u: nodes c-1, c, c+1 (the oracle's expressions)
 __device__ __forceinline__ void axis2(double u, double h, int64_t& c, double* b) {
@@ -1506,6 +1611,21 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
     }
     return nbx * nby * nz;
   }
+}
+
+// the restriction of the fine residual rf (level Lf) to the coarse right-hand side fc
+template <typename T>
+void launch_restrict(cudaStream_t s, const T* rf, int Lf, T* fc, int* err) {
+  if (Lf >= kTmaMinLevel) {
+    typedef GeoRs<T> G;
+    const int res = 1 << Lf, rc = res >> 1;
+    const CUtensorMap m = plane_map<T>(rf, Lf, G::BW, G::SR);
+    const dim3 grid(res / 64, res / 16, (rc + kRestrictCZ - 1) / kRestrictCZ);
+    k_restrict3<T><<<grid, kThreadsR, G::BYTES, s>>>(m, Lf, fc, err);
+  } else {
+    k_restrict4<T><<<grid_for(1ull << (3 * (Lf - 1) - 1)), kThreads, 0, s>>>(rf, Lf, fc);
+  }
+  PR_CHECK_LAUNCH();
 }
 
 // ------------------------------------------------------------------ host: the system
@@ -1910,8 +2030,7 @@ struct System2 {
     Level2<T>& qc = lv[li + 1];
     chebyshev(li, f, X, q.y, true);
     op(li, kOpResid, X, f, nullptr, q.y);
-    k_restrict4<T><<<grid_for(qc.n / 2), kThreads, 0, s>>>(q.y, q.L, qc.f);
-    PR_CHECK_LAUNCH();
+    launch_restrict<T>(s, q.y, q.L, qc.f, err);
     bytes += (double)(q.n + qc.n) * sizeof(T);
     vcycle(li + 1, qc.f, qc.x);
     k_prolong4<T><<<grid_for(qc.n / 2), kThreads, 0, s>>>(X, qc.x, q.L, q.y);
@@ -2301,8 +2420,7 @@ double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
       case 3: sys.op(0, kOpApply, x, nullptr, nullptr, y, 0.0, 0.0, 0); break;
       case 4: sys.op(0, kOpResid, x, f, nullptr, y, 0.0, 0.0, 1); break;
       case 5:
-        k_restrict4<T><<<grid_for(nc / 2), kThreads, 0, s>>>(x, (int)D, ec);
-        PR_CHECK_LAUNCH();
+        launch_restrict<T>(s, x, (int)D, ec, sys.err);
         break;
       case 6:
         k_prolong4<T><<<grid_for(nc / 2), kThreads, 0, s>>>(x, ec, (int)D, y);
