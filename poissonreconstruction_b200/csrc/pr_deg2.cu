@@ -1227,6 +1227,114 @@ __global__ void __launch_bounds__(kThreadsR) k_restrict3(const __grid_constant__
   }
 }
 
+// The prolongation out = xf + P ec on the TMA levels (fine res >= 64), streaming in z: a CTA owns
+// a 64 x 16 fine tile and kProlongCZ coarse planes; the coarse planes cz0 - 1 .. cz1 (rows and
+// columns with a one-node halo) come through a TMA ring and are read once each, into a rolling
+// window of three coarse planes interpolated in x and y. A thread owns the fine 4 x 2 block of one
+// coarse pair in one coarse row (as k_prolong4, same arithmetic), and reads and writes its fine
+// rows with 16-byte accesses.
+constexpr int kProlongCZ = 32;
+template <typename T>
+struct GeoPr {
+  static constexpr int NS = 6;
+  static constexpr int XO = sizeof(T) == 4 ? 4 : 2;   // stage column of coarse cx0 (16-byte aligned start)
+  static constexpr int CW = sizeof(T) == 4 ? 40 : 36;  // staged coarse columns cx0 - XO ..
+  static constexpr int CR = 10;                         // coarse rows cy0 - 1 .. cy0 + 8
+  static constexpr uint32_t SBYTES = CW * CR * sizeof(T);
+  static constexpr uint32_t SSTRIDE = (SBYTES + 127) & ~127u;
+  static constexpr size_t OFF_BAR = (size_t)NS * SSTRIDE;
+  static constexpr size_t BYTES = OFF_BAR + NS * 8 + 16;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreadsR) k_prolong3(const __grid_constant__ CUtensorMap mc, const T* __restrict__ xf,
+                                                        int Lf, T* __restrict__ out, int* __restrict__ err) {
+  typedef GeoPr<T> G;
+  typedef typename Vec2<T>::type V2;
+  constexpr int NS = G::NS, XO = G::XO, CW = G::CW;
+  extern __shared__ __align__(128) unsigned char smem[];
+  auto stage = [&](int st) { return reinterpret_cast<const T*>(smem + (size_t)st * G::SSTRIDE); };  // [CR][CW]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NS * 8);
+  const int rf = 1 << Lf, rc = rf >> 1;
+  const int64_t pf = (int64_t)rf * rf;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  const int x0 = blockIdx.x * 64, y0 = blockIdx.y * 16, cx0 = x0 / 2, cy0 = y0 / 2;
+  const int cz0 = blockIdx.z * kProlongCZ, cz1 = min(cz0 + kProlongCZ, rc);
+  const int nplanes = cz1 - cz0 + 2;  // coarse cz0 - 1 .. cz1
+  if (t == 0) {
+    for (int q = 0; q < NS; ++q) mbar_init(&bar[q], 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int q) {
+    mbar_expect_tx(&bar[q % NS], G::SBYTES);
+    tma_load_3d(const_cast<T*>(stage(q % NS)), &mc, cx0 - XO, cy0 - 1, cz0 - 1 + q, &bar[q % NS]);
+  };
+  if (t == 0)
+    for (int q = 0; q < NS && q < nplanes; ++q) issue(q);
+  // x and y interpolation of staged coarse plane q: B[yo][xo] for fine rows 2ty + yo, columns 4tx + xo
+  auto interp = [&](int q, T B[2][4]) -> bool {
+    const int st = q % NS;
+    bool ok = true;
+    if (!mbar_wait(&bar[st], (uint32_t)(q / NS) & 1u)) {
+      atomicExch(err, 1);
+      *s_abort = 1;
+      ok = false;
+    }
+    T a[3][4];
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy) {
+      const T* row = stage(st) + (ty + dy) * CW + 2 * tx + XO;  // coarse row cy - 1 + dy, column 2tx
+      const V2 e = *reinterpret_cast<const V2*>(row);
+      const T e0 = e.x, e1 = e.y, em = row[-1], ep = row[2];
+      a[dy][0] = T(0.75) * e0 + T(0.25) * em;
+      a[dy][1] = T(0.75) * e0 + T(0.25) * e1;
+      a[dy][2] = T(0.75) * e1 + T(0.25) * e0;
+      a[dy][3] = T(0.75) * e1 + T(0.25) * ep;
+    }
+#pragma unroll
+    for (int xo = 0; xo < 4; ++xo) {
+      B[0][xo] = T(0.75) * a[1][xo] + T(0.25) * a[0][xo];
+      B[1][xo] = T(0.75) * a[1][xo] + T(0.25) * a[2][xo];
+    }
+    __syncthreads();  // stage st is read
+    if (*s_abort) return false;
+    if (t == 0 && q + NS < nplanes) issue(q + NS);
+    return ok;
+  };
+  T B0[2][4], B1[2][4], B2[2][4];  // coarse planes cz - 1, cz, cz + 1
+  int q = 0;                        // the next staged plane to read
+  bool good = interp(q, B1);
+  if (good) good = interp(++q, B2);
+  if (good) ++q;
+  for (int cz = cz0; good && cz < cz1; ++cz, ++q) {
+#pragma unroll
+    for (int yo = 0; yo < 2; ++yo)
+#pragma unroll
+      for (int xo = 0; xo < 4; ++xo) {
+        B0[yo][xo] = B1[yo][xo];
+        B1[yo][xo] = B2[yo][xo];
+      }
+    good = interp(q, B2);
+    if (!good) break;
+#pragma unroll
+    for (int zo = 0; zo < 2; ++zo)
+#pragma unroll
+      for (int yo = 0; yo < 2; ++yo) {
+        const int64_t f = (int64_t)(x0 + 4 * tx) + (int64_t)rf * (y0 + 2 * ty + yo) + pf * (2 * cz + zo);
+        F4<T> v = ld4x(xf + f);
+#pragma unroll
+        for (int xo = 0; xo < 4; ++xo) v.v[xo] += T(0.75) * B1[yo][xo] + T(0.25) * (zo == 0 ? B0 : B2)[yo][xo];
+        st4x(out + f, v);
+      }
+  }
+  if (!good && t == 0) {
+    for (int r = q; r < min(q + NS, nplanes); ++r) mbar_wait(&bar[r % NS], (uint32_t)(r / NS) & 1u);
+  }
+}
+
 // ------------------------------------------------------------------ setup kernels
 // degree-2 basis of one axis at unit coordinate u: nodes c-1, c, c+1 (the oracle's expressions)
 __device__ __forceinline__ void axis2(double u, double h, int64_t& c, double* b) {
@@ -1611,6 +1719,21 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
     }
     return nbx * nby * nz;
   }
+}
+
+// out = xf + P ec (fine level Lf)
+template <typename T>
+void launch_prolong(cudaStream_t s, const T* xf, const T* ec, int Lf, T* out, int* err) {
+  if (Lf >= kTmaMinLevel) {
+    typedef GeoPr<T> G;
+    const int rf = 1 << Lf, rc = rf >> 1;
+    const CUtensorMap m = plane_map<T>(ec, Lf - 1, G::CW, G::CR);
+    const dim3 grid(rf / 64, rf / 16, (rc + kProlongCZ - 1) / kProlongCZ);
+    k_prolong3<T><<<grid, kThreadsR, G::BYTES, s>>>(m, xf, Lf, out, err);
+  } else {
+    k_prolong4<T><<<grid_for(1ull << (3 * (Lf - 1) - 1)), kThreads, 0, s>>>(xf, ec, Lf, out);
+  }
+  PR_CHECK_LAUNCH();
 }
 
 // the restriction of the fine residual rf (level Lf) to the coarse right-hand side fc
@@ -2033,8 +2156,7 @@ struct System2 {
     launch_restrict<T>(s, q.y, q.L, qc.f, err);
     bytes += (double)(q.n + qc.n) * sizeof(T);
     vcycle(li + 1, qc.f, qc.x);
-    k_prolong4<T><<<grid_for(qc.n / 2), kThreads, 0, s>>>(X, qc.x, q.L, q.y);
-    PR_CHECK_LAUNCH();
+    launch_prolong<T>(s, X, qc.x, q.L, q.y, err);
     bytes += (double)(2 * q.n + qc.n) * sizeof(T);
     chebyshev(li, f, X, q.y, false);
   }
@@ -2423,8 +2545,7 @@ double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
         launch_restrict<T>(s, x, (int)D, ec, sys.err);
         break;
       case 6:
-        k_prolong4<T><<<grid_for(nc / 2), kThreads, 0, s>>>(x, ec, (int)D, y);
-        PR_CHECK_LAUNCH();
+        launch_prolong<T>(s, x, ec, (int)D, y, sys.err);
         break;
       case 7:
         k_cheb_first2<T><<<grid_for(n), kThreads, 0, s>>>(f, y, v, (T)0.5);
