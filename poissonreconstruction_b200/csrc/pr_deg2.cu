@@ -1381,28 +1381,33 @@ __global__ void k_pair_keys2(const double* __restrict__ upos, uint64_t P, uint32
 __global__ void k_splat2(const uint32_t* __restrict__ run_key, const uint32_t* __restrict__ run_off, uint64_t T,
                          const uint32_t* __restrict__ sval, const double* __restrict__ phi,
                          const double* __restrict__ unrm, uint64_t P, uint64_t n, double* __restrict__ nf,
-                         double* __restrict__ w) {
+                         double* __restrict__ w) {  // w: the weights alone (nf == nullptr), for the accessor
   for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
     double fx = 0.0, fy = 0.0, fz = 0.0, sw = 0.0;
     for (uint32_t e = run_off[t]; e < run_off[t + 1]; ++e) {
       const uint32_t pk = sval[e];
       const uint32_t p = pk / 27;
       const double wgt = phi[pk];
-      fx = xadd(fx, xmul(unrm[p], wgt));
-      fy = xadd(fy, xmul(unrm[P + p], wgt));
-      fz = xadd(fz, xmul(unrm[2 * P + p], wgt));
+      if (nf) {
+        fx = xadd(fx, xmul(unrm[p], wgt));
+        fy = xadd(fy, xmul(unrm[P + p], wgt));
+        fz = xadd(fz, xmul(unrm[2 * P + p], wgt));
+      }
       sw = xadd(sw, wgt);
+    }
+    const uint32_t node = run_key[t];
+    if (!nf) {
+      w[node] = sw;
+      continue;
     }
     if (sw > 0.0) {
       fx = xdiv(-fx, sw);
       fy = xdiv(-fy, sw);
       fz = xdiv(-fz, sw);
     }
-    const uint32_t node = run_key[t];
     nf[node] = fx;
     nf[n + node] = fy;
     nf[2 * n + node] = fz;
-    w[node] = sw;
   }
 }
 
@@ -1613,6 +1618,36 @@ __global__ void k_nat_to_morton(const T* __restrict__ in, uint32_t D, T* __restr
   const uint64_t n = 1ull << (3 * D), m = (1ull << D) - 1;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     out[morton3((uint32_t)(i & m), (uint32_t)((i >> D) & m), (uint32_t)(i >> (2 * D)))] = in[i];
+}
+
+// The same permutation by 16^3 bricks (D >= 4): an aligned brick is 4096 consecutive Morton codes,
+// so a CTA reads the brick's natural rows (16 contiguous values), reorders them in shared memory
+// and writes one contiguous run.
+template <typename T>
+__global__ void __launch_bounds__(256) k_nat_to_morton_brick(const T* __restrict__ in, uint32_t D, T* __restrict__ out) {
+  __shared__ T s[4096];
+  const uint64_t res = 1ull << D, nb = 1ull << (3 * (D - 4));
+  for (uint64_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    uint32_t bx, by, bz;
+    unmorton3((uint32_t)b, bx, by, bz);
+    const T* src = in + 16 * ((uint64_t)bx + res * ((uint64_t)by + res * (uint64_t)bz));
+#pragma unroll 4
+    for (int i = 0; i < 16; ++i) {
+      const int e = i * 256 + threadIdx.x, lx = e & 15, ly = (e >> 4) & 15, lz = e >> 8;
+      s[morton3((uint32_t)lx, (uint32_t)ly, (uint32_t)lz)] = src[(uint64_t)lx + res * ((uint64_t)ly + res * (uint64_t)lz)];
+    }
+    __syncthreads();
+    T* dst = out + (b << 12);
+#pragma unroll 4
+    for (int i = 0; i < 16; ++i) dst[i * 256 + threadIdx.x] = s[i * 256 + threadIdx.x];
+    __syncthreads();
+  }
+}
+template <typename T>
+void nat_to_morton(cudaStream_t s, const T* in, uint32_t D, T* out) {
+  if (D >= 4) k_nat_to_morton_brick<T><<<(unsigned)std::min<uint64_t>(1ull << (3 * (D - 4)), 148 * 32), 256, 0, s>>>(in, D, out);
+  else k_nat_to_morton<T><<<grid_for(1ull << (3 * D)), kThreads, 0, s>>>(in, D, out);
+  PR_CHECK_LAUNCH();
 }
 template <typename T>
 __global__ void k_morton_to_nat(const T* __restrict__ in, uint32_t D, T* __restrict__ out) {
@@ -2365,12 +2400,10 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
   c->T = T;
   c->P_in = h_nin;
   double* nf = c->buf<double>("d2_nf", 3 * n);
-  double* w = c->buf<double>("d2_w", n);
   PR_CUDA(cudaMemsetAsync(nf, 0, 3 * n * sizeof(double), s));
-  PR_CUDA(cudaMemsetAsync(w, 0, n * sizeof(double), s));
   if (T > 0) {
     k_splat2<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runkey"), c->get<uint32_t>("d2s_runoff"),
-                                                        T, c->get<uint32_t>("d2s_val"), phi64, unrm, P, n, nf, w);
+                                                        T, c->get<uint32_t>("d2s_val"), phi64, unrm, P, n, nf, nullptr);
     PR_CHECK_LAUNCH();
   }
   const double h = 1.0 / (double)(1u << D);
@@ -2493,8 +2526,7 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
   st.converged = st.rel_residual <= target ? 1 : 0;
   st.solve_bytes = bytes;
   double* xm = c->buf<double>("x64", n);
-  k_nat_to_morton<double><<<grid_for(n), kThreads, 0, s>>>(x, D, xm);
-  PR_CHECK_LAUNCH();
+  nat_to_morton<double>(s, x, D, xm);
   c->have_coeffs = true;
 }
 
@@ -2584,14 +2616,25 @@ double deg2_kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int 
 
 // accessors in Morton order (the order of the degree-1 vectors and of the oracle)
 void deg2_rhs_morton(pr_context* c, double* d_out) {
-  k_nat_to_morton<double><<<grid_for(c->n), kThreads, 0, c->stream>>>(c->get<double>("d2_b"), c->D, d_out);
+  nat_to_morton<double>(c->stream, c->get<double>("d2_b"), c->D, d_out);
   PR_CHECK_LAUNCH();
 }
 void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w) {
   k_nat3_to_morton_aos<<<grid_for(c->n), kThreads, 0, c->stream>>>(c->get<double>("d2_nf"), c->D, d_nf3);
   PR_CHECK_LAUNCH();
-  k_nat_to_morton<double><<<grid_for(c->n), kThreads, 0, c->stream>>>(c->get<double>("d2_w"), c->D, d_w);
-  PR_CHECK_LAUNCH();
+  // the per-node weight sums, rebuilt here from the node-sorted pairs (the reconstruction does not
+  // need them): the splat's own loop, so the values are the same
+  cudaStream_t s = c->stream;
+  double* w = c->buf<double>("d2_w", c->n);
+  PR_CUDA(cudaMemsetAsync(w, 0, c->n * sizeof(double), s));
+  if (c->T > 0) {
+    k_splat2<<<grid_for(c->T, 1u << 20), kThreads, 0, s>>>(
+        c->get<uint32_t>("d2s_runkey"), c->get<uint32_t>("d2s_runoff"), c->T, c->get<uint32_t>("d2s_val"),
+        c->get<double>("d2_phi64"), c->get<double>("unrm"), c->P, c->n, nullptr, w);
+    PR_CHECK_LAUNCH();
+  }
+  nat_to_morton<double>(s, w, c->D, d_w);
+  c->release("d2_w");
 }
 // y = A x with the screening, x and y in Morton order (device)
 template <typename T>
@@ -2608,7 +2651,7 @@ void deg2_apply_morton(pr_context* c, const T* d_x, T* d_y) {
   sys.op(0, kOpApply, xn, nullptr, nullptr, yn);
   sys.screen(xn, yn, +1);
   sys.check();
-  k_nat_to_morton<T><<<grid_for(n), kThreads, 0, c->stream>>>(yn, c->D, d_y);
+  nat_to_morton<T>(c->stream, yn, c->D, d_y);
   PR_CHECK_LAUNCH();
 }
 template void deg2_apply_morton<double>(pr_context*, const double*, double*);
