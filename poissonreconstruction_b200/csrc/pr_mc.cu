@@ -444,9 +444,12 @@ __device__ __forceinline__ void mc_build_masks(const double* tile, uint32_t* mas
   }
 }
 // Degree 2: the corner value at grid position p is the sum over the nodes p-1, p per axis of
-// ((x 1/2) 1/2) 1/2, z-major, then y, then x (corner_value2).  The CTA stages nodes
-// [-1, 16]^3 of its block (zeros outside the domain, which add +0 like the skipped terms).
+// ((x 1/2) 1/2) 1/2, z-major, then y, then x (corner_value2).  The CTA stages the terms
+// ((x 1/2) 1/2) 1/2 of nodes [-1, 16]^3 of its block (the same products, formed once per node;
+// zeros outside the domain, which add +0 like the skipped terms).
 constexpr int MCW2 = 18;  // node tile width, tile coordinate = node local + 1
+
+__device__ __forceinline__ double mc_term2(double v) { return xmul(xmul(xmul(v, 0.5), 0.5), 0.5); }
 
 __device__ void mc_load_tile2(double* tile, const double* __restrict__ x, uint32_t blk, int res) {
   uint32_t bx, by, bz;
@@ -455,17 +458,33 @@ __device__ void mc_load_tile2(double* tile, const double* __restrict__ x, uint32
   for (int i = threadIdx.x; i < 4096; i += blockDim.x) {
     uint32_t lx, ly, lz;
     unmorton3((uint32_t)i, lx, ly, lz);
-    tile[((lz + 1) * MCW2 + (ly + 1)) * MCW2 + (lx + 1)] = __ldg(x + base + i);
+    tile[((lz + 1) * MCW2 + (ly + 1)) * MCW2 + (lx + 1)] = mc_term2(__ldg(x + base + i));
   }
-  // the shell: tile coordinates 0 or 17 on some axis
-  for (int i = threadIdx.x; i < MCW2 * MCW2 * MCW2; i += blockDim.x) {
-    const int tx = i % MCW2, ty = (i / MCW2) % MCW2, tz = i / (MCW2 * MCW2);
-    if (tx >= 1 && tx <= 16 && ty >= 1 && ty <= 16 && tz >= 1 && tz <= 16) continue;
+  // the shell, 18^3 - 16^3 = 1736 entries: the z faces (2 x 18 x 18), then the y faces of the
+  // inner z range (2 x 16 x 18), then the x faces of the inner y and z ranges (2 x 16 x 16)
+  for (int i = threadIdx.x; i < 1736; i += blockDim.x) {
+    int tx, ty, tz;
+    if (i < 648) {
+      const int r = i % 324;
+      tz = i < 324 ? 0 : 17;
+      ty = r / 18;
+      tx = r % 18;
+    } else if (i < 1224) {
+      const int j = i - 648, r = j % 288;
+      ty = j < 288 ? 0 : 17;
+      tz = 1 + r / 18;
+      tx = r % 18;
+    } else {
+      const int j = i - 1224, r = j % 256;
+      tx = j < 256 ? 0 : 17;
+      tz = 1 + r / 16;
+      ty = 1 + r % 16;
+    }
     const int gx = (int)bx * 16 + tx - 1, gy = (int)by * 16 + ty - 1, gz = (int)bz * 16 + tz - 1;
     double v = 0.0;
     if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res)
-      v = __ldg(x + morton3((uint32_t)gx, (uint32_t)gy, (uint32_t)gz));
-    tile[i] = v;
+      v = mc_term2(__ldg(x + morton3((uint32_t)gx, (uint32_t)gy, (uint32_t)gz)));
+    tile[(tz * MCW2 + ty) * MCW2 + tx] = v;
   }
 }
 
@@ -480,8 +499,7 @@ __device__ __forceinline__ void mc_build_masks2(const double* tile, uint32_t* ma
 #pragma unroll
         for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-          for (int dx = 0; dx < 2; ++dx)
-            v = xadd(v, xmul(xmul(xmul(tile[((tz + dz) * MCW2 + ty + dy) * MCW2 + tx + dx], 0.5), 0.5), 0.5));
+          for (int dx = 0; dx < 2; ++dx) v = xadd(v, tile[((tz + dz) * MCW2 + ty + dy) * MCW2 + tx + dx]);
       m |= (uint32_t)(v < iso) << tx;
     }
     mask[r] = m;
