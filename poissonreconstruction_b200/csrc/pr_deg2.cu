@@ -11,11 +11,13 @@
 //   wh3 = pw h^3 / 1.5, wg = wh3 / 200 (src/fem_tree.rs:195-200, 276-280).
 //
 // Layout: grid vectors in natural order (x fastest, index x + res (y + res z)).  Every operator
-// is a sum of tensor products of banded 1-D matrices.  One kernel (k_op2) applies a level's
-// operator in a single pass over HBM: a CTA owns 32 x 8 columns and streams up to 64 z planes;
-// per plane it stages the 36 x 12 haloed input in shared memory, filters along x (M and S),
-// then along y (three products) into registers, and keeps a five-plane register window for
-// the z filter.  The epilogue forms A x, f - A x or a Chebyshev smoothing step.
+// is a sum of tensor products of banded 1-D matrices, applied in a single pass over HBM that
+// streams z planes through a CTA and keeps the z filter in registers; the epilogue forms A x,
+// f - A x, a Chebyshev step or a fused CG / refinement update.  Levels with res >= 64 stage their
+// planes with TMA: k_op3r on the finest level (x filter from the stage, y and z in registers),
+// k_op3 on the Galerkin coarse levels (interior and face tiles); smaller levels use k_op2
+// (32 x 8 columns, plain loads into shared memory).  The grid transfers and the right-hand side
+// stream the same way (k_restrict3, k_prolong3, k_rhs3).
 //
 // Solver: conjugate gradients preconditioned by a multigrid V-cycle on K + wg I.  Coarse
 // levels are Galerkin products of the 1-D matrices (P^T X P, P the B2 subdivision
