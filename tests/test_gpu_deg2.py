@@ -168,6 +168,25 @@ def test_small_depths(ctx, depth):
         assert np.linalg.norm(ctx.coefficients() - x_ref) <= COEF_TOL * np.linalg.norm(x_ref)
 
 
+@pytest.mark.parametrize("depth", [7, 8, 9])
+def test_deep_levels_converge(ctx, depth):
+    """Depths beyond the oracle's reach, where the TMA grid transfers and the coarse operators run
+    several z runs per launch (fine levels of 128^3 and more): the V-cycle keeps PCG at the
+    depth-independent iteration count of the shallow depths (9-10 to 1e-10 at depths 5-8), and
+    the mixed and FP64 solutions agree. A wrong transfer or coarse operator cannot pass the FP64
+    residual check with a wrong answer, but it shows here as extra iterations."""
+    pts = cloud("torus")
+    xs = {}
+    for precision in (prb.PR_PRECISION_FP64, prb.PR_PRECISION_MIXED):
+        _, st = ctx.reconstruct(pts, params(depth, 4.0, precision=precision, target_rel_residual=1e-10,
+                                            max_iters=400))
+        assert st.converged == 1 and st.rel_residual <= 1e-10, st
+        assert st.pcg_iterations <= 11, st.pcg_iterations
+        xs[precision] = ctx.coefficients()
+    a, b = xs[prb.PR_PRECISION_FP64], xs[prb.PR_PRECISION_MIXED]
+    assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(a)
+
+
 def test_default_tolerance_error_vs_fp64(ctx):
     """At the default target (1e-6 relative residual) the mixed and the FP64 solves agree with
     each other and with the converged oracle solution to the error that residual allows."""
