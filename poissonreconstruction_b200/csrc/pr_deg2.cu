@@ -1350,33 +1350,39 @@ __device__ __forceinline__ void axis2(double u, double h, int64_t& c, double* b)
 }
 
 // (node, 27 p + k) pairs with the natural node index (sentinel 2^(3D) outside the grid), k =
-// 9 (dz + 1) + 3 (dy + 1) + (dx + 1); basis values (FP64, FP32); count of points with a node
+// 9 (dz + 1) + 3 (dy + 1) + (dx + 1); basis values (FP64, FP32); count of points with a node.
+// One thread per pair (the point's three axis evaluations repeated per pair), so every array is
+// written coalesced; a point has a node in the grid iff [c - 1, c + 1] meets [0, res) on every
+// axis, counted once per block.
 __global__ void k_pair_keys2(const double* __restrict__ upos, uint64_t P, uint32_t D, uint32_t* __restrict__ keys,
                              uint32_t* __restrict__ vals, double* __restrict__ phi64, float* __restrict__ phi32,
                              unsigned long long* __restrict__ nin) {
   const int64_t res = 1ll << D;
   const double h = 1.0 / (double)res;
   const uint32_t sentinel = 1u << (3 * D);
-  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
+  unsigned long long cnt = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 27 * P; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = i / 27;
+    const int k = (int)(i - 27 * p), dx = k % 3, dy = (k / 3) % 3, dz = k / 9;
     int64_t c[3];
     double b[3][3];
     axis2(upos[p], h, c[0], b[0]);
     axis2(upos[P + p], h, c[1], b[1]);
     axis2(upos[2 * P + p], h, c[2], b[2]);
-    bool any = false;
-    for (int k = 0; k < 27; ++k) {
-      const int dx = k % 3, dy = (k / 3) % 3, dz = k / 9;
-      const int64_t x = c[0] + dx - 1, y = c[1] + dy - 1, z = c[2] + dz - 1;
-      const bool ok = x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res;
-      any |= ok;
-      keys[27 * p + k] = ok ? (uint32_t)(x + res * (y + res * z)) : sentinel;
-      vals[27 * p + k] = (uint32_t)(27 * p + k);
-      const double phi = ok ? xmul(xmul(b[0][dx], b[1][dy]), b[2][dz]) : 0.0;
-      phi64[27 * p + k] = phi;
-      phi32[27 * p + k] = (float)phi;
-    }
-    if (any) atomicAdd(nin, 1ull);
+    const int64_t x = c[0] + dx - 1, y = c[1] + dy - 1, z = c[2] + dz - 1;
+    const bool ok = x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res;
+    keys[i] = ok ? (uint32_t)(x + res * (y + res * z)) : sentinel;
+    vals[i] = (uint32_t)i;
+    const double phi = ok ? xmul(xmul(b[0][dx], b[1][dy]), b[2][dz]) : 0.0;
+    phi64[i] = phi;
+    phi32[i] = (float)phi;
+    if (k == 0)
+      cnt += (c[0] + 1 >= 0 && c[0] - 1 < res && c[1] + 1 >= 0 && c[1] - 1 < res && c[2] + 1 >= 0 && c[2] - 1 < res);
   }
+  typedef cub::BlockReduce<unsigned long long, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const unsigned long long tot = BR(tmp).Sum(cnt);
+  if (threadIdx.x == 0 && tot) atomicAdd(nin, tot);
 }
 
 // splat per touched node, points in input order: nf = -(sum phi n) / (sum phi), w = sum phi
@@ -2390,7 +2396,7 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
   float* phi32 = c->buf<float>("d2_phi32", m);
   unsigned long long* nin = c->buf<unsigned long long>("d2_nin", 1);
   PR_CUDA(cudaMemsetAsync(nin, 0, sizeof(unsigned long long), s));
-  k_pair_keys2<<<grid_for(P, 1u << 20), kThreads, 0, s>>>(upos, P, D, kin, vin, phi64, phi32, nin);
+  k_pair_keys2<<<grid_for(m, 1u << 20), kThreads, 0, s>>>(upos, P, D, kin, vin, phi64, phi32, nin);
   PR_CHECK_LAUNCH();
   const uint64_t T = sort_and_segment(c, "d2s", kin, vin, m, D);
   unsigned long long h_nin = 0;
