@@ -1386,6 +1386,15 @@ __global__ void k_pair_keys2(const double* __restrict__ upos, uint64_t P, uint32
 }
 
 // splat per touched node, points in input order: nf = -(sum phi n) / (sum phi), w = sum phi
+// zero the three components of the normal field at the nodes of a previous splat
+__global__ void k_unsplat2(const uint32_t* __restrict__ run_key, uint64_t T, uint64_t n, double* __restrict__ nf) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t node = run_key[t];
+    nf[node] = 0.0;
+    nf[n + node] = 0.0;
+    nf[2 * n + node] = 0.0;
+  }
+}
 __global__ void k_splat2(const uint32_t* __restrict__ run_key, const uint32_t* __restrict__ run_off, uint64_t T,
                          const uint32_t* __restrict__ sval, const double* __restrict__ phi,
                          const double* __restrict__ unrm, uint64_t P, uint64_t n, double* __restrict__ nf,
@@ -2396,6 +2405,17 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
   float* phi32 = c->buf<float>("d2_phi32", m);
   unsigned long long* nin = c->buf<unsigned long long>("d2_nin", 1);
   PR_CUDA(cudaMemsetAsync(nin, 0, sizeof(unsigned long long), s));
+  // the normal field must be zero before the splat: when it still holds only the last splat of
+  // this context (same buffer, same depth), zero those nodes instead of the whole grid (the last
+  // run keys are overwritten by the sort below)
+  double* nf = c->buf<double>("d2_nf", 3 * n);
+  const bool nf_known = c->nf_clean == nf && c->nf_clean_D == D;
+  if (nf_known && c->nf_dirty_T > 0) {
+    k_unsplat2<<<grid_for(c->nf_dirty_T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runkey"), c->nf_dirty_T,
+                                                                       n, nf);
+    PR_CHECK_LAUNCH();
+  }
+  c->nf_clean = nullptr;  // until the splat below has completed
   k_pair_keys2<<<grid_for(m, 1u << 20), kThreads, 0, s>>>(upos, P, D, kin, vin, phi64, phi32, nin);
   PR_CHECK_LAUNCH();
   const uint64_t T = sort_and_segment(c, "d2s", kin, vin, m, D);
@@ -2407,13 +2427,15 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
   c->sync();
   c->T = T;
   c->P_in = h_nin;
-  double* nf = c->buf<double>("d2_nf", 3 * n);
-  PR_CUDA(cudaMemsetAsync(nf, 0, 3 * n * sizeof(double), s));
+  if (!nf_known) PR_CUDA(cudaMemsetAsync(nf, 0, 3 * n * sizeof(double), s));
   if (T > 0) {
     k_splat2<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runkey"), c->get<uint32_t>("d2s_runoff"),
                                                         T, c->get<uint32_t>("d2s_val"), phi64, unrm, P, n, nf, nullptr);
     PR_CHECK_LAUNCH();
   }
+  c->nf_clean = nf;
+  c->nf_clean_D = D;
+  c->nf_dirty_T = T;
   const double h = 1.0 / (double)(1u << D);
   double* b = c->buf<double>("d2_b", n);
   deg2_rhs(c, nf, b, D, h);

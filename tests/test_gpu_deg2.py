@@ -68,6 +68,21 @@ def test_setup(ctx, name, depth, pw):
     assert np.max(np.abs(b_g - b)) <= FP64_TOL * np.max(np.abs(b))
 
 
+def test_setup_reuses_the_normal_field():
+    """A context that reconstructs again at the same depth zeroes only the nodes of its previous
+    splat: a second cloud (and the first one again, and a depth change) gets the same normal field
+    and right-hand side as a fresh context."""
+    with prb.Context(0) as c:
+        for name, depth in [("torus", 6), ("ellipsoid", 6), ("sphere", 5), ("torus", 6), ("torus", 6)]:
+            c.solve(cloud(name), params(depth, 4.0))
+            t, _, _ = oracle_tree(name, depth, 4.0)
+            nf, w = t.normal_field()
+            nf_g, w_g = c.normal_field()
+            assert np.array_equal(nf_g, nf) and np.array_equal(w_g, w), (name, depth)
+            b, b_g = t.rhs(), c.rhs()
+            assert np.max(np.abs(b_g - b)) <= FP64_TOL * np.max(np.abs(b)), (name, depth)
+
+
 @pytest.mark.parametrize("name,depth,pw", CASES)
 def test_operator(ctx, name, depth, pw):
     ctx.solve(cloud(name), params(depth, pw))
