@@ -364,6 +364,7 @@ struct Op3Args {
   int nbx, nby;    // tiles per axis (x: 64 columns, y: 8 rows)
   int all;         // EDGE: the grid enumerates every tile, not only the face tiles
   int ox, oy;      // interior: tile of block (i, j) is (i + ox, j + oy)
+  int oz;          // interior: z run of block k is k + oz
   int* err;
   double* dot;     // optional per-CTA partials: kOpApply x . out, kOpCheb f . out, kOpApplyD d . out
   int dot_base;    // index of this launch's first partial
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(kThreads) k_op3(const __grid_constant__ CUtens
     by = blockIdx.y + A.oy;
   }
   const int x0 = bx * TXP, y0 = by * TY;
-  const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
+  const int z0 = (blockIdx.z + A.oz) * kZChunk3, z1 = min(z0 + kZChunk3, res);
   const int gx = x0 + 2 * p, gy = y0 + ty;  // res >= 64: every column is inside the grid
   const int nplanes = z1 - z0 + 4;
   const int ngroups = (nplanes + NS - 1) / NS;  // planes past z1 + 1 read zeros and emit nothing
@@ -809,8 +810,8 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   const int res = 1 << lv.L;
   const int64_t plane = (int64_t)res * res;
   const int t = threadIdx.x, p = t & 31, ry = RY * (t >> 5);  // tile rows ry, ry + 1; staged ry .. ry + 5
-  const int x0 = blockIdx.x * TXP, y0 = blockIdx.y * TY;
-  const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
+  const int x0 = (blockIdx.x + A.ox) * TXP, y0 = (blockIdx.y + A.oy) * TY;
+  const int z0 = (blockIdx.z + A.oz) * kZChunk3, z1 = min(z0 + kZChunk3, res);
   const int gx = x0 + 2 * p;
   const int nplanes = z1 - z0 + 4;
   const int ngroups = (nplanes + NS - 1) / NS;
@@ -1733,7 +1734,7 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
       attr_r = true;
     }
     Op3Args<T> e = a;
-    e.ox = e.oy = 0;
+    e.ox = e.oy = e.oz = 0;
     e.dot_base = 0;
     k_op3r<T, MODE><<<dim3(a.nbx, a.nby, nz), kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
     PR_CHECK_LAUNCH();
@@ -1748,7 +1749,7 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
     }
     const int nbx = a.nbx, nby = a.nby;
     Op3Args<T> e = a;
-    e.ox = e.oy = 0;
+    e.ox = e.oy = e.oz = 0;
     e.dot_base = 0;
     if (a.edge == 0) {  // every row acts as the interior row: one launch of the register-window variant
       k_op3r<T, MODE><<<dim3(nbx, nby, nz), kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
@@ -1760,9 +1761,33 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
     e.all = split ? 0 : 1;
     if (split) {
       e.ox = e.oy = 1;
-      k_op3<T, MODE, false><<<dim3(nbx - 2, nby - 2, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
-      PR_CHECK_LAUNCH();
-      e.dot_base = (nbx - 2) * (nby - 2) * nz;
+      // z runs of the interior tiles whose staged planes (and, with edge <= 6, the tiles' halo rows
+      // and columns) all act as the interior row run k_op3r, the others k_op3; with fewer than five
+      // runs the extra launches cost more than they save
+      const int res = nbx * G::TXP;
+      int zlo = nz, zhi = nz;
+      if (a.edge <= 6 && nz >= 5) {
+        zlo = 0;
+        while (zlo < nz && zlo * kZChunk3 - 2 < a.edge) ++zlo;
+        zhi = zlo;
+        while (zhi < nz && std::min((zhi + 1) * kZChunk3, res) + 2 <= res - a.edge) ++zhi;
+      }
+      const int ni = (nbx - 2) * (nby - 2);
+      auto run = [&](int z_begin, int z_end, bool regs) {
+        if (z_end <= z_begin) return;
+        e.oz = z_begin;
+        const dim3 g(nbx - 2, nby - 2, z_end - z_begin);
+        if (regs) k_op3r<T, MODE><<<g, kThreadsR, GR::BYTES, s>>>(mx, mf, mp, out, e);
+        else k_op3<T, MODE, false><<<g, kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
+        PR_CHECK_LAUNCH();
+        e.dot_base += ni * (z_end - z_begin);
+      };
+      run(0, zlo, false);
+      run(zlo, zhi, true);
+      run(zhi, nz, false);
+      e.oz = 0;
+      e.ox = e.oy = 0;
+      e.dot_base = ni * nz;
       k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
       PR_CHECK_LAUNCH();
     } else {
@@ -2079,7 +2104,7 @@ struct System2 {
     if (tma) {
       PR_REQUIRE(q.L >= kTmaMinLevel, PR_ERR_INTERNAL, "TMA operator below its minimum level");
       typedef Geo3<T> G;
-      Op3Args<T> A;
+      Op3Args<T> A{};  // every field zero unless set below
       A.lv = v;
       for (int d = 0; d < 5; ++d) {
         A.im[d] = (T)q.im[d];

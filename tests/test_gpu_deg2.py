@@ -202,6 +202,17 @@ def test_deep_levels_converge(ctx, depth):
     assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(a)
 
 
+def test_depth10_converges(ctx):
+    """Depth 10 (2^30 unknowns), whose 512^3 coarse level splits its interior tiles into boundary
+    z runs (k_op3) and middle z runs (k_op3r): the same iteration bound in both precisions."""
+    pts = cloud("torus")
+    for precision in (prb.PR_PRECISION_FP64, prb.PR_PRECISION_MIXED):
+        _, st = ctx.reconstruct(pts, params(10, 4.0, precision=precision, target_rel_residual=1e-10,
+                                            max_iters=400))
+        assert st.converged == 1 and st.rel_residual <= 1e-10, st
+        assert st.pcg_iterations <= 11, st.pcg_iterations
+
+
 def test_default_tolerance_error_vs_fp64(ctx):
     """At the default target (1e-6 relative residual) the mixed and the FP64 solves agree with
     each other and with the converged oracle solution to the error that residual allows."""
