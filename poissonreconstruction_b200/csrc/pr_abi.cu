@@ -284,9 +284,10 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   st.time_solve = t3 - t2;
   st.peak_device_bytes = (double)c->peak_bytes;
   if (!extract) return;
-  const double* x = c->get<double>("x64");
-  double iso = pr::stage_iso(c, x);
-  pr::stage_extract(c, c->D, x, iso, true, c->degree);
+  const bool nat = c->degree == 2;  // degree 2: straight from the solver's natural order
+  const double* x = nat ? c->d2_xnat : c->get<double>("x64");
+  double iso = pr::stage_iso(c, x, nat);
+  pr::stage_extract(c, c->D, x, iso, true, c->degree, nat);
   c->sync();
   double t4 = now_s();
   st.time_extract = t4 - t3;
@@ -705,6 +706,7 @@ int pr_ctx_get_coefficients(pr_context* c, double* out) {
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
     PR_REQUIRE(c->have_coeffs, PR_ERR_STATE, "no solved coefficients");
+    pr::coeffs_morton(c);
     copy_dev_to_host(c, "x64", out, c->n);
   });
 }
@@ -800,7 +802,7 @@ int pr_ctx_evaluate(pr_context* c, const double* coeffs, const double* pts3, uin
       dx = t;
     } else {
       PR_REQUIRE(c->have_coeffs, PR_ERR_STATE, "no solved coefficients");
-      dx = c->get<double>("x64");
+      dx = pr::coeffs_morton(c);
     }
     double* dp = c->buf<double>("acc_pts", 3 * n);
     double* dout = c->buf<double>("acc_out", n);

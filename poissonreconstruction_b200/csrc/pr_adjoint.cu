@@ -276,7 +276,7 @@ void adjoint_backward(pr_context* c, const double* d_q3, uint64_t K, const doubl
   double* qu = c->buf<double>("adj_qu", 3 * K);
   k_query_unit<<<grid_for(K), kThreads, 0, s>>>(d_q3, K, M, qu);
   PR_CHECK_LAUNCH();
-  const double* x = c->get<double>("x64");
+  const double* x = coeffs_morton(c);
   evaluate_points(c, D, x, qu, 3, K, d_chi);
   double* g = c->buf<double>("adj_g", K);
   k_upstream<<<grid_for(K), kThreads, 0, s>>>(d_chi, d_dl, K, g);

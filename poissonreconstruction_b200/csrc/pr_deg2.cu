@@ -2580,9 +2580,20 @@ void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
   st.rel_residual = bn > 0.0 ? rn / bn : 0.0;
   st.converged = st.rel_residual <= target ? 1 : 0;
   st.solve_bytes = bytes;
-  double* xm = c->buf<double>("x64", n);
-  nat_to_morton<double>(s, x, D, xm);
+  // the extraction reads the natural order; the Morton copy is made when an accessor asks for it
+  c->d2_xnat = x;
+  c->x64_ready = false;
   c->have_coeffs = true;
+}
+
+const double* coeffs_morton(pr_context* c) {
+  if (c->degree == 2 && !c->x64_ready) {
+    PR_REQUIRE(c->d2_xnat != nullptr, PR_ERR_INTERNAL, "degree-2 coefficients missing");
+    double* xm = c->buf<double>("x64", c->n);
+    nat_to_morton<double>(c->stream, c->d2_xnat, c->D, xm);
+    c->x64_ready = true;
+  }
+  return c->get<double>("x64");
 }
 
 namespace {

@@ -143,6 +143,10 @@ struct pr_context {
   const void* nf_clean = nullptr;
   uint32_t nf_clean_D = 0;
   uint64_t nf_dirty_T = 0;
+  // degree 2: the solved coefficients in natural order (one of the solver's buffers) and whether
+  // their Morton copy "x64" is up to date (made on demand by coeffs_morton)
+  const double* d2_xnat = nullptr;
+  bool x64_ready = true;
   pr_params params{};             // parameters of the last reconstruction
 
   template <typename T>
@@ -214,10 +218,14 @@ void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w);
 template <typename T>
 void deg2_apply_morton(pr_context* c, const T* d_x, T* d_y);
 double deg2_kernel_bench(pr_context* c, int kid, uint32_t depth, int precision, int reps, double* bytes);
+// the solved coefficients in Morton order ("x64"), permuted from the degree-2 solver's order first
+// when needed
+const double* coeffs_morton(pr_context* c);
 // extract (pr_mc.cu); `degree` selects the node functions (1: the crate's, 2: quadratic)
-double stage_iso(pr_context* c, const double* d_x64);
+// natural: degree-2 coefficients in the solver's natural order instead of Morton order
+double stage_iso(pr_context* c, const double* d_x64, bool natural = false);
 void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform,
-                   int degree = 1);
+                   int degree = 1, bool natural = false);
 void evaluate_points(pr_context* c, uint32_t depth, const double* d_x64, const double* d_pts, uint64_t stride,
                      uint64_t n, double* d_out, int degree = 1);
 

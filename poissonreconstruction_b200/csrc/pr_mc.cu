@@ -104,9 +104,19 @@ __device__ __forceinline__ double corner_value(const double* __restrict__ x, int
   return v;
 }
 
+// Degree-2 coefficients come in Morton order (as every grid vector of the API) or, inside the
+// reconstruction, in the natural order of the degree-2 solver (x + res (y + res z)). The extraction
+// templates take DEG = 1 (the crate's basis), 2 (quadratic, Morton order) or 3 (quadratic, natural
+// order); the arithmetic of 2 and 3 is the same.
+template <bool NAT>
+__device__ __forceinline__ uint64_t node_index(uint32_t x, uint32_t y, uint32_t z, uint32_t D) {
+  return NAT ? (uint64_t)x + ((uint64_t)y << D) + ((uint64_t)z << (2 * D)) : (uint64_t)morton3(x, y, z);
+}
+
 // Degree-2 evaluation (the extension's quadratic node functions): per axis s = u / h, c = floor(s),
 // t = s - c, weights (1-t)^2/2, (-2t^2 + 2t + 1)/2, t^2/2 of nodes c-1, c, c+1; nodes outside the
 // grid are skipped; terms summed z-major, then y, then x, as ((x_j b_x) b_y) b_z.
+template <bool NAT>
 __device__ double eval_fem2(const double* __restrict__ x, uint32_t D, double px, double py, double pz) {
   const int64_t res = 1ll << D;
   const double h = 1.0 / (double)res;
@@ -133,7 +143,8 @@ __device__ double eval_fem2(const double* __restrict__ x, uint32_t D, double px,
       for (int i = 0; i < 3; ++i) {
         const int64_t xx = c[0] + i - 1;
         if (xx < 0 || xx >= res) continue;
-        v = xadd(v, xmul(xmul(xmul(x[morton3((uint32_t)xx, (uint32_t)y, (uint32_t)z)], b[0][i]), b[1][j]), b[2][k]));
+        v = xadd(v, xmul(xmul(xmul(x[node_index<NAT>((uint32_t)xx, (uint32_t)y, (uint32_t)z, D)], b[0][i]), b[1][j]),
+                         b[2][k]));
       }
     }
   }
@@ -143,7 +154,9 @@ __device__ double eval_fem2(const double* __restrict__ x, uint32_t D, double px,
 // eval_fem2 at the integer grid position (kx,ky,kz): t = 0 on every axis, so the weights are
 // 1/2, 1/2, 0 for nodes k-1, k, k+1; the zero-weight terms add +-0 and are left out (the sum
 // never holds -0), which keeps the result identical.
-__device__ __forceinline__ double corner_value2(const double* __restrict__ x, int res, int kx, int ky, int kz) {
+template <bool NAT>
+__device__ __forceinline__ double corner_value2(const double* __restrict__ x, uint32_t D, int kx, int ky, int kz) {
+  const int res = 1 << D;
   double v = 0.0;
 #pragma unroll
   for (int dz = -1; dz <= 0; ++dz) {
@@ -157,7 +170,7 @@ __device__ __forceinline__ double corner_value2(const double* __restrict__ x, in
       for (int dx = -1; dx <= 0; ++dx) {
         const int xx = kx + dx;
         if (xx < 0 || xx >= res) continue;
-        v = xadd(v, xmul(xmul(xmul(x[morton3((uint32_t)xx, (uint32_t)y, (uint32_t)z)], 0.5), 0.5), 0.5));
+        v = xadd(v, xmul(xmul(xmul(x[node_index<NAT>((uint32_t)xx, (uint32_t)y, (uint32_t)z, D)], 0.5), 0.5), 0.5));
       }
     }
   }
@@ -166,19 +179,20 @@ __device__ __forceinline__ double corner_value2(const double* __restrict__ x, in
 
 template <int DEG>
 __device__ __forceinline__ double eval_deg(const double* __restrict__ x, uint32_t D, double px, double py, double pz) {
-  return DEG == 2 ? eval_fem2(x, D, px, py, pz) : eval_fem(x, D, px, py, pz);
+  return DEG >= 2 ? eval_fem2<DEG == 3>(x, D, px, py, pz) : eval_fem(x, D, px, py, pz);
 }
 
 template <int DEG>
-__device__ __forceinline__ uint32_t cell_case(const double* __restrict__ x, int res, uint32_t cell, double iso,
+__device__ __forceinline__ uint32_t cell_case(const double* __restrict__ x, uint32_t D, uint32_t cell, double iso,
                                               double* cv) {
+  const int res = 1 << D;
   uint32_t ox, oy, oz;
   unmorton3(cell, ox, oy, oz);
   uint32_t mc = 0;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int kx = (int)ox + c_co[k][0], ky = (int)oy + c_co[k][1], kz = (int)oz + c_co[k][2];
-    cv[k] = DEG == 2 ? corner_value2(x, res, kx, ky, kz) : corner_value(x, res, kx, ky, kz);
+    cv[k] = DEG >= 2 ? corner_value2<DEG == 3>(x, D, kx, ky, kz) : corner_value(x, res, kx, ky, kz);
     if (cv[k] < iso) mc |= 1u << k;
   }
   return mc;
@@ -239,13 +253,12 @@ __global__ void k_iso_final(const double* __restrict__ part, int nb, double* __r
 // ------------------------------------------------------------------ marching cubes
 template <int DEG>
 __global__ void k_mc_count(const double* __restrict__ x, uint32_t D, double iso, uint32_t* __restrict__ blockcnt) {
-  const int res = 1 << D;
   const uint64_t n = 1ull << (3 * D);
   uint64_t cell = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   int active = 0;
   if (cell < n) {
     double cv[8];
-    uint32_t mc = cell_case<DEG>(x, res, (uint32_t)cell, iso, cv);
+    uint32_t mc = cell_case<DEG>(x, D, (uint32_t)cell, iso, cv);
     active = (mc != 0u && mc != 255u);
   }
   typedef cub::BlockReduce<int, kThreads> BR;
@@ -258,14 +271,13 @@ template <int DEG>
 __global__ void k_mc_compact(const double* __restrict__ x, uint32_t D, double iso, const uint32_t* __restrict__ blockoff,
                              uint32_t* __restrict__ acell, uint8_t* __restrict__ acase, uint32_t* __restrict__ nedge,
                              uint32_t* __restrict__ ntri) {
-  const int res = 1 << D;
   const uint64_t n = 1ull << (3 * D);
   uint64_t cell = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   uint32_t mc = 0;
   int active = 0;
   if (cell < n) {
     double cv[8];
-    mc = cell_case<DEG>(x, res, (uint32_t)cell, iso, cv);
+    mc = cell_case<DEG>(x, D, (uint32_t)cell, iso, cv);
     active = (mc != 0u && mc != 255u);
   }
   typedef cub::BlockScan<int, kThreads> BS;
@@ -292,7 +304,7 @@ __global__ void k_mc_vertices(const double* __restrict__ x, uint32_t D, double i
   for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < A; a += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t cell = acell[a];
     double cv[8];
-    uint32_t mc = cell_case<DEG>(x, res, cell, iso, cv);
+    uint32_t mc = cell_case<DEG>(x, D, cell, iso, cv);
     uint32_t em = edge_mask(mc);
     uint32_t ox, oy, oz;
     unmorton3(cell, ox, oy, oz);
@@ -451,9 +463,22 @@ constexpr int MCW2 = 18;  // node tile width, tile coordinate = node local + 1
 
 __device__ __forceinline__ double mc_term2(double v) { return xmul(xmul(xmul(v, 0.5), 0.5), 0.5); }
 
+template <bool NAT>
 __device__ void mc_load_tile2(double* tile, const double* __restrict__ x, uint32_t blk, int res) {
   uint32_t bx, by, bz;
   unmorton3(blk, bx, by, bz);
+  if (NAT) {  // natural order: the tile's rows are contiguous in memory (18 values per row)
+    const uint32_t D = 31 - __clz(res);
+    for (int i = threadIdx.x; i < MCW2 * MCW2 * MCW2; i += blockDim.x) {
+      const int tx = i % MCW2, ty = (i / MCW2) % MCW2, tz = i / (MCW2 * MCW2);
+      const int gx = (int)bx * 16 + tx - 1, gy = (int)by * 16 + ty - 1, gz = (int)bz * 16 + tz - 1;
+      double v = 0.0;
+      if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res)
+        v = mc_term2(__ldg(x + node_index<true>((uint32_t)gx, (uint32_t)gy, (uint32_t)gz, D)));
+      tile[i] = v;
+    }
+    return;
+  }
   const uint64_t base = (uint64_t)blk << 12;
   for (int i = threadIdx.x; i < 4096; i += blockDim.x) {
     uint32_t lx, ly, lz;
@@ -511,8 +536,8 @@ __device__ __forceinline__ void mc_block_masks(double* tile, uint32_t* mask, con
                                                uint32_t blk, int res, double iso) {
   uint32_t bx, by, bz;
   unmorton3(blk, bx, by, bz);
-  if (DEG == 2) {
-    mc_load_tile2(tile, x, blk, res);
+  if (DEG >= 2) {
+    mc_load_tile2<DEG == 3>(tile, x, blk, res);
     __syncthreads();
     mc_build_masks2(tile, mask, iso);
   } else {
@@ -533,7 +558,7 @@ __device__ __forceinline__ uint32_t mc_mask_case(const uint32_t* mask, int lx, i
 template <int DEG>
 __global__ void __launch_bounds__(256) k_mc_block_count(const double* __restrict__ x, uint32_t D, double iso,
                                                         uint32_t* __restrict__ blockcnt) {
-  __shared__ double tile[DEG == 2 ? MCW2 * MCW2 * MCW2 : MCW * MCW * MCW];
+  __shared__ double tile[DEG >= 2 ? MCW2 * MCW2 * MCW2 : MCW * MCW * MCW];
   __shared__ uint32_t mask[MCW * MCW];
   const int res = 1 << D;
   const uint32_t blk = blockIdx.x;
@@ -560,7 +585,7 @@ __global__ void __launch_bounds__(256) k_mc_block_emit(const double* __restrict_
                                                        const uint32_t* __restrict__ blockoff,
                                                        uint32_t* __restrict__ acell, uint8_t* __restrict__ acase,
                                                        uint32_t* __restrict__ nedge, uint32_t* __restrict__ ntri) {
-  __shared__ double tile[DEG == 2 ? MCW2 * MCW2 * MCW2 : MCW * MCW * MCW];
+  __shared__ double tile[DEG >= 2 ? MCW2 * MCW2 * MCW2 : MCW * MCW * MCW];
   __shared__ uint32_t mask[MCW * MCW];
   const int res = 1 << D;
   const uint32_t blk = ablk[blockIdx.x];
@@ -632,14 +657,16 @@ void evaluate_points(pr_context* c, uint32_t D, const double* d_x64, const doubl
   PR_CHECK_LAUNCH();
 }
 
-double stage_iso(pr_context* c, const double* d_x64) {
+double stage_iso(pr_context* c, const double* d_x64, bool natural) {
   const uint64_t P = c->P;
   int nb = (int)std::min<uint64_t>(kDotBlocks, (P + kThreads - 1) / kThreads);
   if (nb < 1) nb = 1;
   double* part = c->buf<double>("iso_part", 2 * (size_t)nb);
   double* out = c->buf<double>("iso_out", 1);
-  if (c->degree == 2) k_iso_partial<2><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, c->get<double>("upos"), P, part);
-  else k_iso_partial<1><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, c->get<double>("upos"), P, part);
+  const double* up = c->get<double>("upos");
+  if (c->degree == 2 && natural) k_iso_partial<3><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, up, P, part);
+  else if (c->degree == 2) k_iso_partial<2><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, up, P, part);
+  else k_iso_partial<1><<<nb, kThreads, 0, c->stream>>>(d_x64, c->D, up, P, part);
   PR_CHECK_LAUNCH();
   k_iso_final<<<1, 32, 0, c->stream>>>(part, nb, out);
   PR_CHECK_LAUNCH();
@@ -649,7 +676,8 @@ double stage_iso(pr_context* c, const double* d_x64) {
   return sum / (double)P;
 }
 
-void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool back_transform, int degree) {
+void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool back_transform, int degree,
+                   bool natural) {
   const uint64_t n = 1ull << (3 * D);
   cudaStream_t s = c->stream;
   c->nv = c->nt = 0;
@@ -667,7 +695,8 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     uint32_t* flag = c->buf<uint32_t>("mc_flag", (size_t)nblk + 1);
     uint32_t* fpos = c->buf<uint32_t>("mc_fpos", (size_t)nblk + 1);
     uint32_t* ablk = c->buf<uint32_t>("mc_ablk", (size_t)nblk);
-    if (degree == 2) k_mc_block_count<2><<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
+    if (degree == 2 && natural) k_mc_block_count<3><<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
+    else if (degree == 2) k_mc_block_count<2><<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
     else k_mc_block_count<1><<<nblk, 256, 0, s>>>(x, D, iso, blockcnt);
     PR_CHECK_LAUNCH();
     PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
@@ -691,14 +720,16 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     acase = c->buf<uint8_t>("mc_acase", A);
     nedge = c->buf<uint32_t>("mc_nedge", A + 1);
     ntri = c->buf<uint32_t>("mc_ntri", A + 1);
-    if (degree == 2) k_mc_block_emit<2><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    if (degree == 2 && natural) k_mc_block_emit<3><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    else if (degree == 2) k_mc_block_emit<2><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
     else k_mc_block_emit<1><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
     PR_CHECK_LAUNCH();
   } else {
     const unsigned nblk = (unsigned)((n + kThreads - 1) / kThreads);
     uint32_t* blockcnt = c->buf<uint32_t>("mc_blockcnt", (size_t)nblk + 1);
     uint32_t* blockoff = c->buf<uint32_t>("mc_blockoff", (size_t)nblk + 1);
-    if (degree == 2) k_mc_count<2><<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
+    if (degree == 2 && natural) k_mc_count<3><<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
+    else if (degree == 2) k_mc_count<2><<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
     else k_mc_count<1><<<nblk, kThreads, 0, s>>>(x, D, iso, blockcnt);
     PR_CHECK_LAUNCH();
     PR_CUDA(cudaMemsetAsync(blockcnt + nblk, 0, sizeof(uint32_t), s));
@@ -715,7 +746,8 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     acase = c->buf<uint8_t>("mc_acase", A);
     nedge = c->buf<uint32_t>("mc_nedge", A + 1);
     ntri = c->buf<uint32_t>("mc_ntri", A + 1);
-    if (degree == 2) k_mc_compact<2><<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
+    if (degree == 2 && natural) k_mc_compact<3><<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
+    else if (degree == 2) k_mc_compact<2><<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
     else k_mc_compact<1><<<nblk, kThreads, 0, s>>>(x, D, iso, blockoff, acell, acase, nedge, ntri);
     PR_CHECK_LAUNCH();
   }
@@ -745,7 +777,8 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
   uint32_t* sidb = c->buf<uint32_t>("mc_sidb", E);
   int* err = c->buf<int>("mc_err", 1);
   PR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  if (degree == 2) k_mc_vertices<2><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
+  if (degree == 2 && natural) k_mc_vertices<3><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
+  else if (degree == 2) k_mc_vertices<2><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
   else k_mc_vertices<1><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
   PR_CHECK_LAUNCH();
 
