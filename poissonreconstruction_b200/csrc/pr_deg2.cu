@@ -17,7 +17,7 @@
 // planes with TMA: k_op3r on the finest level (x filter from the stage, y and z in registers),
 // k_op3 on the Galerkin coarse levels (interior and face tiles); smaller levels use k_op2
 // (32 x 8 columns, plain loads into shared memory).  The grid transfers and the right-hand side
-// stream the same way (k_restrict3, k_prolong3, k_rhs3).
+// stream the same way (k_restrict3, k_prolong3, k_rhs3r).
 //
 // Solver: conjugate gradients preconditioned by a multigrid V-cycle on K + wg I.  Coarse
 // levels are Galerkin products of the 1-D matrices (P^T X P, P the B2 subdivision
@@ -1429,22 +1429,13 @@ __global__ void k_splat2(const uint32_t* __restrict__ run_key, const uint32_t* _
   }
 }
 
-// b = h^2 sum_a (G_a M M) nf_a on the finest level (res >= 64), TMA-fed like k_op3: a CTA owns
-// 64 x 8 columns (x pairs per thread) and streams up to kZChunk3 planes; four stages, each the three
-// haloed component planes (zero fill outside the grid = the truncated rows).  m is symmetric and
-// g antisymmetric (g[2] = 0), so each 5-tap filter is two pair sums or differences.
+// b = h^2 sum_a (G_a M M) nf_a on the finest level (res >= 64): a CTA owns 64 x 8 columns (x pairs
+// per thread) and streams up to kZChunk3 planes of the three haloed component planes (zero fill
+// outside the grid = the truncated rows).  m is symmetric and g antisymmetric (g[2] = 0), so each
+// 5-tap filter is two pair sums or differences.
 struct RhsCoef {
   double g[5], m[5], h2;
   int* err;
-};
-struct GeoR {
-  static constexpr int NS = 4;
-  static constexpr int TXP = 64;
-  static constexpr int BW = 68;                                      // from x0 - 2 (16-byte aligned)
-  static constexpr uint32_t PBYTES = BW * SH * sizeof(double);       // one component plane
-  static constexpr size_t OFF_U = (size_t)NS * 3 * PBYTES;
-  static constexpr size_t OFF_BAR = OFF_U + 3 * (size_t)SH * TXP * sizeof(double);
-  static constexpr size_t BYTES = OFF_BAR + NS * 8 + 16;
 };
 
 __device__ __forceinline__ double fsym(const double* v, const double* c) {
@@ -1454,106 +1445,123 @@ __device__ __forceinline__ double fanti(const double* v, const double* c) {
   return c[0] * (v[0] - v[4]) + c[1] * (v[1] - v[3]);
 }
 
-__global__ void __launch_bounds__(kThreads) k_rhs3(const __grid_constant__ CUtensorMap m0,
-                                                   const __grid_constant__ CUtensorMap m1,
-                                                   const __grid_constant__ CUtensorMap m2, int L,
-                                                   const __grid_constant__ RhsCoef k, double* __restrict__ b) {
-  typedef GeoR G;
-  constexpr int NS = G::NS, BW = G::BW, TXP = G::TXP;
+// The right-hand side with the y and z filters in registers (the k_op3r structure): 4 warps on
+// the 64 x 8 tile, each thread two output rows; a three-deep TMA ring of the three haloed component
+// planes; per plane and component the thread filters its six staged rows in x straight from the
+// stage and adds their y filter at once (so one component's rows are live at a time), then
+// scatters (M_y G_x n_x + G_y M_x n_y, M_y M_x n_z) into the five output planes they touch with
+// M_z and G_z.
+struct GeoRr {
+  static constexpr int NSS = 3;  // stages
+  static constexpr int BW = 68;  // from x0 - 2 (16-byte aligned)
+  static constexpr uint32_t PBYTES = BW * SH * sizeof(double);  // one component plane
+  static constexpr uint32_t SBYTES = 3 * PBYTES;
+  static_assert(SBYTES % 128 == 0 && PBYTES % 128 == 0, "stage alignment");
+  static constexpr size_t OFF_BAR = (size_t)NSS * SBYTES;
+  static constexpr size_t BYTES = OFF_BAR + NSS * 8 + 16;
+};
+__global__ void __launch_bounds__(kThreadsR) k_rhs3r(const __grid_constant__ CUtensorMap m0,
+                                                     const __grid_constant__ CUtensorMap m1,
+                                                     const __grid_constant__ CUtensorMap m2, int L,
+                                                     const __grid_constant__ RhsCoef k, double* __restrict__ b) {
+  typedef GeoRr G;
+  constexpr int NSS = G::NSS, BW = G::BW, NW = 5;  // NW: output planes a staged plane touches
   extern __shared__ __align__(128) unsigned char smem[];
-  double(*s_in)[3][SH][BW] = reinterpret_cast<double(*)[3][SH][BW]>(smem);
-  double(*s_u)[SH][TXP] = reinterpret_cast<double(*)[SH][TXP]>(smem + G::OFF_U);
+  auto comp = [&](int st, int a) {
+    return reinterpret_cast<const double*>(smem + (size_t)st * G::SBYTES + a * G::PBYTES);
+  };
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
-  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NS * 8);
+  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NSS * 8);
   const int res = 1 << L;
   const int64_t plane = (int64_t)res * res;
-  const int t = threadIdx.x, p = t & 31, ty = t >> 5;
-  const int x0 = blockIdx.x * TXP, y0 = blockIdx.y * TY;
+  const int t = threadIdx.x, p = t & 31, ry = 2 * (t >> 5);
+  const int x0 = blockIdx.x * 64, y0 = blockIdx.y * TY;
   const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
   const int nplanes = z1 - z0 + 4;
+  const int ngroups = (nplanes + NW - 1) / NW;
   if (t == 0) {
-    for (int q = 0; q < NS; ++q) mbar_init(&bar[q], 1);
+    for (int q = 0; q < NSS; ++q) mbar_init(&bar[q], 1);
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  const int nissue = ngroups * NW;  // planes past z1 + 1 read zeros and emit nothing
   auto issue = [&](int it) {
-    const int q = it % NS, zin = z0 - 2 + it;
-    mbar_expect_tx(&bar[q], 3 * G::PBYTES);
-    tma_load_3d(&s_in[q][0][0][0], &m0, x0 - 2, y0 - 2, zin, &bar[q]);
-    tma_load_3d(&s_in[q][1][0][0], &m1, x0 - 2, y0 - 2, zin, &bar[q]);
-    tma_load_3d(&s_in[q][2][0][0], &m2, x0 - 2, y0 - 2, zin, &bar[q]);
+    const int st = it % NSS, zin = z0 - 2 + it;
+    mbar_expect_tx(&bar[st], G::SBYTES);
+    tma_load_3d(const_cast<double*>(comp(st, 0)), &m0, x0 - 2, y0 - 2, zin, &bar[st]);
+    tma_load_3d(const_cast<double*>(comp(st, 1)), &m1, x0 - 2, y0 - 2, zin, &bar[st]);
+    tma_load_3d(const_cast<double*>(comp(st, 2)), &m2, x0 - 2, y0 - 2, zin, &bar[st]);
   };
   if (t == 0)
-    for (int it = 0; it < min(NS, nplanes); ++it) issue(it);
-  double wa[2][5], wb[2][5];
+    for (int it = 0; it < NSS; ++it) issue(it);
+  double2 acc[2][NW];  // [output row][slot of output plane z0 - 4 + it, it mod 5]
 #pragma unroll
   for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int q = 0; q < 5; ++q) wa[j][q] = wb[j][q] = 0.0;
-  double* op = b + (int64_t)(x0 + 2 * p) + (int64_t)res * (y0 + ty) + plane * (z0 - 4);
+    for (int q = 0; q < NW; ++q) acc[j][q] = make_double2(0.0, 0.0);
+  double* op = b + (int64_t)(x0 + 2 * p) + (int64_t)res * (y0 + ry) + plane * (z0 - 4);
   int it = 0;
   bool stop = false;
-  for (; it < nplanes; ++it) {
-    const int q = it % NS;
-    if (!mbar_wait(&bar[q], (uint32_t)(it / NS) & 1u)) {
-      atomicExch(k.err, 1);
-      *s_abort = 1;
-    }
-    // x filters (G on component 0, M on 1 and 2) of rows ty and ty + 8
+  for (int g = 0; g < ngroups; ++g) {
 #pragma unroll
-    for (int rr = 0; rr < 2; ++rr) {
-      const int r = ty + 8 * rr;
-      if (r < SH) {
+    for (int kk = 0; kk < NW; ++kk) {
+      it = g * NW + kk;
+      const int st = it % NSS;
+      if (!mbar_wait(&bar[st], (uint32_t)(it / NSS) & 1u)) {
+        atomicExch(k.err, 1);
+        *s_abort = 1;
+      }
+      double wa[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, wb[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // [row][column]
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const double* row = &s_in[q][a][r][2 * p];
+      for (int a = 0; a < 3; ++a) {
+        double u[6][2];  // x filter of the staged rows ry .. ry + 5 (G on n_x, M on n_y, n_z)
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          const double* row = comp(st, a) + (ry + r) * BW + 2 * p;
           const double2 v0 = *reinterpret_cast<const double2*>(row), v1 = *reinterpret_cast<const double2*>(row + 2),
                         v2 = *reinterpret_cast<const double2*>(row + 4);
           const double v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
-          const double o0 = a == 0 ? fanti(v, k.g) : fsym(v, k.m);
-          const double o1 = a == 0 ? fanti(v + 1, k.g) : fsym(v + 1, k.m);
-          *reinterpret_cast<double2*>(&s_u[a][r][2 * p]) = make_double2(o0, o1);
+          u[r][0] = a == 0 ? fanti(v, k.g) : fsym(v, k.m);
+          u[r][1] = a == 0 ? fanti(v + 1, k.g) : fsym(v + 1, k.m);
         }
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int l = 0; l < 2; ++l) {
+            const double col[5] = {u[j][l], u[j + 1][l], u[j + 2][l], u[j + 3][l], u[j + 4][l]};
+            if (a == 0) wa[j][l] += fsym(col, k.m);        // M_y (G_x n_x)
+            else if (a == 1) wa[j][l] += fanti(col, k.g);  // G_y (M_x n_y)
+            else wb[j][l] = fsym(col, k.m);                // M_y (M_x n_z)
+          }
       }
-    }
-    __syncthreads();  // stage q is read, s_u written
-    if (*s_abort) {
-      stop = true;
-      break;
-    }
-    if (t == 0 && it + NS < nplanes) issue(it + NS);
-    double col[3][2][5];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int d = 0; d < 5; ++d) {
-        const double2 u = *reinterpret_cast<const double2*>(&s_u[a][ty + d][2 * p]);
-        col[a][0][d] = u.x;
-        col[a][1][d] = u.y;
+      __syncthreads();  // stage st is read
+      if (*s_abort) {
+        stop = true;
+        break;
       }
-    __syncthreads();  // s_u is read before the next plane writes it
+      if (t == 0 && it + NSS < nissue) issue(it + NSS);
+      // z: plane zin is tap 4 - e of output plane zin - 2 + e (slot (kk + e) mod 5): M_z on wa, G_z on wb
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
+      for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int q2 = 0; q2 < 4; ++q2) {
-        wa[j][q2] = wa[j][q2 + 1];
-        wb[j][q2] = wb[j][q2 + 1];
+        for (int e = 0; e < NW; ++e) {
+          const double cm = k.m[4 - e], cg = k.g[4 - e];
+          double2& s2 = acc[j][(kk + e) % NW];
+          if (e == NW - 1) s2 = make_double2(cm * wa[j][0] + cg * wb[j][0], cm * wa[j][1] + cg * wb[j][1]);
+          else s2 = make_double2(s2.x + (cm * wa[j][0] + cg * wb[j][0]), s2.y + (cm * wa[j][1] + cg * wb[j][1]));
+        }
+      if ((unsigned)(it - 4) < (unsigned)(z1 - z0)) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          *reinterpret_cast<double2*>(op + (int64_t)j * res) = make_double2(k.h2 * acc[j][kk].x, k.h2 * acc[j][kk].y);
       }
-      wa[j][4] = fsym(col[0][j], k.m) + fanti(col[1][j], k.g);  // (G M) x + (M G) y, then M along z
-      wb[j][4] = fsym(col[2][j], k.m);                          // (M M) z, then G along z
+      op += plane;
     }
-    const int zo = z0 - 4 + it;
-    if (zo >= z0) {
-      double o[2];
-#pragma unroll
-      for (int j = 0; j < 2; ++j) o[j] = k.h2 * (fsym(wa[j], k.m) + fanti(wb[j], k.g));
-      *reinterpret_cast<double2*>(op) = make_double2(o[0], o[1]);
-    }
-    op += plane;
+    if (stop) break;
   }
   if (stop && t == 0)
-    for (int q = it; q < min(it + NS, nplanes); ++q) mbar_wait(&bar[q % NS], (uint32_t)(q / NS) & 1u);
+    for (int q = it; q < min(it + NSS, nissue); ++q) mbar_wait(&bar[q % NSS], (uint32_t)(q / NSS) & 1u);
 }
 
 // screening right-hand side: b[node] += (wh3 / 2) sum of phi over the node's pairs
@@ -2395,14 +2403,14 @@ void deg2_rhs(pr_context* c, const double* nf, double* b, uint32_t D, double h) 
   }
   static bool attr = false;
   if (!attr) {
-    PR_CUDA(cudaFuncSetAttribute(k_rhs3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GeoR::BYTES));
+    PR_CUDA(cudaFuncSetAttribute(k_rhs3r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GeoRr::BYTES));
     attr = true;
   }
-  const CUtensorMap m0 = plane_map<double>(nf, (int)D, GeoR::BW, SH);
-  const CUtensorMap m1 = plane_map<double>(nf + n, (int)D, GeoR::BW, SH);
-  const CUtensorMap m2 = plane_map<double>(nf + 2 * n, (int)D, GeoR::BW, SH);
-  const dim3 grid(res / GeoR::TXP, res / TY, (res + kZChunk3 - 1) / kZChunk3);
-  k_rhs3<<<grid, kThreads, GeoR::BYTES, s>>>(m0, m1, m2, (int)D, k, b);
+  const CUtensorMap m0 = plane_map<double>(nf, (int)D, GeoRr::BW, SH);
+  const CUtensorMap m1 = plane_map<double>(nf + n, (int)D, GeoRr::BW, SH);
+  const CUtensorMap m2 = plane_map<double>(nf + 2 * n, (int)D, GeoRr::BW, SH);
+  const dim3 grid(res / 64, res / TY, (res + kZChunk3 - 1) / kZChunk3);
+  k_rhs3r<<<grid, kThreadsR, GeoRr::BYTES, s>>>(m0, m1, m2, (int)D, k, b);
   PR_CHECK_LAUNCH();
   int h_err = 0;
   PR_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
