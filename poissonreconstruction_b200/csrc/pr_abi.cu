@@ -462,6 +462,12 @@ int pr_context_destroy(pr_context* c) {
     for (cudaEvent_t e : c->copy_events)
       if (e) cudaEventDestroy(e);
     c->copy_events.clear();
+    if (c->side) {
+      cudaStreamSynchronize(c->side);
+      cudaStreamDestroy(c->side);
+      cudaEventDestroy(c->ev_fork);
+      cudaEventDestroy(c->ev_join);
+    }
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->own_stream) cudaStreamDestroy(c->stream);

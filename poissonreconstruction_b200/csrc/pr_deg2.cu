@@ -1730,8 +1730,8 @@ constexpr int kTmaMinLevel = 6;  // res >= 64: full 64-wide x tiles (k_op3)
 // over the interior tiles and the face tiles
 // returns the number of CTAs (= dot partials written when a.dot is set)
 template <typename T, int MODE>
-int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, const CUtensorMap& mp, T* out,
-               const Op3Args<T>& a, int nz) {
+int launch_op3(pr_context* c, cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, const CUtensorMap& mp,
+               T* out, const Op3Args<T>& a, int nz) {
   typedef Geo3<T> G;
   typedef Geo3R<T> GR;
   if constexpr (MODE == kOpRefine) {  // a level without boundary rows only
@@ -1790,14 +1790,22 @@ int launch_op3(cudaStream_t s, const CUtensorMap& mx, const CUtensorMap& mf, con
         PR_CHECK_LAUNCH();
         e.dot_base += ni * (z_end - z_begin);
       };
+      // the face tiles (disjoint outputs and partial slots) run beside the interior launches on
+      // the side stream, forked from and joined back to s
+      Op3Args<T> ef = e;
+      ef.oz = 0;
+      ef.ox = ef.oy = 0;
+      ef.dot_base = ni * nz;
+      cudaStream_t s2 = c->side_stream();
+      PR_CUDA(cudaEventRecord(c->ev_fork, s));
+      PR_CUDA(cudaStreamWaitEvent(s2, c->ev_fork, 0));
+      k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s2>>>(mx, mf, mp, out, ef);
+      PR_CHECK_LAUNCH();
       run(0, zlo, false);
       run(zlo, zhi, true);
       run(zhi, nz, false);
-      e.oz = 0;
-      e.ox = e.oy = 0;
-      e.dot_base = ni * nz;
-      k_op3<T, MODE, true><<<dim3(2 * nbx + 2 * (nby - 2), 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
-      PR_CHECK_LAUNCH();
+      PR_CUDA(cudaEventRecord(c->ev_join, s2));
+      PR_CUDA(cudaStreamWaitEvent(s, c->ev_join, 0));
     } else {
       k_op3<T, MODE, true><<<dim3(nbx * nby, 1, nz), kThreads, G::BYTES, s>>>(mx, mf, mp, out, e);
       PR_CHECK_LAUNCH();
@@ -2146,15 +2154,15 @@ struct System2 {
       const CUtensorMap mp = refine ? plane_map<float>(fu->e32, q.L, 72, SH)
                                     : (xp ? plane_map<T>(xp, q.L, G::TXP, TY) : mx);
       switch (mode) {
-        case kOpApply: nparts = launch_op3<T, kOpApply>(s, mx, mf, mp, out, A, nz); break;
-        case kOpResid: nparts = launch_op3<T, kOpResid>(s, mx, mf, mp, out, A, nz); break;
-        case kOpCheb: nparts = launch_op3<T, kOpCheb>(s, mx, mf, mp, out, A, nz); break;
-        case kOpChebF: nparts = launch_op3<T, kOpChebF>(s, mx, mf, mp, out, A, nz); break;
-        case kOpChebPF: nparts = launch_op3<T, kOpChebPF>(s, mx, mf, mp, out, A, nz); break;
+        case kOpApply: nparts = launch_op3<T, kOpApply>(c, s, mx, mf, mp, out, A, nz); break;
+        case kOpResid: nparts = launch_op3<T, kOpResid>(c, s, mx, mf, mp, out, A, nz); break;
+        case kOpCheb: nparts = launch_op3<T, kOpCheb>(c, s, mx, mf, mp, out, A, nz); break;
+        case kOpChebF: nparts = launch_op3<T, kOpChebF>(c, s, mx, mf, mp, out, A, nz); break;
+        case kOpChebPF: nparts = launch_op3<T, kOpChebPF>(c, s, mx, mf, mp, out, A, nz); break;
         case kOpRefine:
-          if constexpr (sizeof(T) == 8) nparts = launch_op3<T, kOpRefine>(s, mx, mf, mp, out, A, nz);
+          if constexpr (sizeof(T) == 8) nparts = launch_op3<T, kOpRefine>(c, s, mx, mf, mp, out, A, nz);
           break;
-        default: nparts = launch_op3<T, kOpApplyD>(s, mx, mf, mp, out, A, nz); break;
+        default: nparts = launch_op3<T, kOpApplyD>(c, s, mx, mf, mp, out, A, nz); break;
       }
     } else {
       PR_REQUIRE(mode <= kOpCheb, PR_ERR_INTERNAL, "fused Chebyshev modes need the TMA operator");

@@ -147,6 +147,18 @@ struct pr_context {
   // their Morton copy "x64" is up to date (made on demand by coeffs_morton)
   const double* d2_xnat = nullptr;
   bool x64_ready = true;
+  // a second stream for independent launches of one pass (made on first use), with the events that
+  // fork it from and join it back to `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t side_stream() {
+    if (!side) {
+      PR_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      PR_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+      PR_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    }
+    return side;
+  }
   pr_params params{};             // parameters of the last reconstruction
 
   template <typename T>
