@@ -1736,11 +1736,7 @@ int launch_op3(pr_context* c, cudaStream_t s, const CUtensorMap& mx, const CUten
   typedef Geo3R<T> GR;
   if constexpr (MODE == kOpRefine) {  // a level without boundary rows only
     PR_REQUIRE(a.edge == 0, PR_ERR_INTERNAL, "the fused refinement needs a level without boundary rows");
-    static bool attr_r = false;
-    if (!attr_r) {
-      PR_CUDA(cudaFuncSetAttribute(k_op3r<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR::BYTES));
-      attr_r = true;
-    }
+    allow_smem(k_op3r<T, MODE>, GR::BYTES);
     Op3Args<T> e = a;
     e.ox = e.oy = e.oz = 0;
     e.dot_base = 0;
@@ -1748,13 +1744,9 @@ int launch_op3(pr_context* c, cudaStream_t s, const CUtensorMap& mx, const CUten
     PR_CHECK_LAUNCH();
     return a.nbx * a.nby * nz;
   } else {
-    static bool attr = false;  // once per instantiation
-    if (!attr) {
-      PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
-      PR_CUDA(cudaFuncSetAttribute(k_op3<T, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES));
-      PR_CUDA(cudaFuncSetAttribute(k_op3r<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR::BYTES));
-      attr = true;
-    }
+    allow_smem(k_op3<T, MODE, false>, G::BYTES);
+    allow_smem(k_op3<T, MODE, true>, G::BYTES);
+    allow_smem(k_op3r<T, MODE>, GR::BYTES);
     const int nbx = a.nbx, nby = a.nby;
     Op3Args<T> e = a;
     e.ox = e.oy = e.oz = 0;
@@ -2409,11 +2401,7 @@ void deg2_rhs(pr_context* c, const double* nf, double* b, uint32_t D, double h) 
     PR_CHECK_LAUNCH();
     return;
   }
-  static bool attr = false;
-  if (!attr) {
-    PR_CUDA(cudaFuncSetAttribute(k_rhs3r, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GeoRr::BYTES));
-    attr = true;
-  }
+  allow_smem(k_rhs3r, GeoRr::BYTES);
   const CUtensorMap m0 = plane_map<double>(nf, (int)D, GeoRr::BW, SH);
   const CUtensorMap m1 = plane_map<double>(nf + n, (int)D, GeoRr::BW, SH);
   const CUtensorMap m2 = plane_map<double>(nf + 2 * n, (int)D, GeoRr::BW, SH);

@@ -6,8 +6,11 @@
 
 #include <chrono>
 #include <map>
+#include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/poisson_recon.h"
@@ -253,6 +256,21 @@ double dot64(pr_context* c, const double* a, const double* b, uint64_t n);
 // adjoint (pr_adjoint.cu): gradients of a loss on chi at model-space queries (device arrays)
 void adjoint_backward(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
                       double* d_dpos, double* d_dnrm, pr_adjoint_stats& st);
+
+// dynamic shared memory beyond 48 KB needs a per-kernel opt-in on each device: set once per
+// (kernel, device), safe from several host threads
+template <typename K>
+void allow_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+  if (done.count(key)) return;
+  PR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done.insert(key);
+}
 
 inline double now_seconds() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();

@@ -1297,18 +1297,6 @@ DevCoef<T> dev_coef(const LevelCoef& L, const T* table) {
 
 inline int tile_for(uint32_t D) { return D >= 4 ? 16 : 8; }
 
-// dynamic shared memory beyond 48 KB needs a per-kernel opt-in (set once per kernel)
-template <typename K>
-void allow_smem(K kernel, size_t bytes) {
-  static std::mutex mu;
-  static std::set<const void*> done;
-  std::lock_guard<std::mutex> g(mu);
-  const void* key = reinterpret_cast<const void*>(kernel);
-  if (done.count(key)) return;
-  PR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  done.insert(key);
-}
-
 template <typename T, int TB, int MODE, bool DOT, bool FWD>
 void launch_smooth(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const DevCoef<T>& k,
                    double* part) {
