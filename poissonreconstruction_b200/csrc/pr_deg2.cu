@@ -1671,7 +1671,8 @@ __global__ void __launch_bounds__(256) k_nat_to_morton_brick(const T* __restrict
 }
 template <typename T>
 void nat_to_morton(cudaStream_t s, const T* in, uint32_t D, T* out) {
-  if (D >= 4) k_nat_to_morton_brick<T><<<(unsigned)std::min<uint64_t>(1ull << (3 * (D - 4)), 148 * 32), 256, 0, s>>>(in, D, out);
+  if (D >= 4)
+    k_nat_to_morton_brick<T><<<(unsigned)std::min<uint64_t>(1ull << (3 * (D - 4)), 148 * 32), 256, 0, s>>>(in, D, out);
   else k_nat_to_morton<T><<<grid_for(1ull << (3 * D)), kThreads, 0, s>>>(in, D, out);
   PR_CHECK_LAUNCH();
 }
@@ -2170,7 +2171,8 @@ struct System2 {
       bytes += (double)q.n * (sizeof(T) * (fu->xzero ? 3 : 4) + 8);
       return nparts;
     }
-    const int vecs = mode == kOpApplyD ? 4 + (fu->xmode == 2 ? 2 : fu->xmode) : (mode == kOpApply || mode == kOpChebF ? 2 : (mode == kOpCheb && xp ? 4 : 3));
+    const int vecs = mode == kOpApplyD ? 4 + (fu->xmode == 2 ? 2 : fu->xmode)
+                                       : (mode == kOpApply || mode == kOpChebF ? 2 : (mode == kOpCheb && xp ? 4 : 3));
     bytes += (double)q.n * sizeof(T) * vecs;
     return nparts;
   }

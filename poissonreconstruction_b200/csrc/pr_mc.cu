@@ -720,8 +720,10 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
     acase = c->buf<uint8_t>("mc_acase", A);
     nedge = c->buf<uint32_t>("mc_nedge", A + 1);
     ntri = c->buf<uint32_t>("mc_ntri", A + 1);
-    if (degree == 2 && natural) k_mc_block_emit<3><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
-    else if (degree == 2) k_mc_block_emit<2><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    if (degree == 2 && natural)
+      k_mc_block_emit<3><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
+    else if (degree == 2)
+      k_mc_block_emit<2><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
     else k_mc_block_emit<1><<<hv[1], 256, 0, s>>>(x, D, iso, ablk, blockoff, acell, acase, nedge, ntri);
     PR_CHECK_LAUNCH();
   } else {
@@ -777,8 +779,10 @@ void stage_extract(pr_context* c, uint32_t D, const double* x, double iso, bool 
   uint32_t* sidb = c->buf<uint32_t>("mc_sidb", E);
   int* err = c->buf<int>("mc_err", 1);
   PR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  if (degree == 2 && natural) k_mc_vertices<3><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
-  else if (degree == 2) k_mc_vertices<2><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
+  if (degree == 2 && natural)
+    k_mc_vertices<3><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
+  else if (degree == 2)
+    k_mc_vertices<2><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
   else k_mc_vertices<1><<<grid_for(A), kThreads, 0, s>>>(x, D, iso, acell, A, eoff, pos, k1, k2, sid, E, err);
   PR_CHECK_LAUNCH();
 
