@@ -262,13 +262,19 @@ uint64_t pr_kernel_launches(uint64_t* primitive_calls);
  * holds the free device memory (a raw cudaMalloc would fail or fragment it), or a
  * latency-bound loop that must not pay for the device-wide synchronisation of
  * cudaMalloc/cudaFree.  Every input and the output are caller device pointers:
- * d_coefficients (res^3 FP64 values in the FEM index order, res = 2^depth), d_points3 (n
+ * d_coefficients (res^3 FP64 values, res = 2^depth: the coefficients of the crate's linear
+ * (degree-1) basis in the FEM index order, i.e. Morton order with x in bit 0, as
+ * pr_ctx_get_coefficients returns them for a degree-1 reconstruction; degree-2 coefficients are
+ * NOT accepted — the call cannot tell them apart and would return a wrong value), d_points3 (n
  * unit-cube points, x y z each), d_iso (1 double: the mean of the implicit function over the
- * points, as in src/reconstructor.rs:56).  Enqueued on `stream` (NULL = default stream), no
+ * points, as in src/reconstructor.rs:56; the same double as pr_stats.iso_value of a degree-1
+ * reconstruction of these points).  Enqueued on `stream` (NULL = default stream), no
  * synchronisation.  Per-block partial sums live in a fixed 18,944-byte __device__ array that
  * each GPU loading the library keeps until exit; the first call on a device (with that
  * device current) resolves its address — make that first call before any stream capture.
- * All calls share the array: calls whose kernels overlap on the GPU race.  Limits:
+ * All calls share the array: calls whose kernels overlap on the GPU race.  The resolved address
+ * is cached per device; after cudaDeviceReset in the calling process it is stale, so do not call
+ * this function after resetting a device.  Limits:
  * 1 <= n <= 2^28 points, depth 1..10; anything else returns PR_ERR_INVALID_ARGUMENT. */
 int pr_iso_value_noalloc(uint32_t depth, const double* d_coefficients, const double* d_points3, uint64_t n,
                          double* d_iso, void* stream);

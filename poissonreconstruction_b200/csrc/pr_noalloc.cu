@@ -9,9 +9,14 @@
 // passes device pointers for every input and for the output, and the partial sums live in
 // a fixed file-scope __device__ array that every GPU loading this library keeps until exit.
 //
-// The arithmetic (per-point evaluation, block-level Neumaier sums over a fixed grid, the
-// final compensated combine) is the same as the iso value computed inside pr_reconstruct,
-// so for the same coefficients and points both return the same double.
+// Only the crate's linear (degree-1) basis is evaluated, on coefficients in the FEM index
+// order (Morton, x in bit 0).  The arithmetic (per-point evaluation, block-level Neumaier sums
+// over the same fixed grid of at most 1184 blocks, the final compensated combine, one correctly
+// rounded division by n) is the same as the iso value computed inside a degree-1
+// pr_reconstruct, so for the same coefficients and points both return the same double.
+//
+// The device address of the scratch array is resolved once per device and cached; a
+// cudaDeviceReset in the calling process invalidates it (the header says so).
 #include <mutex>
 
 #include "pr_internal.cuh"
@@ -143,13 +148,14 @@ int scratch_address(double** out) {
 
 extern "C" {
 
-// Iso value = mean of the implicit function of `d_coefficients` (res^3 FP64 values in the
-// FEM index order, res = 2^depth) over n unit-cube points (d_points3: n x 3 doubles), written
+// Iso value = mean of the implicit function of `d_coefficients` (res^3 FP64 coefficients of the
+// degree-1 basis in the FEM index order, res = 2^depth) over n unit-cube points (d_points3: n x 3 doubles), written
 // to d_iso[0]; enqueued on `stream` (NULL = the default stream) without synchronising and
 // without allocating.  The first call on a device resolves the scratch address on the
 // current device; make that first call before any stream capture.  Calls share one scratch
 // array per device: calls whose kernels overlap on the GPU (different streams without
-// ordering) race.  Accepts 1 <= n <= 2^28 points and depth 1..10.
+// ordering) race.  The cached scratch address is stale after a cudaDeviceReset in this process.
+// Accepts 1 <= n <= 2^28 points and depth 1..10.
 int pr_iso_value_noalloc(uint32_t depth, const double* d_coefficients, const double* d_points3, uint64_t n,
                          double* d_iso, void* stream) {
   if (!d_coefficients || !d_points3 || !d_iso) {

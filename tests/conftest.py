@@ -35,6 +35,16 @@ def pytest_collection_modifyitems(config, items):
 
 
 @pytest.fixture(scope="session")
+def reference_src():
+    """The reference crate's `src/` directory, named by the environment variable
+    PR_REFERENCE_SRC; tests that read the crate's sources skip when it is unset or absent."""
+    path = os.environ.get("PR_REFERENCE_SRC", "")
+    if not path or not os.path.isdir(path):
+        pytest.skip("reference sources not available (set PR_REFERENCE_SRC to the crate's src/)")
+    return path
+
+
+@pytest.fixture(scope="session")
 def ctx():
     import poissonreconstruction_b200 as prb
     c = prb.Context(0)

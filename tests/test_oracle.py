@@ -10,8 +10,6 @@ import oracle
 from poissonreconstruction_b200 import synthetic
 from tests.adjoint_cases import adjoint_case, fd_coordinates, fd_gradient
 
-REF = "/root/reference/src"
-
 
 # ---------------------------------------------------------------- ported crate unit tests
 def test_cg_simple():
@@ -184,9 +182,9 @@ def test_mc_triangle_count_matches_table():
     assert t.max() < len(v) and len(np.unique(t)) == len(v)
 
 
-def test_edge_table_derivation_matches_reference():
+def test_edge_table_derivation_matches_reference(reference_src):
     """The crate's EDGE_TABLE (src/fem_tree.rs:13-30) equals the corner-sign derivation."""
-    path = os.path.join(REF, "fem_tree.rs")
+    path = os.path.join(reference_src, "fem_tree.rs")
     if not os.path.exists(path):
         pytest.skip("reference sources not present")
     m = re.search(r"const EDGE_TABLE: \[u16; 256\] = \[(.*?)\];", open(path).read(), re.S)
@@ -194,9 +192,9 @@ def test_edge_table_derivation_matches_reference():
     assert [oracle.mc_edge_mask(c) for c in range(256)] == et
 
 
-def test_tri_table_matches_reference():
+def test_tri_table_matches_reference(reference_src):
     """The packed table equals the crate's TRI_TABLE (src/tri_table.inl)."""
-    path = os.path.join(REF, "tri_table.inl")
+    path = os.path.join(reference_src, "tri_table.inl")
     if not os.path.exists(path):
         pytest.skip("reference sources not present")
     rows = re.findall(r"\[([-0-9, ]+)\]", open(path).read())
