@@ -1,28 +1,39 @@
 #!/usr/bin/env python
 """Benchmark of the reconstruction hot path on B200.
 
-Workload: 2,000,000 oriented points on a torus (R = 1.0, r = 0.35, area-uniform, position
-noise 0.002, normals tipped by a 0.05 rad Gaussian, FP32 storage), depth 10 (1.07e9 FEM
-nodes), screening weight 4.0, scale 1.1; FP32 multigrid-preconditioned CG with FP64
-residual refinement to a relative residual <= 1e-6.  One step = one full reconstruction
-(transform, splat, right-hand side, solve, iso value, marching cubes) of that cloud.
+Workload (default): 2,000,000 oriented points on a torus (R = 1.0, r = 0.35, area-uniform,
+position noise 0.002, normals tipped by a 0.05 rad Gaussian, FP32 storage), depth 10 (1.07e9
+FEM nodes), quadratic B-splines (degree 2), screening weight 4.0, scale 1.1; FP32
+multigrid-preconditioned CG with FP64 residual refinement to a relative residual <= 1e-6.
+One step = one full reconstruction (transform, splat, right-hand side, solve, iso value,
+marching cubes) of that cloud.
 
   value      points/s with the points already in HBM (pr_ctx_reconstruct_device)
   e2e        points/s through pr_ctx_reconstruct with pinned host input and the mesh copied
              back to host memory
   solve_gbs  algorithmic bytes of the solve / solve time; the FP64 solve of the same system
              is timed beside it (fp64_* keys)
-  roofline   the solver kernel with the largest share of the step (the FP32 post-smoothing
-             sweep fused with the prolongation and r.z) timed alone with CUDA events on the
-             library's stream; the other fine-level solver kernels are reported under "kernels"
-  cpu_baseline  the CPU oracle (the crate's schedule restated in C++) at depth 7 on the same
-             cloud, extrapolated to depth 10 (x512 nodes): the crate itself needs ~1 TB of
-             host RAM at depth 10
+  roofline   the kernel with the largest share of the step in the ncu launch list: the FP32
+             Chebyshev smoothing step of the degree-2 finest level (k_op3r, mode kOpCheb),
+             timed alone with CUDA events on the library's stream; every other finest-level
+             pass (CG direction pass, fused first Chebyshev steps, residual, transfers, the
+             FP64 refinement step, the plain A x) is under "kernels"
+  accuracy   coefficient relative L2 of the mixed and FP64 solutions against each other and
+             against an FP64 solve to 1e-10, the largest mixed target meeting 1e-6, and the
+             vertex distance between the two meshes over the bbox diagonal (untimed)
+  cpu_baseline  measured on the host: iterations of the crate's CG loop (oracle restatement,
+             FP64, all host threads) on the same depth-10 degree-2 system, one iteration timed
+             per sample and reported as points / (one iteration's time), an upper bound on the
+             CPU path's points/s; the crate's own CSR path needs ~1 TB of host RAM at depth 10
+
+--impl reference times the same CPU leg, one CG iteration per step.  --config 1 runs the plain
+method instead (100,000 sphere points, depth 8, the crate's cascade with cg_iters 8) end to end
+in both arms.
 
 Multi-GPU: one process per GPU (torchrun); each rank reconstructs its own cloud (replicas,
 weak scaling, no collective on the data path); value = all ranks' points / max rank time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1|2]
 """
 import argparse
 import json
@@ -67,6 +78,10 @@ def parse():
                     help="instead of the default workload: the batched workload with this many clouds "
                          "(256 = the full batch), timed through pr_reconstruct_batch")
     ap.add_argument("--concurrency", type=int, default=4, help="--batch: contexts (streams) used")
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2],
+                    help="2: the depth-10 mixed-precision workload (default); 1: the plain method (100k sphere "
+                         "points, depth 8, the crate's cascade with cg_iters 8), end to end in both arms")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the coefficient / vertex error block")
     ap.add_argument("--only-device", action="store_true",
                     help="warm-up + timed device-resident steps only (for profiler launch lists)")
     return ap.parse_args()
@@ -172,24 +187,68 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-CPU_DEPTH = 7
+def _host_gb():
+    try:
+        import psutil
+        return psutil.virtual_memory().available / 1e9
+    except ImportError:
+        return float("inf")
 
 
-def cpu_sample(pts, depth_target):
-    """The crate's schedule (oracle restatement, all host threads) on the full cloud at
-    depth 7; per-node work scales with the node count, so the depth-10 time is
-    extrapolated by 8^(depth_target - 7)."""
-    import oracle
-    t0 = time.perf_counter()
-    v, t, st, _ = oracle.reconstruct(pts, depth=CPU_DEPTH, point_weight=4.0, solve_mode=0, cg_iters=500,
-                                     cg_accuracy=1e-3)
-    dt = time.perf_counter() - t0
-    scale = 8.0 ** (depth_target - CPU_DEPTH)
-    return {"value": len(pts) / (dt * scale), "unit": "points/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": "oracle (C++ FP64 restatement of the crate's cascade schedule) on the full %d-point cloud "
-                      "at depth %d: %.2f s measured, extrapolated x%d to depth %d; the crate's own CSR path "
-                      "needs ~1 TB host RAM at depth 10" % (len(pts), CPU_DEPTH, dt, int(scale), depth_target),
-            "seconds_measured": dt}
+class CpuCG:
+    """The CPU leg: the crate's CG loop (solve_cg, src/solvers.rs:20-69), FP64, all host threads,
+    on the oracle's matrix-free operator of this cloud's system (degree 2: stiffness of the quadratic
+    basis + screening of every point; degree 1: the crate's own assemble_system entries), from
+    x = 0 with a seeded random right-hand side (an iteration costs the same for any b).  One
+    step() = one CG iteration over the full grid, timed with the host clock.  The depth is the
+    benchmark's unless the host lacks the memory (about 6.5 vectors of 8^depth doubles)."""
+
+    def __init__(self, pts, depth, degree, pw=4.0):
+        import oracle
+        self.depth = depth
+        need = 7.0 * 8.0 ** depth * 8 / 1e9
+        while depth > 6 and _host_gb() < need + 4.0:
+            depth -= 1
+            need /= 8.0
+        self.run_depth = depth
+        self.degree = degree
+        unit, _ = oracle.to_unit(pts)
+        t0 = time.perf_counter()
+        if degree == 2:
+            self.tree = oracle.Tree2(depth, unit, pw)
+            self.tree.release_field()
+            b = np.random.default_rng(20260102).standard_normal(8 ** depth)
+            self.cg = oracle.CG2(self.tree, b)
+        else:
+            self.tree = oracle.Tree(depth, unit)
+            self.tree.release_field()
+            b = np.random.default_rng(20260102).standard_normal(8 ** depth)
+            self.cg = oracle.CG1(self.tree, b, pw)
+        del b
+        self.setup_s = time.perf_counter() - t0
+        self.points = len(pts)
+        self.cores = oracle.num_threads()
+
+    def step(self):
+        t0 = time.perf_counter()
+        self.cg.step()
+        return time.perf_counter() - t0
+
+    def describe(self, seconds):
+        n = 8 ** self.run_depth
+        # bytes one iteration of the crate's loop moves: A d (read d, write q), d.q, x += a d,
+        # r -= a q, r.r, d = r + b d, in FP64
+        gb = 14.0 * n * 8 / 1e9
+        sample = ("one iteration of the crate's CG loop (solve_cg, src/solvers.rs:20-69) per step, FP64, %d host "
+                  "threads, on the oracle's matrix-free degree-%d operator of this %d-point cloud at depth %d "
+                  "(%d unknowns, screening of every point), from x = 0 with a seeded random right-hand side; "
+                  "value = points / time of ONE iteration, an upper bound on the CPU path's points/s (a "
+                  "reconstruction adds setup, many iterations and extraction); %.1f s untimed setup"
+                  % (self.cores, self.degree, self.points, self.run_depth, n, self.setup_s))
+        if self.run_depth != self.depth:
+            sample += "; depth %d instead of %d: not enough free host memory" % (self.run_depth, self.depth)
+        return {"value": self.points / seconds, "unit": "points/s", "cores": self.cores, "kind": "port",
+                "sample": sample, "seconds_per_iteration": seconds, "cg_iteration_gbs": gb / seconds}
 
 
 def run_reference(a):
@@ -197,26 +256,129 @@ def run_reference(a):
     if rank != 0:
         return 0
     from poissonreconstruction_b200 import synthetic
+    if a.config == 1:
+        return run_reference_plain(a)
     pts = synthetic.torus(a.points)
+    cpu = CpuCG(pts, a.depth, a.degree)
     for _ in range(a.warmup):
-        cpu_sample(pts[: min(len(pts), 200_000)], a.depth)
-    times = []
-    last = None
-    for _ in range(a.steps):
-        last = cpu_sample(pts, a.depth)
-        times.append(last["seconds_measured"] * 8.0 ** (a.depth - CPU_DEPTH))
-    ms = 1000.0 * statistics.mean(times)
-    value = len(pts) / (ms / 1000.0)
+        cpu.step()
+    times = [cpu.step() for _ in range(a.steps)]
+    sec = statistics.mean(times)
+    d = cpu.describe(sec)
+    value = d["value"]
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": a.gpus,
-           "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "torus_2m_depth%d_degree%d" % (a.depth, a.degree), "points": len(pts),
-                      "depth": a.depth, "point_weight": 4.0, "cpu_sample_depth": CPU_DEPTH,
-                      "reference_basis": "degree 1: the crate's reconstruct has no degree-2 path"},
-           "cpu_baseline": {k: last[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * sec, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": workload_config(a, len(pts)),
+           "solve_gbs": d["cg_iteration_gbs"],
+           "cpu_baseline": {k: d[k] for k in ("value", "unit", "cores", "kind", "sample")},
            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
+
+
+# ------------------------------------------------------------------ plain-method workload (both arms)
+PLAIN = {"points": 100_000, "depth": 8, "point_weight": 4.0, "cg_iters": 8, "cg_accuracy": 1e-3}
+
+
+def plain_config():
+    return {"workload": "sphere_100k_depth8_reference_schedule", "points": PLAIN["points"], "depth": PLAIN["depth"],
+            "degree": 1, "point_weight": PLAIN["point_weight"], "scale": 1.1,
+            "solve": "the crate's cascade: GS(20) + CG(cg_iters=8) at depth 6, prolongation, GS(20) + CG(2)",
+            "parallelism": "single"}
+
+
+def run_reference_plain(a):
+    """The crate's reconstruct (the oracle's restatement: CSR assembly, cascade with sequential
+    Gauss-Seidel, serial marching cubes) on the plain-method cloud, end to end per step."""
+    import oracle
+    from poissonreconstruction_b200 import synthetic
+    pts = synthetic.sphere(PLAIN["points"])
+    kw = dict(depth=PLAIN["depth"], point_weight=PLAIN["point_weight"], solve_mode=0, cg_iters=PLAIN["cg_iters"],
+              cg_accuracy=PLAIN["cg_accuracy"])
+    for _ in range(a.warmup):
+        oracle.reconstruct(pts, **kw)
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        oracle.reconstruct(pts, **kw)
+        times.append(time.perf_counter() - t0)
+    sec = statistics.mean(times)
+    value = len(pts) / sec
+    cpu = {"value": value, "unit": "points/s", "cores": oracle.num_threads(), "kind": "port",
+           "sample": "the whole reconstruction per step (the oracle's restatement of the crate's path, FP64, %d "
+                     "host threads where the crate uses rayon)" % oracle.num_threads()}
+    print(json.dumps({"impl": "reference", "metric": "plain-method reconstruction throughput", "value": value,
+                      "unit": "points/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                      "ms_per_step": 1000.0 * sec, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64", "data": "synthetic", "config": plain_config(), "cpu_baseline": cpu,
+                      "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+    return 0
+
+
+def run_ours_plain(a):
+    """The plain-method workload on the GPU through the public call (pinned host points in, mesh
+    back in host memory), with the crate's own cascade (PR_SOLVE_REFERENCE_SCHEDULE)."""
+    import torch
+
+    import poissonreconstruction_b200 as prb
+    from poissonreconstruction_b200 import synthetic
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ctx = prb.Context(local, stream=stream.cuda_stream)
+    pts = synthetic.sphere(PLAIN["points"])
+    h_pts = torch.from_numpy(pts).pin_memory()
+    d_pts = torch.from_numpy(pts).to(dev)
+    params = prb.ReconstructParams(depth=PLAIN["depth"], point_weight=PLAIN["point_weight"],
+                                   solve_mode=prb.PR_SOLVE_REFERENCE_SCHEDULE, cg_iters=PLAIN["cg_iters"],
+                                   cg_accuracy=PLAIN["cg_accuracy"])
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(a.warmup):
+        ctx.reconstruct(h_pts.numpy(), params)
+    ev = []
+    with ClockSampler(local) as clocks:
+        for _ in range(a.steps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            ctx.reconstruct_device(d_pts.data_ptr(), len(pts), params)
+            e.record(stream)
+            ev.append((s, e))
+        torch.cuda.synchronize(dev)
+    ms = statistics.mean(s.elapsed_time(e) for s, e in ev)
+    e2e = []
+    mesh = None
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        mesh = None
+        t0 = time.perf_counter()
+        mesh, st = ctx.reconstruct(h_pts.numpy(), params)
+        e2e.append(1000.0 * (time.perf_counter() - t0))
+    e2e_ms = statistics.mean(e2e)
+    d2h = int(mesh.vertices.nbytes + mesh.triangles.nbytes)
+    ctx.close()
+    print(json.dumps({"metric": "plain-method reconstruction throughput", "value": len(pts) / (ms / 1000.0),
+                      "unit": "points/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": dict(plain_config(), l2="flushed between steps (256 MiB)"),
+                      "e2e": {"value": len(pts) / (e2e_ms / 1000.0), "unit": "points/s",
+                              "h2d_bytes_per_step": len(pts) * 48, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                      "mesh": {"vertices": int(st.mesh_vertices), "triangles": int(st.mesh_triangles)},
+                      "clocks": clocks.summary()}), flush=True)
+    return 0
+
+
+def workload_config(a, points):
+    return {"workload": "torus_2m_depth%d_degree%d" % (a.depth, a.degree), "points": points,
+            "depth": a.depth, "degree": a.degree, "point_weight": 4.0,
+            "scale": 1.1, "precision": "fp32 pcg + fp64 refinement", "target_rel_residual": 1e-6,
+            "parallelism": "replicas" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "single",
+            "l2": "flushed between steps (256 MiB)"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -314,12 +476,24 @@ def run_ours(a):
 
     # FP64 comparison arm (same system, same target), warmed up like the mixed arm, in a context of
     # its own: at depth 10 the two arms' buffers do not fit one device together
+    # accuracy (untimed): the mixed solution and mesh of the timed configuration
+    acc = None
+    if not a.no_accuracy and rank == 0:
+        ctx.reconstruct_device(d_pts.data_ptr(), P, params)
+        acc = {"x_mixed": ctx.coefficients(), "v_mixed": ctx.mesh().vertices}
     ctx.close()
     ctx = prb.Context(local, stream=stream.cuda_stream)
     k64 = a.fp64_steps if a.fp64_steps is not None else a.steps
     device_steps(params64, 1, False)
     ms64, stats64 = device_steps(params64, max(1, k64), True)
     solve64_s = statistics.mean(s.time_solve for s in stats64)
+    accuracy = None
+    if acc is not None:
+        acc["x_fp64"] = ctx.coefficients()
+        acc["v_fp64"] = ctx.mesh().vertices
+        ctx, accuracy = accuracy_block(ctx, lambda: prb.Context(local, stream=stream.cuda_stream), d_pts, P, pts, a,
+                                       acc)
+    acc = None
     ctx.close()
     ctx = prb.Context(local, stream=stream.cuda_stream)
 
@@ -338,13 +512,18 @@ def run_ours(a):
     peak = peak or 6650.0
     kernels = {}
     if a.degree == 2:
-        names = ("d2_cheb", "d2_cheb_f", "d2_cheb_pf", "d2_resid", "d2_apply", "d2_restrict", "d2_prolong")
+        # every finest-level pass of the degree-2 solve (FP32 unless marked), the FP64 refinement
+        # step, and the plain A x (the SpMV alone)
+        names = ("d2_cheb", "d2_cg_dir", "d2_cheb_f", "d2_cheb_pf", "d2_resid", "d2_restrict", "d2_prolong",
+                 "d2_refine:f64", "d2_apply")
         dom = "d2_cheb"
     else:
         names = ("smooth_prolong_dot", "cg_update_presmooth", "resid_restrict", "spmv_xpby", "spmv")
         dom = "smooth_prolong_dot"
     for nm in names:
-        ms, by = ctx.kernel_bench(nm, a.depth, prb.PR_PRECISION_MIXED, a.roofline_reps)
+        kn, _, prec = nm.partition(":")
+        ms, by = ctx.kernel_bench(kn, a.depth, prb.PR_PRECISION_FP64 if prec == "f64" else prb.PR_PRECISION_MIXED,
+                                  a.roofline_reps)
         kernels[nm] = {"ms_per_launch": ms, "algorithmic_bytes": by, "achieved_gbs": by / (ms / 1000.0) / 1e9,
                        "frac": by / (ms / 1000.0) / 1e9 / peak}
     traffic = None
@@ -357,8 +536,12 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        cpu = cpu_sample(pts, a.depth)
-        cpu.pop("seconds_measured", None)
+        leg = CpuCG(pts, a.depth, a.degree)
+        leg.step()  # warm-up iteration
+        d = leg.describe(statistics.mean(leg.step() for _ in range(3)))
+        cpu = {k: d[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu["cg_iteration_gbs"] = d["cg_iteration_gbs"]
+        leg = None
 
     # the other basis on the same cloud (device-resident steps, mixed and FP64), in a fresh context
     # once the headline context has released its buffers
@@ -386,10 +569,7 @@ def run_ours(a):
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64 refinement", "data": "synthetic",
-            "config": {"workload": "torus_2m_depth%d_degree%d" % (a.depth, a.degree), "points": P,
-                       "depth": a.depth, "degree": a.degree, "point_weight": 4.0,
-                       "scale": 1.1, "precision": "fp32 pcg + fp64 refinement", "target_rel_residual": 1e-6,
-                       "parallelism": "replicas" if ws > 1 else "single", "l2": "flushed between steps (256 MiB)"},
+            "config": workload_config(a, P),
             "solve_gbs": solve_gbs, "solve_ms": 1000.0 * solve_s, "rel_residual": st.rel_residual,
             "pcg_iterations": st.pcg_iterations, "refinement_steps": st.refinement_steps,
             "fp64_solve_ms": 1000.0 * solve64_s, "fp64_ms_per_step": statistics.mean(ms64),
@@ -405,6 +585,7 @@ def run_ours(a):
                          "traffic": traffic, "algorithmic_bytes": kernels[dom]["algorithmic_bytes"],
                          "ms_per_launch": kernels[dom]["ms_per_launch"]},
             "kernels": kernels,
+            "accuracy": accuracy,
             "degree1": other,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -474,6 +655,46 @@ def run_batch(a):
     return 0
 
 
+def accuracy_block(ctx, new_ctx, d_pts, P, pts, a, acc):
+    """Coefficient and vertex error of the timed solves (mixed and FP64 at the 1e-6 target) against
+    each other and against an FP64 solve to 1e-10 (untimed), and the largest mixed target residual
+    whose coefficients are within 1e-6 of that reference.  ctx is the FP64 arm's context; the mixed
+    solves run in a fresh one (at depth 10 the two precisions' buffers do not fit one device
+    together).  Returns (the context in use, the block)."""
+    import poissonreconstruction_b200 as prb
+    from scipy.spatial import cKDTree
+
+    def rel(u, v):
+        return float(np.linalg.norm(u - v) / np.linalg.norm(v))
+
+    def solve(prec, tol):
+        ctx.reconstruct_device(d_pts.data_ptr(), P, prb.ReconstructParams(
+            depth=a.depth, point_weight=4.0, scale=1.1, degree=a.degree, precision=prec, target_rel_residual=tol,
+            max_iters=400))
+        return ctx.coefficients()
+
+    x_ref = solve(prb.PR_PRECISION_FP64, 1e-10)
+    ctx.close()
+    ctx = new_ctx()
+    out = {"coef_rel_l2_mixed_vs_fp64": rel(acc["x_mixed"], acc["x_fp64"]),
+           "coef_rel_l2_mixed_vs_fp64_1e-10": rel(acc["x_mixed"], x_ref),
+           "coef_rel_l2_fp64_vs_fp64_1e-10": rel(acc["x_fp64"], x_ref)}
+    meets = None
+    for tol in (1e-6, 1e-7, 1e-8, 1e-9):
+        e = out["coef_rel_l2_mixed_vs_fp64_1e-10"] if tol == 1e-6 else rel(solve(prb.PR_PRECISION_MIXED, tol), x_ref)
+        out["coef_rel_l2_mixed_%.0e_vs_fp64_1e-10" % tol] = e
+        if e <= 1e-6:
+            meets = tol
+            break
+    out["mixed_target_meeting_1e-6_coefficients"] = meets
+    diag = float(np.linalg.norm(pts[:, :3].max(0) - pts[:, :3].min(0)))
+    d, _ = cKDTree(acc["v_fp64"]).query(acc["v_mixed"])
+    out["vertex_err_mixed_vs_fp64_max_over_bbox_diag"] = float(d.max() / diag)
+    out["vertex_err_mixed_vs_fp64_p999_over_bbox_diag"] = float(np.quantile(d, 0.999) / diag)
+    out["vertices"] = [int(len(acc["v_mixed"])), int(len(acc["v_fp64"]))]
+    return ctx, out
+
+
 def main():
     a = parse()
     if a.batch:
@@ -482,6 +703,8 @@ def main():
         return run_kernel_bench(a)
     if a.impl == "reference":
         return run_reference(a)
+    if a.config == 1:
+        return run_ours_plain(a)
     return run_ours(a)
 
 

@@ -155,6 +155,17 @@ int pr_ctx_get_normal_field(pr_context* ctx, double* out_3n, double* out_weight_
 /* y = A x with the fine operator of src/fem_tree.rs:180-249 (stiffness + screening),
  * matrix-free; precision PR_PRECISION_FP64 or PR_PRECISION_MIXED (FP32 operator, FP64 I/O). */
 int pr_ctx_apply_operator(pr_context* ctx, const double* x_n, double* y_n, int precision);
+/* Reference schedule (PR_SOLVE_REFERENCE_SCHEDULE) only: the right-hand side of its coarse
+ * system (FEMTree::build_system_at_depth, src/fem_tree.rs:386-402) at *coarse_depth = max(D-2, 0),
+ * 8^(*coarse_depth) values in Morton order (out may be NULL to query the depth). */
+int pr_ctx_get_coarse_rhs(pr_context* ctx, uint32_t* coarse_depth, double* out);
+/* The crate's CG loop (solve_cg, src/solvers.rs:20-69: residual recomputed every 10th iteration,
+ * stop at ||r||^2 <= ||r0||^2 accuracy^2) on the fine system of the last degree-1 reconstruction,
+ * FP64 on the device, from x0 (n doubles, FEM order; NULL = 0) for at most max_iters
+ * iterations.  x receives the iterate; delta (may be NULL) receives ||r||^2 before the first
+ * iteration and after each one (max_iters + 1 slots); *out_iters the crate's return value. */
+int pr_ctx_cg_reference(pr_context* ctx, const double* x0, uint64_t max_iters, double accuracy, double* x,
+                        double* delta, uint64_t* out_iters);
 /* Evaluate the implicit function (src/fem_tree.rs:490-513) of `coefficients` (NULL = the
  * solved ones) at unit-cube points (3 doubles each). */
 int pr_ctx_evaluate(pr_context* ctx, const double* coefficients, const double* pts3, uint64_t n, double* out);
@@ -180,7 +191,8 @@ int pr_ctx_apply_operator_device(pr_context* ctx, const void* d_x, void* d_y, in
  * smoothing step (TMA-fed), 21 = the same with register staging, 22 / 23 = A x (TMA / register
  * staging), 24 = f - A x (TMA), 25 = restriction, 26 = prolongation + add, 27 = first
  * Chebyshev step, 28 = the first two steps fused (from f), 29 = the third step recomputing the
- * first from f (TMA variants need depth >= 6).  Times `reps` launches
+ * first from f, 30 = the fused CG direction pass (d = z + beta d, q = A d, x += alpha d), 31 = the
+ * fused FP64 refinement step (x + e, b - A x, FP32 copy; FP64 only) (TMA variants need depth >= 6).  Times `reps` launches
  * with CUDA events on the context's stream; returns the mean ms per launch and the
  * algorithmic HBM bytes per launch. */
 int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precision, int reps, double* ms_per_launch,

@@ -74,6 +74,10 @@ def lib():
         "orc_tree_coarse_rhs": (C.c_int, [_p, _d, _p]),
         "orc_tree_prolongate": (C.c_int, [_p, _p, _u32, _p]),
         "orc_tree_solve_converged": (_u64, [_p, _d, _d, _u64, _p, _p]),
+        "orc_tree_apply_mf": (None, [_p, _d, _p, _p]),
+        "orc_tree_release_field": (None, [_p]),
+        "orc_tree_cg_mf": (_u64, [_p, _d, _p, _p, _u64, _d, _p]),
+        "orc_tree_solve_converged_mf": (_u64, [_p, _d, _p, _d, _u64, _p, _p]),
         "orc_evaluate": (_d, [_u32, _p, _d, _d, _d]),
         "orc_evaluate_many": (None, [_u32, _p, _p, _u64, _u64, _p]),
         "orc_iso": (_d, [_u32, _p, _p, _u64]),
@@ -92,6 +96,11 @@ def lib():
         "orc_tree2_rhs": (None, [_p, _p]),
         "orc_tree2_apply": (None, [_p, _p, _p]),
         "orc_tree2_solve": (_u64, [_p, _d, _u64, _p, _p]),
+        "orc_tree2_release_field": (None, [_p]),
+        "orc_cg2_new": (_p, [_p, _p]),
+        "orc_cg1_new": (_p, [_p, _d, _p]),
+        "orc_cg_step": (_d, [_p]),
+        "orc_cg_free": (None, [_p]),
         "orc_extract_surface2": (C.c_int, [_u32, _p, _d, C.POINTER(OrcMesh)]),
         "orc_reconstruct2": (C.c_int, [_p, _u64, _u32, _d, _d, _d, _u64, C.POINTER(OrcMesh), _p, _p, _p]),
         "orc_loss": (_d, [_p, _u64, _u32, _d, _d, _p, _u64, _p, _d]),
@@ -249,6 +258,35 @@ class Tree:
         return x, it, rr.value
 
 
+    # ---- matrix-free fine operator (depths where the crate's CSR does not fit in host memory)
+    def apply_mf(self, x, pw):
+        """y = A x with the entries of assemble_system computed on the fly."""
+        x = _f64(x)
+        y = np.empty(self.n)
+        lib().orc_tree_apply_mf(self._h, float(pw), _ptr(x), _ptr(y))
+        return y
+
+    def release_field(self):
+        """Free the normal field and weights (rhs() needs them; the matrix-free solves do not)."""
+        lib().orc_tree_release_field(self._h)
+
+    def cg_mf(self, b, pw, iters, acc, x0=None):
+        """The crate's solve_cg (src/solvers.rs:20-69) with the matrix-free operator.
+        Returns (x, iterations, delta) with delta[k] = ||r||^2 after k iterations."""
+        x = np.zeros(self.n) if x0 is None else _f64(x0).copy()
+        delta = np.full(int(iters) + 1, np.nan)
+        it = lib().orc_tree_cg_mf(self._h, float(pw), _ptr(_f64(b)), _ptr(x), int(iters), float(acc), _ptr(delta))
+        return x, it, delta
+
+    def solve_converged_mf(self, b, pw, tol=1e-12, maxit=100000, x0=None):
+        """CG until ||b - A x|| <= tol ||b||, matrix-free, from x0 (default 0)."""
+        x = np.zeros(self.n) if x0 is None else _f64(x0).copy()
+        rr = C.c_double(0.0)
+        it = lib().orc_tree_solve_converged_mf(self._h, float(pw), _ptr(_f64(b)), float(tol), int(maxit), _ptr(x),
+                                               C.byref(rr))
+        return x, it, rr.value
+
+
 def evaluate(depth, sol, pts3):
     pts3 = _f64(pts3, (-1, 3))
     out = np.zeros(pts3.shape[0])
@@ -337,6 +375,36 @@ class Tree2:
         x, rr = np.zeros(self.n), C.c_double()
         it = lib().orc_tree2_solve(self._h, float(tol), int(maxit), _ptr(x), C.byref(rr))
         return x, it, rr.value
+
+    def release_field(self):
+        """Free the normal field and weights (rhs() needs them; apply() does not)."""
+        lib().orc_tree2_release_field(self._h)
+
+
+class _CG:
+    """The crate's CG loop (src/solvers.rs:20-69) on a matrix-free oracle operator, one
+    iteration per step() (the CPU baseline's unit of work); from x = 0 with right-hand side b."""
+
+    def step(self):
+        """One iteration; returns ||r||^2 after it."""
+        return lib().orc_cg_step(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_cg_free(self._h)
+            self._h = None
+
+
+class CG2(_CG):
+    def __init__(self, tree2, b):
+        self.tree = tree2  # keeps the operator alive
+        self._h = lib().orc_cg2_new(tree2._h, _ptr(_f64(b)))
+
+
+class CG1(_CG):
+    def __init__(self, tree, b, pw):
+        self.tree = tree
+        self._h = lib().orc_cg1_new(tree._h, float(pw), _ptr(_f64(b)))
 
 
 def extract_surface2(depth, sol, iso_value):

@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <unordered_map>
 #include <vector>
 #ifdef _OPENMP
@@ -53,15 +54,25 @@ inline uint64_t f64_to_u64(double v) {
 // The crate's FEM index of a max-depth leaf is its position in the depth-first order
 // of `SortedTreeNodes::collect_nodes` (src/octree.rs:235-248) with child i at offset
 // (i&1, (i>>1)&1, (i>>2)&1) (src/octree.rs:145-153): the 3-D Morton code, x in bit 0.
+// bit b of v moves to bit 3b (21-bit coordinates), by the usual shift-and-mask interleave
 inline uint64_t spread3(uint64_t v) {
-  uint64_t r = 0;
-  for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
-  return r;
+  v &= 0x1fffffull;
+  v = (v | v << 32) & 0x1f00000000ffffull;
+  v = (v | v << 16) & 0x1f0000ff0000ffull;
+  v = (v | v << 8) & 0x100f00f00f00f00full;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+  v = (v | v << 2) & 0x1249249249249249ull;
+  return v;
 }
+// inverse of spread3: bit 3b of v moves to bit b
 inline uint64_t compact3(uint64_t v) {
-  uint64_t r = 0;
-  for (int b = 0; b < 21; ++b) r |= ((v >> (3 * b)) & 1ull) << b;
-  return r;
+  v &= 0x1249249249249249ull;
+  v = (v ^ (v >> 2)) & 0x10c30c30c30c30c3ull;
+  v = (v ^ (v >> 4)) & 0x100f00f00f00f00full;
+  v = (v ^ (v >> 8)) & 0x1f0000ff0000ffull;
+  v = (v ^ (v >> 16)) & 0x1f00000000ffffull;
+  v = (v ^ (v >> 32)) & 0x1fffffull;
+  return v;
 }
 inline uint64_t morton(uint64_t x, uint64_t y, uint64_t z) {
   return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
@@ -70,6 +81,93 @@ inline void unmorton(uint64_t m, uint64_t& x, uint64_t& y, uint64_t& z) {
   x = compact3(m);
   y = compact3(m >> 1);
   z = compact3(m >> 2);
+}
+
+// The Morton codes of the 27 neighbours of node m: per axis the interleaved bits of the
+// coordinate minus one, itself and plus one (p[a][0..2]), and whether that coordinate lies in
+// [0, res) (v[a][0..2]); neighbour (dx,dy,dz) = p[0][dx+1] | p[1][dy+1] | p[2][dz+1].  The
+// masked increment carries through the gaps of the other axes' bits.
+struct MortonNbrs {
+  uint64_t p[3][3];
+  bool v[3][3];
+  uint64_t c[3];  // coordinates
+  MortonNbrs(uint64_t m, uint64_t res) {
+    const uint64_t X = 0x1249249249249249ull;
+    for (int a = 0; a < 3; ++a) {
+      const uint64_t mask = X << a, one = 1ull << a;
+      const uint64_t part = m & mask;
+      c[a] = compact3(m >> a);
+      p[a][1] = part;
+      p[a][0] = (part - one) & mask;
+      p[a][2] = ((part | ~mask) + one) & mask;
+      v[a][0] = c[a] > 0;
+      v[a][1] = true;
+      v[a][2] = c[a] + 1 < res;
+    }
+  }
+};
+
+// Visits the 2^D grid Morton-aligned block by block (blocks of B^3 nodes, B = min(8, res), each
+// one contiguous range of the FEM index starting at blk * B^3).  For each block, `tile` holds the
+// C components of src at the block's nodes and its H-node halo, in natural order (x fastest,
+// row length T = B + 2H), zero outside the grid, and blockfn(blk, tile, T, B, loc, base) is
+// called; loc[3l..3l+2] are the local coordinates of the block's l-th node (Morton order) and
+// base[3] the block's first grid coordinates.  Gathering the halo once per block keeps the
+// per-node work free of index arithmetic.
+template <int C, int H, typename BlockFn>
+void blocked_tiles(uint32_t D, const double* src, BlockFn&& blockfn) {
+  const uint64_t res = 1ull << D;
+  const int B = res < 8 ? (int)res : 8;
+  const int T = B + 2 * H;
+  const uint64_t nb = res / (uint64_t)B, bsz = (uint64_t)B * B * B;
+  std::vector<uint64_t> sp(res);
+  for (uint64_t g = 0; g < res; ++g) sp[g] = spread3(g);
+  std::vector<int> loc(3 * bsz);
+  for (uint64_t l = 0; l < bsz; ++l) {
+    uint64_t a, b, c;
+    unmorton(l, a, b, c);
+    loc[3 * l] = (int)a;
+    loc[3 * l + 1] = (int)b;
+    loc[3 * l + 2] = (int)c;
+  }
+#pragma omp parallel
+  {
+    std::vector<double> tile((size_t)T * T * T * C);
+#pragma omp for schedule(static)
+    for (int64_t blk = 0; blk < (int64_t)(nb * nb * nb); ++blk) {
+      uint64_t bx, by, bz;
+      unmorton((uint64_t)blk, bx, by, bz);
+      const int64_t base[3] = {(int64_t)bx * B, (int64_t)by * B, (int64_t)bz * B};
+      for (int z = -H; z < B + H; ++z)
+        for (int y = -H; y < B + H; ++y)
+          for (int x = -H; x < B + H; ++x) {
+            const int64_t gx = base[0] + x, gy = base[1] + y, gz = base[2] + z;
+            double* t = &tile[(size_t)(((z + H) * T + (y + H)) * T + (x + H)) * C];
+            if (gx < 0 || gy < 0 || gz < 0 || gx >= (int64_t)res || gy >= (int64_t)res || gz >= (int64_t)res) {
+              for (int k = 0; k < C; ++k) t[k] = 0.0;
+              continue;
+            }
+            const uint64_t j = sp[gx] | (sp[gy] << 1) | (sp[gz] << 2);
+            for (int k = 0; k < C; ++k) t[k] = src[C * j + k];
+          }
+      blockfn((uint64_t)blk, tile.data(), T, B, loc.data(), base);
+    }
+  }
+}
+
+// blocked_tiles with a per-node callback: row(i, tile, o, T, g) for every node i of the block in
+// index order, o its tile offset, g[3] its grid coordinates.
+template <int C, int H = 1, typename Row>
+void blocked_rows(uint32_t D, const double* src, Row&& row) {
+  blocked_tiles<C, H>(D, src, [&](uint64_t blk, const double* tile, int T, int B, const int* loc,
+                                  const int64_t* base) {
+    const uint64_t bsz = (uint64_t)B * B * B;
+    for (uint64_t l = 0; l < bsz; ++l) {
+      const int* q = &loc[3 * l];
+      const int64_t g[3] = {base[0] + q[0], base[1] + q[1], base[2] + q[2]};
+      row(blk * bsz + l, tile, (size_t)((q[2] + H) * T + (q[1] + H)) * T + (q[0] + H), T, g);
+    }
+  });
 }
 
 // ---------------------------------------------------------------- 1-D constants
@@ -458,26 +556,22 @@ static int screening_basis(const orc_tree* t, const P6& pt, uint64_t* idx, doubl
 
 // FEMTree::assemble_rhs (src/fem_tree.rs:251-299)
 void orc_tree_rhs(const orc_tree* t, double pw, double* rhs) {
-  const uint64_t res = t->res;
+  const isize res = (isize)t->res;
   const double h = t->h;
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < (int64_t)t->n; ++i) {
-    uint64_t ix, iy, iz;
-    unmorton(i, ix, iy, iz);
+  blocked_rows<3>(t->D, t->nf.data(), [&](uint64_t i, const double* tile, size_t o, int T, const int64_t* g) {
     double sum = 0.0;
     for (isize dx = -1; dx <= 1; ++dx)
       for (isize dy = -1; dy <= 1; ++dy)
         for (isize dz = -1; dz <= 1; ++dz) {
-          isize jx = (isize)ix + dx, jy = (isize)iy + dy, jz = (isize)iz + dz;
-          if (jx < 0 || jx >= (isize)res || jy < 0 || jy >= (isize)res || jz < 0 || jz >= (isize)res) continue;
-          uint64_t j = morton(jx, jy, jz);
-          const double* v = &t->nf[3 * j];
+          isize jx = g[0] + dx, jy = g[1] + dy, jz = g[2] + dz;
+          if (jx < 0 || jx >= res || jy < 0 || jy >= res || jz < 0 || jz >= res) continue;
+          const double* v = &tile[3 * (o + (dz * T + dy) * T + dx)];
           sum += h * h * (v[0] * deriv_mass_1d(dx) * mass_1d(dy) * mass_1d(dz) +
                           v[1] * mass_1d(dx) * deriv_mass_1d(dy) * mass_1d(dz) +
                           v[2] * mass_1d(dx) * mass_1d(dy) * deriv_mass_1d(dz));
         }
     rhs[i] = sum;
-  }
+  });
   if (pw > 0.0) {
     double wh3 = pw * (h * h * h) / 1.5;
     double target = 0.5;
@@ -696,6 +790,178 @@ uint64_t orc_tree_solve_converged(orc_tree* t, double pw, double tol, uint64_t m
   }
   t->A.spmv(x, q.data());
   for (uint64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  if (relres) *relres = std::sqrt(det_dot(r.data(), r.data(), n) / bb);
+  return it;
+}
+
+// ---------------------------------------------------------------- matrix-free fine operator
+// The crate's CSR (src/fem_tree.rs:180-249) needs about 1 TB of host memory at depth 10, so
+// the large-depth checks use the same entries computed on the fly.  Row i of A x:
+//   stiffness_entry(h, d) x_{i+d} over the 27 neighbours inside the grid (zero entries skipped,
+//   src/fem_tree.rs:187-193), then + wg x_i (src/fem_tree.rs:195-200), then the screening rows
+//   sum_p wh3 phi_a(p) phi_b(p) x_b of the points whose trunc cell touches node i
+//   (src/fem_tree.rs:201-228).
+// The CSR product sums a row's entries in column order; here they are grouped by kind, so the
+// two agree to rounding (tests/test_oracle.py compares them).
+void orc_tree_apply_mf(const orc_tree* t, double pw, const double* x, double* y) {
+  const uint64_t n = t->n;
+  const isize res = (isize)t->res;
+  const double h = t->h;
+  const double wh3 = pw > 0.0 ? pw * (h * h * h) / 1.5 : 0.0;
+  const double wg = wh3 * 0.005;
+  (void)n;
+  (void)res;
+  // the nonzero entries (21 of 27), in the neighbour order dz, dy, dx
+  double st[27];
+  int off[27], nz = 0;
+  const int T = t->res < 8 ? (int)t->res + 2 : 10;
+  for (int k = 0; k < 27; ++k) {
+    const double v = stiffness_entry(h, k % 3 - 1, (k / 3) % 3 - 1, k / 9 - 1);
+    if (v == 0.0) continue;
+    st[nz] = v;
+    off[nz++] = ((k / 9 - 1) * T + ((k / 3) % 3 - 1)) * T + (k % 3 - 1);
+  }
+  // entries to neighbours outside the grid are omitted: their tile values are zero
+  blocked_rows<1>(t->D, x, [&](uint64_t i, const double* tile, size_t o, int, const int64_t*) {
+    const double* c = tile + o;
+    double s = 0.0;
+    for (int k = 0; k < nz; ++k) s += st[k] * c[off[k]];
+    y[i] = pw > 0.0 ? s + wg * c[0] : s;
+  });
+  if (pw > 0.0) {
+    const uint64_t np = t->pts.size();
+    std::vector<double> proj(np);
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < (int64_t)np; ++p) {
+      uint64_t idx[8];
+      double bx[8], by[8], bz[8];
+      const int m = screening_basis(t, t->pts[p], idx, bx, by, bz);
+      double v = 0.0;
+      for (int k = 0; k < m; ++k) v += bx[k] * by[k] * bz[k] * x[idx[k]];
+      proj[p] = v;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < (int64_t)np; ++p) {
+      uint64_t idx[8];
+      double bx[8], by[8], bz[8];
+      const int m = screening_basis(t, t->pts[p], idx, bx, by, bz);
+      for (int k = 0; k < m; ++k) {
+        const double v = wh3 * (bx[k] * by[k] * bz[k]) * proj[p];
+#pragma omp atomic
+        y[idx[k]] += v;
+      }
+    }
+  }
+}
+
+// Frees the normal field and node weights (the right-hand side no longer needs them): at
+// depth 10 they hold 34 GB that the matrix-free solves below do not use.
+void orc_tree_release_field(orc_tree* t) {
+  std::vector<double>().swap(t->nf);
+  std::vector<double>().swap(t->nw);
+}
+
+}  // extern "C"
+namespace {
+void par_copy(double* dst, const double* src, uint64_t n) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) dst[i] = src[i];
+}
+// r = b - q
+void par_sub(double* r, const double* b, const double* q, uint64_t n) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) r[i] = b[i] - q[i];
+}
+// x += a d
+void par_axpy(double* x, double a, const double* d, uint64_t n) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) x[i] += a * d[i];
+}
+// d = r + beta d
+void par_xpby(double* d, const double* r, double beta, uint64_t n) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) d[i] = r[i] + beta * d[i];
+}
+}  // namespace
+extern "C" {
+
+// solve_cg (src/solvers.rs:20-69) on the fine system with the matrix-free operator and the
+// caller's right-hand side b: from x (initial guess on entry), at most max_iters iterations,
+// the residual recomputed as b - A x every 10th iteration, stop when ||r||^2 <= ||r0||^2 acc^2.
+// delta (may be NULL) receives ||r||^2 before the first iteration and after each one
+// (max_iters + 1 slots; unused slots are left as they were).  Returns the iteration count as
+// the crate does.
+uint64_t orc_tree_cg_mf(const orc_tree* t, double pw, const double* b, double* x, uint64_t max_iters, double accuracy,
+                        double* delta) {
+  const uint64_t n = t->n;
+  std::vector<double> r(n), d(n), q(n);
+  orc_tree_apply_mf(t, pw, x, q.data());
+  par_sub(r.data(), b, q.data(), n);
+  par_copy(d.data(), r.data(), n);
+  double delta_new = det_dot(r.data(), r.data(), n);
+  const double delta_0 = delta_new;
+  if (delta) delta[0] = delta_new;
+  if (delta_new == 0.0) return 0;
+  for (uint64_t iter = 0; iter < max_iters; ++iter) {
+    orc_tree_apply_mf(t, pw, d.data(), q.data());
+    const double dq = det_dot(d.data(), q.data(), n);
+    if (dq == 0.0) return iter + 1;
+    const double alpha = delta_new / dq;
+    par_axpy(x, alpha, d.data(), n);
+    if ((iter + 1) % 10 == 0) {
+      orc_tree_apply_mf(t, pw, x, q.data());
+      par_sub(r.data(), b, q.data(), n);
+    } else {
+      par_axpy(r.data(), -alpha, q.data(), n);
+    }
+    const double delta_old = delta_new;
+    delta_new = det_dot(r.data(), r.data(), n);
+    if (delta) delta[iter + 1] = delta_new;
+    if (delta_new <= delta_0 * accuracy * accuracy) return iter + 1;
+    const double beta = delta_new / delta_old;
+    if (std::isnan(beta) || std::isinf(beta)) break;
+    par_xpby(d.data(), r.data(), beta, n);
+  }
+  return max_iters;
+}
+
+// orc_tree_solve_converged with the matrix-free operator and the caller's b: CG from the
+// initial guess in x until ||b - A x|| <= tol ||b|| (explicit residual every 50 iterations).
+// relres (may be NULL) receives the final explicit relative residual.
+uint64_t orc_tree_solve_converged_mf(const orc_tree* t, double pw, const double* b, double tol, uint64_t maxit,
+                                     double* x, double* relres) {
+  const uint64_t n = t->n;
+  std::vector<double> r(n), d(n), q(n);
+  const double bb = det_dot(b, b, n);
+  if (bb == 0.0) {
+    if (relres) *relres = 0.0;
+    return 0;
+  }
+  orc_tree_apply_mf(t, pw, x, q.data());
+  par_sub(r.data(), b, q.data(), n);
+  par_copy(d.data(), r.data(), n);
+  double rr = det_dot(r.data(), r.data(), n);
+  uint64_t it = 0;
+  while (it < maxit && rr > tol * tol * bb) {
+    orc_tree_apply_mf(t, pw, d.data(), q.data());
+    const double dq = det_dot(d.data(), q.data(), n);
+    if (dq == 0.0) break;
+    const double alpha = rr / dq;
+    par_axpy(x, alpha, d.data(), n);
+    ++it;
+    if (it % 50 == 0) {
+      orc_tree_apply_mf(t, pw, x, q.data());
+      par_sub(r.data(), b, q.data(), n);
+    } else {
+      par_axpy(r.data(), -alpha, q.data(), n);
+    }
+    const double rr_new = det_dot(r.data(), r.data(), n);
+    const double beta = rr_new / rr;
+    rr = rr_new;
+    par_xpby(d.data(), r.data(), beta, n);
+  }
+  orc_tree_apply_mf(t, pw, x, q.data());
+  par_sub(r.data(), b, q.data(), n);
   if (relres) *relres = std::sqrt(det_dot(r.data(), r.data(), n) / bb);
   return it;
 }
@@ -1301,24 +1567,54 @@ void orc_tree2_apply(const orc_tree2* t, const double* x, double* y) {
   const double h = t->h;
   const double wh3 = t->pw > 0.0 ? t->pw * h * h * h / 1.5 : 0.0;
   const double wg = wh3 * 0.005;
-#pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < (int64_t)t->n; ++i) {
-    uint64_t ix, iy, iz;
-    unmorton((uint64_t)i, ix, iy, iz);
-    double sum = 0.0;
-    for (int dz = -2; dz <= 2; ++dz)
-      for (int dy = -2; dy <= 2; ++dy)
-        for (int dx = -2; dx <= 2; ++dx) {
-          const isize jx = (isize)ix + dx, jy = (isize)iy + dy, jz = (isize)iz + dz;
-          if (!in_range(jx, res) || !in_range(jy, res) || !in_range(jz, res)) continue;
-          const int a = dx + 2, bi = dy + 2, c = dz + 2;
-          const double st = K.s[a] * K.m[bi] * K.m[c] + K.m[a] * K.s[bi] * K.m[c] + K.m[a] * K.m[bi] * K.s[c];
-          sum += h * st * x[morton(jx, jy, jz)];
+  (void)res;
+  // h (S m m + m S m + m m S) x on the zero-extended vector (neighbours outside the grid omitted),
+  // as separable passes over each block's tile: z (M, S), then y, then x
+  blocked_tiles<1, 2>(t->D, x, [&](uint64_t blk, const double* tile, int T, int B, const int* loc, const int64_t*) {
+    const int T2 = T * T;
+    thread_local std::vector<double> um, us, w1, w23;  // [z][y][x]: z in the block; y, x in the tile / x in the tile
+    um.resize((size_t)B * T2);
+    us.resize((size_t)B * T2);
+    w1.resize((size_t)B * B * T);
+    w23.resize((size_t)B * B * T);
+    for (int z = 0; z < B; ++z)
+      for (int yx = 0; yx < T2; ++yx) {
+        double am = 0.0, as = 0.0;
+        for (int c = 0; c < 5; ++c) {
+          const double v = tile[(size_t)(z + c) * T2 + yx];
+          am += K.m[c] * v;
+          as += K.s[c] * v;
         }
-    y[i] = sum + wg * x[i];
-  }
+        um[(size_t)z * T2 + yx] = am;
+        us[(size_t)z * T2 + yx] = as;
+      }
+    for (int z = 0; z < B; ++z)
+      for (int y = 0; y < B; ++y)
+        for (int xx = 0; xx < T; ++xx) {
+          double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+          for (int c = 0; c < 5; ++c) {
+            const size_t q = (size_t)z * T2 + (size_t)(y + c) * T + xx;
+            a1 += K.m[c] * um[q];
+            a2 += K.s[c] * um[q];
+            a3 += K.m[c] * us[q];
+          }
+          w1[((size_t)z * B + y) * T + xx] = a1;
+          w23[((size_t)z * B + y) * T + xx] = a2 + a3;
+        }
+    const uint64_t bsz = (uint64_t)B * B * B;
+    for (uint64_t l = 0; l < bsz; ++l) {
+      const int* q = &loc[3 * l];
+      const size_t r = ((size_t)q[2] * B + q[1]) * T + q[0];
+      double acc = 0.0;
+      for (int c = 0; c < 5; ++c) acc += K.s[c] * w1[r + c] + K.m[c] * w23[r + c];
+      const double xc = tile[(size_t)((q[2] + 2) * T + (q[1] + 2)) * T + (q[0] + 2)];
+      y[blk * bsz + l] = h * acc + wg * xc;
+    }
+  });
   if (wh3 > 0.0) {
-    for (const P6& p : t->pts) {
+#pragma omp parallel for schedule(static)
+    for (int64_t pi = 0; pi < (int64_t)t->pts.size(); ++pi) {
+      const P6& p = t->pts[pi];
       isize o[3][3];
       double bb[3][3], db[3][3];
       axis2(p.x, h, res, o[0], bb[0], db[0]);
@@ -1337,10 +1633,69 @@ void orc_tree2_apply(const orc_tree2* t, const double* x, double* y) {
           }
       double proj = 0.0;
       for (int q = 0; q < m; ++q) proj += phi[q] * x[idx[q]];
-      for (int q = 0; q < m; ++q) y[idx[q]] += wh3 * phi[q] * proj;
+      for (int q = 0; q < m; ++q) {
+        const double v = wh3 * phi[q] * proj;
+#pragma omp atomic
+        y[idx[q]] += v;
+      }
     }
   }
 }
+
+// Frees the normal field and weights (the operator needs only the points).
+void orc_tree2_release_field(orc_tree2* t) {
+  std::vector<double>().swap(t->nf);
+  std::vector<double>().swap(t->nw);
+}
+
+// A CG run kept between calls, one iteration per orc_cg_step: the loop body of solve_cg
+// (src/solvers.rs:20-69; residual recomputed as b - A x every 10th iteration) on a matrix-free
+// operator, from x = 0.  The CPU baseline times single iterations of it.
+struct orc_cg {
+  std::function<void(const double*, double*)> apply;
+  uint64_t n = 0;
+  std::vector<double> b, x, r, d, q;
+  double delta = 0.0;
+  uint64_t it = 0;
+};
+static orc_cg* cg_new(std::function<void(const double*, double*)> apply, uint64_t n, const double* b) {
+  orc_cg* s = new orc_cg();
+  s->apply = std::move(apply);
+  s->n = n;
+  s->b.assign(b, b + n);
+  s->x.assign(n, 0.0);
+  s->r = s->b;
+  s->d = s->b;
+  s->q.assign(n, 0.0);
+  s->delta = det_dot(s->r.data(), s->r.data(), n);
+  return s;
+}
+orc_cg* orc_cg2_new(const orc_tree2* t, const double* b) {
+  return cg_new([t](const double* x, double* y) { orc_tree2_apply(t, x, y); }, t->n, b);
+}
+orc_cg* orc_cg1_new(const orc_tree* t, double pw, const double* b) {
+  return cg_new([t, pw](const double* x, double* y) { orc_tree_apply_mf(t, pw, x, y); }, t->n, b);
+}
+double orc_cg_step(orc_cg* s) {
+  const uint64_t n = s->n;
+  s->apply(s->d.data(), s->q.data());
+  const double dq = det_dot(s->d.data(), s->q.data(), n);
+  if (dq == 0.0) return s->delta;
+  const double alpha = s->delta / dq;
+  par_axpy(s->x.data(), alpha, s->d.data(), n);
+  if ((s->it + 1) % 10 == 0) {
+    s->apply(s->x.data(), s->q.data());
+    par_sub(s->r.data(), s->b.data(), s->q.data(), n);
+  } else {
+    par_axpy(s->r.data(), -alpha, s->q.data(), n);
+  }
+  const double delta_old = s->delta;
+  s->delta = det_dot(s->r.data(), s->r.data(), n);
+  par_xpby(s->d.data(), s->r.data(), s->delta / delta_old, n);
+  ++s->it;
+  return s->delta;
+}
+void orc_cg_free(orc_cg* s) { delete s; }
 
 // CG (from x = 0) to ||b - A x|| <= tol ||b||; returns iterations, *relres the final relative residual
 uint64_t orc_tree2_solve(const orc_tree2* t, double tol, uint64_t maxit, double* x, double* relres) {

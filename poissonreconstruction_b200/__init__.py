@@ -90,6 +90,8 @@ SIGNATURES = {
     "pr_ctx_info": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), _P]),
     "pr_ctx_get_coefficients": (C.c_int, [_P, _P]),
     "pr_ctx_get_rhs": (C.c_int, [_P, _P]),
+    "pr_ctx_get_coarse_rhs": (C.c_int, [_P, C.POINTER(C.c_uint32), _P]),
+    "pr_ctx_cg_reference": (C.c_int, [_P, _P, C.c_uint64, C.c_double, _P, _P, C.POINTER(C.c_uint64)]),
     "pr_ctx_get_unit_points": (C.c_int, [_P, _P]),
     "pr_ctx_get_normal_field": (C.c_int, [_P, _P, _P]),
     "pr_ctx_apply_operator": (C.c_int, [_P, _P, _P, C.c_int]),
@@ -420,6 +422,26 @@ class Context:
         _check(lib().pr_ctx_get_rhs(self._h, _ptr(out)))
         return out
 
+    def coarse_rhs(self):
+        """Reference schedule: (coarse depth, right-hand side of its coarse system, Morton order)."""
+        d = C.c_uint32()
+        _check(lib().pr_ctx_get_coarse_rhs(self._h, C.byref(d), None))
+        out = np.zeros(8 ** d.value)
+        _check(lib().pr_ctx_get_coarse_rhs(self._h, C.byref(d), _ptr(out)))
+        return d.value, out
+
+    def cg_reference(self, iters, accuracy, x0=None):
+        """The crate's CG loop on the last degree-1 fine system (FP64, on the device):
+        returns (x, iterations, delta) with delta[k] = ||r||^2 after k iterations."""
+        _, n, _ = self.info()
+        x = np.zeros(n)
+        delta = np.full(int(iters) + 1, np.nan)
+        it = C.c_uint64()
+        x0 = None if x0 is None else np.ascontiguousarray(x0, dtype=np.float64)
+        _check(lib().pr_ctx_cg_reference(self._h, _ptr(x0) if x0 is not None else None, int(iters), float(accuracy),
+                                         _ptr(x), _ptr(delta), C.byref(it)))
+        return x, it.value, delta
+
     def unit_points(self, n_points):
         out = np.zeros((n_points, 6))
         _check(lib().pr_ctx_get_unit_points(self._h, _ptr(out)))
@@ -446,7 +468,8 @@ class Context:
                "resid_restrict_coarse": 8, "cg_update_presmooth": 9,
                # degree 2 (finest level of the given depth)
                "d2_cheb": 20, "d2_cheb_regs": 21, "d2_apply": 22, "d2_apply_regs": 23, "d2_resid": 24,
-               "d2_restrict": 25, "d2_prolong": 26, "d2_cheb_first": 27, "d2_cheb_f": 28, "d2_cheb_pf": 29}
+               "d2_restrict": 25, "d2_prolong": 26, "d2_cheb_first": 27, "d2_cheb_f": 28, "d2_cheb_pf": 29,
+               "d2_cg_dir": 30, "d2_refine": 31}
 
     def kernel_bench(self, kernel, depth, precision=PR_PRECISION_MIXED, reps=10):
         """(ms per launch, algorithmic bytes per launch) of one solver kernel."""

@@ -317,6 +317,7 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
   c->have_mesh = false;
   c->have_coeffs = false;
   c->coeffs_converged = false;
+  c->have_ref_coarse = false;
   c->nv = c->nt = 0;
   if (out_mesh) std::memset(out_mesh, 0, sizeof(*out_mesh));
   if (n == 0) {  // src/reconstructor.rs:28
@@ -730,6 +731,34 @@ int pr_ctx_get_rhs(pr_context* c, double* out) {
       return;
     }
     copy_dev_to_host(c, "b64", out, c->n);
+  });
+}
+
+int pr_ctx_get_coarse_rhs(pr_context* c, uint32_t* coarse_depth, double* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && coarse_depth != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_ref_coarse, PR_ERR_STATE, "the last reconstruction did not run the reference schedule");
+    *coarse_depth = c->ref_coarse_D;
+    if (out) copy_dev_to_host(c, "ref_brhs", out, 1ull << (3 * c->ref_coarse_D));
+  });
+}
+
+int pr_ctx_cg_reference(pr_context* c, const double* x0, uint64_t max_iters, double accuracy, double* x,
+                        double* delta, uint64_t* out_iters) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && x != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(c->degree == 1, PR_ERR_INVALID_ARGUMENT, "the crate's CG runs on the degree-1 system only");
+    set_device(c);
+    const uint64_t n = c->n;
+    double* dx = c->buf<double>("acc_x", n);
+    if (x0) PR_CUDA(cudaMemcpyAsync(dx, x0, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    else PR_CUDA(cudaMemsetAsync(dx, 0, n * sizeof(double), c->stream));
+    const uint64_t it = pr::cg_reference_fine(c, dx, max_iters, accuracy, delta);
+    PR_CUDA(cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    c->release("acc_x");
+    if (out_iters) *out_iters = it;
   });
 }
 

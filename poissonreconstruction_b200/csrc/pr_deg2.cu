@@ -2624,19 +2624,41 @@ double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
   T* p = c->buf<T>("kb2_p_" + tn, n);
   T* y = c->buf<T>("kb2_y_" + tn, n);
   T* ec = c->buf<T>("kb2_c_" + tn, nc);
+  // the fused passes (ids 10, 11) need two more vectors, and the refinement two FP32 ones
+  T* xa = (kid == 10 || kid == 11) ? c->buf<T>("kb2_a_" + tn, n) : nullptr;
+  float* e32 = kid == 11 ? c->buf<float>("kb2_e32", n) : nullptr;
+  float* r32 = kid == 11 ? c->buf<float>("kb2_r32", n) : nullptr;
   k_fill2<T><<<148 * 16, 256, 0, s>>>(x, n, 1u);
   k_fill2<T><<<148 * 16, 256, 0, s>>>(f, n, 2u);
   k_fill2<T><<<148 * 16, 256, 0, s>>>(p, n, 3u);
   k_fill2<T><<<148 * 16, 256, 0, s>>>(ec, nc, 4u);
+  if (xa) k_fill2<T><<<148 * 16, 256, 0, s>>>(xa, n, 5u);
+  if (e32) k_fill2<float><<<148 * 16, 256, 0, s>>>(e32, n, 6u);
   PR_CHECK_LAUNCH();
   System2<T> sys;
   sys.init(c, D, 4.0, false);
   const double nb = (double)n * sizeof(T);
-  const double algo[] = {4 * nb, 4 * nb, 2 * nb, 2 * nb, 3 * nb, nb + nb / 8, 2 * nb + nb / 8, 2 * nb, 2 * nb, 3 * nb};
-  PR_REQUIRE(kid >= 0 && kid < 10, PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
+  // 10: CG direction pass d = z + beta dold, q = A d, x += alpha dold (6 vectors); 11: FP64
+  // refinement step xn = x + e, r = b - A xn, r32 (x, b, xn, r in T; e, r32 in FP32)
+  const double algo[] = {4 * nb, 4 * nb, 2 * nb, 2 * nb, 3 * nb, nb + nb / 8, 2 * nb + nb / 8, 2 * nb, 2 * nb, 3 * nb,
+                         6 * nb, 4 * nb + 8.0 * (double)n};
+  PR_REQUIRE(kid >= 0 && kid < 12, PR_ERR_INVALID_ARGUMENT, "unknown kernel id");
+  PR_REQUIRE(kid != 11 || sizeof(T) == 8, PR_ERR_INVALID_ARGUMENT, "the refinement step is FP64");
   PR_REQUIRE(D >= (uint32_t)kTmaMinLevel || (kid != 0 && kid != 2 && kid != 4 && kid < 8), PR_ERR_INVALID_ARGUMENT,
              "the TMA operator needs depth >= 6");
   *bytes = algo[kid];
+  typename System2<T>::Fuse fu;
+  if (kid == 10) {
+    fu.out2 = p;
+    fu.xacc = xa;
+    fu.s1 = 0.3;
+    fu.s2 = 0.2;
+    fu.xmode = 2;
+  } else if (kid == 11) {
+    fu.out2 = xa;
+    fu.e32 = e32;
+    fu.r32 = r32;
+  }
   const LevelView<T> v = sys.lv[0].view();
   auto run = [&]() {
     switch (kid) {
@@ -2656,7 +2678,9 @@ double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
         PR_CHECK_LAUNCH();
         break;
       case 8: sys.op(0, kOpChebF, f, nullptr, nullptr, y, 0.3, 0.5, 1, 0.6); break;
-      default: sys.op(0, kOpChebPF, x, f, nullptr, y, 0.3, 0.5, 1, 0.6); break;
+      case 9: sys.op(0, kOpChebPF, x, f, nullptr, y, 0.3, 0.5, 1, 0.6); break;
+      case 10: sys.op(0, kOpApplyD, x, f, nullptr, y, 0.0, 0.0, 1, 0.0, nullptr, &fu); break;
+      default: sys.op(0, kOpRefine, x, f, nullptr, y, 0.0, 0.0, 1, 0.0, nullptr, &fu); break;
     }
   };
   run();
@@ -2680,7 +2704,8 @@ double bench2(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
 // Kernel bench of the degree-2 kernels on the finest level of depth D (synthetic vectors):
 // 0 Chebyshev step (TMA), 1 Chebyshev step (register staging), 2 A x (TMA), 3 A x (register
 // staging), 4 f - A x (TMA), 5 restriction, 6 prolongation + add, 7 first Chebyshev step,
-// 8 the first two steps fused (from f), 9 the third step with x1 recomputed from f.
+// 8 the first two steps fused (from f), 9 the third step with x1 recomputed from f, 10 the fused
+// CG direction pass, 11 the fused FP64 refinement step (FP64 only).
 double deg2_kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps, double* bytes) {
   if (reps < 1) reps = 1;
   return precision == PR_PRECISION_FP64 ? bench2<double>(c, kid, D, reps, bytes) : bench2<float>(c, kid, D, reps, bytes);

@@ -140,6 +140,10 @@ struct pr_context {
   uint64_t nv = 0, nt = 0;
   bool have_coeffs = false;
   bool coeffs_converged = false;  // x64 solves A x = b (converged mode), not the reference schedule
+  // reference schedule: its coarse right-hand side "ref_brhs" (depth ref_coarse_D, Morton order)
+  // belongs to the current state
+  bool have_ref_coarse = false;
+  uint32_t ref_coarse_D = 0;
   int degree = 1;                 // node functions of the current state: 1 (the crate's) or 2
   // degree 2: the dense normal field "d2_nf" at address nf_clean (depth nf_clean_D) is zero except
   // at the nf_dirty_T nodes of the last splat (its run keys "d2s_runkey"); nullptr: unknown
@@ -243,6 +247,11 @@ void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double is
                    int degree = 1, bool natural = false);
 void evaluate_points(pr_context* c, uint32_t depth, const double* d_x64, const double* d_pts, uint64_t stride,
                      uint64_t n, double* d_out, int degree = 1);
+
+// the crate's CG loop (src/solvers.rs:20-69) on the current degree-1 fine system, FP64, from the
+// iterate in d_x (n doubles, updated in place); delta (host, may be NULL) receives ||r||^2 before
+// the first iteration and after each one (max_iters + 1 slots); returns the iteration count
+uint64_t cg_reference_fine(pr_context* c, double* d_x, uint64_t max_iters, double accuracy, double* delta);
 
 // operator helpers (pr_operator.cu), exposed for tests through the ABI
 void apply_operator64(pr_context* c, const double* d_x, double* d_y);

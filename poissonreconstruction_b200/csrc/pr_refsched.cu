@@ -143,9 +143,10 @@ __global__ void k_gs_colour(uint32_t D, int colour, double* __restrict__ x, cons
   }
 }
 
-// src/solvers.rs:20-69 with the GPU operator
+// src/solvers.rs:20-69 with the GPU operator; delta (host, may be NULL) receives ||r||^2 before
+// the first iteration and after each one
 uint64_t solve_cg_reference(pr_context* c, const FineOp<double>& A, const double* b, double* x, uint64_t n,
-                            uint64_t max_iters, double accuracy) {
+                            uint64_t max_iters, double accuracy, double* delta = nullptr) {
   cudaStream_t s = c->stream;
   double* r = c->buf<double>("rcg_r", n);
   double* d = c->buf<double>("rcg_d", n);
@@ -154,6 +155,7 @@ uint64_t solve_cg_reference(pr_context* c, const FineOp<double>& A, const double
   PR_CUDA(cudaMemcpyAsync(d, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   double delta_new = dot<double>(c, r, r, n);
   const double delta_0 = delta_new;
+  if (delta) delta[0] = delta_new;
   if (delta_new == 0.0) return 0;
   for (uint64_t iter = 0; iter < max_iters; ++iter) {
     A.apply(s, d, q);
@@ -168,6 +170,7 @@ uint64_t solve_cg_reference(pr_context* c, const FineOp<double>& A, const double
     } else {
       delta_new = cg_update<double>(c, n, alpha, d, q, x, r);
     }
+    if (delta) delta[iter + 1] = delta_new;
     if (delta_new <= delta_0 * accuracy * accuracy) return iter + 1;
     double beta = delta_new / delta_old;
     if (std::isnan(beta) || std::isinf(beta)) break;
@@ -219,6 +222,8 @@ void stage_solve_reference(pr_context* c, const pr_params& p, pr_stats& st) {
   Ac.D = Dc;
   Ac.coef = stencil_coef(Dc, eff_pw > 0.0 ? wh3c * 1.005 : 0.0);
   double* brhs = c->buf<double>("ref_brhs", ncoarse);
+  c->have_ref_coarse = true;
+  c->ref_coarse_D = Dc;
   double* csol = c->buf<double>("ref_csol", ncoarse);
   k_coarse_rhs<<<grid_for(ncoarse), kThreads, 0, s>>>(c->get<uint32_t>("splat_runkey"), c->T, c->get<double>("nfield"),
                                                      Dc, D - Dc, eff_pw > 0.0 ? wh3c * 0.5 : 0.0, brhs);
@@ -250,6 +255,18 @@ void stage_solve_reference(pr_context* c, const pr_params& p, pr_stats& st) {
   st.converged = 0;
   c->have_coeffs = true;
   if (smap) c->release("ref_smap");
+}
+
+uint64_t cg_reference_fine(pr_context* c, double* d_x, uint64_t max_iters, double accuracy, double* delta) {
+  const uint32_t D = c->D;
+  const double h = 1.0 / (double)(1u << D);
+  const double wg = c->pw > 0.0 ? (c->pw * (h * h * h) / 1.5) * 0.005 : 0.0;
+  FineOp<double> A = make_fine_op<double>(c, wg);
+  const uint64_t it = solve_cg_reference(c, A, c->get<double>("b64"), d_x, c->n, max_iters, accuracy, delta);
+  c->release("rcg_r");
+  c->release("rcg_d");
+  c->release("rcg_q");
+  return it;
 }
 
 }  // namespace pr

@@ -357,3 +357,27 @@ def test_deg2_solve_and_pipeline():
     e = np.sort(np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]]), axis=1)
     _, counts = np.unique(e, axis=0, return_counts=True)
     assert np.all(counts == 2)
+
+
+# ---------------------------------------------------------------- matrix-free oracle operator
+@pytest.mark.parametrize("depth,pw", [(3, 4.0), (4, 4.0), (5, 4.0), (4, 0.0)])
+def test_matrix_free_operator_and_cg_match_the_csr(depth, pw):
+    """The matrix-free operator (used where the crate's CSR does not fit in host memory) gives
+    the CSR product of assemble_system to rounding, and its CG (the crate's loop) the same
+    iterates as the CSR CG."""
+    pts = synthetic.sphere(3000, seed=7)
+    unit, _ = oracle.to_unit(pts)
+    t = oracle.Tree(depth, unit)
+    ptr, col, val = t.assemble(pw)
+    x = np.random.default_rng(depth).standard_normal(t.n)
+    y_csr, y_mf = t.spmv(x), t.apply_mf(x, pw)
+    assert np.max(np.abs(y_csr - y_mf)) <= 1e-14 * np.max(np.abs(y_csr))
+    b = t.rhs(pw)
+    x_mf, it_mf, delta = t.cg_mf(b, pw, 20, 1e-30)
+    x_csr, it_csr = oracle.csr_cg(ptr, col, val, b, np.zeros(t.n), 20, 1e-30)
+    assert it_mf == it_csr == 20 and np.all(np.isfinite(delta))
+    assert np.linalg.norm(x_mf - x_csr) <= 1e-13 * np.linalg.norm(x_csr)
+    xc, _, rr = t.solve_converged(pw, tol=1e-12)
+    t.release_field()
+    xm, _, rm = t.solve_converged_mf(b, pw, tol=1e-12)
+    assert rm <= 1e-12 and np.linalg.norm(xm - xc) <= 1e-12 * np.linalg.norm(xc)
