@@ -82,6 +82,7 @@ def parse():
                     help="2: the depth-10 mixed-precision workload (default); 1: the plain method (100k sphere "
                          "points, depth 8, the crate's cascade with cg_iters 8), end to end in both arms")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the coefficient / vertex error block")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload's timing")
     ap.add_argument("--only-device", action="store_true",
                     help="warm-up + timed device-resident steps only (for profiler launch lists)")
     return ap.parse_args()
@@ -564,6 +565,35 @@ def run_ours(a):
                  "pcg_iterations": s1[-1].pcg_iterations, "rel_residual": s1[-1].rel_residual,
                  "fp64_solve_ms": 1000.0 * t1_64, "mixed_vs_fp64_solve_speedup": t1_64 / t1 if t1 > 0 else None}
 
+    # the adjoint workload (1,000,000 superquadric points, depth 9, loss = mean chi^2 at 200,000
+    # surface points): forward solve and backward pass timed on the host clock (mixed precision,
+    # 1e-6), untimed warm-up first
+    adjoint = None
+    if rank == 0 and not a.no_adjoint:
+        ctx.close()
+        ctx = prb.Context(local, stream=stream.cuda_stream)
+        apts = synthetic.superquadric(1_000_000)
+        aq = synthetic.superquadric_queries(200_000)
+        ap = prb.ReconstructParams(depth=9, point_weight=4.0, scale=1.1, precision=prb.PR_PRECISION_MIXED,
+                                   target_rel_residual=1e-6)
+        fw, bw, ast = [], [], None
+        for k in range(4):
+            t0 = time.perf_counter()
+            ctx.solve(apts, ap)
+            t1 = time.perf_counter()
+            _, _, _, ast = ctx.loss_backward(aq)
+            t2 = time.perf_counter()
+            if k > 0:
+                fw.append(1000.0 * (t1 - t0))
+                bw.append(1000.0 * (t2 - t1))
+        adjoint = {"workload": "superquadric_1m_depth9_200k_queries", "forward_ms": statistics.mean(fw),
+                   "backward_ms": statistics.mean(bw), "adjoint_solve_ms": 1000.0 * ast.time_solve,
+                   "adjoint_rel_residual": ast.rel_residual, "adjoint_pcg_iterations": ast.pcg_iterations,
+                   "points_per_s_forward_plus_backward": len(apts) / ((statistics.mean(fw) + statistics.mean(bw))
+                                                                      / 1000.0),
+                   "note": "host clock, points and queries from host memory, gradients copied back"}
+        apts = aq = None
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": a.steps,
@@ -586,6 +616,7 @@ def run_ours(a):
                          "ms_per_launch": kernels[dom]["ms_per_launch"]},
             "kernels": kernels,
             "accuracy": accuracy,
+            "adjoint": adjoint,
             "degree1": other,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

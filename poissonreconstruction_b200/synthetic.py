@@ -166,3 +166,40 @@ def batch_clouds(count=256, seed=SEED_BASE + 4, lo=10_000, hi=500_000):
         depth = 7 if n < 40_000 else (8 if n < 160_000 else 9)
         out.append((pts, depth))
     return out
+
+
+def union_of_spheres(n=20_000_000, seed=SEED_BASE + 5, count=32, rmin=0.05, rmax=0.3, outlier_frac=0.01,
+                     fp32=True):
+    """Large workload: the outer surface of the union of `count` overlapping spheres (centres
+    uniform in the unit cube, radii uniform in [rmin, rmax]) with exact outward normals, plus
+    `outlier_frac` of the points uniform in the cube with random unit normals; n points in all,
+    FP32-rounded.  Surface samples are drawn per sphere in proportion to its area and kept when
+    they lie inside no other sphere."""
+    rng = _rng(seed)
+    c = rng.uniform(0.0, 1.0, (count, 3))
+    r = rng.uniform(rmin, rmax, count)
+    n_out = int(round(outlier_frac * n))
+    n_surf = n - n_out
+    area = r * r
+    chunks, have = [], 0
+    while have < n_surf:
+        m = int((n_surf - have) * 1.5) + 4096
+        k = rng.choice(count, m, p=area / area.sum())
+        g = rng.standard_normal((m, 3))
+        u = g / np.linalg.norm(g, axis=1, keepdims=True)
+        pos = c[k] + r[k, None] * u
+        inside = np.zeros(m, dtype=bool)
+        for j in range(count):
+            d2 = np.sum((pos - c[j]) ** 2, axis=1)
+            inside |= (d2 < r[j] * r[j]) & (k != j)
+        keep = ~inside
+        chunks.append(np.hstack([pos[keep], u[keep]]))
+        have += int(keep.sum())
+    surf = np.concatenate(chunks)[:n_surf]
+    g = rng.standard_normal((n_out, 3))
+    out_pts = np.hstack([rng.uniform(0.0, 1.0, (n_out, 3)), g / np.linalg.norm(g, axis=1, keepdims=True)])
+    pts = np.vstack([surf, out_pts])
+    pts = pts[rng.permutation(n)]
+    if fp32:
+        pts = pts.astype(np.float32).astype(np.float64)
+    return np.ascontiguousarray(pts)

@@ -158,3 +158,53 @@ def test_adjoint_superquadric_depth8(ctx):
         fd = fd_gradient(loss, pts, i, col)
         an = grads[i, col]
         assert abs(fd - an) <= 1e-4 * max(abs(an), 1e-2 * gmax[col]), (i, col, fd, an)
+
+
+def test_adjoint_superquadric_depth9_full_size(ctx, capsys):
+    """The adjoint workload at its own size: 1,000,000 superquadric points (eps1 0.5, eps2 0.8,
+    axes 1/0.7/0.5, normals tilted up to 20 deg), depth 9, loss = mean chi^2 at 200,000 seeded
+    points on the true surface.  The FP64 GPU gradient against 64 central differences (step 1e-4,
+    fourth order: four forward solves to a 1e-13 residual each) at <= 1e-4 relative, with no
+    floor: the coordinates are drawn among those whose gradient is at least 10% of the largest
+    gradient of the same kind (position or normal), off the bbox extremes (the unit-cube transform
+    is held fixed) and 2 steps away from any cell face.  The mixed-precision gradient is checked
+    against the FP64 one (1e-4 relative L2).  The oracle's FP64 adjoint is not run at this size:
+    its CSR system at depth 9 (134 M unknowns) does not fit the host's time; it is compared with
+    the GPU at depths 4-6 above."""
+    D = 9
+    pts = synthetic.superquadric(1_000_000)
+    q = synthetic.superquadric_queries(200_000)
+    p = _params(D, target=1e-13)
+    ctx.solve(pts, p)
+    _, dp64, dn64, st64 = ctx.loss_backward(q)
+    assert st64.converged == 1
+    ctx.solve(pts, _params(D, fp64=False, target=1e-6))
+    _, dp, dn, st = ctx.loss_backward(q)
+    assert st.converged == 1
+    assert _rel(dp, dp64) <= 1e-4 and _rel(dn, dn64) <= 1e-4
+
+    def loss(points):
+        ctx.solve(points, p)
+        _, _, m = ctx.info()
+        m = m.reshape(4, 4).T
+        chi = ctx.evaluate(q @ m[:3, :3].T + m[:3, 3])
+        return float(np.mean(chi ** 2))
+
+    grads = np.hstack([dp64, dn64])
+    big = [np.abs(grads[:, :3]).max(), np.abs(grads[:, 3:]).max()]
+    rng = np.random.default_rng(64)
+    coords = [(i, c) for i, c in fd_coordinates(pts, D, rng, 20000)
+              if abs(grads[i, c]) >= 0.1 * big[c // 3]]
+    assert len(coords) >= 64
+    coords = [coords[k] for k in rng.choice(len(coords), 64, replace=False)]
+    errs = []
+    for i, col in coords:
+        fd = fd_gradient(loss, pts, i, col)
+        an = grads[i, col]
+        errs.append(abs(fd - an) / abs(an))
+    with capsys.disabled():
+        print("\nadjoint, depth 9, 1M points, 200k queries: 64 central differences, relative error max %.2e, "
+              "median %.2e; mixed vs FP64 gradient %.2e / %.2e; adjoint solve %.1f ms (mixed), total %.1f ms"
+              % (max(errs), float(np.median(errs)), _rel(dp, dp64), _rel(dn, dn64), 1000 * st.time_solve,
+                 1000 * st.time_total))
+    assert max(errs) <= 1e-4, errs
