@@ -53,7 +53,7 @@ typedef struct pr_oriented_point {
  * extensions.  pr_params_default() gives ReconstructParams::default() for the crate's
  * fields (src/reconstructor.rs:14). */
 typedef struct pr_params {
-  uint32_t depth;          /* octree depth D; grid res = 2^D; 1 <= D <= 10 */
+  uint32_t depth;          /* octree depth D; grid res = 2^D; 1 <= D <= 10 (12 with coarse_depth) */
   double samples_per_node; /* accepted and ignored, as in the crate */
   double scale;            /* s = scale / max bbox extent (src/geometry.rs:384-388) */
   double cg_accuracy;      /* reference schedule: CG stop ||r||^2 <= ||r0||^2 acc^2 */
@@ -69,8 +69,16 @@ typedef struct pr_params {
   double inner_rel_tol;       /* mixed: relative tolerance of each FP32 inner solve (default 1e-4) */
   uint32_t degree;            /* B-spline degree of the node functions: 1 (the crate's; 0 means 1) or 2
                                  (quadratic B-splines, converged mode only; default 1) */
-  uint32_t reserved[7];
+  uint32_t coarse_depth;      /* 0 (default): one dense grid at `depth`.  Otherwise the adaptive
+                                 (narrow-band) reconstruction, degree 2 only: a dense solve at this
+                                 depth, then the depth-`depth` system on the 8^3-node bricks that hold
+                                 the points' basis functions, with the prolonged coarse solution outside
+                                 them (Jacobi-preconditioned CG, capped at 10 max_iters);
+                                 3 <= depth <= 12, 1 <= depth - coarse_depth <= 4 */
+  uint32_t band_flags;        /* adaptive: PR_BAND_FULL activates every brick (the dense system) */
+  uint32_t reserved[5];
 } pr_params;
+#define PR_BAND_FULL 1u
 
 /* Mesh (src/marching_cubes.rs:8-11).  Vertices are model-space [x,y,z] triples; triangles
  * are vertex-index triples (the crate's usize -> uint64).  Library-owned: free with
@@ -155,6 +163,19 @@ int pr_ctx_get_normal_field(pr_context* ctx, double* out_3n, double* out_weight_
 /* y = A x with the fine operator of src/fem_tree.rs:180-249 (stiffness + screening),
  * matrix-free; precision PR_PRECISION_FP64 or PR_PRECISION_MIXED (FP32 operator, FP64 I/O). */
 int pr_ctx_apply_operator(pr_context* ctx, const double* x_n, double* y_n, int precision);
+/* Adaptive reconstruction (pr_params.coarse_depth > 0) only.  No counterpart in the crate, which
+ * refines every leaf to max_depth (src/fem_tree.rs:83-93); the fine system is the dense one of
+ * pr_params.degree = 2 (src/fem_tree.rs:180-299 with quadratic node functions) restricted to the
+ * band.  Band vectors hold 512 values per active brick, bricks in the order of brick_codes (Morton
+ * codes of the brick coordinates, brick b covering fine nodes 8 b .. 8 b + 7 per axis), nodes in
+ * natural order inside a brick (x fastest).  The dense accessors above refuse an adaptive state. */
+int pr_ctx_band_info(pr_context* ctx, uint32_t* depth, uint32_t* coarse_depth, uint64_t* n_bricks,
+                     uint32_t* brick_codes);
+/* which: 0 = right-hand side b on the band, 1 = the solved coefficients f, 2 = the prolonged coarse
+ * solution g on the band (the function outside the band is g) */
+int pr_ctx_band_get(pr_context* ctx, int which, double* out);
+/* y = A_BB x: the band rows and columns of the fine operator (stiffness, shift, screening), FP64 */
+int pr_ctx_band_apply(pr_context* ctx, const double* x, double* y);
 /* Reference schedule (PR_SOLVE_REFERENCE_SCHEDULE) only: the right-hand side of its coarse
  * system (FEMTree::build_system_at_depth, src/fem_tree.rs:386-402) at *coarse_depth = max(D-2, 0),
  * 8^(*coarse_depth) values in Morton order (out may be NULL to query the depth). */

@@ -32,6 +32,7 @@ PR_SOLVE_CONVERGED = 0
 PR_SOLVE_REFERENCE_SCHEDULE = 1
 PR_PRECISION_MIXED = 0
 PR_PRECISION_FP64 = 1
+PR_BAND_FULL = 1
 
 
 class PrParams(C.Structure):
@@ -39,7 +40,8 @@ class PrParams(C.Structure):
                 ("cg_accuracy", C.c_double), ("cg_iters", C.c_uint64), ("point_weight", C.c_double),
                 ("verbose", C.c_int32), ("solve_mode", C.c_int32), ("precision", C.c_int32),
                 ("target_rel_residual", C.c_double), ("max_iters", C.c_uint32), ("smooth_sweeps", C.c_uint32),
-                ("inner_rel_tol", C.c_double), ("degree", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+                ("inner_rel_tol", C.c_double), ("degree", C.c_uint32), ("coarse_depth", C.c_uint32),
+                ("band_flags", C.c_uint32), ("reserved", C.c_uint32 * 5)]
 
 
 class PrMesh(C.Structure):
@@ -91,6 +93,9 @@ SIGNATURES = {
     "pr_ctx_get_coefficients": (C.c_int, [_P, _P]),
     "pr_ctx_get_rhs": (C.c_int, [_P, _P]),
     "pr_ctx_get_coarse_rhs": (C.c_int, [_P, C.POINTER(C.c_uint32), _P]),
+    "pr_ctx_band_info": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), _P]),
+    "pr_ctx_band_get": (C.c_int, [_P, C.c_int, _P]),
+    "pr_ctx_band_apply": (C.c_int, [_P, _P, _P]),
     "pr_ctx_cg_reference": (C.c_int, [_P, _P, C.c_uint64, C.c_double, _P, _P, C.POINTER(C.c_uint64)]),
     "pr_ctx_get_unit_points": (C.c_int, [_P, _P]),
     "pr_ctx_get_normal_field": (C.c_int, [_P, _P, _P]),
@@ -158,6 +163,8 @@ class ReconstructParams:
     smooth_sweeps: int = 1
     inner_rel_tol: float = 1e-4
     degree: int = 1
+    coarse_depth: int = 0
+    band_flags: int = 0
 
     def to_c(self):
         p = PrParams()
@@ -430,6 +437,29 @@ class Context:
         _check(lib().pr_ctx_get_coarse_rhs(self._h, C.byref(d), _ptr(out)))
         return d.value, out
 
+    # ---- adaptive (coarse_depth > 0) state
+    def band_info(self):
+        """(depth, coarse depth, brick Morton codes (uint32, the band's brick order))."""
+        d, dc, nb = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        _check(lib().pr_ctx_band_info(self._h, C.byref(d), C.byref(dc), C.byref(nb), None))
+        codes = np.zeros(nb.value, dtype=np.uint32)
+        _check(lib().pr_ctx_band_info(self._h, C.byref(d), C.byref(dc), C.byref(nb), _ptr(codes)))
+        return d.value, dc.value, codes
+
+    def band_vector(self, which):
+        """0: right-hand side, 1: solved coefficients, 2: prolonged coarse solution (512 per brick)."""
+        _, _, codes = self.band_info()
+        out = np.zeros(512 * len(codes))
+        _check(lib().pr_ctx_band_get(self._h, int(which), _ptr(out)))
+        return out
+
+    def band_apply(self, x):
+        """A_BB x on the band (FP64)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        _check(lib().pr_ctx_band_apply(self._h, _ptr(x), _ptr(y)))
+        return y
+
     def cg_reference(self, iters, accuracy, x0=None):
         """The crate's CG loop on the last degree-1 fine system (FP64, on the device):
         returns (x, iterations, delta) with delta[k] = ||r||^2 after k iterations."""
@@ -494,6 +524,29 @@ class Context:
         else:
             _check(lib().pr_ctx_extract_at_depth(self._h, int(depth), _ptr(co), float(iso), C.byref(m)))
         return _take_mesh(m)
+
+
+def band_natural_index(codes, depth):
+    """Natural grid index (x + res (y + res z)) of every band entry (bricks in `codes` order, 512
+    nodes per brick, x fastest inside a brick)."""
+    codes = np.asarray(codes, dtype=np.uint64)
+
+    def compact(v):
+        v = v & np.uint64(0x09249249)
+        v = (v | (v >> np.uint64(2))) & np.uint64(0x030C30C3)
+        v = (v | (v >> np.uint64(4))) & np.uint64(0x0300F00F)
+        v = (v | (v >> np.uint64(8))) & np.uint64(0x030000FF)
+        v = (v | (v >> np.uint64(16))) & np.uint64(0x000003FF)
+        return v.astype(np.int64)
+
+    bx, by, bz = compact(codes), compact(codes >> np.uint64(1)), compact(codes >> np.uint64(2))
+    loc = np.arange(512)
+    lx, ly, lz = loc & 7, (loc >> 3) & 7, loc >> 6
+    res = 1 << depth
+    gx = (8 * bx[:, None] + lx[None, :]).ravel()
+    gy = (8 * by[:, None] + ly[None, :]).ravel()
+    gz = (8 * bz[:, None] + lz[None, :]).ravel()
+    return gx + res * (gy + res * gz)
 
 
 def kernel_launches():

@@ -60,8 +60,18 @@ double now_s() {
 
 void validate(const pr_params* p) {
   PR_REQUIRE(p != nullptr, PR_ERR_INVALID_ARGUMENT, "params is NULL");
-  PR_REQUIRE(p->depth >= pr::kMinDepth && p->depth <= pr::kMaxDepth, PR_ERR_INVALID_ARGUMENT,
-             "depth must be in [1, 10] (dense grid of 2^(3 depth) nodes), got " + std::to_string(p->depth));
+  if (p->coarse_depth > 0) {
+    PR_REQUIRE(p->depth >= 3 && p->depth <= pr::kMaxBandDepth, PR_ERR_INVALID_ARGUMENT,
+               "adaptive reconstruction: depth must be in [3, 12], got " + std::to_string(p->depth));
+    PR_REQUIRE(p->coarse_depth < p->depth && p->depth - p->coarse_depth <= 4, PR_ERR_INVALID_ARGUMENT,
+               "adaptive reconstruction: depth - coarse_depth must be in [1, 4]");
+    PR_REQUIRE(p->degree == 2, PR_ERR_INVALID_ARGUMENT, "adaptive reconstruction is built for degree 2");
+    PR_REQUIRE(p->solve_mode == PR_SOLVE_CONVERGED, PR_ERR_INVALID_ARGUMENT,
+               "adaptive reconstruction solves in solve_mode PR_SOLVE_CONVERGED");
+  } else {
+    PR_REQUIRE(p->depth >= pr::kMinDepth && p->depth <= pr::kMaxDepth, PR_ERR_INVALID_ARGUMENT,
+               "depth must be in [1, 10] (dense grid of 2^(3 depth) nodes), got " + std::to_string(p->depth));
+  }
   PR_REQUIRE(std::isfinite(p->scale) && p->scale > 0.0, PR_ERR_INVALID_ARGUMENT, "scale must be finite and > 0");
   PR_REQUIRE(std::isfinite(p->point_weight) && p->point_weight >= 0.0, PR_ERR_INVALID_ARGUMENT,
              "point_weight must be finite and >= 0");
@@ -266,6 +276,19 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   double t1 = now_s();
   st.time_transform = t1 - t0 + (t0 - t_start);
   c->degree = degree_of(p);
+  c->params = p;
+  if (p.coarse_depth > 0) {  // adaptive: coarse level, band setup, band solve, extraction
+    pr::stage_adaptive(c, p, st, extract);
+    st.time_system = 0.0;
+    if (p.verbose)
+      std::fprintf(stderr,
+                   "pr: adaptive depth=%u coarse=%u points=%llu bricks=%llu xform=%.4f tree=%.4f solve=%.4f "
+                   "extract=%.4f s; pcg=%u refine=%u relres=%.3e iso=%.6f verts=%llu tris=%llu\n",
+                   p.depth, p.coarse_depth, (unsigned long long)n, (unsigned long long)c->band_nb, st.time_transform,
+                   st.time_tree, st.time_solve, st.time_extract, st.pcg_iterations, st.refinement_steps,
+                   st.rel_residual, st.iso_value, (unsigned long long)c->nv, (unsigned long long)c->nt);
+    return;
+  }
   if (c->degree == 2) pr::stage_setup_deg2(c, p.depth, p.point_weight);
   else pr::stage_splat_rhs(c, p.depth, p.point_weight);
   c->sync();
@@ -318,6 +341,7 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
   c->have_coeffs = false;
   c->coeffs_converged = false;
   c->have_ref_coarse = false;
+  c->adaptive = false;
   c->nv = c->nt = 0;
   if (out_mesh) std::memset(out_mesh, 0, sizeof(*out_mesh));
   if (n == 0) {  // src/reconstructor.rs:28
@@ -367,6 +391,7 @@ int pr_ctx_apply_operator_device(pr_context* c, const void* d_x, void* d_y, int 
   return guard([&] {
     PR_REQUIRE(c != nullptr && d_x != nullptr && d_y != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     set_device(c);
     if (c->degree == 2) {
       if (precision == PR_PRECISION_FP64) pr::deg2_apply_morton<double>(c, (const double*)d_x, (double*)d_y);
@@ -528,6 +553,7 @@ static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k
   PR_REQUIRE(queries3 != nullptr, PR_ERR_INVALID_ARGUMENT, "queries is NULL");
   PR_REQUIRE(k >= 1 && k <= pr::kMaxPoints, PR_ERR_INVALID_ARGUMENT, "k must be in [1, 2^28] query points");
   PR_REQUIRE(c->have_state && c->have_coeffs, PR_ERR_STATE, "no solved reconstruction on this context");
+  PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
   PR_REQUIRE(c->coeffs_converged, PR_ERR_STATE,
              "the last solve used the reference schedule; the adjoint needs solve_mode PR_SOLVE_CONVERGED");
   PR_REQUIRE(c->degree == 1, PR_ERR_STATE, "the adjoint is implemented for degree 1");
@@ -713,6 +739,7 @@ int pr_ctx_get_coefficients(pr_context* c, double* out) {
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
     PR_REQUIRE(c->have_coeffs, PR_ERR_STATE, "no solved coefficients");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     pr::coeffs_morton(c);
     copy_dev_to_host(c, "x64", out, c->n);
   });
@@ -722,6 +749,7 @@ int pr_ctx_get_rhs(pr_context* c, double* out) {
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     if (c->degree == 2) {
       PR_REQUIRE(out != nullptr, PR_ERR_INVALID_ARGUMENT, "output is NULL");
       set_device(c);
@@ -748,6 +776,7 @@ int pr_ctx_cg_reference(pr_context* c, const double* x0, uint64_t max_iters, dou
   return guard([&] {
     PR_REQUIRE(c != nullptr && x != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     PR_REQUIRE(c->degree == 1, PR_ERR_INVALID_ARGUMENT, "the crate's CG runs on the degree-1 system only");
     set_device(c);
     const uint64_t n = c->n;
@@ -759,6 +788,52 @@ int pr_ctx_cg_reference(pr_context* c, const double* x0, uint64_t max_iters, dou
     c->sync();
     c->release("acc_x");
     if (out_iters) *out_iters = it;
+  });
+}
+
+int pr_ctx_band_info(pr_context* c, uint32_t* depth, uint32_t* coarse_depth, uint64_t* n_bricks, uint32_t* brick_codes) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
+    PR_REQUIRE(c->have_state && c->adaptive, PR_ERR_STATE, "no adaptive reconstruction state");
+    if (depth) *depth = c->D;
+    if (coarse_depth) *coarse_depth = c->band_Dc;
+    if (n_bricks) *n_bricks = c->band_nb;
+    if (brick_codes && c->band_nb) {
+      set_device(c);
+      PR_CUDA(cudaMemcpyAsync(brick_codes, c->get<uint32_t>("ab_bkey"), c->band_nb * sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, c->stream));
+      c->sync();
+    }
+  });
+}
+
+int pr_ctx_band_get(pr_context* c, int which, double* out) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && out != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_state && c->adaptive, PR_ERR_STATE, "no adaptive reconstruction state");
+    set_device(c);
+    double* d = c->buf<double>("acc_band", std::max<uint64_t>(c->n, 1));
+    pr::band_vector(c, which, d);
+    if (c->n) PR_CUDA(cudaMemcpyAsync(out, d, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    c->release("acc_band");
+  });
+}
+
+int pr_ctx_band_apply(pr_context* c, const double* x, double* y) {
+  return guard([&] {
+    PR_REQUIRE(c != nullptr && x != nullptr && y != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
+    PR_REQUIRE(c->have_state && c->adaptive, PR_ERR_STATE, "no adaptive reconstruction state");
+    set_device(c);
+    const uint64_t n = std::max<uint64_t>(c->n, 1);
+    double* dx = c->buf<double>("acc_bx", n);
+    double* dy = c->buf<double>("acc_by", n);
+    PR_CUDA(cudaMemcpyAsync(dx, x, c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    pr::band_apply64(c, dx, dy);
+    PR_CUDA(cudaMemcpyAsync(y, dy, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    c->release("acc_bx");
+    c->release("acc_by");
   });
 }
 
@@ -785,6 +860,7 @@ int pr_ctx_get_normal_field(pr_context* c, double* out3, double* outw) {
   return guard([&] {
     PR_REQUIRE(c != nullptr && out3 != nullptr && outw != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     set_device(c);
     double* nf = c->buf<double>("acc_nf3", 3 * c->n);
     double* w = c->buf<double>("acc_w", c->n);
@@ -802,6 +878,7 @@ int pr_ctx_apply_operator(pr_context* c, const double* x, double* y, int precisi
   return guard([&] {
     PR_REQUIRE(c != nullptr && x != nullptr && y != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL argument");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     set_device(c);
     const uint64_t n = c->n;
     double* dx = c->buf<double>("acc_x", n);
@@ -828,6 +905,7 @@ int pr_ctx_evaluate(pr_context* c, const double* coeffs, const double* pts3, uin
     PR_REQUIRE(c != nullptr && (pts3 != nullptr || n == 0) && (out != nullptr || n == 0), PR_ERR_INVALID_ARGUMENT,
                "NULL argument");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     set_device(c);
     if (n == 0) return;
     const double* dx;
@@ -866,6 +944,7 @@ int pr_ctx_extract(pr_context* c, const double* coeffs, double iso, pr_mesh* out
   return guard([&] {
     PR_REQUIRE(c != nullptr, PR_ERR_INVALID_ARGUMENT, "context is NULL");
     PR_REQUIRE(c->have_state, PR_ERR_STATE, "no reconstruction state");
+    PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
     extract_common(c, c->D, coeffs, iso, out, c->degree);
   });
 }

@@ -1,0 +1,1245 @@
+// Adaptive (narrow-band) reconstruction: depth up to 12 without a dense fine grid.  An
+// extension: the crate refines every leaf to max_depth and ignores the points
+// (src/fem_tree.rs:83-93), so its grid is the dense res^3 one (src/fem_tree.rs:96-126), which at
+// depth 12 would hold 6.9e10 nodes.  Here the fine level exists only where the points are.
+//
+//   1. coarse level: the dense degree-2 reconstruction system at depth Dc (the solver of
+//      pr_deg2.cu), solved to the requested residual; x_c its coefficients;
+//   2. bricks: the fine grid (depth D) is cut into bricks of 8^3 nodes; a brick is active when
+//      it holds a node of some point's 27 basis functions (every point's support lies in active
+//      bricks), or every brick with PR_BAND_FULL.  B = the nodes of active bricks (the band),
+//      H = every other node;
+//   3. the fine function is u = sum_{i in B} f_i phi_i + sum_{j in H} g_j phi_j, where g = P^L x_c
+//      (L = D - Dc levels of the B2 subdivision, the exact depth-D coefficients of the coarse
+//      function): f solves the depth-D system of the dense degree-2 reconstruction restricted to
+//      B with g fixed on H,
+//            A_BB f = b_B - A_BH g_H,
+//      A and b being exactly the dense system's (stiffness, screening of every point, splat of the
+//      normals, right-hand side); with every brick active this IS the dense system.  Written as
+//      f = g_B + e: A_BB e = r0 = b_B - (A g)_B;
+//   4. A_BB e = r0 by Jacobi-preconditioned CG: FP32 inner solves with FP64 residual refinement,
+//      or FP64 throughout (the same precision modes as the dense solve);
+//   5. iso = mean over the points of the fine function; marching cubes over the cells of the
+//      active bricks (corner values from f on B and g on H), vertices deduplicated by grid-edge key.
+//
+// Layout: band vectors are brick-major, 512 nodes per brick in natural order (x fastest); bricks
+// are sorted by their Morton code, so a brick's neighbours are mostly near it in memory.  The
+// operator pass gives each CTA one brick: its 12^3 tile (brick and 2-node halo, gathered from the
+// 27 neighbouring bricks, zero on H) goes to shared memory and the separable stencil
+// h (S M M + M S M + M M S) runs as z, y and x passes there.  The screening term reuses the
+// dense path's (node, point) pair lists, keyed by band index.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "pr_internal.cuh"
+#include "pr_ops.cuh"
+
+#define PR_MC_TABLE_QUAL static __constant__
+#include "mc_tri_table.inc"
+
+namespace pr {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kSent = 0xffffffffu;  // no brick / no node
+constexpr int kBN = 512;                 // nodes per brick
+constexpr int kOT = 12;                  // operator tile edge: brick + 2-node halo
+constexpr int kOT3 = kOT * kOT * kOT;
+constexpr int kMT = 10;                  // marching-cubes node tile edge: brick + 1 node each side
+constexpr int kMaxW = 64;                // taps of the composite prolongation (L <= 4: 46)
+
+inline unsigned grid_for(uint64_t n, uint64_t cap = 1u << 22) {
+  uint64_t g = (n + kThreads - 1) / kThreads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+inline unsigned brick_grid(uint64_t nb) { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(nb, 148 * 64)); }
+
+// 1-D integrals of N2 N2, N2' N2', N2' N2 (offsets -2..2), the operator's scale and shift
+template <typename T>
+struct BandCoef {
+  T m[5], s[5];
+  T H, wg;
+};
+// g_f = sum_I w[f - 2^L I - kmin] x_c[I] per axis
+struct Prolong {
+  double w[kMaxW];
+  int kmin, kmax, L, resc;
+};
+
+// degree-2 basis of one axis at unit coordinate u (the dense setup's expressions, so that the
+// basis values of a point are the same bits in both paths)
+__device__ __forceinline__ void axis2b(double u, double h, int64_t& c, double* b) {
+  const double s = xdiv(u, h);
+  c = sat_i64(floor(s));
+  const double t = xsub(s, (double)c);
+  const double omt = xsub(1.0, t);
+  b[0] = xmul(xmul(0.5, omt), omt);
+  b[1] = xmul(0.5, xadd(xadd(xmul(xmul(-2.0, t), t), xmul(2.0, t)), 1.0));
+  b[2] = xmul(xmul(0.5, t), t);
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// the coarse function's depth-D coefficient at fine node (fx, fy, fz) (x_c natural order)
+__device__ double prolong_at(const double* __restrict__ xc, const Prolong& W, int fx, int fy, int fz) {
+  const int step = 1 << W.L;
+  int i0[3], i1[3];
+  const int f[3] = {fx, fy, fz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    i0[a] = max(0, -floor_div(W.kmax - f[a], step));  // ceil((f - kmax) / step)
+    i1[a] = min(W.resc - 1, floor_div(f[a] - W.kmin, step));
+  }
+  double v = 0.0;
+  for (int iz = i0[2]; iz <= i1[2]; ++iz) {
+    const double wz = W.w[fz - step * iz - W.kmin];
+    for (int iy = i0[1]; iy <= i1[1]; ++iy) {
+      const double wy = wz * W.w[fy - step * iy - W.kmin];
+      const double* row = xc + (int64_t)W.resc * (iy + (int64_t)W.resc * iz);
+      for (int ix = i0[0]; ix <= i1[0]; ++ix) v += wy * W.w[fx - step * ix - W.kmin] * row[ix];
+    }
+  }
+  return v;
+}
+
+// ------------------------------------------------------------------ bricks
+// the bricks holding nodes c-1 .. c+1 of each point (up to 2 per axis), Morton-coded; duplicates
+// and points outside the grid give kSent
+__global__ void k_ab_brick_keys(const double* __restrict__ upos, uint64_t P, uint32_t D, uint32_t* __restrict__ keys) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int64_t c = sat_i64(floor(xdiv(upos[(uint64_t)a * P + p], h)));
+      const int64_t a0 = c - 1 < 0 ? 0 : c - 1, a1 = c + 1 > res - 1 ? res - 1 : c + 1;
+      if (a0 > a1) ok = false;
+      else {
+        lo[a] = (uint32_t)(a0 >> 3);
+        hi[a] = (uint32_t)(a1 >> 3);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int sx = k & 1, sy = (k >> 1) & 1, sz = k >> 2;
+      const bool dup = (sx && hi[0] == lo[0]) || (sy && hi[1] == lo[1]) || (sz && hi[2] == lo[2]);
+      keys[8 * p + k] = (!ok || dup) ? kSent : morton3(sx ? hi[0] : lo[0], sy ? hi[1] : lo[1], sz ? hi[2] : lo[2]);
+    }
+  }
+}
+
+__global__ void k_ab_iota(uint32_t* __restrict__ v, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+
+__global__ void k_ab_brick_map(const uint32_t* __restrict__ bkey, uint64_t NB, uint32_t* __restrict__ bmap) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < NB; s += (uint64_t)gridDim.x * blockDim.x)
+    bmap[bkey[s]] = (uint32_t)s;
+}
+
+// 27 neighbour slots per brick, k = 9 (dz + 1) + 3 (dy + 1) + (dx + 1)
+__global__ void k_ab_neighbours(const uint32_t* __restrict__ bkey, uint64_t NB, uint32_t nbr_res,
+                                const uint32_t* __restrict__ bmap, uint32_t* __restrict__ nbr) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 27 * NB; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = i / 27;
+    const int k = (int)(i - 27 * s);
+    uint32_t bx, by, bz;
+    unmorton3(bkey[s], bx, by, bz);
+    const int x = (int)bx + k % 3 - 1, y = (int)by + (k / 3) % 3 - 1, z = (int)bz + k / 9 - 1;
+    const bool in = x >= 0 && y >= 0 && z >= 0 && x < (int)nbr_res && y < (int)nbr_res && z < (int)nbr_res;
+    nbr[i] = in ? bmap[morton3((uint32_t)x, (uint32_t)y, (uint32_t)z)] : kSent;
+  }
+}
+
+// (band node, 27 p + k) pairs of the points' basis functions, with the basis values (the dense
+// degree-2 setup's pairs with the band index in place of the natural one)
+__global__ void k_ab_pair_keys(const double* __restrict__ upos, uint64_t P, uint32_t D, const uint32_t* __restrict__ bmap,
+                               uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, double* __restrict__ phi64,
+                               float* __restrict__ phi32, unsigned long long* __restrict__ nin) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  unsigned long long cnt = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 27 * P; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = i / 27;
+    const int k = (int)(i - 27 * p), dx = k % 3, dy = (k / 3) % 3, dz = k / 9;
+    int64_t c[3];
+    double b[3][3];
+    axis2b(upos[p], h, c[0], b[0]);
+    axis2b(upos[P + p], h, c[1], b[1]);
+    axis2b(upos[2 * P + p], h, c[2], b[2]);
+    const int64_t x = c[0] + dx - 1, y = c[1] + dy - 1, z = c[2] + dz - 1;
+    bool ok = x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res;
+    uint32_t key = kSent;
+    if (ok) {
+      const uint32_t slot = bmap[morton3((uint32_t)(x >> 3), (uint32_t)(y >> 3), (uint32_t)(z >> 3))];
+      ok = slot != kSent;
+      if (ok) key = slot * (uint32_t)kBN + (uint32_t)(((z & 7) << 6) | ((y & 7) << 3) | (x & 7));
+    }
+    keys[i] = key;
+    vals[i] = (uint32_t)i;
+    const double phi = ok ? xmul(xmul(b[0][dx], b[1][dy]), b[2][dz]) : 0.0;
+    phi64[i] = phi;
+    phi32[i] = (float)phi;
+    if (k == 0)
+      cnt += (c[0] + 1 >= 0 && c[0] - 1 < res && c[1] + 1 >= 0 && c[1] - 1 < res && c[2] + 1 >= 0 && c[2] - 1 < res);
+  }
+  typedef cub::BlockReduce<unsigned long long, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const unsigned long long tot = BR(tmp).Sum(cnt);
+  if (threadIdx.x == 0 && tot) atomicAdd(nin, tot);
+}
+
+// per touched node (points in input order): nf = -(sum phi n) / (sum phi), sum phi, sum phi^2
+__global__ void k_ab_splat(const uint32_t* __restrict__ run_off, uint64_t T, const uint32_t* __restrict__ sval,
+                           const double* __restrict__ phi, const double* __restrict__ unrm, uint64_t P,
+                           double* __restrict__ nfc, double* __restrict__ sphi, double* __restrict__ sphi2) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    double fx = 0.0, fy = 0.0, fz = 0.0, sw = 0.0, s2 = 0.0;
+    for (uint32_t e = run_off[t]; e < run_off[t + 1]; ++e) {
+      const uint32_t pk = sval[e];
+      const uint32_t p = pk / 27;
+      const double wgt = phi[pk];
+      fx = xadd(fx, xmul(unrm[p], wgt));
+      fy = xadd(fy, xmul(unrm[P + p], wgt));
+      fz = xadd(fz, xmul(unrm[2 * P + p], wgt));
+      sw = xadd(sw, wgt);
+      s2 += wgt * wgt;
+    }
+    if (sw > 0.0) {
+      fx = xdiv(-fx, sw);
+      fy = xdiv(-fy, sw);
+      fz = xdiv(-fz, sw);
+    }
+    nfc[3 * t] = fx;
+    nfc[3 * t + 1] = fy;
+    nfc[3 * t + 2] = fz;
+    sphi[t] = sw;
+    sphi2[t] = s2;
+  }
+}
+
+// brun[s] = first run of brick s (runs sorted by band key, key / 512 = brick)
+__global__ void k_ab_brick_runs(const uint32_t* __restrict__ run_key, uint64_t T, uint64_t NB,
+                                uint32_t* __restrict__ brun) {
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s <= NB; s += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t target = s * kBN;
+    uint64_t a = 0, b = T;
+    while (a < b) {
+      const uint64_t m = (a + b) >> 1;
+      if ((uint64_t)run_key[m] < target) a = m + 1;
+      else b = m;
+    }
+    brun[s] = (uint32_t)a;
+  }
+}
+
+// ------------------------------------------------------------------ right-hand side
+// b = h^2 sum_a (G_a M M) nf_a + (wh3 / 2) sum_p phi: per brick, the normal field of the brick
+// and its 2-node halo into a shared tile (zero where no point splatted), then z, y and x passes
+__global__ void __launch_bounds__(kThreads) k_ab_rhs(const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ run_key,
+                                                     const uint32_t* __restrict__ brun, const double* __restrict__ nfc,
+                                                     const double* __restrict__ sphi, double wt, BandCoef<double> K,
+                                                     double g0, double g1, double g3, double g4, double h2, uint64_t NB,
+                                                     double* __restrict__ b) {
+  extern __shared__ double sm[];
+  double* nf = sm;                  // [3][12][12][12]
+  double* tz = nf + 3 * kOT3;       // [8][12][12]
+  double* ty = tz + 8 * kOT * kOT;  // [8][8][12]
+  double* ob = ty + 8 * 8 * kOT;    // [512]
+  __shared__ uint32_t nb[27];
+  const int t = threadIdx.x;
+  const double gg[5] = {g0, g1, 0.0, g3, g4};
+  for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
+    if (t < 27) nb[t] = nbr[27 * slot + t];
+    for (int i = t; i < 3 * kOT3; i += kThreads) nf[i] = 0.0;
+    __syncthreads();
+    for (int k = 0; k < 27; ++k) {
+      const uint32_t s2 = nb[k];
+      if (s2 == kSent) continue;
+      const int ox = k % 3 - 1, oy = (k / 3) % 3 - 1, oz = k / 9 - 1;
+      for (uint32_t r = brun[s2] + t; r < brun[s2 + 1]; r += kThreads) {
+        const uint32_t local = run_key[r] - s2 * (uint32_t)kBN;
+        const int tx = (int)(local & 7) + 8 * ox + 2, ty_ = (int)((local >> 3) & 7) + 8 * oy + 2,
+                  tz_ = (int)(local >> 6) + 8 * oz + 2;
+        if (tx < 0 || ty_ < 0 || tz_ < 0 || tx >= kOT || ty_ >= kOT || tz_ >= kOT) continue;
+        const int o = (tz_ * kOT + ty_) * kOT + tx;
+        nf[o] = nfc[3 * (uint64_t)r];
+        nf[kOT3 + o] = nfc[3 * (uint64_t)r + 1];
+        nf[2 * kOT3 + o] = nfc[3 * (uint64_t)r + 2];
+      }
+    }
+    __syncthreads();
+    double acc[2] = {0.0, 0.0};
+    for (int a = 0; a < 3; ++a) {
+      const double* fz = a == 2 ? gg : K.m;
+      const double* fy = a == 1 ? gg : K.m;
+      const double* fx = a == 0 ? gg : K.m;
+      const double* src = nf + a * kOT3;
+      for (int i = t; i < 8 * kOT * kOT; i += kThreads) {
+        const int z = i / (kOT * kOT), yx = i % (kOT * kOT);
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v += fz[c] * src[(z + c) * kOT * kOT + yx];
+        tz[i] = v;
+      }
+      __syncthreads();
+      for (int i = t; i < 8 * 8 * kOT; i += kThreads) {
+        const int z = i / (8 * kOT), y = (i / kOT) % 8, x = i % kOT;
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v += fy[c] * tz[(z * kOT + y + c) * kOT + x];
+        ty[i] = v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int o = t + j * kThreads, z = o >> 6, y = (o >> 3) & 7, x = o & 7;
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v += fx[c] * ty[(z * 8 + y) * kOT + x + c];
+        acc[j] += v;
+      }
+      __syncthreads();
+    }
+    ob[t] = h2 * acc[0];
+    ob[t + kThreads] = h2 * acc[1];
+    __syncthreads();
+    for (uint32_t r = brun[slot] + t; r < brun[slot + 1]; r += kThreads)
+      ob[run_key[r] - (uint32_t)slot * kBN] += wt * sphi[r];
+    __syncthreads();
+    b[slot * kBN + t] = ob[t];
+    b[slot * kBN + t + kThreads] = ob[t + kThreads];
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ the band operator
+// MODE 0: y = A_BB x;  MODE 1: y = f - A_BB x.  Stiffness and shift only (the screening term is a
+// separate pass).  With xc != nullptr the tile is the prolonged coarse function g everywhere
+// (x unused): y = (K + wg I) g on the band.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) k_ab_op(const T* __restrict__ x, const T* __restrict__ f, T* __restrict__ y,
+                                                    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ bkey,
+                                                    uint64_t NB, BandCoef<T> K, const double* __restrict__ xc, Prolong W,
+                                                    int res) {
+  __shared__ T tile[kOT3];
+  __shared__ T um[8 * kOT * kOT], us[8 * kOT * kOT];
+  __shared__ T w1[8 * 8 * kOT], w23[8 * 8 * kOT];
+  __shared__ uint32_t nb[27];
+  const int t = threadIdx.x;
+  for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
+    if (t < 27) nb[t] = nbr[27 * slot + t];
+    uint32_t bx = 0, by = 0, bz = 0;
+    if (xc) unmorton3(bkey[slot], bx, by, bz);
+    __syncthreads();
+    for (int i = t; i < kOT3; i += kThreads) {
+      const int lz = i / (kOT * kOT) - 2, ly = (i / kOT) % kOT - 2, lx = i % kOT - 2;
+      T v = T(0);
+      if (xc) {
+        const int gx = 8 * (int)bx + lx, gy = 8 * (int)by + ly, gz = 8 * (int)bz + lz;
+        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) v = (T)prolong_at(xc, W, gx, gy, gz);
+      } else {
+        const int ox = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0),
+                  oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
+        const uint32_t s2 = nb[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
+        if (s2 != kSent) v = x[(uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox))];
+      }
+      tile[i] = v;
+    }
+    __syncthreads();
+    for (int i = t; i < 8 * kOT * kOT; i += kThreads) {
+      const int z = i / (kOT * kOT), yx = i % (kOT * kOT);
+      T am = T(0), as = T(0);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const T v = tile[(z + c) * kOT * kOT + yx];
+        am += K.m[c] * v;
+        as += K.s[c] * v;
+      }
+      um[i] = am;
+      us[i] = as;
+    }
+    __syncthreads();
+    for (int i = t; i < 8 * 8 * kOT; i += kThreads) {
+      const int z = i / (8 * kOT), yy = (i / kOT) % 8, xx = i % kOT;
+      T a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const int q = (z * kOT + yy + c) * kOT + xx;
+        a1 += K.m[c] * um[q];
+        a2 += K.s[c] * um[q];
+        a3 += K.m[c] * us[q];
+      }
+      w1[i] = a1;
+      w23[i] = a2 + a3;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int o = t + j * kThreads, z = o >> 6, yy = (o >> 3) & 7, xx = o & 7;
+      const int r = (z * 8 + yy) * kOT + xx;
+      T acc = T(0);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc += K.s[c] * w1[r + c] + K.m[c] * w23[r + c];
+      const T v = K.H * acc + K.wg * tile[((z + 2) * kOT + yy + 2) * kOT + xx + 2];
+      const uint64_t gi = slot * kBN + o;
+      y[gi] = MODE == 0 ? v : f[gi] - v;
+    }
+    __syncthreads();
+  }
+}
+
+// screening: proj_p = sum_k phi x[key]; y[node] += sgn wh3 sum phi proj over the node's pairs
+template <typename T>
+__global__ void k_ab_screen_proj(const uint32_t* __restrict__ key, const T* __restrict__ phi, uint64_t P,
+                                 const T* __restrict__ x, T* __restrict__ proj) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
+    T s = T(0);
+    for (int k = 0; k < 27; ++k) {
+      const uint32_t kk = key[27 * p + k];
+      if (kk != kSent) s += phi[27 * p + k] * x[kk];
+    }
+    proj[p] = s;
+  }
+}
+template <typename T>
+__global__ void k_ab_screen_gather(const uint32_t* __restrict__ snode, const uint32_t* __restrict__ soff, uint64_t S,
+                                   const uint32_t* __restrict__ sval, const T* __restrict__ phi,
+                                   const T* __restrict__ proj, T wh3s, T* __restrict__ y) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < S; u += (uint64_t)gridDim.x * blockDim.x) {
+    T acc = T(0);
+    for (uint32_t e = soff[u]; e < soff[u + 1]; ++e) {
+      const uint32_t pk = sval[e];
+      acc += phi[pk] * proj[pk / 27];
+    }
+    y[snode[u]] += wh3s * acc;
+  }
+}
+
+// Jacobi: 1 / (interior diagonal + wh3 sum phi^2)
+template <typename T>
+__global__ void k_ab_dinv(double diag, uint64_t n, T* __restrict__ dinv) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    dinv[i] = (T)(1.0 / diag);
+}
+template <typename T>
+__global__ void k_ab_dinv_screen(const uint32_t* __restrict__ run_key, const double* __restrict__ sphi2, uint64_t T_runs,
+                                 double diag, double wh3, T* __restrict__ dinv) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < T_runs; r += (uint64_t)gridDim.x * blockDim.x)
+    dinv[run_key[r]] = (T)(1.0 / (diag + wh3 * sphi2[r]));
+}
+template <typename T>
+__global__ void k_ab_mul(const T* __restrict__ a, const T* __restrict__ b, uint64_t n, T* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = a[i] * b[i];
+}
+
+// g on the band nodes
+__global__ void k_ab_prolong_band(const uint32_t* __restrict__ bkey, uint64_t NB, const double* __restrict__ xc,
+                                  Prolong W, double* __restrict__ g) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < NB * kBN; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t bx, by, bz;
+    unmorton3(bkey[i / kBN], bx, by, bz);
+    const int l = (int)(i % kBN);
+    g[i] = prolong_at(xc, W, 8 * (int)bx + (l & 7), 8 * (int)by + ((l >> 3) & 7), 8 * (int)bz + (l >> 6));
+  }
+}
+
+// ------------------------------------------------------------------ iso value
+struct Neu {
+  double s, c;
+};
+__device__ __forceinline__ Neu neu_add(Neu a, double v) {
+  const double t = a.s + v;
+  if (fabs(a.s) >= fabs(v)) a.c += (a.s - t) + v;
+  else a.c += (v - t) + a.s;
+  a.s = t;
+  return a;
+}
+__global__ void k_ab_iso_partial(const double* __restrict__ f, const uint32_t* __restrict__ key,
+                                 const double* __restrict__ phi, uint64_t P, double* __restrict__ part) {
+  Neu acc{0.0, 0.0};
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int k = 0; k < 27; ++k) {
+      const uint32_t kk = key[27 * p + k];
+      if (kk != kSent) v = xadd(v, xmul(f[kk], phi[27 * p + k]));
+    }
+    acc = neu_add(acc, v);
+  }
+  __shared__ double ss[kThreads], sc[kThreads];
+  ss[threadIdx.x] = acc.s;
+  sc[threadIdx.x] = acc.c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Neu t{0.0, 0.0};
+    for (int i = 0; i < kThreads; ++i) {
+      t = neu_add(t, ss[i]);
+      t = neu_add(t, sc[i]);
+    }
+    part[2 * blockIdx.x] = t.s;
+    part[2 * blockIdx.x + 1] = t.c;
+  }
+}
+__global__ void k_ab_iso_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  Neu t{0.0, 0.0};
+  for (int i = 0; i < nb; ++i) {
+    t = neu_add(t, part[2 * i]);
+    t = neu_add(t, part[2 * i + 1]);
+  }
+  out[0] = t.s + t.c;
+}
+
+// ------------------------------------------------------------------ marching cubes
+__constant__ int c_abco[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+__constant__ int c_abev[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+__device__ __forceinline__ uint32_t ab_edge_mask(uint32_t mc) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int e = 0; e < 12; ++e)
+    if (((mc >> c_abev[e][0]) & 1u) != ((mc >> c_abev[e][1]) & 1u)) m |= 1u << e;
+  return m;
+}
+
+// The brick's 9^3 corner values at grid positions 8b + q (q = 0..8 per axis): node tile 10^3
+// (nodes 8b - 1 .. 8b + 8; f on the band, g elsewhere), each corner the in-order sum over the
+// nodes p - 1, p per axis inside the grid of ((x / 2) / 2) / 2 (the dense path's grid-position
+// evaluation).  Returns the brick origin.
+__device__ void ab_corner_values(uint64_t slot, const uint32_t* nb, const double* __restrict__ f,
+                                 const uint32_t* __restrict__ bkey, const double* __restrict__ xc, const Prolong& W,
+                                 int res, double* node, double* cv, int* org) {
+  const int t = threadIdx.x;
+  uint32_t bx, by, bz;
+  unmorton3(bkey[slot], bx, by, bz);
+  org[0] = 8 * (int)bx;
+  org[1] = 8 * (int)by;
+  org[2] = 8 * (int)bz;
+  for (int i = t; i < kMT * kMT * kMT; i += kThreads) {
+    const int lz = i / (kMT * kMT) - 1, ly = (i / kMT) % kMT - 1, lx = i % kMT - 1;
+    const int gx = org[0] + lx, gy = org[1] + ly, gz = org[2] + lz;
+    double v = 0.0;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) {
+      const int ox = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0),
+                oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
+      const uint32_t s2 = nb[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
+      v = s2 != kSent ? f[(uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox))]
+                      : prolong_at(xc, W, gx, gy, gz);
+    }
+    node[i] = v;
+  }
+  __syncthreads();
+  for (int i = t; i < 9 * 9 * 9; i += kThreads) {
+    const int qz = i / 81, qy = (i / 9) % 9, qx = i % 9;
+    double v = 0.0;
+    for (int dz = -1; dz <= 0; ++dz) {
+      const int z = org[2] + qz + dz;
+      if (z < 0 || z >= res) continue;
+      for (int dy = -1; dy <= 0; ++dy) {
+        const int y = org[1] + qy + dy;
+        if (y < 0 || y >= res) continue;
+        for (int dx = -1; dx <= 0; ++dx) {
+          const int x = org[0] + qx + dx;
+          if (x < 0 || x >= res) continue;
+          const double nv = node[((qz + dz + 1) * kMT + qy + dy + 1) * kMT + qx + dx + 1];
+          v = xadd(v, xmul(xmul(xmul(nv, 0.5), 0.5), 0.5));
+        }
+      }
+    }
+    cv[i] = v;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t ab_cell_case(const double* cv, int o, double iso) {
+  const int z = o >> 6, y = (o >> 3) & 7, x = o & 7;
+  uint32_t mc = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const double v = cv[((z + c_abco[k][2]) * 9 + y + c_abco[k][1]) * 9 + x + c_abco[k][0]];
+    if (v < iso) mc |= 1u << k;
+  }
+  return mc;
+}
+
+__global__ void __launch_bounds__(kThreads) k_ab_mc_count(const double* __restrict__ f, const uint32_t* __restrict__ nbr,
+                                                          const uint32_t* __restrict__ bkey, uint64_t NB,
+                                                          const double* __restrict__ xc, Prolong W, int res, double iso,
+                                                          uint32_t* __restrict__ ntri, uint32_t* __restrict__ nedge) {
+  __shared__ double node[kMT * kMT * kMT], cv[729];
+  __shared__ uint32_t nb[27];
+  __shared__ int org[3];
+  typedef cub::BlockReduce<uint32_t, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const int t = threadIdx.x;
+  for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
+    if (t < 27) nb[t] = nbr[27 * slot + t];
+    __syncthreads();
+    ab_corner_values(slot, nb, f, bkey, xc, W, res, node, cv, org);
+    uint32_t a = 0, e = 0;
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t mc = ab_cell_case(cv, 2 * t + j, iso);
+      a += PR_MC_NTRI[mc];
+      e += __popc(ab_edge_mask(mc));
+    }
+    const uint32_t ta = BR(tmp).Sum(a);
+    __syncthreads();
+    const uint32_t te = BR(tmp).Sum(e);
+    if (t == 0) {
+      ntri[slot] = ta;
+      nedge[slot] = te;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_ab_mc_emit(const double* __restrict__ f, const uint32_t* __restrict__ nbr,
+                                                         const uint32_t* __restrict__ bkey, uint64_t NB,
+                                                         const double* __restrict__ xc, Prolong W, int res, double iso,
+                                                         const uint64_t* __restrict__ toff, const uint64_t* __restrict__ eoff,
+                                                         uint64_t* __restrict__ tri_key, uint64_t* __restrict__ edge_key,
+                                                         double* __restrict__ epos) {
+  __shared__ double node[kMT * kMT * kMT], cv[729];
+  __shared__ uint32_t nb[27];
+  __shared__ int org[3];
+  typedef cub::BlockScan<uint32_t, kThreads> BS;
+  __shared__ typename BS::TempStorage tmp;
+  const int t = threadIdx.x;
+  const double w = 1.0 / (double)res;
+  const uint64_t R1 = (uint64_t)res + 1;
+  for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
+    if (t < 27) nb[t] = nbr[27 * slot + t];
+    __syncthreads();
+    ab_corner_values(slot, nb, f, bkey, xc, W, res, node, cv, org);
+    uint32_t mc[2], ct = 0, ce = 0;
+    for (int j = 0; j < 2; ++j) {
+      mc[j] = ab_cell_case(cv, 2 * t + j, iso);
+      ct += PR_MC_NTRI[mc[j]];
+      ce += __popc(ab_edge_mask(mc[j]));
+    }
+    uint32_t pt, pe;
+    BS(tmp).ExclusiveSum(ct, pt);
+    __syncthreads();
+    BS(tmp).ExclusiveSum(ce, pe);
+    uint64_t to = toff[slot] + pt, eo = eoff[slot] + pe;
+    for (int j = 0; j < 2; ++j) {
+      const int o = 2 * t + j, cz = o >> 6, cy = (o >> 3) & 7, cx = o & 7;
+      const int cell[3] = {org[0] + cx, org[1] + cy, org[2] + cz};
+      double c8[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) c8[k] = cv[((cz + c_abco[k][2]) * 9 + cy + c_abco[k][1]) * 9 + cx + c_abco[k][0]];
+      uint64_t ekey[12];
+#pragma unroll
+      for (int e = 0; e < 12; ++e) {
+        const int ia = c_abev[e][0], ib = c_abev[e][1];
+        int st[3], axis = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          st[a] = cell[a] + min(c_abco[ia][a], c_abco[ib][a]);
+          if (c_abco[ia][a] != c_abco[ib][a]) axis = a;
+        }
+        ekey[e] = (((uint64_t)st[2] * R1 + (uint64_t)st[1]) * R1 + (uint64_t)st[0]) * 3 + (uint64_t)axis;
+      }
+      const uint32_t em = ab_edge_mask(mc[j]);
+      for (int e = 0; e < 12; ++e) {
+        if (!((em >> e) & 1u)) continue;
+        const int ia = c_abev[e][0], ib = c_abev[e][1];
+        const double dv = xsub(c8[ib], c8[ia]);
+        const double tt = fabs(dv) < 1e-15 ? 0.5 : xdiv(xsub(iso, c8[ia]), dv);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double base = xmul((double)(cell[a] + c_abco[ia][a]), w);
+          const double d = (double)(c_abco[ib][a] - c_abco[ia][a]);
+          epos[3 * eo + a] = xadd(base, xmul(xmul(tt, d), w));
+        }
+        edge_key[eo] = ekey[e];
+        ++eo;
+      }
+      const uint64_t packed = PR_MC_TRIS[mc[j]];
+      const uint32_t ntr = PR_MC_NTRI[mc[j]];
+      for (uint32_t i = 0; i < 3 * ntr; ++i) tri_key[3 * to + i] = ekey[(packed >> (4 * i)) & 15u];
+      to += ntr;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_ab_heads(const uint64_t* __restrict__ skey, uint64_t E, uint32_t* __restrict__ head) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x)
+    head[i] = (i == 0 || skey[i] != skey[i - 1]) ? 1u : 0u;
+}
+struct Mat16 {
+  double m[16];  // column-major, as the crate's Mat4
+};
+__global__ void k_ab_vertices(const uint64_t* __restrict__ skey, const uint32_t* __restrict__ sslot,
+                              const uint32_t* __restrict__ head, const uint32_t* __restrict__ vid, uint64_t E,
+                              const double* __restrict__ epos, Mat16 Mi, uint64_t* __restrict__ vkey,
+                              double* __restrict__ verts) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (!head[i]) continue;
+    const uint64_t v = vid[i], s = sslot[i];
+    const double p[3] = {epos[3 * s], epos[3 * s + 1], epos[3 * s + 2]};
+    // Mat4::transform_point (src/geometry.rs:256-262) with the inverse transform
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      verts[3 * v + r] = xadd(xadd(xadd(xmul(Mi.m[r], p[0]), xmul(Mi.m[4 + r], p[1])), xmul(Mi.m[8 + r], p[2])), Mi.m[12 + r]);
+    vkey[v] = skey[i];
+  }
+}
+__global__ void k_ab_tris(const uint64_t* __restrict__ tri_key, uint64_t n, const uint64_t* __restrict__ vkey, uint64_t NV,
+                          uint64_t* __restrict__ tris) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = tri_key[i];
+    uint64_t a = 0, b = NV;
+    while (a < b) {
+      const uint64_t m = (a + b) >> 1;
+      if (vkey[m] < k) a = m + 1;
+      else b = m;
+    }
+    tris[i] = a;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+Prolong make_prolong(int L, int resc) {
+  std::vector<double> cur(1, 1.0);
+  int lo = 0;
+  const double wk[4] = {0.25, 0.75, 0.75, 0.25};  // fine 2i + k <- coarse i, k = -1..2
+  for (int l = 0; l < L; ++l) {
+    std::vector<double> nxt(2 * cur.size() + 2, 0.0);
+    const int nlo = 2 * lo - 1;
+    for (size_t i = 0; i < cur.size(); ++i)
+      for (int k = -1; k <= 2; ++k) nxt[(size_t)(2 * (lo + (int)i) + k - nlo)] += cur[i] * wk[k + 1];
+    cur.swap(nxt);
+    lo = nlo;
+  }
+  PR_REQUIRE(cur.size() <= (size_t)kMaxW, PR_ERR_INTERNAL, "prolongation taps exceed the table");
+  Prolong W{};
+  for (size_t i = 0; i < cur.size(); ++i) W.w[i] = cur[i];
+  W.kmin = lo;
+  W.kmax = lo + (int)cur.size() - 1;
+  W.L = L;
+  W.resc = resc;
+  return W;
+}
+
+template <typename T>
+BandCoef<T> band_coef(uint32_t D, double pw) {
+  double m[5], s[5], g[5];
+  deg2_constants(m, s, g);
+  const double h = 1.0 / (double)(1u << D);
+  const double wh3 = pw > 0.0 ? pw * h * h * h / 1.5 : 0.0;
+  BandCoef<T> K;
+  for (int d = 0; d < 5; ++d) {
+    K.m[d] = (T)m[d];
+    K.s[d] = (T)s[d];
+  }
+  K.H = (T)h;
+  K.wg = (T)(wh3 * 0.005);
+  return K;
+}
+
+// the band system of the current adaptive state
+struct Band {
+  pr_context* c = nullptr;
+  uint64_t NB = 0, n = 0, S = 0, P = 0;
+  int res = 0;
+  double wh3 = 0.0;
+  const uint32_t *nbr = nullptr, *bkey = nullptr, *kin = nullptr, *snode = nullptr, *soff = nullptr, *sval = nullptr;
+  const double* xc = nullptr;
+  Prolong W{};
+  double bytes = 0.0;
+
+  void init(pr_context* ctx) {
+    c = ctx;
+    NB = c->band_nb;
+    n = NB * kBN;
+    P = c->P;
+    S = c->S;
+    res = 1 << c->D;
+    const double h = 1.0 / (double)res;
+    wh3 = c->pw > 0.0 ? c->pw * h * h * h / 1.5 : 0.0;
+    nbr = c->get<uint32_t>("ab_nbr");
+    bkey = c->get<uint32_t>("ab_bkey");
+    xc = c->get<double>("ab_xc");
+    W = make_prolong((int)(c->D - c->band_Dc), 1 << c->band_Dc);
+    if (S > 0) {
+      kin = c->get<uint32_t>("ab_kin");
+      snode = c->get<uint32_t>("abs_runkey");
+      soff = c->get<uint32_t>("abs_runoff");
+      sval = c->get<uint32_t>("abs_val");
+    }
+  }
+  template <typename T>
+  const T* phi() {
+    return sizeof(T) == 8 ? (const T*)c->get<double>("ab_phi64") : (const T*)c->get<float>("ab_phi32");
+  }
+  // y = A_BB x (MODE 0) or y = f - A_BB x (MODE 1), screening included
+  template <typename T, int MODE>
+  void op(const T* x, const T* f, T* y) {
+    k_ab_op<T, MODE><<<brick_grid(NB), kThreads, 0, c->stream>>>(x, f, y, nbr, bkey, NB, band_coef<T>(c->D, c->pw),
+                                                                 nullptr, W, res);
+    PR_CHECK_LAUNCH();
+    bytes += 2.0 * n * sizeof(T) + (MODE == 1 ? n * sizeof(T) : 0.0);
+    screen<T>(x, y, MODE == 0 ? 1.0 : -1.0);
+  }
+  template <typename T>
+  void screen(const T* x, T* y, double sign) {
+    if (S == 0 || !(wh3 > 0.0)) return;
+    T* proj = c->buf<T>(std::string("ab_proj_") + tname<T>(), P);
+    k_ab_screen_proj<T><<<grid_for(P, 1u << 20), kThreads, 0, c->stream>>>(kin, phi<T>(), P, x, proj);
+    PR_CHECK_LAUNCH();
+    k_ab_screen_gather<T><<<grid_for(S, 1u << 20), kThreads, 0, c->stream>>>(snode, soff, S, sval, phi<T>(), proj,
+                                                                              (T)(sign * wh3), y);
+    PR_CHECK_LAUNCH();
+    bytes += (double)P * 27 * (4 + 2 * sizeof(T)) + (double)S * (8 + 2 * sizeof(T));
+  }
+  template <typename T>
+  T* dinv() {
+    const std::string nm = std::string("ab_dinv_") + tname<T>();
+    auto it = c->bufs.find(nm);
+    if (it != c->bufs.end() && it->second.ptr) return reinterpret_cast<T*>(it->second.ptr);
+    T* d = c->buf<T>(nm, n);
+    const BandCoef<double> K = band_coef<double>(c->D, c->pw);
+    const double diag = (double)K.H * 3.0 * K.s[2] * K.m[2] * K.m[2] + (double)K.wg;
+    k_ab_dinv<T><<<grid_for(n), kThreads, 0, c->stream>>>(diag, n, d);
+    PR_CHECK_LAUNCH();
+    if (S > 0 && wh3 > 0.0) {
+      k_ab_dinv_screen<T><<<grid_for(S, 1u << 20), kThreads, 0, c->stream>>>(snode, c->get<double>("ab_sphi2"), S, diag,
+                                                                              wh3, d);
+      PR_CHECK_LAUNCH();
+    }
+    return d;
+  }
+};
+
+// Jacobi-preconditioned CG on A_BB x = r from x = 0 until ||r|| <= tol; r is overwritten with
+// the residual; returns the iterations
+template <typename T>
+int band_pcg(Band& B, T* r, T* x, double tol, int maxit, double rr) {
+  pr_context* c = B.c;
+  const uint64_t n = B.n;
+  cudaStream_t s = c->stream;
+  const std::string tn = tname<T>();
+  T* z = c->buf<T>("ab_z_" + tn, n);
+  T* d = c->buf<T>("ab_d_" + tn, n);
+  T* q = c->buf<T>("ab_q_" + tn, n);
+  const T* dv = B.dinv<T>();
+  PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
+  k_ab_mul<T><<<grid_for(n), kThreads, 0, s>>>(r, dv, n, z);
+  PR_CHECK_LAUNCH();
+  double rz = dot<T>(c, r, z, n);
+  PR_CUDA(cudaMemcpyAsync(d, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  B.bytes += 7.0 * n * sizeof(T);
+  int it = 0;
+  while (std::sqrt(rr) > tol && it < maxit) {
+    B.op<T, 0>(d, nullptr, q);
+    const double dq = dot<T>(c, d, q, n);
+    if (!(dq > 0.0)) break;
+    const double alpha = rz / dq;
+    rr = cg_update<T>(c, n, alpha, d, q, x, r);
+    ++it;
+    B.bytes += 8.0 * n * sizeof(T);
+    if (std::sqrt(rr) <= tol) break;
+    k_ab_mul<T><<<grid_for(n), kThreads, 0, s>>>(r, dv, n, z);
+    PR_CHECK_LAUNCH();
+    const double rz_new = dot<T>(c, r, z, n);
+    xpby<T>(s, n, z, rz_new / rz, d);
+    rz = rz_new;
+    B.bytes += 8.0 * n * sizeof(T);
+  }
+  return it;
+}
+
+void release_prefix(pr_context* c, const std::string& prefix) {
+  std::vector<std::string> names;
+  for (const auto& kv : c->bufs)
+    if (kv.first.compare(0, prefix.size(), prefix) == 0) names.push_back(kv.first);
+  for (const auto& nm : names) c->release(nm);
+}
+
+// stable sort of m (key, value) pairs by 32-bit key and run-length encoding into "abs_*"; the
+// run of kSent is dropped; returns the runs
+uint64_t band_sort_segment(pr_context* c, const uint32_t* keys_in, const uint32_t* vals_in, uint64_t m) {
+  uint32_t* keys = c->buf<uint32_t>("abs_key", m);
+  uint32_t* vals = c->buf<uint32_t>("abs_val", m);
+  uint32_t* run_key = c->buf<uint32_t>("abs_runkey", m);
+  uint32_t* run_cnt = c->buf<uint32_t>("abs_runcnt", m + 1);
+  uint32_t* run_off = c->buf<uint32_t>("abs_runoff", m + 1);
+  uint32_t* nrun = c->buf<uint32_t>("ab_nrun", 2);
+  size_t b1 = 0, b2 = 0, b3 = 0;
+  PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, keys_in, keys, vals_in, vals, (int64_t)m, 0, 32, c->stream));
+  PR_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, b2, keys, run_key, run_cnt, nrun, (int64_t)m, c->stream));
+  PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b3, run_cnt, run_off, (int64_t)(m + 1), c->stream));
+  size_t tb = std::max(b1, std::max(b2, b3));
+  void* tmp = c->buf<char>("ab_cub_tmp", tb);
+  PR_COUNT_PRIMITIVE();
+  PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys_in, keys, vals_in, vals, (int64_t)m, 0, 32, c->stream));
+  PR_COUNT_PRIMITIVE();
+  PR_CUDA(cub::DeviceRunLengthEncode::Encode(tmp, tb, keys, run_key, run_cnt, nrun, (int64_t)m, c->stream));
+  uint32_t h_nrun = 0, h_last = 0;
+  PR_CUDA(cudaMemcpyAsync(&h_nrun, nrun, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  c->sync();
+  if (h_nrun > 0) {
+    PR_CUDA(cudaMemcpyAsync(&h_last, run_key + (h_nrun - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+  }
+  uint64_t R = h_nrun;
+  if (R > 0 && h_last == kSent) --R;
+  PR_CUDA(cudaMemsetAsync(run_cnt + R, 0, sizeof(uint32_t), c->stream));
+  PR_COUNT_PRIMITIVE();
+  PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, run_cnt, run_off, (int64_t)(R + 1), c->stream));
+  return R;
+}
+
+// active bricks: sorted unique Morton codes in "ab_bkey"; returns their number
+uint64_t find_bricks(pr_context* c, uint32_t D, bool full) {
+  cudaStream_t s = c->stream;
+  const uint32_t nres = 1u << (D - 3);
+  const uint64_t nall = (uint64_t)nres * nres * nres;
+  if (full) {
+    uint32_t* bkey = c->buf<uint32_t>("ab_bkey", nall);
+    k_ab_iota<<<grid_for(nall), kThreads, 0, s>>>(bkey, nall);
+    PR_CHECK_LAUNCH();
+    return nall;
+  }
+  const uint64_t m = 8 * c->P;
+  uint32_t* kin = c->buf<uint32_t>("ab_bk_in", m);
+  uint32_t* kso = c->buf<uint32_t>("ab_bk_sorted", m);
+  uint32_t* kun = c->buf<uint32_t>("ab_bk_unique", m);
+  uint32_t* nsel = c->buf<uint32_t>("ab_nsel", 2);
+  k_ab_brick_keys<<<grid_for(c->P, 1u << 20), kThreads, 0, s>>>(c->get<double>("upos"), c->P, D, kin);
+  PR_CHECK_LAUNCH();
+  size_t b1 = 0, b2 = 0;
+  PR_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, b1, kin, kso, (int64_t)m, 0, 32, s));
+  PR_CUDA(cub::DeviceSelect::Unique(nullptr, b2, kso, kun, nsel, (int64_t)m, s));
+  void* tmp = c->buf<char>("ab_cub_tmp", std::max(b1, b2));
+  PR_COUNT_PRIMITIVE();
+  PR_CUDA(cub::DeviceRadixSort::SortKeys(tmp, b1, kin, kso, (int64_t)m, 0, 32, s));
+  PR_COUNT_PRIMITIVE();
+  PR_CUDA(cub::DeviceSelect::Unique(tmp, b2, kso, kun, nsel, (int64_t)m, s));
+  uint32_t h_n = 0, h_last = 0;
+  PR_CUDA(cudaMemcpyAsync(&h_n, nsel, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  c->sync();
+  if (h_n > 0) {
+    PR_CUDA(cudaMemcpyAsync(&h_last, kun + (h_n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    c->sync();
+  }
+  uint64_t NB = h_n;
+  if (NB > 0 && h_last == kSent) --NB;
+  PR_REQUIRE(NB < (1ull << 32) / kBN, PR_ERR_INVALID_ARGUMENT,
+             "adaptive reconstruction: more than 8,388,607 active bricks (" + std::to_string(NB) + ")");
+  uint32_t* bkey = c->buf<uint32_t>("ab_bkey", std::max<uint64_t>(NB, 1));
+  if (NB) PR_CUDA(cudaMemcpyAsync(bkey, kun, NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  c->release("ab_bk_in");
+  c->release("ab_bk_sorted");
+  c->release("ab_bk_unique");
+  return NB;
+}
+
+void band_setup(pr_context* c, uint32_t D, uint32_t Dc, double pw, bool full) {
+  cudaStream_t s = c->stream;
+  const uint64_t P = c->P;
+  const uint64_t m = 27 * P;
+  PR_REQUIRE(m < (1ull << 31), PR_ERR_INVALID_ARGUMENT, "degree 2 takes at most 79,536,431 points per call");
+  const uint64_t NB = find_bricks(c, D, full);
+  c->D = D;
+  c->band_Dc = Dc;
+  c->band_nb = NB;
+  c->n = NB * kBN;
+  c->pw = pw;
+  c->adaptive = true;
+  const uint32_t nres = 1u << (D - 3);
+  const uint64_t nall = (uint64_t)nres * nres * nres;
+  uint32_t* bmap = c->buf<uint32_t>("ab_bmap", nall);
+  PR_CUDA(cudaMemsetAsync(bmap, 0xff, nall * sizeof(uint32_t), s));
+  const uint32_t* bkey = c->get<uint32_t>("ab_bkey");
+  if (NB) {
+    k_ab_brick_map<<<grid_for(NB), kThreads, 0, s>>>(bkey, NB, bmap);
+    PR_CHECK_LAUNCH();
+  }
+  uint32_t* nbr = c->buf<uint32_t>("ab_nbr", 27 * std::max<uint64_t>(NB, 1));
+  if (NB) {
+    k_ab_neighbours<<<grid_for(27 * NB, 1u << 20), kThreads, 0, s>>>(bkey, NB, nres, bmap, nbr);
+    PR_CHECK_LAUNCH();
+  }
+  // (band node, point) pairs, splat, right-hand side
+  uint32_t* kin = c->buf<uint32_t>("ab_kin", m);
+  uint32_t* vin = c->buf<uint32_t>("ab_vin", m);
+  double* phi64 = c->buf<double>("ab_phi64", m);
+  float* phi32 = c->buf<float>("ab_phi32", m);
+  unsigned long long* nin = c->buf<unsigned long long>("ab_nin", 1);
+  PR_CUDA(cudaMemsetAsync(nin, 0, sizeof(unsigned long long), s));
+  k_ab_pair_keys<<<grid_for(m, 1u << 20), kThreads, 0, s>>>(c->get<double>("upos"), P, D, bmap, kin, vin, phi64, phi32,
+                                                            nin);
+  PR_CHECK_LAUNCH();
+  const uint64_t T = band_sort_segment(c, kin, vin, m);
+  unsigned long long h_nin = 0;
+  PR_CUDA(cudaMemcpyAsync(&h_nin, nin, sizeof(h_nin), cudaMemcpyDeviceToHost, s));
+  c->sync();
+  c->release("ab_vin");
+  c->release("abs_key");
+  c->release("abs_runcnt");
+  c->release("ab_bmap");
+  c->T = T;
+  c->P_in = h_nin;
+  double* nfc = c->buf<double>("ab_nfc", 3 * std::max<uint64_t>(T, 1));
+  double* sphi = c->buf<double>("ab_sphi", std::max<uint64_t>(T, 1));
+  double* sphi2 = c->buf<double>("ab_sphi2", std::max<uint64_t>(T, 1));
+  const uint32_t* run_key = c->get<uint32_t>("abs_runkey");
+  if (T) {
+    k_ab_splat<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("abs_runoff"), T, c->get<uint32_t>("abs_val"),
+                                                          phi64, c->get<double>("unrm"), P, nfc, sphi, sphi2);
+    PR_CHECK_LAUNCH();
+  }
+  uint32_t* brun = c->buf<uint32_t>("ab_brun", NB + 1);
+  k_ab_brick_runs<<<grid_for(NB + 1), kThreads, 0, s>>>(run_key, T, NB, brun);
+  PR_CHECK_LAUNCH();
+  const double h = 1.0 / (double)(1u << D);
+  const double wh3 = pw > 0.0 ? pw * h * h * h / 1.5 : 0.0;
+  double m5[5], s5[5], g5[5];
+  deg2_constants(m5, s5, g5);
+  BandCoef<double> K = band_coef<double>(D, pw);
+  double* b = c->buf<double>("ab_b", std::max<uint64_t>(c->n, 1));
+  const size_t smem = (3 * kOT3 + 8 * kOT * kOT + 8 * 8 * kOT + kBN) * sizeof(double);
+  allow_smem(k_ab_rhs, smem);
+  if (NB) {
+    k_ab_rhs<<<brick_grid(NB), kThreads, smem, s>>>(nbr, run_key, brun, nfc, sphi, pw > 0.0 ? 0.5 * wh3 : 0.0, K, g5[0],
+                                                    g5[1], g5[3], g5[4], h * h, NB, b);
+    PR_CHECK_LAUNCH();
+  }
+  c->release("ab_nfc");
+  c->release("ab_sphi");
+  c->S = pw > 0.0 ? T : 0;
+  c->S_pairs = 0;
+  c->have_state = true;
+}
+
+}  // namespace
+
+void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extract) {
+  const uint32_t D = p.depth, Dc = p.coarse_depth;
+  const double pw = p.point_weight;
+  cudaStream_t s = c->stream;
+  double t0 = now_seconds();
+  release_prefix(c, "ab_");  // buffers of an earlier adaptive state (the Jacobi scales are cached)
+  // 1. the dense coarse level
+  pr_params pc = p;
+  pc.depth = Dc;
+  pc.coarse_depth = 0;
+  c->adaptive = false;
+  stage_setup_deg2(c, Dc, pw);
+  c->sync();
+  const double tc = now_seconds();
+  pr_stats sc;
+  std::memset(&sc, 0, sizeof(sc));
+  stage_solve_deg2(c, pc, sc);
+  const uint64_t nc = 1ull << (3 * Dc);
+  double* xc = c->buf<double>("ab_xc", nc);
+  PR_CUDA(cudaMemcpyAsync(xc, c->d2_xnat, nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  c->sync();
+  c->d2_xnat = nullptr;
+  release_prefix(c, "d2");
+  release_prefix(c, "cub_tmp");
+  double t1 = now_seconds();
+  // 2. the band
+  band_setup(c, D, Dc, pw, (p.band_flags & PR_BAND_FULL) != 0);
+  c->sync();
+  double t2 = now_seconds();
+  st.time_tree = (tc - t0) + (t2 - t1);
+  // 3. solve A_BB e = r0 = b - (A g)_B, f = g_B + e
+  Band B;
+  B.init(c);
+  const uint64_t n = B.n;
+  const double* b = c->get<double>("ab_b");
+  double* gB = c->buf<double>("ab_g", std::max<uint64_t>(n, 1));
+  double* r0 = c->buf<double>("ab_r0", std::max<uint64_t>(n, 1));
+  double* e64 = c->buf<double>("ab_e64", std::max<uint64_t>(n, 1));
+  double* r64 = c->buf<double>("ab_r64", std::max<uint64_t>(n, 1));
+  const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;
+  // the band solve is Jacobi-preconditioned: it gets 10 x max_iters iterations of its own
+  const int max_iters = 10 * (p.max_iters > 0 ? (int)p.max_iters : 200);
+  const bool mixed = p.precision != PR_PRECISION_FP64;
+  int used = 0;
+  double bn = 0.0, rn = 0.0;
+  st.pcg_iterations = sc.pcg_iterations;
+  st.refinement_steps = 0;
+  if (n > 0) {
+    k_ab_prolong_band<<<grid_for(n, 1u << 20), kThreads, 0, s>>>(B.bkey, B.NB, B.xc, B.W, gB);
+    PR_CHECK_LAUNCH();
+    k_ab_op<double, 1><<<brick_grid(B.NB), kThreads, 0, s>>>(nullptr, b, r0, B.nbr, B.bkey, B.NB,
+                                                             band_coef<double>(D, pw), B.xc, B.W, B.res);
+    PR_CHECK_LAUNCH();
+    B.screen<double>(gB, r0, -1.0);
+    bn = std::sqrt(dot<double>(c, b, b, n));
+    PR_CUDA(cudaMemcpyAsync(r64, r0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    PR_CUDA(cudaMemsetAsync(e64, 0, n * sizeof(double), s));
+    rn = std::sqrt(dot<double>(c, r64, r64, n));
+    if (mixed) {
+      float* r32 = c->buf<float>("ab_r32", n);
+      float* e32 = c->buf<float>("ab_e32", n);
+      const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
+      while (rn > target * bn && used < max_iters) {
+        convert_norm(c, r64, r32, n);
+        const double tol = std::max(inner, 0.5 * target * bn / rn) * rn;
+        const int it = band_pcg<float>(B, r32, e32, tol, max_iters - used, rn * rn);
+        used += it;
+        axpy<float, double>(s, n, 1.0, e32, e64);
+        B.op<double, 1>(e64, r0, r64);
+        const double rn_new = std::sqrt(dot<double>(c, r64, r64, n));
+        st.refinement_steps++;
+        const bool stalled = it == 0 || !(rn_new < rn);
+        rn = rn_new;
+        if (stalled) break;
+      }
+    } else if (rn > target * bn) {
+      used = band_pcg<double>(B, r64, e64, 0.5 * target * bn, max_iters, rn * rn);
+      B.op<double, 1>(e64, r0, r64);
+      rn = std::sqrt(dot<double>(c, r64, r64, n));
+    }
+    double* f = c->buf<double>("ab_f", n);
+    PR_CUDA(cudaMemcpyAsync(f, gB, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    axpy<double, double>(s, n, 1.0, e64, f);
+  }
+  c->release("ab_r0");
+  c->release("ab_e64");
+  c->release("ab_r64");
+  c->release("ab_r32");
+  c->release("ab_e32");
+  release_prefix(c, "ab_z_");
+  release_prefix(c, "ab_d_");
+  release_prefix(c, "ab_q_");
+  c->sync();
+  double t3 = now_seconds();
+  st.time_solve = (t1 - tc) + (t3 - t2);
+  st.rel_residual = bn > 0.0 ? rn / bn : 0.0;
+  st.converged = st.rel_residual <= target ? 1 : 0;
+  st.pcg_iterations += (uint32_t)used;
+  st.solve_bytes = B.bytes + sc.solve_bytes;
+  st.fem_nodes = n;
+  st.points_in_cube = c->P_in;
+  c->have_coeffs = true;
+  c->coeffs_converged = true;
+  if (!extract) return;
+  // 4. iso value and marching cubes over the active bricks
+  const uint64_t P = c->P;
+  const double* f = c->get<double>("ab_f");
+  double iso = 0.0;
+  {
+    int nb = (int)std::min<uint64_t>(kDotBlocks, (P + kThreads - 1) / kThreads);
+    if (nb < 1) nb = 1;
+    double* part = c->buf<double>("iso_part", 2 * (size_t)nb);
+    double* out = c->buf<double>("iso_out", 1);
+    k_ab_iso_partial<<<nb, kThreads, 0, s>>>(f, c->get<uint32_t>("ab_kin"), c->get<double>("ab_phi64"), P, part);
+    PR_CHECK_LAUNCH();
+    k_ab_iso_final<<<1, 32, 0, s>>>(part, nb, out);
+    PR_CHECK_LAUNCH();
+    PR_CUDA(cudaMemcpyAsync(&iso, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    iso /= (double)P;
+  }
+  const uint64_t NB = B.NB;
+  c->nv = c->nt = 0;
+  if (NB > 0) {
+    uint32_t* bt = c->buf<uint32_t>("ab_mc_nt", NB + 1);
+    uint32_t* be = c->buf<uint32_t>("ab_mc_ne", NB + 1);
+    uint64_t* toff = c->buf<uint64_t>("ab_mc_toff", NB + 1);
+    uint64_t* eoff = c->buf<uint64_t>("ab_mc_eoff", NB + 1);
+    k_ab_mc_count<<<brick_grid(NB), kThreads, 0, s>>>(f, B.nbr, B.bkey, NB, B.xc, B.W, B.res, iso, bt, be);
+    PR_CHECK_LAUNCH();
+    PR_CUDA(cudaMemsetAsync(bt + NB, 0, sizeof(uint32_t), s));
+    PR_CUDA(cudaMemsetAsync(be + NB, 0, sizeof(uint32_t), s));
+    size_t b1 = 0;
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b1, bt, toff, (int64_t)(NB + 1), s));
+    void* tmp = c->buf<char>("ab_cub_tmp", b1);
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, b1, bt, toff, (int64_t)(NB + 1), s));
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, b1, be, eoff, (int64_t)(NB + 1), s));
+    uint64_t NT = 0, E = 0;
+    PR_CUDA(cudaMemcpyAsync(&NT, toff + NB, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaMemcpyAsync(&E, eoff + NB, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    if (NT > 0 && E > 0) {
+      PR_REQUIRE(E < (1ull << 32), PR_ERR_INVALID_ARGUMENT, "adaptive marching cubes: more than 2^32 cut edges");
+      uint64_t* tri_key = c->buf<uint64_t>("ab_mc_tkey", 3 * NT);
+      uint64_t* ekey = c->buf<uint64_t>("ab_mc_ekey", E);
+      double* epos = c->buf<double>("ab_mc_epos", 3 * E);
+      k_ab_mc_emit<<<brick_grid(NB), kThreads, 0, s>>>(f, B.nbr, B.bkey, NB, B.xc, B.W, B.res, iso, toff, eoff, tri_key,
+                                                       ekey, epos);
+      PR_CHECK_LAUNCH();
+      uint32_t* eslot = c->buf<uint32_t>("ab_mc_eslot", E);
+      k_ab_iota<<<grid_for(E, 1u << 20), kThreads, 0, s>>>(eslot, E);
+      PR_CHECK_LAUNCH();
+      uint64_t* skey = c->buf<uint64_t>("ab_mc_skey", E);
+      uint32_t* sslot = c->buf<uint32_t>("ab_mc_sslot", E);
+      uint32_t* head = c->buf<uint32_t>("ab_mc_head", E);
+      uint32_t* vid = c->buf<uint32_t>("ab_mc_vid", E);
+      size_t b2 = 0, b3 = 0;
+      PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b2, ekey, skey, eslot, sslot, (int64_t)E, 0, 64, s));
+      PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b3, head, vid, (int64_t)E, s));
+      tmp = c->buf<char>("ab_cub_tmp", std::max(b2, b3));
+      PR_COUNT_PRIMITIVE();
+      PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b2, ekey, skey, eslot, sslot, (int64_t)E, 0, 64, s));
+      k_ab_heads<<<grid_for(E, 1u << 20), kThreads, 0, s>>>(skey, E, head);
+      PR_CHECK_LAUNCH();
+      PR_COUNT_PRIMITIVE();
+      PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, b3, head, vid, (int64_t)E, s));
+      uint32_t h_vid = 0, h_head = 0;
+      PR_CUDA(cudaMemcpyAsync(&h_vid, vid + (E - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      PR_CUDA(cudaMemcpyAsync(&h_head, head + (E - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      c->sync();
+      const uint64_t NV = (uint64_t)h_vid + h_head;
+      uint64_t* vkey = c->buf<uint64_t>("ab_mc_vkey", NV);
+      double* verts = c->buf<double>("mesh_v", 3 * NV);
+      uint64_t* tris = c->buf<uint64_t>("mesh_t", 3 * NT);
+      Mat16 Mi;
+      for (int k = 0; k < 16; ++k) Mi.m[k] = c->Minv[k];
+      k_ab_vertices<<<grid_for(E, 1u << 20), kThreads, 0, s>>>(skey, sslot, head, vid, E, epos, Mi, vkey, verts);
+      PR_CHECK_LAUNCH();
+      k_ab_tris<<<grid_for(3 * NT, 1u << 20), kThreads, 0, s>>>(tri_key, 3 * NT, vkey, NV, tris);
+      PR_CHECK_LAUNCH();
+      c->sync();
+      c->nv = NV;
+      c->nt = NT;
+      release_prefix(c, "ab_mc_");
+    }
+  }
+  c->have_mesh = true;
+  c->sync();
+  double t4 = now_seconds();
+  st.time_extract = t4 - t3;
+  st.iso_value = iso;
+  st.mesh_vertices = c->nv;
+  st.mesh_triangles = c->nt;
+  st.peak_device_bytes = (double)c->peak_bytes;
+}
+
+void band_vector(pr_context* c, int which, double* d_out) {
+  PR_REQUIRE(c->adaptive, PR_ERR_STATE, "no adaptive reconstruction state");
+  const char* nm = which == 0 ? "ab_b" : (which == 1 ? "ab_f" : "ab_g");
+  PR_REQUIRE(which >= 0 && which <= 2, PR_ERR_INVALID_ARGUMENT, "band vector: which must be 0, 1 or 2");
+  PR_REQUIRE(which != 1 || c->have_coeffs, PR_ERR_STATE, "no solved band coefficients");
+  if (c->n) PR_CUDA(cudaMemcpyAsync(d_out, c->get<double>(nm), c->n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+void band_apply64(pr_context* c, const double* d_x, double* d_y) {
+  PR_REQUIRE(c->adaptive, PR_ERR_STATE, "no adaptive reconstruction state");
+  Band B;
+  B.init(c);
+  if (B.n) B.op<double, 0>(d_x, nullptr, d_y);
+}
+
+}  // namespace pr

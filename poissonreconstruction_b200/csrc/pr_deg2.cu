@@ -2711,6 +2711,14 @@ double deg2_kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int 
   return precision == PR_PRECISION_FP64 ? bench2<double>(c, kid, D, reps, bytes) : bench2<float>(c, kid, D, reps, bytes);
 }
 
+void deg2_constants(double* m5, double* s5, double* g5) {
+  for (int d = 0; d < 5; ++d) {
+    m5[d] = consts().m[d];
+    s5[d] = consts().s[d];
+    g5[d] = consts().g[d];
+  }
+}
+
 // accessors in Morton order (the order of the degree-1 vectors and of the oracle)
 void deg2_rhs_morton(pr_context* c, double* d_out) {
   nat_to_morton<double>(c->stream, c->get<double>("d2_b"), c->D, d_out);

@@ -51,6 +51,7 @@ extern "C" void pr_count_launch_(int primitive);
 // ------------------------------------------------------------------ limits
 constexpr uint32_t kMinDepth = 1;
 constexpr uint32_t kMaxDepth = 10;              // dense grid: 2^30 nodes, 32-bit node index
+constexpr uint32_t kMaxBandDepth = 12;          // adaptive band: brick codes of 3 x 9 bits
 constexpr uint64_t kMaxPoints = 1ull << 28;     // 8 x points must fit a 31-bit pair index
 constexpr uint32_t kCoarsestDepth = 3;          // multigrid direct-solve level (512 nodes)
 constexpr int kDotBlocks = 1184;                // 8 x 148 SMs: fixed => deterministic dots
@@ -144,6 +145,11 @@ struct pr_context {
   // belongs to the current state
   bool have_ref_coarse = false;
   uint32_t ref_coarse_D = 0;
+  // adaptive state: D = the band depth, band_Dc the coarse depth, band_nb active bricks (their
+  // Morton brick codes in "ab_bkey"); band vectors hold 512 band_nb values
+  bool adaptive = false;
+  uint32_t band_Dc = 0;
+  uint64_t band_nb = 0;
   int degree = 1;                 // node functions of the current state: 1 (the crate's) or 2
   // degree 2: the dense normal field "d2_nf" at address nf_clean (depth nf_clean_D) is zero except
   // at the nf_dirty_T nodes of the last splat (its run keys "d2s_runkey"); nullptr: unknown
@@ -237,6 +243,16 @@ void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w);
 template <typename T>
 void deg2_apply_morton(pr_context* c, const T* d_x, T* d_y);
 double deg2_kernel_bench(pr_context* c, int kid, uint32_t depth, int precision, int reps, double* bytes);
+// the 1-D integrals of N2 N2, N2' N2', N2' N2 at offsets -2..2
+void deg2_constants(double* m5, double* s5, double* g5);
+// adaptive (narrow-band) reconstruction (pr_adaptive.cu): a dense degree-2 coarse level at
+// p.coarse_depth and the depth-p.depth system on the 8^3-node bricks around the points
+void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extract);
+// band accessors: which 0 = right-hand side, 1 = solved coefficients, 2 = the prolonged coarse
+// function on the band (brick-major, natural order inside a brick); n = 512 band_nb doubles
+void band_vector(pr_context* c, int which, double* d_out);
+// y = A_BB x on the band (FP64, device vectors of 512 band_nb doubles)
+void band_apply64(pr_context* c, const double* d_x, double* d_y);
 // the solved coefficients in Morton order ("x64"), permuted from the degree-2 solver's order first
 // when needed
 const double* coeffs_morton(pr_context* c);

@@ -66,6 +66,10 @@ def test_empty_input_returns_empty_mesh(L):
     (dict(depth=0), "depth"), (dict(depth=11), "depth"), (dict(scale=0.0), "scale"),
     (dict(point_weight=-1.0), "point_weight"), (dict(solve_mode=7), "solve_mode"),
     (dict(precision=3), "precision"), (dict(target_rel_residual=float("nan")), "target_rel_residual"),
+    # adaptive reconstruction: degree 2 only, depth <= 12, at most 4 levels above the coarse one
+    (dict(depth=6, coarse_depth=3), "degree 2"), (dict(depth=13, coarse_depth=10, degree=2), "depth"),
+    (dict(depth=12, coarse_depth=7, degree=2), "coarse_depth"),
+    (dict(depth=8, coarse_depth=5, degree=2, solve_mode=1), "PR_SOLVE_CONVERGED"),
 ])
 def test_invalid_params_rejected(L, kw, msg):
     pts = np.zeros((4, 6))
