@@ -88,26 +88,68 @@ __device__ __forceinline__ void axis2b(double u, double h, int64_t& c, double* b
 
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
-// the coarse function's depth-D coefficient at fine node (fx, fy, fz) (x_c natural order)
-__device__ double prolong_at(const double* __restrict__ xc, const Prolong& W, int fx, int fy, int fz) {
+// The coarse function's depth-D coefficients on a TT^3 tile of fine nodes starting at (ox, oy, oz)
+// (zero outside the grid), by the whole CTA: the coarse coefficients that reach the tile (at most
+// 9 per axis), then the separable sums over x, y and z, every one in increasing coarse index, so
+// a node gets the same bits in any tile.  scratch: 729 + 81 TT + 9 TT^2 doubles.
+__host__ __device__ constexpr int kProlongScratch(int tt) { return 729 + 81 * tt + 9 * tt * tt; }
+template <int TT>
+__device__ void prolong_tile(const double* __restrict__ xc, const Prolong& W, int res, int ox, int oy, int oz,
+                             double* scratch, double* out) {
   const int step = 1 << W.L;
-  int i0[3], i1[3];
-  const int f[3] = {fx, fy, fz};
+  const int o[3] = {ox, oy, oz};
+  int lo[3], cnt[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    i0[a] = max(0, -floor_div(W.kmax - f[a], step));  // ceil((f - kmax) / step)
-    i1[a] = min(W.resc - 1, floor_div(f[a] - W.kmin, step));
+    lo[a] = max(0, -floor_div(W.kmax - o[a], step));  // ceil((o - kmax) / step)
+    const int hi = min(W.resc - 1, floor_div(o[a] + TT - 1 - W.kmin, step));
+    cnt[a] = max(0, hi - lo[a] + 1);
   }
-  double v = 0.0;
-  for (int iz = i0[2]; iz <= i1[2]; ++iz) {
-    const double wz = W.w[fz - step * iz - W.kmin];
-    for (int iy = i0[1]; iy <= i1[1]; ++iy) {
-      const double wy = wz * W.w[fy - step * iy - W.kmin];
-      const double* row = xc + (int64_t)W.resc * (iy + (int64_t)W.resc * iz);
-      for (int ix = i0[0]; ix <= i1[0]; ++ix) v += wy * W.w[fx - step * ix - W.kmin] * row[ix];
-    }
+  double* c = scratch;        // [cz][cy][cx]
+  double* ax = c + 729;       // [cz][cy][TT]
+  double* ay = ax + 81 * TT;  // [cz][TT][TT]
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int i = t; i < cnt[0] * cnt[1] * cnt[2]; i += nt) {
+    const int ix = i % cnt[0], iy = (i / cnt[0]) % cnt[1], iz = i / (cnt[0] * cnt[1]);
+    c[i] = xc[(int64_t)(lo[0] + ix) + (int64_t)W.resc * ((lo[1] + iy) + (int64_t)W.resc * (lo[2] + iz))];
   }
-  return v;
+  __syncthreads();
+  for (int i = t; i < cnt[2] * cnt[1] * TT; i += nt) {
+    const int tx = i % TT, r = i / TT;  // r = iz cnt1 + iy
+    const int f = ox + tx;
+    double v = 0.0;
+    if (f >= 0 && f < res)
+      for (int ix = 0; ix < cnt[0]; ++ix) {
+        const int k = f - step * (lo[0] + ix) - W.kmin;
+        if (k >= 0 && k <= W.kmax - W.kmin) v += W.w[k] * c[r * cnt[0] + ix];
+      }
+    ax[i] = v;
+  }
+  __syncthreads();
+  for (int i = t; i < cnt[2] * TT * TT; i += nt) {
+    const int tx = i % TT, ty = (i / TT) % TT, iz = i / (TT * TT);
+    const int f = oy + ty;
+    double v = 0.0;
+    if (f >= 0 && f < res)
+      for (int iy = 0; iy < cnt[1]; ++iy) {
+        const int k = f - step * (lo[1] + iy) - W.kmin;
+        if (k >= 0 && k <= W.kmax - W.kmin) v += W.w[k] * ax[(iz * cnt[1] + iy) * TT + tx];
+      }
+    ay[i] = v;
+  }
+  __syncthreads();
+  for (int i = t; i < TT * TT * TT; i += nt) {
+    const int yx = i % (TT * TT), tz = i / (TT * TT);
+    const int f = oz + tz;
+    double v = 0.0;
+    if (f >= 0 && f < res)
+      for (int iz = 0; iz < cnt[2]; ++iz) {
+        const int k = f - step * (lo[2] + iz) - W.kmin;
+        if (k >= 0 && k <= W.kmax - W.kmin) v += W.w[k] * ay[iz * TT * TT + yx];
+      }
+    out[i] = v;
+  }
+  __syncthreads();
 }
 
 // ------------------------------------------------------------------ bricks
@@ -325,85 +367,157 @@ __global__ void __launch_bounds__(kThreads) k_ab_rhs(const uint32_t* __restrict_
 }
 
 // ------------------------------------------------------------------ the band operator
-// MODE 0: y = A_BB x;  MODE 1: y = f - A_BB x.  Stiffness and shift only (the screening term is a
-// separate pass).  With xc != nullptr the tile is the prolonged coarse function g everywhere
-// (x unused): y = (K + wg I) g on the band.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kThreads) k_ab_op(const T* __restrict__ x, const T* __restrict__ f, T* __restrict__ y,
-                                                    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ bkey,
-                                                    uint64_t NB, BandCoef<T> K, const double* __restrict__ xc, Prolong W,
-                                                    int res) {
-  __shared__ T tile[kOT3];
-  __shared__ T um[8 * kOT * kOT], us[8 * kOT * kOT];
-  __shared__ T w1[8 * 8 * kOT], w23[8 * 8 * kOT];
+// One brick per CTA iteration, kOpThreads threads.  The brick and its 2-node halo (a 12^3 tile,
+// gathered from the 27 neighbouring bricks, zero outside the band) go to shared memory; the
+// stencil h (S M M + M S M + M M S) + wg then runs as three register passes: a thread per (x, y)
+// column filters z (M and S), a thread per (x, z) column filters y, a thread per (y, z) row filters
+// x and writes its 8 outputs as two 16-byte stores.
+//   kBandApply: y = A x          kBandResid: y = f - A x
+//   kBandDir:   the CG direction step: d = z + beta dold (dold = x, z = f; x unread when beta = 0)
+//               formed while gathering, written to dout (a buffer other than x: neighbouring CTAs
+//               still gather dold) for the brick, and y = A d with per-CTA partials of d . y
+// GSRC (kBandResid, FP64): the tile is the prolonged coarse function on every node (x unused):
+// y = f - (K + wg I) g on the band.
+constexpr int kOpThreads = 160;
+constexpr int kWS = 13;  // row stride of the y-filtered planes (conflict-free x pass)
+enum { kBandApply = 0, kBandResid = 1, kBandDir = 2 };
+
+template <typename T>
+constexpr size_t band_op_smem(bool gsrc) {
+  return (size_t)(kOT3 + 2 * 8 * kOT * kOT + 2 * 8 * 8 * kWS) * sizeof(T) +
+         (gsrc ? (size_t)(kProlongScratch(kOT) + kOT3) * sizeof(double) : 0);
+}
+
+template <typename T, int MODE, bool GSRC>
+__global__ void __launch_bounds__(kOpThreads) k_ab_op(const T* __restrict__ x, const T* __restrict__ f,
+                                                      T* __restrict__ y, T* __restrict__ dout, double beta,
+                                                      const uint32_t* __restrict__ nbr,
+                                                      const uint32_t* __restrict__ bkey, uint64_t NB, BandCoef<T> K,
+                                                      const double* __restrict__ xc, Prolong W, int res,
+                                                      double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);   // [z][y][x], 12^3
+  T* um = tile + kOT3;                         // [z 8][y 12][x 12]
+  T* us = um + 8 * kOT * kOT;
+  T* w1 = us + 8 * kOT * kOT;                  // [z 8][y 8][x kWS]
+  T* w23 = w1 + 8 * 8 * kWS;
+  double* gs = reinterpret_cast<double*>(w23 + 8 * 8 * kWS);  // GSRC: prolongation scratch, then the tile
   __shared__ uint32_t nb[27];
+  __shared__ double red[kOpThreads / 32 + 1];
   const int t = threadIdx.x;
+  const T tb = (T)beta;
+  double dacc = 0.0;
   for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
     if (t < 27) nb[t] = nbr[27 * slot + t];
-    uint32_t bx = 0, by = 0, bz = 0;
-    if (xc) unmorton3(bkey[slot], bx, by, bz);
     __syncthreads();
-    for (int i = t; i < kOT3; i += kThreads) {
-      const int lz = i / (kOT * kOT) - 2, ly = (i / kOT) % kOT - 2, lx = i % kOT - 2;
-      T v = T(0);
-      if (xc) {
-        const int gx = 8 * (int)bx + lx, gy = 8 * (int)by + ly, gz = 8 * (int)bz + lz;
-        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) v = (T)prolong_at(xc, W, gx, gy, gz);
-      } else {
+    if (GSRC) {
+      uint32_t bx, by, bz;
+      unmorton3(bkey[slot], bx, by, bz);
+      double* gt = gs + kProlongScratch(kOT);
+      prolong_tile<kOT>(xc, W, res, 8 * (int)bx - 2, 8 * (int)by - 2, 8 * (int)bz - 2, gs, gt);
+      for (int i = t; i < kOT3; i += kOpThreads) tile[i] = (T)gt[i];
+    } else {
+      for (int i = t; i < kOT3; i += kOpThreads) {
+        const int lz = i / (kOT * kOT) - 2, ly = (i / kOT) % kOT - 2, lx = i % kOT - 2;
         const int ox = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0),
                   oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
         const uint32_t s2 = nb[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
-        if (s2 != kSent) v = x[(uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox))];
+        T v = T(0);
+        if (s2 != kSent) {
+          const uint64_t g = (uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox));
+          if (MODE == kBandDir) {
+            v = beta != 0.0 ? f[g] + tb * x[g] : f[g];
+            if ((ox | oy | oz) == 0) dout[g] = v;
+          } else {
+            v = x[g];
+          }
+        }
+        tile[i] = v;
       }
-      tile[i] = v;
     }
     __syncthreads();
-    for (int i = t; i < 8 * kOT * kOT; i += kThreads) {
-      const int z = i / (kOT * kOT), yx = i % (kOT * kOT);
-      T am = T(0), as = T(0);
+    if (t < kOT * kOT) {  // z filter of column (x, y)
+      T v[kOT];
 #pragma unroll
-      for (int c = 0; c < 5; ++c) {
-        const T v = tile[(z + c) * kOT * kOT + yx];
-        am += K.m[c] * v;
-        as += K.s[c] * v;
+      for (int z = 0; z < kOT; ++z) v[z] = tile[z * kOT * kOT + t];
+#pragma unroll
+      for (int z = 0; z < 8; ++z) {
+        T am = T(0), as = T(0);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          am += K.m[c] * v[z + c];
+          as += K.s[c] * v[z + c];
+        }
+        um[z * kOT * kOT + t] = am;
+        us[z * kOT * kOT + t] = as;
       }
-      um[i] = am;
-      us[i] = as;
     }
     __syncthreads();
-    for (int i = t; i < 8 * 8 * kOT; i += kThreads) {
-      const int z = i / (8 * kOT), yy = (i / kOT) % 8, xx = i % kOT;
-      T a1 = T(0), a2 = T(0), a3 = T(0);
+    if (t < 8 * kOT) {  // y filter of column (x, z)
+      const int xx = t % kOT, z = t / kOT;
+      T a[kOT], b[kOT];
 #pragma unroll
-      for (int c = 0; c < 5; ++c) {
-        const int q = (z * kOT + yy + c) * kOT + xx;
-        a1 += K.m[c] * um[q];
-        a2 += K.s[c] * um[q];
-        a3 += K.m[c] * us[q];
+      for (int yy = 0; yy < kOT; ++yy) {
+        a[yy] = um[(z * kOT + yy) * kOT + xx];
+        b[yy] = us[(z * kOT + yy) * kOT + xx];
       }
-      w1[i] = a1;
-      w23[i] = a2 + a3;
+#pragma unroll
+      for (int yy = 0; yy < 8; ++yy) {
+        T a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+          a1 += K.m[c] * a[yy + c];
+          a2 += K.s[c] * a[yy + c];
+          a3 += K.m[c] * b[yy + c];
+        }
+        w1[(z * 8 + yy) * kWS + xx] = a1;
+        w23[(z * 8 + yy) * kWS + xx] = a2 + a3;
+      }
     }
     __syncthreads();
+    if (t < 64) {  // x filter of row (y, z), 8 outputs
+      const int yy = t % 8, z = t / 8;
+      T p[kOT], q[kOT], o[8];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int o = t + j * kThreads, z = o >> 6, yy = (o >> 3) & 7, xx = o & 7;
-      const int r = (z * 8 + yy) * kOT + xx;
-      T acc = T(0);
+      for (int xx = 0; xx < kOT; ++xx) {
+        p[xx] = w1[(z * 8 + yy) * kWS + xx];
+        q[xx] = w23[(z * 8 + yy) * kWS + xx];
+      }
+      const uint64_t g0 = slot * kBN + (uint64_t)(z * 64 + yy * 8);
 #pragma unroll
-      for (int c = 0; c < 5; ++c) acc += K.s[c] * w1[r + c] + K.m[c] * w23[r + c];
-      const T v = K.H * acc + K.wg * tile[((z + 2) * kOT + yy + 2) * kOT + xx + 2];
-      const uint64_t gi = slot * kBN + o;
-      y[gi] = MODE == 0 ? v : f[gi] - v;
+      for (int xx = 0; xx < 8; ++xx) {
+        T acc = T(0);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) acc += K.s[c] * p[xx + c] + K.m[c] * q[xx + c];
+        const T ctr = tile[((z + 2) * kOT + yy + 2) * kOT + xx + 2];
+        o[xx] = K.H * acc + K.wg * ctr;
+        if (MODE == kBandResid) o[xx] = f[g0 + xx] - o[xx];
+        if (MODE == kBandDir) dacc += (double)ctr * (double)o[xx];
+      }
+#pragma unroll
+      for (int xx = 0; xx < 8; ++xx) y[g0 + xx] = o[xx];
     }
     __syncthreads();
   }
+  if (MODE == kBandDir && part) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) dacc += __shfl_down_sync(0xffffffffu, dacc, off);
+    if ((t & 31) == 0) red[t >> 5] = dacc;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < kOpThreads / 32; ++w) sum += red[w];
+      part[blockIdx.x] = sum;
+    }
+  }
 }
 
-// screening: proj_p = sum_k phi x[key]; y[node] += sgn wh3 sum phi proj over the node's pairs
+// screening: proj_p = sum_k phi x[key]; y[node] += sgn wh3 sum phi proj over the node's pairs;
+// sq (optional): per-block sums of proj^2 (x . wh3 Phi Phi^T x = wh3 sum_p proj_p^2)
 template <typename T>
 __global__ void k_ab_screen_proj(const uint32_t* __restrict__ key, const T* __restrict__ phi, uint64_t P,
-                                 const T* __restrict__ x, T* __restrict__ proj) {
+                                 const T* __restrict__ x, T* __restrict__ proj, double* __restrict__ sq) {
+  double acc = 0.0;
   for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
     T s = T(0);
     for (int k = 0; k < 27; ++k) {
@@ -411,6 +525,13 @@ __global__ void k_ab_screen_proj(const uint32_t* __restrict__ key, const T* __re
       if (kk != kSent) s += phi[27 * p + k] * x[kk];
     }
     proj[p] = s;
+    acc += (double)s * (double)s;
+  }
+  if (sq) {
+    typedef cub::BlockReduce<double, kThreads> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double tot = BR(tmp).Sum(acc);
+    if (threadIdx.x == 0) sq[blockIdx.x] = tot;
   }
 }
 template <typename T>
@@ -439,20 +560,75 @@ __global__ void k_ab_dinv_screen(const uint32_t* __restrict__ run_key, const dou
   for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < T_runs; r += (uint64_t)gridDim.x * blockDim.x)
     dinv[run_key[r]] = (T)(1.0 / (diag + wh3 * sphi2[r]));
 }
+// the CG update with the Jacobi step: x += alpha d, r -= alpha q, z = dinv r; per-block sums of
+// r . r (part[2 b]) and r . z (part[2 b + 1]) in FP64
 template <typename T>
-__global__ void k_ab_mul(const T* __restrict__ a, const T* __restrict__ b, uint64_t n, T* __restrict__ out) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = a[i] * b[i];
+__global__ void k_ab_update(uint64_t n, double alpha, const T* __restrict__ d, const T* __restrict__ q,
+                            T* __restrict__ x, T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ z,
+                            double* __restrict__ part) {
+  const T a = (T)alpha;
+  double rr = 0.0, rz = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    x[i] += a * d[i];
+    const T ri = r[i] - a * q[i];
+    r[i] = ri;
+    const T zi = dinv[i] * ri;
+    z[i] = zi;
+    rr += (double)ri * (double)ri;
+    rz += (double)ri * (double)zi;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double trr = BR(tmp).Sum(rr);
+  __syncthreads();
+  const double trz = BR(tmp).Sum(rz);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = trr;
+    part[2 * blockIdx.x + 1] = trz;
+  }
+}
+// z = dinv r with per-block sums of r . r and r . z (the first step)
+template <typename T>
+__global__ void k_ab_precond(uint64_t n, const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ z,
+                             double* __restrict__ part) {
+  double rr = 0.0, rz = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const T ri = r[i], zi = dinv[i] * ri;
+    z[i] = zi;
+    rr += (double)ri * (double)ri;
+    rz += (double)ri * (double)zi;
+  }
+  typedef cub::BlockReduce<double, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const double trr = BR(tmp).Sum(rr);
+  __syncthreads();
+  const double trz = BR(tmp).Sum(rz);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = trr;
+    part[2 * blockIdx.x + 1] = trz;
+  }
+}
+// out[k] = sum of part[stride i + k] over i < np (k < stride), in a fixed order (one warp per k)
+__global__ void k_ab_sum_parts(const double* __restrict__ part, int np, int stride, double scale, double* __restrict__ out) {
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += 32) s += part[(size_t)i * stride + k];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) out[k] = scale * s;
 }
 
-// g on the band nodes
-__global__ void k_ab_prolong_band(const uint32_t* __restrict__ bkey, uint64_t NB, const double* __restrict__ xc,
-                                  Prolong W, double* __restrict__ g) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < NB * kBN; i += (uint64_t)gridDim.x * blockDim.x) {
+// g on the band nodes, a brick per CTA iteration
+__global__ void __launch_bounds__(kThreads) k_ab_prolong_band(const uint32_t* __restrict__ bkey, uint64_t NB,
+                                                              const double* __restrict__ xc, Prolong W, int res,
+                                                              double* __restrict__ g) {
+  __shared__ double scratch[kProlongScratch(8)], tile[kBN];
+  for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
     uint32_t bx, by, bz;
-    unmorton3(bkey[i / kBN], bx, by, bz);
-    const int l = (int)(i % kBN);
-    g[i] = prolong_at(xc, W, 8 * (int)bx + (l & 7), 8 * (int)by + ((l >> 3) & 7), 8 * (int)bz + (l >> 6));
+    unmorton3(bkey[slot], bx, by, bz);
+    prolong_tile<8>(xc, W, res, 8 * (int)bx, 8 * (int)by, 8 * (int)bz, scratch, tile);
+    for (int i = threadIdx.x; i < kBN; i += kThreads) g[slot * kBN + i] = tile[i];
+    __syncthreads();
   }
 }
 
@@ -517,28 +693,21 @@ __device__ __forceinline__ uint32_t ab_edge_mask(uint32_t mc) {
 // The brick's 9^3 corner values at grid positions 8b + q (q = 0..8 per axis): node tile 10^3
 // (nodes 8b - 1 .. 8b + 8; f on the band, g elsewhere), each corner the in-order sum over the
 // nodes p - 1, p per axis inside the grid of ((x / 2) / 2) / 2 (the dense path's grid-position
-// evaluation).  Returns the brick origin.
+// evaluation).
 __device__ void ab_corner_values(uint64_t slot, const uint32_t* nb, const double* __restrict__ f,
                                  const uint32_t* __restrict__ bkey, const double* __restrict__ xc, const Prolong& W,
-                                 int res, double* node, double* cv, int* org) {
+                                 int res, double* node, double* cv, double* scratch) {
   const int t = threadIdx.x;
   uint32_t bx, by, bz;
   unmorton3(bkey[slot], bx, by, bz);
-  org[0] = 8 * (int)bx;
-  org[1] = 8 * (int)by;
-  org[2] = 8 * (int)bz;
+  const int org[3] = {8 * (int)bx, 8 * (int)by, 8 * (int)bz};
+  prolong_tile<kMT>(xc, W, res, org[0] - 1, org[1] - 1, org[2] - 1, scratch, node);
   for (int i = t; i < kMT * kMT * kMT; i += kThreads) {
     const int lz = i / (kMT * kMT) - 1, ly = (i / kMT) % kMT - 1, lx = i % kMT - 1;
-    const int gx = org[0] + lx, gy = org[1] + ly, gz = org[2] + lz;
-    double v = 0.0;
-    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < res && gy < res && gz < res) {
-      const int ox = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0),
-                oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
-      const uint32_t s2 = nb[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
-      v = s2 != kSent ? f[(uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox))]
-                      : prolong_at(xc, W, gx, gy, gz);
-    }
-    node[i] = v;
+    const int ox = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0),
+              oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
+    const uint32_t s2 = nb[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
+    if (s2 != kSent) node[i] = f[(uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox))];
   }
   __syncthreads();
   for (int i = t; i < 9 * 9 * 9; i += kThreads) {
@@ -563,6 +732,18 @@ __device__ void ab_corner_values(uint64_t slot, const uint32_t* nb, const double
   __syncthreads();
 }
 
+// key of edge e of a cell: its lower grid position and axis, ((z (res+1) + y) (res+1) + x) 3 + axis
+__device__ __forceinline__ uint64_t ab_edge_key(const int* cell, int e, uint64_t R1) {
+  const int ia = c_abev[e][0], ib = c_abev[e][1];
+  int st[3], axis = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    st[a] = cell[a] + min(c_abco[ia][a], c_abco[ib][a]);
+    if (c_abco[ia][a] != c_abco[ib][a]) axis = a;
+  }
+  return (((uint64_t)st[2] * R1 + (uint64_t)st[1]) * R1 + (uint64_t)st[0]) * 3 + (uint64_t)axis;
+}
+
 __device__ __forceinline__ uint32_t ab_cell_case(const double* cv, int o, double iso) {
   const int z = o >> 6, y = (o >> 3) & 7, x = o & 7;
   uint32_t mc = 0;
@@ -578,16 +759,15 @@ __global__ void __launch_bounds__(kThreads) k_ab_mc_count(const double* __restri
                                                           const uint32_t* __restrict__ bkey, uint64_t NB,
                                                           const double* __restrict__ xc, Prolong W, int res, double iso,
                                                           uint32_t* __restrict__ ntri, uint32_t* __restrict__ nedge) {
-  __shared__ double node[kMT * kMT * kMT], cv[729];
+  __shared__ double node[kMT * kMT * kMT], cv[729], scratch[kProlongScratch(kMT)];
   __shared__ uint32_t nb[27];
-  __shared__ int org[3];
   typedef cub::BlockReduce<uint32_t, kThreads> BR;
   __shared__ typename BR::TempStorage tmp;
   const int t = threadIdx.x;
   for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
     if (t < 27) nb[t] = nbr[27 * slot + t];
     __syncthreads();
-    ab_corner_values(slot, nb, f, bkey, xc, W, res, node, cv, org);
+    ab_corner_values(slot, nb, f, bkey, xc, W, res, node, cv, scratch);
     uint32_t a = 0, e = 0;
     for (int j = 0; j < 2; ++j) {
       const uint32_t mc = ab_cell_case(cv, 2 * t + j, iso);
@@ -605,15 +785,14 @@ __global__ void __launch_bounds__(kThreads) k_ab_mc_count(const double* __restri
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_ab_mc_emit(const double* __restrict__ f, const uint32_t* __restrict__ nbr,
+__global__ void __launch_bounds__(kThreads, 2) k_ab_mc_emit(const double* __restrict__ f, const uint32_t* __restrict__ nbr,
                                                          const uint32_t* __restrict__ bkey, uint64_t NB,
                                                          const double* __restrict__ xc, Prolong W, int res, double iso,
                                                          const uint64_t* __restrict__ toff, const uint64_t* __restrict__ eoff,
                                                          uint64_t* __restrict__ tri_key, uint64_t* __restrict__ edge_key,
                                                          double* __restrict__ epos) {
-  __shared__ double node[kMT * kMT * kMT], cv[729];
+  __shared__ double node[kMT * kMT * kMT], cv[729], scratch[kProlongScratch(kMT)];
   __shared__ uint32_t nb[27];
-  __shared__ int org[3];
   typedef cub::BlockScan<uint32_t, kThreads> BS;
   __shared__ typename BS::TempStorage tmp;
   const int t = threadIdx.x;
@@ -622,7 +801,10 @@ __global__ void __launch_bounds__(kThreads) k_ab_mc_emit(const double* __restric
   for (uint64_t slot = blockIdx.x; slot < NB; slot += gridDim.x) {
     if (t < 27) nb[t] = nbr[27 * slot + t];
     __syncthreads();
-    ab_corner_values(slot, nb, f, bkey, xc, W, res, node, cv, org);
+    ab_corner_values(slot, nb, f, bkey, xc, W, res, node, cv, scratch);
+    uint32_t bx, by, bz;
+    unmorton3(bkey[slot], bx, by, bz);
+    const int org[3] = {8 * (int)bx, 8 * (int)by, 8 * (int)bz};
     uint32_t mc[2], ct = 0, ce = 0;
     for (int j = 0; j < 2; ++j) {
       mc[j] = ab_cell_case(cv, 2 * t + j, iso);
@@ -637,39 +819,26 @@ __global__ void __launch_bounds__(kThreads) k_ab_mc_emit(const double* __restric
     for (int j = 0; j < 2; ++j) {
       const int o = 2 * t + j, cz = o >> 6, cy = (o >> 3) & 7, cx = o & 7;
       const int cell[3] = {org[0] + cx, org[1] + cy, org[2] + cz};
-      double c8[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) c8[k] = cv[((cz + c_abco[k][2]) * 9 + cy + c_abco[k][1]) * 9 + cx + c_abco[k][0]];
-      uint64_t ekey[12];
-#pragma unroll
-      for (int e = 0; e < 12; ++e) {
-        const int ia = c_abev[e][0], ib = c_abev[e][1];
-        int st[3], axis = 0;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          st[a] = cell[a] + min(c_abco[ia][a], c_abco[ib][a]);
-          if (c_abco[ia][a] != c_abco[ib][a]) axis = a;
-        }
-        ekey[e] = (((uint64_t)st[2] * R1 + (uint64_t)st[1]) * R1 + (uint64_t)st[0]) * 3 + (uint64_t)axis;
-      }
       const uint32_t em = ab_edge_mask(mc[j]);
       for (int e = 0; e < 12; ++e) {
         if (!((em >> e) & 1u)) continue;
         const int ia = c_abev[e][0], ib = c_abev[e][1];
-        const double dv = xsub(c8[ib], c8[ia]);
-        const double tt = fabs(dv) < 1e-15 ? 0.5 : xdiv(xsub(iso, c8[ia]), dv);
+        const double va = cv[((cz + c_abco[ia][2]) * 9 + cy + c_abco[ia][1]) * 9 + cx + c_abco[ia][0]];
+        const double vb = cv[((cz + c_abco[ib][2]) * 9 + cy + c_abco[ib][1]) * 9 + cx + c_abco[ib][0]];
+        const double dv = xsub(vb, va);
+        const double tt = fabs(dv) < 1e-15 ? 0.5 : xdiv(xsub(iso, va), dv);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           const double base = xmul((double)(cell[a] + c_abco[ia][a]), w);
           const double d = (double)(c_abco[ib][a] - c_abco[ia][a]);
           epos[3 * eo + a] = xadd(base, xmul(xmul(tt, d), w));
         }
-        edge_key[eo] = ekey[e];
+        edge_key[eo] = ab_edge_key(cell, e, R1);
         ++eo;
       }
       const uint64_t packed = PR_MC_TRIS[mc[j]];
       const uint32_t ntr = PR_MC_NTRI[mc[j]];
-      for (uint32_t i = 0; i < 3 * ntr; ++i) tri_key[3 * to + i] = ekey[(packed >> (4 * i)) & 15u];
+      for (uint32_t i = 0; i < 3 * ntr; ++i) tri_key[3 * to + i] = ab_edge_key(cell, (int)((packed >> (4 * i)) & 15u), R1);
       to += ntr;
     }
     __syncthreads();
@@ -786,25 +955,35 @@ struct Band {
   const T* phi() {
     return sizeof(T) == 8 ? (const T*)c->get<double>("ab_phi64") : (const T*)c->get<float>("ab_phi32");
   }
-  // y = A_BB x (MODE 0) or y = f - A_BB x (MODE 1), screening included
+  // y = A_BB x (kBandApply) or y = f - A_BB x (kBandResid), screening included
   template <typename T, int MODE>
   void op(const T* x, const T* f, T* y) {
-    k_ab_op<T, MODE><<<brick_grid(NB), kThreads, 0, c->stream>>>(x, f, y, nbr, bkey, NB, band_coef<T>(c->D, c->pw),
-                                                                 nullptr, W, res);
-    PR_CHECK_LAUNCH();
-    bytes += 2.0 * n * sizeof(T) + (MODE == 1 ? n * sizeof(T) : 0.0);
-    screen<T>(x, y, MODE == 0 ? 1.0 : -1.0);
+    launch_op<T, MODE, false>(x, f, y, nullptr, 0.0, nullptr);
+    bytes += 2.0 * n * sizeof(T) + (MODE == kBandResid ? n * sizeof(T) : 0.0);
+    screen<T>(x, y, MODE == kBandApply ? 1.0 : -1.0, nullptr);
   }
+  template <typename T, int MODE, bool GSRC>
+  void launch_op(const T* x, const T* f, T* y, T* dout, double beta, double* part) {
+    const size_t sm = band_op_smem<T>(GSRC);
+    allow_smem(k_ab_op<T, MODE, GSRC>, sm);
+    k_ab_op<T, MODE, GSRC><<<grid_op(), kOpThreads, sm, c->stream>>>(x, f, y, dout, beta, nbr, bkey, NB,
+                                                                     band_coef<T>(c->D, c->pw), xc, W, res, part);
+    PR_CHECK_LAUNCH();
+  }
+  unsigned grid_op() const { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(NB, 148 * 16)); }
+  // y += sign wh3 Phi Phi^T x; sq: per-block sums of proj^2 (returns their count)
   template <typename T>
-  void screen(const T* x, T* y, double sign) {
-    if (S == 0 || !(wh3 > 0.0)) return;
+  int screen(const T* x, T* y, double sign, double* sq) {
+    if (S == 0 || !(wh3 > 0.0)) return 0;
     T* proj = c->buf<T>(std::string("ab_proj_") + tname<T>(), P);
-    k_ab_screen_proj<T><<<grid_for(P, 1u << 20), kThreads, 0, c->stream>>>(kin, phi<T>(), P, x, proj);
+    const unsigned np = grid_for(P, 1u << 20);
+    k_ab_screen_proj<T><<<np, kThreads, 0, c->stream>>>(kin, phi<T>(), P, x, proj, sq);
     PR_CHECK_LAUNCH();
     k_ab_screen_gather<T><<<grid_for(S, 1u << 20), kThreads, 0, c->stream>>>(snode, soff, S, sval, phi<T>(), proj,
                                                                               (T)(sign * wh3), y);
     PR_CHECK_LAUNCH();
     bytes += (double)P * 27 * (4 + 2 * sizeof(T)) + (double)S * (8 + 2 * sizeof(T));
+    return (int)np;
   }
   template <typename T>
   T* dinv() {
@@ -826,39 +1005,64 @@ struct Band {
 };
 
 // Jacobi-preconditioned CG on A_BB x = r from x = 0 until ||r|| <= tol; r is overwritten with
-// the residual; returns the iterations
+// the residual; returns the iterations.  Per iteration: one operator pass that forms the direction
+// d = z + beta dold and q = A d with d . q (plus the screening pass), and one update pass x, r, z
+// with r . r and r . z; every sum is a fixed-order FP64 sum of per-block partials.
 template <typename T>
-int band_pcg(Band& B, T* r, T* x, double tol, int maxit, double rr) {
+int band_pcg(Band& B, T* r, T* x, double tol, int maxit) {
   pr_context* c = B.c;
   const uint64_t n = B.n;
   cudaStream_t s = c->stream;
   const std::string tn = tname<T>();
   T* z = c->buf<T>("ab_z_" + tn, n);
   T* d = c->buf<T>("ab_d_" + tn, n);
+  T* dn = c->buf<T>("ab_dn_" + tn, n);  // the direction alternates between d and dn
   T* q = c->buf<T>("ab_q_" + tn, n);
   const T* dv = B.dinv<T>();
+  const int nbk = kDotBlocks;
+  double* part = c->buf<double>("ab_part", 2 * (size_t)std::max<unsigned>(nbk, B.grid_op()));
+  double* part2 = c->buf<double>("ab_part2", grid_for(B.P, 1u << 20));
+  double* sums = c->buf<double>("ab_sums", 4);
+  double* h = c->h_scalars;
   PR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), s));
-  k_ab_mul<T><<<grid_for(n), kThreads, 0, s>>>(r, dv, n, z);
+  k_ab_precond<T><<<nbk, kThreads, 0, s>>>(n, r, dv, z, part);
   PR_CHECK_LAUNCH();
-  double rz = dot<T>(c, r, z, n);
-  PR_CUDA(cudaMemcpyAsync(d, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
-  B.bytes += 7.0 * n * sizeof(T);
+  k_ab_sum_parts<<<2, 32, 0, s>>>(part, nbk, 2, 1.0, sums);
+  PR_CHECK_LAUNCH();
+  PR_CUDA(cudaMemcpyAsync(h, sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  c->sync();
+  double rr = h[0], rz = h[1], beta = 0.0;
+  B.bytes += 3.0 * n * sizeof(T);
   int it = 0;
   while (std::sqrt(rr) > tol && it < maxit) {
-    B.op<T, 0>(d, nullptr, q);
-    const double dq = dot<T>(c, d, q, n);
+    // dn = z + beta d, q = A dn (beta = 0 on the first pass: d is not read)
+    const int nop = (int)B.grid_op();
+    B.launch_op<T, kBandDir, false>(d, z, q, dn, beta, part);
+    std::swap(d, dn);
+    const int nsq = B.screen<T>(d, q, 1.0, part2);
+    k_ab_sum_parts<<<1, 32, 0, s>>>(part, nop, 1, 1.0, sums);
+    PR_CHECK_LAUNCH();
+    if (nsq) {
+      k_ab_sum_parts<<<1, 32, 0, s>>>(part2, nsq, 1, B.wh3, sums + 2);
+      PR_CHECK_LAUNCH();
+    }
+    PR_CUDA(cudaMemcpyAsync(h, sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    const double dq = h[0] + (nsq ? h[2] : 0.0);
+    B.bytes += 4.0 * n * sizeof(T);
     if (!(dq > 0.0)) break;
     const double alpha = rz / dq;
-    rr = cg_update<T>(c, n, alpha, d, q, x, r);
-    ++it;
-    B.bytes += 8.0 * n * sizeof(T);
-    if (std::sqrt(rr) <= tol) break;
-    k_ab_mul<T><<<grid_for(n), kThreads, 0, s>>>(r, dv, n, z);
+    k_ab_update<T><<<nbk, kThreads, 0, s>>>(n, alpha, d, q, x, r, dv, z, part);
     PR_CHECK_LAUNCH();
-    const double rz_new = dot<T>(c, r, z, n);
-    xpby<T>(s, n, z, rz_new / rz, d);
-    rz = rz_new;
+    k_ab_sum_parts<<<2, 32, 0, s>>>(part, nbk, 2, 1.0, sums);
+    PR_CHECK_LAUNCH();
+    PR_CUDA(cudaMemcpyAsync(h, sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    c->sync();
     B.bytes += 8.0 * n * sizeof(T);
+    ++it;
+    rr = h[0];
+    beta = h[1] / rz;
+    rz = h[1];
   }
   return it;
 }
@@ -1077,12 +1281,10 @@ void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extrac
   st.pcg_iterations = sc.pcg_iterations;
   st.refinement_steps = 0;
   if (n > 0) {
-    k_ab_prolong_band<<<grid_for(n, 1u << 20), kThreads, 0, s>>>(B.bkey, B.NB, B.xc, B.W, gB);
+    k_ab_prolong_band<<<brick_grid(B.NB), kThreads, 0, s>>>(B.bkey, B.NB, B.xc, B.W, B.res, gB);
     PR_CHECK_LAUNCH();
-    k_ab_op<double, 1><<<brick_grid(B.NB), kThreads, 0, s>>>(nullptr, b, r0, B.nbr, B.bkey, B.NB,
-                                                             band_coef<double>(D, pw), B.xc, B.W, B.res);
-    PR_CHECK_LAUNCH();
-    B.screen<double>(gB, r0, -1.0);
+    B.launch_op<double, kBandResid, true>(nullptr, b, r0, nullptr, 0.0, nullptr);  // r0 = b - (K + wg) g
+    B.screen<double>(gB, r0, -1.0, nullptr);
     bn = std::sqrt(dot<double>(c, b, b, n));
     PR_CUDA(cudaMemcpyAsync(r64, r0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     PR_CUDA(cudaMemsetAsync(e64, 0, n * sizeof(double), s));
@@ -1094,10 +1296,10 @@ void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extrac
       while (rn > target * bn && used < max_iters) {
         convert_norm(c, r64, r32, n);
         const double tol = std::max(inner, 0.5 * target * bn / rn) * rn;
-        const int it = band_pcg<float>(B, r32, e32, tol, max_iters - used, rn * rn);
+        const int it = band_pcg<float>(B, r32, e32, tol, max_iters - used);
         used += it;
         axpy<float, double>(s, n, 1.0, e32, e64);
-        B.op<double, 1>(e64, r0, r64);
+        B.op<double, kBandResid>(e64, r0, r64);
         const double rn_new = std::sqrt(dot<double>(c, r64, r64, n));
         st.refinement_steps++;
         const bool stalled = it == 0 || !(rn_new < rn);
@@ -1105,8 +1307,8 @@ void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extrac
         if (stalled) break;
       }
     } else if (rn > target * bn) {
-      used = band_pcg<double>(B, r64, e64, 0.5 * target * bn, max_iters, rn * rn);
-      B.op<double, 1>(e64, r0, r64);
+      used = band_pcg<double>(B, r64, e64, 0.5 * target * bn, max_iters);
+      B.op<double, kBandResid>(e64, r0, r64);
       rn = std::sqrt(dot<double>(c, r64, r64, n));
     }
     double* f = c->buf<double>("ab_f", n);
@@ -1120,7 +1322,10 @@ void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extrac
   c->release("ab_e32");
   release_prefix(c, "ab_z_");
   release_prefix(c, "ab_d_");
+  release_prefix(c, "ab_dn_");
   release_prefix(c, "ab_q_");
+  c->release("ab_part");
+  c->release("ab_part2");
   c->sync();
   double t3 = now_seconds();
   st.time_solve = (t1 - tc) + (t3 - t2);
@@ -1239,7 +1444,7 @@ void band_apply64(pr_context* c, const double* d_x, double* d_y) {
   PR_REQUIRE(c->adaptive, PR_ERR_STATE, "no adaptive reconstruction state");
   Band B;
   B.init(c);
-  if (B.n) B.op<double, 0>(d_x, nullptr, d_y);
+  if (B.n) B.op<double, kBandApply>(d_x, nullptr, d_y);
 }
 
 }  // namespace pr
