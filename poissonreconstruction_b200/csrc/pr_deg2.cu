@@ -17,7 +17,8 @@
 // planes with TMA: k_op3r on the finest level (x filter from the stage, y and z in registers),
 // k_op3 on the Galerkin coarse levels (interior and face tiles); smaller levels use k_op2
 // (32 x 8 columns, plain loads into shared memory).  The grid transfers and the right-hand side
-// stream the same way (k_restrict3, k_prolong3, k_rhs3r).
+// stream the same way (k_restrict3, k_prolong3).  The right-hand side is built per 8^3 brick from
+// the normal field of the touched nodes only (k_rhs2_bricks).
 //
 // Solver: conjugate gradients preconditioned by a multigrid V-cycle on K + wg I.  Coarse
 // levels are Galerkin products of the 1-D matrices (P^T X P, P the B2 subdivision
@@ -27,6 +28,7 @@
 // or FP64 throughout.  The solved coefficients are permuted to the Morton order of the
 // degree-1 path for evaluation and marching cubes.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cuda.h>
 
 #include <algorithm>
@@ -1387,15 +1389,6 @@ __global__ void k_pair_keys2(const double* __restrict__ upos, uint64_t P, uint32
 }
 
 // splat per touched node, points in input order: nf = -(sum phi n) / (sum phi), w = sum phi
-// zero the three components of the normal field at the nodes of a previous splat
-__global__ void k_unsplat2(const uint32_t* __restrict__ run_key, uint64_t T, uint64_t n, double* __restrict__ nf) {
-  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t node = run_key[t];
-    nf[node] = 0.0;
-    nf[n + node] = 0.0;
-    nf[2 * n + node] = 0.0;
-  }
-}
 __global__ void k_splat2(const uint32_t* __restrict__ run_key, const uint32_t* __restrict__ run_off, uint64_t T,
                          const uint32_t* __restrict__ sval, const double* __restrict__ phi,
                          const double* __restrict__ unrm, uint64_t P, uint64_t n, double* __restrict__ nf,
@@ -1429,139 +1422,145 @@ __global__ void k_splat2(const uint32_t* __restrict__ run_key, const uint32_t* _
   }
 }
 
-// b = h^2 sum_a (G_a M M) nf_a on the finest level (res >= 64): a CTA owns 64 x 8 columns (x pairs
-// per thread) and streams up to kZChunk3 planes of the three haloed component planes (zero fill
-// outside the grid = the truncated rows).  m is symmetric and g antisymmetric (g[2] = 0), so each
-// 5-tap filter is two pair sums or differences.
+// 1-D integrals of the right-hand side (g: N2' N2, m: N2 N2), h^2, the TMA wait flag
 struct RhsCoef {
   double g[5], m[5], h2;
   int* err;
 };
 
-__device__ __forceinline__ double fsym(const double* v, const double* c) {
-  return c[0] * (v[0] + v[4]) + c[1] * (v[1] + v[3]) + c[2] * v[2];
+// the same per touched node, into a compact field: nfc[t], nfc[T + t], nfc[2 T + t] for run t
+__global__ void k_splat2c(const uint32_t* __restrict__ run_off, uint64_t T, const uint32_t* __restrict__ sval,
+                          const double* __restrict__ phi, const double* __restrict__ unrm, uint64_t P,
+                          double* __restrict__ nfc) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    double fx = 0.0, fy = 0.0, fz = 0.0, sw = 0.0;
+    for (uint32_t e = run_off[t]; e < run_off[t + 1]; ++e) {
+      const uint32_t pk = sval[e];
+      const uint32_t p = pk / 27;
+      const double wgt = phi[pk];
+      fx = xadd(fx, xmul(unrm[p], wgt));
+      fy = xadd(fy, xmul(unrm[P + p], wgt));
+      fz = xadd(fz, xmul(unrm[2 * P + p], wgt));
+      sw = xadd(sw, wgt);
+    }
+    if (sw > 0.0) {
+      fx = xdiv(-fx, sw);
+      fy = xdiv(-fy, sw);
+      fz = xdiv(-fz, sw);
+    }
+    nfc[t] = fx;
+    nfc[T + t] = fy;
+    nfc[2 * T + t] = fz;
+  }
 }
-__device__ __forceinline__ double fanti(const double* v, const double* c) {
-  return c[0] * (v[0] - v[4]) + c[1] * (v[1] - v[3]);
+// dense[node] = compact[t] per component (the accessor's and the small levels' dense field)
+__global__ void k_nf_scatter(const uint32_t* __restrict__ run_key, uint64_t T, const double* __restrict__ nfc,
+                             uint64_t n, double* __restrict__ nf) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t node = run_key[t];
+    nf[node] = nfc[t];
+    nf[n + node] = nfc[T + t];
+    nf[2 * n + node] = nfc[2 * T + t];
+  }
 }
 
-// The right-hand side with the y and z filters in registers (the k_op3r structure): 4 warps on
-// the 64 x 8 tile, each thread two output rows; a three-deep TMA ring of the three haloed component
-// planes; per plane and component the thread filters its six staged rows in x straight from the
-// stage and adds their y filter at once (so one component's rows are live at a time), then
-// scatters (M_y G_x n_x + G_y M_x n_y, M_y M_x n_z) into the five output planes they touch with
-// M_z and G_z.
-struct GeoRr {
-  static constexpr int NSS = 3;  // stages
-  static constexpr int BW = 68;  // from x0 - 2 (16-byte aligned)
-  static constexpr uint32_t PBYTES = BW * SH * sizeof(double);  // one component plane
-  static constexpr uint32_t SBYTES = 3 * PBYTES;
-  static_assert(SBYTES % 128 == 0 && PBYTES % 128 == 0, "stage alignment");
-  static constexpr size_t OFF_BAR = (size_t)NSS * SBYTES;
-  static constexpr size_t BYTES = OFF_BAR + NSS * 8 + 16;
-};
-__global__ void __launch_bounds__(kThreadsR) k_rhs3r(const __grid_constant__ CUtensorMap m0,
-                                                     const __grid_constant__ CUtensorMap m1,
-                                                     const __grid_constant__ CUtensorMap m2, int L,
-                                                     const __grid_constant__ RhsCoef k, double* __restrict__ b) {
-  typedef GeoRr G;
-  constexpr int NSS = G::NSS, BW = G::BW, NW = 5;  // NW: output planes a staged plane touches
-  extern __shared__ __align__(128) unsigned char smem[];
-  auto comp = [&](int st, int a) {
-    return reinterpret_cast<const double*>(smem + (size_t)st * G::SBYTES + a * G::PBYTES);
-  };
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
-  int* s_abort = reinterpret_cast<int*>(smem + G::OFF_BAR + NSS * 8);
-  const int res = 1 << L;
-  const int64_t plane = (int64_t)res * res;
-  const int t = threadIdx.x, p = t & 31, ry = 2 * (t >> 5);
-  const int x0 = blockIdx.x * 64, y0 = blockIdx.y * TY;
-  const int z0 = blockIdx.z * kZChunk3, z1 = min(z0 + kZChunk3, res);
-  const int nplanes = z1 - z0 + 4;
-  const int ngroups = (nplanes + NW - 1) / NW;
-  if (t == 0) {
-    for (int q = 0; q < NSS; ++q) mbar_init(&bar[q], 1);
-    *s_abort = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  const int nissue = ngroups * NW;  // planes past z1 + 1 read zeros and emit nothing
-  auto issue = [&](int it) {
-    const int st = it % NSS, zin = z0 - 2 + it;
-    mbar_expect_tx(&bar[st], G::SBYTES);
-    tma_load_3d(const_cast<double*>(comp(st, 0)), &m0, x0 - 2, y0 - 2, zin, &bar[st]);
-    tma_load_3d(const_cast<double*>(comp(st, 1)), &m1, x0 - 2, y0 - 2, zin, &bar[st]);
-    tma_load_3d(const_cast<double*>(comp(st, 2)), &m2, x0 - 2, y0 - 2, zin, &bar[st]);
-  };
-  if (t == 0)
-    for (int it = 0; it < NSS; ++it) issue(it);
-  double2 acc[2][NW];  // [output row][slot of output plane z0 - 4 + it, it mod 5]
+// Bricks (8^3 blocks of the natural-order grid) whose right-hand side can be nonzero: those within
+// 2 nodes of a touched node.  flag[brick] = 1, brick = bx + nb (by + nb bz).
+__global__ void k_rhs_mark_bricks(const uint32_t* __restrict__ run_key, uint64_t T, int D, uint8_t* __restrict__ flag) {
+  const int res = 1 << D, nb = res >> 3;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t node = run_key[t];
+    const int c[3] = {(int)(node & (res - 1)), (int)((node >> D) & (res - 1)), (int)(node >> (2 * D))};
+    int lo[3], hi[3];
 #pragma unroll
-  for (int j = 0; j < 2; ++j)
-#pragma unroll
-    for (int q = 0; q < NW; ++q) acc[j][q] = make_double2(0.0, 0.0);
-  double* op = b + (int64_t)(x0 + 2 * p) + (int64_t)res * (y0 + ry) + plane * (z0 - 4);
-  int it = 0;
-  bool stop = false;
-  for (int g = 0; g < ngroups; ++g) {
-#pragma unroll
-    for (int kk = 0; kk < NW; ++kk) {
-      it = g * NW + kk;
-      const int st = it % NSS;
-      if (!mbar_wait(&bar[st], (uint32_t)(it / NSS) & 1u)) {
-        atomicExch(k.err, 1);
-        *s_abort = 1;
-      }
-      double wa[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, wb[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // [row][column]
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        double u[6][2];  // x filter of the staged rows ry .. ry + 5 (G on n_x, M on n_y, n_z)
-#pragma unroll
-        for (int r = 0; r < 6; ++r) {
-          const double* row = comp(st, a) + (ry + r) * BW + 2 * p;
-          const double2 v0 = *reinterpret_cast<const double2*>(row), v1 = *reinterpret_cast<const double2*>(row + 2),
-                        v2 = *reinterpret_cast<const double2*>(row + 4);
-          const double v[6] = {v0.x, v0.y, v1.x, v1.y, v2.x, v2.y};
-          u[r][0] = a == 0 ? fanti(v, k.g) : fsym(v, k.m);
-          u[r][1] = a == 0 ? fanti(v + 1, k.g) : fsym(v + 1, k.m);
-        }
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int l = 0; l < 2; ++l) {
-            const double col[5] = {u[j][l], u[j + 1][l], u[j + 2][l], u[j + 3][l], u[j + 4][l]};
-            if (a == 0) wa[j][l] += fsym(col, k.m);        // M_y (G_x n_x)
-            else if (a == 1) wa[j][l] += fanti(col, k.g);  // G_y (M_x n_y)
-            else wb[j][l] = fsym(col, k.m);                // M_y (M_x n_z)
-          }
-      }
-      __syncthreads();  // stage st is read
-      if (*s_abort) {
-        stop = true;
-        break;
-      }
-      if (t == 0 && it + NSS < nissue) issue(it + NSS);
-      // z: plane zin is tap 4 - e of output plane zin - 2 + e (slot (kk + e) mod 5): M_z on wa, G_z on wb
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int e = 0; e < NW; ++e) {
-          const double cm = k.m[4 - e], cg = k.g[4 - e];
-          double2& s2 = acc[j][(kk + e) % NW];
-          if (e == NW - 1) s2 = make_double2(cm * wa[j][0] + cg * wb[j][0], cm * wa[j][1] + cg * wb[j][1]);
-          else s2 = make_double2(s2.x + (cm * wa[j][0] + cg * wb[j][0]), s2.y + (cm * wa[j][1] + cg * wb[j][1]));
-        }
-      if ((unsigned)(it - 4) < (unsigned)(z1 - z0)) {
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-          *reinterpret_cast<double2*>(op + (int64_t)j * res) = make_double2(k.h2 * acc[j][kk].x, k.h2 * acc[j][kk].y);
-      }
-      op += plane;
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = max(c[a] - 2, 0) >> 3;
+      hi[a] = min(c[a] + 2, res - 1) >> 3;
     }
-    if (stop) break;
+    for (int z = lo[2]; z <= hi[2]; ++z)
+      for (int y = lo[1]; y <= hi[1]; ++y)
+        for (int x = lo[0]; x <= hi[0]; ++x) flag[x + nb * (y + nb * z)] = 1;
   }
-  if (stop && t == 0)
-    for (int q = it; q < min(it + NSS, nissue); ++q) mbar_wait(&bar[q % NSS], (uint32_t)(q / NSS) & 1u);
+}
+
+// b = h^2 sum_a (G_a M M) nf_a on the listed bricks (b is zero elsewhere): per brick, the compact
+// normal field of the brick and its 2-node halo goes into a shared 12^3 x 3 tile (each of the
+// 144 tile rows found by a binary search of the sorted run keys), then z, y and x passes.
+constexpr int kRB = 12, kRB3 = kRB * kRB * kRB;
+constexpr size_t kRhsBrickSmem = (3 * kRB3 + 8 * kRB * kRB + 8 * 8 * kRB) * sizeof(double);
+__global__ void __launch_bounds__(kThreads) k_rhs2_bricks(const uint32_t* __restrict__ bricks, uint64_t NBo, int D,
+                                                          const uint32_t* __restrict__ run_key, uint64_t T,
+                                                          const double* __restrict__ nfc, RhsCoef k,
+                                                          double* __restrict__ b) {
+  extern __shared__ double sm2[];
+  double* nf = sm2;                 // [3][12][12][12]
+  double* tz = nf + 3 * kRB3;       // [8][12][12]
+  double* ty = tz + 8 * kRB * kRB;  // [8][8][12]
+  const int t = threadIdx.x, res = 1 << D, nb = res >> 3;
+  for (uint64_t i = blockIdx.x; i < NBo; i += gridDim.x) {
+    const uint32_t bid = bricks[i];
+    const int bx = (int)(bid % nb), by = (int)((bid / nb) % nb), bz = (int)(bid / ((uint32_t)nb * nb));
+    const int ox = 8 * bx - 2, oy = 8 * by - 2, oz = 8 * bz - 2;
+    for (int j = t; j < 3 * kRB3; j += kThreads) nf[j] = 0.0;
+    __syncthreads();
+    if (t < kRB * kRB) {
+      const int gy = oy + t % kRB, gz = oz + t / kRB;
+      if (gy >= 0 && gz >= 0 && gy < res && gz < res) {
+        const uint64_t row = (uint64_t)res * (gy + (uint64_t)res * gz);
+        const uint64_t k0 = row + (uint64_t)max(ox, 0), k1 = row + (uint64_t)min(ox + kRB, res);
+        uint64_t a = 0, e = T;
+        while (a < e) {
+          const uint64_t m = (a + e) >> 1;
+          if ((uint64_t)run_key[m] < k0) a = m + 1;
+          else e = m;
+        }
+        for (uint64_t r = a; r < T && (uint64_t)run_key[r] < k1; ++r) {
+          const int o = t * kRB + (int)((uint64_t)run_key[r] - row) - ox;
+          nf[o] = nfc[r];
+          nf[kRB3 + o] = nfc[T + r];
+          nf[2 * kRB3 + o] = nfc[2 * T + r];
+        }
+      }
+    }
+    __syncthreads();
+    double acc[2] = {0.0, 0.0};
+    for (int a = 0; a < 3; ++a) {
+      const double* fz = a == 2 ? k.g : k.m;
+      const double* fy = a == 1 ? k.g : k.m;
+      const double* fx = a == 0 ? k.g : k.m;
+      const double* src = nf + a * kRB3;
+      for (int j = t; j < 8 * kRB * kRB; j += kThreads) {
+        const int z = j / (kRB * kRB), yx = j % (kRB * kRB);
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v += fz[c] * src[(z + c) * kRB * kRB + yx];
+        tz[j] = v;
+      }
+      __syncthreads();
+      for (int j = t; j < 8 * 8 * kRB; j += kThreads) {
+        const int z = j / (8 * kRB), y = (j / kRB) % 8, x = j % kRB;
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v += fy[c] * tz[(z * kRB + y + c) * kRB + x];
+        ty[j] = v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) {
+        const int o = t + jj * kThreads, z = o >> 6, y = (o >> 3) & 7, x = o & 7;
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v += fx[c] * ty[(z * 8 + y) * kRB + x + c];
+        acc[jj] += v;
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj) {
+      const int o = t + jj * kThreads, z = o >> 6, y = (o >> 3) & 7, x = o & 7;
+      b[(uint64_t)(8 * bx + x) + (uint64_t)res * ((8 * by + y) + (uint64_t)res * (8 * bz + z))] = k.h2 * acc[jj];
+    }
+  }
 }
 
 // screening right-hand side: b[node] += (wh3 / 2) sum of phi over the node's pairs
@@ -2385,7 +2384,9 @@ __global__ void k_rhs_small(const double* __restrict__ nf, int L, RhsCoef k, dou
   }
 }
 
-void deg2_rhs(pr_context* c, const double* nf, double* b, uint32_t D, double h) {
+// b = h^2 sum_a (G_a M M) nf_a from the compact normal field of the T touched nodes: zero, then
+// the bricks within 2 nodes of a touched node (the 1-D integrals reach 2 nodes)
+void deg2_rhs(pr_context* c, const double* nfc, uint64_t T, double* b, uint32_t D, double h) {
   cudaStream_t s = c->stream;
   RhsCoef k;
   for (int d = 0; d < 5; ++d) {
@@ -2393,27 +2394,45 @@ void deg2_rhs(pr_context* c, const double* nf, double* b, uint32_t D, double h) 
     k.m[d] = consts().m[d];
   }
   k.h2 = h * h;
-  int* err = c->buf<int>("d2_err", 1);
-  PR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  k.err = err;
+  k.err = nullptr;
   const uint64_t n = 1ull << (3 * D);
-  const int res = 1 << D;
-  if ((int)D < kTmaMinLevel) {
+  PR_CUDA(cudaMemsetAsync(b, 0, n * sizeof(double), s));
+  if (T == 0) return;
+  const uint32_t* run_key = c->get<uint32_t>("d2s_runkey");
+  if (D < 3) {  // a grid smaller than one brick: the dense field
+    double* nf = c->buf<double>("d2_nf_small", 3 * n);
+    PR_CUDA(cudaMemsetAsync(nf, 0, 3 * n * sizeof(double), s));
+    k_nf_scatter<<<grid_for(T), kThreads, 0, s>>>(run_key, T, nfc, n, nf);
+    PR_CHECK_LAUNCH();
     k_rhs_small<<<grid_for(n), kThreads, 0, s>>>(nf, (int)D, k, b);
     PR_CHECK_LAUNCH();
+    c->release("d2_nf_small");
     return;
   }
-  allow_smem(k_rhs3r, GeoRr::BYTES);
-  const CUtensorMap m0 = plane_map<double>(nf, (int)D, GeoRr::BW, SH);
-  const CUtensorMap m1 = plane_map<double>(nf + n, (int)D, GeoRr::BW, SH);
-  const CUtensorMap m2 = plane_map<double>(nf + 2 * n, (int)D, GeoRr::BW, SH);
-  const dim3 grid(res / 64, res / TY, (res + kZChunk3 - 1) / kZChunk3);
-  k_rhs3r<<<grid, kThreadsR, GeoRr::BYTES, s>>>(m0, m1, m2, (int)D, k, b);
+  const uint64_t nb = 1ull << (D - 3), nb3 = nb * nb * nb;
+  uint8_t* flag = c->buf<uint8_t>("d2_rflag", nb3);
+  uint32_t* list = c->buf<uint32_t>("d2_rlist", nb3);
+  uint32_t* nsel = c->buf<uint32_t>("d2_rnsel", 1);
+  PR_CUDA(cudaMemsetAsync(flag, 0, nb3, s));
+  k_rhs_mark_bricks<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(run_key, T, (int)D, flag);
   PR_CHECK_LAUNCH();
-  int h_err = 0;
-  PR_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  thrust::counting_iterator<uint32_t> ids(0);
+  size_t tb = 0;
+  PR_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, ids, flag, list, nsel, (int64_t)nb3, s));
+  void* tmp = c->buf<char>("cub_tmp", tb);
+  PR_COUNT_PRIMITIVE();
+  PR_CUDA(cub::DeviceSelect::Flagged(tmp, tb, ids, flag, list, nsel, (int64_t)nb3, s));
+  uint32_t h_n = 0;
+  PR_CUDA(cudaMemcpyAsync(&h_n, nsel, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   c->sync();
-  PR_REQUIRE(h_err == 0, PR_ERR_CUDA, "degree-2 right-hand side: a TMA pipeline wait timed out");
+  if (h_n > 0) {
+    allow_smem(k_rhs2_bricks, kRhsBrickSmem);
+    const unsigned grid = (unsigned)std::min<uint64_t>(h_n, 148 * 16);
+    k_rhs2_bricks<<<grid, kThreads, kRhsBrickSmem, s>>>(list, h_n, (int)D, run_key, T, nfc, k, b);
+    PR_CHECK_LAUNCH();
+  }
+  c->release("d2_rflag");
+  c->release("d2_rlist");
 }
 }  // namespace
 
@@ -2436,17 +2455,6 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
   float* phi32 = c->buf<float>("d2_phi32", m);
   unsigned long long* nin = c->buf<unsigned long long>("d2_nin", 1);
   PR_CUDA(cudaMemsetAsync(nin, 0, sizeof(unsigned long long), s));
-  // the normal field must be zero before the splat: when it still holds only the last splat of
-  // this context (same buffer, same depth), zero those nodes instead of the whole grid (the last
-  // run keys are overwritten by the sort below)
-  double* nf = c->buf<double>("d2_nf", 3 * n);
-  const bool nf_known = c->nf_clean == nf && c->nf_clean_D == D;
-  if (nf_known && c->nf_dirty_T > 0) {
-    k_unsplat2<<<grid_for(c->nf_dirty_T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runkey"), c->nf_dirty_T,
-                                                                       n, nf);
-    PR_CHECK_LAUNCH();
-  }
-  c->nf_clean = nullptr;  // until the splat below has completed
   k_pair_keys2<<<grid_for(m, 1u << 20), kThreads, 0, s>>>(upos, P, D, kin, vin, phi64, phi32, nin);
   PR_CHECK_LAUNCH();
   const uint64_t T = sort_and_segment(c, "d2s", kin, vin, m, D);
@@ -2458,18 +2466,16 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
   c->sync();
   c->T = T;
   c->P_in = h_nin;
-  if (!nf_known) PR_CUDA(cudaMemsetAsync(nf, 0, 3 * n * sizeof(double), s));
+  // the normal field only at the touched nodes (it is zero elsewhere)
+  double* nfc = c->buf<double>("d2_nfc", 3 * std::max<uint64_t>(T, 1));
   if (T > 0) {
-    k_splat2<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runkey"), c->get<uint32_t>("d2s_runoff"),
-                                                        T, c->get<uint32_t>("d2s_val"), phi64, unrm, P, n, nf, nullptr);
+    k_splat2c<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runoff"), T, c->get<uint32_t>("d2s_val"),
+                                                         phi64, unrm, P, nfc);
     PR_CHECK_LAUNCH();
   }
-  c->nf_clean = nf;
-  c->nf_clean_D = D;
-  c->nf_dirty_T = T;
   const double h = 1.0 / (double)(1u << D);
   double* b = c->buf<double>("d2_b", n);
-  deg2_rhs(c, nf, b, D, h);
+  deg2_rhs(c, nfc, T, b, D, h);
   c->S = 0;
   c->S_pairs = 0;
   if (pw > 0.0 && T > 0) {
@@ -2725,8 +2731,17 @@ void deg2_rhs_morton(pr_context* c, double* d_out) {
   PR_CHECK_LAUNCH();
 }
 void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w) {
-  k_nat3_to_morton_aos<<<grid_for(c->n), kThreads, 0, c->stream>>>(c->get<double>("d2_nf"), c->D, d_nf3);
+  // the dense field, scattered from the compact one for the accessor
+  double* nf = c->buf<double>("d2_nf_acc", 3 * c->n);
+  PR_CUDA(cudaMemsetAsync(nf, 0, 3 * c->n * sizeof(double), c->stream));
+  if (c->T > 0) {
+    k_nf_scatter<<<grid_for(c->T, 1u << 20), kThreads, 0, c->stream>>>(c->get<uint32_t>("d2s_runkey"), c->T,
+                                                                        c->get<double>("d2_nfc"), c->n, nf);
+    PR_CHECK_LAUNCH();
+  }
+  k_nat3_to_morton_aos<<<grid_for(c->n), kThreads, 0, c->stream>>>(nf, c->D, d_nf3);
   PR_CHECK_LAUNCH();
+  c->release("d2_nf_acc");
   // the per-node weight sums, rebuilt here from the node-sorted pairs (the reconstruction does not
   // need them): the splat's own loop, so the values are the same
   cudaStream_t s = c->stream;

@@ -151,11 +151,6 @@ struct pr_context {
   uint32_t band_Dc = 0;
   uint64_t band_nb = 0;
   int degree = 1;                 // node functions of the current state: 1 (the crate's) or 2
-  // degree 2: the dense normal field "d2_nf" at address nf_clean (depth nf_clean_D) is zero except
-  // at the nf_dirty_T nodes of the last splat (its run keys "d2s_runkey"); nullptr: unknown
-  const void* nf_clean = nullptr;
-  uint32_t nf_clean_D = 0;
-  uint64_t nf_dirty_T = 0;
   // degree 2: the solved coefficients in natural order (one of the solver's buffers) and whether
   // their Morton copy "x64" is up to date (made on demand by coeffs_morton)
   const double* d2_xnat = nullptr;
@@ -181,7 +176,6 @@ struct pr_context {
     pr::DBuf& b = bufs[name];
     if (b.cap < bytes) {
       if (b.ptr) {
-        if (b.ptr == nf_clean) nf_clean = nullptr;
         PR_CUDA(cudaStreamSynchronize(stream));
         PR_CUDA(cudaFree(b.ptr));
         bytes_held -= b.cap;
@@ -211,7 +205,6 @@ struct pr_context {
   void release(const std::string& name) {
     auto it = bufs.find(name);
     if (it == bufs.end() || !it->second.ptr) return;
-    if (it->second.ptr == nf_clean) nf_clean = nullptr;
     PR_CUDA(cudaStreamSynchronize(stream));
     PR_CUDA(cudaFree(it->second.ptr));
     bytes_held -= it->second.cap;

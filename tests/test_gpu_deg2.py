@@ -69,9 +69,9 @@ def test_setup(ctx, name, depth, pw):
 
 
 def test_setup_reuses_the_normal_field():
-    """A context that reconstructs again at the same depth zeroes only the nodes of its previous
-    splat: a second cloud (and the first one again, and a depth change) gets the same normal field
-    and right-hand side as a fresh context."""
+    """A context that reconstructs cloud after cloud (a second cloud, the first one again, a depth
+    change) gets the same normal field and right-hand side as the oracle each time: nothing of the
+    previous splat survives in the compact field or the brick-wise right-hand side."""
     with prb.Context(0) as c:
         for name, depth in [("torus", 6), ("ellipsoid", 6), ("sphere", 5), ("torus", 6), ("torus", 6)]:
             c.solve(cloud(name), params(depth, 4.0))
