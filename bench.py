@@ -784,13 +784,25 @@ def run_batch(a):
         conv = all(st.converged for _, st in out)
         del out
     t = statistics.mean(ms)
+    # per-cloud coefficient error of the mixed-precision solve against the FP64 solve (untimed)
+    errs = []
+    with prb.Context(0) as ctx:
+        for c_pts, c_par in zip(pts, params):
+            ctx.solve(c_pts, c_par)
+            xm = ctx.coefficients()
+            ctx.solve(c_pts, prb.ReconstructParams(depth=c_par.depth, point_weight=c_par.point_weight,
+                                                   precision=prb.PR_PRECISION_FP64))
+            x64 = ctx.coefficients()
+            errs.append(float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)))
     print(json.dumps({"metric": "batched reconstruction throughput", "value": a.batch / (t / 1000.0),
                       "unit": "clouds/s", "points_per_s": total / (t / 1000.0), "ms_per_batch": t,
                       "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "data": "synthetic",
                       "config": {"workload": "batch_%d" % a.batch, "clouds": a.batch, "points": total,
                                  "depths": {str(d): sum(1 for _, dd in clouds if dd == d) for d in (7, 8, 9)},
                                  "point_weight": 4.0, "concurrency": a.concurrency},
-                      "triangles": tris, "all_converged": conv}), flush=True)
+                      "triangles": tris, "all_converged": conv,
+                      "coef_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": statistics.median(errs)}}),
+          flush=True)
     return 0
 
 
