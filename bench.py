@@ -83,6 +83,8 @@ def parse():
                          "points, depth 8, the crate's cascade with cg_iters 8), end to end in both arms; 5: the "
                          "large workload (20M points, union of 32 spheres + 1%% outliers, adaptive depth 12)")
     ap.add_argument("--large-points", type=int, default=20_000_000, help="--config 5: cloud size")
+    ap.add_argument("--large-depth", type=int, default=12, help="--config 5: band depth")
+    ap.add_argument("--large-coarse", type=int, default=9, help="--config 5: coarse (dense) depth")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the coefficient / vertex error block")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload's timing")
     ap.add_argument("--only-device", action="store_true",
@@ -403,8 +405,8 @@ def run_ours_large(a):
     d_pts = torch.from_numpy(pts).to(dev)
     h_pts = torch.from_numpy(pts).pin_memory()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    params = prb.ReconstructParams(depth=12, coarse_depth=9, degree=2, point_weight=4.0, scale=1.1,
-                                   precision=prb.PR_PRECISION_MIXED, target_rel_residual=1e-6)
+    params = prb.ReconstructParams(depth=a.large_depth, coarse_depth=a.large_coarse, degree=2, point_weight=4.0,
+                                   scale=1.1, precision=prb.PR_PRECISION_MIXED, target_rel_residual=1e-6)
     params64 = dataclasses_replace(params, precision=prb.PR_PRECISION_FP64)
 
     def steps(par, k):
@@ -462,7 +464,8 @@ def run_ours_large(a):
         "unit": "points/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_mean,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 refinement",
         "data": "synthetic",
-        "config": {"workload": "union32_spheres_20m_depth12_adaptive", "points": P, "depth": 12, "coarse_depth": 9,
+        "config": {"workload": "union32_spheres_%dm_depth%d_adaptive" % (round(P / 1e6), a.large_depth), "points": P,
+                   "depth": a.large_depth, "coarse_depth": a.large_coarse,
                    "degree": 2, "point_weight": 4.0, "scale": 1.1, "target_rel_residual": 1e-6,
                    "l2": "flushed between steps (256 MiB)"},
         "bricks": int(len(codes)), "band_nodes": int(512 * len(codes)),
