@@ -388,6 +388,60 @@ constexpr size_t band_op_smem(bool gsrc) {
          (gsrc ? (size_t)(kProlongScratch(kOT) + kOT3) * sizeof(double) : 0);
 }
 
+// 12 values of a tile row from the band vector v: brick sl[0] at x = 6, 7, sl[1] at x = 0..7,
+// sl[2] at x = 0, 1 of the row at offset rowoff; zero for kSent
+template <typename T>
+__device__ __forceinline__ void ab_load_row(const T* __restrict__ v, const uint32_t* sl, int rowoff, T* out) {
+#pragma unroll
+  for (int k = 0; k < kOT; ++k) out[k] = T(0);
+  if (sl[0] != kSent) {
+    const T* p = v + (uint64_t)sl[0] * kBN + rowoff + 6;
+    out[0] = p[0];
+    out[1] = p[1];
+  }
+  if (sl[1] != kSent) {
+    const T* p = v + (uint64_t)sl[1] * kBN + rowoff;
+    if (sizeof(T) == 4) {
+      const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 4);
+      out[2] = (T)a.x; out[3] = (T)a.y; out[4] = (T)a.z; out[5] = (T)a.w;
+      out[6] = (T)b.x; out[7] = (T)b.y; out[8] = (T)b.z; out[9] = (T)b.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {
+        const double2 a = *reinterpret_cast<const double2*>(p + k);
+        out[2 + k] = (T)a.x;
+        out[3 + k] = (T)a.y;
+      }
+    }
+  }
+  if (sl[2] != kSent) {
+    const T* p = v + (uint64_t)sl[2] * kBN + rowoff;
+    out[10] = p[0];
+    out[11] = p[1];
+  }
+}
+template <typename T>
+__device__ __forceinline__ void ab_store8(T* __restrict__ p, const T* v) {
+  if (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+    *reinterpret_cast<float4*>(p + 4) = make_float4((float)v[4], (float)v[5], (float)v[6], (float)v[7]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k += 2) *reinterpret_cast<double2*>(p + k) = make_double2((double)v[k], (double)v[k + 1]);
+  }
+}
+template <typename T>
+__device__ __forceinline__ void ab_store_tile_row(T* p, const T* v) {
+  if (sizeof(T) == 4) {
+#pragma unroll
+    for (int k = 0; k < kOT; k += 4)
+      *reinterpret_cast<float4*>(p + k) = make_float4((float)v[k], (float)v[k + 1], (float)v[k + 2], (float)v[k + 3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kOT; k += 2) *reinterpret_cast<double2*>(p + k) = make_double2((double)v[k], (double)v[k + 1]);
+  }
+}
+
 template <typename T, int MODE, bool GSRC>
 __global__ void __launch_bounds__(kOpThreads) k_ab_op(const T* __restrict__ x, const T* __restrict__ f,
                                                       T* __restrict__ y, T* __restrict__ dout, double beta,
@@ -416,26 +470,27 @@ __global__ void __launch_bounds__(kOpThreads) k_ab_op(const T* __restrict__ x, c
       double* gt = gs + kProlongScratch(kOT);
       prolong_tile<kOT>(xc, W, res, 8 * (int)bx - 2, 8 * (int)by - 2, 8 * (int)bz - 2, gs, gt);
       for (int i = t; i < kOT3; i += kOpThreads) tile[i] = (T)gt[i];
-    } else {
-      for (int i = t; i < kOT3; i += kOpThreads) {
-        const int lz = i / (kOT * kOT) - 2, ly = (i / kOT) % kOT - 2, lx = i % kOT - 2;
-        const int ox = lx < 0 ? -1 : (lx >= 8 ? 1 : 0), oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0),
-                  oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
-        const uint32_t s2 = nb[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
-        T v = T(0);
-        if (s2 != kSent) {
-          const uint64_t g = (uint64_t)s2 * kBN + (((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3) | (lx - 8 * ox));
-          if (MODE == kBandDir) {
-            v = beta != 0.0 ? f[g] + tb * x[g] : f[g];
-            if ((ox | oy | oz) == 0) dout[g] = v;
-          } else {
-            v = x[g];
-          }
+    } else if (t < kOT * kOT) {
+      // a thread per tile row (y, z): 2 values of the left neighbour brick (its x = 6, 7), 8 of the
+      // centre one, 2 of the right one (x = 0, 1), as vector loads
+      const int ly = t % kOT - 2, lz = t / kOT - 2;
+      const int oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0), oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
+      const int rowoff = ((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3);
+      const int kb = (oz + 1) * 9 + (oy + 1) * 3;
+      const uint32_t sl[3] = {nb[kb], nb[kb + 1], nb[kb + 2]};
+      T v[kOT];
+      ab_load_row<T>(MODE == kBandDir ? f : x, sl, rowoff, v);
+      if (MODE == kBandDir) {
+        if (beta != 0.0) {
+          T w[kOT];
+          ab_load_row<T>(x, sl, rowoff, w);
+#pragma unroll
+          for (int k = 0; k < kOT; ++k) v[k] += tb * w[k];
         }
-        tile[i] = v;
+        if (oy == 0 && oz == 0) ab_store8<T>(dout + slot * kBN + rowoff, v + 2);
       }
-    }
-    __syncthreads();
+      ab_store_tile_row<T>(tile + t * kOT, v);
+    }    __syncthreads();
     if (t < kOT * kOT) {  // z filter of column (x, y)
       T v[kOT];
 #pragma unroll
@@ -484,6 +539,7 @@ __global__ void __launch_bounds__(kOpThreads) k_ab_op(const T* __restrict__ x, c
         q[xx] = w23[(z * 8 + yy) * kWS + xx];
       }
       const uint64_t g0 = slot * kBN + (uint64_t)(z * 64 + yy * 8);
+      T dpart = T(0);  // this row's share of d . q (at most 8 terms, then accumulated in FP64)
 #pragma unroll
       for (int xx = 0; xx < 8; ++xx) {
         T acc = T(0);
@@ -492,10 +548,10 @@ __global__ void __launch_bounds__(kOpThreads) k_ab_op(const T* __restrict__ x, c
         const T ctr = tile[((z + 2) * kOT + yy + 2) * kOT + xx + 2];
         o[xx] = K.H * acc + K.wg * ctr;
         if (MODE == kBandResid) o[xx] = f[g0 + xx] - o[xx];
-        if (MODE == kBandDir) dacc += (double)ctr * (double)o[xx];
+        if (MODE == kBandDir) dpart += ctr * o[xx];
       }
-#pragma unroll
-      for (int xx = 0; xx < 8; ++xx) y[g0 + xx] = o[xx];
+      if (MODE == kBandDir) dacc += (double)dpart;
+      ab_store8<T>(y + g0, o);
     }
     __syncthreads();
   }
