@@ -244,8 +244,9 @@ int pr_reconstruct_batch(const double* const* points6, const uint64_t* n, uint32
  * the evaluation matrix) gives dL/dtheta = lambda . db/dtheta - lambda . (dA/dtheta) x through
  * the normalised splat (src/fem_tree.rs:130-178), the divergence RHS and the screening RHS and
  * matrix.  M follows the bounding box of the input and is HELD FIXED (not differentiated).
- * The basis is piecewise linear: at a point exactly on a cell face the one-sided derivative
- * of the cell the point falls in is returned. */
+ * Degree 1 (the crate's piecewise linear basis) and degree 2 (quadratic B-splines, the same
+ * formulas with 27 nodes per point); dense grids only (not the adaptive band).  At a point exactly
+ * on a cell face the one-sided derivative of the cell the point falls in is returned. */
 typedef struct pr_adjoint_stats {
   double loss;          /* sum_k g_k chi_k, or mean chi_k^2 when dl_dchi was NULL */
   double rel_residual;  /* adjoint solve ||E^T g - A lambda|| / ||E^T g|| */

@@ -407,6 +407,18 @@ class CG1(_CG):
         self._h = lib().orc_cg1_new(tree._h, float(pw), _ptr(_f64(b)))
 
 
+def loss2(pts6, queries3, depth, point_weight=4.0, scale=1.1, tol=1e-13):
+    """Degree-2 forward for finite differences: the unit-cube transform of the points, the
+    degree-2 system solved by CG to `tol`, L = mean over the queries (model space, mapped with
+    the same transform) of the degree-2 implicit function squared."""
+    unit, m = to_unit(pts6, scale)
+    x, _, _ = Tree2(depth, unit, point_weight).solve(tol=tol)
+    mm = np.asarray(m).reshape(4, 4).T
+    qu = np.asarray(queries3, dtype=np.float64) @ mm[:3, :3].T + mm[:3, 3]
+    chi = evaluate2(depth, x, qu)
+    return float(np.mean(chi ** 2))
+
+
 def extract_surface2(depth, sol, iso_value):
     m = OrcMesh()
     lib().orc_extract_surface2(int(depth), _ptr(_f64(sol)), float(iso_value), C.byref(m))

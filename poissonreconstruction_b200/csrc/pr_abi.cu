@@ -556,7 +556,6 @@ static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k
   PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
   PR_REQUIRE(c->coeffs_converged, PR_ERR_STATE,
              "the last solve used the reference schedule; the adjoint needs solve_mode PR_SOLVE_CONVERGED");
-  PR_REQUIRE(c->degree == 1, PR_ERR_STATE, "the adjoint is implemented for degree 1");
   for (uint64_t i = 0; i < 3 * k; ++i)
     PR_REQUIRE(std::isfinite(queries3[i]), PR_ERR_INVALID_ARGUMENT, "non-finite query coordinate");
   set_device(c);
@@ -572,7 +571,8 @@ static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k
   double* dchi = c->buf<double>("adj_chi", k);
   double* dpos = c->buf<double>("adj_dpos", 3 * c->P);
   double* dnrm = c->buf<double>("adj_dnrm", 3 * c->P);
-  pr::adjoint_backward(c, dq, k, ddl, dchi, dpos, dnrm, st);
+  if (c->degree == 2) pr::adjoint_backward2(c, dq, k, ddl, dchi, dpos, dnrm, st);
+  else pr::adjoint_backward(c, dq, k, ddl, dchi, dpos, dnrm, st);
   if (chi) PR_CUDA(cudaMemcpyAsync(chi, dchi, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (dl_dpositions)
     PR_CUDA(cudaMemcpyAsync(dl_dpositions, dpos, 3 * c->P * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -602,7 +602,6 @@ int pr_loss_backward(const double* points6, uint64_t n, const pr_params* params,
     PR_REQUIRE(n >= 1 && points6 != nullptr, PR_ERR_INVALID_ARGUMENT, "the adjoint needs at least one point");
     PR_REQUIRE(params->solve_mode == PR_SOLVE_CONVERGED, PR_ERR_INVALID_ARGUMENT,
                "the adjoint needs solve_mode PR_SOLVE_CONVERGED");
-    PR_REQUIRE(degree_of(*params) == 1, PR_ERR_INVALID_ARGUMENT, "the adjoint is implemented for degree 1");
     if (!g_thread_ctx) {
       pr_context* c = nullptr;
       int rc = pr_context_create(0, nullptr, &c);

@@ -15,7 +15,8 @@
 // c with the unit-cube transform held fixed; nu = v/|v| with v = s n.
 //
 // Every sum has a fixed order (sort-based scatter for E^T g, per-point gathers with the
-// corner loop for the rest), so the result is deterministic.
+// corner loop for the rest), so the result is deterministic.  adjoint_backward2 is the same for
+// the quadratic node functions of pr_params.degree = 2.
 #include <cstring>
 
 #include "pr_internal.cuh"
@@ -262,7 +263,278 @@ __global__ void k_point_grad(PointGradArgs a) {
   }
 }
 
+// ------------------------------------------------------------------ degree 2
+// The same adjoint for quadratic B-spline node functions (pr_params.degree = 2): the forward is
+// the degree-2 system (27 nodes per point for the splat and the screening, floor cells, the
+// divergence stencil h^2 (G M M) per component), its vectors in natural order.  With the 1-D
+// integrals m, g at offsets -2..2:
+//   mu_j^a = h^2 sum_d lambda_{j-d} W_a(d),  W_x(d) = g(dx) m(dy) m(dz) (permuted for y, z),
+// and the per-point formulas above with the degree-2 basis and its gradient.
+
+// degree-2 basis of one axis: nodes c-1, c, c+1 with values b and derivatives db (d/du)
+__device__ __forceinline__ void axis2_grad(double u, double h, int64_t& c, double* b, double* db) {
+  const double s = xdiv(u, h);
+  c = sat_i64(floor(s));
+  const double t = xsub(s, (double)c);
+  const double omt = xsub(1.0, t);
+  b[0] = xmul(xmul(0.5, omt), omt);
+  b[1] = xmul(0.5, xadd(xadd(xmul(xmul(-2.0, t), t), xmul(2.0, t)), 1.0));
+  b[2] = xmul(xmul(0.5, t), t);
+  const double ih = 1.0 / h;
+  db[0] = -omt * ih;
+  db[1] = (1.0 - 2.0 * t) * ih;
+  db[2] = t * ih;
+}
+
+// (node, 27 k + term) pairs of E^T for the degree-2 evaluation: natural node index, sentinel
+// 2^(3D) outside the grid
+__global__ void k_eval_pairs2(const double* __restrict__ qu, uint64_t K, uint32_t D, uint32_t* __restrict__ keys,
+                              uint32_t* __restrict__ vals) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  const uint32_t sentinel = 1u << (3 * D);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 27 * K; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = i / 27;
+    const int e = (int)(i - 27 * k), dx = e % 3, dy = (e / 3) % 3, dz = e / 9;
+    int64_t c[3];
+    double b[3], db[3];
+    axis2_grad(qu[3 * k], h, c[0], b, db);
+    axis2_grad(qu[3 * k + 1], h, c[1], b, db);
+    axis2_grad(qu[3 * k + 2], h, c[2], b, db);
+    const int64_t x = c[0] + dx - 1, y = c[1] + dy - 1, z = c[2] + dz - 1;
+    const bool ok = x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res;
+    keys[i] = ok ? (uint32_t)(x + res * (y + res * z)) : sentinel;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+// rhs[node] = sum over the node's (query, term) pairs in query order of g_k * basis value
+__global__ void k_eval_scatter2(const uint32_t* __restrict__ run_key, const uint32_t* __restrict__ run_off,
+                                uint64_t R, const uint32_t* __restrict__ sval, const double* __restrict__ qu,
+                                const double* __restrict__ g, uint32_t D, double* __restrict__ rhs) {
+  const double h = 1.0 / (double)(1u << D);
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < R; t += (uint64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (uint32_t e = run_off[t]; e < run_off[t + 1]; ++e) {
+      const uint32_t pk = sval[e];
+      const uint32_t k = pk / 27, term = pk % 27;
+      int64_t c;
+      double bx[3], by[3], bz[3], db[3];
+      axis2_grad(qu[3 * k], h, c, bx, db);
+      axis2_grad(qu[3 * k + 1], h, c, by, db);
+      axis2_grad(qu[3 * k + 2], h, c, bz, db);
+      acc = xadd(acc, xmul(g[k], xmul(xmul(bx[term % 3], by[(term / 3) % 3]), bz[term / 9])));
+    }
+    rhs[run_key[t]] = acc;
+  }
+}
+
+struct Deg2K {
+  double m[5], g[5];
+};
+// mu at the touched nodes (natural run keys), 3 x T
+__global__ void k_mu2(const uint32_t* __restrict__ run_key, uint64_t T, const double* __restrict__ lam, uint32_t D,
+                      Deg2K k, double* __restrict__ mu) {
+  const int res = 1 << D;
+  const double h = 1.0 / (double)res;
+  const double h2 = h * h;
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = run_key[t];
+    const int jx = (int)(j & (res - 1)), jy = (int)((j >> D) & (res - 1)), jz = (int)(j >> (2 * D));
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+    for (int dz = -2; dz <= 2; ++dz) {
+      const int iz = jz - dz;
+      if (iz < 0 || iz >= res) continue;
+      for (int dy = -2; dy <= 2; ++dy) {
+        const int iy = jy - dy;
+        if (iy < 0 || iy >= res) continue;
+        for (int dx = -2; dx <= 2; ++dx) {
+          const int ix = jx - dx;
+          if (ix < 0 || ix >= res) continue;
+          const double l = lam[(uint64_t)ix + (uint64_t)res * (iy + (uint64_t)res * iz)] * h2;
+          m0 += l * k.g[dx + 2] * k.m[dy + 2] * k.m[dz + 2];
+          m1 += l * k.m[dx + 2] * k.g[dy + 2] * k.m[dz + 2];
+          m2 += l * k.m[dx + 2] * k.m[dy + 2] * k.g[dz + 2];
+        }
+      }
+    }
+    mu[t] = m0;
+    mu[T + t] = m1;
+    mu[2 * T + t] = m2;
+  }
+}
+
+// per run: w = sum phi (point order, the splat's own sum) and runidx[pair] = run
+__global__ void k_run_weights2(const uint32_t* __restrict__ run_off, uint64_t T, const uint32_t* __restrict__ sval,
+                               const double* __restrict__ phi, double* __restrict__ w, uint32_t* __restrict__ runidx) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    double sw = 0.0;
+    for (uint32_t e = run_off[t]; e < run_off[t + 1]; ++e) {
+      sw = xadd(sw, phi[sval[e]]);
+      runidx[sval[e]] = (uint32_t)t;
+    }
+    w[t] = sw;
+  }
+}
+
+struct PointGrad2Args {
+  const double* upos;
+  const double* unrm;
+  const double* ulen;
+  uint64_t P;
+  uint32_t D;
+  const uint32_t* key;     // 27 P natural node keys (sentinel outside the grid)
+  const uint32_t* runidx;  // 27 P: the pair's run (touched node)
+  const double* nfc;       // 3 x T compact normal field
+  const double* w;         // T
+  const double* mu;        // 3 x T
+  uint64_t T;
+  const double* lam;  // n, natural
+  const double* x;    // n, natural
+  double wh3;
+  double s;
+  double* dpos;
+  double* dnrm;
+};
+
+__global__ void k_point_grad2(PointGrad2Args a) {
+  const double h = 1.0 / (double)(1u << a.D);
+  const uint32_t sentinel = 1u << (3 * a.D);
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < a.P; p += (uint64_t)gridDim.x * blockDim.x) {
+    const double nu[3] = {a.unrm[p], a.unrm[a.P + p], a.unrm[2 * a.P + p]};
+    int64_t c[3];
+    double b[3][3], db[3][3];
+    for (int k = 0; k < 3; ++k) axis2_grad(a.upos[(uint64_t)k * a.P + p], h, c[k], b[k], db[k]);
+    double gu[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
+    double Lv = 0.0, Xv = 0.0, gL[3] = {0.0, 0.0, 0.0}, gX[3] = {0.0, 0.0, 0.0};
+    for (int e = 0; e < 27; ++e) {
+      const uint32_t node = a.key[27 * p + e];
+      if (node == sentinel) continue;
+      const int ix = e % 3, iy = (e / 3) % 3, iz = e / 9;
+      const double phi = b[0][ix] * b[1][iy] * b[2][iz];
+      const double gp[3] = {db[0][ix] * b[1][iy] * b[2][iz], b[0][ix] * db[1][iy] * b[2][iz],
+                            b[0][ix] * b[1][iy] * db[2][iz]};
+      const uint32_t t = a.runidx[27 * p + e];
+      const double wt = a.w[t];
+      if (wt > 0.0) {  // splat
+        const double m[3] = {a.mu[t], a.mu[a.T + t], a.mu[2 * a.T + t]};
+        const double nf[3] = {a.nfc[t], a.nfc[a.T + t], a.nfc[2 * a.T + t]};
+        const double sdot = m[0] * (nu[0] + nf[0]) + m[1] * (nu[1] + nf[1]) + m[2] * (nu[2] + nf[2]);
+        for (int k = 0; k < 3; ++k) {
+          gn[k] -= phi / wt * m[k];
+          gu[k] -= gp[k] / wt * sdot;
+        }
+      }
+      if (a.wh3 > 0.0) {
+        const double lj = a.lam[node], xj = a.x[node];
+        Lv += phi * lj;
+        Xv += phi * xj;
+        for (int k = 0; k < 3; ++k) {
+          gL[k] += gp[k] * lj;
+          gX[k] += gp[k] * xj;
+        }
+      }
+    }
+    if (a.wh3 > 0.0)
+      for (int k = 0; k < 3; ++k) gu[k] += a.wh3 * 0.5 * gL[k] - a.wh3 * (gL[k] * Xv + Lv * gX[k]);
+    const double len = a.ulen[p];
+    const double ng = nu[0] * gn[0] + nu[1] * gn[1] + nu[2] * gn[2];
+    for (int k = 0; k < 3; ++k) {
+      a.dpos[3 * p + k] = a.s * gu[k];
+      a.dnrm[3 * p + k] = len > 0.0 ? a.s / len * (gn[k] - nu[k] * ng) : 0.0;
+    }
+  }
+}
+
 }  // namespace
+
+void adjoint_backward2(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
+                       double* d_dpos, double* d_dnrm, pr_adjoint_stats& st) {
+  const uint32_t D = c->D;
+  const uint64_t n = c->n, P = c->P, T = c->T;
+  cudaStream_t s = c->stream;
+  Affine M;
+  for (int k = 0; k < 16; ++k) M.m[k] = c->M[k];
+  double* qu = c->buf<double>("adj_qu", 3 * K);
+  k_query_unit<<<grid_for(K), kThreads, 0, s>>>(d_q3, K, M, qu);
+  PR_CHECK_LAUNCH();
+  // the forward solution, kept apart from the solver's buffers the adjoint solve reuses
+  double* x = c->buf<double>("adj2_x", n);
+  PR_CUDA(cudaMemcpyAsync(x, c->d2_xnat, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  c->d2_xnat = x;
+  evaluate_points(c, D, x, qu, 3, K, d_chi, 3);
+  double* g = c->buf<double>("adj_g", K);
+  k_upstream<<<grid_for(K), kThreads, 0, s>>>(d_chi, d_dl, K, g);
+  PR_CHECK_LAUNCH();
+  st.loss = d_dl ? dot64(c, d_dl, d_chi, K) : dot64(c, d_chi, d_chi, K) / (double)K;
+
+  uint32_t* kin = c->buf<uint32_t>("adj_kin", 27 * K);
+  uint32_t* vin = c->buf<uint32_t>("adj_vin", 27 * K);
+  k_eval_pairs2<<<grid_for(27 * K), kThreads, 0, s>>>(qu, K, D, kin, vin);
+  PR_CHECK_LAUNCH();
+  const uint64_t R = sort_and_segment(c, "adjq", kin, vin, 27 * K, D);
+  double* rhs = c->buf<double>("adj_rhs", n);
+  PR_CUDA(cudaMemsetAsync(rhs, 0, n * sizeof(double), s));
+  if (R > 0) {
+    k_eval_scatter2<<<grid_for(R), kThreads, 0, s>>>(c->get<uint32_t>("adjq_runkey"), c->get<uint32_t>("adjq_runoff"),
+                                                      R, c->get<uint32_t>("adjq_val"), qu, g, D, rhs);
+    PR_CHECK_LAUNCH();
+  }
+  c->release("adj_kin");
+  c->release("adj_vin");
+
+  pr_stats sst;
+  std::memset(&sst, 0, sizeof(sst));
+  c->sync();
+  const double t0 = now_seconds();
+  solve_deg2(c, c->params, sst, rhs);
+  c->sync();
+  st.time_solve = now_seconds() - t0;
+  st.rel_residual = sst.rel_residual;
+  st.pcg_iterations = sst.pcg_iterations;
+  st.refinement_steps = sst.refinement_steps;
+  st.converged = sst.converged;
+  double* lam = c->buf<double>("adj_lambda", n);
+  PR_CUDA(cudaMemcpyAsync(lam, c->d2_xnat, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  c->d2_xnat = x;  // the context keeps the forward solution
+  c->x64_ready = false;
+
+  double* mu = c->buf<double>("adj_mu", 3 * std::max<uint64_t>(T, 1));
+  double* w = c->buf<double>("adj_w", std::max<uint64_t>(T, 1));
+  uint32_t* runidx = c->buf<uint32_t>("adj_runidx", 27 * P);
+  if (T > 0) {
+    Deg2K k;
+    double s5[5];
+    deg2_constants(k.m, s5, k.g);
+    k_mu2<<<grid_for(T), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runkey"), T, lam, D, k, mu);
+    PR_CHECK_LAUNCH();
+    k_run_weights2<<<grid_for(T), kThreads, 0, s>>>(c->get<uint32_t>("d2s_runoff"), T, c->get<uint32_t>("d2s_val"),
+                                                      c->get<double>("d2_phi64"), w, runidx);
+    PR_CHECK_LAUNCH();
+  }
+  const double h = 1.0 / (double)(1u << D);
+  PointGrad2Args a;
+  a.upos = c->get<double>("upos");
+  a.unrm = c->get<double>("unrm");
+  a.ulen = c->get<double>("ulen");
+  a.P = P;
+  a.D = D;
+  a.key = c->get<uint32_t>("d2_kin");
+  a.runidx = runidx;
+  a.nfc = c->get<double>("d2_nfc");
+  a.w = w;
+  a.mu = mu;
+  a.T = T;
+  a.lam = lam;
+  a.x = x;
+  a.wh3 = c->pw > 0.0 ? c->pw * (h * h * h) / 1.5 : 0.0;
+  a.s = c->M[0];
+  a.dpos = d_dpos;
+  a.dnrm = d_dnrm;
+  k_point_grad2<<<grid_for(P), kThreads, 0, s>>>(a);
+  PR_CHECK_LAUNCH();
+  c->release("adj_runidx");
+}
 
 // d_q3: K model-space queries (device); d_dl: K upstream gradients or nullptr (mean chi^2);
 // outputs on the device: d_chi (K), d_dpos and d_dnrm (P x 3).

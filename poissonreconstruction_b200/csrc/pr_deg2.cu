@@ -2493,10 +2493,15 @@ void stage_setup_deg2(pr_context* c, uint32_t D, double pw) {
 
 // Solve of the degree-2 system; fills "d2_x" (natural order) and "x64" (Morton order).
 void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st) {
+  solve_deg2(c, p, st, c->get<double>("d2_b"));
+}
+
+// A x = b with the degree-2 system of the context (b natural order, any right-hand side); the
+// solution is left at c->d2_xnat (one of the solver's buffers)
+void solve_deg2(pr_context* c, const pr_params& p, pr_stats& st, const double* b) {
   const uint32_t D = c->D;
   const uint64_t n = c->n;
   cudaStream_t s = c->stream;
-  const double* b = c->get<double>("d2_b");
   double* x = c->buf<double>("d2_x", n);
   double* r = c->buf<double>("d2_r", n);
   const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;

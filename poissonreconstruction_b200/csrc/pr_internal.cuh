@@ -231,6 +231,11 @@ void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double*
 // degree 2 (pr_deg2.cu): natural-order system, solve, accessors in Morton order
 void stage_setup_deg2(pr_context* c, uint32_t depth, double pw);
 void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st);
+// A x = b with the degree-2 system of the context (natural order); the solution at c->d2_xnat
+void solve_deg2(pr_context* c, const pr_params& p, pr_stats& st, const double* b);
+// adjoint of a degree-2 reconstruction (pr_adjoint.cu): as adjoint_backward, natural-order state
+void adjoint_backward2(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
+                       double* d_dpos, double* d_dnrm, pr_adjoint_stats& st);
 void deg2_rhs_morton(pr_context* c, double* d_out);
 void deg2_normal_field_morton(pr_context* c, double* d_nf3, double* d_w);
 template <typename T>
@@ -254,6 +259,7 @@ const double* coeffs_morton(pr_context* c);
 double stage_iso(pr_context* c, const double* d_x64, bool natural = false);
 void stage_extract(pr_context* c, uint32_t depth, const double* d_x64, double iso, bool back_transform,
                    int degree = 1, bool natural = false);
+// degree 1 (the crate's basis), 2 (quadratic, Morton order) or 3 (quadratic, natural order)
 void evaluate_points(pr_context* c, uint32_t depth, const double* d_x64, const double* d_pts, uint64_t stride,
                      uint64_t n, double* d_out, int degree = 1);
 

@@ -652,7 +652,8 @@ struct MaxOp {
 void evaluate_points(pr_context* c, uint32_t D, const double* d_x64, const double* d_pts, uint64_t stride,
                      uint64_t n, double* d_out, int degree) {
   if (n == 0) return;
-  if (degree == 2) k_eval_points<2><<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
+  if (degree == 3) k_eval_points<3><<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
+  else if (degree == 2) k_eval_points<2><<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
   else k_eval_points<1><<<grid_for(n), kThreads, 0, c->stream>>>(d_x64, D, d_pts, stride, 1, n, d_out);
   PR_CHECK_LAUNCH();
 }

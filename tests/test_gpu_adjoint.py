@@ -208,3 +208,74 @@ def test_adjoint_superquadric_depth9_full_size(ctx, capsys):
               % (max(errs), float(np.median(errs)), _rel(dp, dp64), _rel(dn, dn64), 1000 * st.time_solve,
                  1000 * st.time_total))
     assert max(errs) <= 1e-4, errs
+
+
+# ---------------------------------------------------------------- degree 2 (quadratic B-splines)
+def _params2(depth, fp64=True, target=1e-12):
+    return prb.ReconstructParams(depth=depth, point_weight=4.0, degree=2,
+                                 precision=prb.PR_PRECISION_FP64 if fp64 else prb.PR_PRECISION_MIXED,
+                                 target_rel_residual=target, max_iters=400)
+
+
+def test_adjoint_degree2_against_oracle_differences(ctx):
+    """Degree-2 gradients of the FP64 GPU adjoint against fourth-order central differences of the
+    oracle's own degree-2 forward (CG to 1e-13), at <= 1e-4 relative on coordinates whose gradient
+    is at least 5% of the largest of its kind; the loss value against the oracle's."""
+    D = 4
+    pts, q, rng = adjoint_case(P=1500, K=500, seed=21)
+    ctx.solve(pts, _params2(D, target=1e-13))
+    chi, dp, dn, st = ctx.loss_backward(q)
+    assert st.converged == 1
+    assert st.loss == pytest.approx(oracle.loss2(pts, q, D), rel=1e-9)
+    grads = np.hstack([dp, dn])
+    big = [np.abs(grads[:, :3]).max(), np.abs(grads[:, 3:]).max()]
+    coords = [(i, c) for i, c in fd_coordinates(pts, D, rng, 400) if abs(grads[i, c]) >= 0.05 * big[c // 3]][:12]
+    assert len(coords) >= 8
+    for i, col in coords:
+        fd = fd_gradient(lambda p: oracle.loss2(p, q, D), pts, i, col)
+        assert abs(fd - grads[i, col]) <= 1e-4 * abs(grads[i, col]), (i, col, fd, grads[i, col])
+
+
+def test_adjoint_degree2_gpu_differences_and_precision(ctx, capsys):
+    """Depth 7, 50k superquadric points, 10k queries: 16 central differences of the GPU's own
+    degree-2 forward (FP64 solves to 1e-13) at <= 1e-4 relative with no floor, the mixed-precision
+    gradient against the FP64 one (1e-4 relative L2), linearity in the upstream gradient, and the
+    context's forward solution left intact by the adjoint solve."""
+    D = 7
+    pts = synthetic.superquadric(50_000, seed=synthetic.SEED_BASE + 33)
+    q = synthetic.superquadric_queries(10_000, seed=synthetic.SEED_BASE + 133)
+    p = _params2(D, target=1e-13)
+    ctx.solve(pts, p)
+    x_before = ctx.coefficients()
+    _, dp64, dn64, st64 = ctx.loss_backward(q)
+    assert st64.converged == 1
+    assert np.array_equal(ctx.coefficients(), x_before)
+    rng = np.random.default_rng(77)
+    g1, g2 = rng.standard_normal(len(q)), rng.standard_normal(len(q))
+    _, a1, b1, _ = ctx.loss_backward(q, dl_dchi=g1)
+    _, a2, b2, _ = ctx.loss_backward(q, dl_dchi=g2)
+    _, a12, b12, _ = ctx.loss_backward(q, dl_dchi=2.0 * g1 - g2)
+    assert _rel(a12, 2.0 * a1 - a2) <= 1e-9 and _rel(b12, 2.0 * b1 - b2) <= 1e-9
+
+    def loss(points):
+        ctx.solve(points, p)
+        _, _, m = ctx.info()
+        m = m.reshape(4, 4).T
+        chi = ctx.evaluate(q @ m[:3, :3].T + m[:3, 3])
+        return float(np.mean(chi ** 2))
+
+    grads = np.hstack([dp64, dn64])
+    big = [np.abs(grads[:, :3]).max(), np.abs(grads[:, 3:]).max()]
+    coords = [(i, c) for i, c in fd_coordinates(pts, D, rng, 4000) if abs(grads[i, c]) >= 0.1 * big[c // 3]]
+    coords = [coords[k] for k in rng.choice(len(coords), min(16, len(coords)), replace=False)]
+    errs = []
+    for i, col in coords:
+        fd = fd_gradient(loss, pts, i, col)
+        errs.append(abs(fd - grads[i, col]) / abs(grads[i, col]))
+    ctx.solve(pts, _params2(D, fp64=False, target=1e-6))
+    _, dp, dn, st = ctx.loss_backward(q)
+    with capsys.disabled():
+        print("\ndegree-2 adjoint, depth 7: %d central differences, max relative error %.2e; mixed vs FP64 %.2e / %.2e"
+              % (len(errs), max(errs), _rel(dp, dp64), _rel(dn, dn64)))
+    assert len(errs) >= 8 and max(errs) <= 1e-4, errs
+    assert st.converged == 1 and _rel(dp, dp64) <= 1e-4 and _rel(dn, dn64) <= 1e-4
