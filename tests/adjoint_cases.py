@@ -16,8 +16,9 @@ def adjoint_case(P=600, K=300, seed=5):
 
 
 def fd_coordinates(pts, depth, rng, count, scale=1.1, eps=1e-4):
-    """(point, column) pairs for central differences: positions off the bbox extremes and
-    with +-2 eps inside one cell of the grid; normals anywhere."""
+    """(point, column) pairs for central differences: positions more than 4 eps inside the bbox
+    (a step of 2 eps must not make the point a new extreme, which would move the unit-cube
+    transform) and with +-2 eps inside one cell of the grid; normals anywhere."""
     pos = pts[:, :3]
     lo, hi = pos.min(0), pos.max(0)
     s = scale / (hi - lo).max()
@@ -26,7 +27,7 @@ def fd_coordinates(pts, depth, rng, count, scale=1.1, eps=1e-4):
     while len(out) < count:
         i, a, kind = int(rng.integers(len(pts))), int(rng.integers(3)), int(rng.integers(2))
         if kind == 0:
-            if pos[i, a] in (lo[a], hi[a]):
+            if pos[i, a] - lo[a] <= 4 * eps or hi[a] - pos[i, a] <= 4 * eps:
                 continue
             u = (pos[i, a] - (lo[a] + hi[a]) / 2) * s + 0.5
             if np.floor((u - 2 * s * eps) / h) != np.floor((u + 2 * s * eps) / h):
