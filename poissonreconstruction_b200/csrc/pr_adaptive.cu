@@ -568,196 +568,6 @@ __global__ void __launch_bounds__(kOpThreads) k_ab_op(const T* __restrict__ x, c
   }
 }
 
-// The CG direction step (kBandDir) with the next brick's tiles prefetched: a row thread issues
-// cp.async copies of its tile row of z and dold for brick i + 1 (zero fill where the neighbour
-// brick is not active) before the CTA filters brick i, so the gather's latency hides behind the
-// filter passes.  Two stages of the two raw tiles; the neighbour slots of the brick after next
-// are loaded into registers one iteration ahead.  Same arithmetic and outputs as
-// k_ab_op<T, kBandDir, false>.
-// raw tile rows are padded to 16 values, tile x at column x + 2, so that the centre brick's 8
-// values start on a 16-byte boundary (the copies' alignment) in both precisions
-constexpr int kPR = 16;
-constexpr int kRawTile = kOT * kOT * kPR;
-template <typename T>
-constexpr size_t band_dir_pipe_smem() {
-  return (size_t)(4 * kRawTile + 2 * 8 * kOT * kOT + 2 * 8 * 8 * kWS) * sizeof(T);
-}
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem, uint32_t bytes_valid, int size) {
-  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
-  if (size == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes_valid) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes_valid) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-// one tile row (12 values) of v into a padded raw row dst (tile x at dst[x + 2]): brick sl[0] at
-// x = 6, 7, sl[1] at x = 0..7, sl[2] at x = 0, 1 of the row at offset rowoff.  Every copy is
-// aligned: dst + 2 and dst + 14 on 8 bytes (16 in FP64), dst + 4 on 16 bytes; the sources at
-// offsets 6, 0, 4 of 32-byte rows.
-template <typename T>
-__device__ __forceinline__ void ab_issue_row(T* dst, const T* __restrict__ v, const uint32_t* sl, int rowoff) {
-  const T* base = v;  // a valid address for the zero-filled copies
-  const uint32_t ok0 = sl[0] != kSent, ok1 = sl[1] != kSent, ok2 = sl[2] != kSent;
-  const T* p0 = ok0 ? v + (uint64_t)sl[0] * kBN + rowoff + 6 : base;
-  const T* p1 = ok1 ? v + (uint64_t)sl[1] * kBN + rowoff : base;
-  const T* p2 = ok2 ? v + (uint64_t)sl[2] * kBN + rowoff : base;
-  cp_async(dst + 2, p0, ok0 ? 2 * sizeof(T) : 0u, 2 * sizeof(T));
-  if (sizeof(T) == 4) {
-    cp_async(dst + 4, p1, ok1 ? 16u : 0u, 16);
-    cp_async(dst + 8, p1 + 4, ok1 ? 16u : 0u, 16);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 8; k += 2) cp_async(dst + 4 + k, p1 + k, ok1 ? 16u : 0u, 16);
-  }
-  cp_async(dst + 12, p2, ok2 ? 2 * sizeof(T) : 0u, 2 * sizeof(T));
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kOpThreads) k_ab_dir_pipe(const T* __restrict__ dold, const T* __restrict__ z,
-                                                            T* __restrict__ q, T* __restrict__ dout, double beta,
-                                                            const uint32_t* __restrict__ nbr, uint64_t NB,
-                                                            BandCoef<T> K, double* __restrict__ part) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* rz = reinterpret_cast<T*>(smem_raw);  // [stage][z 12][y 12][16]: z, tile x at column x + 2
-  T* rd = rz + 2 * kRawTile;               // the same for dold
-  T* um = rd + 2 * kRawTile;
-  T* us = um + 8 * kOT * kOT;
-  T* w1 = us + 8 * kOT * kOT;
-  T* w23 = w1 + 8 * 8 * kWS;
-  __shared__ double red[kOpThreads / 32 + 1];
-  const int t = threadIdx.x;
-  const T tb = (T)beta;
-  const bool use_d = beta != 0.0;
-  // this thread's tile row (row threads t < 144)
-  const int ly = t % kOT - 2, lz = t / kOT - 2;
-  const int oy = ly < 0 ? -1 : (ly >= 8 ? 1 : 0), oz = lz < 0 ? -1 : (lz >= 8 ? 1 : 0);
-  const int rowoff = ((lz - 8 * oz) << 6) | ((ly - 8 * oy) << 3);
-  const int kb = (oz + 1) * 9 + (oy + 1) * 3;
-  const bool row_thread = t < kOT * kOT;
-  auto slots = [&](uint64_t sl, uint32_t* out) {
-    if (row_thread && sl < NB) {
-      out[0] = nbr[27 * sl + kb];
-      out[1] = nbr[27 * sl + kb + 1];
-      out[2] = nbr[27 * sl + kb + 2];
-    }
-  };
-  auto issue = [&](uint32_t* sl, int stage) {
-    if (!row_thread) return;
-    ab_issue_row<T>(rz + stage * kRawTile + t * kPR, z, sl, rowoff);
-    if (use_d) ab_issue_row<T>(rd + stage * kRawTile + t * kPR, dold, sl, rowoff);
-  };
-  const uint64_t G = gridDim.x;
-  uint32_t snext[3] = {kSent, kSent, kSent}, safter[3] = {kSent, kSent, kSent};
-  double dacc = 0.0;
-  uint64_t slot = blockIdx.x;
-  if (slot < NB) {
-    uint32_t s0[3] = {kSent, kSent, kSent};
-    slots(slot, s0);
-    issue(s0, 0);
-  }
-  cp_async_commit();
-  slots(slot + G, snext);
-  int it = 0;
-  for (; slot < NB; slot += G, ++it) {
-    const int st = it & 1;
-    if (slot + G < NB) issue(snext, st ^ 1);
-    cp_async_commit();
-    slots(slot + 2 * G, safter);
-    cp_async_wait1();
-    __syncthreads();
-    const T* tz = rz + st * kRawTile;
-    const T* td = rd + st * kRawTile;
-    if (row_thread && oy == 0 && oz == 0) {  // d of the brick's own rows
-      T v[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = use_d ? tz[t * kPR + 4 + k] + tb * td[t * kPR + 4 + k] : tz[t * kPR + 4 + k];
-      ab_store8<T>(dout + slot * kBN + rowoff, v);
-    }
-    if (t < kOT * kOT) {  // z filter of column (x, y) of d = z + beta dold
-      const int col = (t / kOT) * kPR + t % kOT + 2;  // row y, column x + 2 of plane 0
-      T v[kOT];
-#pragma unroll
-      for (int zz = 0; zz < kOT; ++zz)
-        v[zz] = use_d ? tz[zz * kOT * kPR + col] + tb * td[zz * kOT * kPR + col] : tz[zz * kOT * kPR + col];
-#pragma unroll
-      for (int zz = 0; zz < 8; ++zz) {
-        T am = T(0), as = T(0);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-          am += K.m[c] * v[zz + c];
-          as += K.s[c] * v[zz + c];
-        }
-        um[zz * kOT * kOT + t] = am;
-        us[zz * kOT * kOT + t] = as;
-      }
-    }
-    __syncthreads();
-    if (t < 8 * kOT) {  // y filter of column (x, z)
-      const int xx = t % kOT, zz = t / kOT;
-      T a[kOT], b[kOT];
-#pragma unroll
-      for (int yy = 0; yy < kOT; ++yy) {
-        a[yy] = um[(zz * kOT + yy) * kOT + xx];
-        b[yy] = us[(zz * kOT + yy) * kOT + xx];
-      }
-#pragma unroll
-      for (int yy = 0; yy < 8; ++yy) {
-        T a1 = T(0), a2 = T(0), a3 = T(0);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-          a1 += K.m[c] * a[yy + c];
-          a2 += K.s[c] * a[yy + c];
-          a3 += K.m[c] * b[yy + c];
-        }
-        w1[(zz * 8 + yy) * kWS + xx] = a1;
-        w23[(zz * 8 + yy) * kWS + xx] = a2 + a3;
-      }
-    }
-    __syncthreads();
-    if (t < 64) {  // x filter of row (y, z), 8 outputs
-      const int yy = t % 8, zz = t / 8;
-      T p[kOT], qq[kOT], o[8];
-#pragma unroll
-      for (int xx = 0; xx < kOT; ++xx) {
-        p[xx] = w1[(zz * 8 + yy) * kWS + xx];
-        qq[xx] = w23[(zz * 8 + yy) * kWS + xx];
-      }
-      const uint64_t g0 = slot * kBN + (uint64_t)(zz * 64 + yy * 8);
-      const int ci = ((zz + 2) * kOT + yy + 2) * kPR + 4;  // tile x = 2 of row (yy + 2, zz + 2)
-      T dpart = T(0);
-#pragma unroll
-      for (int xx = 0; xx < 8; ++xx) {
-        T acc = T(0);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) acc += K.s[c] * p[xx + c] + K.m[c] * qq[xx + c];
-        const T ctr = use_d ? tz[ci + xx] + tb * td[ci + xx] : tz[ci + xx];
-        o[xx] = K.H * acc + K.wg * ctr;
-        dpart += ctr * o[xx];
-      }
-      dacc += (double)dpart;
-      ab_store8<T>(q + g0, o);
-    }
-    __syncthreads();  // the stage is read: the next iteration's copies may overwrite it
-#pragma unroll
-    for (int k = 0; k < 3; ++k) snext[k] = safter[k];
-  }
-  cp_async_commit();
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  if (part) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) dacc += __shfl_down_sync(0xffffffffu, dacc, off);
-    if ((t & 31) == 0) red[t >> 5] = dacc;
-    __syncthreads();
-    if (t == 0) {
-      double sum = 0.0;
-      for (int w = 0; w < kOpThreads / 32; ++w) sum += red[w];
-      part[blockIdx.x] = sum;
-    }
-  }
-}
-
 // screening: proj_p = sum_k phi x[key]; y[node] += sgn wh3 sum phi proj over the node's pairs;
 // sq (optional): per-block sums of proj^2 (x . wh3 Phi Phi^T x = wh3 sum_p proj_p^2)
 template <typename T>
@@ -1217,15 +1027,6 @@ struct Band {
     PR_CHECK_LAUNCH();
   }
   unsigned grid_op() const { return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(NB, 148 * 16)); }
-  // dn = z + beta d, q = A dn (stiffness and shift) with per-CTA partials of dn . q
-  template <typename T>
-  void launch_dir(const T* d, const T* z, T* q, T* dn, double beta, double* part) {
-    const size_t sm = band_dir_pipe_smem<T>();
-    allow_smem(k_ab_dir_pipe<T>, sm);
-    k_ab_dir_pipe<T><<<grid_op(), kOpThreads, sm, c->stream>>>(d, z, q, dn, beta, nbr, NB, band_coef<T>(c->D, c->pw),
-                                                               part);
-    PR_CHECK_LAUNCH();
-  }
   // y += sign wh3 Phi Phi^T x; sq: per-block sums of proj^2 (returns their count)
   template <typename T>
   int screen(const T* x, T* y, double sign, double* sq) {
@@ -1292,7 +1093,7 @@ int band_pcg(Band& B, T* r, T* x, double tol, int maxit) {
   while (std::sqrt(rr) > tol && it < maxit) {
     // dn = z + beta d, q = A dn (beta = 0 on the first pass: d is not read)
     const int nop = (int)B.grid_op();
-    B.launch_dir(d, z, q, dn, beta, part);
+    B.launch_op<T, kBandDir, false>(d, z, q, dn, beta, part);
     std::swap(d, dn);
     const int nsq = B.screen<T>(d, q, 1.0, part2);
     k_ab_sum_parts<<<1, 32, 0, s>>>(part, nop, 1, 1.0, sums);
