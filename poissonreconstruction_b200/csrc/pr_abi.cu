@@ -6,6 +6,7 @@
 //   marching cubes (stage_iso / stage_extract), back-transform of the vertices.
 // Every entry point converts exceptions into a status code and a thread-local message.
 #include <sys/mman.h>
+#include <unistd.h>
 
 #include <atomic>
 #include <unordered_map>
@@ -18,6 +19,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 #include <algorithm>
 
@@ -92,8 +94,11 @@ void set_device(pr_context* c) { PR_CUDA(cudaSetDevice(c->device)); }
 
 // Pool of pinned host blocks for returned meshes.  A mesh copied into pinned memory needs one
 // DMA and no host copy; pinning fresh memory is slow, so blocks released by pr_mesh_free /
-// pr_host_free are kept (up to PR_HOST_POOL_MB, default 4096; 0 disables the pool) and
-// handed out again to later meshes of a similar size.  Blocks stay pinned until exit.
+// pr_host_free are kept (up to PR_HOST_POOL_MB; 0 disables the pool) and handed out again to
+// later meshes of a similar size.  Blocks stay pinned until exit.  The default keeps up to an
+// eighth of the physical memory, between 4 and 32 GiB: a batch of a few hundred clouds returns
+// several GiB of meshes, and a pool smaller than one batch's output re-pins (and unpins, both
+// device-synchronising) the difference on every batch.
 struct HostPool {
   std::mutex mu;
   std::multimap<size_t, void*> idle;        // capacity -> block
@@ -102,7 +107,13 @@ struct HostPool {
   size_t limit = 0;
   HostPool() {
     const char* e = std::getenv("PR_HOST_POOL_MB");
-    limit = (size_t)(e ? std::strtoull(e, nullptr, 10) : 4096ull) << 20;
+    if (e) {
+      limit = (size_t)std::strtoull(e, nullptr, 10) << 20;
+    } else {
+      const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
+      const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : 0;
+      limit = std::min(std::max(phys / 8, size_t(4) << 30), size_t(32) << 30);
+    }
   }
 };
 HostPool& host_pool() {
@@ -267,6 +278,19 @@ void copy_mesh_to_host(pr_context* c, pr_mesh* out) {
   out->triangles = reinterpret_cast<uint64_t*>(ot);
 }
 
+void pipeline_setup(pr_context* c, const pr_params& p, pr_stats& st, double t1);
+void pipeline_extract(pr_context* c, const pr_params& p, uint64_t n, pr_stats& st, double t3);
+
+void reset_state(pr_context* c) {
+  c->have_state = false;
+  c->have_mesh = false;
+  c->have_coeffs = false;
+  c->coeffs_converged = false;
+  c->have_ref_coarse = false;
+  c->adaptive = false;
+  c->nv = c->nt = 0;
+}
+
 // The pipeline on device-resident points (c->buf "pts6" or caller memory).
 void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_params& p, pr_stats& st, double t_start,
                   bool extract = true) {
@@ -289,15 +313,8 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
                    st.rel_residual, st.iso_value, (unsigned long long)c->nv, (unsigned long long)c->nt);
     return;
   }
-  if (c->degree == 2) pr::stage_setup_deg2(c, p.depth, p.point_weight);
-  else pr::stage_splat_rhs(c, p.depth, p.point_weight);
-  c->sync();
-  double t2 = now_s();
-  st.time_tree = t2 - t1;  // tree (implicit) + splat + RHS + screening payload
-  st.time_system = 0.0;
-  st.fem_nodes = c->n;
-  st.points_in_cube = c->P_in;
-  c->params = p;
+  pipeline_setup(c, p, st, t1);
+  const double t2 = now_s();
   if (c->degree == 2) pr::stage_solve_deg2(c, p, st);
   else if (p.solve_mode == PR_SOLVE_REFERENCE_SCHEDULE) pr::stage_solve_reference(c, p, st);
   else pr::stage_solve(c, p, st);
@@ -307,6 +324,24 @@ void run_pipeline(pr_context* c, const double* d_pts6, uint64_t n, const pr_para
   st.time_solve = t3 - t2;
   st.peak_device_bytes = (double)c->peak_bytes;
   if (!extract) return;
+  pipeline_extract(c, p, n, st, t3);
+}
+
+// Tree, splat, right-hand side and screening payload of the dense grid (after the transform).
+void pipeline_setup(pr_context* c, const pr_params& p, pr_stats& st, double t1) {
+  if (c->degree == 2) pr::stage_setup_deg2(c, p.depth, p.point_weight);
+  else pr::stage_splat_rhs(c, p.depth, p.point_weight);
+  c->sync();
+  const double t2 = now_s();
+  st.time_tree = t2 - t1;  // tree (implicit) + splat + RHS + screening payload
+  st.time_system = 0.0;
+  st.fem_nodes = c->n;
+  st.points_in_cube = c->P_in;
+  c->params = p;
+}
+
+// Iso value and marching cubes of the solved dense grid (t3: end of the solve).
+void pipeline_extract(pr_context* c, const pr_params& p, uint64_t n, pr_stats& st, double t3) {
   const bool nat = c->degree == 2;  // degree 2: straight from the solver's natural order
   const double* x = nat ? c->d2_xnat : c->get<double>("x64");
   double iso = pr::stage_iso(c, x, nat);
@@ -336,13 +371,7 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
   set_device(c);
   pr_stats st;
   std::memset(&st, 0, sizeof(st));
-  c->have_state = false;
-  c->have_mesh = false;
-  c->have_coeffs = false;
-  c->coeffs_converged = false;
-  c->have_ref_coarse = false;
-  c->adaptive = false;
-  c->nv = c->nt = 0;
+  reset_state(c);
   if (out_mesh) std::memset(out_mesh, 0, sizeof(*out_mesh));
   if (n == 0) {  // src/reconstructor.rs:28
     c->have_mesh = true;
@@ -366,6 +395,242 @@ void reconstruct_impl(pr_context* c, const double* points6, uint64_t n, const pr
 }
 
 thread_local std::unique_ptr<pr_context, int (*)(pr_context*)> g_thread_ctx(nullptr, pr_context_destroy);
+
+// ------------------------------------------------------------------ packed batches
+// Clouds of a batch that share the solver's parameters and a dense degree-1 grid of depth >= 5
+// (converged solve) are reconstructed in packs: each cloud is set up in a context of its own (host
+// threads, one stream each), the pack's systems are solved together (pr::solve_packed: one launch
+// per solver step for every cloud of the pack) and each cloud is extracted and copied out in its
+// context.  A pack takes as many clouds of one depth as the free device memory holds.  The
+// contexts are kept for later batches (one engine per device); their memory is given back when an
+// allocation elsewhere in the process fails (pr::release_cached_memory).
+thread_local bool t_in_batch = false;
+
+struct BatchEngine {
+  std::mutex mu;
+  int device = 0;
+  pr_context* solver = nullptr;
+  std::vector<pr_context*> cl;
+  pr_context* make() {
+    pr_context* c = nullptr;
+    const int rc = pr_context_create(device, nullptr, &c);
+    if (rc != PR_OK) throw pr::Error(rc, g_last_error);
+    return c;
+  }
+  void ensure(size_t k) {
+    if (!solver) solver = make();
+    while (cl.size() < k) cl.push_back(make());
+  }
+  size_t held() const {
+    size_t b = solver ? solver->bytes_held : 0;
+    for (const pr_context* c : cl) b += c->bytes_held;
+    return b;
+  }
+  void release() {
+    if (solver) pr_context_destroy(solver);
+    solver = nullptr;
+    for (pr_context* c : cl) pr_context_destroy(c);
+    cl.clear();
+  }
+};
+BatchEngine& batch_engine(int device) {
+  static std::mutex m;
+  static std::map<int, BatchEngine*>* engines = new std::map<int, BatchEngine*>();  // never destroyed
+  std::lock_guard<std::mutex> g(m);
+  BatchEngine*& e = (*engines)[device];
+  if (!e) {
+    e = new BatchEngine();
+    e->device = device;
+  }
+  return *e;
+}
+
+struct PackKey {
+  uint32_t depth, precision, max_iters, smooth_sweeps;
+  double pw, target, inner;
+  bool operator<(const PackKey& o) const {
+    return std::tie(depth, precision, max_iters, smooth_sweeps, pw, target, inner) <
+           std::tie(o.depth, o.precision, o.max_iters, o.smooth_sweeps, o.pw, o.target, o.inner);
+  }
+};
+PackKey pack_key(const pr_params& p) {
+  return PackKey{p.depth, (uint32_t)p.precision, p.max_iters, p.smooth_sweeps, p.point_weight, p.target_rel_residual,
+                 p.inner_rel_tol};
+}
+bool packable(const pr_params& p, const double* pts, uint64_t n) {
+  try {
+    validate(&p);
+  } catch (const pr::Error&) {
+    return false;  // reported by the single-cloud path
+  }
+  return pts != nullptr && n > 0 && n <= pr::kMaxPoints && degree_of(p) == 1 && p.coarse_depth == 0 &&
+         p.solve_mode == PR_SOLVE_CONVERGED && p.depth >= 5;
+}
+// device bytes of one cloud of a pack: its context (input, setup, solution, extraction) and its
+// share of the packed solve's vectors
+double pack_cloud_bytes(const pr_params& p, uint64_t P) {
+  const double nodes = std::ldexp(1.0, 3 * (int)p.depth), res2 = std::ldexp(1.0, 2 * (int)p.depth);
+  const double solver = (p.precision == PR_PRECISION_FP64 ? 96.0 : 64.0) * nodes;
+  return 20.0 * nodes + 800.0 * (double)P + 1000.0 * res2 + 64e6 + solver;
+}
+
+template <typename F>
+void parallel_for(size_t m, unsigned max_threads, F f) {
+  std::atomic<size_t> next{0};
+  auto w = [&] {
+    t_in_batch = true;
+    for (;;) {
+      const size_t j = next.fetch_add(1);
+      if (j >= m) return;
+      f(j);
+    }
+  };
+  const unsigned nt = (unsigned)std::max<size_t>(1, std::min<size_t>(m, max_threads));
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t) th.emplace_back(w);
+  w();
+  for (auto& t : th) t.join();
+}
+
+void run_pack(BatchEngine& E, const std::vector<uint32_t>& pk, const double* const* points6, const uint64_t* n,
+              const pr_params* params, pr_mesh* out_meshes, pr_stats* out_stats, std::vector<int>& status,
+              std::vector<std::string>& msgs) {
+  const size_t m = pk.size();
+  E.ensure(m);
+  std::vector<pr_stats> st(m);
+  std::vector<char> ok(m, 1);
+  const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  parallel_for(m, hw, [&](size_t j) {  // input, transform, tree, splat, right-hand side
+    const uint32_t i = pk[j];
+    pr_context* c = E.cl[j];
+    const int r = guard([&] {
+      const double ts = now_s();
+      set_device(c);
+      std::memset(&st[j], 0, sizeof(pr_stats));
+      reset_state(c);
+      double* dp = c->buf<double>("pts6", 6 * n[i]);
+      PR_CUDA(cudaMemcpyAsync(dp, points6[i], 6 * n[i] * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      pr::stage_transform(c, dp, n[i], params[i].scale);
+      c->sync();
+      const double t1 = now_s();
+      st[j].time_transform = t1 - ts;
+      c->degree = 1;
+      c->params = params[i];
+      pipeline_setup(c, params[i], st[j], t1);
+    });
+    if (r != PR_OK) {
+      status[i] = r;
+      msgs[i] = g_last_error;
+      ok[j] = 0;
+    }
+  });
+  std::vector<pr_context*> sc;
+  std::vector<size_t> idx;
+  for (size_t j = 0; j < m; ++j)
+    if (ok[j]) {
+      sc.push_back(E.cl[j]);
+      idx.push_back(j);
+    }
+  if (!sc.empty()) {  // the packed solve
+    std::vector<pr_stats> sst(sc.size());
+    for (size_t k = 0; k < sc.size(); ++k) sst[k] = st[idx[k]];
+    const double ts = now_s();
+    const int r = guard([&] {
+      set_device(E.solver);
+      pr::solve_packed(E.solver, sc, params[pk[idx[0]]], sst);
+    });
+    const double share = (now_s() - ts) / (double)sc.size();
+    for (size_t k = 0; k < sc.size(); ++k) {
+      const size_t j = idx[k];
+      if (r != PR_OK) {
+        status[pk[j]] = r;
+        msgs[pk[j]] = g_last_error;
+        ok[j] = 0;
+        continue;
+      }
+      st[j] = sst[k];
+      st[j].time_solve = share;  // the cloud's share of the packed solve
+      sc[k]->coeffs_converged = true;
+    }
+  }
+  parallel_for(m, hw, [&](size_t j) {  // iso value, marching cubes, mesh to host
+    if (!ok[j]) return;
+    const uint32_t i = pk[j];
+    pr_context* c = E.cl[j];
+    const int r = guard([&] {
+      set_device(c);
+      pipeline_extract(c, params[i], n[i], st[j], now_s());
+      const double tc = now_s();
+      copy_mesh_to_host(c, &out_meshes[i]);
+      st[j].time_mesh_copy = now_s() - tc;
+      c->have_mesh = true;
+      st[j].peak_device_bytes = (double)c->peak_bytes + (double)E.solver->peak_bytes / (double)m;
+      st[j].time_total = st[j].time_transform + st[j].time_tree + st[j].time_solve + st[j].time_extract +
+                         st[j].time_mesh_copy;
+    });
+    if (r != PR_OK) {
+      status[i] = r;
+      msgs[i] = g_last_error;
+    } else if (out_stats) {
+      out_stats[i] = st[j];
+    }
+  });
+}
+
+void run_packed(int device, const std::map<PackKey, std::vector<uint32_t>>& groups, const double* const* points6,
+                const uint64_t* n, const pr_params* params, pr_mesh* out_meshes, pr_stats* out_stats,
+                std::vector<int>& status, std::vector<std::string>& msgs) {
+  BatchEngine& E = batch_engine(device);
+  std::lock_guard<std::mutex> g(E.mu);
+  struct Flag {
+    Flag() { t_in_batch = true; }
+    ~Flag() { t_in_batch = false; }
+  } flag;
+  std::vector<std::vector<uint32_t>> order;
+  for (const auto& kv : groups) order.push_back(kv.second);
+  // deepest first: later packs reuse the buffers of earlier ones
+  std::stable_sort(order.begin(), order.end(), [&](const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) {
+    return params[a[0]].depth > params[b[0]].depth;
+  });
+  const char* lim = std::getenv("PR_PACK_MAX_CLOUDS");  // cap on the clouds of one pack (0: none)
+  const size_t max_clouds = lim ? (size_t)std::strtoull(lim, nullptr, 10) : 0;
+  for (std::vector<uint32_t> grp : order) {
+    std::stable_sort(grp.begin(), grp.end(), [&](uint32_t a, uint32_t b) { return n[a] > n[b]; });
+    size_t pos = 0;
+    while (pos < grp.size()) {
+      size_t free_b = 0, total_b = 0;
+      PR_CUDA(cudaSetDevice(device));
+      PR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      const double budget = (double)free_b + (double)E.held() - std::max(8e9, 0.05 * (double)total_b);
+      std::vector<uint32_t> pk;
+      double acc = 0.0;
+      while (pos < grp.size()) {
+        const double b = pack_cloud_bytes(params[grp[pos]], n[grp[pos]]);
+        if (!pk.empty() && (acc + b > budget || (max_clouds && pk.size() >= max_clouds))) break;
+        pk.push_back(grp[pos++]);
+        acc += b;
+      }
+      run_pack(E, pk, points6, n, params, out_meshes, out_stats, status, msgs);
+    }
+  }
+}
+
+}  // namespace
+
+namespace pr {
+bool release_cached_memory(int device) {
+  if (t_in_batch) return false;
+  BatchEngine& e = batch_engine(device);
+  std::unique_lock<std::mutex> g(e.mu, std::try_to_lock);
+  if (!g.owns_lock() || e.held() == 0) return false;
+  e.release();
+  cudaSetDevice(device);
+  return true;
+}
+}  // namespace pr
+
+namespace {
+
 
 }  // namespace
 
@@ -495,6 +760,7 @@ int pr_context_destroy(pr_context* c) {
       cudaEventDestroy(c->ev_join);
     }
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    if (c->h_pack) cudaFreeHost(c->h_pack);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -625,18 +891,25 @@ int pr_ctx_reconstruct_batch(pr_context* const* ctxs, uint32_t n_ctx, const doub
     for (uint32_t i = 0; i < n_ctx && count > 0; ++i) PR_REQUIRE(ctxs[i] != nullptr, PR_ERR_INVALID_ARGUMENT, "NULL context");
     for (uint32_t i = 0; i < count; ++i) std::memset(&out_meshes[i], 0, sizeof(pr_mesh));
     if (count == 0) return;
-    // largest clouds first, one host thread per context pulling the next cloud
-    std::vector<uint32_t> order(count);
-    for (uint32_t i = 0; i < count; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return n[a] > n[b]; });
     status.assign(count, PR_OK);
     msgs.assign(count, std::string());
+    // packs of clouds that share the solver's parameters; the others one per context
+    std::map<PackKey, std::vector<uint32_t>> groups;
+    std::vector<uint32_t> rest;
+    for (uint32_t i = 0; i < count; ++i) {
+      if (packable(params[i], points6[i], n[i])) groups[pack_key(params[i])].push_back(i);
+      else rest.push_back(i);
+    }
+    if (!groups.empty())
+      run_packed(ctxs[0]->device, groups, points6, n, params, out_meshes, out_stats, status, msgs);
+    // largest clouds first, one host thread per context pulling the next cloud
+    std::stable_sort(rest.begin(), rest.end(), [&](uint32_t a, uint32_t b) { return n[a] > n[b]; });
     std::atomic<uint32_t> next{0};
     auto worker = [&](uint32_t w) {
       for (;;) {
         const uint32_t k = next.fetch_add(1);
-        if (k >= count) return;
-        const uint32_t i = order[k];
+        if (k >= rest.size()) return;
+        const uint32_t i = rest[k];
         pr_stats st;
         const int r = pr_ctx_reconstruct(ctxs[w], points6[i], n[i], &params[i], &out_meshes[i], &st);
         status[i] = r;
@@ -644,10 +917,10 @@ int pr_ctx_reconstruct_batch(pr_context* const* ctxs, uint32_t n_ctx, const doub
         else if (out_stats) out_stats[i] = st;
       }
     };
-    const uint32_t nw = std::min(n_ctx, count);
+    const uint32_t nw = std::min<uint32_t>(n_ctx, (uint32_t)rest.size());
     std::vector<std::thread> th;
     for (uint32_t w = 1; w < nw; ++w) th.emplace_back(worker, w);
-    worker(0);
+    if (nw > 0) worker(0);
     for (auto& t : th) t.join();
   });
   if (out_status)

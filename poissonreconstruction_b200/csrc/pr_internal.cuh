@@ -82,6 +82,14 @@ __host__ __device__ __forceinline__ void unmorton3(uint32_t m, uint32_t& x, uint
   z = compact3(m >> 2);
 }
 
+// Packed launches over several clouds of one depth: cloud blockIdx.y owns the slice
+// [blockIdx.y * count, (blockIdx.y + 1) * count) of every vector (count = its per-cloud size), so
+// a kernel shifts its pointers once and then runs its single-cloud body.  A null pointer stays null.
+template <typename P>
+__device__ __forceinline__ P* cloud_slice(P* p, uint64_t count) {
+  return p ? p + (uint64_t)blockIdx.y * count : p;
+}
+
 // ------------------------------------------------------------------ exact FP64 (no contraction)
 // The crate (Rust) never fuses multiply-add; kernels that must match it bit for bit use
 // these round-to-nearest intrinsics, which the compiler never contracts.
@@ -109,6 +117,9 @@ struct DBuf {
   void* ptr = nullptr;
   size_t cap = 0;
 };
+// Frees the device memory the batch engine keeps between batches on `device` (pr_abi.cu); false
+// if it holds none or is running.  A failed allocation calls it once and retries.
+bool release_cached_memory(int device);
 
 }  // namespace pr
 
@@ -121,6 +132,19 @@ struct pr_context {
   size_t bytes_held = 0, peak_bytes = 0;
   // pinned scalar staging (dot products, counters)
   double* h_scalars = nullptr;  // 64 doubles
+  double* h_pack = nullptr;     // more of them for packed solves (grown on demand)
+  size_t h_pack_cap = 0;
+  double* pinned_scalars(size_t count) {
+    if (count <= 64) return h_scalars;
+    if (h_pack_cap < count) {
+      if (h_pack) PR_CUDA(cudaFreeHost(h_pack));
+      h_pack = nullptr;
+      h_pack_cap = 0;
+      PR_CUDA(cudaMallocHost(&h_pack, count * sizeof(double)));
+      h_pack_cap = count;
+    }
+    return h_pack;
+  }
   // pinned staging for device->host mesh copies (grown on demand)
   unsigned char* h_stage = nullptr;
   size_t h_stage_cap = 0;
@@ -184,6 +208,10 @@ struct pr_context {
       }
       size_t cap = (bytes + 255) & ~size_t(255);
       cudaError_t e = cudaMalloc(&b.ptr, cap);
+      if (e == cudaErrorMemoryAllocation && pr::release_cached_memory(device)) {
+        cudaGetLastError();
+        e = cudaMalloc(&b.ptr, cap);
+      }
       if (e != cudaSuccess) {
         cudaGetLastError();
         b.ptr = nullptr;
@@ -228,6 +256,12 @@ uint64_t sort_and_segment(pr_context* c, const std::string& tag, uint32_t* keys_
 void stage_solve(pr_context* c, const pr_params& p, pr_stats& st);
 // A x = b with the current system's operator (x = 0 initially; b, x: n doubles)
 void solve_system(pr_context* c, const pr_params& p, pr_stats& st, const double* b, double* x);
+// The degree-1 systems of several contexts (set up, one depth and screening weight, depth >= 5)
+// solved together, one launch per step for all of them, on the stream and buffers of `sc`; each
+// context's solution goes to its "x64" and its solve figures to st[k].  Bit-identical to
+// stage_solve on each context.
+void solve_packed(pr_context* sc, const std::vector<pr_context*>& clouds, const pr_params& p,
+                  std::vector<pr_stats>& st);
 // degree 2 (pr_deg2.cu): natural-order system, solve, accessors in Morton order
 void stage_setup_deg2(pr_context* c, uint32_t depth, double pw);
 void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st);

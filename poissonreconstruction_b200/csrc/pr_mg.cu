@@ -110,6 +110,14 @@ __global__ void __launch_bounds__(Geo<TB>::THREADS) k_smooth(uint32_t D, const T
   T* fs = tile + W * W * W;                  // N, colour-major: fs[col * C3 + lattice index]
   T* ctile = fs + N;                         // CW^3 (MODE 2)
   const int res = 1 << D;
+  {
+    const uint64_t nl = 1ull << (3 * D);
+    xi = cloud_slice(xi, nl);
+    xo = cloud_slice(xo, nl);
+    f = cloud_slice(f, nl);
+    ec = cloud_slice(ec, nl / 8);
+    part = cloud_slice(part, gridDim.x);
+  }
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * N;
   uint32_t bx, by, bz;
@@ -305,6 +313,14 @@ __global__ void __launch_bounds__(Geo<TB>::THREADS) k_spmv(uint32_t D, const T* 
   T* tile = reinterpret_cast<T*>(smem_raw);  // W^3 natural
   T* out = tile + W * W * W;                 // N, Morton-local
   const int res = 1 << D;
+  {
+    const uint64_t nl = 1ull << (3 * D);
+    z = cloud_slice(z, nl);
+    d = cloud_slice(d, nl);
+    dn = cloud_slice(dn, nl);
+    q = cloud_slice(q, nl);
+    part = cloud_slice(part, gridDim.x);
+  }
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * N;
   uint32_t bx, by, bz;
@@ -372,6 +388,12 @@ __global__ void __launch_bounds__(Geo<TB>::THREADS) k_resid_restrict(uint32_t D,
   T* et = reinterpret_cast<T*>(smem_raw);  // WE^3 natural, tile coordinate = local + 2
   T* rt = et + WE * WE * WE;               // WR^3 natural, coordinate = local + 1
   const int res = 1 << D;
+  {
+    const uint64_t nl = 1ull << (3 * D);
+    e = cloud_slice(e, nl);
+    f = cloud_slice(f, nl);
+    fc = cloud_slice(fc, nl / 8);
+  }
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * N;
   uint32_t bx, by, bz;
@@ -453,32 +475,13 @@ __global__ void __launch_bounds__(Geo<TB>::THREADS) k_resid_restrict(uint32_t D,
   }
 }
 
-// screening projection with the fused sum of squares: proj[p] = phi(p).x, part = sum proj^2
-template <typename T>
-__global__ void k_screen_project_sq(const uint32_t* __restrict__ key, const T* __restrict__ phi, uint64_t P,
-                                    uint32_t sentinel, const T* __restrict__ x, T* __restrict__ proj,
-                                    double* __restrict__ part) {
-  double acc = 0.0;
-  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x) {
-    T s = 0;
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-      const uint32_t key_ = key[8 * p + kk];
-      if (key_ != sentinel) s += phi[8 * p + kk] * x[key_];
-    }
-    proj[p] = s;
-    acc += (double)s * (double)s;
-  }
-  typedef cub::BlockReduce<double, 256> BR;
-  __shared__ typename BR::TempStorage tmp;
-  const double t = BR(tmp).Sum(acc);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
 // fixed-order sum of two partial arrays: out = sum(part) + scale2 * sum(part2)
 __global__ void __launch_bounds__(1024) k_sum_parts(const double* __restrict__ part, int np, double scale2,
                                                     const double* __restrict__ part2, int np2,
                                                     double* __restrict__ out) {
+  part += (uint64_t)blockIdx.x * np;  // block k: cloud k's partials (packed launches)
+  part2 += (uint64_t)blockIdx.x * np2;
+  out += blockIdx.x;
   double s = 0.0, s2 = 0.0;
   for (int i = threadIdx.x; i < np; i += 1024) s += part[i];
   for (int i = threadIdx.x; i < np2; i += 1024) s2 += part2[i];
@@ -720,14 +723,26 @@ __device__ __forceinline__ void plane_terms(const T r[4][4], T c0, T ce, T cc, T
 
 // KIND 0: q = A a, part = a.q;  1: an = bvec + beta a, q = A an, part = an.q;
 // 2: an = a + beta bvec (FP64 solution + correction of type E), q = rhs - A an.
+// beta_dev (packed launches): the cloud's beta, in place of the beta argument.
 template <typename T, int KIND, typename E>
 __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
     k_spmv16(uint32_t D, const T* __restrict__ a, const E* __restrict__ bvec, T* __restrict__ an, T beta,
-             T* __restrict__ q, T c0, T ce, T cc, const T* __restrict__ rhs, double* __restrict__ part) {
+             T* __restrict__ q, T c0, T ce, T cc, const T* __restrict__ rhs, double* __restrict__ part,
+             const double* __restrict__ beta_dev) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);
   __shared__ uint32_t nb[27];
   const int res = 1 << D;
+  {
+    const uint64_t nl = 1ull << (3 * D);
+    a = cloud_slice(a, nl);
+    bvec = cloud_slice(bvec, nl);
+    an = cloud_slice(an, nl);
+    q = cloud_slice(q, nl);
+    rhs = cloud_slice(rhs, nl);
+    part = cloud_slice(part, gridDim.x);
+    if (beta_dev) beta = (T)beta_dev[blockIdx.y];
+  }
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * N;
   uint32_t bx, by, bz;
@@ -737,7 +752,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
   auto val = [&](uint32_t m) -> T {
     if (KIND == 0) return __ldg(a + m);
     if (KIND == 1) return (T)__ldg(bvec + m) + beta * __ldg(a + m);
-    return __ldg(a + m) + beta * (T)__ldg(bvec + m);
+    // KIND 2 with beta 0: a cloud of a packed launch that has stopped keeps its solution
+    return beta == (T)0 ? __ldg(a + m) : __ldg(a + m) + beta * (T)__ldg(bvec + m);
   };
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -750,7 +766,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
       const typename s16::Vec4<E>::type bv = s16::ld4(bvec + m);
       if (KIND == 1) {
         v.x = (T)bv.x + beta * v.x; v.y = (T)bv.y + beta * v.y; v.z = (T)bv.z + beta * v.z; v.w = (T)bv.w + beta * v.w;
-      } else {
+      } else if (beta != (T)0) {
         v.x += beta * (T)bv.x; v.y += beta * (T)bv.y; v.z += beta * (T)bv.z; v.w += beta * (T)bv.w;
       }
       s16::st4(an + m, v);
@@ -837,6 +853,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   T* rt = et + n16::TILE;                  // RTILE
   __shared__ uint32_t nb[27];
   const int res = 1 << D;
+  {
+    const uint64_t nl = 1ull << (3 * D);
+    e = cloud_slice(e, nl);
+    f = cloud_slice(f, nl);
+    fc = cloud_slice(fc, nl / 8);
+    face = cloud_slice(face, (uint64_t)gridDim.x * FACE);
+  }
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * N;
   uint32_t bx, by, bz;
@@ -985,6 +1008,8 @@ template <typename T>
 __global__ void __launch_bounds__(768) k_restrict_faces(uint32_t D, const T* __restrict__ face, T* __restrict__ fc,
                                                        uint32_t nblk) {
   const int nba = 1 << (D - 4);
+  face = cloud_slice(face, (uint64_t)nblk * FACE);
+  fc = cloud_slice(fc, (uint64_t)nblk * 512);
   const uint32_t blk = blockIdx.x * 4 + threadIdx.x / 192;
   const int j = threadIdx.x % 192;
   if (blk >= nblk || j >= 169) return;
@@ -1132,6 +1157,21 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   T* ctile = tile + TILE;                    // CW^3 (MODE 2)
   __shared__ uint32_t nb[27], cnb[27];
   const int res = 1 << D;
+  {
+    const uint64_t nl = 1ull << (3 * D);
+    xi = cloud_slice(xi, nl);
+    xo = cloud_slice(xo, nl);
+    f = cloud_slice(f, nl);
+    ec = cloud_slice(ec, nl / 8);
+    part = cloud_slice(part, gridDim.x);
+    if (MODE == 3) {
+      cg.x = cloud_slice(cg.x, nl);
+      cg.d = cloud_slice(cg.d, nl);
+      cg.q = cloud_slice(cg.q, nl);
+      cg.r = cloud_slice(cg.r, nl);
+      if (cg.alpha_dev) cg.alpha = (T)cg.alpha_dev[blockIdx.y];
+    }
+  }
   const uint32_t blk = blockIdx.x;
   const uint64_t base = (uint64_t)blk * 4096;
   uint32_t bx, by, bz;
@@ -1154,13 +1194,15 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     typename s16::Vec4<T>::type fq;
     if (MODE == 3) {  // the CG update of this quad (plain loads: x and r are written here)
       typedef typename s16::Vec4<T>::type V4;
-      V4 xq = *reinterpret_cast<const V4*>(cg.x + m);
-      const V4 dq = s16::ld4(cg.d + m), qq = s16::ld4(cg.q + m);
       fq = *reinterpret_cast<const V4*>(cg.r + m);
-      xq.x += cg.alpha * dq.x; xq.y += cg.alpha * dq.y; xq.z += cg.alpha * dq.z; xq.w += cg.alpha * dq.w;
-      fq.x -= cg.alpha * qq.x; fq.y -= cg.alpha * qq.y; fq.z -= cg.alpha * qq.z; fq.w -= cg.alpha * qq.w;
-      s16::st4(cg.x + m, xq);
-      s16::st4(cg.r + m, fq);
+      if (cg.alpha != (T)0) {  // alpha 0: a cloud of a packed launch that has stopped keeps x and r
+        V4 xq = *reinterpret_cast<const V4*>(cg.x + m);
+        const V4 dq = s16::ld4(cg.d + m), qq = s16::ld4(cg.q + m);
+        xq.x += cg.alpha * dq.x; xq.y += cg.alpha * dq.y; xq.z += cg.alpha * dq.z; xq.w += cg.alpha * dq.w;
+        fq.x -= cg.alpha * qq.x; fq.y -= cg.alpha * qq.y; fq.z -= cg.alpha * qq.z; fq.w -= cg.alpha * qq.w;
+        s16::st4(cg.x + m, xq);
+        s16::st4(cg.r + m, fq);
+      }
       rr += (double)fq.x * fq.x + (double)fq.y * fq.y + (double)fq.z * fq.z + (double)fq.w * fq.w;
     } else {
       fq = s16::ld4(f + m);
@@ -1299,19 +1341,19 @@ inline int tile_for(uint32_t D) { return D >= 4 ? 16 : 8; }
 
 template <typename T, int TB, int MODE, bool DOT, bool FWD>
 void launch_smooth(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const DevCoef<T>& k,
-                   double* part) {
+                   double* part, uint32_t clouds) {
   using G = Geo<TB>;
   constexpr int CW = TB / 2 + 2;
   const size_t sm = sizeof(T) * (G::W * G::W * G::W + G::N + (MODE == 2 ? CW * CW * CW : 0));
   const unsigned nb = 1u << (3 * (D - (TB == 16 ? 4 : 3)));
   allow_smem(k_smooth<T, TB, MODE, DOT, FWD>, sm);
-  k_smooth<T, TB, MODE, DOT, FWD><<<nb, G::THREADS, sm, s>>>(D, xi, xo, f, ec, k, part);
+  k_smooth<T, TB, MODE, DOT, FWD><<<dim3(nb, clouds), G::THREADS, sm, s>>>(D, xi, xo, f, ec, k, part);
 }
 
 template <typename T, int TB>
 void smooth_dispatch(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const DevCoef<T>& k,
-                     int mode, bool forward, double* part) {
-#define PR_SM(M, DT, FW) launch_smooth<T, TB, M, DT, FW>(s, D, xi, xo, f, ec, k, part)
+                     int mode, bool forward, double* part, uint32_t clouds) {
+#define PR_SM(M, DT, FW) launch_smooth<T, TB, M, DT, FW>(s, D, xi, xo, f, ec, k, part, clouds)
   if (mode == 1) {
     if (forward) PR_SM(1, false, true);
     else PR_SM(1, false, false);
@@ -1337,24 +1379,24 @@ void smooth_dispatch(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f,
 
 template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
 void launch_s16(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const LevelCoef& L,
-                const T* table, double* part) {
+                const T* table, double* part, uint32_t clouds) {
   const size_t sm = g16::smem_bytes<T>(MODE);
   allow_smem(g16::k_smooth16<T, MODE, DOT, FWD, FACES>, sm);
-  g16::k_smooth16<T, MODE, DOT, FWD, FACES><<<1u << (3 * (D - 4)), g16::THREADS, sm, s>>>(
+  g16::k_smooth16<T, MODE, DOT, FWD, FACES><<<dim3(1u << (3 * (D - 4)), clouds), g16::THREADS, sm, s>>>(
       D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, CgFuse<T>());
 }
 
 template <typename T, int MODE, bool DOT, bool FWD>
 void launch_s16f(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const LevelCoef& L,
-                 const T* table, double* part) {
-  if (L.has_faces) launch_s16<T, MODE, DOT, FWD, true>(s, D, xi, xo, f, ec, L, table, part);
-  else launch_s16<T, MODE, DOT, FWD, false>(s, D, xi, xo, f, ec, L, table, part);
+                 const T* table, double* part, uint32_t clouds) {
+  if (L.has_faces) launch_s16<T, MODE, DOT, FWD, true>(s, D, xi, xo, f, ec, L, table, part, clouds);
+  else launch_s16<T, MODE, DOT, FWD, false>(s, D, xi, xo, f, ec, L, table, part, clouds);
 }
 
 template <typename T>
 void smooth16_dispatch(cudaStream_t s, const LevelCoef& L, uint32_t D, const T* xi, T* xo, const T* f, const T* ec,
-                       const T* table, int mode, bool forward, double* part) {
-#define PR_S16(M, DT, FW) launch_s16f<T, M, DT, FW>(s, D, xi, xo, f, ec, L, table, part)
+                       const T* table, int mode, bool forward, double* part, uint32_t clouds) {
+#define PR_S16(M, DT, FW) launch_s16f<T, M, DT, FW>(s, D, xi, xo, f, ec, L, table, part, clouds)
   if (mode == 1) {
     if (forward) PR_S16(1, false, true);
     else PR_S16(1, false, false);
@@ -1429,28 +1471,29 @@ LevelCoef level_coef(uint32_t D, uint32_t l, double shift_l) {
 
 template <typename T>
 void mg_smooth(cudaStream_t s, const LevelCoef& L, const T* table, const T* xi, T* xo, const T* f, const T* ec,
-               int mode, bool forward, double* part) {
+               int mode, bool forward, double* part, uint32_t clouds) {
   const uint32_t D = L.depth;
   const DevCoef<T> k = dev_coef<T>(L, table);
-  if (tile_for(D) == 16) smooth16_dispatch<T>(s, L, D, xi, xo, f, ec, table, mode, forward, part);
-  else smooth_dispatch<T, 8>(s, D, xi, xo, f, ec, k, mode, forward, part);
+  if (tile_for(D) == 16) smooth16_dispatch<T>(s, L, D, xi, xo, f, ec, table, mode, forward, part, clouds);
+  else smooth_dispatch<T, 8>(s, D, xi, xo, f, ec, k, mode, forward, part, clouds);
   PR_CHECK_LAUNCH();
 }
 
 template <typename T>
 void mg_cg_update_presmooth(cudaStream_t s, const LevelCoef& L, const T* table, const CgFuse<T>& cg, T* xo,
-                            double* part) {
+                            double* part, uint32_t clouds) {
   const uint32_t D = L.depth;
   if (D < 4 || L.has_faces) throw Error(PR_ERR_INTERNAL, "the fused CG update needs the finest level, depth >= 4");
   const size_t sm = g16::smem_bytes<T>(3);
   allow_smem(g16::k_smooth16<T, 3, false, true, false>, sm);
-  g16::k_smooth16<T, 3, false, true, false><<<1u << (3 * (D - 4)), g16::THREADS, sm, s>>>(
+  g16::k_smooth16<T, 3, false, true, false><<<dim3(1u << (3 * (D - 4)), clouds), g16::THREADS, sm, s>>>(
       D, nullptr, xo, nullptr, nullptr, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, cg);
   PR_CHECK_LAUNCH();
 }
 
 template <typename T>
-void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc, T* face) {
+void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const T* e, const T* f, T* fc, T* face,
+                       uint32_t clouds) {
   const uint32_t D = L.depth;
   const DevCoef<T> k = dev_coef<T>(L, table);
   if (tile_for(D) == 16) {
@@ -1458,17 +1501,19 @@ void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const
     const unsigned nb = 1u << (3 * (D - 4));
     if (L.has_faces) {
       allow_smem(r16::k_resid16<T, true>, sm);
-      r16::k_resid16<T, true><<<nb, r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce, (T)L.cc, table);
+      r16::k_resid16<T, true><<<dim3(nb, clouds), r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce,
+                                                                        (T)L.cc, table);
     } else {
       allow_smem(r16::k_resid16<T, false>, sm);
-      r16::k_resid16<T, false><<<nb, r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce, (T)L.cc, table);
+      r16::k_resid16<T, false><<<dim3(nb, clouds), r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce,
+                                                                         (T)L.cc, table);
     }
     PR_CHECK_LAUNCH();
-    r16::k_restrict_faces<T><<<(nb + 3) / 4, 768, 0, s>>>(D, face, fc, nb);
+    r16::k_restrict_faces<T><<<dim3((nb + 3) / 4, clouds), 768, 0, s>>>(D, face, fc, nb);
   } else {
     const size_t sm = sizeof(T) * (11 * 11 * 11 + 9 * 9 * 9);
     allow_smem(k_resid_restrict<T, 8>, sm);
-    k_resid_restrict<T, 8><<<1u << (3 * (D - 3)), Geo<8>::THREADS, sm, s>>>(D, e, f, fc, k);
+    k_resid_restrict<T, 8><<<dim3(1u << (3 * (D - 3)), clouds), Geo<8>::THREADS, sm, s>>>(D, e, f, fc, k);
   }
   PR_CHECK_LAUNCH();
 }
@@ -1477,23 +1522,24 @@ size_t mg_face_entries(uint32_t D) { return D >= 4 ? (size_t)r16::FACE << (3 * (
 
 template <typename T>
 void mg_spmv(cudaStream_t s, const LevelCoef& L, const T* table, const T* z, const T* d, T* dn, double beta,
-             bool xpby, T* q, double* part) {
+             bool xpby, T* q, double* part, uint32_t clouds, const double* beta_dev) {
   const uint32_t D = L.depth;
   const DevCoef<T> k = dev_coef<T>(L, table);
   if (L.has_faces) throw Error(PR_ERR_INTERNAL, "mg_spmv is for the finest level");
   if (tile_for(D) == 16) {
-    const unsigned nb = 1u << (3 * (D - 4));
+    const dim3 g(1u << (3 * (D - 4)), clouds);
     const size_t sm = n16::smem_bytes<T>();
     if (xpby) {
       allow_smem(n16::k_spmv16<T, 1, T>, sm);
-      n16::k_spmv16<T, 1, T><<<nb, n16::THREADS, sm, s>>>(D, d, z, dn, (T)beta, q, (T)L.c0, (T)L.ce, (T)L.cc,
-                                                          nullptr, part);
+      n16::k_spmv16<T, 1, T><<<g, n16::THREADS, sm, s>>>(D, d, z, dn, (T)beta, q, (T)L.c0, (T)L.ce, (T)L.cc,
+                                                         nullptr, part, beta_dev);
     } else {
       allow_smem(n16::k_spmv16<T, 0, T>, sm);
-      n16::k_spmv16<T, 0, T><<<nb, n16::THREADS, sm, s>>>(D, d, nullptr, nullptr, (T)0, q, (T)L.c0, (T)L.ce,
-                                                          (T)L.cc, nullptr, part);
+      n16::k_spmv16<T, 0, T><<<g, n16::THREADS, sm, s>>>(D, d, nullptr, nullptr, (T)0, q, (T)L.c0, (T)L.ce,
+                                                         (T)L.cc, nullptr, part, nullptr);
     }
   } else {
+    if (clouds != 1 || beta_dev) throw Error(PR_ERR_INTERNAL, "packed SpMV needs depth >= 4");
     const unsigned nb = 1u << (3 * (D - 3));
     const size_t sm = sizeof(T) * (10 * 10 * 10 + 512);
     if (xpby) k_spmv<T, 8, true><<<nb, Geo<8>::THREADS, sm, s>>>(D, z, d, dn, (T)beta, q, k, part);
@@ -1504,30 +1550,25 @@ void mg_spmv(cudaStream_t s, const LevelCoef& L, const T* table, const T* z, con
 
 template <typename E>
 void mg_resid_update(cudaStream_t s, const LevelCoef& L, const double* x, const E* e, double scale, double* xn,
-                     const double* b, double* r) {
+                     const double* b, double* r, uint32_t clouds, const double* scale_dev) {
   const uint32_t D = L.depth;
   if (D < 4 || L.has_faces) throw Error(PR_ERR_INTERNAL, "mg_resid_update needs the finest level, depth >= 4");
   const size_t sm = n16::smem_bytes<double>();
   allow_smem(n16::k_spmv16<double, 2, E>, sm);
-  n16::k_spmv16<double, 2, E><<<1u << (3 * (D - 4)), n16::THREADS, sm, s>>>(D, x, e, xn, scale, r, L.c0, L.ce, L.cc,
-                                                                            b, nullptr);
+  n16::k_spmv16<double, 2, E><<<dim3(1u << (3 * (D - 4)), clouds), n16::THREADS, sm, s>>>(
+      D, x, e, xn, scale, r, L.c0, L.ce, L.cc, b, nullptr, scale_dev);
   PR_CHECK_LAUNCH();
 }
 template void mg_resid_update<float>(cudaStream_t, const LevelCoef&, const double*, const float*, double, double*,
-                                     const double*, double*);
+                                     const double*, double*, uint32_t, const double*);
 template void mg_resid_update<double>(cudaStream_t, const LevelCoef&, const double*, const double*, double, double*,
-                                      const double*, double*);
+                                      const double*, double*, uint32_t, const double*);
 
 uint32_t mg_blocks(uint32_t D) { return tile_for(D) == 16 ? (1u << (3 * (D - 4))) : (1u << (3 * (D - 3))); }
 
-template <typename T>
-void screen_project_sq(cudaStream_t s, const Screen<T>& scr, const T* x, double* part, int nparts) {
-  k_screen_project_sq<T><<<nparts, 256, 0, s>>>(scr.key, scr.phi, scr.P, scr.sentinel, x, scr.proj, part);
-  PR_CHECK_LAUNCH();
-}
-
-void sum_parts(cudaStream_t s, const double* part, int np, double scale2, const double* part2, int np2, double* out) {
-  k_sum_parts<<<1, 1024, 0, s>>>(part, np, scale2, part2, np2, out);
+void sum_parts(cudaStream_t s, const double* part, int np, double scale2, const double* part2, int np2, double* out,
+               uint32_t clouds) {
+  k_sum_parts<<<clouds, 1024, 0, s>>>(part, np, scale2, part2, np2, out);
   PR_CHECK_LAUNCH();
 }
 
@@ -1629,12 +1670,13 @@ double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps,
 
 #define PR_INST(T)                                                                                                 \
   template void mg_smooth<T>(cudaStream_t, const LevelCoef&, const T*, const T*, T*, const T*, const T*, int, bool, \
-                             double*);                                                                            \
-  template void mg_resid_restrict<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, T*);       \
-  template void mg_cg_update_presmooth<T>(cudaStream_t, const LevelCoef&, const T*, const CgFuse<T>&, T*, double*); \
+                             double*, uint32_t);                                                                  \
+  template void mg_resid_restrict<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, T*,        \
+                                     uint32_t);                                                                   \
+  template void mg_cg_update_presmooth<T>(cudaStream_t, const LevelCoef&, const T*, const CgFuse<T>&, T*, double*, \
+                                          uint32_t);                                                              \
   template void mg_spmv<T>(cudaStream_t, const LevelCoef&, const T*, const T*, const T*, T*, double, bool, T*,    \
-                           double*);                                                                              \
-  template void screen_project_sq<T>(cudaStream_t, const Screen<T>&, const T*, double*, int);
+                           double*, uint32_t, const double*);
 PR_INST(float)
 PR_INST(double)
 #undef PR_INST

@@ -95,6 +95,64 @@ __global__ void k_screen_gather(const uint32_t* __restrict__ snode, const uint32
   }
 }
 
+// packed screening: cloud blockIdx.y, its descriptor and vector slice (n per cloud); the per-point
+// and per-node arithmetic of k_screen_project / k_screen_gather
+template <typename T>
+__device__ __forceinline__ const T* sd_phi(const ScreenDesc& d);
+template <>
+__device__ __forceinline__ const float* sd_phi<float>(const ScreenDesc& d) { return d.phi32; }
+template <>
+__device__ __forceinline__ const double* sd_phi<double>(const ScreenDesc& d) { return d.phi64; }
+template <typename T>
+__device__ __forceinline__ T* sd_proj(const ScreenDesc& d);
+template <>
+__device__ __forceinline__ float* sd_proj<float>(const ScreenDesc& d) { return d.proj32; }
+template <>
+__device__ __forceinline__ double* sd_proj<double>(const ScreenDesc& d) { return d.proj64; }
+
+// proj = Phi^T x; part (nullable): per-block sums of proj^2 (blockDim 256)
+template <typename T>
+__global__ void k_screen_project_pk(const ScreenDesc* __restrict__ desc, uint32_t sentinel, const T* __restrict__ x,
+                                    uint64_t n, double* __restrict__ part) {
+  const ScreenDesc d = desc[blockIdx.y];
+  x = cloud_slice(x, n);
+  const T* __restrict__ phi = sd_phi<T>(d);
+  T* __restrict__ proj = sd_proj<T>(d);
+  double acc = 0.0;
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < d.P; p += (uint64_t)gridDim.x * blockDim.x) {
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t kk = d.key[8 * p + k];
+      if (kk != sentinel) s += phi[8 * p + k] * x[kk];
+    }
+    proj[p] = s;
+    acc += (double)s * (double)s;
+  }
+  if (part) {
+    typedef cub::BlockReduce<double, kThreads> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const double t = BR(tmp).Sum(acc);
+    if (threadIdx.x == 0) part[(uint64_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+template <typename T>
+__global__ void k_screen_gather_pk(const ScreenDesc* __restrict__ desc, T wh3s, T* __restrict__ y, uint64_t n) {
+  const ScreenDesc d = desc[blockIdx.y];
+  y = cloud_slice(y, n);
+  const T* __restrict__ phi = sd_phi<T>(d);
+  const T* __restrict__ proj = sd_proj<T>(d);
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < d.S; u += (uint64_t)gridDim.x * blockDim.x) {
+    T acc = 0;
+    for (uint32_t e = d.soff[u]; e < d.soff[u + 1]; ++e) {
+      const uint32_t pk = d.sval[e];
+      acc += phi[pk] * proj[pk >> 3];
+    }
+    y[d.snode[u]] += wh3s * acc;
+  }
+}
+
 // ------------------------------------------------------------------ dots / vector ops
 template <typename TA, typename TB>
 __global__ void k_dot_partial(const TA* __restrict__ a, const TB* __restrict__ b, uint64_t n, double* __restrict__ part) {
@@ -134,6 +192,9 @@ inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 
 template <typename T>
 __global__ void k_dot_partial4(const T* __restrict__ a, const T* __restrict__ b, uint64_t n, double* __restrict__ part) {
+  a = cloud_slice(a, n);  // packed launches: cloud blockIdx.y
+  b = cloud_slice(b, n);
+  part = cloud_slice(part, gridDim.x);
   double s = 0.0;
   const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
@@ -235,6 +296,9 @@ __global__ void k_axpy4(uint64_t n, double a, const Tin* __restrict__ x, Tout* _
 
 __global__ void k_convert_norm4(uint64_t n, const double* __restrict__ x, float* __restrict__ y,
                                 double* __restrict__ part) {
+  x = cloud_slice(x, n);  // packed launches: cloud blockIdx.y
+  y = cloud_slice(y, n);
+  part = cloud_slice(part, gridDim.x);
   double s = 0.0;
   const uint64_t n4 = n / 4, stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
@@ -259,7 +323,10 @@ __global__ void k_convert_norm4(uint64_t n, const double* __restrict__ x, float*
 }
 
 __global__ void k_sum_final(const double* __restrict__ part, int np, double* __restrict__ out) {
-  // one warp, fixed order: lane-strided partial sums then a fixed shuffle tree
+  // one warp, fixed order: lane-strided partial sums then a fixed shuffle tree; block b sums the
+  // partials of cloud b (packed launches)
+  part += (uint64_t)blockIdx.x * np;
+  out += blockIdx.x;
   double s = 0.0;
   for (int i = threadIdx.x; i < np; i += 32) s += part[i];
 #pragma unroll
@@ -430,6 +497,8 @@ __global__ void k_prolong_add(uint32_t Df, const T* __restrict__ ec, T* __restri
 template <typename T>
 __global__ void k_dense_solve(uint32_t nc, const T* __restrict__ inv, const T* __restrict__ f, T* __restrict__ e) {
   __shared__ T fs[512];
+  f = cloud_slice(f, nc);  // packed launches: cloud blockIdx.y
+  e = cloud_slice(e, nc);
   for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) fs[i] = f[i];
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) {
@@ -498,6 +567,39 @@ double dot(pr_context* c, const T* a, const T* b, uint64_t n) {
   PR_CUDA(cudaMemcpyAsync(c->h_scalars, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   c->sync();
   return c->h_scalars[0];
+}
+
+template <typename T>
+void screen_project_pk(cudaStream_t s, const ScreenPack& scr, const T* x, uint64_t n, double* part, int nparts) {
+  if (!scr.active()) return;
+  const unsigned g = part ? (unsigned)nparts : grid_for(scr.maxP);
+  k_screen_project_pk<T><<<dim3(g, scr.clouds), kThreads, 0, s>>>(scr.desc, scr.sentinel, x, n, part);
+  PR_CHECK_LAUNCH();
+}
+
+template <typename T>
+void screen_gather_pk(cudaStream_t s, const ScreenPack& scr, T* y, uint64_t n, int sign) {
+  if (!scr.active()) return;
+  k_screen_gather_pk<T><<<dim3(grid_for(scr.maxS), scr.clouds), kThreads, 0, s>>>(scr.desc, (T)sign * (T)scr.wh3,
+                                                                                   y, n);
+  PR_CHECK_LAUNCH();
+}
+
+template <typename T>
+void dots_pk(cudaStream_t s, const T* a, const T* b, uint64_t n, uint32_t clouds, double* part, double* out) {
+  PR_REQUIRE(aligned16(a) && aligned16(b), PR_ERR_INTERNAL, "packed dot products need 16-byte aligned vectors");
+  k_dot_partial4<T><<<dim3(kDotBlocks, clouds), kThreads, 0, s>>>(a, b, n, part);
+  PR_CHECK_LAUNCH();
+  k_sum_final<<<clouds, 32, 0, s>>>(part, kDotBlocks, out);
+  PR_CHECK_LAUNCH();
+}
+
+void convert_sq_pk(cudaStream_t s, const double* x, float* y, uint64_t n, uint32_t clouds, double* part, double* out) {
+  PR_REQUIRE(aligned16(x) && aligned16(y), PR_ERR_INTERNAL, "packed conversion needs 16-byte aligned vectors");
+  k_convert_norm4<<<dim3(kDotBlocks, clouds), kThreads, 0, s>>>(n, x, y, part);
+  PR_CHECK_LAUNCH();
+  k_sum_final<<<clouds, 32, 0, s>>>(part, kDotBlocks, out);
+  PR_CHECK_LAUNCH();
 }
 
 template <typename T>
@@ -594,8 +696,8 @@ void prolong_add(cudaStream_t s, uint32_t Df, const T* ec, T* ef) {
 }
 
 template <typename T>
-void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e) {
-  k_dense_solve<T><<<1, 512, 0, s>>>(nc, inv, f, e);
+void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e, uint32_t clouds) {
+  k_dense_solve<T><<<dim3(1, clouds), 512, 0, s>>>(nc, inv, f, e);
   PR_CHECK_LAUNCH();
 }
 
@@ -612,7 +714,10 @@ void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e) {
   template void gs_sweep<T>(cudaStream_t, uint32_t, T*, const T*, Coef<T>, bool);                     \
   template void restrict_to_coarse<T>(cudaStream_t, uint32_t, const T*, T*);                          \
   template void prolong_add<T>(cudaStream_t, uint32_t, const T*, T*);                                 \
-  template void dense_solve<T>(cudaStream_t, uint32_t, const T*, const T*, T*);
+  template void dense_solve<T>(cudaStream_t, uint32_t, const T*, const T*, T*, uint32_t);              \
+  template void screen_project_pk<T>(cudaStream_t, const ScreenPack&, const T*, uint64_t, double*, int); \
+  template void screen_gather_pk<T>(cudaStream_t, const ScreenPack&, T*, uint64_t, int);                \
+  template void dots_pk<T>(cudaStream_t, const T*, const T*, uint64_t, uint32_t, double*, double*);
 PR_INST(float)
 PR_INST(double)
 #undef PR_INST

@@ -37,6 +37,38 @@ struct Screen {
   bool active() const { return S > 0; }
 };
 
+// One cloud's screening payload in a packed solve (several clouds of one depth and screening
+// weight, vectors concatenated): a device array holds one descriptor per cloud.
+struct ScreenDesc {
+  const uint32_t* key = nullptr;  // 8P
+  const float* phi32 = nullptr;   // 8P
+  const double* phi64 = nullptr;  // 8P
+  const uint32_t* snode = nullptr, *soff = nullptr, *sval = nullptr;
+  float* proj32 = nullptr;        // P scratch
+  double* proj64 = nullptr;       // P scratch
+  uint64_t P = 0, S = 0;
+};
+struct ScreenPack {
+  const ScreenDesc* desc = nullptr;  // device, one per cloud
+  uint32_t clouds = 0;
+  uint64_t maxP = 0, maxS = 0;
+  uint32_t sentinel = 0;  // res^3
+  double wh3 = 0.0;
+  bool active() const { return maxS > 0; }
+};
+// per cloud: proj = Phi^T x; part (nullable, nparts per cloud): per-block sums of proj^2
+template <typename T>
+void screen_project_pk(cudaStream_t s, const ScreenPack& scr, const T* x, uint64_t n, double* part = nullptr,
+                       int nparts = 0);
+// per cloud: y += sign * wh3 * Phi proj
+template <typename T>
+void screen_gather_pk(cudaStream_t s, const ScreenPack& scr, T* y, uint64_t n, int sign);
+// per cloud k: out[k] = a_k . b_k (fixed order), part: kDotBlocks per cloud (device results)
+template <typename T>
+void dots_pk(cudaStream_t s, const T* a, const T* b, uint64_t n, uint32_t clouds, double* part, double* out);
+// per cloud k: y_k = (float) x_k, out[k] = x_k . x_k (device results)
+void convert_sq_pk(cudaStream_t s, const double* x, float* y, uint64_t n, uint32_t clouds, double* part, double* out);
+
 // y = A' x (mode 0) or y = f - A' x (mode 1), A' = constant stencil at `depth`
 template <typename T>
 void stencil_apply(cudaStream_t s, uint32_t depth, const T* x, const T* f, T* y, Coef<T> c, int mode);
@@ -79,8 +111,9 @@ template <typename T>
 void restrict_to_coarse(cudaStream_t s, uint32_t fine_depth, const T* r_fine, T* f_coarse);
 template <typename T>
 void prolong_add(cudaStream_t s, uint32_t fine_depth, const T* e_coarse, T* e_fine);
+// e = inv f per cloud (clouds > 1: packed vectors of nc entries per cloud)
 template <typename T>
-void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e);
+void dense_solve(cudaStream_t s, uint32_t nc, const T* inv, const T* f, T* e, uint32_t clouds = 1);
 
 // ------------------------------------------------------------------ the fine operator
 template <typename T>

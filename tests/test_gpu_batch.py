@@ -61,3 +61,46 @@ def test_batch_empty_and_zero_point_clouds():
     out = prb.reconstruct_batch([np.zeros((0, 6)), synthetic.sphere(3000, seed=2)],
                                 prb.ReconstructParams(depth=5, point_weight=4.0))
     assert out[0][0].triangles.shape == (0, 3) and out[1][0].triangles.shape[0] > 0
+
+
+def _mixed_shapes(seed=91):
+    """Clouds of depth 5 and 6 whose solves stop after different numbers of iterations: clean and
+    noisy surfaces, a few hundred points and tens of thousands."""
+    rng = np.random.default_rng(seed)
+    clouds, depths = [], []
+    for i in range(9):
+        n = [300, 2_000, 40_000][i % 3]
+        kind = (i // 3) % 3
+        if kind == 0:
+            pts = synthetic.sphere(n, seed=500 + i)
+        elif kind == 1:
+            pts = synthetic.torus(n, 600 + i, R=0.8, r=0.25, noise=0.01, normal_sigma=0.3, fp32=True)
+        else:
+            pts = synthetic.ellipsoid(n, 700 + i, radii=tuple(rng.uniform(0.3, 1.0, 3)), noise=0.02, fp32=True)
+        clouds.append(pts)
+        depths.append(5 + (i % 2))
+    return clouds, depths
+
+
+@pytest.mark.parametrize("precision", [prb.PR_PRECISION_MIXED, prb.PR_PRECISION_FP64])
+def test_packed_solve_matches_single_calls(ctx, precision, monkeypatch, capsys):
+    """Clouds of one depth are solved together (one launch per solver step for all of them); packs
+    of at most 3 clouds here, so a depth group spans several packs.  Every cloud's coefficients,
+    iteration counts, residual and mesh equal a single-cloud call's, also for clouds that stop
+    before the others of their pack."""
+    monkeypatch.setenv("PR_PACK_MAX_CLOUDS", "3")
+    clouds, depths = _mixed_shapes()
+    params = [prb.ReconstructParams(depth=d, point_weight=4.0, precision=precision) for d in depths]
+    out = prb.reconstruct_batch(clouds, params, concurrency=2)
+    iters = {}
+    for pts, p, (mesh, st) in zip(clouds, params, out):
+        m1, st1 = ctx.reconstruct(pts, p)
+        assert st.converged == 1
+        assert (st.pcg_iterations, st.refinement_steps) == (st1.pcg_iterations, st1.refinement_steps)
+        assert st.rel_residual == st1.rel_residual
+        assert st.iso_value == st1.iso_value
+        assert np.array_equal(mesh.triangles, m1.triangles)
+        assert np.array_equal(mesh.vertices, m1.vertices)
+        iters.setdefault(p.depth, []).append((st.pcg_iterations, st.refinement_steps))
+    with capsys.disabled():
+        print("\npacked batch (%s): iterations per depth %s" % ("FP64" if precision else "mixed", iters))

@@ -259,7 +259,8 @@ def test_rejected_combinations(ctx):
     with pytest.raises(prb.ReconstructError) as e:
         ctx.reconstruct(pts, params(4, 4.0, solve_mode=prb.PR_SOLVE_REFERENCE_SCHEDULE))
     assert e.value.code == prb.PR_ERR_INVALID_ARGUMENT
-    ctx.solve(pts, params(4, 4.0))
+    # the adjoint covers the dense degree-2 grid, not the adaptive band
+    ctx.solve(pts, params(6, 4.0, coarse_depth=4))
     with pytest.raises(prb.ReconstructError) as e:
         ctx.loss_backward(pts[:10, :3], n_points=len(pts))
     assert e.value.code == prb.PR_ERR_STATE
