@@ -220,13 +220,21 @@ int pr_ctx_kernel_bench(pr_context* ctx, int kernel, uint32_t depth, int precisi
                         double* bytes_per_launch);
 
 /* ------------------------------------------------------------------ batches
- * Many independent clouds (each with its own params, e.g. its own depth).  One host thread per
- * context drives that context's stream; clouds are taken largest first, so the kernels of
- * several small reconstructions overlap on the GPU.  out_meshes[i] / out_stats[i] /
- * out_status[i] belong to cloud i (out_stats and out_status may be NULL).  Returns PR_OK if
- * every cloud succeeded, else the status of the lowest-numbered failed cloud (its message in
- * pr_last_error); the other clouds' results are still written.  No counterpart in the
- * reference crate, which reconstructs one cloud per call (src/reconstructor.rs:25). */
+ * Many independent clouds (each with its own params, e.g. its own depth).  Clouds on a dense
+ * degree-1 grid of depth >= 5 in solve_mode PR_SOLVE_CONVERGED that share depth, point_weight,
+ * precision, target_rel_residual, inner_rel_tol, max_iters and smooth_sweeps are reconstructed in
+ * packs: set up and extracted one per context on host threads, their systems solved together
+ * with one launch per solver step for every cloud of the pack (a pack holds as many clouds as
+ * the free device memory does; PR_PACK_MAX_CLOUDS caps it).  Packed results equal single calls
+ * bit for bit; a packed cloud's time_solve is its share of the pack's solve.  The packs use
+ * library-owned contexts on ctxs[0]'s device, kept for later batches (their memory is released
+ * when an allocation elsewhere in the process fails).  Every other cloud goes through ctxs: one
+ * host thread per context drives that context's stream, clouds taken largest first.
+ * out_meshes[i] / out_stats[i] / out_status[i] belong to cloud i (out_stats and out_status may
+ * be NULL).  Returns PR_OK if every cloud succeeded, else the status of the lowest-numbered
+ * failed cloud (its message in pr_last_error); the other clouds' results are still written.  No
+ * counterpart in the reference crate, which reconstructs one cloud per call
+ * (src/reconstructor.rs:25). */
 int pr_ctx_reconstruct_batch(pr_context* const* ctxs, uint32_t n_ctx, const double* const* points6, const uint64_t* n,
                              uint32_t count, const pr_params* params, pr_mesh* out_meshes, pr_stats* out_stats,
                              int* out_status);
@@ -290,6 +298,12 @@ int pr_ply_write_mesh(const char* path, const pr_mesh* mesh, int format);
 /* Number of kernels launched by this library in this process (own kernels; library
  * primitives such as radix sorts and scans are counted in *primitive_calls). */
 uint64_t pr_kernel_launches(uint64_t* primitive_calls);
+
+/* The z-segment choices of the degree-1 block kernels made so far in this process: the first
+ * FP32 launch of a (kernel family, level, launch size) times 2, 4 and 8 z planes per thread
+ * (identical results) and keeps the fastest; one line per choice with its timings.  Library
+ * memory, valid until the next call. */
+const char* pr_autotune_log(void);
 
 /* Iso value without any device allocation.  No counterpart in the reference crate: it exists
  * for callers that cannot allocate device memory — a host whose caching allocator already

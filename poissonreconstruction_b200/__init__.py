@@ -71,6 +71,7 @@ SIGNATURES = {
     "pr_version": (C.c_char_p, []),
     "pr_abi_layout": (None, [_P]),
     "pr_kernel_launches": (C.c_uint64, [C.POINTER(C.c_uint64)]),
+    "pr_autotune_log": (C.c_char_p, []),
     "pr_ctx_apply_operator_device": (C.c_int, [_P, _P, _P, C.c_int]),
     "pr_iso_value_noalloc": (C.c_int, [C.c_uint32, _P, _P, C.c_uint64, _P, _P]),
     "pr_ctx_kernel_bench": (C.c_int, [_P, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_double),
@@ -557,3 +558,8 @@ def kernel_launches():
 
 
 __all__ = ["ReconstructParams", "ReconstructStats", "Mesh", "reconstruct", "Context", "ReconstructError", "lib"]
+
+
+def autotune_log():
+    """The z-segment choices of the degree-1 block kernels made so far in this process."""
+    return lib().pr_autotune_log().decode()

@@ -426,6 +426,20 @@ struct BatchEngine {
     for (const pr_context* c : cl) b += c->bytes_held;
     return b;
   }
+  // frees every buffer (and graph) of the contexts, keeping the contexts
+  void free_buffers() {
+    auto drop = [](pr_context* c) {
+      PR_CUDA(cudaStreamSynchronize(c->stream));
+      for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+      c->graphs.clear();
+      for (auto& kv : c->bufs)
+        if (kv.second.ptr) cudaFree(kv.second.ptr);
+      c->bufs.clear();
+      c->bytes_held = 0;
+    };
+    if (solver) drop(solver);
+    for (pr_context* c : cl) drop(c);
+  }
   void release() {
     if (solver) pr_context_destroy(solver);
     solver = nullptr;
@@ -594,13 +608,19 @@ void run_packed(int device, const std::map<PackKey, std::vector<uint32_t>>& grou
   });
   const char* lim = std::getenv("PR_PACK_MAX_CLOUDS");  // cap on the clouds of one pack (0: none)
   const size_t max_clouds = lim ? (size_t)std::strtoull(lim, nullptr, 10) : 0;
+  uint32_t depth = 0;
   for (std::vector<uint32_t> grp : order) {
     std::stable_sort(grp.begin(), grp.end(), [&](uint32_t a, uint32_t b) { return n[a] > n[b]; });
+    // a new depth: the packs of the previous one held buffers of other sizes, which the next
+    // clouds would not reuse
+    if (params[grp[0]].depth != depth && E.held() > 0) E.free_buffers();
+    depth = params[grp[0]].depth;
     size_t pos = 0;
     while (pos < grp.size()) {
       size_t free_b = 0, total_b = 0;
       PR_CUDA(cudaSetDevice(device));
       PR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      // the packs of this depth reuse the buffers held so far
       const double budget = (double)free_b + (double)E.held() - std::max(8e9, 0.05 * (double)total_b);
       std::vector<uint32_t> pk;
       double acc = 0.0;
@@ -639,10 +659,15 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace pr
 
 static std::atomic<uint64_t> g_launches{0}, g_primitives{0};
+static thread_local uint64_t t_counts[2] = {0, 0};
+namespace pr {
+uint64_t thread_launch_count(int primitive) { return t_counts[primitive ? 1 : 0]; }
+}  // namespace pr
 
 extern "C" {
 
 void pr_count_launch_(int primitive) {
+  ++t_counts[primitive ? 1 : 0];
   if (primitive) g_primitives.fetch_add(1, std::memory_order_relaxed);
   else g_launches.fetch_add(1, std::memory_order_relaxed);
 }
@@ -679,6 +704,12 @@ int pr_ctx_kernel_bench(pr_context* c, int kernel, uint32_t depth, int precision
 }
 
 const char* pr_version(void) { return "poisson_recon_b200 0.1 (sm_100a)"; }
+
+const char* pr_autotune_log(void) {
+  static thread_local std::string text;
+  text = pr::autotune_log();
+  return text.c_str();
+}
 
 void pr_abi_layout(uint64_t* out4) {
   if (!out4) return;
@@ -753,6 +784,8 @@ int pr_context_destroy(pr_context* c) {
     for (cudaEvent_t e : c->copy_events)
       if (e) cudaEventDestroy(e);
     c->copy_events.clear();
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+    c->graphs.clear();
     if (c->side) {
       cudaStreamSynchronize(c->side);
       cudaStreamDestroy(c->side);

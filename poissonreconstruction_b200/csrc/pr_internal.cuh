@@ -36,6 +36,8 @@ struct Error : std::runtime_error {
 // Every kernel launch of the library is followed by PR_CHECK_LAUNCH (error check + count);
 // every CUB primitive call by PR_COUNT_PRIMITIVE.
 extern "C" void pr_count_launch_(int primitive);
+// launches (primitive 0) or primitive calls (1) counted on the calling thread so far
+uint64_t thread_launch_count(int primitive);
 #define PR_CHECK_LAUNCH()   \
   do {                      \
     pr_count_launch_(0);    \
@@ -192,6 +194,46 @@ struct pr_context {
     return side;
   }
   pr_params params{};             // parameters of the last reconstruction
+  // Instantiated CUDA graphs of repeated launch sequences on `stream` (the solver's V-cycle),
+  // keyed by everything they were captured with (sizes, coefficients, buffer addresses); kept for
+  // reuse, with the kernel launches they hold (counted again at every replay).
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0, primitives = 0;
+  };
+  std::map<std::string, Graph> graphs;
+  // Runs body() through the graph of `key`, capturing it on first use.
+  template <typename F>
+  void run_graph(const std::string& key, F body) {
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+      cudaGraph_t g = nullptr;
+      const uint64_t l0 = pr::thread_launch_count(0), p0 = pr::thread_launch_count(1);
+      PR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        body();
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+      }
+      PR_CUDA(cudaStreamEndCapture(stream, &g));
+      const uint64_t l1 = pr::thread_launch_count(0), p1 = pr::thread_launch_count(1);
+      Graph gr;
+      const cudaError_t e = cudaGraphInstantiate(&gr.exec, g, 0);
+      cudaGraphDestroy(g);
+      PR_CUDA(e);
+      gr.launches = l1 - l0;
+      gr.primitives = p1 - p0;
+      PR_CUDA(cudaGraphLaunch(gr.exec, stream));  // counted by the capture
+      graphs.emplace(key, gr);
+      return;
+    }
+    PR_CUDA(cudaGraphLaunch(it->second.exec, stream));
+    for (uint64_t k = 0; k < it->second.launches; ++k) pr::pr_count_launch_(0);
+    for (uint64_t k = 0; k < it->second.primitives; ++k) pr::pr_count_launch_(1);
+  }
 
   template <typename T>
   T* buf(const std::string& name, size_t count) {

@@ -23,6 +23,10 @@
 #include <cub/cub.cuh>
 
 #include <mutex>
+#include <tuple>
+#include <map>
+#include <cstdio>
+#include <cstdlib>
 #include <set>
 #include <string>
 #include <type_traits>
@@ -495,7 +499,6 @@ __global__ void __launch_bounds__(1024) k_sum_parts(const double* __restrict__ p
 
 // ------------------------------------------------------------------ helpers of the 16^3 block kernels
 namespace s16 {
-constexpr int THREADS = 256;
 constexpr int CW = 10;  // coarse tile width
 
 // spread the 4 low bits of v to bit positions 0,3,6,9
@@ -533,11 +536,12 @@ __device__ __forceinline__ void quad_coords(int q, int& lx, int& ly, int& lz) {
 
 // Load the one-node halo of the block into a tile (idx: tile index of tile coordinates).
 // nb[27]: Morton base of the neighbour block (dx+1)+3(dy+1)+9(dz+1), or ~0u if outside.
-template <typename T, typename Idx, typename Xf>
+// NT: threads of the CTA.
+template <int NT, typename T, typename Idx, typename Xf>
 __device__ __forceinline__ void load_halo(T* tile, const T* __restrict__ x, const uint32_t* nb, Idx idx, Xf xf) {
-  const int t = threadIdx.x;
-  {  // faces: (a, b) = thread's in-face coordinates
-    const int a = t & 15, b = t >> 4;
+#pragma unroll
+  for (int i = threadIdx.x; i < 256; i += NT) {  // faces: (a, b) = in-face coordinates of position i
+    const int a = i & 15, b = i >> 4;
     const uint32_t sa = sp4(a), sb = sp4(b);
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -554,8 +558,19 @@ __device__ __forceinline__ void load_halo(T* tile, const T* __restrict__ x, cons
       tile[idx(ux, uy, uz)] = base != ~0u ? xf(base + m) : (T)0;
     }
   }
-  if (t < 192) {  // edges: 4 per axis, 16 nodes each
-    const int e = t >> 4, a = t & 15, axis = e >> 2, s1 = e & 1, s2 = (e >> 1) & 1;
+#pragma unroll
+  for (int i = threadIdx.x; i < 200; i += NT) {
+    if (i >= 192) {  // corners
+      const int c = i - 192;
+      const int sx = c & 1, sy = (c >> 1) & 1, sz = (c >> 2) & 1;
+      const uint32_t m = (sx ? 0u : 0x249u) | ((sy ? 0u : 0x249u) << 1) | ((sz ? 0u : 0x249u) << 2);
+      const int nbi = (sx ? 2 : 0) + 3 * (sy ? 2 : 0) + 9 * (sz ? 2 : 0);
+      const uint32_t base = nb[nbi];
+      tile[idx(sx ? 17 : 0, sy ? 17 : 0, sz ? 17 : 0)] = base != ~0u ? xf(base + m) : (T)0;
+      continue;
+    }
+    // edges: 4 per axis, 16 nodes each
+    const int e = i >> 4, a = i & 15, axis = e >> 2, s1 = e & 1, s2 = (e >> 1) & 1;
     const uint32_t sa = sp4(a);
     const uint32_t c1 = s1 ? 0u : 0x249u, c2 = s2 ? 0u : 0x249u;
     const int d1 = s1 ? 1 : -1, d2 = s2 ? 1 : -1;
@@ -567,14 +582,31 @@ __device__ __forceinline__ void load_halo(T* tile, const T* __restrict__ x, cons
     else { m = c1 | (c2 << 1) | (sa << 2); ux = u1; uy = u2; uz = a + 1; nbi = (d1 + 1) + 3 * (d2 + 1) + 9; }
     const uint32_t base = nb[nbi];
     tile[idx(ux, uy, uz)] = base != ~0u ? xf(base + m) : (T)0;
-  } else if (t < 200) {  // corners
-    const int c = t - 192;
-    const int sx = c & 1, sy = (c >> 1) & 1, sz = (c >> 2) & 1;
-    const uint32_t m = (sx ? 0u : 0x249u) | ((sy ? 0u : 0x249u) << 1) | ((sz ? 0u : 0x249u) << 2);
-    const int nbi = (sx ? 2 : 0) + 3 * (sy ? 2 : 0) + 9 * (sz ? 2 : 0);
-    const uint32_t base = nb[nbi];
-    tile[idx(sx ? 17 : 0, sy ? 17 : 0, sz ? 17 : 0)] = base != ~0u ? xf(base + m) : (T)0;
   }
+}
+
+// The sum over a 16^3 block of one value per (quad column q, plane z), in an order fixed by the
+// block whatever the launch shape: each column's planes in z order, then the 64 column sums by a
+// fixed tree.  red: 1024 doubles of shared memory holding the value of (q, z) at [z 64 + q] (the
+// caller writes it after a barrier that ends every other use of that memory).  Every thread calls
+// this (it has barriers); thread 0 returns the sum.
+__device__ __forceinline__ double block_sum_fixed(double* red) {
+  __syncthreads();
+  const int t = threadIdx.x;
+  double s = 0.0;
+  if (t < 64) {
+#pragma unroll
+    for (int z = 0; z < 16; ++z) s += red[z * 64 + t];
+  }
+  __syncthreads();
+  if (t < 64) red[t] = s;
+  __syncthreads();
+  if (t < 32) {
+    s = red[t] + red[t + 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;
 }
 
 __device__ __forceinline__ void neighbour_bases(uint32_t* nb, uint32_t bx, uint32_t by, uint32_t bz, int nblk_axis) {
@@ -590,12 +622,12 @@ __device__ __forceinline__ void neighbour_bases(uint32_t* nb, uint32_t bx, uint3
 
 // Coarse tile for the prolongation: coarse block (8^3, Morton-contiguous) with a one-node
 // halo, natural layout 10^3, coordinate = coarse local + 1.  Ends with a barrier.
-template <typename T>
+template <int NT, typename T>
 __device__ __forceinline__ void load_coarse_tile(T* ctile, const T* __restrict__ ec, uint32_t blk, uint32_t bx,
                                                  uint32_t by, uint32_t bz, int nblk_axis, uint32_t* cnb) {
   const int t = threadIdx.x;
   // interior: 512 contiguous coarse values
-  for (int i = t; i < 512; i += THREADS) {
+  for (int i = t; i < 512; i += NT) {
     uint32_t cx, cy, cz;
     unmorton3((uint32_t)i, cx, cy, cz);
     ctile[((cz + 1) * CW + (cy + 1)) * CW + (cx + 1)] = __ldg(ec + (uint64_t)blk * 512 + i);
@@ -610,7 +642,7 @@ __device__ __forceinline__ void load_coarse_tile(T* ctile, const T* __restrict__
   }
   __syncthreads();
   auto sp3 = [](uint32_t v) { return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4); };
-  for (int i = t; i < 488; i += THREADS) {
+  for (int i = t; i < 488; i += NT) {
     int ux, uy, uz;
     uint32_t mloc;
     int nbi;
@@ -675,7 +707,13 @@ __device__ __forceinline__ T prolong_at(const T* ctile, int ux, int uy, int uz) 
 // in-plane edges) and to the rows above and below (edges and corners), so a thread keeps two
 // accumulators per node instead of three planes of sums.
 namespace n16 {
-constexpr int N = 4096, THREADS = 256, ZT = 4;
+// ZT: z planes per thread (2, 4 or 8); the CTA has 1024 / ZT threads (64 quad columns x 16 / ZT
+// z segments).  The arithmetic of a node, and every per-block sum, is the same for every ZT.
+constexpr int N = 4096;
+template <int ZT>
+struct Zt {
+  static constexpr int NT = 1024 / ZT;
+};
 constexpr int RS = 24, PS = 18 * RS + 4, TILE = 18 * PS;
 __device__ __forceinline__ int nat(int ux, int uy, int uz) { return uz * PS + uy * RS + ux; }  // u = local + 1
 
@@ -724,11 +762,12 @@ __device__ __forceinline__ void plane_terms(const T r[4][4], T c0, T ce, T cc, T
 // KIND 0: q = A a, part = a.q;  1: an = bvec + beta a, q = A an, part = an.q;
 // 2: an = a + beta bvec (FP64 solution + correction of type E), q = rhs - A an.
 // beta_dev (packed launches): the cloud's beta, in place of the beta argument.
-template <typename T, int KIND, typename E>
-__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
+template <typename T, int KIND, typename E, int ZT>
+__global__ void __launch_bounds__(Zt<ZT>::NT, (sizeof(T) == 4 ? 5 : 3) * ZT / 4)
     k_spmv16(uint32_t D, const T* __restrict__ a, const E* __restrict__ bvec, T* __restrict__ an, T beta,
              T* __restrict__ q, T c0, T ce, T cc, const T* __restrict__ rhs, double* __restrict__ part,
              const double* __restrict__ beta_dev) {
+  constexpr int NT = Zt<ZT>::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);
   __shared__ uint32_t nb[27];
@@ -756,8 +795,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
     return beta == (T)0 ? __ldg(a + m) : __ldg(a + m) + beta * (T)__ldg(bvec + m);
   };
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int qd = t + THREADS * r;
+  for (int r = 0; r < ZT; ++r) {
+    const int qd = t + NT * r;
     int lx, ly, lz;
     s16::quad_coords(qd, lx, ly, lz);
     const uint64_t m = base + 4 * qd;
@@ -778,13 +817,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
     p0[RS + 1] = v.w;
   }
   __syncthreads();  // nb
-  s16::load_halo<T>(tile, a, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); }, val);
+  s16::load_halo<NT>(tile, a, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); }, val);
   __syncthreads();
   const int qi = t & 63, zs = t >> 6;
   const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
   const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
   T cur[4] = {0, 0, 0, 0}, nxt[4] = {0, 0, 0, 0}, cprev[4] = {0, 0, 0, 0};
-  double acc = 0.0;
+  double pv[ZT];  // per plane: the quad's four products of the dot
 #pragma unroll
   for (int p = 0; p < ZT + 2; ++p) {  // tile plane z0 + p = local z0 + p - 1
     T r[4][4], tz[4], own[4], ctr[4];
@@ -803,8 +842,10 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
         o.x = rv.x - cur[0]; o.y = rv.y - cur[1]; o.z = rv.z - cur[2]; o.w = rv.w - cur[3];
       } else {
         o.x = cur[0]; o.y = cur[1]; o.z = cur[2]; o.w = cur[3];
+        double a4 = 0.0;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc += (double)cprev[e] * (double)cur[e];
+        for (int e = 0; e < 4; ++e) a4 += (double)cprev[e] * (double)cur[e];
+        pv[p - 2] = a4;
       }
       s16::st4(q + m, o);
     }
@@ -816,9 +857,11 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 5 : 3)
     }
   }
   if (KIND != 2) {
-    typedef cub::BlockReduce<double, THREADS> BR;
-    __shared__ typename BR::TempStorage tmp;
-    const double sdot = BR(tmp).Sum(acc);
+    __syncthreads();  // the tile's last reads: its memory takes the per-plane sums
+    double* red = reinterpret_cast<double*>(smem_raw);
+#pragma unroll
+    for (int k = 0; k < ZT; ++k) red[(z0 + k) * 64 + qi] = pv[k];
+    const double sdot = s16::block_sum_fixed(red);
     if (t == 0) part[blk] = sdot;
   }
 }
@@ -838,16 +881,17 @@ constexpr size_t smem_bytes() {
 // these partials of its low neighbours, scaled by 1/2 per crossed axis.  Restriction: coarse c
 // gathers fine 2c-1, 2c, 2c+1 per axis with weights 1/2, 1, 1/2.
 namespace r16 {
-constexpr int N = 4096, THREADS = 256, ZT = 4, FACE = 224;
+constexpr int N = 4096, FACE = 224;  // ZT, NT: as n16 (the residual is the same for every ZT)
 // face buffer layout: [0,64) x face (cy + 8 cz), [64,128) y face (cx + 8 cz), [128,192) z face
 // (cx + 8 cy), [192,200) xy edge (cz), [200,208) xz edge (cy), [208,216) yz edge (cx), 216 corner
 constexpr int RSR = 20, PSR = 16 * RSR + 8, RTILE = 16 * PSR;  // half-warps of the restriction on disjoint banks
 __device__ __forceinline__ int ridx(int x, int y, int z) { return z * PSR + y * RSR + x; }  // local coordinates
 
-template <typename T, bool FACES>
-__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
+template <typename T, bool FACES, int ZT>
+__global__ void __launch_bounds__(n16::Zt<ZT>::NT, (sizeof(T) == 4 ? 4 : 2) * ZT / 4)
     k_resid16(uint32_t D, const T* __restrict__ e, const T* __restrict__ f, T* __restrict__ fc,
               T* __restrict__ face, T c0, T ce, T cc, const T* __restrict__ table) {
+  constexpr int NT = n16::Zt<ZT>::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* et = reinterpret_cast<T*>(smem_raw);  // n16::TILE
   T* rt = et + n16::TILE;                  // RTILE
@@ -868,8 +912,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   const int t = threadIdx.x;
   s16::neighbour_bases(nb, bx, by, bz, res >> 4);
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int qd = t + THREADS * r;
+  for (int r = 0; r < ZT; ++r) {
+    const int qd = t + NT * r;
     int lx, ly, lz;
     s16::quad_coords(qd, lx, ly, lz);
     const typename s16::Vec4<T>::type ev = s16::ld4(e + base + 4 * qd);
@@ -880,7 +924,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     p0[n16::RS + 1] = ev.w;
   }
   __syncthreads();  // nb
-  s16::load_halo<T>(et, e, nb, [](int ux, int uy, int uz) { return n16::nat(ux, uy, uz); },
+  s16::load_halo<NT>(et, e, nb, [](int ux, int uy, int uz) { return n16::nat(ux, uy, uz); },
                     [&](uint32_t m) { return __ldg(e + m); });
   __syncthreads();
   {  // r = f - A e on quad columns, z swept once
@@ -917,7 +961,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   __syncthreads();
   if (FACES && (ox == 0 || oy == 0 || oz == 0)) {
     // nodes on a low domain face: replace the interior row by the face row
-    for (int i = t; i < N; i += THREADS) {
+    for (int i = t; i < N; i += NT) {
       uint32_t lx, ly, lz;
       unmorton3((uint32_t)i, lx, ly, lz);
       const int mask = ((ox + (int)lx) == 0) | (((oy + (int)ly) == 0) << 1) | (((oz + (int)lz) == 0) << 2);
@@ -942,8 +986,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   // own part of the restriction
   const uint64_t cbase = (uint64_t)blk * 512;
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int ci = t + THREADS * k;
+  for (int ci = t; ci < 512; ci += NT) {
     uint32_t cx, cy, cz;
     unmorton3((uint32_t)ci, cx, cy, cz);
     T s = 0;
@@ -968,35 +1011,37 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   {
     T* fb = face + (uint64_t)blk * FACE;
     auto w = [](int d) { return (T)(d == 0 ? 1.0 : 0.5); };
-    if (t < 192) {  // faces: the two free axes restricted, the face axis at local 15
-      const int axis = t >> 6, i = t & 7, j = (t >> 3) & 7;
-      T acc = 0;
+    for (int u = t; u < 217; u += NT) {
+      if (u < 192) {  // faces: the two free axes restricted, the face axis at local 15
+        const int axis = u >> 6, i = u & 7, j = (u >> 3) & 7;
+        T acc = 0;
 #pragma unroll
-      for (int dj = -1; dj <= 1; ++dj) {
-        const int fj = 2 * j + dj;
-        if (fj < 0) continue;
+        for (int dj = -1; dj <= 1; ++dj) {
+          const int fj = 2 * j + dj;
+          if (fj < 0) continue;
+#pragma unroll
+          for (int di = -1; di <= 1; ++di) {
+            const int fi = 2 * i + di;
+            if (fi < 0) continue;
+            const int x = axis == 0 ? 15 : fi, y = axis == 1 ? 15 : (axis == 0 ? fi : fj), z = axis == 2 ? 15 : fj;
+            acc += w(di) * w(dj) * rt[ridx(x, y, z)];
+          }
+        }
+        fb[u] = acc;
+      } else if (u < 216) {  // edges: the free axis restricted
+        const int e = (u - 192) >> 3, i = (u - 192) & 7;
+        T acc = 0;
 #pragma unroll
         for (int di = -1; di <= 1; ++di) {
           const int fi = 2 * i + di;
           if (fi < 0) continue;
-          const int x = axis == 0 ? 15 : fi, y = axis == 1 ? 15 : (axis == 0 ? fi : fj), z = axis == 2 ? 15 : fj;
-          acc += w(di) * w(dj) * rt[ridx(x, y, z)];
+          const int x = e == 2 ? fi : 15, y = e == 1 ? fi : 15, z = e == 0 ? fi : 15;
+          acc += w(di) * rt[ridx(x, y, z)];
         }
+        fb[u] = acc;
+      } else {
+        fb[216] = rt[ridx(15, 15, 15)];
       }
-      fb[t] = acc;
-    } else if (t < 216) {  // edges: the free axis restricted
-      const int e = (t - 192) >> 3, i = (t - 192) & 7;
-      T acc = 0;
-#pragma unroll
-      for (int di = -1; di <= 1; ++di) {
-        const int fi = 2 * i + di;
-        if (fi < 0) continue;
-        const int x = e == 2 ? fi : 15, y = e == 1 ? fi : 15, z = e == 0 ? fi : 15;
-        acc += w(di) * rt[ridx(x, y, z)];
-      }
-      fb[t] = acc;
-    } else if (t == 216) {
-      fb[216] = rt[ridx(15, 15, 15)];
     }
   }
 }
@@ -1063,7 +1108,7 @@ constexpr size_t smem_bytes() {
 // couple z-neighbours of the same class; those take the values from before the phase (new
 // values are written after a barrier), a Jacobi step along the column for those rows only.
 namespace g16 {
-constexpr int THREADS = 256, ZT = 4, CW = s16::CW;
+constexpr int CW = s16::CW;  // ZT, NT: as n16 (a node's relaxation is the same for every ZT)
 using n16::nat;
 using n16::PS;
 using n16::RS;
@@ -1074,7 +1119,7 @@ using n16::TILE;
 // other five from the tile (a pair and three scalars); the two halo planes read all eight.
 // ZERO: a forward sweep from zero, in which the classes after CLS are still zero everywhere
 // (their loads are skipped; phase 0 needs none).
-template <typename T, int CLS, bool ZERO>
+template <typename T, int CLS, bool ZERO, int ZT>
 __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int z0, const T (&fv)[ZT][4],
                                              const T (&v)[ZT][4], T ce, T cc, T c0inv, T (&nv)[ZT]) {
   typedef typename n16::Pair<T>::type P2;
@@ -1112,7 +1157,9 @@ __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int 
           q2 = pr.y;
         }
       }
-      if (ND) Dp = (q0 + q2) + r0[(1 - EDY) * RS + EDX + 1] + v[k][ED];
+      // the same pairing as a halo plane's (row y-1 pair + row y+1 pair), so that a node's sums
+      // do not depend on which of its planes are a thread's own
+      if (ND) Dp = (q0 + q2) + (r0[(1 - EDY) * RS + EDX + 1] + v[k][ED]);
       if (NFY) Fp += q1 + v[k][EFY];
       if (NFX) Fp += r0[RS + EDX + 1] + v[k][EFX];
     } else {  // halo plane: the whole ring from the tile
@@ -1146,12 +1193,13 @@ __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int 
 // MODE 3 (finest level, forward): first the CG update x += alpha d, r -= alpha q in place
 // (pointwise), then xo = sweep(0) with f = the new r; part = per-block sums of r^2.  A sweep
 // from zero reads no halo, so updating r in place is race-free.
-template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
-__global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
+template <typename T, int MODE, bool DOT, bool FWD, bool FACES, int ZT>
+__global__ void __launch_bounds__(n16::Zt<ZT>::NT, (sizeof(T) == 4 ? 4 : 2) * ZT / 4)
     k_smooth16(uint32_t D, const T* __restrict__ xi, T* __restrict__ xo, const T* __restrict__ f,
                const T* __restrict__ ec, T c0inv, T ce, T cc, const T* __restrict__ table,
                double* __restrict__ part, CgFuse<T> cg) {
   static_assert(MODE != 3 || (FWD && !FACES), "the fused CG update is a forward sweep on the finest level");
+  constexpr int NT = n16::Zt<ZT>::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);  // TILE
   T* ctile = tile + TILE;                    // CW^3 (MODE 2)
@@ -1181,13 +1229,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
   constexpr bool FROM_ZERO = MODE == 1 || MODE == 3;
   if (!FROM_ZERO) s16::neighbour_bases(nb, bx, by, bz, res >> 4);
   else if (t < 27) nb[t] = ~0u;  // zero halo
-  if (MODE == 2) s16::load_coarse_tile<T>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // ends with a barrier
+  if (MODE == 2) s16::load_coarse_tile<NT>(ctile, ec, blk, bx, by, bz, res >> 4, cnb);  // ends with a barrier
   else __syncthreads();                                                                 // nb
   const int qi = t & 63, zs = t >> 6;
   const int x0 = 2 * (qi & 7), y0 = 2 * (qi >> 3), z0 = ZT * zs;
   const uint32_t mq = s16::sp4(x0) | (s16::sp4(y0) << 1);
   T fv[ZT][4], v[ZT][4];
-  double rr = 0.0;
+  double rr[ZT];  // MODE 3: per plane, the quad's r^2
 #pragma unroll
   for (int k = 0; k < ZT; ++k) {
     const uint64_t m = base + (mq | (s16::sp4(z0 + k) << 2));
@@ -1203,7 +1251,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
         s16::st4(cg.x + m, xq);
         s16::st4(cg.r + m, fq);
       }
-      rr += (double)fq.x * fq.x + (double)fq.y * fq.y + (double)fq.z * fq.z + (double)fq.w * fq.w;
+      rr[k] = (double)fq.x * fq.x + (double)fq.y * fq.y + (double)fq.z * fq.z + (double)fq.w * fq.w;
     } else {
       fq = s16::ld4(f + m);
     }
@@ -1219,9 +1267,9 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     // P ec on the quad column: coarse (cx, cx+1) x (cy, cy+1) at the coarse planes z0/2 .. z0/2+2
     // (z0 even: planes z0, z0+2 lie on a coarse plane, z0+1, z0+3 halfway between two)
     const int ax = x0 / 2 + 1, ay = y0 / 2 + 1, az = z0 / 2 + 1;
-    T pl[3][4];
+    T pl[ZT / 2 + 1][4];
 #pragma unroll
-    for (int w = 0; w < 3; ++w) {
+    for (int w = 0; w <= ZT / 2; ++w) {
       const T* c = ctile + ((az + w) * CW + ay) * CW + ax;
       const T c00 = c[0], c10 = c[1], c01 = c[CW], c11 = c[CW + 1];
       pl[w][0] = c00;
@@ -1230,12 +1278,9 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
       pl[w][3] = (T)0.25 * ((c00 + c10) + (c01 + c11));
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      v[0][e] += pl[0][e];
-      v[1][e] += (T)0.5 * (pl[0][e] + pl[1][e]);
-      v[2][e] += pl[1][e];
-      v[3][e] += (T)0.5 * (pl[1][e] + pl[2][e]);
-    }
+    for (int k = 0; k < ZT; ++k)  // even planes on a coarse plane, odd halfway between two
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[k][e] += (k & 1) ? (T)0.5 * (pl[k / 2][e] + pl[k / 2 + 1][e]) : pl[k / 2][e];
   }
 #pragma unroll
   for (int k = 0; k < ZT; ++k) {
@@ -1245,11 +1290,11 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     p0[RS] = v[k][2];
     p0[RS + 1] = v[k][3];
   }
-  s16::load_halo<T>(tile, xi, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); },
+  s16::load_halo<NT>(tile, xi, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); },
                     [&](uint32_t m) -> T { return FROM_ZERO ? (T)0 : __ldg(xi + m); });
   __syncthreads();
   if (MODE == 2) {  // add P ec on the halo shell (in-domain positions only)
-    for (int i = t; i < 1736; i += THREADS) {
+    for (int i = t; i < 1736; i += NT) {
       int ux, uy, uz;
       halo_u<16>(i, ux, uy, uz);
       const int gx = ox - 1 + ux, gy = oy - 1 + uy, gz = oz - 1 + uz;
@@ -1267,10 +1312,10 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     T nv[ZT];
     constexpr bool ZERO = FROM_ZERO && FWD;
     switch (cls) {
-      case 0: relax_column<T, 0, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
-      case 1: relax_column<T, 1, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
-      case 2: relax_column<T, 2, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
-      default: relax_column<T, 3, ZERO>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      case 0: relax_column<T, 0, ZERO, ZT>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      case 1: relax_column<T, 1, ZERO, ZT>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      case 2: relax_column<T, 2, ZERO, ZT>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
+      default: relax_column<T, 3, ZERO, ZT>(tile, x0, y0, z0, fv, v, ce, cc, c0inv, nv); break;
     }
     if (faces) {  // low-domain-face nodes of this column: their table rows, neighbours from the tile
 #pragma unroll 1
@@ -1286,12 +1331,14 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
           if (o == 13) continue;
           off += cm[o] * tile[ei + (o % 3 - 1) + RS * ((o / 3) % 3 - 1) + PS * (o / 9 - 1)];
         }
-        const T fk = k == 0 ? fv[0][cls] : (k == 1 ? fv[1][cls] : (k == 2 ? fv[2][cls] : fv[3][cls]));
+        T fk = fv[0][cls];
+#pragma unroll
+        for (int kk = 1; kk < ZT; ++kk)
+          if (kk == k) fk = fv[kk][cls];
         const T nvk = (fk - off) / cm[13];
-        if (k == 0) nv[0] = nvk;
-        else if (k == 1) nv[1] = nvk;
-        else if (k == 2) nv[2] = nvk;
-        else nv[3] = nvk;
+#pragma unroll
+        for (int kk = 0; kk < ZT; ++kk)
+          if (kk == k) nv[kk] = nvk;
       }
     }
     if (FACES) __syncthreads();  // same-class column neighbours were read with their old values
@@ -1302,21 +1349,24 @@ __global__ void __launch_bounds__(THREADS, sizeof(T) == 4 ? 4 : 2)
     }
     __syncthreads();
   }
-  double acc = 0.0;
+  double acc[ZT];  // DOT: per plane, the quad's f.x
 #pragma unroll
   for (int k = 0; k < ZT; ++k) {
     const uint64_t m = base + (mq | (s16::sp4(z0 + k) << 2));
     typename s16::Vec4<T>::type o;
     o.x = v[k][0]; o.y = v[k][1]; o.z = v[k][2]; o.w = v[k][3];
     s16::st4(xo + m, o);
+    acc[k] = 0.0;
     if (DOT)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc += (double)fv[k][e] * (double)v[k][e];
+      for (int e = 0; e < 4; ++e) acc[k] += (double)fv[k][e] * (double)v[k][e];
   }
   if (DOT || MODE == 3) {
-    typedef cub::BlockReduce<double, THREADS> BR;
-    __shared__ typename BR::TempStorage tmp;
-    const double sum = BR(tmp).Sum(MODE == 3 ? rr : acc);
+    // the last phase ended with a barrier: the tile's memory takes the per-plane sums
+    double* red = reinterpret_cast<double*>(smem_raw);
+#pragma unroll
+    for (int k = 0; k < ZT; ++k) red[(z0 + k) * 64 + qi] = MODE == 3 ? rr[k] : acc[k];
+    const double sum = s16::block_sum_fixed(red);
     if (t == 0) part[blk] = sum;
   }
 }
@@ -1377,13 +1427,120 @@ void smooth_dispatch(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f,
 #undef PR_SM
 }
 
+// ------------------------------------------------------------------ the z-segment autotuner
+// The 16^3 block kernels (SpMV, residual + restriction, smoother) run with ZT = 2, 4 or 8 z planes
+// per thread, i.e. 512, 256 or 128 threads per 16^3 brick: more planes per thread read fewer halo
+// planes from shared memory per node but leave fewer threads to hide latency.  Every ZT computes
+// the same values (per-block sums in a fixed order), so the choice is free and made by timing: the
+// first FP32 launch of a (kernel family, level, launch size) key times each ZT (one warm-up and
+// three timed launches on the launch's own buffers; every candidate writes what the real launch
+// then overwrites) and keeps the fastest for the process.  FP64 launches and launches inside a
+// stream capture use ZT = 4.  PR_AUTOTUNE=0 fixes ZT = 4; PR_ZT=2|4|8 forces one.
+enum TuneFamily { kTuneSpmv = 0, kTuneResid = 1, kTuneSmooth = 2, kTuneSmoothPost = 3 };
+struct TuneTable {
+  std::mutex mu;
+  std::map<std::tuple<int, int, int, int>, int> zt;  // (device, family, level, log2 blocks) -> ZT
+  std::string log;
+};
+TuneTable& tune_table() {
+  static TuneTable* t = new TuneTable();  // never destroyed
+  return *t;
+}
+const char* family_name(int f) {
+  return f == kTuneSpmv ? "spmv16" : (f == kTuneResid ? "resid16" : (f == kTuneSmooth ? "smooth16" : "smooth16-post"));
+}
+// PR_ZT_<FAMILY> (e.g. PR_ZT_SPMV16), else PR_ZT, forces a choice; read at every launch, so that a
+// process may switch
+int forced_zt(int family) {
+  auto valid = [](const char* v) { return v && (std::atoi(v) == 2 || std::atoi(v) == 4 || std::atoi(v) == 8); };
+  char name[32];
+  std::snprintf(name, sizeof(name), "PR_ZT_%s", family == kTuneSpmv ? "SPMV16" : (family == kTuneResid ? "RESID16" : "SMOOTH16"));
+  // (both smoother families answer to PR_ZT_SMOOTH16)
+  if (valid(std::getenv(name))) return std::atoi(std::getenv(name));
+  if (valid(std::getenv("PR_ZT"))) return std::atoi(std::getenv("PR_ZT"));
+  const char* a = std::getenv("PR_AUTOTUNE");
+  return (a && std::atoi(a) == 0) ? 4 : 0;
+}
+
+// Runs launch(zt) with the ZT of the key, timing the candidates first for a new key.
+template <typename L>
+void tuned_launch(cudaStream_t s, int family, uint32_t level, uint64_t blocks, bool tunable, L launch) {
+  if (!tunable) {
+    launch(4);
+    return;
+  }
+  if (const int f = forced_zt(family)) {
+    launch(f);
+    return;
+  }
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  int bin = 0;
+  while ((2ull << bin) <= blocks) ++bin;
+  const auto key = std::make_tuple(dev, family, (int)level, bin);
+  TuneTable& tt = tune_table();
+  {
+    std::lock_guard<std::mutex> g(tt.mu);
+    auto it = tt.zt.find(key);
+    if (it != tt.zt.end()) {
+      launch(it->second);
+      return;
+    }
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  PR_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    launch(4);
+    return;
+  }
+  cudaEvent_t e0, e1;
+  PR_CUDA(cudaEventCreate(&e0));
+  PR_CUDA(cudaEventCreate(&e1));
+  const int cand[3] = {2, 4, 8};
+  float ms[3];
+  for (int k = 0; k < 3; ++k) {
+    launch(cand[k]);
+    PR_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < 3; ++r) launch(cand[k]);
+    PR_CUDA(cudaEventRecord(e1, s));
+    PR_CUDA(cudaEventSynchronize(e1));
+    PR_CUDA(cudaEventElapsedTime(&ms[k], e0, e1));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int best = 1;  // ZT = 4 unless another is faster
+  for (int k = 0; k < 3; ++k)
+    if (ms[k] < ms[best]) best = k;
+  {
+    std::lock_guard<std::mutex> g(tt.mu);
+    tt.zt[key] = cand[best];
+    char line[200];
+    std::snprintf(line, sizeof(line), "%s level %u blocks 2^%d: ZT 2/4/8 = %.4f/%.4f/%.4f ms -> ZT %d\n",
+                  family_name(family), level, bin, ms[0] / 3, ms[1] / 3, ms[2] / 3, cand[best]);
+    tt.log += line;
+  }
+  launch(cand[best]);
+}
+
 template <typename T, int MODE, bool DOT, bool FWD, bool FACES>
 void launch_s16(cudaStream_t s, uint32_t D, const T* xi, T* xo, const T* f, const T* ec, const LevelCoef& L,
                 const T* table, double* part, uint32_t clouds) {
   const size_t sm = g16::smem_bytes<T>(MODE);
-  allow_smem(g16::k_smooth16<T, MODE, DOT, FWD, FACES>, sm);
-  g16::k_smooth16<T, MODE, DOT, FWD, FACES><<<dim3(1u << (3 * (D - 4)), clouds), g16::THREADS, sm, s>>>(
-      D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, CgFuse<T>());
+  const dim3 grid(1u << (3 * (D - 4)), clouds);
+  auto go = [&](auto z) {
+    constexpr int ZT = decltype(z)::value;
+    allow_smem(g16::k_smooth16<T, MODE, DOT, FWD, FACES, ZT>, sm);
+    g16::k_smooth16<T, MODE, DOT, FWD, FACES, ZT><<<grid, n16::Zt<ZT>::NT, sm, s>>>(
+        D, xi, xo, f, ec, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, CgFuse<T>());
+  };
+  constexpr bool kTunable = std::is_same<T, float>::value && MODE != 0;
+  tuned_launch(s, MODE == 2 ? kTuneSmoothPost : kTuneSmooth, D, (uint64_t)grid.x * grid.y, kTunable, [&](int zt) {
+    if constexpr (kTunable) {
+      if (zt == 2) return go(std::integral_constant<int, 2>());
+      if (zt == 8) return go(std::integral_constant<int, 8>());
+    }
+    go(std::integral_constant<int, 4>());
+  });
 }
 
 template <typename T, int MODE, bool DOT, bool FWD>
@@ -1485,9 +1642,22 @@ void mg_cg_update_presmooth(cudaStream_t s, const LevelCoef& L, const T* table, 
   const uint32_t D = L.depth;
   if (D < 4 || L.has_faces) throw Error(PR_ERR_INTERNAL, "the fused CG update needs the finest level, depth >= 4");
   const size_t sm = g16::smem_bytes<T>(3);
-  allow_smem(g16::k_smooth16<T, 3, false, true, false>, sm);
-  g16::k_smooth16<T, 3, false, true, false><<<dim3(1u << (3 * (D - 4)), clouds), g16::THREADS, sm, s>>>(
-      D, nullptr, xo, nullptr, nullptr, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, cg);
+  const dim3 grid(1u << (3 * (D - 4)), clouds);
+  auto go = [&](auto z) {
+    constexpr int ZT = decltype(z)::value;
+    allow_smem(g16::k_smooth16<T, 3, false, true, false, ZT>, sm);
+    g16::k_smooth16<T, 3, false, true, false, ZT><<<grid, n16::Zt<ZT>::NT, sm, s>>>(
+        D, nullptr, xo, nullptr, nullptr, (T)(1.0 / L.c0), (T)L.ce, (T)L.cc, table, part, cg);
+  };
+  // in place (x and r), so not timed: ZT = 4 unless forced
+  const int zt = std::is_same<T, float>::value && forced_zt(kTuneSmooth) ? forced_zt(kTuneSmooth) : 4;
+  if constexpr (std::is_same<T, float>::value) {
+    if (zt == 2) go(std::integral_constant<int, 2>());
+    else if (zt == 8) go(std::integral_constant<int, 8>());
+    else go(std::integral_constant<int, 4>());
+  } else {
+    go(std::integral_constant<int, 4>());
+  }
   PR_CHECK_LAUNCH();
 }
 
@@ -1499,15 +1669,25 @@ void mg_resid_restrict(cudaStream_t s, const LevelCoef& L, const T* table, const
   if (tile_for(D) == 16) {
     const size_t sm = r16::smem_bytes<T>();
     const unsigned nb = 1u << (3 * (D - 4));
-    if (L.has_faces) {
-      allow_smem(r16::k_resid16<T, true>, sm);
-      r16::k_resid16<T, true><<<dim3(nb, clouds), r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce,
-                                                                        (T)L.cc, table);
-    } else {
-      allow_smem(r16::k_resid16<T, false>, sm);
-      r16::k_resid16<T, false><<<dim3(nb, clouds), r16::THREADS, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce,
-                                                                         (T)L.cc, table);
-    }
+    auto go = [&](auto z, auto fcs) {
+      constexpr int ZT = decltype(z)::value;
+      constexpr bool FC = decltype(fcs)::value;
+      allow_smem(r16::k_resid16<T, FC, ZT>, sm);
+      r16::k_resid16<T, FC, ZT><<<dim3(nb, clouds), n16::Zt<ZT>::NT, sm, s>>>(D, e, f, fc, face, (T)L.c0, (T)L.ce,
+                                                                              (T)L.cc, table);
+    };
+    auto go_f = [&](auto z) {
+      if (L.has_faces) go(z, std::true_type());
+      else go(z, std::false_type());
+    };
+    constexpr bool kTunable = std::is_same<T, float>::value;
+    tuned_launch(s, kTuneResid, D, (uint64_t)nb * clouds, kTunable, [&](int zt) {
+      if constexpr (kTunable) {
+        if (zt == 2) return go_f(std::integral_constant<int, 2>());
+        if (zt == 8) return go_f(std::integral_constant<int, 8>());
+      }
+      go_f(std::integral_constant<int, 4>());
+    });
     PR_CHECK_LAUNCH();
     r16::k_restrict_faces<T><<<dim3((nb + 3) / 4, clouds), 768, 0, s>>>(D, face, fc, nb);
   } else {
@@ -1529,15 +1709,26 @@ void mg_spmv(cudaStream_t s, const LevelCoef& L, const T* table, const T* z, con
   if (tile_for(D) == 16) {
     const dim3 g(1u << (3 * (D - 4)), clouds);
     const size_t sm = n16::smem_bytes<T>();
-    if (xpby) {
-      allow_smem(n16::k_spmv16<T, 1, T>, sm);
-      n16::k_spmv16<T, 1, T><<<g, n16::THREADS, sm, s>>>(D, d, z, dn, (T)beta, q, (T)L.c0, (T)L.ce, (T)L.cc,
-                                                         nullptr, part, beta_dev);
-    } else {
-      allow_smem(n16::k_spmv16<T, 0, T>, sm);
-      n16::k_spmv16<T, 0, T><<<g, n16::THREADS, sm, s>>>(D, d, nullptr, nullptr, (T)0, q, (T)L.c0, (T)L.ce,
-                                                         (T)L.cc, nullptr, part, nullptr);
-    }
+    auto go = [&](auto zc) {
+      constexpr int ZT = decltype(zc)::value;
+      if (xpby) {
+        allow_smem(n16::k_spmv16<T, 1, T, ZT>, sm);
+        n16::k_spmv16<T, 1, T, ZT><<<g, n16::Zt<ZT>::NT, sm, s>>>(D, d, z, dn, (T)beta, q, (T)L.c0, (T)L.ce,
+                                                                  (T)L.cc, nullptr, part, beta_dev);
+      } else {
+        allow_smem(n16::k_spmv16<T, 0, T, ZT>, sm);
+        n16::k_spmv16<T, 0, T, ZT><<<g, n16::Zt<ZT>::NT, sm, s>>>(D, d, nullptr, nullptr, (T)0, q, (T)L.c0,
+                                                                  (T)L.ce, (T)L.cc, nullptr, part, nullptr);
+      }
+    };
+    constexpr bool kTunable = std::is_same<T, float>::value;
+    tuned_launch(s, kTuneSpmv, D, (uint64_t)g.x * g.y, kTunable, [&](int zt) {
+      if constexpr (kTunable) {
+        if (zt == 2) return go(std::integral_constant<int, 2>());
+        if (zt == 8) return go(std::integral_constant<int, 8>());
+      }
+      go(std::integral_constant<int, 4>());
+    });
   } else {
     if (clouds != 1 || beta_dev) throw Error(PR_ERR_INTERNAL, "packed SpMV needs depth >= 4");
     const unsigned nb = 1u << (3 * (D - 3));
@@ -1554,8 +1745,8 @@ void mg_resid_update(cudaStream_t s, const LevelCoef& L, const double* x, const 
   const uint32_t D = L.depth;
   if (D < 4 || L.has_faces) throw Error(PR_ERR_INTERNAL, "mg_resid_update needs the finest level, depth >= 4");
   const size_t sm = n16::smem_bytes<double>();
-  allow_smem(n16::k_spmv16<double, 2, E>, sm);
-  n16::k_spmv16<double, 2, E><<<dim3(1u << (3 * (D - 4)), clouds), n16::THREADS, sm, s>>>(
+  allow_smem(n16::k_spmv16<double, 2, E, 4>, sm);
+  n16::k_spmv16<double, 2, E, 4><<<dim3(1u << (3 * (D - 4)), clouds), n16::Zt<4>::NT, sm, s>>>(
       D, x, e, xn, scale, r, L.c0, L.ce, L.cc, b, nullptr, scale_dev);
   PR_CHECK_LAUNCH();
 }
@@ -1659,6 +1850,12 @@ double bench_one(pr_context* c, int kid, uint32_t D, int reps, double* bytes) {
   return (double)ms / reps;
 }
 }  // namespace
+
+std::string autotune_log() {
+  TuneTable& tt = tune_table();
+  std::lock_guard<std::mutex> g(tt.mu);
+  return tt.log;
+}
 
 double kernel_bench(pr_context* c, int kid, uint32_t D, int precision, int reps, double* bytes) {
   if (D < 4 || D > kMaxDepth) throw Error(PR_ERR_INVALID_ARGUMENT, "kernel bench depth must be in [4, 10]");

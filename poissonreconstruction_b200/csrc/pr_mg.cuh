@@ -66,6 +66,10 @@ void mg_resid_update(cudaStream_t s, const LevelCoef& L, const double* x, const 
 void sum_parts(cudaStream_t s, const double* part, int np, double scale2, const double* part2, int np2, double* out,
                uint32_t clouds = 1);
 
+// The z-segment choices of the 16^3 block kernels made so far in this process (one line per
+// kernel family, level and launch size, with the timings).
+std::string autotune_log();
+
 // Time `reps` launches of one kernel (ids: 0 spmv, 1 spmv+xpby, 2 smooth from zero,
 // 3 smooth, 4 smooth+prolongation+dot, 5 residual+restriction, 6 per-node stencil) at
 // depth D on context-owned buffers; returns ms per launch and the algorithmic bytes.

@@ -17,6 +17,8 @@
 // diagonal at depth >= 8; they only slow convergence, never prevent it).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "pr_mg.cuh"
@@ -220,6 +222,8 @@ struct Multigrid {
     return pk->fetch();
   }
   // z = M r; returns r.z per cloud.  presmoothed: a_D already holds the first sweep on r.
+  // After the first V-cycle of a solve (which runs plainly: the kernels' z segments are tuned on
+  // first use) the V-cycle is replayed from a CUDA graph kept by the context.
   std::vector<double> apply(const T* r, T* z, bool presmoothed = false) {
     const uint64_t n = 1ull << (3 * D);
     if (D == Dc) {
@@ -229,9 +233,44 @@ struct Multigrid {
       return pk->fetch();
     }
     double* part = c->buf<double>("mg_part", (size_t)mg_blocks(D) * clouds);
-    vcycle(D, r, z, part, presmoothed);
-    sum_parts(c->stream, part, (int)mg_blocks(D), 0.0, part, 0, pk->ds(Pack::kOut), clouds);
+    auto body = [&] {
+      vcycle(D, r, z, part, presmoothed);
+      sum_parts(c->stream, part, (int)mg_blocks(D), 0.0, part, 0, pk->ds(Pack::kOut), clouds);
+    };
+    const char* gr = std::getenv("PR_GRAPHS");
+    if (applies++ == 0 || (gr && std::atoi(gr) == 0)) body();
+    else c->run_graph(graph_key(r, z, part, presmoothed), body);
     return pk->fetch();
+  }
+  int applies = 0;
+  // everything a captured V-cycle depends on: sizes, the shift (kernel arguments), every buffer
+  std::string graph_key(const T* r, const T* z, const double* part, bool presmoothed) const {
+    char b[96];
+    std::snprintf(b, sizeof(b), "vcycle/%s/%u/%u/%d/%d/%a", tname<T>(), D, clouds, sweeps, presmoothed ? 1 : 0, pk->wg);
+    std::string k = b;
+    auto add = [&](const void* p) {
+      std::snprintf(b, sizeof(b), "/%p", p);
+      k += b;
+    };
+    add(r);
+    add(z);
+    add(part);
+    add(pk->ds(Pack::kOut));
+    add(tables);
+    add(inv);
+    for (uint32_t l = Dc; l <= D; ++l) {
+      add(f[l]);
+      add(e[l]);
+      add(a[l]);
+      add(t[l]);
+      add(face[l]);
+    }
+    for (const char* v : {"PR_ZT", "PR_AUTOTUNE", "PR_ZT_SPMV16", "PR_ZT_RESID16", "PR_ZT_SMOOTH16"}) {
+      const char* x = std::getenv(v);
+      k += "/";
+      k += x ? x : "-";
+    }
+    return k;
   }
 };
 
