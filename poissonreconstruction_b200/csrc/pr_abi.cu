@@ -482,10 +482,12 @@ bool packable(const pr_params& p, const double* pts, uint64_t n) {
 }
 // device bytes of one cloud of a pack: its context (input, setup, solution, extraction) and its
 // share of the packed solve's vectors
-double pack_cloud_bytes(const pr_params& p, uint64_t P) {
+double pack_ctx_bytes(const pr_params& p, uint64_t P) {
   const double nodes = std::ldexp(1.0, 3 * (int)p.depth), res2 = std::ldexp(1.0, 2 * (int)p.depth);
-  const double solver = (p.precision == PR_PRECISION_FP64 ? 96.0 : 64.0) * nodes;
-  return 20.0 * nodes + 800.0 * (double)P + 1000.0 * res2 + 64e6 + solver;
+  return 20.0 * nodes + 800.0 * (double)P + 1000.0 * res2 + 64e6;
+}
+double pack_solver_bytes(const pr_params& p) {
+  return (p.precision == PR_PRECISION_FP64 ? 96.0 : 64.0) * std::ldexp(1.0, 3 * (int)p.depth);
 }
 
 template <typename F>
@@ -510,6 +512,7 @@ void run_pack(BatchEngine& E, const std::vector<uint32_t>& pk, const double* con
               const pr_params* params, pr_mesh* out_meshes, pr_stats* out_stats, std::vector<int>& status,
               std::vector<std::string>& msgs) {
   const size_t m = pk.size();
+  const double tp0 = now_s();
   E.ensure(m);
   std::vector<pr_stats> st(m);
   std::vector<char> ok(m, 1);
@@ -538,6 +541,7 @@ void run_pack(BatchEngine& E, const std::vector<uint32_t>& pk, const double* con
       ok[j] = 0;
     }
   });
+  const double tp1 = now_s();
   std::vector<pr_context*> sc;
   std::vector<size_t> idx;
   for (size_t j = 0; j < m; ++j)
@@ -567,6 +571,7 @@ void run_pack(BatchEngine& E, const std::vector<uint32_t>& pk, const double* con
       sc[k]->coeffs_converged = true;
     }
   }
+  const double tp2 = now_s();
   parallel_for(m, hw, [&](size_t j) {  // iso value, marching cubes, mesh to host
     if (!ok[j]) return;
     const uint32_t i = pk[j];
@@ -589,6 +594,10 @@ void run_pack(BatchEngine& E, const std::vector<uint32_t>& pk, const double* con
       out_stats[i] = st[j];
     }
   });
+  const char* vb = std::getenv("PR_BATCH_VERBOSE");
+  if (vb && std::atoi(vb) != 0)
+    std::fprintf(stderr, "pr: pack of %zu: setup %.4f s, solve %.4f s, extract + copy %.4f s\n", m, tp1 - tp0,
+                 tp2 - tp1, now_s() - tp2);
 }
 
 void run_packed(int device, const std::map<PackKey, std::vector<uint32_t>>& groups, const double* const* points6,
@@ -608,29 +617,59 @@ void run_packed(int device, const std::map<PackKey, std::vector<uint32_t>>& grou
   });
   const char* lim = std::getenv("PR_PACK_MAX_CLOUDS");  // cap on the clouds of one pack (0: none)
   const size_t max_clouds = lim ? (size_t)std::strtoull(lim, nullptr, 10) : 0;
-  uint32_t depth = 0;
+  const char* vb = std::getenv("PR_BATCH_VERBOSE");
+  const bool verbose = vb && std::atoi(vb) != 0;
+  // Packs are sized against a fixed share of the device (PR_PACK_MEMORY_FRACTION, default 0.65)
+  // rather than against the free memory of the moment, so that every batch of the same clouds forms
+  // the same packs and reuses the buffers of the last one: the solver's vectors for the largest
+  // pack, and per context the largest cloud it served.  A group is split into packs of even size.
+  size_t free_b = 0, total_b = 0;
+  PR_CUDA(cudaSetDevice(device));
+  PR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const char* fr = std::getenv("PR_PACK_MEMORY_FRACTION");
+  const double frac = fr ? std::min(0.9, std::max(0.05, std::atof(fr))) : 0.65;
+  const double cap = frac * (double)total_b;
   for (std::vector<uint32_t> grp : order) {
     std::stable_sort(grp.begin(), grp.end(), [&](uint32_t a, uint32_t b) { return n[a] > n[b]; });
-    // a new depth: the packs of the previous one held buffers of other sizes, which the next
-    // clouds would not reuse
-    if (params[grp[0]].depth != depth && E.held() > 0) E.free_buffers();
-    depth = params[grp[0]].depth;
+    double sum = 0.0;
+    for (uint32_t i : grp) sum += pack_ctx_bytes(params[i], n[i]) + pack_solver_bytes(params[i]);
+    size_t packs = (size_t)std::max(1.0, std::ceil(sum / cap));
+    if (max_clouds) packs = std::max(packs, (grp.size() + max_clouds - 1) / max_clouds);
     size_t pos = 0;
-    while (pos < grp.size()) {
-      size_t free_b = 0, total_b = 0;
-      PR_CUDA(cudaSetDevice(device));
-      PR_CUDA(cudaMemGetInfo(&free_b, &total_b));
-      // the packs of this depth reuse the buffers held so far
-      const double budget = (double)free_b + (double)E.held() - std::max(8e9, 0.05 * (double)total_b);
+    for (size_t k = 0; k < packs && pos < grp.size(); ++k) {
+      // even split by estimated bytes (the clouds are largest first): the remaining bytes over the
+      // remaining packs, at least one cloud
+      double rest = 0.0;
+      for (size_t j = pos; j < grp.size(); ++j) rest += pack_ctx_bytes(params[grp[j]], n[grp[j]]) + pack_solver_bytes(params[grp[j]]);
+      const double share = rest / (double)(packs - k);
       std::vector<uint32_t> pk;
       double acc = 0.0;
       while (pos < grp.size()) {
-        const double b = pack_cloud_bytes(params[grp[pos]], n[grp[pos]]);
-        if (!pk.empty() && (acc + b > budget || (max_clouds && pk.size() >= max_clouds))) break;
-        pk.push_back(grp[pos++]);
+        const uint32_t i = grp[pos];
+        const double b = pack_ctx_bytes(params[i], n[i]) + pack_solver_bytes(params[i]);
+        if (!pk.empty() && (acc + 0.5 * b > share || (max_clouds && pk.size() >= max_clouds))) break;
+        pk.push_back(i);
         acc += b;
+        ++pos;
       }
+      if (k + 1 == packs)
+        while (pos < grp.size()) pk.push_back(grp[pos++]);  // (rounding) the last pack takes the rest
+      const double t0 = now_s();
       run_pack(E, pk, points6, n, params, out_meshes, out_stats, status, msgs);
+      bool oom = false;
+      for (uint32_t i : pk) oom = oom || status[i] == PR_ERR_OUT_OF_MEMORY;
+      if (oom && E.held() > 0) {  // other users took the memory: free the held buffers, try again once
+        for (uint32_t i : pk) {
+          pr_mesh_free(&out_meshes[i]);
+          status[i] = PR_OK;
+          msgs[i].clear();
+        }
+        E.free_buffers();
+        run_pack(E, pk, points6, n, params, out_meshes, out_stats, status, msgs);
+      }
+      if (verbose)
+        std::fprintf(stderr, "pr: pack depth=%u clouds=%zu est=%.2f GB held=%.2f GB %.4f s\n", params[pk[0]].depth,
+                     pk.size(), acc / 1e9, (double)E.held() / 1e9, now_s() - t0);
     }
   }
 }
