@@ -253,15 +253,20 @@ int pr_reconstruct_batch(const double* const* points6, const uint64_t* n, uint32
  * the normalised splat (src/fem_tree.rs:130-178), the divergence RHS and the screening RHS and
  * matrix.  M follows the bounding box of the input and is HELD FIXED (not differentiated).
  * Degree 1 (the crate's piecewise linear basis) and degree 2 (quadratic B-splines, the same
- * formulas with 27 nodes per point); dense grids only (not the adaptive band).  At a point exactly
- * on a cell face the one-sided derivative of the cell the point falls in is returned. */
+ * formulas with 27 nodes per point), dense grids and the adaptive band.  For the band, chi is the
+ * fine function (f on the band, the prolonged coarse solution elsewhere); the adjoint solves the
+ * band system (A_BB lambda = E^T g on the band) and then the coarse system with the right-hand side
+ * P^T (E^T g - A E lambda), and adds both levels' per-point terms; the brick set is held fixed.
+ * At a point exactly on a cell face the one-sided derivative of the cell the point falls in is
+ * returned. */
 typedef struct pr_adjoint_stats {
   double loss;          /* sum_k g_k chi_k, or mean chi_k^2 when dl_dchi was NULL */
   double rel_residual;  /* adjoint solve ||E^T g - A lambda|| / ||E^T g|| */
   uint32_t pcg_iterations;
   uint32_t refinement_steps;
   int32_t converged;
-  int32_t reserved_i;
+  int32_t queries_off_band; /* adaptive state: queries with a basis node outside the band (their
+                               terms go through the coarse function) */
   double time_solve;  /* seconds in the adjoint solve */
   double time_total;  /* seconds in the whole call */
   double reserved[4];

@@ -61,7 +61,7 @@ class PrStats(C.Structure):
 
 class PrAdjointStats(C.Structure):
     _fields_ = [("loss", C.c_double), ("rel_residual", C.c_double), ("pcg_iterations", C.c_uint32),
-                ("refinement_steps", C.c_uint32), ("converged", C.c_int32), ("reserved_i", C.c_int32),
+                ("refinement_steps", C.c_uint32), ("converged", C.c_int32), ("queries_off_band", C.c_int32),
                 ("time_solve", C.c_double), ("time_total", C.c_double), ("reserved", C.c_double * 4)]
 
 
@@ -301,6 +301,7 @@ class AdjointStats:
     pcg_iterations: int = 0
     refinement_steps: int = 0
     converged: int = 0
+    queries_off_band: int = 0
     time_solve: float = 0.0
     time_total: float = 0.0
 

@@ -891,7 +891,6 @@ static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k
   PR_REQUIRE(queries3 != nullptr, PR_ERR_INVALID_ARGUMENT, "queries is NULL");
   PR_REQUIRE(k >= 1 && k <= pr::kMaxPoints, PR_ERR_INVALID_ARGUMENT, "k must be in [1, 2^28] query points");
   PR_REQUIRE(c->have_state && c->have_coeffs, PR_ERR_STATE, "no solved reconstruction on this context");
-  PR_REQUIRE(!c->adaptive, PR_ERR_STATE, "the last reconstruction was adaptive: read it with the band accessors");
   PR_REQUIRE(c->coeffs_converged, PR_ERR_STATE,
              "the last solve used the reference schedule; the adjoint needs solve_mode PR_SOLVE_CONVERGED");
   for (uint64_t i = 0; i < 3 * k; ++i)
@@ -909,7 +908,8 @@ static void loss_backward_impl(pr_context* c, const double* queries3, uint64_t k
   double* dchi = c->buf<double>("adj_chi", k);
   double* dpos = c->buf<double>("adj_dpos", 3 * c->P);
   double* dnrm = c->buf<double>("adj_dnrm", 3 * c->P);
-  if (c->degree == 2) pr::adjoint_backward2(c, dq, k, ddl, dchi, dpos, dnrm, st);
+  if (c->adaptive) pr::adjoint_backward_band(c, dq, k, ddl, dchi, dpos, dnrm, st);
+  else if (c->degree == 2) pr::adjoint_backward2(c, dq, k, ddl, dchi, dpos, dnrm, st);
   else pr::adjoint_backward(c, dq, k, ddl, dchi, dpos, dnrm, st);
   if (chi) PR_CUDA(cudaMemcpyAsync(chi, dchi, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (dl_dpositions)

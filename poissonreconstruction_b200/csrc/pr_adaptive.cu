@@ -1060,6 +1060,8 @@ struct Band {
   }
 };
 
+void release_prefix(pr_context* c, const std::string& prefix);
+
 // Jacobi-preconditioned CG on A_BB x = r from x = 0 until ||r|| <= tol; r is overwritten with
 // the residual; returns the iterations.  Per iteration: one operator pass that forms the direction
 // d = z + beta dold and q = A d with d . q (plus the screening pass), and one update pass x, r, z
@@ -1121,6 +1123,56 @@ int band_pcg(Band& B, T* r, T* x, double tol, int maxit) {
     rz = h[1];
   }
   return it;
+}
+
+// A_BB e = r0 from e = 0 to ||r0 - A_BB e|| <= target ||b|| (bn = ||b||): Jacobi-PCG in FP32 with
+// FP64 residual refinement, or in FP64 throughout.  The band solve gets 10 x max_iters PCG
+// iterations (Jacobi preconditioning).  Returns the iterations; rn: the final residual norm.
+int band_solve(Band& B, const double* r0, double bn, double* e64, const pr_params& p, double& rn, uint32_t& refinements) {
+  pr_context* c = B.c;
+  const uint64_t n = B.n;
+  cudaStream_t s = c->stream;
+  double* r64 = c->buf<double>("ab_r64", std::max<uint64_t>(n, 1));
+  const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;
+  const int max_iters = 10 * (p.max_iters > 0 ? (int)p.max_iters : 200);
+  const bool mixed = p.precision != PR_PRECISION_FP64;
+  int used = 0;
+  refinements = 0;
+  PR_CUDA(cudaMemcpyAsync(r64, r0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  PR_CUDA(cudaMemsetAsync(e64, 0, n * sizeof(double), s));
+  rn = std::sqrt(dot<double>(c, r64, r64, n));
+  if (mixed) {
+    float* r32 = c->buf<float>("ab_r32", n);
+    float* e32 = c->buf<float>("ab_e32", n);
+    const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
+    while (rn > target * bn && used < max_iters) {
+      convert_norm(c, r64, r32, n);
+      const double tol = std::max(inner, 0.5 * target * bn / rn) * rn;
+      const int it = band_pcg<float>(B, r32, e32, tol, max_iters - used);
+      used += it;
+      axpy<float, double>(s, n, 1.0, e32, e64);
+      B.op<double, kBandResid>(e64, r0, r64);
+      const double rn_new = std::sqrt(dot<double>(c, r64, r64, n));
+      refinements++;
+      const bool stalled = it == 0 || !(rn_new < rn);
+      rn = rn_new;
+      if (stalled) break;
+    }
+  } else if (rn > target * bn) {
+    used = band_pcg<double>(B, r64, e64, 0.5 * target * bn, max_iters);
+    B.op<double, kBandResid>(e64, r0, r64);
+    rn = std::sqrt(dot<double>(c, r64, r64, n));
+  }
+  c->release("ab_r64");
+  c->release("ab_r32");
+  c->release("ab_e32");
+  release_prefix(c, "ab_z_");
+  release_prefix(c, "ab_d_");
+  release_prefix(c, "ab_dn_");
+  release_prefix(c, "ab_q_");
+  c->release("ab_part");
+  c->release("ab_part2");
+  return used;
 }
 
 void release_prefix(pr_context* c, const std::string& prefix) {
@@ -1325,63 +1377,26 @@ void stage_adaptive(pr_context* c, const pr_params& p, pr_stats& st, bool extrac
   const uint64_t n = B.n;
   const double* b = c->get<double>("ab_b");
   double* gB = c->buf<double>("ab_g", std::max<uint64_t>(n, 1));
-  double* r0 = c->buf<double>("ab_r0", std::max<uint64_t>(n, 1));
-  double* e64 = c->buf<double>("ab_e64", std::max<uint64_t>(n, 1));
-  double* r64 = c->buf<double>("ab_r64", std::max<uint64_t>(n, 1));
   const double target = p.target_rel_residual > 0.0 ? p.target_rel_residual : 1e-6;
-  // the band solve is Jacobi-preconditioned: it gets 10 x max_iters iterations of its own
-  const int max_iters = 10 * (p.max_iters > 0 ? (int)p.max_iters : 200);
-  const bool mixed = p.precision != PR_PRECISION_FP64;
   int used = 0;
   double bn = 0.0, rn = 0.0;
   st.pcg_iterations = sc.pcg_iterations;
   st.refinement_steps = 0;
   if (n > 0) {
+    double* r0 = c->buf<double>("ab_r0", n);
+    double* e64 = c->buf<double>("ab_e64", n);
     k_ab_prolong_band<<<brick_grid(B.NB), kThreads, 0, s>>>(B.bkey, B.NB, B.xc, B.W, B.res, gB);
     PR_CHECK_LAUNCH();
     B.launch_op<double, kBandResid, true>(nullptr, b, r0, nullptr, 0.0, nullptr);  // r0 = b - (K + wg) g
     B.screen<double>(gB, r0, -1.0, nullptr);
     bn = std::sqrt(dot<double>(c, b, b, n));
-    PR_CUDA(cudaMemcpyAsync(r64, r0, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    PR_CUDA(cudaMemsetAsync(e64, 0, n * sizeof(double), s));
-    rn = std::sqrt(dot<double>(c, r64, r64, n));
-    if (mixed) {
-      float* r32 = c->buf<float>("ab_r32", n);
-      float* e32 = c->buf<float>("ab_e32", n);
-      const double inner = p.inner_rel_tol > 0.0 ? p.inner_rel_tol : 1e-4;
-      while (rn > target * bn && used < max_iters) {
-        convert_norm(c, r64, r32, n);
-        const double tol = std::max(inner, 0.5 * target * bn / rn) * rn;
-        const int it = band_pcg<float>(B, r32, e32, tol, max_iters - used);
-        used += it;
-        axpy<float, double>(s, n, 1.0, e32, e64);
-        B.op<double, kBandResid>(e64, r0, r64);
-        const double rn_new = std::sqrt(dot<double>(c, r64, r64, n));
-        st.refinement_steps++;
-        const bool stalled = it == 0 || !(rn_new < rn);
-        rn = rn_new;
-        if (stalled) break;
-      }
-    } else if (rn > target * bn) {
-      used = band_pcg<double>(B, r64, e64, 0.5 * target * bn, max_iters);
-      B.op<double, kBandResid>(e64, r0, r64);
-      rn = std::sqrt(dot<double>(c, r64, r64, n));
-    }
+    used = band_solve(B, r0, bn, e64, p, rn, st.refinement_steps);
     double* f = c->buf<double>("ab_f", n);
     PR_CUDA(cudaMemcpyAsync(f, gB, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     axpy<double, double>(s, n, 1.0, e64, f);
   }
   c->release("ab_r0");
   c->release("ab_e64");
-  c->release("ab_r64");
-  c->release("ab_r32");
-  c->release("ab_e32");
-  release_prefix(c, "ab_z_");
-  release_prefix(c, "ab_d_");
-  release_prefix(c, "ab_dn_");
-  release_prefix(c, "ab_q_");
-  c->release("ab_part");
-  c->release("ab_part2");
   c->sync();
   double t3 = now_seconds();
   st.time_solve = (t1 - tc) + (t3 - t2);
@@ -1501,6 +1516,569 @@ void band_apply64(pr_context* c, const double* d_x, double* d_y) {
   Band B;
   B.init(c);
   if (B.n) B.op<double, kBandApply>(d_x, nullptr, d_y);
+}
+
+namespace {
+
+// ------------------------------------------------------------------ adjoint of the band
+// L = sum_q g_q chi(q), chi the fine function u = sum_B f_i phi_i + sum_H g_j phi_j (g = P x_c).
+// With w = d L / d u (the queries' basis values times g_q), the band equations R_B (A u - b) = 0
+// and the coarse system A_c x_c = b_c:
+//   A_BB lam = w_B                                   (band adjoint solve)
+//   A_c mu_c = P^T (w_H - E_H A_HB lam)              (coarse adjoint solve)
+// and every point's gradient is -lam^T (dA u - db) at depth D plus -mu_c^T (dA_c x_c - db_c) at
+// the coarse depth (the dense degree-2 adjoint's per-point terms, pr_adjoint.cu).  dL/dg =
+// w - A E lam (E: extension by zero), whose band rows w_B - A_BB lam vanish by the band adjoint
+// equation: they are dropped rather than formed as a difference (A_c is nearly singular on smooth
+// functions, and would amplify the solver's residual).  So only the ring of H nodes next to the
+// band (A_HB lam: the stiffness, the screening stays inside the band) and the queries' terms on H
+// nodes (w_H) reach the coarse level; with every brick active both are empty.
+
+// band index of the in-grid fine node (x, y, z), kSent when its brick is not active
+__device__ __forceinline__ uint32_t abj_index(const uint32_t* __restrict__ bmap, int64_t x, int64_t y, int64_t z) {
+  const uint32_t slot = bmap[morton3((uint32_t)(x >> 3), (uint32_t)(y >> 3), (uint32_t)(z >> 3))];
+  return slot == kSent ? kSent : slot * (uint32_t)kBN + (uint32_t)(((z & 7) << 6) | ((y & 7) << 3) | (x & 7));
+}
+
+// the coarse indices I (and taps k = f - 2^L I - kmin) of fine coordinate f: I in [lo, hi]
+__device__ __forceinline__ void abj_coarse_range(const Prolong& W, int64_t f, int& lo, int& hi) {
+  const int step = 1 << W.L;
+  lo = max(0, -floor_div((int)(W.kmax - f), step));  // ceil((f - kmax) / step)
+  hi = min(W.resc - 1, floor_div((int)(f - W.kmin), step));
+}
+
+// g at the in-grid fine node (x, y, z): the coarse function's depth-D coefficient
+__device__ double abj_prolong_node(const double* __restrict__ xc, const Prolong& W, int64_t x, int64_t y, int64_t z) {
+  const int step = 1 << W.L;
+  int lo[3], hi[3];
+  const int64_t f[3] = {x, y, z};
+  for (int a = 0; a < 3; ++a) abj_coarse_range(W, f[a], lo[a], hi[a]);
+  double v = 0.0;
+  for (int iz = lo[2]; iz <= hi[2]; ++iz) {
+    const double wz = W.w[f[2] - (int64_t)step * iz - W.kmin];
+    for (int iy = lo[1]; iy <= hi[1]; ++iy) {
+      const double wy = W.w[f[1] - (int64_t)step * iy - W.kmin];
+      for (int ix = lo[0]; ix <= hi[0]; ++ix)
+        v += W.w[f[0] - (int64_t)step * ix - W.kmin] * wy * wz *
+             xc[(int64_t)ix + (int64_t)W.resc * (iy + (int64_t)W.resc * iz)];
+    }
+  }
+  return v;
+}
+
+// chi at the queries (qu: 3 K, AoS unit coordinates) from f on the band and g elsewhere; missing:
+// the queries with a node outside the band
+__global__ void k_abj_eval(const double* __restrict__ qu, uint64_t K, uint32_t D, const uint32_t* __restrict__ bmap,
+                           const double* __restrict__ f, const double* __restrict__ xc, Prolong W,
+                           double* __restrict__ chi, unsigned long long* __restrict__ missing) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  unsigned long long cnt = 0;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < K; q += (uint64_t)gridDim.x * blockDim.x) {
+    int64_t c[3];
+    double b[3][3];
+    for (int a = 0; a < 3; ++a) axis2b(qu[3 * q + a], h, c[a], b[a]);
+    double v = 0.0;
+    bool miss = false;
+    for (int e = 0; e < 27; ++e) {
+      const int64_t x = c[0] + e % 3 - 1, y = c[1] + (e / 3) % 3 - 1, z = c[2] + e / 9 - 1;
+      if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res) continue;
+      const double phi = xmul(xmul(b[0][e % 3], b[1][(e / 3) % 3]), b[2][e / 9]);
+      const uint32_t j = abj_index(bmap, x, y, z);
+      double u;
+      if (j != kSent) {
+        u = f[j];
+      } else {
+        u = abj_prolong_node(xc, W, x, y, z);
+        miss = true;
+      }
+      v = xadd(v, xmul(u, phi));
+    }
+    chi[q] = v;
+    cnt += miss;
+  }
+  typedef cub::BlockReduce<unsigned long long, kThreads> BR;
+  __shared__ typename BR::TempStorage tmp;
+  const unsigned long long tot = BR(tmp).Sum(cnt);
+  if (threadIdx.x == 0 && tot) atomicAdd(missing, tot);
+}
+
+// dL/dchi: the upstream gradient, or d mean(chi^2) / d chi
+__global__ void k_abj_upstream(const double* __restrict__ chi, const double* __restrict__ dl, uint64_t K,
+                               double* __restrict__ g) {
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < K; q += (uint64_t)gridDim.x * blockDim.x)
+    g[q] = dl ? dl[q] : 2.0 * chi[q] / (double)K;
+}
+
+// (band node, 27 q + e) pairs of the queries' band nodes (kSent for the others) with the basis values
+__global__ void k_abj_pairs(const double* __restrict__ qu, uint64_t K, uint32_t D, const uint32_t* __restrict__ bmap,
+                            uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, double* __restrict__ phi) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 27 * K; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t q = i / 27;
+    const int e = (int)(i - 27 * q);
+    int64_t c[3];
+    double b[3][3];
+    for (int a = 0; a < 3; ++a) axis2b(qu[3 * q + a], h, c[a], b[a]);
+    const int64_t x = c[0] + e % 3 - 1, y = c[1] + (e / 3) % 3 - 1, z = c[2] + e / 9 - 1;
+    uint32_t key = kSent;
+    if (x >= 0 && y >= 0 && z >= 0 && x < res && y < res && z < res) key = abj_index(bmap, x, y, z);
+    keys[i] = key;
+    vals[i] = (uint32_t)i;
+    phi[i] = key != kSent ? xmul(xmul(b[0][e % 3], b[1][(e / 3) % 3]), b[2][e / 9]) : 0.0;
+  }
+}
+
+// w on the band: per run (band node), the pairs' phi g_q in query order
+__global__ void k_abj_scatter(const uint32_t* __restrict__ run_key, const uint32_t* __restrict__ run_off, uint64_t R,
+                              const uint32_t* __restrict__ sval, const double* __restrict__ phi,
+                              const double* __restrict__ g, double* __restrict__ w) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < R; r += (uint64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (uint32_t e = run_off[r]; e < run_off[r + 1]; ++e) acc += phi[sval[e]] * g[sval[e] / 27];
+    w[run_key[r]] = acc;
+  }
+}
+
+// P^T of the queries' terms on nodes outside the band (w_H), added to the coarse right-hand side
+__global__ void k_abj_missing(const double* __restrict__ qu, uint64_t K, uint32_t D, const uint32_t* __restrict__ bmap,
+                              const double* __restrict__ g, Prolong W, double* __restrict__ yc) {
+  const int64_t res = 1ll << D;
+  const double h = 1.0 / (double)res;
+  const int step = 1 << W.L;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < K; q += (uint64_t)gridDim.x * blockDim.x) {
+    int64_t c[3];
+    double b[3][3];
+    for (int a = 0; a < 3; ++a) axis2b(qu[3 * q + a], h, c[a], b[a]);
+    for (int e = 0; e < 27; ++e) {
+      const int64_t f[3] = {c[0] + e % 3 - 1, c[1] + (e / 3) % 3 - 1, c[2] + e / 9 - 1};
+      if (f[0] < 0 || f[1] < 0 || f[2] < 0 || f[0] >= res || f[1] >= res || f[2] >= res) continue;
+      if (abj_index(bmap, f[0], f[1], f[2]) != kSent) continue;
+      const double v = xmul(xmul(b[0][e % 3], b[1][(e / 3) % 3]), b[2][e / 9]) * g[q];
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; ++a) abj_coarse_range(W, f[a], lo[a], hi[a]);
+      for (int iz = lo[2]; iz <= hi[2]; ++iz)
+        for (int iy = lo[1]; iy <= hi[1]; ++iy)
+          for (int ix = lo[0]; ix <= hi[0]; ++ix)
+            atomicAdd(yc + (int64_t)ix + (int64_t)W.resc * (iy + (int64_t)W.resc * iz),
+                      v * W.w[f[0] - (int64_t)step * ix - W.kmin] * W.w[f[1] - (int64_t)step * iy - W.kmin] *
+                          W.w[f[2] - (int64_t)step * iz - W.kmin]);
+    }
+  }
+}
+
+// mu = h^2 (G M M, M G M, M M G)^T lam at the band's touched nodes (run keys), lam 0 off the band
+__global__ void k_abj_mu(const uint32_t* __restrict__ run_key, uint64_t T, const double* __restrict__ lam,
+                         const uint32_t* __restrict__ nbr, uint32_t D, BandCoef<double> K, double g0, double g1,
+                         double g3, double g4, double* __restrict__ mu) {
+  const double h = 1.0 / (double)(1u << D);
+  const double h2 = h * h;
+  const double gg[5] = {g0, g1, 0.0, g3, g4};
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < T; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t j = run_key[t];
+    const uint32_t slot = j / kBN, loc = j % kBN;
+    const int lx = (int)(loc & 7), ly = (int)((loc >> 3) & 7), lz = (int)(loc >> 6);
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+    for (int dz = -2; dz <= 2; ++dz) {
+      const int nz = lz - dz, bz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
+      for (int dy = -2; dy <= 2; ++dy) {
+        const int ny = ly - dy, by = ny < 0 ? -1 : (ny > 7 ? 1 : 0);
+        for (int dx = -2; dx <= 2; ++dx) {
+          const int nx = lx - dx, bx = nx < 0 ? -1 : (nx > 7 ? 1 : 0);
+          const uint32_t ns = nbr[27 * (uint64_t)slot + 9 * (bz + 1) + 3 * (by + 1) + (bx + 1)];
+          if (ns == kSent) continue;
+          const double l = lam[(uint64_t)ns * kBN + (uint32_t)((((nz - 8 * bz)) << 6) | ((ny - 8 * by) << 3) | (nx - 8 * bx))] * h2;
+          m0 += l * gg[dx + 2] * K.m[dy + 2] * K.m[dz + 2];
+          m1 += l * K.m[dx + 2] * gg[dy + 2] * K.m[dz + 2];
+          m2 += l * K.m[dx + 2] * K.m[dy + 2] * gg[dz + 2];
+        }
+      }
+    }
+    mu[t] = m0;
+    mu[T + t] = m1;
+    mu[2 * T + t] = m2;
+  }
+}
+
+// Per brick: -(K E lam) on the window of the brick and its 2-node ring (12^3) for the brick's own
+// lam, kept on the ring's H nodes (in the grid, in an inactive brick), then P^T of those into the
+// coarse right-hand side yc (atomic adds: the sums over bricks come in no fixed order).
+constexpr int kRW = 12, kRW3 = kRW * kRW * kRW;
+constexpr size_t kRestrictSmem = (kBN + 2 * 8 * 8 * kRW + 3 * 8 * kRW * kRW + kRW3 + 9 * kRW * kRW + 81 * kRW) *
+                                 sizeof(double);
+__global__ void __launch_bounds__(kThreads) k_abj_restrict(const double* __restrict__ lam, const uint32_t* __restrict__ nbr,
+                                                           const uint32_t* __restrict__ bkey, uint64_t NB,
+                                                           BandCoef<double> K, Prolong W, int res,
+                                                           double* __restrict__ yc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* lt = reinterpret_cast<double*>(smem_raw);  // [z][y][x] 8^3
+  double* am = lt + kBN;                              // [z][y][ox] 8 x 8 x 12
+  double* as = am + 8 * 8 * kRW;
+  double* mm = as + 8 * 8 * kRW;                      // [z][oy][ox] 8 x 12 x 12
+  double* ms = mm + 8 * kRW * kRW;
+  double* sm = ms + 8 * kRW * kRW;
+  double* tw = sm + 8 * kRW * kRW;                    // [oz][oy][ox] 12^3
+  double* r1 = tw + kRW3;                             // [cz][oy][ox] 9 x 12 x 12
+  double* r2 = r1 + 9 * kRW * kRW;                    // [cz][cy][ox] 9 x 9 x 12
+  const int t = threadIdx.x;
+  const int step = 1 << W.L;
+  for (uint64_t sl = blockIdx.x; sl < NB; sl += gridDim.x) {
+    uint32_t bx, by, bz;
+    unmorton3(bkey[sl], bx, by, bz);
+    const int o[3] = {8 * (int)bx - 2, 8 * (int)by - 2, 8 * (int)bz - 2};  // fine coordinate of window index 0
+    for (int i = t; i < kBN; i += kThreads) lt[i] = lam[sl * kBN + i];
+    __syncthreads();
+    for (int i = t; i < 8 * 8 * kRW; i += kThreads) {  // x filters
+      const int ox = i % kRW, zy = i / kRW;
+      double a = 0.0, b = 0.0;
+      for (int ix = max(0, ox - 4); ix <= min(7, ox); ++ix) {
+        const int d = ox - 2 - ix + 2;
+        a += K.m[d] * lt[zy * 8 + ix];
+        b += K.s[d] * lt[zy * 8 + ix];
+      }
+      am[i] = a;
+      as[i] = b;
+    }
+    __syncthreads();
+    for (int i = t; i < 8 * kRW * kRW; i += kThreads) {  // y filters
+      const int ox = i % kRW, oy = (i / kRW) % kRW, z = i / (kRW * kRW);
+      double a = 0.0, b = 0.0, c = 0.0;
+      for (int iy = max(0, oy - 4); iy <= min(7, oy); ++iy) {
+        const int d = oy - 2 - iy + 2;
+        const double xm = am[(z * 8 + iy) * kRW + ox], xs = as[(z * 8 + iy) * kRW + ox];
+        a += K.m[d] * xm;
+        b += K.s[d] * xm;
+        c += K.m[d] * xs;
+      }
+      mm[i] = a;
+      ms[i] = b;
+      sm[i] = c;
+    }
+    __syncthreads();
+    for (int i = t; i < kRW3; i += kThreads) {  // z filters; H nodes of the ring only
+      const int ox = i % kRW, oy = (i / kRW) % kRW, oz = i / (kRW * kRW);
+      const int bxo = ox < 2 ? -1 : (ox >= 10 ? 1 : 0), byo = oy < 2 ? -1 : (oy >= 10 ? 1 : 0),
+                bzo = oz < 2 ? -1 : (oz >= 10 ? 1 : 0);
+      const int fx = o[0] + ox, fy = o[1] + oy, fz = o[2] + oz;
+      bool h_node = (bxo | byo | bzo) != 0 && fx >= 0 && fy >= 0 && fz >= 0 && fx < res && fy < res && fz < res;
+      if (h_node) h_node = nbr[27 * sl + 9 * (bzo + 1) + 3 * (byo + 1) + (bxo + 1)] == kSent;
+      double val = 0.0;
+      if (h_node) {
+        double a = 0.0;
+        for (int iz = max(0, oz - 4); iz <= min(7, oz); ++iz) {
+          const int d = oz - 2 - iz + 2;
+          const int j = (iz * kRW + oy) * kRW + ox;
+          a += K.m[d] * (sm[j] + ms[j]) + K.s[d] * mm[j];
+        }
+        val = -K.H * a;
+      }
+      tw[i] = val;
+    }
+    __syncthreads();
+    int lo[3], cnt[3];
+    for (int a = 0; a < 3; ++a) {
+      int l, hh;
+      abj_coarse_range(W, o[a], l, hh);
+      int l2, h2;
+      abj_coarse_range(W, o[a] + kRW - 1, l2, h2);
+      lo[a] = l;
+      cnt[a] = max(0, h2 - l + 1);
+    }
+    for (int i = t; i < cnt[2] * kRW * kRW; i += kThreads) {  // z: fine planes -> coarse planes
+      const int yx = i % (kRW * kRW), cz = i / (kRW * kRW);
+      const int I = lo[2] + cz;
+      double a = 0.0;
+      for (int oz = 0; oz < kRW; ++oz) {
+        const int k = o[2] + oz - step * I - W.kmin;
+        if (k >= 0 && k <= W.kmax - W.kmin) a += W.w[k] * tw[oz * kRW * kRW + yx];
+      }
+      r1[i] = a;
+    }
+    __syncthreads();
+    for (int i = t; i < cnt[2] * cnt[1] * kRW; i += kThreads) {  // y
+      const int ox = i % kRW, cy = (i / kRW) % cnt[1], cz = i / (kRW * cnt[1]);
+      const int I = lo[1] + cy;
+      double a = 0.0;
+      for (int oy = 0; oy < kRW; ++oy) {
+        const int k = o[1] + oy - step * I - W.kmin;
+        if (k >= 0 && k <= W.kmax - W.kmin) a += W.w[k] * r1[(cz * kRW + oy) * kRW + ox];
+      }
+      r2[i] = a;
+    }
+    __syncthreads();
+    for (int i = t; i < cnt[2] * cnt[1] * cnt[0]; i += kThreads) {  // x, then into the coarse grid
+      const int cx = i % cnt[0], cy = (i / cnt[0]) % cnt[1], cz = i / (cnt[0] * cnt[1]);
+      const int I = lo[0] + cx;
+      double a = 0.0;
+      for (int ox = 0; ox < kRW; ++ox) {
+        const int k = o[0] + ox - step * I - W.kmin;
+        if (k >= 0 && k <= W.kmax - W.kmin) a += W.w[k] * r2[(cz * cnt[1] + cy) * kRW + ox];
+      }
+      if (a != 0.0)
+        atomicAdd(yc + (int64_t)I + (int64_t)W.resc * ((lo[1] + cy) + (int64_t)W.resc * (lo[2] + cz)), a);
+    }
+    __syncthreads();
+  }
+}
+
+// Mat4::transform_point (src/geometry.rs:256-262), the forward transform's operation order
+__global__ void k_abj_query_unit(const double* __restrict__ q3, uint64_t K, Mat16 M, double* __restrict__ qu) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < K; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double* p = q3 + 3 * i;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      qu[3 * i + r] =
+          xadd(xadd(xadd(xmul(M.m[r], p[0]), xmul(M.m[4 + r], p[1])), xmul(M.m[8 + r], p[2])), M.m[12 + r]);
+  }
+}
+
+}  // namespace
+
+void adjoint_backward_band(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
+                           double* d_dpos, double* d_dnrm, pr_adjoint_stats& st) {
+  cudaStream_t s = c->stream;
+  const uint32_t D = c->D, Dc = c->band_Dc;
+  const uint64_t NB = c->band_nb, n = c->n, P = c->P, T = c->T, S = c->S, Pin = c->P_in, Spairs = c->S_pairs;
+  const double pw = c->pw;
+  const pr_params prm = c->params;
+  PR_REQUIRE(NB > 0, PR_ERR_STATE, "the adaptive reconstruction has no active bricks");
+  Band B;
+  B.init(c);
+  const uint32_t nres = 1u << (D - 3);
+  const uint64_t nall = (uint64_t)nres * nres * nres;
+  uint32_t* bmap = c->buf<uint32_t>("ab_bmap", nall);
+  PR_CUDA(cudaMemsetAsync(bmap, 0xff, nall * sizeof(uint32_t), s));
+  k_ab_brick_map<<<grid_for(NB), kThreads, 0, s>>>(B.bkey, NB, bmap);
+  PR_CHECK_LAUNCH();
+  // chi and dL/dchi at the queries
+  Mat16 M;
+  for (int k = 0; k < 16; ++k) M.m[k] = c->M[k];
+  double* qu = c->buf<double>("abj_qu", 3 * K);
+  k_abj_query_unit<<<grid_for(K), kThreads, 0, s>>>(d_q3, K, M, qu);
+  PR_CHECK_LAUNCH();
+  const double* f = c->get<double>("ab_f");
+  unsigned long long* miss = c->buf<unsigned long long>("abj_miss", 1);
+  PR_CUDA(cudaMemsetAsync(miss, 0, sizeof(unsigned long long), s));
+  k_abj_eval<<<grid_for(K), kThreads, 0, s>>>(qu, K, D, bmap, f, B.xc, B.W, d_chi, miss);
+  PR_CHECK_LAUNCH();
+  double* g = c->buf<double>("abj_g", K);
+  k_abj_upstream<<<grid_for(K), kThreads, 0, s>>>(d_chi, d_dl, K, g);
+  PR_CHECK_LAUNCH();
+  st.loss = d_dl ? dot<double>(c, d_dl, d_chi, K) : dot<double>(c, d_chi, d_chi, K) / (double)K;
+  unsigned long long h_miss = 0;
+  PR_CUDA(cudaMemcpyAsync(&h_miss, miss, sizeof(h_miss), cudaMemcpyDeviceToHost, s));
+  // w on the band: the queries' (band node, term) pairs sorted by node, summed in query order
+  double* w = c->buf<double>("abj_w", n);
+  PR_CUDA(cudaMemsetAsync(w, 0, n * sizeof(double), s));
+  {
+    uint32_t* kin = c->buf<uint32_t>("abj_kin", 27 * K);
+    uint32_t* vin = c->buf<uint32_t>("abj_vin", 27 * K);
+    double* qphi = c->buf<double>("abj_phi", 27 * K);
+    k_abj_pairs<<<grid_for(27 * K, 1u << 20), kThreads, 0, s>>>(qu, K, D, bmap, kin, vin, qphi);
+    PR_CHECK_LAUNCH();
+    // the band's own sorted pairs ("abs_*") stay: sort the queries' under other names
+    uint32_t* keys = c->buf<uint32_t>("abjs_key", 27 * K);
+    uint32_t* vals = c->buf<uint32_t>("abjs_val", 27 * K);
+    uint32_t* rkey = c->buf<uint32_t>("abjs_runkey", 27 * K);
+    uint32_t* rcnt = c->buf<uint32_t>("abjs_runcnt", 27 * K + 1);
+    uint32_t* roff = c->buf<uint32_t>("abjs_runoff", 27 * K + 1);
+    uint32_t* nrun = c->buf<uint32_t>("abjs_nrun", 1);
+    const int64_t m = (int64_t)(27 * K);
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, kin, keys, vin, vals, m, 0, 32, s));
+    PR_CUDA(cub::DeviceRunLengthEncode::Encode(nullptr, b2, keys, rkey, rcnt, nrun, m, s));
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b3, rcnt, roff, m + 1, s));
+    size_t tb = std::max(b1, std::max(b2, b3));
+    void* tmp = c->buf<char>("abj_cub_tmp", tb);
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, keys, vin, vals, m, 0, 32, s));
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceRunLengthEncode::Encode(tmp, tb, keys, rkey, rcnt, nrun, m, s));
+    uint32_t h_nrun = 0, h_last = 0;
+    PR_CUDA(cudaMemcpyAsync(&h_nrun, nrun, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    c->sync();
+    if (h_nrun > 0) {
+      PR_CUDA(cudaMemcpyAsync(&h_last, rkey + (h_nrun - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      c->sync();
+    }
+    uint64_t R = h_nrun;
+    if (R > 0 && h_last == kSent) --R;
+    PR_CUDA(cudaMemsetAsync(rcnt + R, 0, sizeof(uint32_t), s));
+    PR_COUNT_PRIMITIVE();
+    PR_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, rcnt, roff, (int64_t)(R + 1), s));
+    if (R > 0) {
+      k_abj_scatter<<<grid_for(R, 1u << 20), kThreads, 0, s>>>(rkey, roff, R, vals, qphi, g, w);
+      PR_CHECK_LAUNCH();
+    }
+    release_prefix(c, "abjs_");
+    c->release("abj_kin");
+    c->release("abj_vin");
+    c->release("abj_phi");
+    c->release("abj_cub_tmp");
+  }
+  // band adjoint solve A_BB lam = w_B
+  double* lam = c->buf<double>("abj_lam", n);
+  c->sync();
+  const double t0 = now_seconds();
+  const double wn = std::sqrt(dot<double>(c, w, w, n));
+  double rn = 0.0;
+  uint32_t refine = 0;
+  int used = 0;
+  if (wn > 0.0) used = band_solve(B, w, wn, lam, prm, rn, refine);
+  else PR_CUDA(cudaMemsetAsync(lam, 0, n * sizeof(double), s));
+  c->sync();
+  const double t_band = now_seconds() - t0;
+  const double target = prm.target_rel_residual > 0.0 ? prm.target_rel_residual : 1e-6;
+  const double band_rel = wn > 0.0 ? rn / wn : 0.0;
+  // the fine level's per-point terms (the band's pairs, runs, normal field; lam and u = f)
+  const double h = 1.0 / (double)(1u << D);
+  const double wh3 = pw > 0.0 ? pw * h * h * h / 1.5 : 0.0;
+  if (T > 0) {
+    double* nfc = c->buf<double>("ab_nfc", 3 * T);
+    double* sphi = c->buf<double>("ab_sphi", T);
+    double* sphi2 = c->buf<double>("ab_sphi2", T);
+    k_ab_splat<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("abs_runoff"), T, c->get<uint32_t>("abs_val"),
+                                                          c->get<double>("ab_phi64"), c->get<double>("unrm"), P, nfc,
+                                                          sphi, sphi2);
+    PR_CHECK_LAUNCH();
+    double* mu = c->buf<double>("abj_mu", 3 * T);
+    double m5[5], s5[5], g5[5];
+    deg2_constants(m5, s5, g5);
+    k_abj_mu<<<grid_for(T, 1u << 20), kThreads, 0, s>>>(c->get<uint32_t>("abs_runkey"), T, lam, B.nbr, D,
+                                                        band_coef<double>(D, pw), g5[0], g5[1], g5[3], g5[4], mu);
+    PR_CHECK_LAUNCH();
+    double* wt = c->buf<double>("abj_wt", T);
+    uint32_t* runidx = c->buf<uint32_t>("abj_runidx", 27 * P);
+    run_weights2(c, c->get<uint32_t>("abs_runoff"), T, c->get<uint32_t>("abs_val"), c->get<double>("ab_phi64"), wt,
+                 runidx);
+    PointGrad2In a;
+    a.upos = c->get<double>("upos");
+    a.unrm = c->get<double>("unrm");
+    a.ulen = c->get<double>("ulen");
+    a.P = P;
+    a.D = D;
+    a.key = c->get<uint32_t>("ab_kin");
+    a.sentinel = kSent;
+    a.runidx = runidx;
+    a.nfc = nfc;
+    a.nfc_aos = 1;
+    a.w = wt;
+    a.mu = mu;
+    a.T = T;
+    a.lam = lam;
+    a.x = f;
+    a.wh3 = wh3;
+    a.s = c->M[0];
+    a.dpos = d_dpos;
+    a.dnrm = d_dnrm;
+    a.accumulate = 0;
+    point_grad2(c, a);
+    c->sync();
+    c->release("ab_nfc");
+    c->release("ab_sphi");
+    c->release("abj_mu");
+    c->release("abj_wt");
+    c->release("abj_runidx");
+  } else {
+    PR_CUDA(cudaMemsetAsync(d_dpos, 0, 3 * P * sizeof(double), s));
+    PR_CUDA(cudaMemsetAsync(d_dnrm, 0, 3 * P * sizeof(double), s));
+  }
+  // the coarse right-hand side P^T (w_H - E_H A_HB lam)
+  const uint64_t ncs = 1ull << (3 * Dc);
+  double* yc = c->buf<double>("abj_yc", ncs);
+  PR_CUDA(cudaMemsetAsync(yc, 0, ncs * sizeof(double), s));
+  allow_smem(k_abj_restrict, kRestrictSmem);
+  k_abj_restrict<<<brick_grid(NB), kThreads, kRestrictSmem, s>>>(lam, B.nbr, B.bkey, NB, band_coef<double>(D, pw),
+                                                                 B.W, B.res, yc);
+  PR_CHECK_LAUNCH();
+  if (h_miss > 0) {
+    k_abj_missing<<<grid_for(K), kThreads, 0, s>>>(qu, K, D, bmap, g, B.W, yc);
+    PR_CHECK_LAUNCH();
+  }
+  c->sync();
+  c->release("abj_w");
+  c->release("ab_bmap");
+  c->release("abj_qu");
+  c->release("abj_g");
+  // the coarse adjoint: the dense degree-2 system at the coarse depth (set up again), A_c mu_c = yc,
+  // and its per-point terms with mu_c and x_c, added
+  double* xc_keep = c->buf<double>("abj_xc", ncs);
+  PR_CUDA(cudaMemcpyAsync(xc_keep, B.xc, ncs * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  pr_params pc = prm;
+  pc.depth = Dc;
+  pc.coarse_depth = 0;
+  stage_setup_deg2(c, Dc, pw);
+  pr_stats sst;
+  std::memset(&sst, 0, sizeof(sst));
+  c->sync();
+  const double t1 = now_seconds();
+  solve_deg2(c, pc, sst, yc);
+  c->sync();
+  const double t_coarse = now_seconds() - t1;
+  const uint64_t Tc = c->T;
+  if (Tc > 0) {
+    double* muc = c->buf<double>("abj_muc", 3 * Tc);
+    mu2_dense(c, c->get<uint32_t>("d2s_runkey"), Tc, c->d2_xnat, Dc, muc);
+    double* wc = c->buf<double>("abj_wc", Tc);
+    uint32_t* runidx = c->buf<uint32_t>("abj_runidx", 27 * P);
+    run_weights2(c, c->get<uint32_t>("d2s_runoff"), Tc, c->get<uint32_t>("d2s_val"), c->get<double>("d2_phi64"), wc,
+                 runidx);
+    const double hc = 1.0 / (double)(1u << Dc);
+    PointGrad2In a;
+    a.upos = c->get<double>("upos");
+    a.unrm = c->get<double>("unrm");
+    a.ulen = c->get<double>("ulen");
+    a.P = P;
+    a.D = Dc;
+    a.key = c->get<uint32_t>("d2_kin");
+    a.sentinel = 1u << (3 * Dc);
+    a.runidx = runidx;
+    a.nfc = c->get<double>("d2_nfc");
+    a.w = wc;
+    a.mu = muc;
+    a.T = Tc;
+    a.lam = c->d2_xnat;
+    a.x = xc_keep;
+    a.wh3 = pw > 0.0 ? pw * hc * hc * hc / 1.5 : 0.0;
+    a.s = c->M[0];
+    a.dpos = d_dpos;
+    a.dnrm = d_dnrm;
+    a.accumulate = 1;
+    point_grad2(c, a);
+    c->sync();
+    c->release("abj_muc");
+    c->release("abj_wc");
+    c->release("abj_runidx");
+  }
+  // back to the band state
+  c->d2_xnat = nullptr;
+  release_prefix(c, "d2");
+  release_prefix(c, "cub_tmp");
+  c->release("abj_yc");
+  c->release("abj_xc");
+  c->release("abj_lam");
+  c->D = D;
+  c->n = n;
+  c->T = T;
+  c->S = S;
+  c->S_pairs = Spairs;
+  c->P_in = Pin;
+  c->pw = pw;
+  c->band_Dc = Dc;
+  c->band_nb = NB;
+  c->adaptive = true;
+  c->degree = 2;
+  c->params = prm;
+  c->have_state = true;
+  c->have_coeffs = true;
+  c->coeffs_converged = true;
+  st.time_solve = t_band + t_coarse;
+  st.pcg_iterations = (uint32_t)used + sst.pcg_iterations;
+  st.refinement_steps = refine + sst.refinement_steps;
+  st.rel_residual = std::max(band_rel, sst.rel_residual);
+  st.converged = band_rel <= target && sst.converged ? 1 : 0;
+  st.queries_off_band = (int32_t)std::min<unsigned long long>(h_miss, 0x7fffffff);
 }
 
 }  // namespace pr

@@ -377,29 +377,9 @@ __global__ void k_run_weights2(const uint32_t* __restrict__ run_off, uint64_t T,
   }
 }
 
-struct PointGrad2Args {
-  const double* upos;
-  const double* unrm;
-  const double* ulen;
-  uint64_t P;
-  uint32_t D;
-  const uint32_t* key;     // 27 P natural node keys (sentinel outside the grid)
-  const uint32_t* runidx;  // 27 P: the pair's run (touched node)
-  const double* nfc;       // 3 x T compact normal field
-  const double* w;         // T
-  const double* mu;        // 3 x T
-  uint64_t T;
-  const double* lam;  // n, natural
-  const double* x;    // n, natural
-  double wh3;
-  double s;
-  double* dpos;
-  double* dnrm;
-};
-
-__global__ void k_point_grad2(PointGrad2Args a) {
+__global__ void k_point_grad2(PointGrad2In a) {
   const double h = 1.0 / (double)(1u << a.D);
-  const uint32_t sentinel = 1u << (3 * a.D);
+  const uint32_t sentinel = a.sentinel;
   for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < a.P; p += (uint64_t)gridDim.x * blockDim.x) {
     const double nu[3] = {a.unrm[p], a.unrm[a.P + p], a.unrm[2 * a.P + p]};
     int64_t c[3];
@@ -418,7 +398,8 @@ __global__ void k_point_grad2(PointGrad2Args a) {
       const double wt = a.w[t];
       if (wt > 0.0) {  // splat
         const double m[3] = {a.mu[t], a.mu[a.T + t], a.mu[2 * a.T + t]};
-        const double nf[3] = {a.nfc[t], a.nfc[a.T + t], a.nfc[2 * a.T + t]};
+        const double nf[3] = {a.nfc[a.nfc_aos ? 3 * t : t], a.nfc[a.nfc_aos ? 3 * t + 1 : a.T + t],
+                              a.nfc[a.nfc_aos ? 3 * t + 2 : 2 * a.T + t]};
         const double sdot = m[0] * (nu[0] + nf[0]) + m[1] * (nu[1] + nf[1]) + m[2] * (nu[2] + nf[2]);
         for (int k = 0; k < 3; ++k) {
           gn[k] -= phi / wt * m[k];
@@ -440,13 +421,34 @@ __global__ void k_point_grad2(PointGrad2Args a) {
     const double len = a.ulen[p];
     const double ng = nu[0] * gn[0] + nu[1] * gn[1] + nu[2] * gn[2];
     for (int k = 0; k < 3; ++k) {
-      a.dpos[3 * p + k] = a.s * gu[k];
-      a.dnrm[3 * p + k] = len > 0.0 ? a.s / len * (gn[k] - nu[k] * ng) : 0.0;
+      const double dp = a.s * gu[k], dn = len > 0.0 ? a.s / len * (gn[k] - nu[k] * ng) : 0.0;
+      a.dpos[3 * p + k] = a.accumulate ? a.dpos[3 * p + k] + dp : dp;
+      a.dnrm[3 * p + k] = a.accumulate ? a.dnrm[3 * p + k] + dn : dn;
     }
   }
 }
 
 }  // namespace
+
+void point_grad2(pr_context* c, const PointGrad2In& a) {
+  if (a.P == 0) return;
+  k_point_grad2<<<grid_for(a.P), kThreads, 0, c->stream>>>(a);
+  PR_CHECK_LAUNCH();
+}
+void run_weights2(pr_context* c, const uint32_t* run_off, uint64_t T, const uint32_t* sval, const double* phi, double* w,
+                  uint32_t* runidx) {
+  if (T == 0) return;
+  k_run_weights2<<<grid_for(T), kThreads, 0, c->stream>>>(run_off, T, sval, phi, w, runidx);
+  PR_CHECK_LAUNCH();
+}
+void mu2_dense(pr_context* c, const uint32_t* run_key, uint64_t T, const double* lam, uint32_t D, double* mu) {
+  if (T == 0) return;
+  Deg2K k;
+  double s5[5];
+  deg2_constants(k.m, s5, k.g);
+  k_mu2<<<grid_for(T), kThreads, 0, c->stream>>>(run_key, T, lam, D, k, mu);
+  PR_CHECK_LAUNCH();
+}
 
 void adjoint_backward2(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
                        double* d_dpos, double* d_dnrm, pr_adjoint_stats& st) {
@@ -513,7 +515,9 @@ void adjoint_backward2(pr_context* c, const double* d_q3, uint64_t K, const doub
     PR_CHECK_LAUNCH();
   }
   const double h = 1.0 / (double)(1u << D);
-  PointGrad2Args a;
+  PointGrad2In a;
+  a.sentinel = 1u << (3 * D);
+  a.accumulate = 0;
   a.upos = c->get<double>("upos");
   a.unrm = c->get<double>("unrm");
   a.ulen = c->get<double>("ulen");
@@ -531,8 +535,7 @@ void adjoint_backward2(pr_context* c, const double* d_q3, uint64_t K, const doub
   a.s = c->M[0];
   a.dpos = d_dpos;
   a.dnrm = d_dnrm;
-  k_point_grad2<<<grid_for(P), kThreads, 0, s>>>(a);
-  PR_CHECK_LAUNCH();
+  point_grad2(c, a);
   c->release("adj_runidx");
 }
 

@@ -309,6 +309,43 @@ void stage_setup_deg2(pr_context* c, uint32_t depth, double pw);
 void stage_solve_deg2(pr_context* c, const pr_params& p, pr_stats& st);
 // A x = b with the degree-2 system of the context (natural order); the solution at c->d2_xnat
 void solve_deg2(pr_context* c, const pr_params& p, pr_stats& st, const double* b);
+// Pieces of the degree-2 adjoint (pr_adjoint.cu), shared by the dense grid and the adaptive band.
+// Per point p: the gradient of L = lam^T (b - A x) w.r.t. its unit-cube position and normal, b and A
+// the degree-2 system's (splat of the normals, screening) at depth D; key: 27 P node indices into
+// lam and x (sentinel: no node), runidx: 27 P runs (touched nodes) of the pairs, nfc / w / mu: the
+// runs' normal field, basis sums and the divergence stencil applied to lam (3 x T).  Writes (or with
+// accumulate adds) s x the gradients into dpos / dnrm (P x 3 each, model space by s = M[0]).
+struct PointGrad2In {
+  const double* upos = nullptr;
+  const double* unrm = nullptr;
+  const double* ulen = nullptr;
+  uint64_t P = 0;
+  uint32_t D = 0;
+  const uint32_t* key = nullptr;
+  uint32_t sentinel = 0;
+  const uint32_t* runidx = nullptr;
+  const double* nfc = nullptr;
+  int nfc_aos = 0;  // nfc as [T][3] (the band's) rather than [3][T]
+  const double* w = nullptr;
+  const double* mu = nullptr;
+  uint64_t T = 0;
+  const double* lam = nullptr;
+  const double* x = nullptr;
+  double wh3 = 0.0;
+  double s = 0.0;
+  double* dpos = nullptr;
+  double* dnrm = nullptr;
+  int accumulate = 0;
+};
+void point_grad2(pr_context* c, const PointGrad2In& a);
+// w[t] = sum of the run's basis values (pair order), runidx[pair] = its run
+void run_weights2(pr_context* c, const uint32_t* run_off, uint64_t T, const uint32_t* sval, const double* phi, double* w,
+                  uint32_t* runidx);
+// mu = h^2 (G M M, M G M, M M G)^T lam at the touched nodes of a dense natural-order grid
+void mu2_dense(pr_context* c, const uint32_t* run_key, uint64_t T, const double* lam, uint32_t D, double* mu);
+// adjoint of an adaptive reconstruction (pr_adaptive.cu): as adjoint_backward, band state
+void adjoint_backward_band(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
+                           double* d_dpos, double* d_dnrm, pr_adjoint_stats& st);
 // adjoint of a degree-2 reconstruction (pr_adjoint.cu): as adjoint_backward, natural-order state
 void adjoint_backward2(pr_context* c, const double* d_q3, uint64_t K, const double* d_dl, double* d_chi,
                        double* d_dpos, double* d_dnrm, pr_adjoint_stats& st);

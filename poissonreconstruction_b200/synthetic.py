@@ -169,15 +169,18 @@ def batch_clouds(count=256, seed=SEED_BASE + 4, lo=10_000, hi=500_000):
 
 
 def union_of_spheres(n=20_000_000, seed=SEED_BASE + 5, count=32, rmin=0.05, rmax=0.3, outlier_frac=0.01,
-                     fp32=True):
+                     fp32=True, sample_seed=None):
     """Large workload: the outer surface of the union of `count` overlapping spheres (centres
     uniform in the unit cube, radii uniform in [rmin, rmax]) with exact outward normals, plus
     `outlier_frac` of the points uniform in the cube with random unit normals; n points in all,
     FP32-rounded.  Surface samples are drawn per sphere in proportion to its area and kept when
-    they lie inside no other sphere."""
+    they lie inside no other sphere.  sample_seed: other samples of the same spheres (the spheres
+    come from `seed`)."""
     rng = _rng(seed)
     c = rng.uniform(0.0, 1.0, (count, 3))
     r = rng.uniform(rmin, rmax, count)
+    if sample_seed is not None:
+        rng = _rng(sample_seed)
     n_out = int(round(outlier_frac * n))
     n_surf = n - n_out
     area = r * r

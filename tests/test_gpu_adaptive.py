@@ -163,19 +163,98 @@ def test_partial_band_against_the_oracle(ctx, precision, capsys):
 
 
 def test_depth12_union_of_spheres(ctx, capsys):
+    """Depth 12 over 9 on 1 M points of the union of spheres with outliers: the mixed-precision
+    solve within 1e-5 of the FP64 one, and the adjoint (mean chi^2 at 50 k other samples of the
+    surface) converged in both precisions with gradients within 1e-3 of each other."""
     pts = synthetic.union_of_spheres(1_000_000)
+    q = synthetic.union_of_spheres(50_000, outlier_frac=0.0, sample_seed=synthetic.SEED_BASE + 56)[:, :3]
     D, Dc = 12, 9
     _, st64 = ctx.reconstruct(pts, _adaptive(D, Dc, precision=prb.PR_PRECISION_FP64, target_rel_residual=1e-6))
     f64 = ctx.band_vector(1)
+    _, dp64, dn64, a64 = ctx.loss_backward(q)
     mesh, st = ctx.reconstruct(pts, _adaptive(D, Dc, target_rel_residual=1e-6))
     f32 = ctx.band_vector(1)
+    _, dp, dn, a32 = ctx.loss_backward(q)
     _, _, codes = ctx.band_info()
     err = np.linalg.norm(f32 - f64) / np.linalg.norm(f64)
+    gp = np.linalg.norm(dp - dp64) / np.linalg.norm(dp64)
+    gn = np.linalg.norm(dn - dn64) / np.linalg.norm(dn64)
     with capsys.disabled():
         print("\nadaptive depth 12 over 9, 1M points: %d bricks (%.3g nodes), mixed %.0f ms (%d PCG, %d refinements, "
-              "relres %.1e), FP64 %.0f ms, coefficient error %.2e, %d triangles, peak %.1f GB"
+              "relres %.1e), FP64 %.0f ms, coefficient error %.2e, %d triangles, peak %.1f GB; adjoint %.0f ms "
+              "(%d PCG), %d of %d queries off the band, gradients mixed vs FP64 %.2e / %.2e"
               % (len(codes), 512.0 * len(codes), 1000 * st.time_total, st.pcg_iterations, st.refinement_steps,
-                 st.rel_residual, 1000 * st64.time_total, err, len(mesh.triangles), st.peak_device_bytes / 1e9))
+                 st.rel_residual, 1000 * st64.time_total, err, len(mesh.triangles), st.peak_device_bytes / 1e9,
+                 1000 * a32.time_total, a32.pcg_iterations, a32.queries_off_band, len(q), gp, gn))
     assert st.converged == 1 and st64.converged == 1
     assert err <= 1e-5
     assert len(mesh.triangles) > 0 and np.all(np.isfinite(mesh.vertices))
+    assert a32.converged == 1 and a64.converged == 1
+    assert gp <= 1e-3 and gn <= 1e-3
+
+
+def _band_params(D, Dc, fp64=True, target=1e-12, **kw):
+    return prb.ReconstructParams(depth=D, coarse_depth=Dc, degree=2, point_weight=4.0, max_iters=400,
+                                 precision=prb.PR_PRECISION_FP64 if fp64 else prb.PR_PRECISION_MIXED,
+                                 target_rel_residual=target, **kw)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_band_adjoint_full_band_is_the_dense_adjoint(ctx):
+    """With every brick active the band system is the dense degree-2 system and the fine function
+    does not depend on the coarse solution (its adjoint right-hand side P^T (E^T g - A lambda)
+    vanishes with the band adjoint's residual): chi and the gradients equal the dense adjoint's."""
+    from tests.adjoint_cases import adjoint_case
+    pts, q, _ = adjoint_case(P=3000, K=800, seed=41)
+    D, Dc = 6, 3
+    ctx.solve(pts, _band_params(D, Dc, band_flags=prb.PR_BAND_FULL))
+    chi_a, dp_a, dn_a, st_a = ctx.loss_backward(q)
+    assert st_a.converged == 1 and st_a.queries_off_band == 0
+    ctx.solve(pts, prb.ReconstructParams(depth=D, degree=2, point_weight=4.0, max_iters=400,
+                                         precision=prb.PR_PRECISION_FP64, target_rel_residual=1e-12))
+    chi_d, dp_d, dn_d, st_d = ctx.loss_backward(q)
+    assert _rel(chi_a, chi_d) <= 1e-9 and abs(st_a.loss - st_d.loss) <= 1e-9 * abs(st_d.loss)
+    assert _rel(dp_a, dp_d) <= 1e-7 and _rel(dn_a, dn_d) <= 1e-7
+
+
+def test_band_adjoint_finite_differences(ctx, capsys):
+    """A partial band (depth 7 over 4): the gradient of mean chi^2 at queries on the surface against
+    fourth-order central differences of the band forward (FP64 solves to 1e-12) on coordinates
+    whose gradient is at least 10% of the largest of its kind, at <= 1e-4 relative; linear in the
+    upstream gradient; the forward state left as it was."""
+    from tests.adjoint_cases import adjoint_case, fd_coordinates, fd_gradient
+    pts, q, rng = adjoint_case(P=4000, K=1000, seed=43)
+    D, Dc = 7, 4
+    p = _band_params(D, Dc)
+    ctx.solve(pts, p)
+    _, _, codes = ctx.band_info()
+    assert 0 < len(codes) < 8 ** (D - 3)
+    f_before = ctx.band_vector(1)
+    chi, dp, dn, st = ctx.loss_backward(q)
+    assert st.converged == 1
+    assert np.array_equal(ctx.band_vector(1), f_before)
+    g1, g2 = rng.standard_normal(len(q)), rng.standard_normal(len(q))
+    _, a1, b1, _ = ctx.loss_backward(q, dl_dchi=g1)
+    _, a2, b2, _ = ctx.loss_backward(q, dl_dchi=g2)
+    _, a12, b12, _ = ctx.loss_backward(q, dl_dchi=2.0 * g1 - g2)
+    assert _rel(a12, 2.0 * a1 - a2) <= 1e-9 and _rel(b12, 2.0 * b1 - b2) <= 1e-9
+
+    def loss(points):
+        ctx.solve(points, p)
+        return ctx.loss_backward(q)[3].loss
+
+    grads = np.hstack([dp, dn])
+    big = [np.abs(grads[:, :3]).max(), np.abs(grads[:, 3:]).max()]
+    coords = [(i, c) for i, c in fd_coordinates(pts, D, rng, 4000) if abs(grads[i, c]) >= 0.1 * big[c // 3]]
+    coords = [coords[k] for k in rng.choice(len(coords), min(12, len(coords)), replace=False)]
+    errs = []
+    for i, col in coords:
+        fd = fd_gradient(loss, pts, i, col)
+        errs.append(abs(fd - grads[i, col]) / abs(grads[i, col]))
+    with capsys.disabled():
+        print("\nband adjoint, depth 7 over 4: %d bricks, %d of %d queries off the band, %d central differences, "
+              "max relative error %.2e" % (len(codes), st.queries_off_band, len(q), len(errs), max(errs)))
+    assert len(errs) >= 8 and max(errs) <= 1e-4, errs

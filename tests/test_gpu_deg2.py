@@ -259,11 +259,6 @@ def test_rejected_combinations(ctx):
     with pytest.raises(prb.ReconstructError) as e:
         ctx.reconstruct(pts, params(4, 4.0, solve_mode=prb.PR_SOLVE_REFERENCE_SCHEDULE))
     assert e.value.code == prb.PR_ERR_INVALID_ARGUMENT
-    # the adjoint covers the dense degree-2 grid, not the adaptive band
-    ctx.solve(pts, params(6, 4.0, coarse_depth=4))
-    with pytest.raises(prb.ReconstructError) as e:
-        ctx.loss_backward(pts[:10, :3], n_points=len(pts))
-    assert e.value.code == prb.PR_ERR_STATE
     # the context still serves degree 1 afterwards
     mesh, st = ctx.reconstruct(pts, prb.ReconstructParams(depth=4, point_weight=4.0))
     assert len(mesh.triangles) > 0
