@@ -11,6 +11,7 @@
 #include <atomic>
 #include <unordered_map>
 #include <map>
+#include <set>
 #include <mutex>
 #include <chrono>
 #include <cstdio>
@@ -435,6 +436,7 @@ struct BatchEngine {
       for (auto& kv : c->bufs)
         if (kv.second.ptr) cudaFree(kv.second.ptr);
       c->bufs.clear();
+      c->free_spare();
       c->bytes_held = 0;
     };
     if (solver) drop(solver);
@@ -677,6 +679,19 @@ void run_packed(int device, const std::map<PackKey, std::vector<uint32_t>>& grou
 }  // namespace
 
 namespace pr {
+std::mutex& spare_mutex() {
+  static std::mutex* m = new std::mutex();  // never destroyed
+  return *m;
+}
+std::set<pr_context*>& context_registry() {  // every live context; guarded by spare_mutex
+  static std::set<pr_context*>* r = new std::set<pr_context*>();
+  return *r;
+}
+void free_all_spare(int device) {
+  std::lock_guard<std::mutex> g(spare_mutex());
+  for (pr_context* c : context_registry())
+    if (c->device == device) c->free_spare_locked();
+}
 bool release_cached_memory(int device) {
   if (t_in_batch) return false;
   BatchEngine& e = batch_engine(device);
@@ -808,6 +823,10 @@ int pr_context_create(int device, void* stream, pr_context** out_ctx) {
       c->own_stream = true;
     }
     PR_CUDA(cudaMallocHost(&c->h_scalars, 64 * sizeof(double)));
+    {
+      std::lock_guard<std::mutex> g(pr::spare_mutex());
+      pr::context_registry().insert(c.get());
+    }
     *out_ctx = c.release();
   });
 }
@@ -820,6 +839,11 @@ int pr_context_destroy(pr_context* c) {
     for (auto& kv : c->bufs)
       if (kv.second.ptr) cudaFree(kv.second.ptr);
     c->bufs.clear();
+    {
+      std::lock_guard<std::mutex> g(pr::spare_mutex());
+      c->free_spare_locked();
+      pr::context_registry().erase(c);
+    }
     for (cudaEvent_t e : c->copy_events)
       if (e) cudaEventDestroy(e);
     c->copy_events.clear();

@@ -122,6 +122,11 @@ struct DBuf {
 // Frees the device memory the batch engine keeps between batches on `device` (pr_abi.cu); false
 // if it holds none or is running.  A failed allocation calls it once and retries.
 bool release_cached_memory(int device);
+// Every context's spare blocks (released, kept for reuse) are guarded by one process-wide lock; a
+// failed allocation frees the spare blocks of every context on its device (pr_abi.cu keeps the
+// registry of contexts) and retries.
+std::mutex& spare_mutex();
+void free_all_spare(int device);
 
 }  // namespace pr
 
@@ -241,30 +246,62 @@ struct pr_context {
     if (bytes == 0) bytes = 16;
     pr::DBuf& b = bufs[name];
     if (b.cap < bytes) {
-      if (b.ptr) {
-        PR_CUDA(cudaStreamSynchronize(stream));
-        PR_CUDA(cudaFree(b.ptr));
-        bytes_held -= b.cap;
+      if (b.ptr) PR_CUDA(cudaStreamSynchronize(stream));
+      std::unique_lock<std::mutex> lk(pr::spare_mutex());
+      if (b.ptr) {  // too small: back to the spare blocks
+        spare.insert({b.cap, b.ptr});
+        spare_bytes += b.cap;
         b.ptr = nullptr;
         b.cap = 0;
       }
       size_t cap = (bytes + 255) & ~size_t(255);
-      cudaError_t e = cudaMalloc(&b.ptr, cap);
-      if (e == cudaErrorMemoryAllocation && pr::release_cached_memory(device)) {
-        cudaGetLastError();
-        e = cudaMalloc(&b.ptr, cap);
+      auto it = spare.lower_bound(cap);  // the smallest spare block that holds it, if not far larger
+      if (it != spare.end() && it->first <= 2 * cap + (size_t(64) << 20)) {
+        b.ptr = it->second;
+        b.cap = it->first;
+        spare_bytes -= it->first;
+        spare.erase(it);
+      } else {
+        lk.unlock();
+        cudaError_t e = cudaMalloc(&b.ptr, cap);
+        if (e == cudaErrorMemoryAllocation) {  // every context's spare blocks, then the batch engine's
+          cudaGetLastError();
+          pr::free_all_spare(device);
+          e = cudaMalloc(&b.ptr, cap);
+          if (e == cudaErrorMemoryAllocation && pr::release_cached_memory(device)) {
+            cudaGetLastError();
+            e = cudaMalloc(&b.ptr, cap);
+          }
+        }
+        lk.lock();
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          b.ptr = nullptr;
+          throw pr::Error(PR_ERR_OUT_OF_MEMORY, "cudaMalloc(" + std::to_string(cap) + " bytes) for '" + name +
+                                                    "' failed: " + cudaGetErrorString(e));
+        }
+        b.cap = cap;
+        bytes_held += cap;
       }
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        b.ptr = nullptr;
-        throw pr::Error(PR_ERR_OUT_OF_MEMORY, "cudaMalloc(" + std::to_string(cap) + " bytes) for '" + name +
-                                                  "' failed: " + cudaGetErrorString(e));
-      }
-      b.cap = cap;
-      bytes_held += cap;
-      if (bytes_held > peak_bytes) peak_bytes = bytes_held;
+      const size_t live = bytes_held - spare_bytes;
+      if (live > peak_bytes) peak_bytes = live;
     }
     return reinterpret_cast<T*>(b.ptr);
+  }
+  // Released blocks stay allocated and serve later requests of a similar size (cudaMalloc and
+  // cudaFree synchronise the device and cost milliseconds per GB at this size); they are freed
+  // when an allocation fails or the context is destroyed.  peak_bytes counts live buffers only.
+  std::multimap<size_t, void*> spare;
+  size_t spare_bytes = 0;
+  void free_spare() {
+    std::lock_guard<std::mutex> g(pr::spare_mutex());
+    free_spare_locked();
+  }
+  void free_spare_locked() {  // the caller holds spare_mutex (spare blocks are idle: their stream was synchronised)
+    for (auto& kv : spare) cudaFree(kv.second);
+    bytes_held -= spare_bytes;
+    spare.clear();
+    spare_bytes = 0;
   }
   template <typename T>
   T* get(const std::string& name) {
@@ -276,8 +313,9 @@ struct pr_context {
     auto it = bufs.find(name);
     if (it == bufs.end() || !it->second.ptr) return;
     PR_CUDA(cudaStreamSynchronize(stream));
-    PR_CUDA(cudaFree(it->second.ptr));
-    bytes_held -= it->second.cap;
+    std::lock_guard<std::mutex> g(pr::spare_mutex());
+    spare.insert({it->second.cap, it->second.ptr});
+    spare_bytes += it->second.cap;
     bufs.erase(it);
   }
   void sync() { PR_CUDA(cudaStreamSynchronize(stream)); }
