@@ -21,6 +21,8 @@ marching cubes) of that cloud.
   accuracy   coefficient relative L2 of the mixed and FP64 solutions against each other and
              against an FP64 solve to 1e-10, the largest mixed target meeting 1e-6, and the
              vertex distance between the two meshes over the bbox diagonal (untimed)
+  degree1    the same cloud with the crate's basis (linear B-splines): device-resident step,
+             mixed and FP64 solves, and its finest-level solver kernels timed alone
   cpu_baseline  measured on the host: iterations of the crate's CG loop (oracle restatement,
              FP64, all host threads) on the same depth-10 degree-2 system, one iteration timed
              per sample and reported as points / (one iteration's time), an upper bound on the
@@ -698,11 +700,18 @@ def run_ours(a):
         m1_64, s1_64 = device_steps(q1_64, max(1, k64), True)
         t1 = statistics.mean(x.time_solve for x in s1)
         t1_64 = statistics.mean(x.time_solve for x in s1_64)
+        # the degree-1 finest-level solver kernels, each timed alone as above (FP32)
+        k1 = {}
+        for nm in ("smooth_prolong_dot", "cg_update_presmooth", "resid_restrict", "spmv_xpby", "spmv"):
+            ms, by = ctx.kernel_bench(nm, a.depth, prb.PR_PRECISION_MIXED, a.roofline_reps)
+            k1[nm] = {"ms_per_launch": ms, "algorithmic_bytes": by, "achieved_gbs": by / (ms / 1000.0) / 1e9,
+                      "frac": by / (ms / 1000.0) / 1e9 / peak}
         other = {"degree": 1, "value": total_points / (reduce_max(dist, statistics.mean(m1), dev) / 1000.0),
                  "unit": "points/s", "ms_per_step": statistics.mean(m1), "solve_ms": 1000.0 * t1,
                  "solve_gbs": s1[-1].solve_bytes / t1 / 1e9 if t1 > 0 else None,
                  "pcg_iterations": s1[-1].pcg_iterations, "rel_residual": s1[-1].rel_residual,
-                 "fp64_solve_ms": 1000.0 * t1_64, "mixed_vs_fp64_solve_speedup": t1_64 / t1 if t1 > 0 else None}
+                 "fp64_solve_ms": 1000.0 * t1_64, "mixed_vs_fp64_solve_speedup": t1_64 / t1 if t1 > 0 else None,
+                 "kernels": k1}
 
     # the adjoint workload (1,000,000 superquadric points, depth 9, loss = mean chi^2 at 200,000
     # surface points): forward solve and backward pass timed on the host clock (mixed precision,
