@@ -165,8 +165,18 @@ def test_reference_schedule_mode(ctx):
           % (dev, dev_conv))
     assert np.all(np.isfinite(x_gpu)) and len(mesh.triangles) > 0
     assert dev < max(0.5, 2 * dev_conv)
-    # coarse RHS of the schedule is bit-exact with the crate's build_system_at_depth
     assert st.pcg_iterations > 0
+    # the schedule's coarse right-hand side (depth D - 2) is bit-exact with the oracle's
+    # restatement of build_system_at_depth (src/fem_tree.rs:386-402); the oracle's coarse vectors
+    # are lexicographic (x fastest), the GPU's Morton
+    dc, brhs_gpu = ctx.coarse_rhs()
+    assert dc == depth - 2
+    res = 1 << dc
+    z, y, x = np.meshgrid(np.arange(res), np.arange(res), np.arange(res), indexing="ij")
+    m = np.array([oracle.morton(int(a), int(b), int(c)) for a, b, c in zip(x.ravel(), y.ravel(), z.ravel())])
+    brhs_ref = np.empty(res ** 3)
+    brhs_ref[m] = t.coarse_rhs(pw)
+    assert np.array_equal(brhs_gpu, brhs_ref), "coarse right-hand side differs from build_system_at_depth"
 
 
 @pytest.mark.parametrize("depth", [1, 2, 3])
