@@ -1100,8 +1100,8 @@ constexpr size_t smem_bytes() {
 // the sweep.  Every level's interior stencil has no face couplings, so nodes that share the
 // parity of x and y are uncoupled along z: the sweep has 4 phases, one per (x, y) parity class,
 // each relaxing whole columns of that class at once (forward order (0,0) (1,0) (0,1) (1,1),
-// backward the reverse, each the adjoint of the other).  Thread = one 2x2 quad column over 4 z
-// planes of the SpMV's tile; in phase k it relaxes the class-k column of its quad, sweeping
+// backward the reverse, each the adjoint of the other).  Thread = one 2x2 quad column over ZT z
+// planes of a parity-split tile (below); in phase k it relaxes the class-k column of its quad, sweeping
 // the planes once: a plane's ring around the column gives its in-plane edge sum D (diagonals)
 // and face-adjacent sum F, and the node at z uses D(z), F(z-1), F(z+1), D(z-1), D(z+1).
 // FACES (coarse levels): nodes on the low domain faces use their 27-entry table row, which does
@@ -1109,20 +1109,23 @@ constexpr size_t smem_bytes() {
 // values are written after a barrier), a Jacobi step along the column for those rows only.
 namespace g16 {
 constexpr int CW = s16::CW;  // ZT, NT: as n16 (a node's relaxation is the same for every ZT)
-using n16::nat;
-using n16::PS;
-using n16::RS;
-using n16::TILE;
+// Parity-split tile (u = local + 1 in 0..17 per axis): each row holds its even columns (u even)
+// first, then its odd ones, HS words each, so the columns of one class that a warp relaxes
+// (x0 = 0, 2, .., 14: stride 2 in x) are consecutive words, and its four quad rows (y two apart,
+// 2 RS = 40 words = 8 banks apart) fill the 32 banks once: every tile access of a phase is free
+// of bank conflicts for FP32, and per half-warp for FP64.
+constexpr int HS = 10, RS = 2 * HS, PS = 18 * RS + 4, TILE = 18 * PS;
+__device__ __forceinline__ int col(int ux) { return (ux & 1) * HS + (ux >> 1); }
+__device__ __forceinline__ int nat(int ux, int uy, int uz) { return uz * PS + uy * RS + col(ux); }
 
 // One phase: new values of the class-CLS column of the thread's quad (planes z0..z0+ZT-1).
 // On the thread's own planes the ring members inside its quad come from registers (v), the
-// other five from the tile (a pair and three scalars); the two halo planes read all eight.
+// other five from the tile; the two halo planes read all eight.
 // ZERO: a forward sweep from zero, in which the classes after CLS are still zero everywhere
 // (their loads are skipped; phase 0 needs none).
 template <typename T, int CLS, bool ZERO, int ZT>
 __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int z0, const T (&fv)[ZT][4],
                                              const T (&v)[ZT][4], T ce, T cc, T c0inv, T (&nv)[ZT]) {
-  typedef typename n16::Pair<T>::type P2;
   constexpr int CX = CLS & 1, CY = CLS >> 1;
   constexpr int EDX = CX == 0 ? -1 : 1, EDY = CY == 0 ? -1 : 1;  // direction of the external ring side
   constexpr int EFX = (CX ^ 1) | (CY << 1), EFY = CX | ((CY ^ 1) << 1), ED = (CX ^ 1) | ((CY ^ 1) << 1);
@@ -1133,8 +1136,11 @@ __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int 
     for (int k = 0; k < ZT; ++k) nv[k] = fv[k][CLS] * c0inv;
     return;
   }
-  const int x = x0 + CX, y = y0 + CY;
-  const T* rbase = tile + nat(x, y, 0);  // ring row y-1, column x-1 of tile plane 0
+  // the ring's columns x-1, x, x+1 (x = x0 + CX, tile column x + 1; x0 even): their row offsets
+  const int xh = x0 >> 1;
+  const int cm = CX * HS + xh, cz = (1 - CX) * HS + xh + CX, cp = CX * HS + xh + 1;
+  const int cxe = EDX < 0 ? cm : cp;  // the external column x + EDX
+  const T* rbase = tile + (y0 + CY) * RS;  // ring row y-1 of tile plane 0
   T Dm = 0, Fm = 0, D0 = 0, F0 = 0;
 #pragma unroll
   for (int p = 0; p < ZT + 2; ++p) {  // local plane z0 + p - 1
@@ -1144,39 +1150,21 @@ __device__ __forceinline__ void relax_column(const T* tile, int x0, int y0, int 
       const int k = p - 1;
       const T* rr = r0 + (EDY + 1) * RS;  // external row: columns x-1, x, x+1
       T q0 = 0, q1 = 0, q2 = 0;
-      if (ND || NFY) {
-        if (CX == 0) {
-          const P2 pr = *reinterpret_cast<const P2*>(rr);
-          q0 = pr.x;
-          q1 = pr.y;
-          if (ND) q2 = rr[2];
-        } else {
-          const P2 pr = *reinterpret_cast<const P2*>(rr + 1);
-          if (ND) q0 = rr[0];
-          q1 = pr.x;
-          q2 = pr.y;
-        }
+      if (ND) {
+        q0 = rr[cm];
+        q2 = rr[cp];
       }
+      if (NFY) q1 = rr[cz];
       // the same pairing as a halo plane's (row y-1 pair + row y+1 pair), so that a node's sums
       // do not depend on which of its planes are a thread's own
-      if (ND) Dp = (q0 + q2) + (r0[(1 - EDY) * RS + EDX + 1] + v[k][ED]);
+      if (ND) Dp = (q0 + q2) + (r0[(1 - EDY) * RS + cxe] + v[k][ED]);
       if (NFY) Fp += q1 + v[k][EFY];
-      if (NFX) Fp += r0[RS + EDX + 1] + v[k][EFX];
+      if (NFX) Fp += r0[RS + cxe] + v[k][EFX];
     } else {  // halo plane: the whole ring from the tile
-      T a0, a1, a2, c0v, c1, c2;
-      if (CX == 0) {
-        const P2 pa = *reinterpret_cast<const P2*>(r0);
-        const P2 pc = *reinterpret_cast<const P2*>(r0 + 2 * RS);
-        a0 = pa.x; a1 = pa.y; a2 = r0[2];
-        c0v = pc.x; c1 = pc.y; c2 = r0[2 * RS + 2];
-      } else {
-        const P2 pa = *reinterpret_cast<const P2*>(r0 + 1);
-        const P2 pc = *reinterpret_cast<const P2*>(r0 + 2 * RS + 1);
-        a0 = r0[0]; a1 = pa.x; a2 = pa.y;
-        c0v = r0[2 * RS]; c1 = pc.x; c2 = pc.y;
-      }
+      const T a0 = r0[cm], a1 = r0[cz], a2 = r0[cp];
+      const T c0v = r0[2 * RS + cm], c1 = r0[2 * RS + cz], c2 = r0[2 * RS + cp];
       Dp = (a0 + a2) + (c0v + c2);
-      Fp = (a1 + c1) + (r0[RS] + r0[RS + 2]);
+      Fp = (a1 + c1) + (r0[RS + cm] + r0[RS + cp]);
     }
     if (p >= 2) {  // node at local z0 + p - 2: edges D0 + Fm + Fp, corners Dm + Dp
       const int k = p - 2;
@@ -1284,11 +1272,11 @@ __global__ void __launch_bounds__(n16::Zt<ZT>::NT, (sizeof(T) == 4 ? 4 : 2) * ZT
   }
 #pragma unroll
   for (int k = 0; k < ZT; ++k) {
-    T* p0 = tile + nat(x0 + 1, y0 + 1, z0 + k + 1);
-    p0[0] = v[k][0];
-    p0[1] = v[k][1];
-    p0[RS] = v[k][2];
-    p0[RS + 1] = v[k][3];
+    T* p0 = tile + nat(0, y0 + 1, z0 + k + 1);
+    p0[col(x0 + 1)] = v[k][0];
+    p0[col(x0 + 2)] = v[k][1];
+    p0[RS + col(x0 + 1)] = v[k][2];
+    p0[RS + col(x0 + 2)] = v[k][3];
   }
   s16::load_halo<NT>(tile, xi, nb, [](int ux, int uy, int uz) { return nat(ux, uy, uz); },
                     [&](uint32_t m) -> T { return FROM_ZERO ? (T)0 : __ldg(xi + m); });
@@ -1324,12 +1312,11 @@ __global__ void __launch_bounds__(n16::Zt<ZT>::NT, (sizeof(T) == 4 ? 4 : 2) * ZT
         const int mask = ((ox + x) == 0) | (((oy + y) == 0) << 1) | (((oz + z) == 0) << 2);
         if (!mask) continue;
         const T* cm = table + 27 * mask;
-        const int ei = nat(x + 1, y + 1, z + 1);
         T off = 0;
 #pragma unroll 1
         for (int o = 0; o < 27; ++o) {
           if (o == 13) continue;
-          off += cm[o] * tile[ei + (o % 3 - 1) + RS * ((o / 3) % 3 - 1) + PS * (o / 9 - 1)];
+          off += cm[o] * tile[nat(x + 1 + (o % 3 - 1), y + 1 + ((o / 3) % 3 - 1), z + 1 + (o / 9 - 1))];
         }
         T fk = fv[0][cls];
 #pragma unroll
