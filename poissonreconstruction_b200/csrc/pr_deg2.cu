@@ -877,20 +877,30 @@ __global__ void __launch_bounds__(kThreadsR) k_op3r(const __grid_constant__ CUte
   double dacc = 0.0;
   int it = 0;
   bool stop = false;
+  // kOpApplyD with xmode 2: the iterate's rows of the staged plane zin = z0 - 2 + it, loaded one
+  // plane ahead (issued while the previous plane is filtered) so the load latency stays hidden
+  // (the first staged plane that is one of this CTA's comes at it = 2, so nothing is loaded before
+  // the loop)
+  const bool xread = two && A.xmode == 2;
+  V2 xnext[RY];
+#pragma unroll
+  for (int j = 0; j < RY; ++j) xnext[j] = V2{T(0), T(0)};
   for (int g = 0; g < ngroups; ++g) {
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
       it = g * NS + k;
       const bool emit = (unsigned)(it - 4) < (unsigned)(z1 - z0);
       // kOpApplyD: xacc += s2 dold on the staged plane zin = zo + 2 when it is one of this CTA's
-      // planes (the iterate of those rows, loaded before the wait)
+      // planes (the iterate of those rows, loaded one plane ahead)
       const bool own = (unsigned)(it - 2) < (unsigned)(z1 - z0);  // staged plane zin is one of this CTA's
       const bool upd = two && A.xmode && own;
       V2 xold[RY];
 #pragma unroll
       for (int j = 0; j < RY; ++j) {
-        xold[j] = V2{T(0), T(0)};
-        if (upd && A.xmode == 2) xold[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + 2 * plane + (int64_t)j * res);
+        xold[j] = xnext[j];
+        xnext[j] = V2{T(0), T(0)};
+        if (xread && (unsigned)(it + 1 - 2) < (unsigned)(z1 - z0))
+          xnext[j] = *reinterpret_cast<const V2*>(A.xacc + (op - out) + 3 * plane + (int64_t)j * res);
       }
       if (!mbar_wait(&bar[k], (uint32_t)g & 1u)) {
         atomicExch(A.err, 1);
