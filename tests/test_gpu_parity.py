@@ -148,6 +148,47 @@ def test_pipeline_mesh_vs_oracle(ctx, name):
         assert np.quantile(d, 0.99) <= VERT_TOL * diag
 
 
+def _open_edges(tri):
+    """Edges used by exactly one triangle (0 for a closed mesh)."""
+    e = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]])
+    e.sort(axis=1)
+    _, cnt = np.unique(e, axis=0, return_counts=True)
+    return int((cnt == 1).sum())
+
+
+def test_scale_clipping_vs_oracle(ctx, capsys):
+    """The unit-cube scale (src/geometry.rs:384-402; default 1.1, src/reconstructor.rs:14): at 1.1
+    the longest axis maps to [-0.05, 1.05]: a sample outside the unit cube splats only onto its
+    cell corners that lie on the grid (src/fem_tree.rs:148-153), and marching cubes covers only the
+    cube, so the sphere's mesh is clipped open at the six extremes; at 0.9 every sample is inside.  Both scales against the oracle's reconstruct (iso value,
+    vertices, and the count of edges used by one triangle only)."""
+    depth, pw = 5, 4.0
+    pts = clouds()["sphere"]
+    lo, hi = pts[:, :3].min(0), pts[:, :3].max(0)
+    diag = np.linalg.norm(hi - lo)
+    opened = {}
+    for scale in (0.9, 1.1):
+        mesh, st = run(ctx, pts, depth, pw, scale=scale, target_rel_residual=1e-10)
+        v_ref, t_ref, st_ref, _ = oracle.reconstruct(pts, depth=depth, scale=scale, point_weight=pw, solve_mode=1,
+                                                      target_rel_residual=1e-13, want_coeffs=True)
+        assert abs(st.iso_value - st_ref["iso_value"]) <= ISO_TOL * abs(st_ref["iso_value"])
+        if mesh.triangles.shape == t_ref.shape and np.array_equal(mesh.triangles, t_ref):
+            assert np.max(np.abs(mesh.vertices - v_ref)) <= VERT_TOL * diag
+            assert _open_edges(mesh.triangles) == _open_edges(t_ref)
+        else:  # a corner value within rounding of iso flipped: compare nearest vertices
+            from scipy.spatial import cKDTree
+            d, _ = cKDTree(v_ref).query(mesh.vertices)
+            assert np.quantile(d, 0.99) <= VERT_TOL * diag
+        unit, _ = oracle.to_unit(pts, scale)
+        outside = int(np.any((unit[:, :3] < 0.0) | (unit[:, :3] >= 1.0), axis=1).sum())
+        opened[scale] = _open_edges(mesh.triangles)
+        with capsys.disabled():
+            print("\nscale %.1f: %d of %d samples outside the unit cube, %d triangles, %d edges used once"
+                  % (scale, outside, len(pts), len(mesh.triangles), opened[scale]))
+        assert (outside > 0) == (scale > 1.0)
+    assert opened[1.1] > opened[0.9]
+
+
 def test_reference_schedule_mode(ctx):
     """The crate's cascade with 8-colour GS: tracked against the oracle's sequential-GS
     schedule (deviation reported, not gated) and against the converged solution."""
