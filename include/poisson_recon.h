@@ -103,7 +103,7 @@ typedef struct pr_stats {
   uint32_t refinement_steps;    /* FP64 outer residual steps (mixed precision) */
   uint64_t points_in_cube;      /* points with at least one screening node */
   double solve_bytes;           /* algorithmic HBM bytes moved by the solve */
-  double peak_device_bytes;     /* peak device memory held by the context */
+  double peak_device_bytes;     /* peak device memory of the context's live buffers (spare blocks kept for reuse not counted) */
   int32_t converged;            /* converged mode: 1 if rel_residual <= target_rel_residual */
   int32_t reserved_i;
   double time_mesh_copy;        /* seconds copying the mesh to the caller's host memory */
