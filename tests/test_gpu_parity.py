@@ -2,7 +2,7 @@
 
 Bit-exact: unit-cube transform, normal splat, right-hand side, implicit-function
 evaluation, marching-cubes vertices and triangles given identical coefficients and iso.
-Tolerance (north-star): solved coefficients relative L2 <= 1e-6 against the FP64 oracle
+Tolerance (the workloads' accuracy targets): solved coefficients relative L2 <= 1e-6 against the FP64 oracle
 solve of the same fine system; iso relative 1e-9; vertices <= 1e-5 x bbox diagonal.
 """
 import numpy as np
